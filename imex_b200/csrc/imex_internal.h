@@ -1,0 +1,134 @@
+// Internal declarations shared by the CUDA sources of libimex_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "../../include/imex_b200.h"
+
+namespace imex {
+
+constexpr int kMaxRK = 3;
+constexpr int kMaxKrylov = 32;  // upper bound on gmres_restart (reference: 25)
+
+// Solver constants of one context, passed to kernels by value.
+struct DevParams {
+  int nx, ny;
+  long long N;  // nx * ny
+  double dx, dy, hmin;
+  int formula, magfield, recon, reconstate, vortex_minmod, GLF, add_bvisc, add_pvisc;
+  int U_update, PressureSolver, Energy_Modify, floor_on, Pnewton_max, eos_type, caltimestep, RKs;
+  double gamma, m_alfa, m_b, m_R, m_cv;
+  double p_floor, Mbig_fac, theta, Pnewton_tol, shock_kappa1, GMREStol, CFL, time_stop, fixed_dt;
+};
+
+// Scalars living in device memory (the reference's hidden globals).
+struct DevScalars {
+  double dt, adt, B_max_x, B_max_y, vx_max, vy_max, v_max, a_max;
+  double ch, ch_x, ch_y, cA, cA_x, cA_y, t, prev_dt, Mbig;
+  double gmax_bx, gmax_by;  // A-form viscosity maxima of the current solve
+  double h;                 // implicit step of the current sub-step
+  int timestep;
+  int pad;
+};
+
+// Device-side counters and status of the implicit solves.
+struct DevStats {
+  int gmres_solves, gmres_iters, gmres_restarts, newton_iters, max_floored, refine_sweeps;
+  int status;      // worst imex_status
+  int barrier_fail;
+  double last_residual, min_p;
+};
+
+// Grid-barrier and reduction workspace of the persistent solver kernels.
+struct SyncState {
+  unsigned int count;
+  unsigned int generation;
+  int abort;
+  int pad;
+};
+
+}  // namespace imex
+
+struct imex_ctx {
+  imex_config cfg{};
+  imex::DevParams P{};
+  int nx = 0, ny = 0;
+  size_t N = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int num_sms = 0;
+
+  // device state (interior planes)
+  double *prim = nullptr, *cons = nullptr, *cons_n = nullptr, *Qe = nullptr, *Qs = nullptr;
+  double *bx = nullptr, *by = nullptr, *bx_n = nullptr, *by_n = nullptr, *bxQe = nullptr, *byQe = nullptr;
+  double *bxQs = nullptr, *byQs = nullptr, *Fx = nullptr, *Fy = nullptr;
+  double *A = nullptr, *A_s = nullptr, *A_e = nullptr, *A_snap = nullptr;
+  double *Hs = nullptr, *HsA = nullptr, *HsB = nullptr, *w = nullptr, *Bsave = nullptr;
+  // per-stage derived planes
+  double *pe = nullptr;    // pressure of Qe
+  double *hQe = nullptr;   // enthalpy e + p/rho of Qe
+  // implicit-solve planes
+  double *hh = nullptr, *eta = nullptr, *vscale = nullptr, *tdiag = nullptr, *vdiag = nullptr;
+  double *rv = nullptr;    // rho v* snapshot (3 planes)
+  double *pb = nullptr, *pp = nullptr, *pf = nullptr, *pg = nullptr, *pdp = nullptr;  // pressure vectors
+  double *mx = nullptr, *mb = nullptr;  // magnetic solution / rhs (3 planes each)
+  double *chit = nullptr, *Epp = nullptr, *Et = nullptr;
+  // GMRES workspace
+  double* V = nullptr;      // (restart + 1) * 3 planes
+  double* AV = nullptr;     // 2 * 3 planes
+  double* partial = nullptr;
+  int max_blocks = 0;
+  float* Vf = nullptr;      // FP32 basis (mixed precision)
+  float* AVf = nullptr;
+  double* mres = nullptr;   // refinement residual (3 planes)
+  double* mcor = nullptr;   // refinement correction (3 planes)
+  // scalars and stats
+  imex::DevScalars* sc = nullptr;
+  imex::DevStats* st = nullptr;
+  imex::SyncState* sync = nullptr;
+  imex::DevScalars* h_sc = nullptr;  // pinned mirrors
+  imex::DevStats* h_st = nullptr;
+  double* red = nullptr;    // small reduction buffer (device)
+  double* h_red = nullptr;  // pinned mirror
+  std::vector<void*> allocations;
+};
+
+namespace imex {
+
+// error helpers
+imex_status set_error(imex_ctx* ctx, imex_status s, const std::string& msg);
+imex_status cuda_check(imex_ctx* ctx, cudaError_t e, const char* what);
+
+// launchers implemented in kernels_stage.cu
+imex_status launch_step_prologue(imex_ctx* ctx);
+imex_status launch_stage_combine(imex_ctx* ctx, int rks);
+imex_status launch_reconstruct(imex_ctx* ctx);
+imex_status launch_flux_update(imex_ctx* ctx, int pressure_form);
+imex_status launch_stage_derivative(imex_ctx* ctx, int rks);
+imex_status launch_ct(imex_ctx* ctx, int variant);
+imex_status launch_prim_from_cons(imex_ctx* ctx);
+imex_status launch_cons_from_prim(imex_ctx* ctx);
+imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta);
+imex_status launch_divergence(imex_ctx* ctx, double* out4);
+imex_status launch_min_pressure(imex_ctx* ctx, double* pmin);
+imex_status launch_qe_derived(imex_ctx* ctx);
+imex_status launch_vslope(imex_ctx* ctx);
+
+// launchers implemented in kernels_solve.cu
+// the implicit step h of these sub-steps is read from device scalars (set_h or the stage combination)
+imex_status set_h(imex_ctx* ctx, double h);
+imex_status run_mag_subsystem_B(imex_ctx* ctx);
+imex_status run_mag_subsystem_A(imex_ctx* ctx);
+imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks);
+imex_status prepare_operator(imex_ctx* ctx, int op, double h);
+imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax);
+imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b);
+imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b);
+imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig);
+
+}  // namespace imex

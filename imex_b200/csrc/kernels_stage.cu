@@ -1,0 +1,793 @@
+// Explicit parts of one IMEX stage: step prologue (global wave-speed maxima
+// and dt), stage combination, reconstruction, the two explicit flux updates,
+// constrained transport, stage derivative, and diagnostics.
+//
+// Every kernel here is a memory-bound stencil over interior-only SoA planes
+// with periodic wrap-around (no ghost cells): one thread per cell, loads
+// through the read-only path so the stencil neighbours hit L1.
+#include <cstdio>
+#include <cstring>
+
+#include "device_common.cuh"
+
+namespace imex {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+// ---------------------------------------------------------------- reductions
+template <typename T, typename F>
+__device__ inline T warp_reduce(T v, F f) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = f(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+struct FMax {
+  __device__ double operator()(double a, double b) const { return fmax(a, b); }
+};
+struct FMin {
+  __device__ double operator()(double a, double b) const { return fmin(a, b); }
+};
+struct FSum {
+  __device__ double operator()(double a, double b) const { return a + b; }
+};
+// block-wide reduction of K values; result valid in thread 0
+template <int K, typename F>
+__device__ inline void block_reduce(double (&v)[K], F f, double identity) {
+  __shared__ double sh[K][kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double r = warp_reduce(v[k], f);
+    if (lane == 0) sh[k][wid] = r;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double r = lane < (int)(blockDim.x >> 5) ? sh[k][lane] : identity;
+      v[k] = warp_reduce(r, f);
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- step prologue
+// calch / calca / caldt maxima / MagneticEigenvalues over the primitive state,
+// timestep.cpp:5-148,254-273.  Max is exact, so block order does not matter.
+constexpr int kStepVals = 11;
+__global__ void k_step_reduce(DevParams P, const double* __restrict__ prim, double* __restrict__ partial) {
+  double v[kStepVals];
+  v[0] = v[1] = v[2] = v[3] = v[4] = v[5] = 1e-8;  // ch_x ch_y ch cA_x cA_y cA
+  v[6] = v[7] = v[8] = v[9] = v[10] = 0.0;         // |vx| |vy| |v| bmax_x bmax_y
+  const long long N = P.N;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+    double p[8];
+    load_cell<8>(prim, N, n, p);
+    double B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
+    double B = sqrt(B2);
+    double vv = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+    double cfx = eos_fast(P, p[0], p[4], p[5], B2);
+    double cfy = eos_fast(P, p[0], p[4], p[6], B2);
+    double cf = eos_fast(P, p[0], p[4], B, B2);
+    v[0] = fmax(v[0], p[1] + cfx);
+    v[1] = fmax(v[1], p[2] + cfy);
+    v[2] = fmax(v[2], vv + cf);
+    v[3] = fmax(v[3], p[5] / sqrt(p[0]));
+    v[4] = fmax(v[4], p[6] / sqrt(p[0]));
+    v[5] = fmax(v[5], B / sqrt(p[0]));
+    v[6] = fmax(v[6], fabs(p[1]));
+    v[7] = fmax(v[7], fabs(p[2]));
+    v[8] = fmax(v[8], vv);
+    v[9] = fmax(v[9], 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4 * B2 / p[0])));
+    v[10] = fmax(v[10], 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4 * B2 / p[0])));
+  }
+  block_reduce(v, FMax(), -INFINITY);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kStepVals; ++k) partial[blockIdx.x * kStepVals + k] = v[k];
+}
+
+// caldt (timestep.cpp:5-67) + main.cpp:341-353 on one thread
+__global__ void k_step_finalize(DevParams P, const double* __restrict__ partial, int nblk, DevScalars* sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double v[kStepVals];
+  for (int k = 0; k < kStepVals; ++k) v[k] = partial[k];
+  for (int b = 1; b < nblk; ++b)
+    for (int k = 0; k < kStepVals; ++k) v[k] = fmax(v[k], partial[b * kStepVals + k]);
+  sc->timestep += 1;
+  const int ts = sc->timestep;
+  sc->ch_x = v[0];
+  sc->ch_y = v[1];
+  sc->ch = v[2];
+  sc->cA_x = v[3];
+  sc->cA_y = v[4];
+  sc->cA = v[5];
+  sc->vx_max = v[6];
+  sc->vy_max = v[7];
+  sc->v_max = v[8];
+  const int full_step = 1;
+  double a_max;
+  if (P.caltimestep == IMEX_Fullydt) a_max = sc->ch;
+  else if (P.caltimestep == IMEX_Alfvendt) a_max = (ts < full_step + 1) ? sc->ch : sc->cA;
+  else a_max = (ts < full_step + 1) ? sc->ch : sc->v_max;
+  double dt = P.CFL * 1 / (2 * a_max / fmin(P.dx, P.dy));
+  if (ts > 1 && sc->prev_dt > 0.0) dt = fmin(dt, 2.0 * sc->prev_dt);
+  sc->prev_dt = dt;
+  if (ts > full_step) a_max = sc->v_max;
+  sc->a_max = a_max;
+  dt = fmin(dt, P.time_stop - sc->t);
+  if (P.fixed_dt > 0.0) dt = fmin(P.fixed_dt, P.time_stop - sc->t);
+  sc->dt = dt;
+  sc->B_max_x = v[9];
+  sc->B_max_y = v[10];
+  sc->t = sc->t + dt;
+}
+
+// cons = pri2con(prim); cons_n = cons  (main.cpp:356-358)
+__global__ void k_cons_from_prim(DevParams P, const double* __restrict__ prim, double* __restrict__ cons,
+                                 double* __restrict__ cons_n) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  double p[8], c[8];
+  load_cell<8>(prim, P.N, n, p);
+  pri2con(P, c, p);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    cons[k * P.N + n] = c[k];
+    if (cons_n) cons_n[k * P.N + n] = c[k];
+  }
+}
+__global__ void k_prim_from_cons(DevParams P, const double* __restrict__ cons, double* __restrict__ prim) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  double p[8], c[8];
+  load_cell<8>(cons, P.N, n, c);
+  con2pri(P, p, c);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) prim[k * P.N + n] = p[k];
+}
+
+// ---------------------------------------------------------------- stage combination
+struct Tableau {
+  double ae[kMaxRK], ai[kMaxRK], aii;
+};
+// Qe, Qs, face and A stage states (main.cpp:368-414), plus the pressure and
+// enthalpy of Qe that the implicit sub-systems freeze for the stage.
+__global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc, const double* __restrict__ cons_n,
+                                const double* __restrict__ Hs, const double* __restrict__ bx_n,
+                                const double* __restrict__ by_n, const double* __restrict__ HsB,
+                                const double* __restrict__ A_snap, const double* __restrict__ HsA,
+                                double* __restrict__ Qe, double* __restrict__ Qs, double* __restrict__ bxQe,
+                                double* __restrict__ byQe, double* __restrict__ bxQs, double* __restrict__ byQs,
+                                double* __restrict__ A_s, double* __restrict__ A_e, double* __restrict__ A,
+                                double* __restrict__ pe, double* __restrict__ hQe) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double dt = sc->dt;
+  if (n == 0) {
+    sc->adt = T.aii * dt;
+    sc->h = T.aii * dt;
+  }
+  if (n >= N) return;
+  double qe[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double e = cons_n[k * N + n], s = e;
+    for (int r = 0; r < rks; ++r) {
+      double h = Hs[((long long)r * 8 + k) * N + n];
+      e = e + T.ae[r] * dt * h;
+      s = s + T.ai[r] * dt * h;
+    }
+    qe[k] = e;
+    Qe[k * N + n] = e;
+    Qs[k * N + n] = s;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double e = A_snap[k * N + n], s = e;
+    for (int r = 0; r < rks; ++r) {
+      double h = HsA[((long long)r * 3 + k) * N + n];
+      e += T.ae[r] * dt * h;
+      s += T.ai[r] * dt * h;
+    }
+    A_e[k * N + n] = e;
+    A_s[k * N + n] = s;
+    A[k * N + n] = s;
+  }
+  double fxe = bx_n[n], fxs = fxe, fye = by_n[n], fys = fye;
+  for (int r = 0; r < rks; ++r) {
+    double h0 = HsB[((long long)r * 2 + 0) * N + n], h1 = HsB[((long long)r * 2 + 1) * N + n];
+    fxe += T.ae[r] * dt * h0;
+    fye += T.ae[r] * dt * h1;
+    fxs += T.ai[r] * dt * h0;
+    fys += T.ai[r] * dt * h1;
+  }
+  bxQe[n] = fxe;
+  byQe[n] = fye;
+  bxQs[n] = fxs;
+  byQs[n] = fys;
+  double e = calecon(qe);
+  double p = eos_p(P, qe[0], e);
+  pe[n] = p;
+  hQe[n] = e + p / qe[0];
+}
+
+// ---------------------------------------------------------------- reconstruction
+// TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes.
+// nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
+__global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  long long ix[5], iy[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    ix[d] = cid(P, i + d - 2, j);
+    iy[d] = cid(P, i, j + d - 2);
+  }
+  const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
+  if (P.reconstate == IMEX_ConsState) {
+    for (int k = 0; k < nstore; ++k) {
+      const double* a = Q + k * N;
+      double xl, xr, yl, yr;
+      recon_1d(P.recon, __ldg(a + ix[0]), __ldg(a + ix[1]), __ldg(a + ix[2]), __ldg(a + ix[3]), __ldg(a + ix[4]), xl,
+               xr, false);
+      recon_1d(P.recon, __ldg(a + iy[0]), __ldg(a + iy[1]), __ldg(a + iy[2]), __ldg(a + iy[3]), __ldg(a + iy[4]), yl,
+               yr, vortex);
+      w[(0 * 8 + k) * N + n] = xl;
+      w[(1 * 8 + k) * N + n] = xr;
+      w[(2 * 8 + k) * N + n] = yl;
+      w[(3 * 8 + k) * N + n] = yr;
+    }
+    return;
+  }
+  // PrimState: reconstruct primitive variables, convert each face state back (reconstruction.cpp:272-281)
+  double px[5][8], py[5][8];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    double c[8];
+    load_cell<8>(Q, N, ix[d], c);
+    con2pri(P, px[d], c);
+    load_cell<8>(Q, N, iy[d], c);
+    con2pri(P, py[d], c);
+  }
+  double wxl[8], wxr[8], wyl[8], wyr[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    recon_1d(P.recon, px[0][k], px[1][k], px[2][k], px[3][k], px[4][k], wxl[k], wxr[k], false);
+    recon_1d(P.recon, py[0][k], py[1][k], py[2][k], py[3][k], py[4][k], wyl[k], wyr[k], vortex);
+  }
+  double c[8];
+  double* outs[4] = {wxl, wxr, wyl, wyr};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    pri2con(P, c, outs[q]);
+    for (int k = 0; k < nstore; ++k) w[(q * 8 + k) * N + n] = c[k];
+  }
+}
+
+// ---------------------------------------------------------------- flux updates
+// RusanovC_Update (flux.cpp:409-455) or Pressure_flux_Update (flux.cpp:290-326) with the
+// B slots of the face states taken from cell B of u_con (main.cpp:447-467).
+template <bool kPressureForm>
+__global__ void k_flux_update(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ w,
+                              const double* __restrict__ Qs, double* __restrict__ ucon) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double h = sc->h, a_max = sc->a_max;
+  const double* wxL = w;
+  const double* wxR = w + 8 * N;
+  const double* wyL = w + 16 * N;
+  const double* wyR = w + 24 * N;
+  auto state = [&](const double* wq, long long m, double* Q) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Q[k] = __ldg(wq + k * N + m);
+    if (kPressureForm) {
+#pragma unroll
+      for (int k = 5; k < 8; ++k) Q[k] = __ldg(ucon + k * N + m);
+    } else {
+      Q[5] = Q[6] = Q[7] = 0.0;
+    }
+  };
+  const long long ip = cid(P, i + 1, j), im = cid(P, i - 1, j), jp = cid(P, i, j + 1), jm = cid(P, i, j - 1);
+  double QL[8], QR[8], fp[5], fm[5], gp[5], gm[5];
+  state(wxR, n, QL);
+  state(wxL, ip, QR);
+  face_flux<kPressureForm>(P, QL, QR, 0, a_max, fp);
+  state(wyR, n, QL);
+  state(wyL, jp, QR);
+  face_flux<kPressureForm>(P, QL, QR, 1, a_max, gp);
+  state(wxR, im, QL);
+  state(wxL, n, QR);
+  face_flux<kPressureForm>(P, QL, QR, 0, a_max, fm);
+  state(wyR, jm, QL);
+  state(wyL, n, QR);
+  face_flux<kPressureForm>(P, QL, QR, 1, a_max, gm);
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    ucon[k * N + n] = Qs[k * N + n] - h / P.dx * (fp[k] - fm[k]) - h / P.dy * (gp[k] - gm[k]);
+}
+
+// ---------------------------------------------------------------- constrained transport
+__device__ __forceinline__ double cell_ez(const double* __restrict__ u, long long N, long long m) {
+  double r = __ldg(u + m);
+  return __ldg(u + 2 * N + m) / r * __ldg(u + 5 * N + m) - __ldg(u + N + m) / r * __ldg(u + 6 * N + m);
+}
+// Corner EMF: CT_CornerAssemble (constrained_transport.cpp:338-355) of the face EMFs
+// ep0 = sx * fx, e0p = sy * fy and the cell EMF of u_con (ct_flux.cpp:165-168).
+__global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
+                            double sy, const double* __restrict__ ucon, double* __restrict__ Epp) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const long long c00 = n, c10 = cid(P, i + 1, j), c01 = cid(P, i, j + 1), c11 = cid(P, i + 1, j + 1);
+  const double dx = P.dx, dy = P.dy;
+  double Ep0_00 = sx * __ldg(fx + c00), Ep0_01 = sx * __ldg(fx + c01);
+  double E0p_00 = sy * __ldg(fy + c00), E0p_10 = sy * __ldg(fy + c10);
+  double Et00 = cell_ez(ucon, N, c00), Et10 = cell_ez(ucon, N, c10), Et01 = cell_ez(ucon, N, c01),
+         Et11 = cell_ez(ucon, N, c11);
+  double bar = 0.25 * (Ep0_00 + Ep0_01 + E0p_00 + E0p_10);
+  double t1 = 0.5 * ((Ep0_00 - Et00) / (dx / 2.0) + (Ep0_01 - Et01) / (dx / 2.0));
+  double t2 = 0.5 * ((Et10 - Ep0_00) / (dx / 2.0) + (Et11 - Ep0_01) / (dx / 2.0));
+  double t3 = 0.5 * ((E0p_00 - Et00) / (dy / 2.0) + (E0p_10 - Et10) / (dy / 2.0));
+  double t4 = 0.5 * ((Et01 - E0p_00) / (dy / 2.0) + (Et11 - E0p_10) / (dy / 2.0));
+  Epp[n] = bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
+}
+// Face update from the corner EMF and cell B = face average
+// (ct_flux.cpp:174-189, constrained_transport.cpp:319-332).  The neighbour faces
+// are recomputed with the same arithmetic rather than re-read.
+__global__ void k_ct_faces(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
+                           const double* __restrict__ bxQs, const double* __restrict__ byQs, double* __restrict__ bx,
+                           double* __restrict__ by, double* __restrict__ ucon) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double h = sc->h;
+  const long long im = cid(P, i - 1, j), jm = cid(P, i, j - 1), imjm = cid(P, i - 1, j - 1);
+  double e00 = __ldg(Epp + n), em0 = __ldg(Epp + im), e0m = __ldg(Epp + jm), emm = __ldg(Epp + imjm);
+  double fx = __ldg(bxQs + n) - h / P.dy * (e00 - e0m);
+  double fy = __ldg(byQs + n) + h / P.dx * (e00 - em0);
+  double fxm = __ldg(bxQs + im) - h / P.dy * (em0 - emm);
+  double fym = __ldg(byQs + jm) + h / P.dx * (e0m - emm);
+  bx[n] = fx;
+  by[n] = fy;
+  ucon[5 * N + n] = 0.5 * (fxm + fx);
+  ucon[6 * N + n] = 0.5 * (fym + fy);
+}
+// Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:714-720)
+__global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
+                              const double* __restrict__ A_s, double* __restrict__ A) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  double Ec = 0.25 * (__ldg(Epp + n) + __ldg(Epp + cid(P, i - 1, j)) + __ldg(Epp + cid(P, i, j - 1)) +
+                      __ldg(Epp + cid(P, i - 1, j - 1)));
+  A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
+}
+// Unstaggered_CT upwind A_z advection (constrained_transport.cpp:627-679)
+__device__ __forceinline__ double vanleer_lim(double a, double b) {
+  if (a * b <= 0.0) return 0.0;
+  return 2.0 * a * b / (a + b);
+}
+__global__ void k_ct_unstag_legacy_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ u,
+                                     const double* __restrict__ A_s, double* __restrict__ A) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double h = sc->h, dx = P.dx, dy = P.dy;
+  const double* As = A_s + 2 * N;
+  auto vxc = [&](long long m) { return __ldg(u + N + m) / __ldg(u + m); };
+  auto vyc = [&](long long m) { return __ldg(u + 2 * N + m) / __ldg(u + m); };
+  long long c = n, xm = cid(P, i - 1, j), xp = cid(P, i + 1, j), xmm = cid(P, i - 2, j), xpp = cid(P, i + 2, j);
+  long long ym = cid(P, i, j - 1), yp = cid(P, i, j + 1), ymm = cid(P, i, j - 2), ypp = cid(P, i, j + 2);
+  double uL = 0.5 * (vxc(xm) + vxc(c)), uR = 0.5 * (vxc(c) + vxc(xp));
+  double dAL = As[c] - As[xm], dAR = As[xp] - As[c], dALL = As[xm] - As[xmm], dARR = As[xpp] - As[xp];
+  double fluct_x = fmax(uL, 0.0) * dAL + fmin(uR, 0.0) * dAR;
+  double corrL = 0.5 * fabs(uL) * (1.0 - fabs(uL) * h / dx) * vanleer_lim(dAL, (uL >= 0.0 ? dALL : dAR));
+  double corrR = 0.5 * fabs(uR) * (1.0 - fabs(uR) * h / dx) * vanleer_lim(dAR, (uR >= 0.0 ? dAL : dARR));
+  double dAdt_x = fluct_x / dx + (corrR - corrL) / dx;
+  double vL = 0.5 * (vyc(ym) + vyc(c)), vR = 0.5 * (vyc(c) + vyc(yp));
+  double dAB = As[c] - As[ym], dAT = As[yp] - As[c], dABB = As[ym] - As[ymm], dATT = As[ypp] - As[yp];
+  double fluct_y = fmax(vL, 0.0) * dAB + fmin(vR, 0.0) * dAT;
+  double corrB = 0.5 * fabs(vL) * (1.0 - fabs(vL) * h / dy) * vanleer_lim(dAB, (vL >= 0.0 ? dABB : dAT));
+  double corrT = 0.5 * fabs(vR) * (1.0 - fabs(vR) * h / dy) * vanleer_lim(dAT, (vR >= 0.0 ? dAB : dATT));
+  double dAdt_y = fluct_y / dy + (corrT - corrB) / dy;
+  A[2 * N + n] = As[c] - h * (dAdt_x + dAdt_y);
+}
+// B = curl A_z for the unstaggered schemes (constrained_transport.cpp:724-729)
+__global__ void k_curl_Az(DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double* Az = A + 2 * N;
+  ucon[5 * N + n] = (__ldg(Az + cid(P, i, j + 1)) - __ldg(Az + cid(P, i, j - 1))) / (2.0 * P.dy);
+  ucon[6 * N + n] = -(__ldg(Az + cid(P, i + 1, j)) - __ldg(Az + cid(P, i - 1, j))) / (2.0 * P.dx);
+}
+// Face EMFs of the legacy Staggered_CT from the reconstruction of u_con
+// (constrained_transport.cpp:264-288): Ez_p0 = -(f6_L + f6_R)/2, Ez_0p = (g5_L + g5_R)/2.
+__global__ void k_ct_legacy_faces(DevParams P, const double* __restrict__ w, double* __restrict__ ep0,
+                                  double* __restrict__ e0p) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
+  auto f6 = [&](const double* q, long long m) {
+    double r = __ldg(q + m);
+    return __ldg(q + 6 * N + m) * (__ldg(q + N + m) / r) - (__ldg(q + 2 * N + m) / r) * __ldg(q + 5 * N + m);
+  };
+  auto g5 = [&](const double* q, long long m) {
+    double r = __ldg(q + m);
+    return __ldg(q + 5 * N + m) * (__ldg(q + 2 * N + m) / r) - (__ldg(q + N + m) / r) * __ldg(q + 6 * N + m);
+  };
+  ep0[n] = -(0.5 * (f6(wxR, n) + f6(wxL, cid(P, i + 1, j))));
+  e0p[n] = (0.5 * (g5(wyR, n) + g5(wyL, cid(P, i, j + 1))));
+}
+
+// ---------------------------------------------------------------- stage derivative
+// Energy_Modify (main.cpp:528-534), Hs / HsA / HsB (main.cpp:539-555), u_pri (main.cpp:537).
+__global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __restrict__ sc, double* __restrict__ cons,
+                                   const double* __restrict__ Qs, const double* __restrict__ A,
+                                   const double* __restrict__ A_s, const double* __restrict__ bx,
+                                   const double* __restrict__ bxQs, const double* __restrict__ by,
+                                   const double* __restrict__ byQs, const double* __restrict__ Bsave,
+                                   double* __restrict__ Hs, double* __restrict__ HsA, double* __restrict__ HsB,
+                                   double* __restrict__ prim) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double adt = sc->adt;
+  double c[8];
+  load_cell<8>(cons, N, n, c);
+  if (P.Energy_Modify) {
+    double o5 = Bsave[n], o6 = Bsave[N + n], o7 = Bsave[2 * N + n];
+    c[4] = c[4] + ((c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) - (o5 * o5 + o6 * o6 + o7 * o7)) / 2.0;
+    cons[4 * N + n] = c[4];
+  }
+  double* H = Hs + (long long)rks * 8 * N;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) H[k * N + n] = (c[k] - Qs[k * N + n]) / adt;
+  double* HA = HsA + (long long)rks * 3 * N;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) HA[k * N + n] = (A[k * N + n] - A_s[k * N + n]) / adt;
+  double* HB = HsB + (long long)rks * 2 * N;
+  HB[n] = (bx[n] - bxQs[n]) / adt;
+  HB[N + n] = (by[n] - byQs[n]) / adt;
+  double p[8];
+  con2pri(P, p, c);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) prim[k * N + n] = p[k];
+}
+
+// ---------------------------------------------------------------- shock detector
+// ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41).
+__global__ void k_shock_cf(DevParams P, const double* __restrict__ Q, double* __restrict__ cf) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  double c[8];
+  load_cell<8>(Q, P.N, n, c);
+  double p = pressure_of(P, c);
+  double a2 = eos_a2(P, c[0], p);
+  double cA2 = (c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) / c[0];
+  cf[n] = sqrt(a2 + cA2);
+}
+__global__ void k_shock_tilde(DevParams P, const double* __restrict__ Q, const double* __restrict__ cf,
+                              double* __restrict__ chit) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  double m = 1.0e300;
+  for (int di = -1; di <= 1; di++)
+    for (int dj = -1; dj <= 1; dj++) {
+      double v = __ldg(cf + cid(P, i + di, j + dj));
+      if (v < m) m = v;
+    }
+  long long xp = cid(P, i + 1, j), xm = cid(P, i - 1, j), yp = cid(P, i, j + 1), ym = cid(P, i, j - 1);
+  double div_u = (__ldg(Q + N + xp) / __ldg(Q + xp) - __ldg(Q + N + xm) / __ldg(Q + xm)) / (2.0 * P.dx) +
+                 (__ldg(Q + 2 * N + yp) / __ldg(Q + yp) - __ldg(Q + 2 * N + ym) / __ldg(Q + ym)) / (2.0 * P.dy);
+  double num = P.hmin * div_u + P.shock_kappa1 * m;
+  double den = P.shock_kappa1 * m;
+  double q = -num / den;
+  double mx = (0.0 < q) ? q : 0.0;
+  chit[n] = (mx < 1.0) ? mx : 1.0;
+}
+__global__ void k_shock_max(DevParams P, const double* __restrict__ chit, double* __restrict__ eta) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  double m = 0.0;
+  for (int di = -1; di <= 1; di++)
+    for (int dj = -1; dj <= 1; dj++) {
+      double v = __ldg(chit + cid(P, i + di, j + dj));
+      if (v > m) m = v;
+    }
+  eta[n] = m;
+}
+
+// ---------------------------------------------------------------- diagnostics
+// face FV div (StaggerCT), wrapped central div of cell B, reference cell metric
+// (imex_subsystems.cpp:646-654), max |central div|
+__global__ void k_divergence(DevParams P, const double* __restrict__ ucon, const double* __restrict__ bx,
+                             const double* __restrict__ by, double* __restrict__ partial) {
+  const long long N = P.N;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  double m = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    double d = (bx[n] - bx[cid(P, i - 1, j)]) / P.dx + (by[n] - by[cid(P, i, j - 1)]) / P.dy;
+    v[0] += P.dx * P.dy * d * d;
+    const double* B5 = ucon + 5 * N;
+    const double* B6 = ucon + 6 * N;
+    double cx = (B5[cid(P, i + 1, j)] - B5[cid(P, i - 1, j)]) / (2.0 * P.dx);
+    double cy = (B6[cid(P, i, j + 1)] - B6[cid(P, i, j - 1)]) / (2.0 * P.dy);
+    double c = cx + cy;
+    v[1] += P.dx * P.dy * c * c;
+    double rx = i == 0 ? (B5[cid(P, i + 1, j)] - B5[n]) / P.dx
+                       : (i == P.nx - 1 ? (B5[n] - B5[cid(P, i - 1, j)]) / P.dx : cx);
+    double ry = j == 0 ? (B6[cid(P, i, j + 1)] - B6[n]) / P.dy
+                       : (j == P.ny - 1 ? (B6[n] - B6[cid(P, i, j - 1)]) / P.dy : cy);
+    double r = rx + ry;
+    v[2] += P.dx * P.dy * r * r;
+    m = fmax(m, fabs(c));
+  }
+  v[3] = 0.0;
+  block_reduce(v, FSum(), 0.0);
+  double mm[1] = {m};
+  block_reduce(mm, FMax(), 0.0);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x * 4 + 0] = v[0];
+    partial[blockIdx.x * 4 + 1] = v[1];
+    partial[blockIdx.x * 4 + 2] = v[2];
+    partial[blockIdx.x * 4 + 3] = mm[0];
+  }
+}
+__global__ void k_min_pressure(DevParams P, const double* __restrict__ prim, double* __restrict__ partial) {
+  double m[1] = {INFINITY};
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < P.N; n += (long long)gridDim.x * blockDim.x)
+    m[0] = fmin(m[0], prim[4 * P.N + n]);
+  block_reduce(m, FMin(), INFINITY);
+  if (threadIdx.x == 0) partial[blockIdx.x] = m[0];
+}
+
+// pressure and enthalpy of Qe (the planes k_stage_combine produces)
+__global__ void k_qe_derived(DevParams P, const double* __restrict__ Qe, double* __restrict__ pe,
+                             double* __restrict__ hQe) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  double q[8];
+  load_cell<8>(Qe, P.N, n, q);
+  double e = calecon(q);
+  double p = eos_p(P, q[0], e);
+  pe[n] = p;
+  hQe[n] = e + p / q[0];
+}
+// Newton Jacobian diagonal V_slope(p_freeze, rho) (config.hpp:236-239)
+__global__ void k_vslope(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ pf,
+                         const double* __restrict__ ucon, double* __restrict__ vdiag) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= P.N) return;
+  vdiag[n] = V_slope(P, sc->Mbig, pf[n], ucon[n]);
+}
+
+}  // namespace
+
+// ================================================================ launchers
+#define LAUNCH_CHECK(ctx, what)                                         \
+  do {                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                \
+    if (e_ != cudaSuccess) return cuda_check(ctx, e_, what);            \
+  } while (0)
+
+imex_status launch_step_prologue(imex_ctx* ctx) {
+  const DevParams& P = ctx->P;
+  int nblk = blocks_for(P.N);
+  if (nblk > ctx->max_blocks) nblk = ctx->max_blocks;
+  k_step_reduce<<<nblk, kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->partial);
+  LAUNCH_CHECK(ctx, "k_step_reduce");
+  k_step_finalize<<<1, 32, 0, ctx->stream>>>(P, ctx->partial, nblk, ctx->sc);
+  LAUNCH_CHECK(ctx, "k_step_finalize");
+  k_cons_from_prim<<<blocks_for(P.N), kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->cons, ctx->cons_n);
+  LAUNCH_CHECK(ctx, "k_cons_from_prim");
+  const size_t plane = ctx->N * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(ctx->bx_n, ctx->bx, plane, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by_n, ctx->by, plane, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A_snap, ctx->A, 3 * plane, cudaMemcpyDeviceToDevice, ctx->stream);
+  return cuda_check(ctx, e, "step snapshot copies");
+}
+
+imex_status launch_qe_derived(imex_ctx* ctx) {
+  k_qe_derived<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->pe, ctx->hQe);
+  LAUNCH_CHECK(ctx, "k_qe_derived");
+  return IMEX_OK;
+}
+imex_status launch_vslope(imex_ctx* ctx) {
+  k_vslope<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->pf, ctx->cons, ctx->vdiag);
+  LAUNCH_CHECK(ctx, "k_vslope");
+  return IMEX_OK;
+}
+
+imex_status launch_cons_from_prim(imex_ctx* ctx) {
+  k_cons_from_prim<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->prim, ctx->cons, nullptr);
+  LAUNCH_CHECK(ctx, "k_cons_from_prim");
+  return IMEX_OK;
+}
+imex_status launch_prim_from_cons(imex_ctx* ctx) {
+  k_prim_from_cons<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->cons, ctx->prim);
+  LAUNCH_CHECK(ctx, "k_prim_from_cons");
+  return IMEX_OK;
+}
+
+// Butcher tableaux of main.cpp:269-319
+static void tableau(int RKs, double ae[kMaxRK][kMaxRK], double ai[kMaxRK][kMaxRK]) {
+  for (int r = 0; r < kMaxRK; ++r)
+    for (int c = 0; c < kMaxRK; ++c) ae[r][c] = ai[r][c] = 0.0;
+  if (RKs == 1) {
+    ai[0][0] = 1.0;
+  } else if (RKs == 2) {
+    double bb = 1.0 - 1.0 / sqrt(2.0), cc = 1.0 / (2.0 * bb);
+    ae[1][0] = cc;
+    ai[0][0] = bb;
+    ai[1][0] = 1 - bb;
+    ai[1][1] = bb;
+  } else {
+    double r12 = 0.5, r13 = 1.0 / 3.0, r14 = 1.0 / 4.0;
+    ae[1][0] = r12;
+    ae[2][0] = r12;
+    ae[2][1] = r12;
+    ai[0][0] = r14;
+    ai[1][1] = r14;
+    ai[2][0] = r13;
+    ai[2][1] = r13;
+    ai[2][2] = r13;
+  }
+}
+
+imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
+  double ae[kMaxRK][kMaxRK], ai[kMaxRK][kMaxRK];
+  tableau(ctx->P.RKs, ae, ai);
+  Tableau T{};
+  for (int r = 0; r < kMaxRK; ++r) {
+    T.ae[r] = ae[rks][r];
+    T.ai[r] = ai[rks][r];
+  }
+  T.aii = ai[rks][rks];
+  k_stage_combine<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
+      ctx->P, T, rks, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
+      ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe);
+  LAUNCH_CHECK(ctx, "k_stage_combine");
+  return IMEX_OK;
+}
+
+imex_status launch_reconstruct(imex_ctx* ctx) {
+  k_reconstruct<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, 8);
+  LAUNCH_CHECK(ctx, "k_reconstruct");
+  return IMEX_OK;
+}
+
+imex_status launch_flux_update(imex_ctx* ctx, int pressure_form) {
+  int nb = blocks_for(ctx->P.N);
+  if (pressure_form)
+    k_flux_update<true><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  else
+    k_flux_update<false><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  LAUNCH_CHECK(ctx, "k_flux_update");
+  return IMEX_OK;
+}
+
+// variant: 0 Staggered_CT_Consistent, 1 Unstaggered_CT_Consistent, 2 Staggered_CT, 3 Unstaggered_CT
+imex_status launch_ct(imex_ctx* ctx, int variant) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
+  cudaStream_t s = ctx->stream;
+  if (variant == 0 || variant == 1) {
+    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp);
+    LAUNCH_CHECK(ctx, "k_ct_corner");
+  } else if (variant == 2) {
+    k_reconstruct<<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
+    LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
+    k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
+    LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
+    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->chit, 1.0, ctx->Et, 1.0, ctx->cons, ctx->Epp);
+    LAUNCH_CHECK(ctx, "k_ct_corner");
+  }
+  if (variant == 0 || variant == 2) {
+    k_ct_faces<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->bxQs, ctx->byQs, ctx->bx, ctx->by, ctx->cons);
+    LAUNCH_CHECK(ctx, "k_ct_faces");
+  } else {
+    if (variant == 1) k_ct_unstag_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A);
+    else k_ct_unstag_legacy_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->cons, ctx->A_s, ctx->A);
+    LAUNCH_CHECK(ctx, "k_ct_unstag_A");
+    k_curl_Az<<<nb, kThreads, 0, s>>>(P, ctx->A, ctx->cons);
+    LAUNCH_CHECK(ctx, "k_curl_Az");
+  }
+  return IMEX_OK;
+}
+
+imex_status launch_stage_derivative(imex_ctx* ctx, int rks) {
+  k_stage_derivative<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
+      ctx->P, rks, ctx->sc, ctx->cons, ctx->Qs, ctx->A, ctx->A_s, ctx->bx, ctx->bxQs, ctx->by, ctx->byQs, ctx->Bsave,
+      ctx->Hs, ctx->HsA, ctx->HsB, ctx->prim);
+  LAUNCH_CHECK(ctx, "k_stage_derivative");
+  return IMEX_OK;
+}
+
+imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
+  k_shock_cf<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et);
+  k_shock_tilde<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et, ctx->chit);
+  k_shock_max<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->chit, eta);
+  LAUNCH_CHECK(ctx, "shock detector");
+  return IMEX_OK;
+}
+
+imex_status launch_divergence(imex_ctx* ctx, double* out4) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
+  if (nb > ctx->max_blocks) nb = ctx->max_blocks;
+  k_divergence<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->cons, ctx->bx, ctx->by, ctx->partial);
+  LAUNCH_CHECK(ctx, "k_divergence");
+  std::vector<double> h((size_t)nb * 4);
+  cudaError_t e = cudaMemcpyAsync(h.data(), ctx->partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "divergence readback");
+  double s0 = 0, s1 = 0, s2 = 0, m = 0;
+  for (int b = 0; b < nb; ++b) {
+    s0 += h[b * 4 + 0];
+    s1 += h[b * 4 + 1];
+    s2 += h[b * 4 + 2];
+    m = fmax(m, h[b * 4 + 3]);
+  }
+  out4[0] = sqrt(s0);
+  out4[1] = sqrt(s1);
+  out4[2] = sqrt(s2);
+  out4[3] = m;
+  return IMEX_OK;
+}
+
+imex_status launch_min_pressure(imex_ctx* ctx, double* pmin) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
+  if (nb > ctx->max_blocks) nb = ctx->max_blocks;
+  k_min_pressure<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->partial);
+  LAUNCH_CHECK(ctx, "k_min_pressure");
+  std::vector<double> h(nb);
+  cudaError_t e = cudaMemcpyAsync(h.data(), ctx->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "min pressure readback");
+  double m = INFINITY;
+  for (int b = 0; b < nb; ++b) m = fmin(m, h[b]);
+  *pmin = m;
+  return IMEX_OK;
+}
+
+
+imex_status eos_flag_stage(imex_ctx* ctx, int* flag, bool reset) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(&ctx->h_red[0], d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,
+                                            ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "eos flag");
+  int v = 0;
+  memcpy(&v, &ctx->h_red[0], sizeof(int));
+  *flag = v;
+  if (reset && v) {
+    static const int zero = 0;
+    e = cudaMemcpyToSymbolAsync(d_eos_flag, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  return cuda_check(ctx, e, "eos flag reset");
+}
+
+}  // namespace imex

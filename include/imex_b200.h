@@ -1,0 +1,251 @@
+/*
+ * imex_b200 - one IMEX Runge-Kutta stage of the 2D ideal-MHD scheme of the
+ * IMEX reference solver, as hand-written CUDA for B200 (sm_100a).
+ *
+ * This header is the whole drop-in boundary: plain C, plain pointers and
+ * sizes.  Each entry point replaces one function of the reference's C++
+ * interface (include/declarations.hpp) or one block of its driver
+ * (src/main.cpp); the citation is given beside it.  A time-marching driver
+ * that used to call the reference's sub-system functions calls these in the
+ * same order.
+ *
+ * Data layout exchanged through the interface (host or device pointers are
+ * both accepted wherever an array is passed; copies use cudaMemcpyDefault):
+ *   - a "plane" is nx*ny doubles of interior cells, index i + nx*j;
+ *   - cell state = 8 planes: rho, rho vx, rho vy, rho vz, E, Bx, By, Bz
+ *     (conserved) or rho, vx, vy, vz, p, Bx, By, Bz (primitive);
+ *   - face fields: plane(i,j) is Bx at the x-face (i+1/2, j), resp. By at the
+ *     y-face (i, j+1/2);
+ *   - vector potential = 3 planes (Ax, Ay, Az) at cell centres;
+ *   - a GMRES vector of the pressure system is one plane; of the magnetic
+ *     systems three planes, in the order of the reference's M_P / M_B maps
+ *     (implicit_operators.cpp:5-139).
+ * Ghost cells do not exist: boundaries are periodic in both directions and
+ * handled by wrap-around indexing inside the kernels.
+ *
+ * Conventions: every function returns imex_status (0 = OK).  Non-convergence
+ * and non-finite values found on the device are reported through the status
+ * and imex_solve_stats, never by trapping the GPU.  The context owns all
+ * device memory.  One context must not be used by two host threads at once.
+ * Work is enqueued on the context's stream (imex_set_stream); functions that
+ * return results to host memory synchronise that stream.
+ */
+#ifndef IMEX_B200_H
+#define IMEX_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum imex_status {
+  IMEX_OK = 0,
+  IMEX_ERR_INVALID = 1,     /* bad argument, size or call order */
+  IMEX_ERR_UNSUPPORTED = 2, /* configuration this implementation does not cover */
+  IMEX_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  IMEX_GMRES_MAXIT = 4,     /* GMRES reached its restart cap without converging */
+  IMEX_NEWTON_MAXIT = 5,    /* nested Newton reached Pnewton_max */
+  IMEX_NONFINITE = 6,       /* a NaN or Inf appeared in a solve */
+  IMEX_POSITIVITY = 7,      /* p < theta * p_floor after a floored pressure solve */
+  IMEX_ERR_SYNC = 8,        /* a device-wide barrier timed out (kernel returned early) */
+  IMEX_ERR_EOS = 9          /* a per-cell EOS Newton iteration hit its cap */
+} imex_status;
+
+/* Enumerations: names and ordinals of the reference include/config.hpp:27-41,118. */
+typedef enum { IMEX_EnergyFormula = 0, IMEX_PressureFormula = 1 } imex_formula;
+typedef enum { IMEX_StaggerCT = 0, IMEX_UnStaggerCT = 1, IMEX_PotentialA = 2, IMEX_NoDivFree = 3 } imex_magfield;
+typedef enum { IMEX_NoRecon = 0, IMEX_Minmod = 1, IMEX_VanLeer = 2, IMEX_ENO3 = 3, IMEX_WENO5 = 4 } imex_reconstruction;
+typedef enum { IMEX_PrimState = 0, IMEX_ConsState = 1 } imex_recon_state;
+typedef enum { IMEX_Fullydt = 0, IMEX_Alfvendt = 1, IMEX_IMEXdt = 2 } imex_dt_calculation;
+typedef enum { IMEX_x_Transmissive = 0, IMEX_x_Reflective = 1, IMEX_x_Periodic = 2, IMEX_x_Dirichlet = 3 } imex_x_bc;
+typedef enum {
+  IMEX_y_Transmissive = 0, IMEX_y_Reflective = 1, IMEX_y_Periodic = 2, IMEX_y_Dirichlet = 3, IMEX_y_JetInflow = 4
+} imex_y_bc;
+typedef enum { IMEX_MaterialSpeedp = 0, IMEX_AlfvenSpeedp = 1, IMEX_Noaddvisp = 2 } imex_add_pvisc;
+typedef enum { IMEX_ConservationofU = 0, IMEX_DefinitionofU = 1 } imex_energy_update;
+typedef enum { IMEX_Local_Diss = 0, IMEX_Global_Diss = 1 } imex_flux_diss;
+typedef enum { IMEX_no_correction = 0, IMEX_once_correction = 1, IMEX_all_correction = 2 } imex_solve_pressure;
+typedef enum { IMEX_IDEAL_GAS = 0, IMEX_REDLICH_KWONG = 1 } imex_eos_type;
+
+/* Arithmetic of the implicit solves. */
+typedef enum {
+  IMEX_PRECISION_FP64 = 0,  /* everything in FP64 (the plain form) */
+  IMEX_PRECISION_MIXED = 1  /* FP32 operator + Krylov vectors inside FP64 iterative refinement */
+} imex_precision;
+
+/* Run-time form of the reference's compile-time configuration
+ * (include/config.hpp:43-125 and the per-test settings of main.cpp:9-224).
+ * Field names follow the reference globals. */
+typedef struct imex_config {
+  int caltimestep;     /* imex_dt_calculation      (config.hpp:43) */
+  int formula;         /* imex_formula             (config.hpp:44) */
+  int magfield;        /* imex_magfield            (config.hpp:45) */
+  int add_pvisc;       /* imex_add_pvisc           (config.hpp:46) */
+  int flux_diss;       /* imex_flux_diss           (config.hpp:47) */
+  int GLF;             /* global Lax-Friedrichs dissipation (config.hpp:48) */
+  int add_bvisc;       /* A-form numerical viscosity (config.hpp:49) */
+  int U_update;        /* imex_energy_update       (config.hpp:50) */
+  int vortex_test;     /* nonzero reproduces `test == testMHD_vortex` (Minmod y-slope special case) */
+  int RKs;             /* IMEX-RK stages: 1, 2 or 3 (config.hpp:56) */
+  double CFL;          /* (config.hpp:57) */
+  int recon;           /* imex_reconstruction      (config.hpp:60) */
+  int reconstate;      /* imex_recon_state         (config.hpp:61) */
+  int x_bc, y_bc;      /* boundary conditions; only periodic is implemented */
+  int PressureSolver;  /* imex_solve_pressure      (config.hpp:65) */
+  int Energy_Modify;   /* (config.hpp:69) */
+  double GMREStol;     /* (config.hpp:71) */
+  double shock_kappa1; /* (config.hpp:77) */
+  int floor_on;        /* pressure-positivity nested Newton (config.hpp:100) */
+  double p_floor;      /* (config.hpp:101) */
+  double Mbig_fac;     /* (config.hpp:102) */
+  double theta;        /* (config.hpp:103) */
+  int Pnewton_max;     /* (config.hpp:106) */
+  double Pnewton_tol;  /* (config.hpp:107) */
+  int eos_type;        /* imex_eos_type            (config.hpp:119) */
+  double gamma_plasma; /* (config.hpp:122) */
+  double m_alfa, m_b, m_R, m_cv; /* Redlich-Kwong constants (config.hpp:125) */
+  double x_0, x_1, y_0, y_1;     /* domain (main.cpp:9-224) */
+  double time_stop;    /* end time; dt is clipped to reach it (main.cpp:341) */
+  double fixed_dt;     /* g_fixed_dt: > 0 forces dt (config.hpp:249) */
+  /* additions of this implementation */
+  int gmres_restart;      /* Krylov vectors per cycle; the reference hard-codes 25 (implicit_operators.cpp:801) */
+  int gmres_max_restarts; /* restart cap; 0 = the vector dimension, as the reference (implicit_operators.cpp:802) */
+  int precision;          /* imex_precision */
+  double mixed_inner_tol; /* relative tolerance of each FP32 inner solve in mixed mode */
+  int mixed_max_refine;   /* cap on FP64 refinement sweeps in mixed mode */
+} imex_config;
+
+/* Scalars that the reference keeps in hidden globals and that one stage consumes
+ * (dt, adt, B_max_x/y, vx_max/vy_max, a_max; timestep.cpp:5-67,254-273). */
+typedef struct imex_step_scalars {
+  double dt, adt, B_max_x, B_max_y, vx_max, vy_max, v_max, a_max, ch, cA_x, cA_y, t;
+  int timestep;
+} imex_step_scalars;
+
+/* Counters of the implicit solves, accumulated since the last imex_reset_stats. */
+typedef struct imex_solve_stats {
+  int gmres_solves;      /* GMRES calls */
+  int gmres_iters;       /* Arnoldi steps (operator applications inside cycles) */
+  int gmres_restarts;    /* restart cycles */
+  int newton_iters;      /* nested-Newton Jacobian solves */
+  int max_floored;       /* largest number of cells below p_floor after a Newton solve */
+  int refine_sweeps;     /* FP64 refinement sweeps (mixed precision) */
+  double last_residual;  /* residual estimate at exit of the last GMRES solve */
+  double min_p;          /* smallest pressure after a floored solve */
+  int status;            /* worst imex_status seen */
+} imex_solve_stats;
+
+typedef struct imex_ctx imex_ctx;
+
+/* Context and configuration ------------------------------------------------ */
+void imex_config_default(imex_config* cfg); /* the reference defaults, config.hpp:43-125 */
+imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out);
+imex_status imex_destroy(imex_ctx* ctx);
+imex_status imex_set_stream(imex_ctx* ctx, void* cuda_stream); /* cudaStream_t; NULL = own stream */
+imex_status imex_synchronize(imex_ctx* ctx);
+const char* imex_status_string(imex_status s);
+const char* imex_last_error(const imex_ctx* ctx);
+imex_status imex_get_config(const imex_ctx* ctx, imex_config* cfg);
+
+/* State I/O ---------------------------------------------------------------- */
+/* Initial data as primitive planes + faces + vector potential; converts to conserved
+ * like main.cpp:240-244 (u_initialization, upri2ucon, A_initial). */
+imex_status imex_upload_prim(imex_ctx* ctx, const double* prim8, const double* bx, const double* by,
+                             const double* A3);
+/* Current state; any pointer may be NULL. */
+imex_status imex_download_state(imex_ctx* ctx, double* cons8, double* prim8, double* bx, double* by, double* A3);
+
+/* Time stepping ------------------------------------------------------------ */
+/* One full time step of main.cpp:335-561: global wave-speed maxima, dt, every stage. */
+imex_status imex_step(imex_ctx* ctx, double* dt_out);
+/* Step prologue alone (main.cpp:335-366): scalars, dt, u^n snapshot. */
+imex_status imex_begin_step(imex_ctx* ctx);
+/* One IMEX stage (main.cpp:367-559 body for stage rks). */
+imex_status imex_stage(imex_ctx* ctx, int rks);
+/* Step epilogue (main.cpp:561): primitive state of the new step. */
+imex_status imex_end_step(imex_ctx* ctx);
+imex_status imex_set_step_scalars(imex_ctx* ctx, const imex_step_scalars* s);
+imex_status imex_get_step_scalars(imex_ctx* ctx, imex_step_scalars* s);
+
+/* Sub-steps of one stage, in the order of main.cpp:368-555.  Each reads and writes
+ * the context's stage buffers (imex_buffer) exactly as the reference function
+ * reads and writes its arguments. */
+imex_status imex_stage_combine(imex_ctx* ctx, int rks);                       /* main.cpp:368-414 */
+imex_status imex_TVDReconstruction(imex_ctx* ctx);                            /* reconstruction.cpp:5 (Qe -> w) */
+imex_status imex_RusanovC_Update(imex_ctx* ctx, double h, int rks);           /* flux.cpp:409 */
+imex_status imex_MagSubsystem_UpdateB(imex_ctx* ctx, double h, int rks);      /* imex_subsystems.cpp:537 */
+imex_status imex_MagSubsystem_UpdateA(imex_ctx* ctx, double h, int rks);      /* imex_subsystems.cpp:5 */
+imex_status imex_Pressure_flux_Update(imex_ctx* ctx, double h, int rks);      /* flux.cpp:290 + main.cpp:447-467 */
+imex_status imex_PreSubsystem_Pressure(imex_ctx* ctx, double h, int rks);     /* imex_subsystems.cpp:76 */
+imex_status imex_PreSubsystem_Energy(imex_ctx* ctx, double h, int rks);       /* imex_subsystems.cpp:415 */
+imex_status imex_Staggered_CT_Consistent(imex_ctx* ctx, double h, int rks);   /* ct_flux.cpp:150 */
+imex_status imex_Unstaggered_CT_Consistent(imex_ctx* ctx, double h, int rks); /* constrained_transport.cpp:691 */
+imex_status imex_Staggered_CT(imex_ctx* ctx, double h, int rks);             /* constrained_transport.cpp:257 */
+imex_status imex_Unstaggered_CT(imex_ctx* ctx, double h, int rks);           /* constrained_transport.cpp:627 */
+imex_status imex_stage_derivative(imex_ctx* ctx, int rks);                    /* main.cpp:537-555 */
+
+/* Stage buffers, for drivers and tests that run sub-steps individually. */
+typedef enum imex_buffer {
+  IMEX_BUF_CONS = 0,  /* u_con, 8 planes */
+  IMEX_BUF_PRIM = 1,  /* u_pri, 8 planes */
+  IMEX_BUF_CONS_N = 2,/* u_con_n (state at the start of the step), 8 planes */
+  IMEX_BUF_QE = 3,    /* explicit stage state Qe, 8 planes */
+  IMEX_BUF_QS = 4,    /* implicit stage state Qs, 8 planes */
+  IMEX_BUF_BX = 5,    /* Bx_p0 faces */
+  IMEX_BUF_BY = 6,    /* By_0p faces */
+  IMEX_BUF_BX_QS = 7, /* Bx_p0_Qs */
+  IMEX_BUF_BY_QS = 8, /* By_0p_Qs */
+  IMEX_BUF_A = 9,     /* A, 3 planes */
+  IMEX_BUF_A_S = 10,  /* A_s, 3 planes */
+  IMEX_BUF_FLUX_X = 11, /* gFluxBy_p0 */
+  IMEX_BUF_FLUX_Y = 12, /* gFluxBx_0p */
+  IMEX_BUF_W = 13,    /* reconstruction w_xL, w_xR, w_yL, w_yR: 32 planes */
+  IMEX_BUF_HS = 14,   /* Hs[index], 8 planes */
+  IMEX_BUF_HSA = 15,  /* HsA[index], 3 planes */
+  IMEX_BUF_HSB = 16,  /* HsB[index], 2 planes */
+  IMEX_BUF_SHOCK = 17 /* shock detector eta of the last pressure solve, 1 plane */
+} imex_buffer;
+imex_status imex_buffer_count(const imex_ctx* ctx, int buffer, size_t* ndoubles);
+imex_status imex_set_buffer(imex_ctx* ctx, int buffer, int index, const double* src);
+imex_status imex_get_buffer(imex_ctx* ctx, int buffer, int index, double* dst);
+
+/* Operators, GMRES and the nested Newton --------------------------------- */
+typedef enum imex_op {
+  IMEX_OP_PRESSURE_L = 0, /* Pressure_Subsystem_AX, g_AX_jacobian = false (implicit_operators.cpp:505) */
+  IMEX_OP_PRESSURE_J = 1, /* Pressure_Subsystem_AX, g_AX_jacobian = true */
+  IMEX_OP_MAGNETIC_B = 2, /* Magnetic_Subsystem_AX (implicit_operators.cpp:141) */
+  IMEX_OP_MAGNETIC_A = 3, /* Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355) */
+  IMEX_OP_ENERGY = 4      /* Energy_Subsystem_AX (implicit_operators.cpp:741) */
+} imex_op;
+/* Freeze the coefficients of `op` from the current CONS (rho), QE and QS buffers,
+ * exactly what the reference operator reads on each application. */
+imex_status imex_prepare_operator(imex_ctx* ctx, int op, double h);
+/* Newton state for IMEX_OP_PRESSURE_J: p_freeze (one plane) and Mbig (config.hpp:104,108). */
+imex_status imex_set_newton_state(imex_ctx* ctx, const double* p_freeze, double mbig);
+/* Ax = op(x), no preconditioner (the reference X_Subsystem_AX functions). */
+imex_status imex_apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax);
+/* GMRES_Solver (implicit_operators.cpp:793): x in/out, b in.  The pressure operators use
+ * the reference's Jacobi preconditioner precP (implicit_operators.cpp:650), the magnetic
+ * ones none, as in the reference call sites. */
+imex_status imex_gmres(imex_ctx* ctx, int op, double* x, const double* b, imex_solve_stats* stats);
+/* Pressure_NestedNewton (implicit_operators.cpp:625): p in/out, b in. */
+imex_status imex_pressure_nested_newton(imex_ctx* ctx, double* p, const double* b, imex_solve_stats* stats);
+/* ShockDetector (flux.cpp:5) of 8 conserved planes into one plane. */
+imex_status imex_shock_detector(imex_ctx* ctx, const double* Q8, double* eta);
+
+/* Statistics and diagnostics ---------------------------------------------- */
+imex_status imex_get_stats(imex_ctx* ctx, imex_solve_stats* stats);
+imex_status imex_reset_stats(imex_ctx* ctx);
+/* Divergence of B (imex_subsystems.cpp:630): face finite-volume L2 of the staggered
+ * field; L2 of the periodic central difference of cell B; the reference's own
+ * cell metric (one-sided at the domain edge); max |central div| of cell B. */
+imex_status imex_divergence(imex_ctx* ctx, double* face_l2, double* cell_wrapped_l2, double* cell_ref_l2,
+                            double* cell_inf);
+/* Minimum pressure and the reference's L2 divergence error for the active CT scheme. */
+imex_status imex_min_pressure(imex_ctx* ctx, double* pmin);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMEX_B200_H */
