@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Throughput of the IMEX-RK stage on B200: cell-updates/s per IMEX stage.
+
+Workload (default): the periodic vortex-sheet MHD problem on [0, 2*pi]^2 at
+1024 x 1024 cells, gamma = 5/3, WENO5 reconstruction, vector-potential (A-form)
+magnetic solve, nested-Newton pressure floor (p_floor = 1e-8, theta = 0.5),
+IMEX-RK3, CFL 0.8, GMRES tolerance 1e-14 (the reference default).  One
+benchmark step = one full time step = 3 IMEX stages.  Inputs are analytic
+(no dataset).  The working set (~2 GB of state and Krylov vectors) is far
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl imex|reference]
+                    [--workload vortex_sheet_1024|vortex_64] [--precision fp64|mixed]
+
+Multi-GPU: the path does not shard (one 2D domain per GPU, "replicas only"):
+N ranks each run an independent copy of the workload; value = total
+cell-stage updates of all ranks / max over ranks of the timed span.
+
+--impl reference times the reference solver's own CPU code (oracle/_ref,
+built from the reference sources; else the C restatement) on the host with
+the threads it can use (it is single-threaded), on a bounded sample of the
+same physics: the same problem on a 256 x 256 grid, one time step per
+benchmark step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per IMEX stage"
+CFG1 = dict(recon="WENO5", magfield="PotentialA", floor_on=1, p_floor=1e-8, theta=0.5,
+            GMREStol=1e-14, CFL=0.8)
+CFG0 = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12, CFL=0.8)
+WORKLOADS = {
+    "vortex_sheet_1024": dict(problem="vortex_sheet", n=1024, rks=3, settings=CFG1,
+                              desc="vortex-sheet MHD 1024^2, WENO5, A-form CT, floor on, RK3"),
+    "vortex_sheet_2048": dict(problem="vortex_sheet", n=2048, rks=3, settings=CFG1,
+                              desc="vortex-sheet MHD 2048^2, WENO5, A-form CT, floor on, RK3"),
+    "vortex_64": dict(problem="vortex", n=64, rks=2, settings=CFG0,
+                      desc="smooth MHD vortex 64^2, VanLeer, staggered CT, RK2"),
+}
+REF_SAMPLE_N = 256
+
+
+def make_problem(kind: str, n: int):
+    from imex_b200.problems import vortex, vortex_sheet
+    return vortex(n) if kind == "vortex" else vortex_sheet(n)
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(family: str) -> float | None:
+    """Per-launch DRAM bytes of `family` at this workload from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)[family]["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def reduce_max(value: float, world: int, device: str = "cuda") -> float:
+    """Max of a per-rank value over all ranks (the timed span of the slowest replica)."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_rate(steps: int, max_seconds: float) -> dict:
+    """Reference CPU solver on the sample: cell-stage updates per second over `steps` steps."""
+    from oracle.bindings import RefSolver, make_solver, PortSolver
+    kind = "reference" if RefSolver.available() else "port"
+    wl = WORKLOADS["vortex_sheet_1024"]
+    prob = make_problem(wl["problem"], REF_SAMPLE_N)
+    solver = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
+    done, t_total = 0, 0.0
+    while done < steps:
+        t0 = time.perf_counter()
+        solver.step()
+        t_total += time.perf_counter() - t0
+        done += 1
+        if t_total > max_seconds:
+            break
+    cells = prob.nx * prob.ny * wl["rks"] * done
+    return dict(value=cells / t_total, unit="cell-updates/s", cores=1, kind=kind,
+                sample=(f"{done} time step(s) x {wl['rks']} stages of the same physics on a "
+                        f"{REF_SAMPLE_N}x{REF_SAMPLE_N} grid, from t=0, one core"),
+                seconds=t_total)
+
+
+def run_reference(args, world: int, rank: int) -> None:
+    if rank != 0:
+        return
+    try:
+        from oracle.bindings import RefSolver, make_solver
+    except Exception as exc:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle import failed: {exc}"}))
+        return
+    kind = "reference" if RefSolver.available() else "port"
+    wl = WORKLOADS[args.workload]
+    prob = make_problem(wl["problem"], REF_SAMPLE_N)
+    solver = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
+    for _ in range(args.warmup):
+        solver.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solver.step()
+    t = time.perf_counter() - t0
+    cells = prob.nx * prob.ny * wl["rks"] * args.steps
+    value = cells / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial data)",
+        "config": {"workload": args.workload, "description": wl["desc"],
+                   "grid": f"{REF_SAMPLE_N}x{REF_SAMPLE_N} sample", "stages_per_step": wl["rks"],
+                   "parallelism": "single-threaded reference"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+                         "sample": f"{args.steps} timed time steps (after {args.warmup} warm-up) "
+                                   f"on a {REF_SAMPLE_N}x{REF_SAMPLE_N} grid of the same physics"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="imex", choices=["imex", "reference"])
+    ap.add_argument("--workload", default="vortex_sheet_1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--n", type=int, default=None, help="override the grid side (profiling cases)")
+    ap.add_argument("--json-out", default=None)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    import torch
+    import imex_b200 as ix
+
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    prob = make_problem(wl["problem"], args.n or wl["n"])
+    settings = dict(wl["settings"])
+    settings["precision"] = args.precision
+    solver = ix.Solver.for_problem(prob, wl["rks"], settings)
+    stream = torch.cuda.Stream()
+    solver.set_stream(stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        solver.step()
+    solver.reset_stats()
+    solver.profile_enable(True)
+    k0 = solver.kernel_launches()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            solver.step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t_ms = start.elapsed_time(stop)
+    launches = solver.kernel_launches() - k0
+    prof = solver.profile()
+    solver.profile_enable(False)
+    stats = solver.stats()
+    t_max = reduce_max(t_ms, world)
+    cells_per_step = prob.nx * prob.ny * wl["rks"]
+    value = world * cells_per_step * args.steps / (t_max / 1e3)
+
+    # roofline of the dominant kernel family (largest share of the timed region)
+    peak, peak_kind = measured_peaks()
+    dom = max(prof, key=lambda r: r["total_ms"])
+    achieved = dom["alg_bytes"] / (dom["total_ms"] / 1e3) / 1e9
+    traffic = ncu_traffic(dom["name"])
+    total_prof_ms = sum(r["total_ms"] for r in prof)
+    roofline = {"kernel": dom["name"], "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic if traffic is None else traffic,
+                "alg_bytes_per_launch": dom["alg_bytes"] / dom["launches"],
+                "launches": dom["launches"], "ms_per_launch": dom["total_ms"] / dom["launches"],
+                "share_of_step": dom["total_ms"] / total_prof_ms if total_prof_ms else None,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                else "fallback 6650 GB/s"}
+    step_bytes = sum(r["alg_bytes"] for r in prof)
+
+    # end to end through the C ABI: pinned host state in, step, state out, every step
+    e2e = None
+    if not args.no_e2e:
+        N = prob.nx * prob.ny
+        h_prim = torch.empty(8 * N, dtype=torch.float64, pin_memory=True)
+        h_bx = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        h_by = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        h_A = torch.empty(3 * N, dtype=torch.float64, pin_memory=True)
+        ptrs = (h_prim.data_ptr(), h_bx.data_ptr(), h_by.data_ptr(), h_A.data_ptr())
+        solver.download_state_ptr(*ptrs)
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        start.record(stream)
+        for _ in range(args.steps):
+            solver.upload_state_ptr(*ptrs)
+            solver.step()
+            solver.download_state_ptr(*ptrs)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_ms = reduce_max(max(start.elapsed_time(stop), wall * 1e3), world)
+        nbytes = (8 + 1 + 1 + 3) * N * 8
+        e2e = {"value": world * cells_per_step * args.steps / (e2e_ms / 1e3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "path": "imex_upload_state + imex_step + imex_download_state, pinned host buffers"}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                cpu = cpu_reference_rate(steps=3, max_seconds=12.0)
+                cpu.pop("seconds", None)
+            except Exception as exc:
+                cpu = {"value": None, "error": str(exc)}
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic initial data, no dataset)",
+            "config": {"workload": args.workload, "description": wl["desc"],
+                       "grid": f"{prob.nx}x{prob.ny}", "stages_per_step": wl["rks"],
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "working set ~2 GB >> 126 MB L2; no flush"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "solver": {"gmres_iters": stats["gmres_iters"], "gmres_solves": stats["gmres_solves"],
+                       "newton_iters": stats["newton_iters"], "status": stats["status"],
+                       "alg_bytes_per_step": step_bytes / args.steps,
+                       "stage_hbm_frac": step_bytes / (t_ms / 1e3) / 1e9 / peak},
+            "kernels": sorted(({"name": r["name"], "share": r["total_ms"] / total_prof_ms,
+                                "launches": r["launches"],
+                                "GBps": r["alg_bytes"] / (r["total_ms"] / 1e3) / 1e9 if r["total_ms"] else 0}
+                               for r in prof), key=lambda r: -r["share"]),
+        }
+        print(json.dumps(line))
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                json.dump(line, f, indent=1)
+    solver.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

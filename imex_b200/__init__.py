@@ -88,6 +88,11 @@ class SolveStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class KernelProfile(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double),
+                ("alg_bytes", C.c_double)]
+
+
 _D = C.POINTER(C.c_double)
 _SIGS = {
     "imex_config_default": (None, [C.POINTER(Config)]),
@@ -99,6 +104,7 @@ _SIGS = {
     "imex_last_error": (C.c_char_p, [C.c_void_p]),
     "imex_get_config": (C.c_int, [C.c_void_p, C.POINTER(Config)]),
     "imex_upload_prim": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "imex_upload_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "imex_download_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D]),
     "imex_step": (C.c_int, [C.c_void_p, _D]),
     "imex_begin_step": (C.c_int, [C.c_void_p]),
@@ -132,6 +138,10 @@ _SIGS = {
     "imex_reset_stats": (C.c_int, [C.c_void_p]),
     "imex_divergence": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "imex_min_pressure": (C.c_int, [C.c_void_p, _D]),
+    "imex_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "imex_profile_read": (C.c_int, [C.c_void_p, C.POINTER(KernelProfile), C.c_int,
+                                    C.POINTER(C.c_int)]),
+    "imex_kernel_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
 }
 
 _lib = None
@@ -259,6 +269,38 @@ class Solver:
         out = self._planes(3)
         self._check(self.lib.imex_download_state(self.ctx, None, None, None, None, _dp(out)))
         return out
+
+    def upload_state(self, prim, bx, by, A) -> None:
+        """Hand the solver a state mid-run (keeps t, the step counter and dt history)."""
+        prim, bx, by, A = _c(prim), _c(bx), _c(by), _c(A)
+        self._check(self.lib.imex_upload_state(self.ctx, _dp(prim), _dp(bx), _dp(by), _dp(A)))
+
+    def upload_state_ptr(self, prim: int, bx: int, by: int, A: int) -> None:
+        """Same with raw host or device addresses (e.g. pinned buffers)."""
+        self._check(self.lib.imex_upload_state(self.ctx, C.cast(prim, _D), C.cast(bx, _D),
+                                               C.cast(by, _D), C.cast(A, _D)))
+
+    def download_state_ptr(self, prim: int, bx: int, by: int, A: int) -> None:
+        self._check(self.lib.imex_download_state(self.ctx, None, C.cast(prim, _D), C.cast(bx, _D),
+                                                 C.cast(by, _D), C.cast(A, _D)))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._check(self.lib.imex_set_stream(self.ctx, C.c_void_p(stream_ptr or 0)))
+
+    def profile_enable(self, on: bool = True) -> None:
+        self._check(self.lib.imex_profile_enable(self.ctx, 1 if on else 0))
+
+    def profile(self) -> list[dict]:
+        buf = (KernelProfile * 64)()
+        n = C.c_int()
+        self._check(self.lib.imex_profile_read(self.ctx, buf, 64, C.byref(n)))
+        return [dict(name=buf[k].name.decode(), launches=buf[k].launches,
+                     total_ms=buf[k].total_ms, alg_bytes=buf[k].alg_bytes) for k in range(n.value)]
+
+    def kernel_launches(self) -> int:
+        n = C.c_longlong()
+        self._check(self.lib.imex_kernel_launch_count(self.ctx, C.byref(n)))
+        return n.value
 
     # ---- stepping
     def step(self) -> float:

@@ -18,6 +18,54 @@ imex_status cuda_check(imex_ctx* ctx, cudaError_t e, const char* what) {
   return set_error(ctx, IMEX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// ---- live profile
+static const char* kFamilyNames[NFAM] = {
+    "step_reduce", "cons_from_prim", "stage_combine", "reconstruct", "flux_convective", "flux_pressure",
+    "magnetic_rhs", "gmres_magnetic_B", "gmres_magnetic_A", "magnetic_out", "collect_mag_fluxes",
+    "pressure_setup", "shock_detector", "pressure_rhs", "nested_newton", "momentum", "energy_define",
+    "constrained_transport", "stage_derivative", "gmax", "gmres_pressure", "apply_operator", "mixed_refine"};
+const char* family_name(int fam) { return fam >= 0 && fam < NFAM ? kFamilyNames[fam] : "?"; }
+
+static cudaEvent_t prof_event(imex_ctx* ctx) {
+  if (!ctx->prof_pool.empty()) {
+    cudaEvent_t e = ctx->prof_pool.back();
+    ctx->prof_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+void prof_begin(imex_ctx* ctx) {
+  if (!ctx->prof_on) return;
+  ctx->prof_open = prof_event(ctx);
+  cudaEventRecord(ctx->prof_open, ctx->stream);
+}
+void prof_end(imex_ctx* ctx, int fam, double bytes, int kernels) {
+  ctx->kernel_launches += kernels;
+  if (!ctx->prof_on || !ctx->prof_open) return;
+  cudaEvent_t b = prof_event(ctx);
+  cudaEventRecord(b, ctx->stream);
+  ctx->prof_pending.push_back(ProfRec{ctx->prof_open, b, fam, bytes});
+  ctx->prof_open = nullptr;
+  if (ctx->prof_pending.size() > 4096) prof_harvest(ctx);
+}
+void prof_harvest(imex_ctx* ctx) {
+  if (ctx->prof_pending.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (const ProfRec& r : ctx->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      ctx->prof_ms[r.fam] += ms;
+      ctx->prof_bytes[r.fam] += r.bytes;
+      ctx->prof_launches[r.fam] += 1;
+    }
+    ctx->prof_pool.push_back(r.a);
+    ctx->prof_pool.push_back(r.b);
+  }
+  ctx->prof_pending.clear();
+}
+
 // EOS iteration-cap flags of the two kernel translation units
 imex_status eos_flag_stage(imex_ctx* ctx, int* flag, bool reset);
 imex_status eos_flag_solve(imex_ctx* ctx, int* flag, bool reset);
@@ -128,7 +176,7 @@ imex_status stage_body(imex_ctx* ctx, int rks) {
   const DevParams& P = ctx->P;
   imex_status s;
   if ((s = launch_stage_combine(ctx, rks)) != IMEX_OK) return s;
-  if ((s = launch_reconstruct(ctx)) != IMEX_OK) return s;
+  if ((s = launch_reconstruct(ctx, false)) != IMEX_OK) return s;
   if ((s = launch_flux_update(ctx, 0)) != IMEX_OK) return s;
   if (P.magfield == IMEX_PotentialA) s = run_mag_subsystem_A(ctx);
   else s = run_mag_subsystem_B(ctx);
@@ -376,6 +424,8 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
 imex_status imex_destroy(imex_ctx* ctx) {
   if (!ctx) return IMEX_OK;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  prof_harvest(ctx);
+  for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
   for (void* p : ctx->allocations) cudaFree(p);
   if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
@@ -427,6 +477,18 @@ imex_status imex_upload_prim(imex_ctx* ctx, const double* prim8, const double* b
   ctx->h_sc->timestep = 0;
   ctx->h_sc->prev_dt = 0.0;
   return write_scalars(ctx);
+}
+
+imex_status imex_upload_state(imex_ctx* ctx, const double* prim8, const double* bx, const double* by,
+                              const double* A3) {
+  if (!ctx || !prim8 || !bx || !by || !A3) return IMEX_ERR_INVALID;
+  const size_t pl = ctx->N * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(ctx->prim, prim8, 8 * pl, cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->bx, bx, pl, cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by, by, pl, cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A, A3, 3 * pl, cudaMemcpyDefault, ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "state upload");
+  return launch_cons_from_prim(ctx);
 }
 
 imex_status imex_download_state(imex_ctx* ctx, double* cons8, double* prim8, double* bx, double* by, double* A3) {
@@ -519,7 +581,7 @@ imex_status imex_stage_combine(imex_ctx* ctx, int rks) {
 }
 imex_status imex_TVDReconstruction(imex_ctx* ctx) {
   if (!ctx) return IMEX_ERR_INVALID;
-  return launch_reconstruct(ctx);
+  return launch_reconstruct(ctx, true);
 }
 imex_status imex_RusanovC_Update(imex_ctx* ctx, double h, int rks) {
   if (!ctx) return IMEX_ERR_INVALID;
@@ -678,6 +740,45 @@ imex_status imex_divergence(imex_ctx* ctx, double* face_l2, double* wrapped_l2, 
   if (wrapped_l2) *wrapped_l2 = o[1];
   if (ref_l2) *ref_l2 = o[2];
   if (cell_inf) *cell_inf = o[3];
+  return IMEX_OK;
+}
+imex_status imex_profile_enable(imex_ctx* ctx, int on) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  prof_harvest(ctx);
+  for (int f = 0; f < NFAM; ++f) {
+    ctx->prof_ms[f] = 0.0;
+    ctx->prof_bytes[f] = 0.0;
+    ctx->prof_launches[f] = 0;
+  }
+  static const double zeros[NFAM] = {};
+  cudaError_t e = cudaMemcpyAsync(ctx->st->alg_bytes, zeros, sizeof(zeros), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  ctx->prof_on = on != 0;
+  return cuda_check(ctx, e, "profile reset");
+}
+imex_status imex_kernel_launch_count(const imex_ctx* ctx, long long* count) {
+  if (!ctx || !count) return IMEX_ERR_INVALID;
+  *count = ctx->kernel_launches;
+  return IMEX_OK;
+}
+imex_status imex_profile_read(imex_ctx* ctx, imex_kernel_profile* out, int max, int* count) {
+  if (!ctx || !out || !count) return IMEX_ERR_INVALID;
+  prof_harvest(ctx);
+  double dev[NFAM];
+  cudaError_t e = cudaMemcpyAsync(dev, ctx->st->alg_bytes, sizeof(dev), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "profile readback");
+  int n = 0;
+  for (int f = 0; f < NFAM && n < max; ++f) {
+    if (ctx->prof_launches[f] == 0) continue;
+    imex_kernel_profile& r = out[n++];
+    std::memset(&r, 0, sizeof(r));
+    std::strncpy(r.name, family_name(f), sizeof(r.name) - 1);
+    r.launches = ctx->prof_launches[f];
+    r.total_ms = ctx->prof_ms[f];
+    r.alg_bytes = ctx->prof_bytes[f] + dev[f];
+  }
+  *count = n;
   return IMEX_OK;
 }
 imex_status imex_min_pressure(imex_ctx* ctx, double* pmin) {

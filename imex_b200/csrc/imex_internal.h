@@ -35,12 +35,27 @@ struct DevScalars {
   int pad;
 };
 
+// Kernel launch families of the live profile.
+enum Family {
+  F_PROLOGUE_REDUCE, F_CONS_FROM_PRIM, F_COMBINE, F_RECON, F_FLUX_CONV, F_FLUX_PRES, F_MAG_RHS,
+  F_GMRES_MAG_B, F_GMRES_MAG_A, F_MAG_OUT, F_COLLECT_FLUX, F_PRES_SETUP, F_SHOCK, F_PRES_RHS, F_NEWTON,
+  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, NFAM
+};
+
 // Device-side counters and status of the implicit solves.
 struct DevStats {
   int gmres_solves, gmres_iters, gmres_restarts, newton_iters, max_floored, refine_sweeps;
   int status;      // worst imex_status
   int barrier_fail;
   double last_residual, min_p;
+  double alg_bytes[NFAM];  // algorithmic bytes counted by the persistent kernels
+};
+
+// Host-side event profiler of launch families.
+struct ProfRec {
+  cudaEvent_t a, b;
+  int fam;
+  double bytes;
 };
 
 // Grid-barrier and reduction workspace of the persistent solver kernels.
@@ -96,9 +111,24 @@ struct imex_ctx {
   double* red = nullptr;    // small reduction buffer (device)
   double* h_red = nullptr;  // pinned mirror
   std::vector<void*> allocations;
+  // live profile
+  bool prof_on = false;
+  std::vector<imex::ProfRec> prof_pending;
+  std::vector<cudaEvent_t> prof_pool;
+  double prof_ms[imex::NFAM] = {};
+  double prof_bytes[imex::NFAM] = {};
+  long long prof_launches[imex::NFAM] = {};
+  cudaEvent_t prof_open = nullptr;
+  long long kernel_launches = 0;  // every kernel this context launched
 };
 
 namespace imex {
+
+// live profile: bracket a launch family with events (no-ops when profiling is off)
+void prof_begin(imex_ctx* ctx);
+void prof_end(imex_ctx* ctx, int fam, double bytes, int kernels);
+void prof_harvest(imex_ctx* ctx);
+const char* family_name(int fam);
 
 // error helpers
 imex_status set_error(imex_ctx* ctx, imex_status s, const std::string& msg);
@@ -107,7 +137,7 @@ imex_status cuda_check(imex_ctx* ctx, cudaError_t e, const char* what);
 // launchers implemented in kernels_stage.cu
 imex_status launch_step_prologue(imex_ctx* ctx);
 imex_status launch_stage_combine(imex_ctx* ctx, int rks);
-imex_status launch_reconstruct(imex_ctx* ctx);
+imex_status launch_reconstruct(imex_ctx* ctx, bool full);
 imex_status launch_flux_update(imex_ctx* ctx, int pressure_form);
 imex_status launch_stage_derivative(imex_ctx* ctx, int rks);
 imex_status launch_ct(imex_ctx* ctx, int variant);

@@ -23,7 +23,7 @@
 namespace imex {
 namespace {
 
-constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int TX = 32, TY = 16, NT = 256;
 constexpr int KCAP = 30;        // largest supported restart length
 constexpr int NP = KCAP + 2;    // partial-sum slots per CTA
 constexpr long long kSpinLimit = 20000000;  // ~ seconds of __nanosleep(64); a barrier never legitimately waits this long
@@ -83,33 +83,31 @@ __host__ __device__ inline Tiling make_tiling(int nx, int ny) {
   return t;
 }
 
-// block-wide sum of the K per-thread values v[k]; slot dst(k) (or none if < 0) of
-// `out` receives the CTA total of v[k].  Register indices stay compile-time.
-template <int K, class D>
-__device__ inline void block_sum_store(double (&v)[K], D dst, double* out) {
-  __shared__ double sh[K][NT / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int d = dst(k);
-    if (d >= 0) {
-      double r = v[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-      if (lane == 0) sh[d][wid] = r;
-    }
-  }
+// Per-CTA accumulation of dot products without register arrays: each warp owns one
+// row of `wacc`; per tile, a value is warp-reduced and lane 0 adds it to the row.
+// Tiles are visited in a fixed order, so the sums are deterministic.
+struct WarpAcc {
+  double v[NT / 32][NP];
+};
+__device__ __forceinline__ void wacc_clear(WarpAcc& a) {
+  for (int q = threadIdx.x; q < (NT / 32) * NP; q += NT) (&a.v[0][0])[q] = 0.0;
   __syncthreads();
-  if (threadIdx.x < K) {
+}
+__device__ __forceinline__ void wacc_add(WarpAcc& a, int k, double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if ((threadIdx.x & 31) == 0) a.v[threadIdx.x >> 5][k] += x;
+}
+// CTA totals of slots [0, kn) -> out[0, kn)
+__device__ __forceinline__ void wacc_store(WarpAcc& a, int kn, double* out) {
+  __syncthreads();
+  if (threadIdx.x < kn) {
     double sum = 0.0;
-    for (int w = 0; w < NT / 32; ++w) sum += sh[threadIdx.x][w];
+    for (int w = 0; w < NT / 32; ++w) sum += a.v[w][threadIdx.x];
     out[threadIdx.x] = sum;
   }
   __syncthreads();
 }
-struct Slot0 {
-  __device__ __forceinline__ int operator()(int k) const { return k == 0 ? 0 : -1; }
-};
 
 // identical-in-every-CTA reduction of partial[0..nblk)[0..kn) into red[0..kn)
 __device__ inline void grid_sum(const double* partial, int nblk, int kn, double* red) {
@@ -123,11 +121,43 @@ __device__ inline void grid_sum(const double* partial, int nblk, int kn, double*
   }
   __syncthreads();
 }
+// ------------------------------------------------------------------ tiles
+// A CTA works on a TX x TY tile of interior cells plus a halo; each thread owns
+// CPT cells of the tile (rows ly and ly + RY).  The vector being multiplied and
+// the operator's frozen coefficients are staged in shared memory together.
+constexpr int RY = NT / TX;     // rows covered by one pass of the CTA
+constexpr int CPT = TY / RY;    // interior cells per thread
+
+__device__ __forceinline__ int wrapc(int i, int n) {
+  if (i < 0) {
+    i += n;
+    if (i < 0) i = wrap(i, n);
+  } else if (i >= n) {
+    i -= n;
+    if (i >= n) i = wrap(i, n);
+  }
+  return i;
+}
+
+template <class Op>
+struct TileBuf {
+  static constexpr int H = Op::HALO;
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SN = SX * SY;
+  static constexpr int PX = TX + 2, PY = TY + 2, PN = PX * PY;  // halo-1 region of the pre-pass
+  double s[Op::M * SN];           // vector tile
+  double c[Op::QT * SN];          // frozen coefficients on the same cells
+  double p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
+};
+
 // ------------------------------------------------------------------ operators
 // Pressure_Subsystem_AX (implicit_operators.cpp:505-616), GLF viscosity, periodic,
 // with the frozen coefficient planes of one solve; precP (implicit_operators.cpp:650-662).
 struct PressureOp {
   static constexpr int M = 1, HALO = 1;
+  static constexpr int COEF = 5;  // hh, eta, rho, vscale, tdiag (+ vdiag in J mode)
+  static constexpr int QT = 2;    // staged: hh, eta
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 2;
   DevParams P;
   const DevScalars* sc;
   const double *hh, *eta, *rho, *vscale, *tdiag, *vdiag;
@@ -152,19 +182,24 @@ struct PressureOp {
     cvy = nu_y / (P.dy * P.dy);
     a = 1.0 / (P.gamma - 1.0);
   }
-  __device__ __forceinline__ void matvec(const double* s, int sx, int sn, int lx, int ly, long long c, int gi, int gj,
-                                         double* out) const {
-    (void)sn;
-    const int o = ly * sx + lx;
-    const double xc = s[o], xe = s[o + 1], xw = s[o - 1], xn = s[o + sx], xs = s[o - sx];
-    const long long e = cid(P, gi + 1, gj), w = cid(P, gi - 1, gj), n = cid(P, gi, gj + 1), so = cid(P, gi, gj - 1);
-    const double h00 = __ldg(hh + c), hp0 = __ldg(hh + e), hm0 = __ldg(hh + w), h0p = __ldg(hh + n),
-                 h0m = __ldg(hh + so);
+  __device__ __forceinline__ void coef(long long c, double* q) const {
+    q[0] = __ldg(hh + c);
+    q[1] = __ldg(eta + c);
+  }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB&, int, int) const {}
+  template <class TB>
+  __device__ __forceinline__ void matvec(const TB& tb, int lx, int ly, long long c, double* out) const {
+    const int sx = TB::SX, o = (ly + 1) * sx + lx + 1;
+    const double* x = tb.s;
+    const double* hq = tb.c;
+    const double* eq = tb.c + TB::SN;
+    const double xc = x[o], xe = x[o + 1], xw = x[o - 1], xn = x[o + sx], xs = x[o - sx];
+    const double h00 = hq[o], hp0 = hq[o + 1], hm0 = hq[o - 1], h0p = hq[o + sx], h0m = hq[o - sx];
     const double Vd = jac ? __ldcg(vdiag + c) : a;
     double r = Vd * xc - hh2 * (idx2 * (0.5 * (hp0 + h00) * (xe - xc) - 0.5 * (h00 + hm0) * (xc - xw)) +
                                 idy2 * (0.5 * (h0p + h00) * (xn - xc) - 0.5 * (h0m + h00) * (xc - xs)));
-    const double ec = __ldg(eta + c), ee = __ldg(eta + e), ew = __ldg(eta + w), en = __ldg(eta + n),
-                 es = __ldg(eta + so);
+    const double ec = eq[o], ee = eq[o + 1], ew = eq[o - 1], en = eq[o + sx], es = eq[o - sx];
     double lap = cvx * (0.5 * (ee + ec) * (xe - xc) - 0.5 * (ec + ew) * (xc - xw)) +
                  cvy * (0.5 * (en + ec) * (xn - xc) - 0.5 * (ec + es) * (xc - xs));
     out[0] = r - __ldg(vscale + c) * h * lap;
@@ -178,180 +213,221 @@ struct PressureOp {
 // Magnetic_Subsystem_AX (implicit_operators.cpp:141-353), GLF viscosity, periodic.
 struct MagneticBOp {
   static constexpr int M = 3, HALO = 1;
+  static constexpr int COEF = 4;  // Qe B (3), rho
+  static constexpr int QT = 4;    // staged: Qe Bx, By, Bz, rho
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 1;  // the 9-point stencil keeps many corner averages live
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
-  double h, nu_x, nu_y;
+  double h, nu_x, nu_y, cx, cy;
   __device__ __forceinline__ void bind() {
     h = sc->h;
     nu_x = sc->B_max_x * P.dx;
     nu_y = sc->B_max_y * P.dy;
+    cx = nu_x / (P.dx * P.dx);
+    cy = nu_y / (P.dy * P.dy);
   }
+  __device__ __forceinline__ void coef(long long c, double* q) const {
+    q[0] = __ldg(Qe + 5 * P.N + c);
+    q[1] = __ldg(Qe + 6 * P.N + c);
+    q[2] = __ldg(Qe + 7 * P.N + c);
+    q[3] = __ldg(rho + c);
+  }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB&, int, int) const {}
   __device__ __forceinline__ void precond(long long, double*) const {}
-  __device__ void matvec(const double* s, int sx, int sn, int lx, int ly, long long c, int gi, int gj,
-                         double* out) const {
-    const long long N = P.N;
+  template <class TB>
+  __device__ void matvec(const TB& tb, int lx, int ly, long long, double* out) const {
+    constexpr int SX = TB::SX, SN = TB::SN;
     const double dx = P.dx, dy = P.dy;
-    // neighbour cells: index (di+1) + 3 (dj+1)
-    long long cc[9];
-#pragma unroll
-    for (int dj = -1; dj <= 1; ++dj)
-#pragma unroll
-      for (int di = -1; di <= 1; ++di) cc[(di + 1) + 3 * (dj + 1)] = cid(P, gi + di, gj + dj);
-    double q5[9], q6[9], q7[9], x5[9], x6[9], x7[9];
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
-      q5[t] = __ldg(Qe + 5 * N + cc[t]);
-      q6[t] = __ldg(Qe + 6 * N + cc[t]);
-      q7[t] = __ldg(Qe + 7 * N + cc[t]);
-      const int so = (ly + t / 3 - 1) * sx + (lx + t % 3 - 1);
-      x5[t] = s[so];
-      x6[t] = s[sn + so];
-      x7[t] = s[2 * sn + so];
+    const int o = (ly + 1) * SX + lx + 1;
+    // offsets: C, E, W, N, S, NE, SE, NW, SW
+    const int E = o + 1, W = o - 1, No = o + SX, S = o - SX, NE = No + 1, SE = S + 1, NW = No - 1, SW = S - 1;
+    const double* q5 = tb.c;
+    const double* q6 = tb.c + SN;
+    const double* q7 = tb.c + 2 * SN;
+    const double* rr = tb.c + 3 * SN;
+    const double* x5 = tb.s;
+    const double* x6 = tb.s + SN;
+    const double* x7 = tb.s + 2 * SN;
+    const double r0 = rr[o];
+    const double rho_p0 = 0.5 * (r0 + rr[E]), rho_m0 = 0.5 * (r0 + rr[W]);
+    const double rho_0p = 0.5 * (r0 + rr[No]), rho_0m = 0.5 * (r0 + rr[S]);
+#define FA(a, t) (0.5 * (a[o] + a[t]))
+#define CA(a, t1, t2, t3) (0.25 * (a[o] + a[t1] + a[t2] + a[t3]))
+#define QX(t) (0.5 * (q5[t] * x5[t] + q6[t] * x6[t] + q7[t] * x7[t]))
+    const double Bxn_pp = CA(q5, E, No, NE), Bxn_pm = CA(q5, E, S, SE), Bxn_mp = CA(q5, W, No, NW),
+                 Bxn_mm = CA(q5, W, S, SW);
+    const double Byn_pp = CA(q6, E, No, NE), Byn_pm = CA(q6, E, S, SE), Byn_mp = CA(q6, W, No, NW),
+                 Byn_mm = CA(q6, W, S, SW);
+    const double Bzn_pp = CA(q7, E, No, NE), Bzn_pm = CA(q7, E, S, SE), Bzn_mp = CA(q7, W, No, NW),
+                 Bzn_mm = CA(q7, W, S, SW);
+    const double Bx_pp = CA(x5, E, No, NE), Bx_pm = CA(x5, E, S, SE), Bx_mp = CA(x5, W, No, NW),
+                 Bx_mm = CA(x5, W, S, SW);
+    const double By_pp = CA(x6, E, No, NE), By_pm = CA(x6, E, S, SE), By_mp = CA(x6, W, No, NW),
+                 By_mm = CA(x6, W, S, SW);
+    const double Bz_pp = CA(x7, E, No, NE), Bz_pm = CA(x7, E, S, SE), Bz_mp = CA(x7, W, No, NW),
+                 Bz_mm = CA(x7, W, S, SW);
+    // the energy-like corner sums shared by several terms
+    const double Wpp = 0.5 * (Bxn_pp * Bx_pp + Byn_pp * By_pp + Bzn_pp * Bz_pp);
+    const double Wpm = 0.5 * (Bxn_pm * Bx_pm + Byn_pm * By_pm + Bzn_pm * Bz_pm);
+    const double Wmp = 0.5 * (Bxn_mp * Bx_mp + Byn_mp * By_mp + Bzn_mp * Bz_mp);
+    const double Wmm = 0.5 * (Bxn_mm * Bx_mm + Byn_mm * By_mm + Bzn_mm * Bz_mm);
+    const double QXc = QX(o);
+    {  // x component (implicit_operators.cpp:266-275)
+      const double QXn = QX(No), QXs = QX(S);
+      const double Bx_1 = FA(q5, No) / rho_0p *
+                          (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
+                           1 / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
+      const double Bx_2 = FA(q6, No) / rho_0p *
+                          (1 / dx * ((Wpp - Bxn_pp * Bx_pp) - (Wmp - Bxn_mp * Bx_mp)) -
+                           1 / dy * (q6[No] * x5[No] - q6[o] * x5[o]));
+      const double Bx_3 = FA(q5, S) / rho_0m *
+                          (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
+                           1 / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
+      const double Bx_4 = FA(q6, S) / rho_0m *
+                          (1 / dx * ((Wpm - Bxn_pm * Bx_pm) - (Wmm - Bxn_mm * Bx_mm)) -
+                           1 / dy * (q6[o] * x5[o] - q6[S] * x5[S]));
+      const double ax5 = x5[o] + (h * h / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
+      out[0] = ax5 - h * (cx * (x5[W] - 2.0 * x5[o] + x5[E]) + cy * (x5[S] - 2.0 * x5[o] + x5[No]));
     }
-    // C=4 centre, E=5, W=3, N=7, S=1, NE=8, SE=2, NW=6, SW=0
-    const double r0 = __ldg(rho + c);
-    const double rho_p0 = 0.5 * (r0 + __ldg(rho + cc[5])), rho_m0 = 0.5 * (r0 + __ldg(rho + cc[3]));
-    const double rho_0p = 0.5 * (r0 + __ldg(rho + cc[7])), rho_0m = 0.5 * (r0 + __ldg(rho + cc[1]));
-#define FA(a, t) (0.5 * (a[4] + a[t]))
-#define CA(a, t1, t2, t3) (0.25 * (a[4] + a[t1] + a[t2] + a[t3]))
-    const double Bxn_p0 = FA(q5, 5), Bxn_m0 = FA(q5, 3), Bxn_0p = FA(q5, 7), Bxn_0m = FA(q5, 1);
-    const double Bxn_pp = CA(q5, 5, 7, 8), Bxn_pm = CA(q5, 5, 1, 2), Bxn_mp = CA(q5, 3, 7, 6), Bxn_mm = CA(q5, 3, 1, 0);
-    const double Byn_p0 = FA(q6, 5), Byn_m0 = FA(q6, 3), Byn_0p = FA(q6, 7), Byn_0m = FA(q6, 1);
-    const double Byn_pp = CA(q6, 5, 7, 8), Byn_pm = CA(q6, 5, 1, 2), Byn_mp = CA(q6, 3, 7, 6), Byn_mm = CA(q6, 3, 1, 0);
-    const double Bzn_p0 = FA(q7, 5), Bzn_m0 = FA(q7, 3), Bzn_0p = FA(q7, 7), Bzn_0m = FA(q7, 1);
-    const double Bzn_pp = CA(q7, 5, 7, 8), Bzn_pm = CA(q7, 5, 1, 2), Bzn_mp = CA(q7, 3, 7, 6), Bzn_mm = CA(q7, 3, 1, 0);
-    const double Bx_pp = CA(x5, 5, 7, 8), Bx_pm = CA(x5, 5, 1, 2), Bx_mp = CA(x5, 3, 7, 6), Bx_mm = CA(x5, 3, 1, 0);
-    const double By_pp = CA(x6, 5, 7, 8), By_pm = CA(x6, 5, 1, 2), By_mp = CA(x6, 3, 7, 6), By_mm = CA(x6, 3, 1, 0);
-    const double Bz_pp = CA(x7, 5, 7, 8), Bz_pm = CA(x7, 5, 1, 2), Bz_mp = CA(x7, 3, 7, 6), Bz_mm = CA(x7, 3, 1, 0);
+    const double QXe = QX(E), QXw = QX(W);
+    {  // y component (implicit_operators.cpp:277-285)
+      const double By_1 = FA(q6, E) / rho_p0 *
+                          (-1 / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
+                           1 / dy * (Bxn_pp * By_pp - Bxn_pm * By_pm));
+      const double By_2 = FA(q5, E) / rho_p0 *
+                          (-1 / dx * (q5[E] * x6[E] - q5[o] * x6[o]) +
+                           1 / dy * ((Wpp - Byn_pp * By_pp) - (Wpm - Byn_pm * By_pm)));
+      const double By_3 = FA(q6, W) / rho_m0 *
+                          (-1 / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
+                           1 / dy * (Bxn_mp * By_mp - Bxn_mm * By_mm));
+      const double By_4 = FA(q5, W) / rho_m0 *
+                          (-1 / dx * (q5[o] * x6[o] - q5[W] * x6[W]) +
+                           1 / dy * ((Wmp - Byn_mp * By_mp) - (Wmm - Byn_mm * By_mm)));
+      const double ax6 = x6[o] + (h * h / dx) * ((By_1 + By_2) - (By_3 + By_4));
+      out[1] = ax6 - h * (cx * (x6[W] - 2.0 * x6[o] + x6[E]) + cy * (x6[S] - 2.0 * x6[o] + x6[No]));
+    }
+    {  // z component (implicit_operators.cpp:288-306)
+      const double QXn = QX(No), QXs = QX(S);
+      const double Bz_1 = FA(q7, E) / rho_p0 *
+                          (-1 / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
+                           1 / dy * (Byn_pp * Bx_pp - Byn_pm * Bx_pm));
+      const double Bz_2 = FA(q5, E) / rho_p0 *
+                          (-1 / dx * (q5[E] * x7[E] - q5[o] * x7[o]) - 1 / dy * (Byn_pp * Bz_pp - Byn_pm * Bz_pm));
+      const double Bz_3 = FA(q7, W) / rho_m0 *
+                          (-1 / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
+                           1 / dy * (Byn_mp * Bx_mp - Byn_mm * Bx_mm));
+      const double Bz_4 = FA(q5, W) / rho_m0 *
+                          (-1 / dx * (q5[o] * x7[o] - q5[W] * x7[W]) - 1 / dy * (Byn_mp * Bz_mp - Byn_mm * Bz_mm));
+      const double Bz_5 = FA(q7, No) / rho_0p *
+                          (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
+                           1 / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
+      const double Bz_6 = FA(q6, No) / rho_0p *
+                          (-1 / dx * (Bxn_pp * Bz_pp - Bxn_mp * Bz_mp) - 1 / dy * (q6[No] * x7[No] - q6[o] * x7[o]));
+      const double Bz_7 = FA(q7, S) / rho_0m *
+                          (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
+                           1 / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
+      const double Bz_8 = FA(q6, S) / rho_0m *
+                          (-1 / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - 1 / dy * (q6[o] * x7[o] - q6[S] * x7[S]));
+      const double ax7 =
+          x7[o] + h * h / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + h * h / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
+      out[2] = ax7 - h * (cx * (x7[W] - 2.0 * x7[o] + x7[E]) + cy * (x7[S] - 2.0 * x7[o] + x7[No]));
+    }
 #undef FA
 #undef CA
-#define QX(t) (0.5 * (q5[t] * x5[t] + q6[t] * x6[t] + q7[t] * x7[t]))
-    const double Bx_1 = Bxn_0p / rho_0p *
-                        (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
-                         1 / dy * ((QX(7) - q6[7] * x6[7]) - (QX(4) - q6[4] * x6[4])));
-    const double Bx_2 = Byn_0p / rho_0p *
-                        (1 / dx * ((0.5 * (Bxn_pp * Bx_pp + Byn_pp * By_pp + Bzn_pp * Bz_pp) - Bxn_pp * Bx_pp) -
-                                   (0.5 * (Bxn_mp * Bx_mp + Byn_mp * By_mp + Bzn_mp * Bz_mp) - Bxn_mp * Bx_mp)) -
-                         1 / dy * (q6[7] * x5[7] - q6[4] * x5[4]));
-    const double Bx_3 = Bxn_0m / rho_0m *
-                        (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
-                         1 / dy * ((QX(4) - q6[4] * x6[4]) - (QX(1) - q6[1] * x6[1])));
-    const double Bx_4 = Byn_0m / rho_0m *
-                        (1 / dx * ((0.5 * (Bxn_pm * Bx_pm + Byn_pm * By_pm + Bzn_pm * Bz_pm) - Bxn_pm * Bx_pm) -
-                                   (0.5 * (Bxn_mm * Bx_mm + Byn_mm * By_mm + Bzn_mm * Bz_mm) - Bxn_mm * Bx_mm)) -
-                         1 / dy * (q6[4] * x5[4] - q6[1] * x5[1]));
-    const double ax5 = x5[4] + (h * h / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
-    const double By_1 = Byn_p0 / rho_p0 *
-                        (-1 / dx * ((QX(5) - q5[5] * x5[5]) - (QX(4) - q5[4] * x5[4])) +
-                         1 / dy * (Bxn_pp * By_pp - Bxn_pm * By_pm));
-    const double By_2 = Bxn_p0 / rho_p0 *
-                        (-1 / dx * (q5[5] * x6[5] - q5[4] * x6[4]) +
-                         1 / dy * ((0.5 * (Bxn_pp * Bx_pp + Byn_pp * By_pp + Bzn_pp * Bz_pp) - Byn_pp * By_pp) -
-                                   (0.5 * (Bxn_pm * Bx_pm + Byn_pm * By_pm + Bzn_pm * Bz_pm) - Byn_pm * By_pm)));
-    const double By_3 = Byn_m0 / rho_m0 *
-                        (-1 / dx * ((QX(4) - q5[4] * x5[4]) - (QX(3) - q5[3] * x5[3])) +
-                         1 / dy * (Bxn_mp * By_mp - Bxn_mm * By_mm));
-    const double By_4 = Bxn_m0 / rho_m0 *
-                        (-1 / dx * (q5[4] * x6[4] - q5[3] * x6[3]) +
-                         1 / dy * ((0.5 * (Bxn_mp * Bx_mp + Byn_mp * By_mp + Bzn_mp * Bz_mp) - Byn_mp * By_mp) -
-                                   (0.5 * (Bxn_mm * Bx_mm + Byn_mm * By_mm + Bzn_mm * Bz_mm) - Byn_mm * By_mm)));
-    const double ax6 = x6[4] + (h * h / dx) * ((By_1 + By_2) - (By_3 + By_4));
-    const double Bz_1 = Bzn_p0 / rho_p0 *
-                        (-1 / dx * ((QX(5) - q5[5] * x5[5]) - (QX(4) - q5[4] * x5[4])) +
-                         1 / dy * (Byn_pp * Bx_pp - Byn_pm * Bx_pm));
-    const double Bz_2 = Bxn_p0 / rho_p0 *
-                        (-1 / dx * (q5[5] * x7[5] - q5[4] * x7[4]) - 1 / dy * (Byn_pp * Bz_pp - Byn_pm * Bz_pm));
-    const double Bz_3 = Bzn_m0 / rho_m0 *
-                        (-1 / dx * ((QX(4) - q5[4] * x5[4]) - (QX(3) - q5[3] * x5[3])) +
-                         1 / dy * (Byn_mp * Bx_mp - Byn_mm * Bx_mm));
-    const double Bz_4 = Bxn_m0 / rho_m0 *
-                        (-1 / dx * (q5[4] * x7[4] - q5[3] * x7[3]) - 1 / dy * (Byn_mp * Bz_mp - Byn_mm * Bz_mm));
-    const double Bz_5 = Bzn_0p / rho_0p *
-                        (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
-                         1 / dy * ((QX(7) - q6[7] * x6[7]) - (QX(4) - q6[4] * x6[4])));
-    const double Bz_6 = Byn_0p / rho_0p *
-                        (-1 / dx * (Bxn_pp * Bz_pp - Bxn_mp * Bz_mp) - 1 / dy * (q6[7] * x7[7] - q6[4] * x7[4]));
-    const double Bz_7 = Bzn_0m / rho_0m *
-                        (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
-                         1 / dy * ((QX(4) - q6[4] * x6[4]) - (QX(1) - q6[1] * x6[1])));
-    const double Bz_8 = Byn_0m / rho_0m *
-                        (-1 / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - 1 / dy * (q6[4] * x7[4] - q6[1] * x7[1]));
 #undef QX
-    const double ax7 =
-        x7[4] + h * h / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + h * h / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
-    const double cx = nu_x / (dx * dx), cy = nu_y / (dy * dy);
-    out[0] = ax5 - h * (cx * (x5[3] - 2.0 * x5[4] + x5[5]) + cy * (x5[1] - 2.0 * x5[4] + x5[7]));
-    out[1] = ax6 - h * (cx * (x6[3] - 2.0 * x6[4] + x6[5]) + cy * (x6[1] - 2.0 * x6[4] + x6[7]));
-    out[2] = ax7 - h * (cx * (x7[3] - 2.0 * x7[4] + x7[5]) + cy * (x7[1] - 2.0 * x7[4] + x7[7]));
   }
 };
 
 // Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355-503), GLF, periodic.
+// The reference evaluates B = curl A and the stress tensor T^B at the four
+// neighbours of each cell; those values are exactly curl A and T^B of the
+// neighbouring cells, so the tile pre-pass computes them once per cell (same
+// arithmetic) and the per-cell pass only differences them.
 struct MagneticAOp {
   static constexpr int M = 3, HALO = 2;
+  static constexpr int COEF = 4;  // Qe B (3), rho
+  static constexpr int QT = 3;    // staged: Qe Bx, By, Bz
+  static constexpr int PT = 6;    // Txx, Tyx, Tzx, Txy, Tyy, Tzy on the halo-1 region
+  static constexpr int MIN_BLOCKS = 2;
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
-  double h, nu_x, nu_y;
+  double h, nu_x, nu_y, cx, cy;
   int add_bvisc;
   __device__ __forceinline__ void bind() {
     h = sc->h;
     nu_x = sc->gmax_bx * P.dx;
     nu_y = sc->gmax_by * P.dy;
+    cx = nu_x / (P.dx * P.dx);
+    cy = nu_y / (P.dy * P.dy);
+  }
+  __device__ __forceinline__ void coef(long long c, double* q) const {
+    q[0] = __ldg(Qe + 5 * P.N + c);
+    q[1] = __ldg(Qe + 6 * P.N + c);
+    q[2] = __ldg(Qe + 7 * P.N + c);
   }
   __device__ __forceinline__ void precond(long long, double*) const {}
-  __device__ void matvec(const double* s, int sx, int sn, int lx, int ly, long long c, int gi, int gj,
-                         double* out) const {
-    const long long N = P.N;
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB& tb, int, int) const {
+    constexpr int SX = TB::SX, SN = TB::SN;
     const double dx = P.dx, dy = P.dy;
-    auto AG = [&](int di, int dj, int k) { return s[k * sn + (ly + dj) * sx + (lx + di)]; };
-    auto QE = [&](int k, int di, int dj) { return __ldg(Qe + k * N + cid(P, gi + di, gj + dj)); };
-    const double Bxn_00 = __ldg(Qe + 5 * N + c), Byn_00 = __ldg(Qe + 6 * N + c), Bzn_00 = __ldg(Qe + 7 * N + c);
-    const double Bxn_P0 = QE(5, 1, 0), Byn_P0 = QE(6, 1, 0), Bzn_P0 = QE(7, 1, 0);
-    const double Bxn_M0 = QE(5, -1, 0), Byn_M0 = QE(6, -1, 0), Bzn_M0 = QE(7, -1, 0);
-    const double Bxn_0P = QE(5, 0, 1), Byn_0P = QE(6, 0, 1), Bzn_0P = QE(7, 0, 1);
-    const double Bxn_0M = QE(5, 0, -1), Byn_0M = QE(6, 0, -1), Bzn_0M = QE(7, 0, -1);
-    const double rho_00 = __ldg(rho + c);
-    const double bx_P0 = (AG(1, 1, 2) - AG(1, -1, 2)) / (2.0 * dy);
-    const double by_P0 = -(AG(2, 0, 2) - AG(0, 0, 2)) / (2.0 * dx);
-    const double bz_P0 = (AG(2, 0, 1) - AG(0, 0, 1)) / (2.0 * dx) - (AG(1, 1, 0) - AG(1, -1, 0)) / (2.0 * dy);
-    const double bx_M0 = (AG(-1, 1, 2) - AG(-1, -1, 2)) / (2.0 * dy);
-    const double by_M0 = -(AG(0, 0, 2) - AG(-2, 0, 2)) / (2.0 * dx);
-    const double bz_M0 = (AG(0, 0, 1) - AG(-2, 0, 1)) / (2.0 * dx) - (AG(-1, 1, 0) - AG(-1, -1, 0)) / (2.0 * dy);
-    const double bx_0P = (AG(0, 2, 2) - AG(0, 0, 2)) / (2.0 * dy);
-    const double by_0P = -(AG(1, 1, 2) - AG(-1, 1, 2)) / (2.0 * dx);
-    const double bz_0P = (AG(1, 1, 1) - AG(-1, 1, 1)) / (2.0 * dx) - (AG(0, 2, 0) - AG(0, 0, 0)) / (2.0 * dy);
-    const double bx_0M = (AG(0, 0, 2) - AG(0, -2, 2)) / (2.0 * dy);
-    const double by_0M = -(AG(1, -1, 2) - AG(-1, -1, 2)) / (2.0 * dx);
-    const double bz_0M = (AG(1, -1, 1) - AG(-1, -1, 1)) / (2.0 * dx) - (AG(0, 0, 0) - AG(0, -2, 0)) / (2.0 * dy);
-    const double bdot_P0 = Bxn_P0 * bx_P0 + Byn_P0 * by_P0 + Bzn_P0 * bz_P0;
-    const double Txx_P0 = bdot_P0 / 2.0 - Bxn_P0 * bx_P0, Tyx_P0 = -Bxn_P0 * by_P0, Tzx_P0 = -Bxn_P0 * bz_P0;
-    const double bdot_M0 = Bxn_M0 * bx_M0 + Byn_M0 * by_M0 + Bzn_M0 * bz_M0;
-    const double Txx_M0 = bdot_M0 / 2.0 - Bxn_M0 * bx_M0, Tyx_M0 = -Bxn_M0 * by_M0, Tzx_M0 = -Bxn_M0 * bz_M0;
-    const double bdot_0P = Bxn_0P * bx_0P + Byn_0P * by_0P + Bzn_0P * bz_0P;
-    const double Txy_0P = -Byn_0P * bx_0P, Tyy_0P = bdot_0P / 2.0 - Byn_0P * by_0P, Tzy_0P = -Byn_0P * bz_0P;
-    const double bdot_0M = Bxn_0M * bx_0M + Byn_0M * by_0M + Bzn_0M * bz_0M;
-    const double Txy_0M = -Byn_0M * bx_0M, Tyy_0M = bdot_0M / 2.0 - Byn_0M * by_0M, Tzy_0M = -Byn_0M * bz_0M;
-    const double divT_x = (Txx_P0 - Txx_M0) / (2.0 * dx) + (Txy_0P - Txy_0M) / (2.0 * dy);
-    const double divT_y = (Tyx_P0 - Tyx_M0) / (2.0 * dx) + (Tyy_0P - Tyy_0M) / (2.0 * dy);
-    const double divT_z = (Tzx_P0 - Tzx_M0) / (2.0 * dx) + (Tzy_0P - Tzy_0M) / (2.0 * dy);
-    const double Fx = h / rho_00 * divT_x, Fy = h / rho_00 * divT_y, Fz = h / rho_00 * divT_z;
-    const double cross_x = Byn_00 * Fz - Bzn_00 * Fy;
-    const double cross_y = Bzn_00 * Fx - Bxn_00 * Fz;
-    const double cross_z = Bxn_00 * Fy - Byn_00 * Fx;
-    double lap[3] = {0.0, 0.0, 0.0};
-    if (add_bvisc) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-        lap[k] = nu_x / (dx * dx) * (AG(-1, 0, k) - 2.0 * AG(0, 0, k) + AG(1, 0, k)) +
-                 nu_y / (dy * dy) * (AG(0, -1, k) - 2.0 * AG(0, 0, k) + AG(0, 1, k));
+    for (int q = threadIdx.x; q < TB::PN; q += NT) {
+      const int px = q % TB::PX, py = q / TB::PX;
+      const int o = (py + 1) * SX + (px + 1);  // same cell in the halo-2 tile
+      const double* A0 = tb.s;
+      const double* A1 = tb.s + SN;
+      const double* A2 = tb.s + 2 * SN;
+      const double bx = (A2[o + SX] - A2[o - SX]) / (2.0 * dy);
+      const double by = -(A2[o + 1] - A2[o - 1]) / (2.0 * dx);
+      const double bz = (A1[o + 1] - A1[o - 1]) / (2.0 * dx) - (A0[o + SX] - A0[o - SX]) / (2.0 * dy);
+      const double Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
+      const double bdot = Bx * bx + By * by + Bz * bz;
+      tb.p[0 * TB::PN + q] = bdot / 2.0 - Bx * bx;  // Txx
+      tb.p[1 * TB::PN + q] = -Bx * by;              // Tyx
+      tb.p[2 * TB::PN + q] = -Bx * bz;              // Tzx
+      tb.p[3 * TB::PN + q] = -By * bx;              // Txy
+      tb.p[4 * TB::PN + q] = bdot / 2.0 - By * by;  // Tyy
+      tb.p[5 * TB::PN + q] = -By * bz;              // Tzy
     }
-    out[0] = AG(0, 0, 0) - h * cross_x - h * lap[0];
-    out[1] = AG(0, 0, 1) - h * cross_y - h * lap[1];
-    out[2] = AG(0, 0, 2) - h * cross_z - h * lap[2];
+  }
+  template <class TB>
+  __device__ void matvec(const TB& tb, int lx, int ly, long long c, double* out) const {
+    constexpr int SX = TB::SX, SN = TB::SN, PX = TB::PX, PN = TB::PN;
+    const double dx = P.dx, dy = P.dy;
+    const int o = (ly + 2) * SX + lx + 2;  // halo-2 tile
+    const int p = (ly + 1) * PX + lx + 1;  // halo-1 pre-pass region
+    const double* T = tb.p;
+    const double divT_x = (T[0 * PN + p + 1] - T[0 * PN + p - 1]) / (2.0 * dx) +
+                          (T[3 * PN + p + PX] - T[3 * PN + p - PX]) / (2.0 * dy);
+    const double divT_y = (T[1 * PN + p + 1] - T[1 * PN + p - 1]) / (2.0 * dx) +
+                          (T[4 * PN + p + PX] - T[4 * PN + p - PX]) / (2.0 * dy);
+    const double divT_z = (T[2 * PN + p + 1] - T[2 * PN + p - 1]) / (2.0 * dx) +
+                          (T[5 * PN + p + PX] - T[5 * PN + p - PX]) / (2.0 * dy);
+    const double hr = h / __ldg(rho + c);
+    const double Fx = hr * divT_x, Fy = hr * divT_y, Fz = hr * divT_z;
+    const double Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
+    const double cross_x = By * Fz - Bz * Fy;
+    const double cross_y = Bz * Fx - Bx * Fz;
+    const double cross_z = Bx * Fy - By * Fx;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double* A = tb.s + k * SN;
+      double lap = 0.0;
+      if (add_bvisc)
+        lap = cx * (A[o - 1] - 2.0 * A[o] + A[o + 1]) + cy * (A[o - SX] - 2.0 * A[o] + A[o + SX]);
+      const double cr = k == 0 ? cross_x : (k == 1 ? cross_y : cross_z);
+      out[k] = A[o] - h * cr - h * lap;
+    }
   }
 };
+
+template <class Op>
+__device__ __forceinline__ bool op_uses_vdiag(const Op&) { return false; }
+template <>
+__device__ __forceinline__ bool op_uses_vdiag<PressureOp>(const PressureOp& o) { return o.jac != 0; }
 
 // ------------------------------------------------------------------ GMRES
 struct GmresWork {
@@ -359,6 +435,7 @@ struct GmresWork {
   SyncState* sync;
   DevStats* st;
   int kmax, max_restarts, nblk;
+  int fam;  // profile family whose algorithmic bytes this solve accumulates
   double tol;
   Tiling T;
 };
@@ -367,28 +444,49 @@ struct GmresShared {
   double H[KCAP + 2][KCAP + 2];
   double cs[KCAP + 2], sn[KCAP + 2], gam[KCAP + 2], alpha[KCAP + 2], sigma[KCAP + 2];
   double red[NP];
+  WarpAcc acc;
 };
 
-template <class Op>
-struct TileBuf {
-  static constexpr int SX = TX + 2 * Op::HALO, SY = TY + 2 * Op::HALO, SN = SX * SY;
-  double s[Op::M * SN];
-};
-
-// fill the halo tile at origin (x0, y0) with f(global cell index) (M components)
+// Stage the vector f(cell) and the operator's coefficients on the tile at
+// (x0, y0) plus halo, then run the operator's pre-pass.
 template <class Op, class F>
-__device__ __forceinline__ void fill_tile(TileBuf<Op>& tb, const Tiling& T, int x0, int y0, F f) {
+__device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const Tiling& T, int x0, int y0, F f) {
   using TB = TileBuf<Op>;
   for (int q = threadIdx.x; q < TB::SN; q += NT) {
     const int sxq = q % TB::SX, syq = q / TB::SX;
-    const int gi = wrap(x0 + sxq - Op::HALO, T.nx), gj = wrap(y0 + syq - Op::HALO, T.ny);
+    const int gi = wrapc(x0 + sxq - Op::HALO, T.nx), gj = wrapc(y0 + syq - Op::HALO, T.ny);
     const long long c = (long long)gi + (long long)T.nx * gj;
     double v[Op::M];
     f(c, v);
 #pragma unroll
     for (int m = 0; m < Op::M; ++m) tb.s[m * TB::SN + q] = v[m];
+    double qv[Op::QT > 0 ? Op::QT : 1];
+    op.coef(c, qv);
+#pragma unroll
+    for (int m = 0; m < Op::QT; ++m) tb.c[m * TB::SN + q] = qv[m];
   }
   __syncthreads();
+  if (Op::PT > 0) {
+    op.prepass(tb, x0, y0);
+    __syncthreads();
+  }
+}
+
+// interior cell r of this thread in the tile at (x0, y0)
+struct Cell {
+  int lx, ly, gi, gj;
+  long long c;
+  bool in;
+};
+__device__ __forceinline__ Cell tile_cell(const Tiling& T, int x0, int y0, int r) {
+  Cell k;
+  k.lx = threadIdx.x % TX;
+  k.ly = threadIdx.x / TX + r * RY;
+  k.gi = x0 + k.lx;
+  k.gj = y0 + k.ly;
+  k.in = k.gi < T.nx && k.gj < T.ny;
+  k.c = (long long)k.gi + (long long)T.nx * k.gj;
+  return k;
 }
 
 // Result codes of gmres_device
@@ -402,84 +500,97 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
   const Tiling& T = g.T;
   const long long N = T.N;
   const int kmax = g.kmax;
-  const int lx = threadIdx.x % TX, ly = threadIdx.x / TX;
-  double acc[NP];
   double tol_eff = g.tol;
   int iters = 0;
   auto Vp = [&](int i) { return g.V + (long long)i * M * N; };
   auto AVp = [&](int i) { return g.AV + (long long)(i & 1) * M * N; };
   auto part = [&]() { return g.partial + (long long)(phase & 1) * g.nblk * NP; };
+  const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
+  const int coef = Op::COEF + (op_uses_vdiag(op) ? 1 : 0);
+  // algorithmic bytes of a pass that moves `vals` doubles per cell
+  auto count = [&](int vals) {
+    if (lead) g.st->alg_bytes[g.fam] += (double)vals * 8.0 * (double)N;
+  };
+  (void)HALO;
 
   for (int outer = 0; outer < g.max_restarts; ++outer) {
     // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
-    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile<Op>(tb, T, x0, y0, [&](long long c, double* v) {
+      fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
 #pragma unroll
         for (int m = 0; m < M; ++m) v[m] = ldcg(x + m * N + c);
       });
-      const int gi = x0 + lx, gj = y0 + ly;
-      if (gi < T.nx && gj < T.ny) {
-        const long long c = (long long)gi + (long long)T.nx * gj;
-        double ax[M];
-        op.matvec(tb.s, TB::SX, TB::SN, lx + HALO, ly + HALO, c, gi, gj, ax);
-        double r[M];
+      double rr = 0.0;
 #pragma unroll
-        for (int m = 0; m < M; ++m) r[m] = ldcg(b + m * N + c) - ax[m];
-        op.precond(c, r);
+      for (int r = 0; r < CPT; ++r) {
+        const Cell k = tile_cell(T, x0, y0, r);
+        if (!k.in) continue;
+        double ax[M];
+        op.matvec(tb, k.lx, k.ly, k.c, ax);
+        double res[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) res[m] = ldcg(b + m * N + k.c) - ax[m];
+        op.precond(k.c, res);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-          Vp(0)[m * N + c] = r[m];
-          acc[0] += r[m] * r[m];
+          Vp(0)[m * N + k.c] = res[m];
+          rr += res[m] * res[m];
         }
       }
+      wacc_add(S.acc, 0, rr);
       __syncthreads();
     }
-    block_sum_store<NP>(acc, Slot0(), part() + (long long)blockIdx.x * NP);
+    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
     grid_sum(part(), g.nblk, 1, S.red);
     ++phase;
+    count(3 * M + coef);
     S.gam[0] = sqrt(S.red[0]);
     if (outer == 0) tol_eff = g.tol * S.gam[0] + g.tol;
     if (!isfinite(S.gam[0])) return GM_NONFINITE;
     if (S.gam[0] <= tol_eff) {
-      if (threadIdx.x == 0 && blockIdx.x == 0) {
+      if (lead) {
         g.st->gmres_iters += iters;
         g.st->last_residual = S.gam[0];
       }
       return GM_CONVERGED;
     }
-    if (threadIdx.x == 0 && blockIdx.x == 0) g.st->gmres_restarts += 1;
+    if (lead) g.st->gmres_restarts += 1;
     S.sigma[0] = 1.0 / S.gam[0];
 
     // ---- Av0 = M^-1 A V0 (unnormalised), H[0][0]
-    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile<Op>(tb, T, x0, y0, [&](long long c, double* v) {
+      fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
 #pragma unroll
         for (int m = 0; m < M; ++m) v[m] = ldcg(Vp(0) + m * N + c);
       });
-      const int gi = x0 + lx, gj = y0 + ly;
-      if (gi < T.nx && gj < T.ny) {
-        const long long c = (long long)gi + (long long)T.nx * gj;
+      double va = 0.0;
+#pragma unroll
+      for (int r = 0; r < CPT; ++r) {
+        const Cell k = tile_cell(T, x0, y0, r);
+        if (!k.in) continue;
         double aw[M];
-        op.matvec(tb.s, TB::SX, TB::SN, lx + HALO, ly + HALO, c, gi, gj, aw);
-        op.precond(c, aw);
-        const int o = (ly + HALO) * TB::SX + lx + HALO;
+        op.matvec(tb, k.lx, k.ly, k.c, aw);
+        op.precond(k.c, aw);
+        const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-          AVp(0)[m * N + c] = aw[m];
-          acc[0] += tb.s[m * TB::SN + o] * aw[m];
+          AVp(0)[m * N + k.c] = aw[m];
+          va += tb.s[m * TB::SN + o] * aw[m];
         }
       }
+      wacc_add(S.acc, 0, va);
       __syncthreads();
     }
-    block_sum_store<NP>(acc, Slot0(), part() + (long long)blockIdx.x * NP);
+    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
     grid_sum(part(), g.nblk, 1, S.red);
     ++phase;
+    count(2 * M + coef);
     for (int r = threadIdx.x; r < (KCAP + 2) * (KCAP + 2); r += NT) (&S.H[0][0])[r] = 0.0;
     __syncthreads();
     if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[0];
@@ -489,47 +600,71 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
     bool converged = false;
     for (int j = 0; j < kmax; ++j) {
       // ---- fused pass: w = Av_j - sum_i H[i][j] v_i ; V_{j+1} = w ; AV_{j+1} = M^-1 A w ; dots
-      for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+      wacc_clear(S.acc);
       const double sj = S.sigma[j];
       for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        fill_tile<Op>(tb, T, x0, y0, [&](long long c, double* v) {
+        fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
 #pragma unroll
           for (int m = 0; m < M; ++m) {
             double wv = sj * ldcg(AVp(j) + m * N + c);
+#pragma unroll 4
             for (int i = 0; i <= j; ++i) wv = wv - S.H[i][j] * (S.sigma[i] * ldcg(Vp(i) + m * N + c));
             v[m] = wv;
           }
         });
-        const int gi = x0 + lx, gj = y0 + ly;
-        if (gi < T.nx && gj < T.ny) {
-          const long long c = (long long)gi + (long long)T.nx * gj;
-          double aw[M];
-          op.matvec(tb.s, TB::SX, TB::SN, lx + HALO, ly + HALO, c, gi, gj, aw);
-          op.precond(c, aw);
-          const int o = (ly + HALO) * TB::SX + lx + HALO;
+        double aw[CPT][M], wc[CPT][M];
+        long long cc[CPT];
+        bool in[CPT];
 #pragma unroll
-          for (int m = 0; m < M; ++m) {
-            const double wv = tb.s[m * TB::SN + o];
-            Vp(j + 1)[m * N + c] = wv;
-            AVp(j + 1)[m * N + c] = aw[m];
-            acc[KCAP] += wv * aw[m];
-            acc[KCAP + 1] += wv * wv;
+        for (int r = 0; r < CPT; ++r) {
+          const Cell k = tile_cell(T, x0, y0, r);
+          cc[r] = k.c;
+          in[r] = k.in;
+          if (k.in) {
+            op.matvec(tb, k.lx, k.ly, k.c, aw[r]);
+            op.precond(k.c, aw[r]);
+            const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
 #pragma unroll
-            for (int i = 0; i < KCAP; ++i)
-              if (i <= j) acc[i] += ldcg(Vp(i) + m * N + c) * aw[m];
+            for (int m = 0; m < M; ++m) {
+              wc[r][m] = tb.s[m * TB::SN + o];
+              Vp(j + 1)[m * N + k.c] = wc[r][m];
+              AVp(j + 1)[m * N + k.c] = aw[r][m];
+            }
+          } else {
+#pragma unroll
+            for (int m = 0; m < M; ++m) aw[r][m] = wc[r][m] = 0.0;
           }
         }
+        // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2
+        for (int i = 0; i <= j; ++i) {
+          double d = 0.0;
+#pragma unroll
+          for (int r = 0; r < CPT; ++r)
+            if (in[r]) {
+#pragma unroll
+              for (int m = 0; m < M; ++m) d += ldcg(Vp(i) + m * N + cc[r]) * aw[r][m];
+            }
+          wacc_add(S.acc, i, d);
+        }
+        double wa = 0.0, ww = 0.0;
+#pragma unroll
+        for (int r = 0; r < CPT; ++r)
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            wa += wc[r][m] * aw[r][m];
+            ww += wc[r][m] * wc[r][m];
+          }
+        wacc_add(S.acc, j + 1, wa);
+        wacc_add(S.acc, j + 2, ww);
         __syncthreads();
       }
-      // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2
-      block_sum_store<NP>(
-          acc, [j](int k) { return k <= j ? k : (k == KCAP ? j + 1 : (k == KCAP + 1 ? j + 2 : -1)); },
-          part() + (long long)blockIdx.x * NP);
+      wacc_store(S.acc, j + 3, part() + (long long)blockIdx.x * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_sum(part(), g.nblk, j + 3, S.red);
       ++phase;
       ++iters;
+      count((j + 4) * M + coef);
       if (threadIdx.x == 0) {
         // H[j+1][j] = |w|; Givens on column j (implicit_operators.cpp:857-873)
         const double beta_w = sqrt(S.red[j + 2]);
@@ -581,6 +716,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       }
     }
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
+    count((jend + 3) * M);
     if (converged) {
       if (threadIdx.x == 0 && blockIdx.x == 0) {
         g.st->gmres_iters += iters;
@@ -603,10 +739,19 @@ __device__ __forceinline__ void record_status(DevStats* st, int code) {
   }
 }
 
+// shared memory of one solver CTA (dynamic, opted in above 48 KB)
 template <class Op>
-__global__ void __launch_bounds__(NT) k_gmres(Op op, GmresWork g, double* x, const double* b) {
-  __shared__ GmresShared S;
-  __shared__ TileBuf<Op> tb;
+struct SolveSmem {
+  GmresShared S;
+  TileBuf<Op> tb;
+};
+
+template <class Op>
+__global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g, double* x, const double* b) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  SolveSmem<Op>& sm = *reinterpret_cast<SolveSmem<Op>*>(dsm);
+  GmresShared& S = sm.S;
+  TileBuf<Op>& tb = sm.tb;
   unsigned phase = 0;
   op.bind();
   if (threadIdx.x == 0 && blockIdx.x == 0) g.st->gmres_solves += 1;
@@ -622,18 +767,18 @@ struct NewtonArgs {
   DevScalars* sc;
 };
 
-__global__ void __launch_bounds__(NT) k_nested_newton(PressureOp op, GmresWork gw, NewtonArgs na) {
+__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWork gw, NewtonArgs na) {
   op.bind();
-  __shared__ GmresShared S;
-  __shared__ TileBuf<PressureOp> tb;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  SolveSmem<PressureOp>& sm = *reinterpret_cast<SolveSmem<PressureOp>*>(dsm);
+  GmresShared& S = sm.S;
+  TileBuf<PressureOp>& tb = sm.tb;
   using TB = TileBuf<PressureOp>;
   const DevParams& P = op.P;
   const Tiling& T = gw.T;
   const long long N = T.N;
-  const int lx = threadIdx.x % TX, ly = threadIdx.x / TX;
   unsigned phase = 0;
   auto part = [&]() { return gw.partial + (long long)(phase & 1) * gw.nblk * NP; };
-  double acc[NP];
   const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
 
   if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS) {
@@ -700,7 +845,10 @@ __global__ void __launch_bounds__(NT) k_nested_newton(PressureOp op, GmresWork g
     double M_cor = ((0.0 < q) ? q : 0.0) / ((1.0 - P.theta) * P.p_floor);
     double M_base = P.Mbig_fac / (P.gamma - 1.0);
     Mbig = (M_base < M_cor) ? M_cor : M_base;
-    if (lead) na.sc->Mbig = Mbig;
+    if (lead) {
+      na.sc->Mbig = Mbig;
+      gw.st->alg_bytes[gw.fam] += 3.0 * 8.0 * (double)N;
+    }
   } else {
     for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) na.pf[c] = na.p[c];
     if (!grid_barrier(gw.sync, gw.nblk)) {
@@ -717,32 +865,36 @@ __global__ void __launch_bounds__(NT) k_nested_newton(PressureOp op, GmresWork g
   int it;
   for (it = 0; it < P.Pnewton_max; it++) {
     // ---- residual g = L pf - a pf + V_mod(pf) - b  -> na.g = -g ; dp = 0 ; vdiag = V_slope(pf)
-    for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+    wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile<PressureOp>(tb, T, x0, y0, [&](long long c, double* v) { v[0] = ldcg(na.pf + c); });
-      const int gi = x0 + lx, gj = y0 + ly;
-      if (gi < T.nx && gj < T.ny) {
-        const long long c = (long long)gi + (long long)T.nx * gj;
+      fill_tile(L, tb, T, x0, y0, [&](long long c, double* v) { v[0] = ldcg(na.pf + c); });
+      double gg = 0.0;
+#pragma unroll
+      for (int r = 0; r < CPT; ++r) {
+        const Cell k = tile_cell(T, x0, y0, r);
+        if (!k.in) continue;
         double lp[1];
-        L.matvec(tb.s, TB::SX, TB::SN, lx + 1, ly + 1, c, gi, gj, lp);
-        const double pfc = tb.s[(ly + 1) * TB::SX + lx + 1];
-        const double rc = __ldg(op.rho + c);
-        const double gv = lp[0] - a * pfc + V_mod(P, Mbig, pfc, rc) - na.b[c];
-        acc[0] += gv * gv;
-        na.g[c] = -gv;
-        na.dp[c] = 0.0;
-        na.vdiag[c] = V_slope(P, Mbig, pfc, rc);
+        L.matvec(tb, k.lx, k.ly, k.c, lp);
+        const double pfc = tb.s[(k.ly + 1) * TB::SX + k.lx + 1];
+        const double rc = __ldg(op.rho + k.c);
+        const double gv = lp[0] - a * pfc + V_mod(P, Mbig, pfc, rc) - na.b[k.c];
+        gg += gv * gv;
+        na.g[k.c] = -gv;
+        na.dp[k.c] = 0.0;
+        na.vdiag[k.c] = V_slope(P, Mbig, pfc, rc);
       }
+      wacc_add(S.acc, 0, gg);
       __syncthreads();
     }
-    block_sum_store<NP>(acc, Slot0(), part() + (long long)blockIdx.x * NP);
+    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
     if (!grid_barrier(gw.sync, gw.nblk)) {
       record_status(gw.st, GM_SYNC);
       return;
     }
     grid_sum(part(), gw.nblk, 1, S.red);
     ++phase;
+    if (lead) gw.st->alg_bytes[gw.fam] += (double)(PressureOp::COEF + 5) * 8.0 * (double)N;
     const double res = sqrt(S.red[0]);
     if (it == 0) res0 = res;
     if (!isfinite(res)) {
@@ -766,8 +918,10 @@ __global__ void __launch_bounds__(NT) k_nested_newton(PressureOp op, GmresWork g
       record_status(gw.st, GM_SYNC);
       return;
     }
+    if (lead) gw.st->alg_bytes[gw.fam] += 3.0 * 8.0 * (double)N;
   }
   if (it == P.Pnewton_max && lead) atomicMax(&gw.st->status, (int)IMEX_NEWTON_MAXIT);
+  if (lead) gw.st->alg_bytes[gw.fam] += 2.0 * 8.0 * (double)N;
   // ---- p = pf, floored-cell count and min p (implicit_operators.cpp:722-737)
   double st2[2] = {0.0, INFINITY};
   for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
@@ -1065,14 +1219,29 @@ __global__ void k_gmax(DevParams P, const double* __restrict__ Qs, double* __res
   }
 }
 __global__ void k_gmax_finalize(const double* __restrict__ partial, int nblk, DevScalars* sc) {
-  if (threadIdx.x != 0) return;
   double a = 0.0, b = 0.0;
-  for (int k = 0; k < nblk; ++k) {
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
     a = fmax(a, partial[2 * k]);
     b = fmax(b, partial[2 * k + 1]);
   }
-  sc->gmax_bx = a;
-  sc->gmax_by = b;
+  __shared__ double sh[2][kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a;
+    sh[1][threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      a = fmax(a, sh[0][w]);
+      b = fmax(b, sh[1][w]);
+    }
+    sc->gmax_bx = a;
+    sc->gmax_by = b;
+  }
 }
 // B = curl A after the A solve (imex_subsystems.cpp:65-72)
 __global__ void k_curl_A(DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
@@ -1090,22 +1259,22 @@ __global__ void k_curl_A(DevParams P, const double* __restrict__ A, double* __re
 template <class Op>
 __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, double* Ax) {
   op.bind();
-  __shared__ TileBuf<Op> tb;
-  using TB = TileBuf<Op>;
-  const int lx = threadIdx.x % TX, ly = threadIdx.x / TX;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  TileBuf<Op>& tb = *reinterpret_cast<TileBuf<Op>*>(dsm);
   for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
     const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-    fill_tile<Op>(tb, T, x0, y0, [&](long long c, double* v) {
+    fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
 #pragma unroll
       for (int m = 0; m < Op::M; ++m) v[m] = x[m * T.N + c];
     });
-    const int gi = x0 + lx, gj = y0 + ly;
-    if (gi < T.nx && gj < T.ny) {
-      const long long c = (long long)gi + (long long)T.nx * gj;
-      double ax[Op::M];
-      op.matvec(tb.s, TB::SX, TB::SN, lx + Op::HALO, ly + Op::HALO, c, gi, gj, ax);
 #pragma unroll
-      for (int m = 0; m < Op::M; ++m) Ax[m * T.N + c] = ax[m];
+    for (int r = 0; r < CPT; ++r) {
+      const Cell k = tile_cell(T, x0, y0, r);
+      if (!k.in) continue;
+      double ax[Op::M];
+      op.matvec(tb, k.lx, k.ly, k.c, ax);
+#pragma unroll
+      for (int m = 0; m < Op::M; ++m) Ax[m * T.N + k.c] = ax[m];
     }
     __syncthreads();
   }
@@ -1119,13 +1288,16 @@ __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, 
     cudaError_t e_ = cudaGetLastError();                     \
     if (e_ != cudaSuccess) return cuda_check(ctx, e_, what); \
   } while (0)
+#define BYTES(vals) ((double)(vals) * 8.0 * (double)ctx->N)
 
 namespace {
 
 template <class Op>
 int coop_blocks(imex_ctx* ctx, const void* kernel, const Tiling& T) {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, 0);
+  const size_t smem = sizeof(SolveSmem<Op>);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, smem);
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 4) per_sm = 4;
   int nb = per_sm * ctx->num_sms;
@@ -1135,8 +1307,9 @@ int coop_blocks(imex_ctx* ctx, const void* kernel, const Tiling& T) {
   return nb;
 }
 
-GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk) {
+GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
   GmresWork g{};
+  g.fam = fam;
   g.V = ctx->V;
   g.AV = ctx->AV;
   g.partial = ctx->partial;
@@ -1161,7 +1334,8 @@ imex_status launch_coop(imex_ctx* ctx, K kernel, int nblk, Args... args) {
   imex_status s = reset_sync(ctx);
   if (s != IMEX_OK) return s;
   void* params[] = {(void*)&args...};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(nblk), dim3(NT), params, 0, ctx->stream);
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(nblk), dim3(NT), params,
+                                              sizeof(SolveSmem<Op>), ctx->stream);
   return cuda_check(ctx, e, "cooperative launch");
 }
 
@@ -1196,14 +1370,25 @@ MagneticAOp make_magA_op(imex_ctx* ctx) {
   return op;
 }
 
+template <class Op>
+void launch_apply(imex_ctx* ctx, const Op& o, int nb, const Tiling& T, const double* x, double* Ax) {
+  const size_t smem = sizeof(TileBuf<Op>);
+  cudaFuncSetAttribute((const void*)k_apply<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  prof_begin(ctx);
+  k_apply<Op><<<nb, NT, smem, ctx->stream>>>(o, T, x, Ax);
+  prof_end(ctx, F_APPLY, (double)(2 * Op::M + Op::COEF) * 8.0 * (double)T.N, 1);
+}
+
 imex_status pressure_setup(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
+  prof_begin(ctx);
   k_pressure_coeffs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->Qe, ctx->cons, ctx->hQe, ctx->pe, ctx->hh, ctx->vscale,
                                                      ctx->rv);
   LAUNCH_CHECK(ctx, "k_pressure_coeffs");
   k_pressure_tdiag<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->hh, ctx->tdiag);
   LAUNCH_CHECK(ctx, "k_pressure_tdiag");
+  prof_end(ctx, F_PRES_SETUP, BYTES(12 + 2), 2);
   return launch_shock(ctx, ctx->Qe, ctx->eta);
 }
 
@@ -1214,20 +1399,29 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
     o.jac = op == IMEX_OP_PRESSURE_J;
     auto kern = k_gmres<PressureOp>;
     int nb = coop_blocks<PressureOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb);
-    return launch_coop<PressureOp>(ctx, kern, nb, o, g, x, b);
+    GmresWork g = make_work(ctx, T, nb, F_GMRES_PRES);
+    prof_begin(ctx);
+    imex_status s = launch_coop<PressureOp>(ctx, kern, nb, o, g, x, b);
+    prof_end(ctx, F_GMRES_PRES, 0.0, 1);
+    return s;
   } else if (op == IMEX_OP_MAGNETIC_B) {
     MagneticBOp o = make_magB_op(ctx);
     auto kern = k_gmres<MagneticBOp>;
     int nb = coop_blocks<MagneticBOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb);
-    return launch_coop<MagneticBOp>(ctx, kern, nb, o, g, x, b);
+    GmresWork g = make_work(ctx, T, nb, F_GMRES_MAG_B);
+    prof_begin(ctx);
+    imex_status s = launch_coop<MagneticBOp>(ctx, kern, nb, o, g, x, b);
+    prof_end(ctx, F_GMRES_MAG_B, 0.0, 1);
+    return s;
   } else if (op == IMEX_OP_MAGNETIC_A) {
     MagneticAOp o = make_magA_op(ctx);
     auto kern = k_gmres<MagneticAOp>;
     int nb = coop_blocks<MagneticAOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb);
-    return launch_coop<MagneticAOp>(ctx, kern, nb, o, g, x, b);
+    GmresWork g = make_work(ctx, T, nb, F_GMRES_MAG_A);
+    prof_begin(ctx);
+    imex_status s = launch_coop<MagneticAOp>(ctx, kern, nb, o, g, x, b);
+    prof_end(ctx, F_GMRES_MAG_A, 0.0, 1);
+    return s;
   }
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
 }
@@ -1237,7 +1431,7 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   PressureOp o = make_pressure_op(ctx);
   auto kern = k_nested_newton;
   int nb = coop_blocks<PressureOp>(ctx, (const void*)kern, T);
-  GmresWork g = make_work(ctx, T, nb);
+  GmresWork g = make_work(ctx, T, nb, F_NEWTON);
   NewtonArgs na{};
   na.p = p;
   na.pf = ctx->pf;
@@ -1246,7 +1440,10 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   na.vdiag = ctx->vdiag;
   na.b = b;
   na.sc = ctx->sc;
-  return launch_coop<PressureOp>(ctx, kern, nb, o, g, na);
+  prof_begin(ctx);
+  imex_status s = launch_coop<PressureOp>(ctx, kern, nb, o, g, na);
+  prof_end(ctx, F_NEWTON, 0.0, 1);
+  return s;
 }
 
 }  // namespace
@@ -1265,13 +1462,19 @@ imex_status run_mag_subsystem_B(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   imex_status s;
   int nb = blocks_for(P.N);
+  prof_begin(ctx);
   k_magnetic_rhs_B<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->Qs, ctx->pe, ctx->mb, ctx->mx);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_B");
+  prof_end(ctx, F_MAG_RHS, BYTES(17), 1);
   if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_B, ctx->mx, ctx->mb)) != IMEX_OK) return s;
+  prof_begin(ctx);
   k_copy3<<<blocks_for(3 * P.N), kThreads, 0, ctx->stream>>>(P.N, ctx->mx, ctx->cons + 5 * P.N);
   LAUNCH_CHECK(ctx, "k_copy3");
+  prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
+  prof_begin(ctx);
   k_collect_mag_fluxes<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
   LAUNCH_CHECK(ctx, "k_collect_mag_fluxes");
+  prof_end(ctx, F_COLLECT_FLUX, BYTES(12), 1);
   return IMEX_OK;
 }
 
@@ -1281,18 +1484,24 @@ imex_status run_mag_subsystem_A(imex_ctx* ctx) {
   imex_status s;
   int nb = blocks_for(P.N);
   int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
+  prof_begin(ctx);
   k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
   LAUNCH_CHECK(ctx, "k_gmax");
-  k_gmax_finalize<<<1, 32, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
+  k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
   LAUNCH_CHECK(ctx, "k_gmax_finalize");
+  prof_end(ctx, F_GMAX, BYTES(8), 2);
+  prof_begin(ctx);
   k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->A, ctx->mb,
                                                     ctx->mx);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
+  prof_end(ctx, F_MAG_RHS, BYTES(20), 1);
   if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_A, ctx->mx, ctx->mb)) != IMEX_OK) return s;
+  prof_begin(ctx);
   k_copy3<<<blocks_for(3 * P.N), kThreads, 0, ctx->stream>>>(P.N, ctx->mx, ctx->A);
   LAUNCH_CHECK(ctx, "k_copy3");
   k_curl_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->A, ctx->cons);
   LAUNCH_CHECK(ctx, "k_curl_A");
+  prof_end(ctx, F_MAG_OUT, BYTES(6 + 6), 2);
   return IMEX_OK;
 }
 
@@ -1302,20 +1511,28 @@ imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
   imex_status s;
   if ((s = pressure_setup(ctx)) != IMEX_OK) return s;
   int nb = blocks_for(P.N);
+  prof_begin(ctx);
   k_pressure_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->rv, ctx->pb, ctx->pe,
                                                   ctx->pp);
   LAUNCH_CHECK(ctx, "k_pressure_rhs");
+  prof_end(ctx, F_PRES_RHS, BYTES(14), 1);
   if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  prof_begin(ctx);
   k_momentum<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->rv, ctx->cons);
   LAUNCH_CHECK(ctx, "k_momentum");
+  prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
   if (P.PressureSolver == IMEX_all_correction || (P.PressureSolver == IMEX_once_correction && rks == P.RKs - 1)) {
+    prof_begin(ctx);
     k_pressure_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->cons + P.N, ctx->pb,
                                                     nullptr, nullptr);
     LAUNCH_CHECK(ctx, "k_pressure_rhs(2)");
+    prof_end(ctx, F_PRES_RHS, BYTES(15), 1);
     if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
   }
+  prof_begin(ctx);
   k_energy_define<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->pp, ctx->cons);
   LAUNCH_CHECK(ctx, "k_energy_define");
+  prof_end(ctx, F_ENERGY, BYTES(9), 1);
   return IMEX_OK;
 }
 
@@ -1325,7 +1542,7 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
     const DevParams& P = ctx->P;
     int nred = blocks_for(P.N) < ctx->max_blocks ? blocks_for(P.N) : ctx->max_blocks;
     k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
-    k_gmax_finalize<<<1, 32, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
+    k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
     LAUNCH_CHECK(ctx, "k_gmax");
   }
   if ((s = set_h(ctx, h)) != IMEX_OK) return s;
@@ -1354,11 +1571,11 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
   if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
     PressureOp o = make_pressure_op(ctx);
     o.jac = op == IMEX_OP_PRESSURE_J;
-    k_apply<PressureOp><<<nb, NT, 0, ctx->stream>>>(o, T, x, Ax);
+    launch_apply(ctx, o, nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_B) {
-    k_apply<MagneticBOp><<<nb, NT, 0, ctx->stream>>>(make_magB_op(ctx), T, x, Ax);
+    launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_A) {
-    k_apply<MagneticAOp><<<nb, NT, 0, ctx->stream>>>(make_magA_op(ctx), T, x, Ax);
+    launch_apply(ctx, make_magA_op(ctx), nb, T, x, Ax);
   } else {
     return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
   }

@@ -92,11 +92,12 @@ __global__ void k_step_reduce(DevParams P, const double* __restrict__ prim, doub
 
 // caldt (timestep.cpp:5-67) + main.cpp:341-353 on one thread
 __global__ void k_step_finalize(DevParams P, const double* __restrict__ partial, int nblk, DevScalars* sc) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double v[kStepVals];
-  for (int k = 0; k < kStepVals; ++k) v[k] = partial[k];
-  for (int b = 1; b < nblk; ++b)
+  for (int k = 0; k < kStepVals; ++k) v[k] = -INFINITY;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
     for (int k = 0; k < kStepVals; ++k) v[k] = fmax(v[k], partial[b * kStepVals + k]);
+  block_reduce(v, FMax(), -INFINITY);
+  if (threadIdx.x != 0) return;
   sc->timestep += 1;
   const int ts = sc->timestep;
   sc->ch_x = v[0];
@@ -218,6 +219,7 @@ __global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc,
 // ---------------------------------------------------------------- reconstruction
 // TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes.
 // nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
+template <bool kPrim>
 __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -230,7 +232,7 @@ __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double*
     iy[d] = cid(P, i, j + d - 2);
   }
   const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
-  if (P.reconstate == IMEX_ConsState) {
+  if (!kPrim) {
     for (int k = 0; k < nstore; ++k) {
       const double* a = Q + k * N;
       double xl, xr, yl, yr;
@@ -274,7 +276,7 @@ __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double*
 // RusanovC_Update (flux.cpp:409-455) or Pressure_flux_Update (flux.cpp:290-326) with the
 // B slots of the face states taken from cell B of u_con (main.cpp:447-467).
 template <bool kPressureForm>
-__global__ void k_flux_update(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ w,
+__global__ void __launch_bounds__(kThreads, 2) k_flux_update(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ w,
                               const double* __restrict__ Qs, double* __restrict__ ucon) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -589,27 +591,35 @@ __global__ void k_vslope(DevParams P, const DevScalars* __restrict__ sc, const d
     cudaError_t e_ = cudaGetLastError();                                \
     if (e_ != cudaSuccess) return cuda_check(ctx, e_, what);            \
   } while (0)
+// algorithmic bytes of a launch family: `vals` doubles moved per cell
+#define BYTES(vals) ((double)(vals) * 8.0 * (double)ctx->N)
 
 imex_status launch_step_prologue(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nblk = blocks_for(P.N);
   if (nblk > ctx->max_blocks) nblk = ctx->max_blocks;
+  prof_begin(ctx);
   k_step_reduce<<<nblk, kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->partial);
   LAUNCH_CHECK(ctx, "k_step_reduce");
-  k_step_finalize<<<1, 32, 0, ctx->stream>>>(P, ctx->partial, nblk, ctx->sc);
+  k_step_finalize<<<1, kThreads, 0, ctx->stream>>>(P, ctx->partial, nblk, ctx->sc);
   LAUNCH_CHECK(ctx, "k_step_finalize");
+  prof_end(ctx, F_PROLOGUE_REDUCE, BYTES(8), 2);
+  prof_begin(ctx);
   k_cons_from_prim<<<blocks_for(P.N), kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->cons, ctx->cons_n);
   LAUNCH_CHECK(ctx, "k_cons_from_prim");
   const size_t plane = ctx->N * sizeof(double);
   cudaError_t e = cudaMemcpyAsync(ctx->bx_n, ctx->bx, plane, cudaMemcpyDeviceToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by_n, ctx->by, plane, cudaMemcpyDeviceToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A_snap, ctx->A, 3 * plane, cudaMemcpyDeviceToDevice, ctx->stream);
+  prof_end(ctx, F_CONS_FROM_PRIM, BYTES(24 + 10), 1);
   return cuda_check(ctx, e, "step snapshot copies");
 }
 
 imex_status launch_qe_derived(imex_ctx* ctx) {
+  prof_begin(ctx);
   k_qe_derived<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->pe, ctx->hQe);
   LAUNCH_CHECK(ctx, "k_qe_derived");
+  prof_end(ctx, F_COMBINE, BYTES(10), 1);
   return IMEX_OK;
 }
 imex_status launch_vslope(imex_ctx* ctx) {
@@ -663,26 +673,38 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
     T.ai[r] = ai[rks][r];
   }
   T.aii = ai[rks][rks];
+  prof_begin(ctx);
   k_stage_combine<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
       ctx->P, T, rks, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
       ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe);
   LAUNCH_CHECK(ctx, "k_stage_combine");
+  prof_end(ctx, F_COMBINE, BYTES(44 + 13 * rks), 1);
   return IMEX_OK;
 }
 
-imex_status launch_reconstruct(imex_ctx* ctx) {
-  k_reconstruct<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, 8);
+// full = true stores all 8 variables (the public buffer); the stage needs only 0..4
+imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
+  const int nstore = full ? 8 : 5;
+  const int nread = ctx->P.reconstate == IMEX_PrimState ? 8 : nstore;
+  prof_begin(ctx);
+  if (ctx->P.reconstate == IMEX_PrimState)
+    k_reconstruct<true><<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
+  else
+    k_reconstruct<false><<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
   LAUNCH_CHECK(ctx, "k_reconstruct");
+  prof_end(ctx, F_RECON, BYTES(nread + 4 * nstore), 1);
   return IMEX_OK;
 }
 
 imex_status launch_flux_update(imex_ctx* ctx, int pressure_form) {
   int nb = blocks_for(ctx->P.N);
+  prof_begin(ctx);
   if (pressure_form)
     k_flux_update<true><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else
     k_flux_update<false><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   LAUNCH_CHECK(ctx, "k_flux_update");
+  prof_end(ctx, pressure_form ? F_FLUX_PRES : F_FLUX_CONV, BYTES(pressure_form ? 33 : 30), 1);
   return IMEX_OK;
 }
 
@@ -691,11 +713,13 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
   cudaStream_t s = ctx->stream;
+  prof_begin(ctx);
   if (variant == 0 || variant == 1) {
     k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
-    k_reconstruct<<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
+    if (P.reconstate == IMEX_PrimState) k_reconstruct<true><<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
+    else k_reconstruct<false><<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
     k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
@@ -712,24 +736,30 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
     k_curl_Az<<<nb, kThreads, 0, s>>>(P, ctx->A, ctx->cons);
     LAUNCH_CHECK(ctx, "k_curl_Az");
   }
+  // corner EMF 8 + faces/cell B 7 (consistent); legacy variants add the reconstruction of u_con
+  prof_end(ctx, F_CT, BYTES(variant == 0 ? 15 : (variant == 1 ? 14 : (variant == 2 ? 15 + 40 + 22 : 17))), (variant == 0 ? 2 : (variant == 1 ? 3 : (variant == 2 ? 4 : 2))));
   return IMEX_OK;
 }
 
 imex_status launch_stage_derivative(imex_ctx* ctx, int rks) {
+  prof_begin(ctx);
   k_stage_derivative<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
       ctx->P, rks, ctx->sc, ctx->cons, ctx->Qs, ctx->A, ctx->A_s, ctx->bx, ctx->bxQs, ctx->by, ctx->byQs, ctx->Bsave,
       ctx->Hs, ctx->HsA, ctx->HsB, ctx->prim);
   LAUNCH_CHECK(ctx, "k_stage_derivative");
+  prof_end(ctx, F_DERIVATIVE, BYTES(47), 1);
   return IMEX_OK;
 }
 
 imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
+  prof_begin(ctx);
   k_shock_cf<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et);
   k_shock_tilde<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et, ctx->chit);
   k_shock_max<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->chit, eta);
   LAUNCH_CHECK(ctx, "shock detector");
+  prof_end(ctx, F_SHOCK, BYTES(16), 3);
   return IMEX_OK;
 }
 

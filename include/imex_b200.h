@@ -153,6 +153,10 @@ imex_status imex_get_config(const imex_ctx* ctx, imex_config* cfg);
  * like main.cpp:240-244 (u_initialization, upri2ucon, A_initial). */
 imex_status imex_upload_prim(imex_ctx* ctx, const double* prim8, const double* bx, const double* by,
                              const double* A3);
+/* Same as imex_upload_prim but keeps the simulation time, step counter and dt history,
+ * so a driver can hand the solver a state it holds in host memory at every step. */
+imex_status imex_upload_state(imex_ctx* ctx, const double* prim8, const double* bx, const double* by,
+                              const double* A3);
 /* Current state; any pointer may be NULL. */
 imex_status imex_download_state(imex_ctx* ctx, double* cons8, double* prim8, double* bx, double* by, double* A3);
 
@@ -244,6 +248,23 @@ imex_status imex_divergence(imex_ctx* ctx, double* face_l2, double* cell_wrapped
                             double* cell_inf);
 /* Minimum pressure and the reference's L2 divergence error for the active CT scheme. */
 imex_status imex_min_pressure(imex_ctx* ctx, double* pmin);
+
+/* Live kernel profile -------------------------------------------------------
+ * With profiling on, every kernel launch family is bracketed by CUDA events on the
+ * context's stream and its algorithmic HBM bytes (compulsory traffic: each input
+ * read once, each output written once) are accumulated; the persistent solver
+ * kernels count their own phases on the device. */
+typedef struct imex_kernel_profile {
+  char name[32];
+  long long launches;
+  double total_ms;     /* sum of event-timed durations */
+  double alg_bytes;    /* algorithmic bytes over all launches */
+} imex_kernel_profile;
+imex_status imex_profile_enable(imex_ctx* ctx, int on); /* also clears the counters */
+/* Fills up to `max` entries (families with at least one launch); *count = entries written. */
+imex_status imex_profile_read(imex_ctx* ctx, imex_kernel_profile* out, int max, int* count);
+/* Number of CUDA kernels this context has launched since it was created. */
+imex_status imex_kernel_launch_count(const imex_ctx* ctx, long long* count);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,113 @@
+"""Generate the golden fixtures of tests/golden from the reference solver itself.
+
+The reference has no tests or known-answer vectors of its own, so the fixtures
+are outputs of the reference's own code (oracle/_ref/libimexref.so, built from
+the reference sources by `make -C oracle ref`) on small analytic inputs:
+
+  step_<case>.npz  - initial data + state after a few full time steps
+                     (main.cpp:335-561) and the dt of each step;
+  fn_<case>.npz    - single reference functions on fixed inputs:
+                     TVDReconstruction, ShockDetector and the four matrix-free
+                     operators of implicit_operators.cpp.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from imex_b200.problems import vortex, vortex_sheet  # noqa: E402
+from oracle.bindings import RefSolver, make_solver  # noqa: E402
+
+CFG0 = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12)
+CFG1 = dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GMREStol=1e-12)
+STEP_CASES = {
+    # name: (problem factory, RK stages, settings, steps)
+    "vortex16_cfg0": (lambda: vortex(16), 2, CFG0, 3),
+    "sheet16_cfg1": (lambda: vortex_sheet(16), 3, CFG1, 2),
+    "vortex12x10_minmod_unstag": (lambda: vortex(12, 10), 2, dict(recon="Minmod", magfield="UnStaggerCT"), 2),
+    "vortex16_eno3_nodivfree_rk1": (lambda: vortex(16), 1, dict(recon="ENO3", magfield="NoDivFree"), 2),
+    "vortex16_norecon_nofloor_rk3": (lambda: vortex(16), 3,
+                                     dict(recon="NoRecon", magfield="StaggerCT", floor_on=0), 2),
+    "vortex16_primstate": (lambda: vortex(16), 2,
+                           dict(recon="VanLeer", magfield="StaggerCT", reconstate="PrimState"), 2),
+    "vortex16_rkeos": (lambda: vortex(16), 2,
+                       dict(recon="VanLeer", magfield="StaggerCT", eos_type="REDLICH_KWONG",
+                            m_alfa=0.4275, m_b=0.0866), 1),
+    "vortex16_energy_modify": (lambda: vortex(16), 2,
+                               dict(recon="WENO5", magfield="StaggerCT", Energy_modify=1), 1),
+}
+
+
+def step_case(name: str, factory, rks: int, settings: dict, steps: int) -> None:
+    prob = factory()
+    ref = make_solver("ref", prob, rks, settings)
+    dts, cons, faces_x, faces_y, As = [], [], [], [], []
+    for _ in range(steps):
+        dts.append(ref.step())
+        cons.append(ref.cons())
+        bx, by = ref.faces()
+        faces_x.append(bx)
+        faces_y.append(by)
+        As.append(ref.vector_potential())
+    np.savez_compressed(
+        os.path.join(HERE, f"step_{name}.npz"),
+        prim0=prob.prim, bx0=prob.bx, by0=prob.by, A0=prob.A, rks=rks,
+        domain=np.array([prob.x0, prob.x1, prob.y0, prob.y1]),
+        settings=np.array(repr(dict(prob.settings, **settings))),
+        dt=np.array(dts), cons=np.array(cons), bx=np.array(faces_x), by=np.array(faces_y),
+        A=np.array(As), div=np.array(ref.div_error()))
+
+
+def fn_case() -> None:
+    """Single functions on a perturbed vortex state (16 x 12 grid)."""
+    prob = vortex(16, 12)
+    rng = np.random.default_rng(20261203)
+    base = make_solver("ref", prob, 2, CFG0)
+    Q = base.cons()
+    Qp = Q * (1.0 + 1e-3 * rng.standard_normal(Q.shape))
+    ucon = Q * (1.0 + 1e-3 * rng.standard_normal(Q.shape))
+    h = 0.013
+    out = dict(Q=Qp, ucon=ucon, Qs=Q, h=h)
+    for scheme in ("NoRecon", "Minmod", "VanLeer", "ENO3", "WENO5"):
+        s = make_solver("ref", prob, 2, dict(recon=scheme, magfield="StaggerCT"))
+        out[f"recon_{scheme}"] = s.reconstruct(Qp)
+    s = make_solver("ref", prob, 2, dict(recon="Minmod", reconstate="PrimState", magfield="StaggerCT"))
+    out["recon_Minmod_prim"] = s.reconstruct(Qp)
+    s = make_solver("ref", prob, 2, CFG0)
+    out["shock"] = s.shock(Qp)
+    N = prob.nx * prob.ny
+    x1 = rng.standard_normal(N)
+    x3 = rng.standard_normal(3 * N)
+    pf = np.abs(rng.standard_normal(N)) * 2e-7
+    s.set_scalars(0.02, h, 1.3, 1.1, 0.9, 0.8, 1.5)
+    out.update(x1=x1, x3=x3, pfreeze=pf, mbig=1.5e6,
+               scalars=np.array([0.02, h, 1.3, 1.1, 0.9, 0.8, 1.5]))
+    out["op_pressure_L"] = s.operator(0, ucon, Qp, Q, h, x1)
+    out["op_pressure_J"] = s.operator(1, ucon, Qp, Q, h, x1, pfreeze=pf, mbig=1.5e6)
+    out["op_magnetic_B"] = s.operator(2, ucon, Qp, Q, h, x3)
+    sa = make_solver("ref", prob, 2, dict(CFG1))
+    sa.set_scalars(0.02, h, 1.3, 1.1, 0.9, 0.8, 1.5)
+    out["op_magnetic_A"] = sa.operator(3, ucon, Qp, Q, h, x3)
+    np.savez_compressed(os.path.join(HERE, "fn_vortex16x12.npz"), **out)
+
+
+def main() -> None:
+    if not RefSolver.available():
+        raise SystemExit("oracle/_ref/libimexref.so missing: run `make -C oracle ref` first")
+    for name, (factory, rks, settings, steps) in STEP_CASES.items():
+        step_case(name, factory, rks, settings, steps)
+        print("wrote", name)
+    fn_case()
+    print("wrote fn_vortex16x12")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,57 @@
+"""Failure paths on the GPU: every failure is reported as a status, the GPU is never
+trapped, and the context stays usable.  Failures are provoked from the host
+(tolerance 0, a restart cap of 1, NaN in the initial data, misuse of the API)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import imex_b200 as ix
+from imex_b200.problems import vortex
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gmres_restart_cap_is_reported_and_context_survives():
+    prob = vortex(32)
+    sv = ix.Solver.for_problem(prob, 2, dict(recon="VanLeer", magfield="StaggerCT", GMREStol=0.0,
+                                             gmres_max_restarts=1, gmres_restart=5))
+    with pytest.raises(ix.ImexError) as err:
+        sv.step()
+    assert err.value.status in (ix.ImexError(4, "").status, 5)
+    # the context is still usable after the error
+    d = sv.divergence()
+    assert np.isfinite(d["face_l2"])
+    sv.close()
+
+
+def test_nonfinite_input_is_reported():
+    prob = vortex(32)
+    prob.prim[0, 5, 7] = np.nan
+    sv = ix.Solver.for_problem(prob, 2, dict(recon="VanLeer", magfield="StaggerCT"))
+    with pytest.raises(ix.ImexError) as err:
+        sv.step()
+    assert err.value.status == 6
+    sv.close()
+
+
+def test_ct_variant_must_match_magfield():
+    prob = vortex(16)
+    sv = ix.Solver.for_problem(prob, 2, dict(recon="VanLeer", magfield="PotentialA"))
+    with pytest.raises(ix.ImexError) as err:
+        sv.Staggered_CT_Consistent(0.01, 0)
+    assert err.value.status == 1
+    with pytest.raises(ix.ImexError) as err:
+        sv.lib_energy = sv.lib.imex_PreSubsystem_Energy(sv.ctx, 0.01, 0)
+        sv._check(sv.lib_energy)
+    assert err.value.status == 2
+    sv.close()
+
+
+def test_bad_buffer_and_stage_indices():
+    sv = ix.Solver.for_problem(vortex(16), 2, dict(recon="VanLeer", magfield="StaggerCT"))
+    with pytest.raises(ix.ImexError):
+        sv.get_buffer("Hs", index=2)
+    with pytest.raises(ix.ImexError):
+        sv.stage(5)
+    sv.close()

@@ -1,0 +1,206 @@
+"""CUDA path vs the oracle on identical inputs, through the C ABI.
+
+Explicit sub-steps and the matrix-free operators use the reference's operand
+order and no FMA contraction, so they must be bit-identical.  Implicit solves
+reduce dot products in a different (parallel, fixed) order than the
+reference's serial loop, so GMRES/Newton results agree to round-off of the
+solve, asserted at 1e-12 relative L2 (the per-step target of the north star
+is 1e-10).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import imex_b200 as ix
+from conftest import golden_problem, golden_step_cases, load_golden, rel
+from imex_b200.problems import vortex, vortex_sheet
+from oracle.bindings import make_solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", golden_step_cases())
+def test_gpu_steps_match_reference_golden(case):
+    g = load_golden(f"step_{case}.npz")
+    prob, rks, settings = golden_problem(g)
+    tol = 1e-11 if settings.get("eos_type") == "REDLICH_KWONG" else 1e-12
+    gpu = ix.Solver.for_problem(prob, rks, settings)
+    for s in range(len(g["dt"])):
+        dt = gpu.step()
+        assert dt == pytest.approx(float(g["dt"][s]), rel=1e-13)
+        cons = gpu.cons()
+        for k in range(8):
+            assert rel(cons[k], g["cons"][s][k]) <= tol, (s, k)
+        bx, by = gpu.faces()
+        assert rel(bx, g["bx"][s]) <= tol and rel(by, g["by"][s]) <= tol
+        assert rel(gpu.vector_potential(), g["A"][s]) <= tol
+    gpu.close()
+
+
+def _fn_solver(settings):
+    prob = vortex(16, 12)
+    s = dict(prob.settings)
+    s.update(settings)
+    return ix.Solver(prob.nx, prob.ny, s, (prob.x0, prob.x1, prob.y0, prob.y1), 2)
+
+
+def test_gpu_reconstruction_and_shock_detector_bit_exact():
+    g = load_golden("fn_vortex16x12.npz")
+    for scheme in ("NoRecon", "Minmod", "VanLeer", "ENO3", "WENO5"):
+        sv = _fn_solver(dict(recon=scheme, magfield="StaggerCT"))
+        sv.set_buffer("Qe", g["Q"])
+        sv.TVDReconstruction()
+        np.testing.assert_array_equal(sv.get_buffer("w").reshape(4, 8, 12, 16), g[f"recon_{scheme}"],
+                                      err_msg=scheme)
+        sv.close()
+    sv = _fn_solver(dict(recon="Minmod", reconstate="PrimState", magfield="StaggerCT"))
+    sv.set_buffer("Qe", g["Q"])
+    sv.TVDReconstruction()
+    np.testing.assert_array_equal(sv.get_buffer("w").reshape(4, 8, 12, 16), g["recon_Minmod_prim"])
+    np.testing.assert_array_equal(sv.shock_detector(g["Q"]), g["shock"])
+    sv.close()
+
+
+@pytest.mark.parametrize("op,settings", [
+    ("pressure_L", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("pressure_J", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("magnetic_B", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("magnetic_A", dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+])
+def test_gpu_operators_bit_exact(op, settings):
+    g = load_golden("fn_vortex16x12.npz")
+    sv = _fn_solver(settings)
+    dt, h, bmx, bmy, vxm, vym, amax = (float(v) for v in g["scalars"])
+    sv.set_scalars(dt=dt, adt=h, B_max_x=bmx, B_max_y=bmy, vx_max=vxm, vy_max=vym, a_max=amax)
+    sv.set_buffer("cons", g["ucon"])
+    sv.set_buffer("Qe", g["Q"])
+    sv.set_buffer("Qs", g["Qs"])
+    sv.prepare_operator(op, float(g["h"]))
+    if op == "pressure_J":
+        sv.set_newton_state(g["pfreeze"], float(g["mbig"]))
+    x = g["x3"] if op.startswith("magnetic") else g["x1"]
+    np.testing.assert_array_equal(sv.apply_operator(op, x), g[f"op_{op}"])
+    sv.close()
+
+
+SUB_CASES = [
+    ("vortex", (32, 32), 2, dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12)),
+    ("vortex", (20, 14), 2, dict(recon="Minmod", magfield="UnStaggerCT")),
+    ("sheet", (24, 20), 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+    ("vortex", (16, 16), 2, dict(recon="ENO3", magfield="StaggerCT", reconstate="PrimState")),
+    ("vortex", (16, 16), 2, dict(recon="VanLeer", magfield="StaggerCT", eos_type="REDLICH_KWONG",
+                                  m_alfa=0.4275, m_b=0.0866)),
+]
+
+
+@pytest.mark.parametrize("kind,shape,rks,settings", SUB_CASES)
+def test_gpu_substeps_match_oracle(kind, shape, rks, settings):
+    """Each sub-step of each stage on the oracle's inputs of that sub-step."""
+    prob = vortex(*shape) if kind == "vortex" else vortex_sheet(*shape)
+    o = make_solver("port", prob, rks, settings)
+    o.step(snapshots=True)
+    sc = o.scalars()
+    ae, ai = o.tableau()
+    rk_eos = settings.get("eos_type") == "REDLICH_KWONG"
+    exact = (lambda a, b, msg: np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-15, err_msg=msg)) if rk_eos \
+        else (lambda a, b, msg: np.testing.assert_array_equal(a, b, err_msg=msg))
+    g = ix.Solver.for_problem(prob, rks, settings)
+    for k in range(rks):
+        S = lambda sub, w: o.snapshot(k, sub, w)
+        adt = ai[k, k] * sc["dt"]
+        g.set_scalars(dt=sc["dt"], adt=adt, B_max_x=sc["B_max_x"], B_max_y=sc["B_max_y"],
+                      vx_max=sc["vx_max"], vy_max=sc["vy_max"], a_max=sc["a_max"], v_max=sc["v_max"])
+        Qe, Qs = S("combine", "Qe"), S("combine", "Qs")
+        g.set_buffer("Qe", Qe)
+        g.set_buffer("Qs", Qs)
+        g.TVDReconstruction()
+        g.set_buffer("cons", S("combine", "u_con"))
+        g.RusanovC_Update(adt, k)
+        exact(g.get_buffer("cons")[:5], S("convective", "u_con")[:5], f"RusanovC stage {k}")
+        g.set_buffer("cons", S("convective", "u_con"))
+        g.set_buffer("A", S("convective", "A"))
+        g.set_buffer("A_s", S("combine", "A_s"))
+        if settings["magfield"] == "PotentialA":
+            g.MagSubsystem_UpdateA(adt, k)
+            assert rel(g.get_buffer("A"), S("magnetic", "A")) < 1e-12
+        else:
+            g.MagSubsystem_UpdateB(adt, k)
+            assert rel(g.get_buffer("Fx"), S("magnetic", "Fx")) < 1e-12
+            assert rel(g.get_buffer("Fy"), S("magnetic", "Fy")) < 1e-12
+        assert rel(g.get_buffer("cons")[5:], S("magnetic", "u_con")[5:]) < 1e-12
+        g.set_buffer("cons", S("magnetic", "u_con"))
+        g.Pressure_flux_Update(adt, k)
+        exact(g.get_buffer("cons")[:5], S("pflux", "u_con")[:5], f"Pressure_flux stage {k}")
+        g.set_buffer("cons", S("pflux", "u_con"))
+        g.PreSubsystem_Pressure(adt, k)
+        out = g.get_buffer("cons")
+        for q in (1, 2, 4):
+            assert rel(out[q], S("pressure", "u_con")[q]) < 1e-12, (k, q)
+        if settings["magfield"] in ("StaggerCT", "UnStaggerCT"):
+            g.set_buffer("cons", S("pressure", "u_con"))
+            g.set_buffer("Fx", S("magnetic", "Fx"))
+            g.set_buffer("Fy", S("magnetic", "Fy"))
+            g.set_buffer("bxQs", S("combine", "bxQs"))
+            g.set_buffer("byQs", S("combine", "byQs"))
+            g.set_buffer("A", S("pressure", "A"))
+            if settings["magfield"] == "StaggerCT":
+                g.Staggered_CT_Consistent(adt, k)
+                exact(g.get_buffer("bx"), S("ct", "bx"), "CT bx")
+                exact(g.get_buffer("by"), S("ct", "by"), "CT by")
+            else:
+                g.Unstaggered_CT_Consistent(adt, k)
+                exact(g.get_buffer("A"), S("ct", "A"), "CT A")
+            exact(g.get_buffer("cons"), S("ct", "u_con"), f"CT stage {k}")
+    g.close()
+
+
+@pytest.mark.parametrize("magfield", ["StaggerCT", "UnStaggerCT"])
+def test_gpu_legacy_ct_bit_exact(magfield):
+    prob = vortex(16)
+    settings = dict(recon="VanLeer", magfield=magfield)
+    o = make_solver("port", prob, 2, settings)
+    o.step(snapshots=True)
+    Q, Qs = o.snapshot(0, "combine", "Qe"), o.snapshot(0, "combine", "Qs")
+    u = o.snapshot(0, "pressure", "u_con")
+    bxq, byq = o.snapshot(0, "combine", "bxQs"), o.snapshot(0, "combine", "byQs")
+    A, As = o.snapshot(0, "pressure", "A"), o.snapshot(0, "combine", "A_s")
+    bx, by = o.snapshot(0, "pressure", "bx"), o.snapshot(0, "pressure", "by")
+    h = 0.01
+    ref = o.substep(6, h, 0, u, Q, Qs, bx, by, bxq, byq, A, As)
+    g = ix.Solver.for_problem(prob, 2, settings)
+    for name, val in (("cons", u), ("Qe", Q), ("Qs", Qs), ("bx", bx), ("by", by), ("bxQs", bxq),
+                      ("byQs", byq), ("A", A), ("A_s", As)):
+        g.set_buffer(name, val)
+    (g.Staggered_CT if magfield == "StaggerCT" else g.Unstaggered_CT)(h, 0)
+    np.testing.assert_array_equal(g.get_buffer("cons"), ref["u_con"])
+    np.testing.assert_array_equal(g.get_buffer("bx"), ref["bx"])
+    np.testing.assert_array_equal(g.get_buffer("by"), ref["by"])
+    np.testing.assert_array_equal(g.get_buffer("A"), ref["A"])
+    g.close()
+
+
+def test_gpu_nested_newton_matches_oracle():
+    prob = vortex(24)
+    settings = dict(recon="VanLeer", magfield="StaggerCT")
+    o = make_solver("port", prob, 2, settings)
+    o.step(snapshots=True)
+    ucon, Qe, Qs = o.snapshot(0, "pflux", "u_con"), o.snapshot(0, "combine", "Qe"), o.snapshot(0, "combine", "Qs")
+    sc = o.scalars()
+    h = 0.02
+    rng = np.random.default_rng(5)
+    b = (Qe[4] - 0.5 * (Qe[5] ** 2 + Qe[6] ** 2)).ravel() * (1 + 1e-2 * rng.standard_normal(24 * 24))
+    b[:7] = -1e-3  # a few cells driven below the floor
+    p0 = np.full(24 * 24, 0.9)
+    pref = o.nested_newton(ucon, Qe, Qs, h, b, p0)
+    g = ix.Solver.for_problem(prob, 2, settings)
+    g.set_scalars(dt=sc["dt"], adt=h, B_max_x=sc["B_max_x"], B_max_y=sc["B_max_y"], vx_max=sc["vx_max"],
+                  vy_max=sc["vy_max"], a_max=sc["a_max"])
+    g.set_buffer("cons", ucon)
+    g.set_buffer("Qe", Qe)
+    g.set_buffer("Qs", Qs)
+    g.prepare_operator("pressure_L", h)
+    p, st = g.nested_newton(p0, b)
+    assert rel(p, pref) < 1e-12
+    assert st["newton_iters"] >= 1 and p.min() > 0
+    g.close()
