@@ -142,6 +142,8 @@ _SIGS = {
     "imex_profile_read": (C.c_int, [C.c_void_p, C.POINTER(KernelProfile), C.c_int,
                                     C.POINTER(C.c_int)]),
     "imex_kernel_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "imex_set_barrier_timeout": (C.c_int, [C.c_void_p, C.c_double]),
+    "imex_selftest_barrier": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, _D]),
 }
 
 _lib = None
@@ -296,6 +298,16 @@ class Solver:
         self._check(self.lib.imex_profile_read(self.ctx, buf, 64, C.byref(n)))
         return [dict(name=buf[k].name.decode(), launches=buf[k].launches,
                      total_ms=buf[k].total_ms, alg_bytes=buf[k].alg_bytes) for k in range(n.value)]
+
+    def set_barrier_timeout(self, seconds: float) -> None:
+        self._check(self.lib.imex_set_barrier_timeout(self.ctx, seconds))
+
+    def selftest_barrier(self, iterations: int, phantom_blocks: int = 0, timeout_s: float = 1.0) -> float:
+        """Mean microseconds per device-wide barrier (raises ImexError on a timeout)."""
+        us = C.c_double()
+        self._check(self.lib.imex_selftest_barrier(self.ctx, iterations, phantom_blocks, timeout_s,
+                                                   C.byref(us)))
+        return us.value
 
     def kernel_launches(self) -> int:
         n = C.c_longlong()

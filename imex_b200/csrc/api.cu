@@ -781,6 +781,17 @@ imex_status imex_profile_read(imex_ctx* ctx, imex_kernel_profile* out, int max, 
   *count = n;
   return IMEX_OK;
 }
+imex_status imex_selftest_barrier(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
+                                  double* us_per_barrier) {
+  if (!ctx || iterations < 0 || phantom_blocks < 0 || !(timeout_s > 0.0) || timeout_s > 60.0) return IMEX_ERR_INVALID;
+  imex_status s = run_barrier_selftest(ctx, iterations, phantom_blocks, timeout_s, us_per_barrier);
+  return s != IMEX_OK ? s : device_status(ctx);
+}
+imex_status imex_set_barrier_timeout(imex_ctx* ctx, double seconds) {
+  if (!ctx || !(seconds > 0.0) || seconds > 600.0) return IMEX_ERR_INVALID;
+  ctx->barrier_timeout_s = seconds;
+  return IMEX_OK;
+}
 imex_status imex_min_pressure(imex_ctx* ctx, double* pmin) {
   if (!ctx || !pmin) return IMEX_ERR_INVALID;
   return launch_min_pressure(ctx, pmin);

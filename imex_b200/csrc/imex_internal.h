@@ -64,6 +64,7 @@ struct SyncState {
   unsigned int generation;
   int abort;
   int pad;
+  long long spin_limit;  // iterations of the bounded wait (each ~64 ns of __nanosleep)
 };
 
 }  // namespace imex
@@ -120,6 +121,7 @@ struct imex_ctx {
   long long prof_launches[imex::NFAM] = {};
   cudaEvent_t prof_open = nullptr;
   long long kernel_launches = 0;  // every kernel this context launched
+  double barrier_timeout_s = 2.0;  // bound on any single device-wide wait
 };
 
 namespace imex {
@@ -160,5 +162,7 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax);
 imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b);
 imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b);
 imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig);
+imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
+                                 double* us_per_barrier);
 
 }  // namespace imex

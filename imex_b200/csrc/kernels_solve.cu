@@ -26,7 +26,6 @@ namespace {
 constexpr int TX = 32, TY = 16, NT = 256;
 constexpr int KCAP = 30;        // largest supported restart length
 constexpr int NP = KCAP + 2;    // partial-sum slots per CTA
-constexpr long long kSpinLimit = 20000000;  // ~ seconds of __nanosleep(64); a barrier never legitimately waits this long
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
@@ -53,7 +52,7 @@ __device__ bool grid_barrier(SyncState* s, unsigned nblk) {
           ok = 0;
           break;
         }
-        if (++spins > kSpinLimit) {
+        if (++spins > s->spin_limit) {
           atomicExch(&s->abort, 1);
           ok = 0;
           break;
@@ -1280,6 +1279,22 @@ __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, 
   }
 }
 
+// Device-wide barrier self-test: `iters` barriers over the launched CTAs plus
+// `phantom` CTAs that are never launched (so with phantom > 0 the bounded wait
+// must run out and report IMEX_ERR_SYNC).  Block 0 reports clock cycles.
+__global__ void k_barrier_selftest(SyncState* sync, unsigned phantom, int iters, DevStats* st,
+                                   long long* cycles) {
+  const unsigned nblk = gridDim.x + phantom;
+  long long t0 = clock64();
+  for (int k = 0; k < iters; ++k) {
+    if (!grid_barrier(sync, nblk)) {
+      if (threadIdx.x == 0) atomicMax(&st->status, (int)IMEX_ERR_SYNC);
+      return;
+    }
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) *cycles = clock64() - t0;
+}
+
 }  // namespace
 
 // ================================================================== host side
@@ -1325,8 +1340,19 @@ GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
   return g;
 }
 
+}  // namespace
+__global__ void k_reset_sync(SyncState* s, long long limit) {
+  s->count = 0;
+  s->generation = 0;
+  s->abort = 0;
+  s->spin_limit = limit;
+}
+namespace {
+// every device-wide wait gives up after ~barrier_timeout_s (a wait never legitimately lasts that long)
 imex_status reset_sync(imex_ctx* ctx) {
-  return cuda_check(ctx, cudaMemsetAsync(ctx->sync, 0, sizeof(SyncState), ctx->stream), "sync reset");
+  const long long limit = (long long)(ctx->barrier_timeout_s / 64e-9) + 1;
+  k_reset_sync<<<1, 1, 0, ctx->stream>>>(ctx->sync, limit);
+  return cuda_check(ctx, cudaGetLastError(), "sync reset");
 }
 
 template <class Op, class K, class... Args>
@@ -1584,6 +1610,31 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
 }
 
 imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b) { return gmres_launch(ctx, op, x, b); }
+
+imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
+                                 double* us_per_barrier) {
+  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  int nb = coop_blocks<MagneticAOp>(ctx, (const void*)k_gmres<MagneticAOp>, T);
+  const double saved = ctx->barrier_timeout_s;
+  ctx->barrier_timeout_s = timeout_s;
+  imex_status s = reset_sync(ctx);
+  ctx->barrier_timeout_s = saved;
+  if (s != IMEX_OK) return s;
+  long long* cyc = reinterpret_cast<long long*>(ctx->red);
+  unsigned phantom = (unsigned)(phantom_blocks > 0 ? phantom_blocks : 0);
+  void* params[] = {(void*)&ctx->sync, (void*)&phantom, (void*)&iterations, (void*)&ctx->st, (void*)&cyc};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(nb), dim3(NT), params, 0,
+                                              ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "barrier self-test launch");
+  long long h = 0;
+  e = cudaMemcpyAsync(&h, cyc, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "barrier self-test");
+  int clk_khz = 0;
+  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, 0);
+  if (us_per_barrier) *us_per_barrier = (iterations > 0 && clk_khz > 0) ? (double)h / iterations / (clk_khz * 1e-3) : 0.0;
+  return IMEX_OK;
+}
 imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b) { return newton_launch(ctx, p, b); }
 
 

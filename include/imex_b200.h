@@ -246,7 +246,18 @@ imex_status imex_reset_stats(imex_ctx* ctx);
  * cell metric (one-sided at the domain edge); max |central div| of cell B. */
 imex_status imex_divergence(imex_ctx* ctx, double* face_l2, double* cell_wrapped_l2, double* cell_ref_l2,
                             double* cell_inf);
-/* Minimum pressure and the reference's L2 divergence error for the active CT scheme. */
+/* Failure detection ---------------------------------------------------------
+ * Every device-wide wait inside the persistent solver kernels is bounded: after
+ * `seconds` (default 2 s) the waiting CTAs give up, the kernel returns and the
+ * call reports IMEX_ERR_SYNC; the context stays usable. */
+imex_status imex_set_barrier_timeout(imex_ctx* ctx, double seconds);
+/* Runs `iterations` device-wide barriers with the solver's CTA count and reports the
+ * mean cost per barrier.  `phantom_blocks` > 0 makes the barrier wait for CTAs that
+ * were never launched, so the bounded wait must run out after `timeout_s` and the
+ * call must return IMEX_ERR_SYNC (a self-test of the failure path). */
+imex_status imex_selftest_barrier(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
+                                  double* us_per_barrier);
+/* Minimum pressure of the current primitive state. */
 imex_status imex_min_pressure(imex_ctx* ctx, double* pmin);
 
 /* Live kernel profile -------------------------------------------------------

@@ -55,3 +55,17 @@ def test_bad_buffer_and_stage_indices():
     with pytest.raises(ix.ImexError):
         sv.stage(5)
     sv.close()
+
+
+def test_barrier_wait_times_out_and_reports_sync_error():
+    """A device-wide barrier that waits for CTAs that never launch must give up after its
+    bound (0.2 s here), return IMEX_ERR_SYNC, and leave the context usable."""
+    sv = ix.Solver.for_problem(vortex(64), 2, dict(recon="VanLeer", magfield="StaggerCT"))
+    us = sv.selftest_barrier(200)           # healthy barriers complete
+    assert 0.0 < us < 1000.0
+    with pytest.raises(ix.ImexError) as err:
+        sv.selftest_barrier(5, phantom_blocks=1, timeout_s=0.2)
+    assert err.value.status == 8
+    dt = sv.step()                          # the solver still works afterwards
+    assert dt > 0 and sv.divergence()["face_l2"] < 1e-12
+    sv.close()
