@@ -85,8 +85,9 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if (c->recon < IMEX_NoRecon || c->recon > IMEX_WENO5) return why = "bad recon", IMEX_ERR_INVALID;
   if (c->magfield < IMEX_StaggerCT || c->magfield > IMEX_NoDivFree) return why = "bad magfield", IMEX_ERR_INVALID;
   if (c->gmres_restart < 1 || c->gmres_restart > 30) return why = "gmres_restart must be in 1..30", IMEX_ERR_INVALID;
-  if (c->precision != IMEX_PRECISION_FP64 && c->precision != IMEX_PRECISION_MIXED)
-    return why = "bad precision", IMEX_ERR_INVALID;
+  if (c->precision == IMEX_PRECISION_MIXED)
+    return why = "mixed precision is not built yet", IMEX_ERR_UNSUPPORTED;
+  if (c->precision != IMEX_PRECISION_FP64) return why = "bad precision", IMEX_ERR_INVALID;
   if (!(c->x_1 > c->x_0) || !(c->y_1 > c->y_0)) return why = "empty domain", IMEX_ERR_INVALID;
   return IMEX_OK;
 }

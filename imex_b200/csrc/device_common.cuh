@@ -151,13 +151,13 @@ __device__ __forceinline__ void pri2con(const DevParams& P, double* con, const d
   con[6] = pri[6];
   con[7] = pri[7];
 }
-// calenthalpy, timestep.cpp:596-602: e + p / rho
+// calenthalpy, timestep.cpp:224-230: e + p / rho
 __device__ __forceinline__ double calenthalpy(const DevParams& P, const double* c) {
   double e = calecon(c);
   double p = eos_p(P, c[0], e);
   return e + p / c[0];
 }
-// calkinetic, timestep.cpp:611-619
+// calkinetic, timestep.cpp:239-247
 __device__ __forceinline__ double calkinetic(const double* c) {
   double rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
   return 0.5 * rho * (vx * vx + vy * vy + vz * vz);

@@ -321,7 +321,7 @@ __device__ __forceinline__ double cell_ez(const double* __restrict__ u, long lon
   double r = __ldg(u + m);
   return __ldg(u + 2 * N + m) / r * __ldg(u + 5 * N + m) - __ldg(u + N + m) / r * __ldg(u + 6 * N + m);
 }
-// Corner EMF: CT_CornerAssemble (constrained_transport.cpp:338-355) of the face EMFs
+// Corner EMF: CT_CornerAssemble (constrained_transport.cpp:147-164) of the face EMFs
 // ep0 = sx * fx, e0p = sy * fy and the cell EMF of u_con (ct_flux.cpp:165-168).
 __global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
                             double sy, const double* __restrict__ ucon, double* __restrict__ Epp) {
@@ -343,7 +343,7 @@ __global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double s
   Epp[n] = bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
 }
 // Face update from the corner EMF and cell B = face average
-// (ct_flux.cpp:174-189, constrained_transport.cpp:319-332).  The neighbour faces
+// (ct_flux.cpp:174-189, constrained_transport.cpp:128-141).  The neighbour faces
 // are recomputed with the same arithmetic rather than re-read.
 __global__ void k_ct_faces(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
                            const double* __restrict__ bxQs, const double* __restrict__ byQs, double* __restrict__ bx,
@@ -364,7 +364,7 @@ __global__ void k_ct_faces(DevParams P, const DevScalars* __restrict__ sc, const
   ucon[5 * N + n] = 0.5 * (fxm + fx);
   ucon[6 * N + n] = 0.5 * (fym + fy);
 }
-// Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:714-720)
+// Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:523-529)
 __global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
                               const double* __restrict__ A_s, double* __restrict__ A) {
   const long long N = P.N;
@@ -375,7 +375,7 @@ __global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, co
                       __ldg(Epp + cid(P, i - 1, j - 1)));
   A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
 }
-// Unstaggered_CT upwind A_z advection (constrained_transport.cpp:627-679)
+// Unstaggered_CT upwind A_z advection (constrained_transport.cpp:436-488)
 __device__ __forceinline__ double vanleer_lim(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return 2.0 * a * b / (a + b);
@@ -406,7 +406,7 @@ __global__ void k_ct_unstag_legacy_A(DevParams P, const DevScalars* __restrict__
   double dAdt_y = fluct_y / dy + (corrT - corrB) / dy;
   A[2 * N + n] = As[c] - h * (dAdt_x + dAdt_y);
 }
-// B = curl A_z for the unstaggered schemes (constrained_transport.cpp:724-729)
+// B = curl A_z for the unstaggered schemes (constrained_transport.cpp:533-538)
 __global__ void k_curl_Az(DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -417,7 +417,7 @@ __global__ void k_curl_Az(DevParams P, const double* __restrict__ A, double* __r
   ucon[6 * N + n] = -(__ldg(Az + cid(P, i + 1, j)) - __ldg(Az + cid(P, i - 1, j))) / (2.0 * P.dx);
 }
 // Face EMFs of the legacy Staggered_CT from the reconstruction of u_con
-// (constrained_transport.cpp:264-288): Ez_p0 = -(f6_L + f6_R)/2, Ez_0p = (g5_L + g5_R)/2.
+// (constrained_transport.cpp:73-97): Ez_p0 = -(f6_L + f6_R)/2, Ez_0p = (g5_L + g5_R)/2.
 __global__ void k_ct_legacy_faces(DevParams P, const double* __restrict__ w, double* __restrict__ ep0,
                                   double* __restrict__ e0p) {
   const long long N = P.N;

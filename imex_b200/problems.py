@@ -11,7 +11,7 @@ Every field is returned as interior-only SoA planes of shape (ny, nx), index
 Formulas follow the reference's initial conditions:
   * vortex:  initial_conditions.cpp:641-669 (cell state) and :698-717 (faces
     from corner A_z, cell B = face average), A_initial
-    constrained_transport.cpp:580-585, generalised by the background flow
+    constrained_transport.cpp:389-394, generalised by the background flow
     (1,1) and the kappa/mu amplitudes of the vortex workload;
   * vortex sheet: the Orszag-Tang field of initial_conditions.cpp:426-435 in
     [0, 2*pi]^2 form, faces = average of neighbouring cell B as in

@@ -7,7 +7,7 @@
  * interface (include/declarations.hpp) or one block of its driver
  * (src/main.cpp); the citation is given beside it.  A time-marching driver
  * that used to call the reference's sub-system functions calls these in the
- * same order (see INTEGRATION.md).
+ * same order.
  *
  * Data layout exchanged through the interface (host or device pointers are
  * both accepted wherever an array is passed; copies use cudaMemcpyDefault):
@@ -184,9 +184,9 @@ imex_status imex_Pressure_flux_Update(imex_ctx* ctx, double h, int rks);      /*
 imex_status imex_PreSubsystem_Pressure(imex_ctx* ctx, double h, int rks);     /* imex_subsystems.cpp:76 */
 imex_status imex_PreSubsystem_Energy(imex_ctx* ctx, double h, int rks);       /* imex_subsystems.cpp:415 */
 imex_status imex_Staggered_CT_Consistent(imex_ctx* ctx, double h, int rks);   /* ct_flux.cpp:150 */
-imex_status imex_Unstaggered_CT_Consistent(imex_ctx* ctx, double h, int rks); /* constrained_transport.cpp:691 */
-imex_status imex_Staggered_CT(imex_ctx* ctx, double h, int rks);             /* constrained_transport.cpp:257 */
-imex_status imex_Unstaggered_CT(imex_ctx* ctx, double h, int rks);           /* constrained_transport.cpp:627 */
+imex_status imex_Unstaggered_CT_Consistent(imex_ctx* ctx, double h, int rks); /* constrained_transport.cpp:500 */
+imex_status imex_Staggered_CT(imex_ctx* ctx, double h, int rks);             /* constrained_transport.cpp:66 */
+imex_status imex_Unstaggered_CT(imex_ctx* ctx, double h, int rks);           /* constrained_transport.cpp:436 */
 imex_status imex_stage_derivative(imex_ctx* ctx, int rks);                    /* main.cpp:537-555 */
 
 /* Stage buffers, for drivers and tests that run sub-steps individually. */

@@ -8,8 +8,8 @@
  * because reductions are summed serially in index order here.
  *
  * Periodic boundaries only: ghost cells are replaced by wrap-around indexing,
- * which reproduces the reference's periodic ghost fills (boundary.cpp:472,544,
- * timestep.cpp:556,585, constrained_transport.cpp:204,223) exactly.
+ * which reproduces the reference's periodic ghost fills (boundary.cpp:46,118,
+ * timestep.cpp:184,213, constrained_transport.cpp:13,32) exactly.
  */
 #include "imex_oracle.h"
 
@@ -226,12 +226,12 @@ static void grid_pri2con(double* con, const double* pri) {
     for (int k = 0; k < 8; ++k) con[(size_t)k * G.N + n] = c[k];
   }
 }
-/* timestep.cpp:611-619 */
+/* timestep.cpp:239-247 */
 static double calkinetic(const double* c) {
   double rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
   return 0.5 * rho * (vx * vx + vy * vy + vz * vz);
 }
-/* timestep.cpp:596-602 */
+/* timestep.cpp:224-230 */
 static double calenthalpy(const double* c) {
   double e = calecon(c);
   double pri[8];
@@ -1153,7 +1153,7 @@ static void mag_subsystem_A(double* ucon, const double* Qs, const double* Qe, do
 /* ------------------------------------------------------------------ */
 /* constrained transport                                              */
 /* ------------------------------------------------------------------ */
-/* CT_CornerAssemble, constrained_transport.cpp:338-355 */
+/* CT_CornerAssemble, constrained_transport.cpp:147-164 */
 static void corner_assemble(double* Epp, const double* Ep0, const double* E0p, const double* Et) {
   const double dx = G.dx, dy = G.dy;
   for (int j = 0; j < G.ny; j++)
@@ -1201,7 +1201,7 @@ static void staggered_ct_consistent(double* ucon, double* bx, double* by, const 
   face_update(bx, by, bxQs, byQs, Epp, h, ucon);
   free(Ep0); free(E0p); free(Et); free(Epp);
 }
-/* Unstaggered_CT_Consistent, constrained_transport.cpp:691-731 */
+/* Unstaggered_CT_Consistent, constrained_transport.cpp:500-540 */
 static void unstaggered_ct_consistent(double* ucon, double* A, const double* A_s, const double* Fx, const double* Fy,
                                       double h) {
   const size_t N = G.N;
@@ -1224,7 +1224,7 @@ static void unstaggered_ct_consistent(double* ucon, double* A, const double* A_s
     }
   free(Ep0); free(E0p); free(Et); free(Epp);
 }
-/* Staggered_CT (legacy), constrained_transport.cpp:257-334 */
+/* Staggered_CT (legacy), constrained_transport.cpp:66-143 */
 static void staggered_ct_legacy(double* ucon, double* bx, double* by, const double* bxQs, const double* byQs, double h) {
   const size_t N = G.N;
   double *w = alloc(32 * N), *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc(N);
@@ -1253,7 +1253,7 @@ static double vanleer_lim(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return 2.0 * a * b / (a + b);
 }
-/* Unstaggered_CT (legacy), constrained_transport.cpp:627-689 */
+/* Unstaggered_CT (legacy), constrained_transport.cpp:436-498 */
 static void unstaggered_ct_legacy(double* ucon, double* A, const double* A_s, double h) {
   const size_t N = G.N;
   const double dx = G.dx, dy = G.dy;
