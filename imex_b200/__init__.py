@@ -132,6 +132,7 @@ _SIGS = {
     "imex_set_newton_state": (C.c_int, [C.c_void_p, _D, C.c_double]),
     "imex_apply_operator": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "imex_gmres": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
+    "imex_gmres_noalloc": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
     "imex_pressure_nested_newton": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(SolveStats)]),
     "imex_shock_detector": (C.c_int, [C.c_void_p, _D, _D]),
     "imex_get_stats": (C.c_int, [C.c_void_p, C.POINTER(SolveStats)]),
@@ -421,6 +422,14 @@ class Solver:
         b = _c(b)
         st = SolveStats()
         self._check(self.lib.imex_gmres(self.ctx, OP[op], _dp(x), _dp(b), C.byref(st)))
+        return x, st.as_dict()
+
+    def gmres_noalloc(self, op: str, x0, b) -> tuple[np.ndarray, dict]:
+        """imex_gmres on the library's fixed device scratch: no device allocation."""
+        x = np.array(x0, dtype=np.float64, copy=True)
+        b = _c(b)
+        st = SolveStats()
+        self._check(self.lib.imex_gmres_noalloc(self.ctx, OP[op], _dp(x), _dp(b), C.byref(st)))
         return x, st.as_dict()
 
     def nested_newton(self, p0, b) -> tuple[np.ndarray, dict]:

@@ -683,6 +683,17 @@ imex_status imex_gmres(imex_ctx* ctx, int op, double* x, const double* b, imex_s
   if (stats) imex_get_stats(ctx, stats);
   return s;
 }
+imex_status imex_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b, imex_solve_stats* stats) {
+  if (!ctx || !x || !b) return IMEX_ERR_INVALID;
+  unsigned char* base = nullptr;
+  imex_status s = static_scratch(ctx, &base);
+  if (s != IMEX_OK) return s;
+  s = run_gmres_noalloc(ctx, op, x, b, base, kStaticScratchBytes);
+  if (s != IMEX_OK) return s;
+  s = device_status(ctx);
+  if (stats) imex_get_stats(ctx, stats);
+  return s;
+}
 imex_status imex_pressure_nested_newton(imex_ctx* ctx, double* p, const double* b, imex_solve_stats* stats) {
   if (!ctx || !p || !b) return IMEX_ERR_INVALID;
   imex_status s = with_device_vectors(ctx, ctx->N, p, b, true,

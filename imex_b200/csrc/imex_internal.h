@@ -165,4 +165,10 @@ imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig);
 imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                  double* us_per_barrier);
 
+// fixed device scratch of imex_gmres_noalloc (noalloc.cu) and the solve that uses it
+constexpr size_t kStaticScratchBytes = IMEX_NOALLOC_SCRATCH_BYTES;
+imex_status static_scratch(imex_ctx* ctx, unsigned char** base);
+imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b, unsigned char* base,
+                              size_t capacity);
+
 }  // namespace imex

@@ -1452,6 +1452,71 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
 }
 
+bool on_device(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// The same GMRES launch as gmres_launch, with every work array carved out of the
+// caller's fixed scratch [base, base + capacity) instead of the context's buffers:
+//   barrier state | partial sums (2 x CTAs x NP) | V ((restart+1) vectors) | AV (2) | x, b staging (host only)
+// Nothing here allocates; a solve that does not fit is rejected before any work.
+template <class Op>
+imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, unsigned char* base,
+                             size_t capacity) {
+  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  auto kern = k_gmres<Op>;
+  const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
+  const size_t n = (size_t)Op::M * (size_t)T.N;
+  const bool hx = !on_device(x), hb = !on_device(b);
+  size_t used = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = used;
+    used += (bytes + 255) & ~(size_t)255;
+    return at;
+  };
+  const size_t o_sync = take(sizeof(SyncState));
+  const size_t o_part = take((size_t)2 * nb * NP * sizeof(double));
+  const size_t o_V = take(((size_t)ctx->cfg.gmres_restart + 1) * n * sizeof(double));
+  const size_t o_AV = take(2 * n * sizeof(double));
+  const size_t o_x = hx ? take(n * sizeof(double)) : 0;
+  const size_t o_b = hb ? take(n * sizeof(double)) : 0;
+  if (used > capacity) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "imex_gmres_noalloc: this solve needs %zu bytes of scratch (restart %d, %zu unknowns), "
+             "the static scratch holds %zu",
+             used, ctx->cfg.gmres_restart, n, capacity);
+    return set_error(ctx, IMEX_ERR_INVALID, msg);
+  }
+  GmresWork g = make_work(ctx, T, nb, fam);
+  g.sync = reinterpret_cast<SyncState*>(base + o_sync);
+  g.partial = reinterpret_cast<double*>(base + o_part);
+  g.V = reinterpret_cast<double*>(base + o_V);
+  g.AV = reinterpret_cast<double*>(base + o_AV);
+  double* xd = hx ? reinterpret_cast<double*>(base + o_x) : x;
+  const double* bd = hb ? reinterpret_cast<const double*>(base + o_b) : b;
+  cudaError_t e = cudaSuccess;
+  if (hx) e = cudaMemcpyAsync(xd, x, n * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (hb && e == cudaSuccess) e = cudaMemcpyAsync((void*)bd, b, n * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "imex_gmres_noalloc: vector upload");
+  // the barrier state must start at zero on every call
+  const long long limit = (long long)(ctx->barrier_timeout_s / 64e-9) + 1;
+  k_reset_sync<<<1, 1, 0, ctx->stream>>>(g.sync, limit);
+  LAUNCH_CHECK(ctx, "imex_gmres_noalloc: sync reset");
+  void* params[] = {(void*)&o, (void*)&g, (void*)&xd, (void*)&bd};
+  e = cudaLaunchCooperativeKernel((const void*)kern, dim3(nb), dim3(NT), params, sizeof(SolveSmem<Op>), ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "imex_gmres_noalloc: cooperative launch");
+  ctx->kernel_launches += 2;
+  if (hx) e = cudaMemcpyAsync(x, xd, n * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_check(ctx, e, "imex_gmres_noalloc: solve");
+}
+
 imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   Tiling T = make_tiling(ctx->nx, ctx->ny);
   PressureOp o = make_pressure_op(ctx);
@@ -1610,6 +1675,20 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
 }
 
 imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b) { return gmres_launch(ctx, op, x, b); }
+
+imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b, unsigned char* base,
+                              size_t capacity) {
+  if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
+    PressureOp o = make_pressure_op(ctx);
+    o.jac = op == IMEX_OP_PRESSURE_J;
+    return gmres_noalloc_op(ctx, o, F_GMRES_PRES, x, b, base, capacity);
+  } else if (op == IMEX_OP_MAGNETIC_B) {
+    return gmres_noalloc_op(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, base, capacity);
+  } else if (op == IMEX_OP_MAGNETIC_A) {
+    return gmres_noalloc_op(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, base, capacity);
+  }
+  return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
+}
 
 imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                  double* us_per_barrier) {

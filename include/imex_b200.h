@@ -233,6 +233,33 @@ imex_status imex_apply_operator(imex_ctx* ctx, int op, const double* x, double* 
  * the reference's Jacobi preconditioner precP (implicit_operators.cpp:650), the magnetic
  * ones none, as in the reference call sites. */
 imex_status imex_gmres(imex_ctx* ctx, int op, double* x, const double* b, imex_solve_stats* stats);
+/* imex_gmres without any allocation.  This entry point has no counterpart in the
+ * reference (whose GMRES_Solver allocates its Krylov and work vectors on every
+ * call, implicit_operators.cpp:808-810); it is an addition of this implementation.
+ *
+ * imex_gmres takes its temporaries for host x/b from cudaMallocAsync.  Callers that
+ * cannot enter the device allocator during a solve use this one instead: a host
+ * whose own allocator has reserved the device's free memory (a cudaMalloc would
+ * fail or force that allocator to release memory), and a per-step loop with a hard
+ * latency budget, where an allocation may block on the pool.  Here the Krylov
+ * basis, the AV ring, the per-CTA partial sums, the barrier state and the staged
+ * host vectors all live in one fixed device array of IMEX_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) per device; no cudaMalloc, cudaFree or other allocating call is made.
+ * Same kernel, same arithmetic and same results as imex_gmres.
+ *
+ * Limit: the solve needs about (gmres_restart + 3) x unknowns x 8 bytes, plus
+ * 2 x unknowns x 8 bytes when x or b are host pointers.  For restart 25 that is
+ * up to ~73,000 pressure unknowns (256 x 256 cells) or ~24,000 cells for the
+ * magnetic systems (3 unknowns per cell).  Larger solves are rejected with
+ * IMEX_ERR_INVALID before any work, and imex_last_error names the bytes needed.
+ *
+ * The first call on a device resolves the array's address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.
+ * The barrier state in the array is cleared by every call.  The array is shared by
+ * every context and stream on a device, so calls that overlap in time on one
+ * device race: serialise them. */
+#define IMEX_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+imex_status imex_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b, imex_solve_stats* stats);
 /* Pressure_NestedNewton (implicit_operators.cpp:625): p in/out, b in. */
 imex_status imex_pressure_nested_newton(imex_ctx* ctx, double* p, const double* b, imex_solve_stats* stats);
 /* ShockDetector (flux.cpp:5) of 8 conserved planes into one plane. */
