@@ -335,6 +335,7 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->clock_khz, cudaDevAttrClockRate, dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     fprintf(stderr, "imex_create: %s\n", cudaGetErrorString(e));

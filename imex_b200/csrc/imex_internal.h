@@ -60,11 +60,11 @@ struct ProfRec {
 
 // Grid-barrier and reduction workspace of the persistent solver kernels.
 struct SyncState {
-  unsigned int count;
-  unsigned int generation;
+  unsigned int count;   // barrier arrivals since the launch started (monotonic)
+  unsigned int pad0;
   int abort;
-  int pad;
-  long long spin_limit;  // iterations of the bounded wait (each ~64 ns of __nanosleep)
+  int pad1;
+  long long wait_cycles;  // bound of any single barrier wait, in SM clock cycles
 };
 
 }  // namespace imex
@@ -78,6 +78,7 @@ struct imex_ctx {
   bool own_stream = false;
   std::string last_error;
   int num_sms = 0;
+  int clock_khz = 0;  // maximum SM clock, read once at creation (bounds of device-side waits)
 
   // device state (interior planes)
   double *prim = nullptr, *cons = nullptr, *cons_n = nullptr, *Qe = nullptr, *Qs = nullptr;

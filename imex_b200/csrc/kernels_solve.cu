@@ -6,7 +6,7 @@
 // rotations, left preconditioning, tolerance GMREStol*|r0| + GMREStol.
 // Device layout of one Arnoldi step j, done as ONE pass over the grid plus
 // ONE grid barrier:
-//   each CTA, per 32x8 tile: w = Av_j - sum_i H[i][j] v_i on the tile plus a
+//   each CTA, per 32x16 tile: w = Av_j - sum_i H[i][j] v_i on the tile plus a
 //   halo (shared memory), w -> basis slot j+1 (unnormalised), Aw = M^-1 A w on
 //   the tile from shared memory, and partial sums of v_i.Aw, w.Aw, w.w;
 //   barrier; every CTA reduces the partials in the same fixed order, so all
@@ -30,38 +30,52 @@ constexpr int NP = KCAP + 2;    // partial-sum slots per CTA
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
 // ------------------------------------------------------------------ grid barrier
-// Bounded-spin barrier over a cooperative launch (all CTAs co-resident).
-// Returns false if any CTA gave up; the caller then leaves the kernel.
+// Bounded barrier over a cooperative launch (all CTAs co-resident).  The arrival
+// counter only ever grows: barrier number g is complete once it reaches
+// (g + 1) * nblk, so the last CTA to arrive releases everyone with its own
+// arrival (no reset, no second counter).  Arrival is a release atomic and the
+// wait ends with an acquire fence, so the CTA's writes before the barrier are
+// visible to every CTA after it.  The wait polls with relaxed loads: an acquire
+// load per poll would invalidate the SM's L1 on every poll, under the feet of
+// the other CTA working on the same SM.  A wait
+// longer than s->wait_cycles SM cycles sets the abort flag; every CTA then
+// returns false and the caller leaves the kernel.
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ unsigned atom_add_release_gpu(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
 __device__ bool grid_barrier(SyncState* s, unsigned nblk) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    unsigned gen = atomicAdd(&s->generation, 0u);
-    __threadfence();
-    unsigned arrived = atomicAdd(&s->count, 1u);
-    if (arrived == nblk - 1) {
-      atomicExch(&s->count, 0u);
-      __threadfence();
-      atomicAdd(&s->generation, 1u);
-    } else {
-      long long spins = 0;
-      while (true) {
-        if (*((volatile unsigned*)&s->generation) != gen) break;
+    const unsigned old = atom_add_release_gpu(&s->count, 1u);
+    const unsigned target = (old / nblk + 1u) * nblk;
+    const long long limit = s->wait_cycles;
+    const long long t0 = clock64();
+    for (unsigned spin = 0;; ++spin) {
+      if ((int)(ld_relaxed_gpu(&s->count) - target) >= 0) break;
+      __nanosleep(32);
+      if ((spin & 15u) == 15u) {
         if (*((volatile int*)&s->abort)) {
           ok = 0;
           break;
         }
-        if (++spins > s->spin_limit) {
+        if (clock64() - t0 > limit) {
           atomicExch(&s->abort, 1);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
-    __threadfence();
-    if (*((volatile int*)&s->abort)) ok = 0;
+    fence_acq_rel_gpu();
   }
   __syncthreads();
   return ok != 0;
@@ -97,6 +111,16 @@ __device__ __forceinline__ void wacc_add(WarpAcc& a, int k, double x) {
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   if ((threadIdx.x & 31) == 0) a.v[threadIdx.x >> 5][k] += x;
 }
+// four consecutive slots k..k+3 at once (independent shuffles interleave)
+__device__ __forceinline__ void wacc_add4(WarpAcc& a, int k, double (&x)[4]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] += __shfl_xor_sync(0xffffffffu, x[u], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a.v[threadIdx.x >> 5][k + u] += x[u];
+}
 // CTA totals of slots [0, kn) -> out[0, kn)
 __device__ __forceinline__ void wacc_store(WarpAcc& a, int kn, double* out) {
   __syncthreads();
@@ -108,18 +132,48 @@ __device__ __forceinline__ void wacc_store(WarpAcc& a, int kn, double* out) {
   __syncthreads();
 }
 
-// identical-in-every-CTA reduction of partial[0..nblk)[0..kn) into red[0..kn)
-__device__ inline void grid_sum(const double* partial, int nblk, int kn, double* red) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int k = wid; k < kn; k += NT / 32) {
-    double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += ldcg(partial + (long long)b * NP + k);
+// Identical-in-every-CTA reduction of partial[0..nblk)[0..kn) into red[0..kn).
+// Slot k is summed unless bit 2k / 2k+1 of `minmax` asks for its minimum / maximum.
+// Thread (w, k) combines blocks w, w + 8, w + 16, ... of slot k in increasing order
+// (16 loads in flight, consecutive threads read consecutive slots), then the eight
+// warp results of each slot are combined in warp order: a fixed order, so every CTA
+// and every run gets the same bits.  `tmp` is free CTA scratch of 8 x NP doubles.
+enum { RED_SUM = 0, RED_MIN = 1, RED_MAX = 2 };
+__device__ __forceinline__ double red_op(int kind, double a, double b) {
+  return kind == RED_SUM ? a + b : (kind == RED_MIN ? fmin(a, b) : fmax(a, b));
+}
+__device__ __forceinline__ double red_init(int kind) {
+  return kind == RED_SUM ? 0.0 : (kind == RED_MIN ? INFINITY : -INFINITY);
+}
+__device__ inline void grid_reduce(const double* partial, int nblk, int kn, double* red, WarpAcc& tmp,
+                                   unsigned minmax = 0u) {
+  constexpr int NW = NT / 32, U = 16;
+  const int k = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int kind = k < 16 ? (int)((minmax >> (2 * k)) & 3u) : RED_SUM;
+  double s = red_init(kind);
+  if (k < kn) {
+    for (int b0 = w; b0 < nblk; b0 += NW * U) {
+      double v[U];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) red[k] = s;
+      for (int u = 0; u < U; ++u) {
+        const int b = b0 + u * NW;
+        v[u] = b < nblk ? ldcg(partial + (long long)b * NP + k) : red_init(kind);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) s = red_op(kind, s, v[u]);
+    }
+  }
+  tmp.v[w][k] = s;
+  __syncthreads();
+  if (threadIdx.x < kn) {
+    const int kk = threadIdx.x < 16 ? (int)((minmax >> (2 * threadIdx.x)) & 3u) : RED_SUM;
+    double t = red_init(kk);
+    for (int q = 0; q < NW; ++q) t = red_op(kk, t, tmp.v[q][threadIdx.x]);
+    red[threadIdx.x] = t;
   }
   __syncthreads();
 }
+
 // ------------------------------------------------------------------ tiles
 // A CTA works on a TX x TY tile of interior cells plus a halo; each thread owns
 // CPT cells of the tile (rows ly and ly + RY).  The vector being multiplied and
@@ -444,25 +498,44 @@ struct GmresShared {
   double cs[KCAP + 2], sn[KCAP + 2], gam[KCAP + 2], alpha[KCAP + 2], sigma[KCAP + 2];
   double red[NP];
   WarpAcc acc;
+  int nalpha;  // terms of an update left to the caller (deferred mode), else 0
 };
 
-// Stage the vector f(cell) and the operator's coefficients on the tile at
-// (x0, y0) plus halo, then run the operator's pre-pass.
+// Stage the vector and the operator's coefficients on the tile at (x0, y0) plus
+// halo, then run the operator's pre-pass.  Each thread stages FillQ<Op> cells and
+// issues all of their loads before using any: f(c, v) receives the thread's cell
+// indices c[FillQ] and fills v[FillQ][M] for all of them at once.
+template <class Op>
+constexpr int FillQ = (TileBuf<Op>::SN + NT - 1) / NT;
+
 template <class Op, class F>
 __device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const Tiling& T, int x0, int y0, F f) {
   using TB = TileBuf<Op>;
-  for (int q = threadIdx.x; q < TB::SN; q += NT) {
+  constexpr int Q = FillQ<Op>;
+  constexpr int QC = Op::QT > 0 ? Op::QT : 1;
+  long long c[Q];
+#pragma unroll
+  for (int r = 0; r < Q; ++r) {
+    int q = threadIdx.x + r * NT;
+    if (q >= TB::SN) q = TB::SN - 1;  // an already staged cell: loaded again, never stored
     const int sxq = q % TB::SX, syq = q / TB::SX;
     const int gi = wrapc(x0 + sxq - Op::HALO, T.nx), gj = wrapc(y0 + syq - Op::HALO, T.ny);
-    const long long c = (long long)gi + (long long)T.nx * gj;
-    double v[Op::M];
-    f(c, v);
+    c[r] = (long long)gi + (long long)T.nx * gj;
+  }
+  double qv[Q][QC];
 #pragma unroll
-    for (int m = 0; m < Op::M; ++m) tb.s[m * TB::SN + q] = v[m];
-    double qv[Op::QT > 0 ? Op::QT : 1];
-    op.coef(c, qv);
+  for (int r = 0; r < Q; ++r) op.coef(c[r], qv[r]);
+  double v[Q][Op::M];
+  f(c, v);
 #pragma unroll
-    for (int m = 0; m < Op::QT; ++m) tb.c[m * TB::SN + q] = qv[m];
+  for (int r = 0; r < Q; ++r) {
+    const int q = threadIdx.x + r * NT;
+    if (q < TB::SN) {
+#pragma unroll
+      for (int m = 0; m < Op::M; ++m) tb.s[m * TB::SN + q] = v[r][m];
+#pragma unroll
+      for (int m = 0; m < Op::QT; ++m) tb.c[m * TB::SN + q] = qv[r][m];
+    }
   }
   __syncthreads();
   if (Op::PT > 0) {
@@ -491,11 +564,18 @@ __device__ __forceinline__ Cell tile_cell(const Tiling& T, int x0, int y0, int r
 // Result codes of gmres_device
 enum { GM_CONVERGED = 0, GM_MAXIT = 1, GM_NONFINITE = 2, GM_SYNC = 3 };
 
+// x_zero: x is treated as zero on entry (its contents are never read), so the first
+//   cycle's residual is M^-1 b, a per-cell quantity: it is formed while staging the
+//   first matvec tile, and the residual pass and the A v_0 pass become one pass.
+// defer: when the solve converges, the last cycle's update sum_i alpha_i v_i is not
+//   written; S.alpha[0..S.nalpha) and S.sigma stay in shared memory for the caller to
+//   apply in its next pass (the basis stays in g.V).  x_written reports whether an
+//   earlier cycle wrote x, in which case the full update is x + that sum.
 template <class Op>
 __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const double* b, GmresShared& S,
-                            TileBuf<Op>& tb, unsigned& phase) {
+                            TileBuf<Op>& tb, unsigned& phase, bool x_zero, bool defer, bool& x_written) {
   using TB = TileBuf<Op>;
-  constexpr int M = Op::M, HALO = Op::HALO;
+  constexpr int M = Op::M, HALO = Op::HALO, FQ = FillQ<Op>;
   const Tiling& T = g.T;
   const long long N = T.N;
   const int kmax = g.kmax;
@@ -511,15 +591,82 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
     if (lead) g.st->alg_bytes[g.fam] += (double)vals * 8.0 * (double)N;
   };
   (void)HALO;
+  x_written = false;
+  if (threadIdx.x == 0) S.nalpha = 0;
 
   for (int outer = 0; outer < g.max_restarts; ++outer) {
+    const bool from_zero = x_zero && outer == 0;
+    if (from_zero) {
+      // ---- r0 = M^-1 b -> V0 and Av0 = M^-1 A V0 in one pass; |r0|^2 and r0.Av0
+      wacc_clear(S.acc);
+      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+#pragma unroll
+          for (int r = 0; r < FQ; ++r)
+#pragma unroll
+            for (int m = 0; m < M; ++m) v[r][m] = ldcg(b + m * N + c[r]);
+#pragma unroll
+          for (int r = 0; r < FQ; ++r) op.precond(c[r], v[r]);
+        });
+        double rr = 0.0, va = 0.0;
+#pragma unroll
+        for (int r = 0; r < CPT; ++r) {
+          const Cell k = tile_cell(T, x0, y0, r);
+          if (!k.in) continue;
+          double aw[M];
+          op.matvec(tb, k.lx, k.ly, k.c, aw);
+          op.precond(k.c, aw);
+          const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            const double w = tb.s[m * TB::SN + o];
+            Vp(0)[m * N + k.c] = w;
+            AVp(0)[m * N + k.c] = aw[m];
+            rr += w * w;
+            va += w * aw[m];
+          }
+        }
+        wacc_add(S.acc, 0, rr);
+        wacc_add(S.acc, 1, va);
+        __syncthreads();
+      }
+      wacc_store(S.acc, 2, part() + (long long)blockIdx.x * NP);
+      if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
+      grid_reduce(part(), g.nblk, 2, S.red, S.acc);
+      ++phase;
+      count(3 * M + coef);
+      S.gam[0] = sqrt(S.red[0]);
+      tol_eff = g.tol * S.gam[0] + g.tol;
+      if (!isfinite(S.gam[0])) return GM_NONFINITE;
+      if (S.gam[0] <= tol_eff) {
+        if (lead) {
+          g.st->gmres_iters += iters;
+          g.st->last_residual = S.gam[0];
+        }
+        if (!defer) {  // x = 0
+          for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)gridDim.x * NT)
+            x[c] = 0.0;
+          x_written = true;
+        }
+        return GM_CONVERGED;
+      }
+      if (lead) g.st->gmres_restarts += 1;
+      S.sigma[0] = 1.0 / S.gam[0];
+      for (int r = threadIdx.x; r < (KCAP + 2) * (KCAP + 2); r += NT) (&S.H[0][0])[r] = 0.0;
+      __syncthreads();
+      if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[1];
+      __syncthreads();
+    } else {
     // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
     wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
+      fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
-        for (int m = 0; m < M; ++m) v[m] = ldcg(x + m * N + c);
+        for (int r = 0; r < FQ; ++r)
+#pragma unroll
+          for (int m = 0; m < M; ++m) v[r][m] = ldcg(x + m * N + c[r]);
       });
       double rr = 0.0;
 #pragma unroll
@@ -543,7 +690,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
     }
     wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    grid_sum(part(), g.nblk, 1, S.red);
+    grid_reduce(part(), g.nblk, 1, S.red, S.acc);
     ++phase;
     count(3 * M + coef);
     S.gam[0] = sqrt(S.red[0]);
@@ -563,9 +710,11 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
     wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
+      fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
-        for (int m = 0; m < M; ++m) v[m] = ldcg(Vp(0) + m * N + c);
+        for (int r = 0; r < FQ; ++r)
+#pragma unroll
+          for (int m = 0; m < M; ++m) v[r][m] = ldcg(Vp(0) + m * N + c[r]);
       });
       double va = 0.0;
 #pragma unroll
@@ -587,13 +736,14 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
     }
     wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    grid_sum(part(), g.nblk, 1, S.red);
+    grid_reduce(part(), g.nblk, 1, S.red, S.acc);
     ++phase;
     count(2 * M + coef);
     for (int r = threadIdx.x; r < (KCAP + 2) * (KCAP + 2); r += NT) (&S.H[0][0])[r] = 0.0;
     __syncthreads();
     if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[0];
     __syncthreads();
+    }
 
     int jend = -1;  // last Arnoldi index used in the update
     bool converged = false;
@@ -603,13 +753,20 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       const double sj = S.sigma[j];
       for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+          const double* AVj = AVp(j);
 #pragma unroll
-          for (int m = 0; m < M; ++m) {
-            double wv = sj * ldcg(AVp(j) + m * N + c);
-#pragma unroll 4
-            for (int i = 0; i <= j; ++i) wv = wv - S.H[i][j] * (S.sigma[i] * ldcg(Vp(i) + m * N + c));
-            v[m] = wv;
+          for (int r = 0; r < FQ; ++r)
+#pragma unroll
+            for (int m = 0; m < M; ++m) v[r][m] = sj * ldcg(AVj + m * N + c[r]);
+#pragma unroll 2
+          for (int i = 0; i <= j; ++i) {
+            const double hij = S.H[i][j], si = S.sigma[i];
+            const double* Vi = Vp(i);
+#pragma unroll
+            for (int r = 0; r < FQ; ++r)
+#pragma unroll
+              for (int m = 0; m < M; ++m) v[r][m] = v[r][m] - hij * (si * ldcg(Vi + m * N + c[r]));
           }
         });
         double aw[CPT][M], wc[CPT][M];
@@ -635,8 +792,21 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
             for (int m = 0; m < M; ++m) aw[r][m] = wc[r][m] = 0.0;
           }
         }
-        // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2
-        for (int i = 0; i <= j; ++i) {
+        // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2; four basis vectors at a time
+        int i = 0;
+        for (; i + 3 <= j; i += 4) {
+          double d[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int r = 0; r < CPT; ++r)
+            if (in[r]) {
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int m = 0; m < M; ++m) d[u] += ldcg(Vp(i + u) + m * N + cc[r]) * aw[r][m];
+            }
+          wacc_add4(S.acc, i, d);
+        }
+        for (; i <= j; ++i) {
           double d = 0.0;
 #pragma unroll
           for (int r = 0; r < CPT; ++r)
@@ -660,7 +830,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       }
       wacc_store(S.acc, j + 3, part() + (long long)blockIdx.x * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-      grid_sum(part(), g.nblk, j + 3, S.red);
+      grid_reduce(part(), g.nblk, j + 3, S.red, S.acc);
       ++phase;
       ++iters;
       count((j + 4) * M + coef);
@@ -706,16 +876,26 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       }
     }
     __syncthreads();
+    if (converged && defer) {
+      if (threadIdx.x == 0) S.nalpha = jend + 1;
+      __syncthreads();
+      if (lead) {
+        g.st->gmres_iters += iters;
+        g.st->last_residual = S.gam[jend + 1];
+      }
+      return GM_CONVERGED;
+    }
     for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        double xv = ldcg(x + m * N + c);
+        double xv = from_zero ? 0.0 : ldcg(x + m * N + c);
         for (int i = 0; i <= jend; ++i) xv = xv + S.alpha[i] * (S.sigma[i] * ldcg(Vp(i) + m * N + c));
         x[m * N + c] = xv;
       }
     }
+    x_written = true;
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    count((jend + 3) * M);
+    count((jend + (from_zero ? 2 : 3)) * M);
     if (converged) {
       if (threadIdx.x == 0 && blockIdx.x == 0) {
         g.st->gmres_iters += iters;
@@ -754,7 +934,8 @@ __global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g
   unsigned phase = 0;
   op.bind();
   if (threadIdx.x == 0 && blockIdx.x == 0) g.st->gmres_solves += 1;
-  int code = gmres_device(op, g, x, b, S, tb, phase);
+  bool written = false;
+  int code = gmres_device(op, g, x, b, S, tb, phase, false, false, written);
   record_status(g.st, code);
 }
 
@@ -785,11 +966,12 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
     PressureOp L = op;
     L.jac = 0;
     if (lead) gw.st->gmres_solves += 1;
-    int code = gmres_device(L, gw, na.p, na.b, S, tb, phase);
+    bool written = false;
+    int code = gmres_device(L, gw, na.p, na.b, S, tb, phase, false, false, written);
     record_status(gw.st, code);
     return;
   }
-  // ---- Cor. 1 slope Mbig (implicit_operators.cpp:670-686); pf = p
+  // ---- Cor. 1 slope Mbig (implicit_operators.cpp:670-686)
   double Mbig = na.sc->Mbig;
   if (P.floor_on) {
     double mn = INFINITY, vpe = -INFINITY;
@@ -799,7 +981,6 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
         double v = Vbase(P, P.p_floor, __ldg(op.rho + c));
         if (isfinite(v)) vpe = fmax(vpe, v);
       }
-      na.pf[c] = na.p[c];
     }
     double a2[2] = {mn, vpe};
     // block min / max via shared memory
@@ -826,33 +1007,18 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       record_status(gw.st, GM_SYNC);
       return;
     }
-    __shared__ double mm[2];
-    if (threadIdx.x < 2) {
-      double v = threadIdx.x == 0 ? INFINITY : -INFINITY;
-      for (int bb = 0; bb < gw.nblk; ++bb) {
-        double q = ldcg(part() + (long long)bb * NP + threadIdx.x);
-        v = threadIdx.x == 0 ? fmin(v, q) : fmax(v, q);
-      }
-      mm[threadIdx.x] = v;
-    }
-    __syncthreads();
+    grid_reduce(part(), gw.nblk, 2, S.red, S.acc, RED_MIN | (RED_MAX << 2));
     ++phase;
-    double bmin = mm[0];
+    double bmin = S.red[0];
     double Vpe = P.p_floor / (P.gamma - 1.0);
-    if (P.eos_type != IMEX_IDEAL_GAS && mm[1] > Vpe) Vpe = mm[1];
+    if (P.eos_type != IMEX_IDEAL_GAS && S.red[1] > Vpe) Vpe = S.red[1];
     double q = Vpe - bmin;
     double M_cor = ((0.0 < q) ? q : 0.0) / ((1.0 - P.theta) * P.p_floor);
     double M_base = P.Mbig_fac / (P.gamma - 1.0);
     Mbig = (M_base < M_cor) ? M_cor : M_base;
     if (lead) {
       na.sc->Mbig = Mbig;
-      gw.st->alg_bytes[gw.fam] += 3.0 * 8.0 * (double)N;
-    }
-  } else {
-    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) na.pf[c] = na.p[c];
-    if (!grid_barrier(gw.sync, gw.nblk)) {
-      record_status(gw.st, GM_SYNC);
-      return;
+      gw.st->alg_bytes[gw.fam] += (P.eos_type != IMEX_IDEAL_GAS ? 2.0 : 1.0) * 8.0 * (double)N;
     }
   }
   PressureOp L = op, J = op;
@@ -861,13 +1027,35 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   J.vdiag = na.vdiag;
   const double a = op.a;
   double res0 = -1.0;
+  // The Newton iterate pf is double buffered between p (which holds the initial guess) and
+  // the pf plane: each residual pass reads pf_cur at the tile halo and writes the updated
+  // iterate to pf_nxt.  The Jacobian GMRES runs in deferred mode, so its update
+  // dp = sum_i alpha_i v_i (+ dp when an earlier restart cycle wrote it) is added to pf
+  // inside the next residual pass instead of in two passes of its own.
+  double* pf_cur = na.p;
+  double* pf_nxt = na.pf;
+  bool pending = false;  // a GMRES update waits to be added to pf
+  bool dp_live = false;  // dp holds the part of that update written by restart cycles
+  auto pf_update = [&](long long c) {
+    double d = dp_live ? ldcg(na.dp + c) : 0.0;
+    for (int i = 0; i < S.nalpha; ++i) d = d + S.alpha[i] * (S.sigma[i] * ldcg(gw.V + (long long)i * N + c));
+    return ldcg(pf_cur + c) + d;
+  };
   int it;
   for (it = 0; it < P.Pnewton_max; it++) {
-    // ---- residual g = L pf - a pf + V_mod(pf) - b  -> na.g = -g ; dp = 0 ; vdiag = V_slope(pf)
+    // ---- pf += pending update; residual g = L pf - a pf + V_mod(pf) - b -> na.g = -g; vdiag = V_slope(pf)
     wacc_clear(S.acc);
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile(L, tb, T, x0, y0, [&](long long c, double* v) { v[0] = ldcg(na.pf + c); });
+      fill_tile(L, tb, T, x0, y0, [&](const long long* c, double (*v)[1]) {
+        if (pending) {
+#pragma unroll
+          for (int r = 0; r < FillQ<PressureOp>; ++r) v[r][0] = pf_update(c[r]);
+        } else {
+#pragma unroll
+          for (int r = 0; r < FillQ<PressureOp>; ++r) v[r][0] = ldcg(pf_cur + c[r]);
+        }
+      });
       double gg = 0.0;
 #pragma unroll
       for (int r = 0; r < CPT; ++r) {
@@ -876,11 +1064,11 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
         double lp[1];
         L.matvec(tb, k.lx, k.ly, k.c, lp);
         const double pfc = tb.s[(k.ly + 1) * TB::SX + k.lx + 1];
+        if (pending) pf_nxt[k.c] = pfc;
         const double rc = __ldg(op.rho + k.c);
         const double gv = lp[0] - a * pfc + V_mod(P, Mbig, pfc, rc) - na.b[k.c];
         gg += gv * gv;
         na.g[k.c] = -gv;
-        na.dp[k.c] = 0.0;
         na.vdiag[k.c] = V_slope(P, Mbig, pfc, rc);
       }
       wacc_add(S.acc, 0, gg);
@@ -891,9 +1079,17 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       record_status(gw.st, GM_SYNC);
       return;
     }
-    grid_sum(part(), gw.nblk, 1, S.red);
+    grid_reduce(part(), gw.nblk, 1, S.red, S.acc);
     ++phase;
-    if (lead) gw.st->alg_bytes[gw.fam] += (double)(PressureOp::COEF + 5) * 8.0 * (double)N;
+    if (lead)
+      gw.st->alg_bytes[gw.fam] +=
+          (double)(PressureOp::COEF + 4 + (pending ? 1 + S.nalpha + (dp_live ? 1 : 0) : 0)) * 8.0 * (double)N;
+    if (pending) {
+      double* t = pf_cur;
+      pf_cur = pf_nxt;
+      pf_nxt = t;
+      pending = false;
+    }
     const double res = sqrt(S.red[0]);
     if (it == 0) res0 = res;
     if (!isfinite(res)) {
@@ -901,30 +1097,25 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       break;
     }
     if (res < P.Pnewton_tol * res0 + P.Pnewton_tol) break;
-    // ---- Jacobian solve J dp = -g (GMRES with precP)
+    // ---- Jacobian solve J dp = -g (GMRES with precP), from dp = 0, update deferred
     if (lead) {
       gw.st->gmres_solves += 1;
       gw.st->newton_iters += 1;
     }
-    int code = gmres_device(J, gw, na.dp, na.g, S, tb, phase);
+    int code = gmres_device(J, gw, na.dp, na.g, S, tb, phase, true, true, dp_live);
     if (code != GM_CONVERGED) {
       record_status(gw.st, code);
       if (code == GM_SYNC || code == GM_NONFINITE) return;
     }
-    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT)
-      na.pf[c] = ldcg(na.pf + c) + ldcg(na.dp + c);
-    if (!grid_barrier(gw.sync, gw.nblk)) {
-      record_status(gw.st, GM_SYNC);
-      return;
-    }
-    if (lead) gw.st->alg_bytes[gw.fam] += 3.0 * 8.0 * (double)N;
+    pending = true;
   }
   if (it == P.Pnewton_max && lead) atomicMax(&gw.st->status, (int)IMEX_NEWTON_MAXIT);
-  if (lead) gw.st->alg_bytes[gw.fam] += 2.0 * 8.0 * (double)N;
-  // ---- p = pf, floored-cell count and min p (implicit_operators.cpp:722-737)
+  if (lead) gw.st->alg_bytes[gw.fam] += (double)(2 + (pending ? S.nalpha + (dp_live ? 1 : 0) : 0)) * 8.0 * (double)N;
+  // ---- p = pf (+ an update still pending after Pnewton_max), floored-cell count and min p
+  // (implicit_operators.cpp:722-737)
   double st2[2] = {0.0, INFINITY};
   for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
-    const double pv = ldcg(na.pf + c);
+    const double pv = pending ? pf_update(c) : ldcg(pf_cur + c);
     na.p[c] = pv;
     if (pv < P.p_floor) st2[0] += 1.0;
     st2[1] = fmin(st2[1], pv);
@@ -953,12 +1144,9 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       record_status(gw.st, GM_SYNC);
       return;
     }
+    grid_reduce(part(), gw.nblk, 2, S.red, S.acc, RED_SUM | (RED_MIN << 2));
     if (lead) {
-      double nf = 0.0, pmin = INFINITY;
-      for (int bb = 0; bb < gw.nblk; ++bb) {
-        nf += ldcg(part() + (long long)bb * NP + 0);
-        pmin = fmin(pmin, ldcg(part() + (long long)bb * NP + 1));
-      }
+      const double nf = S.red[0], pmin = S.red[1];
       if ((int)nf > gw.st->max_floored) gw.st->max_floored = (int)nf;
       if (pmin < gw.st->min_p) gw.st->min_p = pmin;
       if (pmin < P.theta * P.p_floor - 1e-14) atomicMax(&gw.st->status, (int)IMEX_POSITIVITY);
@@ -1167,8 +1355,7 @@ __global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__
 // A** right-hand side (imex_subsystems.cpp:18-51), x0 = A
 __global__ void k_magnetic_rhs_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                  const double* __restrict__ Qe, const double* __restrict__ pe,
-                                 const double* __restrict__ A_s, const double* __restrict__ A,
-                                 double* __restrict__ b, double* __restrict__ x0) {
+                                 const double* __restrict__ A_s, double* __restrict__ b) {
   const long long N = P.N;
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1182,9 +1369,6 @@ __global__ void k_magnetic_rhs_A(DevParams P, const DevScalars* __restrict__ sc,
   b[n] = A_s[n] - h * (Byn * Sz - Bzn * Sy);
   b[N + n] = A_s[N + n] - h * (Bzn * Sx - Bxn * Sz);
   b[2 * N + n] = A_s[2 * N + n] - h * (Bxn * Sy - Byn * Sx);
-  x0[n] = A[n];
-  x0[N + n] = A[N + n];
-  x0[2 * N + n] = A[2 * N + n];
 }
 // global A-viscosity maxima of prim(Qs) over real cells (implicit_operators.cpp:364-374)
 __global__ void k_gmax(DevParams P, const double* __restrict__ Qs, double* __restrict__ partial) {
@@ -1262,9 +1446,11 @@ __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, 
   TileBuf<Op>& tb = *reinterpret_cast<TileBuf<Op>*>(dsm);
   for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
     const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-    fill_tile(op, tb, T, x0, y0, [&](long long c, double* v) {
+    fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[Op::M]) {
 #pragma unroll
-      for (int m = 0; m < Op::M; ++m) v[m] = x[m * T.N + c];
+      for (int r = 0; r < FillQ<Op>; ++r)
+#pragma unroll
+        for (int m = 0; m < Op::M; ++m) v[r][m] = x[m * T.N + c[r]];
     });
 #pragma unroll
     for (int r = 0; r < CPT; ++r) {
@@ -1343,15 +1529,19 @@ GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
 }  // namespace
 __global__ void k_reset_sync(SyncState* s, long long limit) {
   s->count = 0;
-  s->generation = 0;
   s->abort = 0;
-  s->spin_limit = limit;
+  s->wait_cycles = limit;
 }
 namespace {
-// every device-wide wait gives up after ~barrier_timeout_s (a wait never legitimately lasts that long)
+// every device-wide wait gives up after ~barrier_timeout_s (a wait never legitimately lasts that
+// long); counted in SM cycles at the maximum clock, so a slower clock only lengthens the bound.
+// The clock rate is read once at creation: querying it per launch stalls the host.
+long long wait_cycles(const imex_ctx* ctx) {
+  const double khz = ctx->clock_khz > 0 ? (double)ctx->clock_khz : 2.0e6;
+  return (long long)(ctx->barrier_timeout_s * khz * 1e3) + 1;
+}
 imex_status reset_sync(imex_ctx* ctx) {
-  const long long limit = (long long)(ctx->barrier_timeout_s / 64e-9) + 1;
-  k_reset_sync<<<1, 1, 0, ctx->stream>>>(ctx->sync, limit);
+  k_reset_sync<<<1, 1, 0, ctx->stream>>>(ctx->sync, wait_cycles(ctx));
   return cuda_check(ctx, cudaGetLastError(), "sync reset");
 }
 
@@ -1505,8 +1695,7 @@ imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, con
   if (hb && e == cudaSuccess) e = cudaMemcpyAsync((void*)bd, b, n * sizeof(double), cudaMemcpyDefault, ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "imex_gmres_noalloc: vector upload");
   // the barrier state must start at zero on every call
-  const long long limit = (long long)(ctx->barrier_timeout_s / 64e-9) + 1;
-  k_reset_sync<<<1, 1, 0, ctx->stream>>>(g.sync, limit);
+  k_reset_sync<<<1, 1, 0, ctx->stream>>>(g.sync, wait_cycles(ctx));
   LAUNCH_CHECK(ctx, "imex_gmres_noalloc: sync reset");
   void* params[] = {(void*)&o, (void*)&g, (void*)&xd, (void*)&bd};
   e = cudaLaunchCooperativeKernel((const void*)kern, dim3(nb), dim3(NT), params, sizeof(SolveSmem<Op>), ctx->stream);
@@ -1554,14 +1743,13 @@ imex_status run_mag_subsystem_B(imex_ctx* ctx) {
   imex_status s;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
-  k_magnetic_rhs_B<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->Qs, ctx->pe, ctx->mb, ctx->mx);
+  // the initial guess Qe B goes straight into the cell B planes of u_con (planes 5-7; the
+  // kernel reads only planes 0-3 of u_con), which GMRES then overwrites with the solution
+  k_magnetic_rhs_B<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->Qs, ctx->pe, ctx->mb,
+                                                    ctx->cons + 5 * P.N);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_B");
   prof_end(ctx, F_MAG_RHS, BYTES(17), 1);
-  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_B, ctx->mx, ctx->mb)) != IMEX_OK) return s;
-  prof_begin(ctx);
-  k_copy3<<<blocks_for(3 * P.N), kThreads, 0, ctx->stream>>>(P.N, ctx->mx, ctx->cons + 5 * P.N);
-  LAUNCH_CHECK(ctx, "k_copy3");
-  prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
+  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_B, ctx->cons + 5 * P.N, ctx->mb)) != IMEX_OK) return s;
   prof_begin(ctx);
   k_collect_mag_fluxes<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
   LAUNCH_CHECK(ctx, "k_collect_mag_fluxes");
@@ -1582,17 +1770,15 @@ imex_status run_mag_subsystem_A(imex_ctx* ctx) {
   LAUNCH_CHECK(ctx, "k_gmax_finalize");
   prof_end(ctx, F_GMAX, BYTES(8), 2);
   prof_begin(ctx);
-  k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->A, ctx->mb,
-                                                    ctx->mx);
+  k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
-  prof_end(ctx, F_MAG_RHS, BYTES(20), 1);
-  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_A, ctx->mx, ctx->mb)) != IMEX_OK) return s;
+  prof_end(ctx, F_MAG_RHS, BYTES(14), 1);
+  // solved in place: the initial guess is the current A (imex_subsystems.cpp:46-60)
+  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_A, ctx->A, ctx->mb)) != IMEX_OK) return s;
   prof_begin(ctx);
-  k_copy3<<<blocks_for(3 * P.N), kThreads, 0, ctx->stream>>>(P.N, ctx->mx, ctx->A);
-  LAUNCH_CHECK(ctx, "k_copy3");
   k_curl_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->A, ctx->cons);
   LAUNCH_CHECK(ctx, "k_curl_A");
-  prof_end(ctx, F_MAG_OUT, BYTES(6 + 6), 2);
+  prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
   return IMEX_OK;
 }
 
@@ -1709,8 +1895,7 @@ imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_bloc
   e = cudaMemcpyAsync(&h, cyc, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "barrier self-test");
-  int clk_khz = 0;
-  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, 0);
+  const int clk_khz = ctx->clock_khz;
   if (us_per_barrier) *us_per_barrier = (iterations > 0 && clk_khz > 0) ? (double)h / iterations / (clk_khz * 1e-3) : 0.0;
   return IMEX_OK;
 }
