@@ -316,6 +316,22 @@ def main() -> int:
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "path": "imex_upload_state + imex_step + imex_download_state, pinned host buffers"}
 
+    # accuracy of the mixed form: the same two steps in FP64 and in the mixed form
+    accuracy = None
+    if args.precision == "mixed" and rank == 0:
+        import numpy as np
+        res = []
+        for prec in ("fp64", "mixed"):
+            sv = ix.Solver.for_problem(prob, wl["rks"], dict(wl["settings"], precision=prec))
+            for _ in range(2):
+                sv.step()
+            res.append(sv.cons())
+            sv.close()
+        errs = [float(np.linalg.norm(res[1][k] - res[0][k]) / max(np.linalg.norm(res[0][k]), 1e-300))
+                for k in range(8)]
+        accuracy = {"reference": "FP64 GPU path (parity-tested against the FP64 oracle)", "steps": 2,
+                    "max_rel_l2_per_field": max(errs), "rel_l2_per_field": errs}
+
     line = None
     if rank == 0:
         cpu = None
@@ -328,7 +344,8 @@ def main() -> int:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (analytic initial data, no dataset)",
             "config": {"workload": args.workload, "description": wl["desc"],
                        "grid": f"{prob.nx}x{prob.ny}", "stages_per_step": wl["rks"],
@@ -339,8 +356,10 @@ def main() -> int:
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
+            "accuracy": accuracy,
             "solver": {"gmres_iters": stats["gmres_iters"], "gmres_solves": stats["gmres_solves"],
-                       "newton_iters": stats["newton_iters"], "status": stats["status"],
+                       "newton_iters": stats["newton_iters"], "refine_sweeps": stats["refine_sweeps"],
+                       "status": stats["status"],
                        "alg_bytes_per_step": step_bytes / args.steps,
                        "stage_hbm_frac": step_bytes / (t_ms / 1e3) / 1e9 / peak},
             "kernels": sorted(({"name": r["name"], "share": r["total_ms"] / total_prof_ms,

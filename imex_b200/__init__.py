@@ -69,7 +69,7 @@ class Config(C.Structure):
         ("x_0", C.c_double), ("x_1", C.c_double), ("y_0", C.c_double), ("y_1", C.c_double),
         ("time_stop", C.c_double), ("fixed_dt", C.c_double), ("gmres_restart", C.c_int),
         ("gmres_max_restarts", C.c_int), ("precision", C.c_int), ("mixed_inner_tol", C.c_double),
-        ("mixed_max_refine", C.c_int),
+        ("mixed_max_refine", C.c_int), ("mixed_solves", C.c_int),
     ]
 
 

@@ -85,9 +85,15 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if (c->recon < IMEX_NoRecon || c->recon > IMEX_WENO5) return why = "bad recon", IMEX_ERR_INVALID;
   if (c->magfield < IMEX_StaggerCT || c->magfield > IMEX_NoDivFree) return why = "bad magfield", IMEX_ERR_INVALID;
   if (c->gmres_restart < 1 || c->gmres_restart > 30) return why = "gmres_restart must be in 1..30", IMEX_ERR_INVALID;
-  if (c->precision == IMEX_PRECISION_MIXED)
-    return why = "mixed precision is not built yet", IMEX_ERR_UNSUPPORTED;
-  if (c->precision != IMEX_PRECISION_FP64) return why = "bad precision", IMEX_ERR_INVALID;
+  if (c->precision != IMEX_PRECISION_FP64 && c->precision != IMEX_PRECISION_MIXED)
+    return why = "bad precision", IMEX_ERR_INVALID;
+  if (c->precision == IMEX_PRECISION_MIXED) {
+    if (!(c->mixed_inner_tol > 0.0 && c->mixed_inner_tol < 1.0))
+      return why = "mixed_inner_tol must be in (0, 1)", IMEX_ERR_INVALID;
+    if (c->mixed_max_refine < 1) return why = "mixed_max_refine must be at least 1", IMEX_ERR_INVALID;
+    if (c->mixed_solves & ~(IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC))
+      return why = "bad mixed_solves", IMEX_ERR_INVALID;
+  }
   if (!(c->x_1 > c->x_0) || !(c->y_1 > c->y_0)) return why = "empty domain", IMEX_ERR_INVALID;
   return IMEX_OK;
 }
@@ -313,8 +319,9 @@ void imex_config_default(imex_config* c) {
   c->gmres_restart = 25;
   c->gmres_max_restarts = 1000;
   c->precision = IMEX_PRECISION_FP64;
-  c->mixed_inner_tol = 1e-5;
+  c->mixed_inner_tol = 1e-6;
   c->mixed_max_refine = 50;
+  c->mixed_solves = IMEX_MIXED_PRESSURE;
 }
 
 imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) {
@@ -399,6 +406,9 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   A_(mx, 3 * N); A_(mb, 3 * N);
   A_(chit, N); A_(Epp, N); A_(Et, N);
   A_(V, kv * 3 * N); A_(AV, 2 * 3 * N);
+  if (cfg->precision == IMEX_PRECISION_MIXED) {
+    A_(Vf, kv * 3 * N); A_(AVf, 2 * 3 * N); A_(mres, 3 * N); A_(mcor, 3 * N);
+  }
   A_(partial, 2 * (size_t)ctx->max_blocks * NPSLOTS);
   A_(red, 64);
   A_(sc, 1); A_(st, 1); A_(sync, 1);

@@ -28,6 +28,9 @@ constexpr int KCAP = 30;        // largest supported restart length
 constexpr int NP = KCAP + 2;    // partial-sum slots per CTA
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+// Krylov vectors are stored as double (plain form) or float (mixed form); both load as double
+__device__ __forceinline__ double ldv(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldv(const float* p) { return (double)__ldcg(p); }
 
 // ------------------------------------------------------------------ grid barrier
 // Bounded barrier over a cooperative launch (all CTAs co-resident).  The arrival
@@ -194,23 +197,24 @@ __device__ __forceinline__ int wrapc(int i, int n) {
 
 template <class Op>
 struct TileBuf {
+  using T = typename Op::value_type;
   static constexpr int H = Op::HALO;
   static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SN = SX * SY;
   static constexpr int PX = TX + 2, PY = TY + 2, PN = PX * PY;  // halo-1 region of the pre-pass
-  double s[Op::M * SN];           // vector tile
-  double c[Op::QT * SN];          // frozen coefficients on the same cells
-  double p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
+  T s[Op::M * SN];           // vector tile
+  T c[Op::QT * SN];          // frozen coefficients on the same cells
+  T p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
 };
 
 // ------------------------------------------------------------------ operators
+// Each operator is a template on its arithmetic type T: double is the plain FP64
+// path (the same operations, in the same order, as the reference), float the
+// operator of the inner solves of the mixed-precision form.  Coefficients are
+// read from the FP64 planes and rounded to T when a tile is staged.
+//
 // Pressure_Subsystem_AX (implicit_operators.cpp:505-616), GLF viscosity, periodic,
 // with the frozen coefficient planes of one solve; precP (implicit_operators.cpp:650-662).
-struct PressureOp {
-  static constexpr int M = 1, HALO = 1;
-  static constexpr int COEF = 5;  // hh, eta, rho, vscale, tdiag (+ vdiag in J mode)
-  static constexpr int QT = 2;    // staged: hh, eta
-  static constexpr int PT = 0;
-  static constexpr int MIN_BLOCKS = 2;
+struct PressureCoef {
   DevParams P;
   const DevScalars* sc;
   const double *hh, *eta, *rho, *vscale, *tdiag, *vdiag;
@@ -235,41 +239,54 @@ struct PressureOp {
     cvy = nu_y / (P.dy * P.dy);
     a = 1.0 / (P.gamma - 1.0);
   }
-  __device__ __forceinline__ void coef(long long c, double* q) const {
-    q[0] = __ldg(hh + c);
-    q[1] = __ldg(eta + c);
+};
+template <class T>
+struct PressureOpT : PressureCoef {
+  using value_type = T;
+  static constexpr int M = 1, HALO = 1;
+  static constexpr int COEF = 5;  // hh, eta, rho, vscale, tdiag (+ vdiag in J mode)
+  static constexpr int QT = 2;    // staged: hh, eta
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 2;
+  // the same operator with arithmetic type U
+  template <class U>
+  __device__ __forceinline__ PressureOpT<U> as() const {
+    PressureOpT<U> o;
+    static_cast<PressureCoef&>(o) = *this;
+    return o;
+  }
+  __device__ __forceinline__ void coef(long long c, T* q) const {
+    q[0] = (T)__ldg(hh + c);
+    q[1] = (T)__ldg(eta + c);
   }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>
-  __device__ __forceinline__ void matvec(const TB& tb, int lx, int ly, long long c, double* out) const {
+  __device__ __forceinline__ void matvec(const TB& tb, int lx, int ly, long long c, T* out) const {
     const int sx = TB::SX, o = (ly + 1) * sx + lx + 1;
-    const double* x = tb.s;
-    const double* hq = tb.c;
-    const double* eq = tb.c + TB::SN;
-    const double xc = x[o], xe = x[o + 1], xw = x[o - 1], xn = x[o + sx], xs = x[o - sx];
-    const double h00 = hq[o], hp0 = hq[o + 1], hm0 = hq[o - 1], h0p = hq[o + sx], h0m = hq[o - sx];
-    const double Vd = jac ? __ldcg(vdiag + c) : a;
-    double r = Vd * xc - hh2 * (idx2 * (0.5 * (hp0 + h00) * (xe - xc) - 0.5 * (h00 + hm0) * (xc - xw)) +
-                                idy2 * (0.5 * (h0p + h00) * (xn - xc) - 0.5 * (h0m + h00) * (xc - xs)));
-    const double ec = eq[o], ee = eq[o + 1], ew = eq[o - 1], en = eq[o + sx], es = eq[o - sx];
-    double lap = cvx * (0.5 * (ee + ec) * (xe - xc) - 0.5 * (ec + ew) * (xc - xw)) +
-                 cvy * (0.5 * (en + ec) * (xn - xc) - 0.5 * (ec + es) * (xc - xs));
-    out[0] = r - __ldg(vscale + c) * h * lap;
+    const T hf = T(0.5);
+    const T* x = tb.s;
+    const T* hq = tb.c;
+    const T* eq = tb.c + TB::SN;
+    const T xc = x[o], xe = x[o + 1], xw = x[o - 1], xn = x[o + sx], xs = x[o - sx];
+    const T h00 = hq[o], hp0 = hq[o + 1], hm0 = hq[o - 1], h0p = hq[o + sx], h0m = hq[o - sx];
+    const T Vd = jac ? (T)__ldcg(vdiag + c) : (T)a;
+    T r = Vd * xc - (T)hh2 * ((T)idx2 * (hf * (hp0 + h00) * (xe - xc) - hf * (h00 + hm0) * (xc - xw)) +
+                              (T)idy2 * (hf * (h0p + h00) * (xn - xc) - hf * (h0m + h00) * (xc - xs)));
+    const T ec = eq[o], ee = eq[o + 1], ew = eq[o - 1], en = eq[o + sx], es = eq[o - sx];
+    T lap = (T)cvx * (hf * (ee + ec) * (xe - xc) - hf * (ec + ew) * (xc - xw)) +
+            (T)cvy * (hf * (en + ec) * (xn - xc) - hf * (ec + es) * (xc - xs));
+    out[0] = r - (T)__ldg(vscale + c) * (T)h * lap;
   }
-  __device__ __forceinline__ void precond(long long c, double* v) const {
-    const double Vd = jac ? __ldcg(vdiag + c) : a;
-    v[0] = v[0] / (Vd + __ldg(tdiag + c));
+  __device__ __forceinline__ void precond(long long c, T* v) const {
+    const T Vd = jac ? (T)__ldcg(vdiag + c) : (T)a;
+    v[0] = v[0] / (Vd + (T)__ldg(tdiag + c));
   }
 };
+using PressureOp = PressureOpT<double>;
 
 // Magnetic_Subsystem_AX (implicit_operators.cpp:141-353), GLF viscosity, periodic.
-struct MagneticBOp {
-  static constexpr int M = 3, HALO = 1;
-  static constexpr int COEF = 4;  // Qe B (3), rho
-  static constexpr int QT = 4;    // staged: Qe Bx, By, Bz, rho
-  static constexpr int PT = 0;
-  static constexpr int MIN_BLOCKS = 1;  // the 9-point stencil keeps many corner averages live
+struct MagneticBCoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
@@ -281,130 +298,142 @@ struct MagneticBOp {
     cx = nu_x / (P.dx * P.dx);
     cy = nu_y / (P.dy * P.dy);
   }
-  __device__ __forceinline__ void coef(long long c, double* q) const {
-    q[0] = __ldg(Qe + 5 * P.N + c);
-    q[1] = __ldg(Qe + 6 * P.N + c);
-    q[2] = __ldg(Qe + 7 * P.N + c);
-    q[3] = __ldg(rho + c);
+};
+template <class T>
+struct MagneticBOpT : MagneticBCoef {
+  using value_type = T;
+  static constexpr int M = 3, HALO = 1;
+  static constexpr int COEF = 4;  // Qe B (3), rho
+  static constexpr int QT = 4;    // staged: Qe Bx, By, Bz, rho
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 1;  // the 9-point stencil keeps many corner averages live
+  template <class U>
+  __device__ __forceinline__ MagneticBOpT<U> as() const {
+    MagneticBOpT<U> o;
+    static_cast<MagneticBCoef&>(o) = *this;
+    return o;
+  }
+  __device__ __forceinline__ void coef(long long c, T* q) const {
+    q[0] = (T)__ldg(Qe + 5 * P.N + c);
+    q[1] = (T)__ldg(Qe + 6 * P.N + c);
+    q[2] = (T)__ldg(Qe + 7 * P.N + c);
+    q[3] = (T)__ldg(rho + c);
   }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
-  __device__ __forceinline__ void precond(long long, double*) const {}
+  __device__ __forceinline__ void precond(long long, T*) const {}
   template <class TB>
-  __device__ void matvec(const TB& tb, int lx, int ly, long long, double* out) const {
+  __device__ void matvec(const TB& tb, int lx, int ly, long long, T* out) const {
     constexpr int SX = TB::SX, SN = TB::SN;
-    const double dx = P.dx, dy = P.dy;
+    const T dx = (T)P.dx, dy = (T)P.dy, hT = (T)h, cxT = (T)cx, cyT = (T)cy;
+    const T hf = T(0.5), qf = T(0.25), one = T(1), two = T(2);
     const int o = (ly + 1) * SX + lx + 1;
     // offsets: C, E, W, N, S, NE, SE, NW, SW
     const int E = o + 1, W = o - 1, No = o + SX, S = o - SX, NE = No + 1, SE = S + 1, NW = No - 1, SW = S - 1;
-    const double* q5 = tb.c;
-    const double* q6 = tb.c + SN;
-    const double* q7 = tb.c + 2 * SN;
-    const double* rr = tb.c + 3 * SN;
-    const double* x5 = tb.s;
-    const double* x6 = tb.s + SN;
-    const double* x7 = tb.s + 2 * SN;
-    const double r0 = rr[o];
-    const double rho_p0 = 0.5 * (r0 + rr[E]), rho_m0 = 0.5 * (r0 + rr[W]);
-    const double rho_0p = 0.5 * (r0 + rr[No]), rho_0m = 0.5 * (r0 + rr[S]);
-#define FA(a, t) (0.5 * (a[o] + a[t]))
-#define CA(a, t1, t2, t3) (0.25 * (a[o] + a[t1] + a[t2] + a[t3]))
-#define QX(t) (0.5 * (q5[t] * x5[t] + q6[t] * x6[t] + q7[t] * x7[t]))
-    const double Bxn_pp = CA(q5, E, No, NE), Bxn_pm = CA(q5, E, S, SE), Bxn_mp = CA(q5, W, No, NW),
-                 Bxn_mm = CA(q5, W, S, SW);
-    const double Byn_pp = CA(q6, E, No, NE), Byn_pm = CA(q6, E, S, SE), Byn_mp = CA(q6, W, No, NW),
-                 Byn_mm = CA(q6, W, S, SW);
-    const double Bzn_pp = CA(q7, E, No, NE), Bzn_pm = CA(q7, E, S, SE), Bzn_mp = CA(q7, W, No, NW),
-                 Bzn_mm = CA(q7, W, S, SW);
-    const double Bx_pp = CA(x5, E, No, NE), Bx_pm = CA(x5, E, S, SE), Bx_mp = CA(x5, W, No, NW),
-                 Bx_mm = CA(x5, W, S, SW);
-    const double By_pp = CA(x6, E, No, NE), By_pm = CA(x6, E, S, SE), By_mp = CA(x6, W, No, NW),
-                 By_mm = CA(x6, W, S, SW);
-    const double Bz_pp = CA(x7, E, No, NE), Bz_pm = CA(x7, E, S, SE), Bz_mp = CA(x7, W, No, NW),
-                 Bz_mm = CA(x7, W, S, SW);
+    const T* q5 = tb.c;
+    const T* q6 = tb.c + SN;
+    const T* q7 = tb.c + 2 * SN;
+    const T* rr = tb.c + 3 * SN;
+    const T* x5 = tb.s;
+    const T* x6 = tb.s + SN;
+    const T* x7 = tb.s + 2 * SN;
+    const T r0 = rr[o];
+    const T rho_p0 = hf * (r0 + rr[E]), rho_m0 = hf * (r0 + rr[W]);
+    const T rho_0p = hf * (r0 + rr[No]), rho_0m = hf * (r0 + rr[S]);
+#define FA(a, t) (hf * (a[o] + a[t]))
+#define CA(a, t1, t2, t3) (qf * (a[o] + a[t1] + a[t2] + a[t3]))
+#define QX(t) (hf * (q5[t] * x5[t] + q6[t] * x6[t] + q7[t] * x7[t]))
+    const T Bxn_pp = CA(q5, E, No, NE), Bxn_pm = CA(q5, E, S, SE), Bxn_mp = CA(q5, W, No, NW),
+            Bxn_mm = CA(q5, W, S, SW);
+    const T Byn_pp = CA(q6, E, No, NE), Byn_pm = CA(q6, E, S, SE), Byn_mp = CA(q6, W, No, NW),
+            Byn_mm = CA(q6, W, S, SW);
+    const T Bzn_pp = CA(q7, E, No, NE), Bzn_pm = CA(q7, E, S, SE), Bzn_mp = CA(q7, W, No, NW),
+            Bzn_mm = CA(q7, W, S, SW);
+    const T Bx_pp = CA(x5, E, No, NE), Bx_pm = CA(x5, E, S, SE), Bx_mp = CA(x5, W, No, NW),
+            Bx_mm = CA(x5, W, S, SW);
+    const T By_pp = CA(x6, E, No, NE), By_pm = CA(x6, E, S, SE), By_mp = CA(x6, W, No, NW),
+            By_mm = CA(x6, W, S, SW);
+    const T Bz_pp = CA(x7, E, No, NE), Bz_pm = CA(x7, E, S, SE), Bz_mp = CA(x7, W, No, NW),
+            Bz_mm = CA(x7, W, S, SW);
     // the energy-like corner sums shared by several terms
-    const double Wpp = 0.5 * (Bxn_pp * Bx_pp + Byn_pp * By_pp + Bzn_pp * Bz_pp);
-    const double Wpm = 0.5 * (Bxn_pm * Bx_pm + Byn_pm * By_pm + Bzn_pm * Bz_pm);
-    const double Wmp = 0.5 * (Bxn_mp * Bx_mp + Byn_mp * By_mp + Bzn_mp * Bz_mp);
-    const double Wmm = 0.5 * (Bxn_mm * Bx_mm + Byn_mm * By_mm + Bzn_mm * Bz_mm);
-    const double QXc = QX(o);
+    const T Wpp = hf * (Bxn_pp * Bx_pp + Byn_pp * By_pp + Bzn_pp * Bz_pp);
+    const T Wpm = hf * (Bxn_pm * Bx_pm + Byn_pm * By_pm + Bzn_pm * Bz_pm);
+    const T Wmp = hf * (Bxn_mp * Bx_mp + Byn_mp * By_mp + Bzn_mp * Bz_mp);
+    const T Wmm = hf * (Bxn_mm * Bx_mm + Byn_mm * By_mm + Bzn_mm * Bz_mm);
+    const T QXc = QX(o);
     {  // x component (implicit_operators.cpp:266-275)
-      const double QXn = QX(No), QXs = QX(S);
-      const double Bx_1 = FA(q5, No) / rho_0p *
-                          (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
-                           1 / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
-      const double Bx_2 = FA(q6, No) / rho_0p *
-                          (1 / dx * ((Wpp - Bxn_pp * Bx_pp) - (Wmp - Bxn_mp * Bx_mp)) -
-                           1 / dy * (q6[No] * x5[No] - q6[o] * x5[o]));
-      const double Bx_3 = FA(q5, S) / rho_0m *
-                          (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
-                           1 / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
-      const double Bx_4 = FA(q6, S) / rho_0m *
-                          (1 / dx * ((Wpm - Bxn_pm * Bx_pm) - (Wmm - Bxn_mm * Bx_mm)) -
-                           1 / dy * (q6[o] * x5[o] - q6[S] * x5[S]));
-      const double ax5 = x5[o] + (h * h / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
-      out[0] = ax5 - h * (cx * (x5[W] - 2.0 * x5[o] + x5[E]) + cy * (x5[S] - 2.0 * x5[o] + x5[No]));
+      const T QXn = QX(No), QXs = QX(S);
+      const T Bx_1 = FA(q5, No) / rho_0p *
+                     (one / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
+                      one / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
+      const T Bx_2 = FA(q6, No) / rho_0p *
+                     (one / dx * ((Wpp - Bxn_pp * Bx_pp) - (Wmp - Bxn_mp * Bx_mp)) -
+                      one / dy * (q6[No] * x5[No] - q6[o] * x5[o]));
+      const T Bx_3 = FA(q5, S) / rho_0m *
+                     (one / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
+                      one / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
+      const T Bx_4 = FA(q6, S) / rho_0m *
+                     (one / dx * ((Wpm - Bxn_pm * Bx_pm) - (Wmm - Bxn_mm * Bx_mm)) -
+                      one / dy * (q6[o] * x5[o] - q6[S] * x5[S]));
+      const T ax5 = x5[o] + (hT * hT / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
+      out[0] = ax5 - hT * (cxT * (x5[W] - two * x5[o] + x5[E]) + cyT * (x5[S] - two * x5[o] + x5[No]));
     }
-    const double QXe = QX(E), QXw = QX(W);
+    const T QXe = QX(E), QXw = QX(W);
     {  // y component (implicit_operators.cpp:277-285)
-      const double By_1 = FA(q6, E) / rho_p0 *
-                          (-1 / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
-                           1 / dy * (Bxn_pp * By_pp - Bxn_pm * By_pm));
-      const double By_2 = FA(q5, E) / rho_p0 *
-                          (-1 / dx * (q5[E] * x6[E] - q5[o] * x6[o]) +
-                           1 / dy * ((Wpp - Byn_pp * By_pp) - (Wpm - Byn_pm * By_pm)));
-      const double By_3 = FA(q6, W) / rho_m0 *
-                          (-1 / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
-                           1 / dy * (Bxn_mp * By_mp - Bxn_mm * By_mm));
-      const double By_4 = FA(q5, W) / rho_m0 *
-                          (-1 / dx * (q5[o] * x6[o] - q5[W] * x6[W]) +
-                           1 / dy * ((Wmp - Byn_mp * By_mp) - (Wmm - Byn_mm * By_mm)));
-      const double ax6 = x6[o] + (h * h / dx) * ((By_1 + By_2) - (By_3 + By_4));
-      out[1] = ax6 - h * (cx * (x6[W] - 2.0 * x6[o] + x6[E]) + cy * (x6[S] - 2.0 * x6[o] + x6[No]));
+      const T By_1 = FA(q6, E) / rho_p0 *
+                     (-one / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
+                      one / dy * (Bxn_pp * By_pp - Bxn_pm * By_pm));
+      const T By_2 = FA(q5, E) / rho_p0 *
+                     (-one / dx * (q5[E] * x6[E] - q5[o] * x6[o]) +
+                      one / dy * ((Wpp - Byn_pp * By_pp) - (Wpm - Byn_pm * By_pm)));
+      const T By_3 = FA(q6, W) / rho_m0 *
+                     (-one / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
+                      one / dy * (Bxn_mp * By_mp - Bxn_mm * By_mm));
+      const T By_4 = FA(q5, W) / rho_m0 *
+                     (-one / dx * (q5[o] * x6[o] - q5[W] * x6[W]) +
+                      one / dy * ((Wmp - Byn_mp * By_mp) - (Wmm - Byn_mm * By_mm)));
+      const T ax6 = x6[o] + (hT * hT / dx) * ((By_1 + By_2) - (By_3 + By_4));
+      out[1] = ax6 - hT * (cxT * (x6[W] - two * x6[o] + x6[E]) + cyT * (x6[S] - two * x6[o] + x6[No]));
     }
     {  // z component (implicit_operators.cpp:288-306)
-      const double QXn = QX(No), QXs = QX(S);
-      const double Bz_1 = FA(q7, E) / rho_p0 *
-                          (-1 / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
-                           1 / dy * (Byn_pp * Bx_pp - Byn_pm * Bx_pm));
-      const double Bz_2 = FA(q5, E) / rho_p0 *
-                          (-1 / dx * (q5[E] * x7[E] - q5[o] * x7[o]) - 1 / dy * (Byn_pp * Bz_pp - Byn_pm * Bz_pm));
-      const double Bz_3 = FA(q7, W) / rho_m0 *
-                          (-1 / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
-                           1 / dy * (Byn_mp * Bx_mp - Byn_mm * Bx_mm));
-      const double Bz_4 = FA(q5, W) / rho_m0 *
-                          (-1 / dx * (q5[o] * x7[o] - q5[W] * x7[W]) - 1 / dy * (Byn_mp * Bz_mp - Byn_mm * Bz_mm));
-      const double Bz_5 = FA(q7, No) / rho_0p *
-                          (1 / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
-                           1 / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
-      const double Bz_6 = FA(q6, No) / rho_0p *
-                          (-1 / dx * (Bxn_pp * Bz_pp - Bxn_mp * Bz_mp) - 1 / dy * (q6[No] * x7[No] - q6[o] * x7[o]));
-      const double Bz_7 = FA(q7, S) / rho_0m *
-                          (1 / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
-                           1 / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
-      const double Bz_8 = FA(q6, S) / rho_0m *
-                          (-1 / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - 1 / dy * (q6[o] * x7[o] - q6[S] * x7[S]));
-      const double ax7 =
-          x7[o] + h * h / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + h * h / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
-      out[2] = ax7 - h * (cx * (x7[W] - 2.0 * x7[o] + x7[E]) + cy * (x7[S] - 2.0 * x7[o] + x7[No]));
+      const T QXn = QX(No), QXs = QX(S);
+      const T Bz_1 = FA(q7, E) / rho_p0 *
+                     (-one / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
+                      one / dy * (Byn_pp * Bx_pp - Byn_pm * Bx_pm));
+      const T Bz_2 = FA(q5, E) / rho_p0 *
+                     (-one / dx * (q5[E] * x7[E] - q5[o] * x7[o]) - one / dy * (Byn_pp * Bz_pp - Byn_pm * Bz_pm));
+      const T Bz_3 = FA(q7, W) / rho_m0 *
+                     (-one / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
+                      one / dy * (Byn_mp * Bx_mp - Byn_mm * Bx_mm));
+      const T Bz_4 = FA(q5, W) / rho_m0 *
+                     (-one / dx * (q5[o] * x7[o] - q5[W] * x7[W]) - one / dy * (Byn_mp * Bz_mp - Byn_mm * Bz_mm));
+      const T Bz_5 = FA(q7, No) / rho_0p *
+                     (one / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
+                      one / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
+      const T Bz_6 = FA(q6, No) / rho_0p *
+                     (-one / dx * (Bxn_pp * Bz_pp - Bxn_mp * Bz_mp) - one / dy * (q6[No] * x7[No] - q6[o] * x7[o]));
+      const T Bz_7 = FA(q7, S) / rho_0m *
+                     (one / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
+                      one / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
+      const T Bz_8 = FA(q6, S) / rho_0m *
+                     (-one / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - one / dy * (q6[o] * x7[o] - q6[S] * x7[S]));
+      const T ax7 =
+          x7[o] + hT * hT / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + hT * hT / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
+      out[2] = ax7 - hT * (cxT * (x7[W] - two * x7[o] + x7[E]) + cyT * (x7[S] - two * x7[o] + x7[No]));
     }
 #undef FA
 #undef CA
 #undef QX
   }
 };
+using MagneticBOp = MagneticBOpT<double>;
 
 // Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355-503), GLF, periodic.
 // The reference evaluates B = curl A and the stress tensor T^B at the four
 // neighbours of each cell; those values are exactly curl A and T^B of the
 // neighbouring cells, so the tile pre-pass computes them once per cell (same
 // arithmetic) and the per-cell pass only differences them.
-struct MagneticAOp {
-  static constexpr int M = 3, HALO = 2;
-  static constexpr int COEF = 4;  // Qe B (3), rho
-  static constexpr int QT = 3;    // staged: Qe Bx, By, Bz
-  static constexpr int PT = 6;    // Txx, Tyx, Tzx, Txy, Tyy, Tzy on the halo-1 region
-  static constexpr int MIN_BLOCKS = 2;
+struct MagneticACoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
@@ -417,81 +446,100 @@ struct MagneticAOp {
     cx = nu_x / (P.dx * P.dx);
     cy = nu_y / (P.dy * P.dy);
   }
-  __device__ __forceinline__ void coef(long long c, double* q) const {
-    q[0] = __ldg(Qe + 5 * P.N + c);
-    q[1] = __ldg(Qe + 6 * P.N + c);
-    q[2] = __ldg(Qe + 7 * P.N + c);
+};
+template <class T>
+struct MagneticAOpT : MagneticACoef {
+  using value_type = T;
+  static constexpr int M = 3, HALO = 2;
+  static constexpr int COEF = 4;  // Qe B (3), rho
+  static constexpr int QT = 3;    // staged: Qe Bx, By, Bz
+  static constexpr int PT = 6;    // Txx, Tyx, Tzx, Txy, Tyy, Tzy on the halo-1 region
+  static constexpr int MIN_BLOCKS = 2;
+  template <class U>
+  __device__ __forceinline__ MagneticAOpT<U> as() const {
+    MagneticAOpT<U> o;
+    static_cast<MagneticACoef&>(o) = *this;
+    return o;
   }
-  __device__ __forceinline__ void precond(long long, double*) const {}
+  __device__ __forceinline__ void coef(long long c, T* q) const {
+    q[0] = (T)__ldg(Qe + 5 * P.N + c);
+    q[1] = (T)__ldg(Qe + 6 * P.N + c);
+    q[2] = (T)__ldg(Qe + 7 * P.N + c);
+  }
+  __device__ __forceinline__ void precond(long long, T*) const {}
   template <class TB>
   __device__ __forceinline__ void prepass(TB& tb, int, int) const {
     constexpr int SX = TB::SX, SN = TB::SN;
-    const double dx = P.dx, dy = P.dy;
+    const T dx = (T)P.dx, dy = (T)P.dy, two = T(2);
     for (int q = threadIdx.x; q < TB::PN; q += NT) {
       const int px = q % TB::PX, py = q / TB::PX;
       const int o = (py + 1) * SX + (px + 1);  // same cell in the halo-2 tile
-      const double* A0 = tb.s;
-      const double* A1 = tb.s + SN;
-      const double* A2 = tb.s + 2 * SN;
-      const double bx = (A2[o + SX] - A2[o - SX]) / (2.0 * dy);
-      const double by = -(A2[o + 1] - A2[o - 1]) / (2.0 * dx);
-      const double bz = (A1[o + 1] - A1[o - 1]) / (2.0 * dx) - (A0[o + SX] - A0[o - SX]) / (2.0 * dy);
-      const double Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
-      const double bdot = Bx * bx + By * by + Bz * bz;
-      tb.p[0 * TB::PN + q] = bdot / 2.0 - Bx * bx;  // Txx
+      const T* A0 = tb.s;
+      const T* A1 = tb.s + SN;
+      const T* A2 = tb.s + 2 * SN;
+      const T bx = (A2[o + SX] - A2[o - SX]) / (two * dy);
+      const T by = -(A2[o + 1] - A2[o - 1]) / (two * dx);
+      const T bz = (A1[o + 1] - A1[o - 1]) / (two * dx) - (A0[o + SX] - A0[o - SX]) / (two * dy);
+      const T Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
+      const T bdot = Bx * bx + By * by + Bz * bz;
+      tb.p[0 * TB::PN + q] = bdot / two - Bx * bx;  // Txx
       tb.p[1 * TB::PN + q] = -Bx * by;              // Tyx
       tb.p[2 * TB::PN + q] = -Bx * bz;              // Tzx
       tb.p[3 * TB::PN + q] = -By * bx;              // Txy
-      tb.p[4 * TB::PN + q] = bdot / 2.0 - By * by;  // Tyy
+      tb.p[4 * TB::PN + q] = bdot / two - By * by;  // Tyy
       tb.p[5 * TB::PN + q] = -By * bz;              // Tzy
     }
   }
   template <class TB>
-  __device__ void matvec(const TB& tb, int lx, int ly, long long c, double* out) const {
+  __device__ void matvec(const TB& tb, int lx, int ly, long long c, T* out) const {
     constexpr int SX = TB::SX, SN = TB::SN, PX = TB::PX, PN = TB::PN;
-    const double dx = P.dx, dy = P.dy;
+    const T dx = (T)P.dx, dy = (T)P.dy, hT = (T)h, two = T(2);
     const int o = (ly + 2) * SX + lx + 2;  // halo-2 tile
     const int p = (ly + 1) * PX + lx + 1;  // halo-1 pre-pass region
-    const double* T = tb.p;
-    const double divT_x = (T[0 * PN + p + 1] - T[0 * PN + p - 1]) / (2.0 * dx) +
-                          (T[3 * PN + p + PX] - T[3 * PN + p - PX]) / (2.0 * dy);
-    const double divT_y = (T[1 * PN + p + 1] - T[1 * PN + p - 1]) / (2.0 * dx) +
-                          (T[4 * PN + p + PX] - T[4 * PN + p - PX]) / (2.0 * dy);
-    const double divT_z = (T[2 * PN + p + 1] - T[2 * PN + p - 1]) / (2.0 * dx) +
-                          (T[5 * PN + p + PX] - T[5 * PN + p - PX]) / (2.0 * dy);
-    const double hr = h / __ldg(rho + c);
-    const double Fx = hr * divT_x, Fy = hr * divT_y, Fz = hr * divT_z;
-    const double Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
-    const double cross_x = By * Fz - Bz * Fy;
-    const double cross_y = Bz * Fx - Bx * Fz;
-    const double cross_z = Bx * Fy - By * Fx;
+    const T* Tq = tb.p;
+    const T divT_x = (Tq[0 * PN + p + 1] - Tq[0 * PN + p - 1]) / (two * dx) +
+                     (Tq[3 * PN + p + PX] - Tq[3 * PN + p - PX]) / (two * dy);
+    const T divT_y = (Tq[1 * PN + p + 1] - Tq[1 * PN + p - 1]) / (two * dx) +
+                     (Tq[4 * PN + p + PX] - Tq[4 * PN + p - PX]) / (two * dy);
+    const T divT_z = (Tq[2 * PN + p + 1] - Tq[2 * PN + p - 1]) / (two * dx) +
+                     (Tq[5 * PN + p + PX] - Tq[5 * PN + p - PX]) / (two * dy);
+    const T hr = hT / (T)__ldg(rho + c);
+    const T Fx = hr * divT_x, Fy = hr * divT_y, Fz = hr * divT_z;
+    const T Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
+    const T cross_x = By * Fz - Bz * Fy;
+    const T cross_y = Bz * Fx - Bx * Fz;
+    const T cross_z = Bx * Fy - By * Fx;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const double* A = tb.s + k * SN;
-      double lap = 0.0;
+      const T* A = tb.s + k * SN;
+      T lap = T(0);
       if (add_bvisc)
-        lap = cx * (A[o - 1] - 2.0 * A[o] + A[o + 1]) + cy * (A[o - SX] - 2.0 * A[o] + A[o + SX]);
-      const double cr = k == 0 ? cross_x : (k == 1 ? cross_y : cross_z);
-      out[k] = A[o] - h * cr - h * lap;
+        lap = (T)cx * (A[o - 1] - two * A[o] + A[o + 1]) + (T)cy * (A[o - SX] - two * A[o] + A[o + SX]);
+      const T cr = k == 0 ? cross_x : (k == 1 ? cross_y : cross_z);
+      out[k] = A[o] - hT * cr - hT * lap;
     }
   }
 };
+using MagneticAOp = MagneticAOpT<double>;
 
 template <class Op>
 __device__ __forceinline__ bool op_uses_vdiag(const Op&) { return false; }
-template <>
-__device__ __forceinline__ bool op_uses_vdiag<PressureOp>(const PressureOp& o) { return o.jac != 0; }
+template <class T>
+__device__ __forceinline__ bool op_uses_vdiag(const PressureOpT<T>& o) { return o.jac != 0; }
 
 // ------------------------------------------------------------------ GMRES
-struct GmresWork {
-  double *V, *AV, *partial;
+template <class TS>
+struct GmresWorkT {
+  TS *V, *AV;  // Krylov basis (kmax + 1 vectors) and the A v ring (2 vectors)
+  double* partial;
   SyncState* sync;
   DevStats* st;
   int kmax, max_restarts, nblk;
   int fam;  // profile family whose algorithmic bytes this solve accumulates
-  double tol;
+  double tol, tol_abs;  // stop when |r| <= tol * |r0| + tol_abs
   Tiling T;
 };
+using GmresWork = GmresWorkT<double>;
 
 struct GmresShared {
   double H[KCAP + 2][KCAP + 2];
@@ -511,6 +559,7 @@ constexpr int FillQ = (TileBuf<Op>::SN + NT - 1) / NT;
 template <class Op, class F>
 __device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const Tiling& T, int x0, int y0, F f) {
   using TB = TileBuf<Op>;
+  using VT = typename Op::value_type;
   constexpr int Q = FillQ<Op>;
   constexpr int QC = Op::QT > 0 ? Op::QT : 1;
   long long c[Q];
@@ -522,10 +571,10 @@ __device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const T
     const int gi = wrapc(x0 + sxq - Op::HALO, T.nx), gj = wrapc(y0 + syq - Op::HALO, T.ny);
     c[r] = (long long)gi + (long long)T.nx * gj;
   }
-  double qv[Q][QC];
+  VT qv[Q][QC];
 #pragma unroll
   for (int r = 0; r < Q; ++r) op.coef(c[r], qv[r]);
-  double v[Q][Op::M];
+  VT v[Q][Op::M];
   f(c, v);
 #pragma unroll
   for (int r = 0; r < Q; ++r) {
@@ -571,10 +620,11 @@ enum { GM_CONVERGED = 0, GM_MAXIT = 1, GM_NONFINITE = 2, GM_SYNC = 3 };
 //   written; S.alpha[0..S.nalpha) and S.sigma stay in shared memory for the caller to
 //   apply in its next pass (the basis stays in g.V).  x_written reports whether an
 //   earlier cycle wrote x, in which case the full update is x + that sum.
-template <class Op>
-__device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const double* b, GmresShared& S,
+template <class Op, class TS>
+__device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, const double* b, GmresShared& S,
                             TileBuf<Op>& tb, unsigned& phase, bool x_zero, bool defer, bool& x_written) {
   using TB = TileBuf<Op>;
+  using VT = typename Op::value_type;  // arithmetic of the operator and the staged tile
   constexpr int M = Op::M, HALO = Op::HALO, FQ = FillQ<Op>;
   const Tiling& T = g.T;
   const long long N = T.N;
@@ -586,9 +636,10 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
   auto part = [&]() { return g.partial + (long long)(phase & 1) * g.nblk * NP; };
   const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
   const int coef = Op::COEF + (op_uses_vdiag(op) ? 1 : 0);
-  // algorithmic bytes of a pass that moves `vals` doubles per cell
-  auto count = [&](int vals) {
-    if (lead) g.st->alg_bytes[g.fam] += (double)vals * 8.0 * (double)N;
+  // algorithmic bytes of a pass that moves `vals` vector values (of type TS) and `cvals`
+  // doubles per cell
+  auto count = [&](int vals, int cvals) {
+    if (lead) g.st->alg_bytes[g.fam] += ((double)vals * sizeof(TS) + (double)cvals * 8.0) * (double)N;
   };
   (void)HALO;
   x_written = false;
@@ -596,16 +647,17 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
 
   for (int outer = 0; outer < g.max_restarts; ++outer) {
     const bool from_zero = x_zero && outer == 0;
+    const bool last_cycle = outer + 1 >= g.max_restarts;
     if (from_zero) {
       // ---- r0 = M^-1 b -> V0 and Av0 = M^-1 A V0 in one pass; |r0|^2 and r0.Av0
       wacc_clear(S.acc);
       for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
 #pragma unroll
-            for (int m = 0; m < M; ++m) v[r][m] = ldcg(b + m * N + c[r]);
+            for (int m = 0; m < M; ++m) v[r][m] = (VT)ldcg(b + m * N + c[r]);
 #pragma unroll
           for (int r = 0; r < FQ; ++r) op.precond(c[r], v[r]);
         });
@@ -614,17 +666,17 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
         for (int r = 0; r < CPT; ++r) {
           const Cell k = tile_cell(T, x0, y0, r);
           if (!k.in) continue;
-          double aw[M];
+          VT aw[M];
           op.matvec(tb, k.lx, k.ly, k.c, aw);
           op.precond(k.c, aw);
           const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
 #pragma unroll
           for (int m = 0; m < M; ++m) {
-            const double w = tb.s[m * TB::SN + o];
-            Vp(0)[m * N + k.c] = w;
-            AVp(0)[m * N + k.c] = aw[m];
+            const double w = (double)tb.s[m * TB::SN + o];
+            Vp(0)[m * N + k.c] = (TS)w;
+            AVp(0)[m * N + k.c] = (TS)aw[m];
             rr += w * w;
-            va += w * aw[m];
+            va += w * (double)aw[m];
           }
         }
         wacc_add(S.acc, 0, rr);
@@ -635,9 +687,9 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_reduce(part(), g.nblk, 2, S.red, S.acc);
       ++phase;
-      count(3 * M + coef);
+      count(2 * M, M + coef);
       S.gam[0] = sqrt(S.red[0]);
-      tol_eff = g.tol * S.gam[0] + g.tol;
+      tol_eff = g.tol * S.gam[0] + g.tol_abs;
       if (!isfinite(S.gam[0])) return GM_NONFINITE;
       if (S.gam[0] <= tol_eff) {
         if (lead) {
@@ -658,118 +710,125 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[1];
       __syncthreads();
     } else {
-    // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
-    wacc_clear(S.acc);
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
-      const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+      // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
+      wacc_clear(S.acc);
+      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
-        for (int r = 0; r < FQ; ++r)
+          for (int r = 0; r < FQ; ++r)
 #pragma unroll
-          for (int m = 0; m < M; ++m) v[r][m] = ldcg(x + m * N + c[r]);
-      });
-      double rr = 0.0;
+            for (int m = 0; m < M; ++m) v[r][m] = (VT)ldcg(x + m * N + c[r]);
+        });
+        double rr = 0.0;
 #pragma unroll
-      for (int r = 0; r < CPT; ++r) {
-        const Cell k = tile_cell(T, x0, y0, r);
-        if (!k.in) continue;
-        double ax[M];
-        op.matvec(tb, k.lx, k.ly, k.c, ax);
-        double res[M];
+        for (int r = 0; r < CPT; ++r) {
+          const Cell k = tile_cell(T, x0, y0, r);
+          if (!k.in) continue;
+          VT ax[M];
+          op.matvec(tb, k.lx, k.ly, k.c, ax);
+          VT res[M];
 #pragma unroll
-        for (int m = 0; m < M; ++m) res[m] = ldcg(b + m * N + k.c) - ax[m];
-        op.precond(k.c, res);
+          for (int m = 0; m < M; ++m) res[m] = (VT)(ldcg(b + m * N + k.c) - (double)ax[m]);
+          op.precond(k.c, res);
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
-          Vp(0)[m * N + k.c] = res[m];
-          rr += res[m] * res[m];
+          for (int m = 0; m < M; ++m) {
+            const double rv = (double)res[m];
+            Vp(0)[m * N + k.c] = (TS)rv;
+            rr += rv * rv;
+          }
         }
+        wacc_add(S.acc, 0, rr);
+        __syncthreads();
       }
-      wacc_add(S.acc, 0, rr);
-      __syncthreads();
-    }
-    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
-    if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    grid_reduce(part(), g.nblk, 1, S.red, S.acc);
-    ++phase;
-    count(3 * M + coef);
-    S.gam[0] = sqrt(S.red[0]);
-    if (outer == 0) tol_eff = g.tol * S.gam[0] + g.tol;
-    if (!isfinite(S.gam[0])) return GM_NONFINITE;
-    if (S.gam[0] <= tol_eff) {
-      if (lead) {
-        g.st->gmres_iters += iters;
-        g.st->last_residual = S.gam[0];
+      wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+      if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
+      grid_reduce(part(), g.nblk, 1, S.red, S.acc);
+      ++phase;
+      count(M, 2 * M + coef);
+      S.gam[0] = sqrt(S.red[0]);
+      if (outer == 0) tol_eff = g.tol * S.gam[0] + g.tol_abs;
+      if (!isfinite(S.gam[0])) return GM_NONFINITE;
+      if (S.gam[0] <= tol_eff) {
+        if (lead) {
+          g.st->gmres_iters += iters;
+          g.st->last_residual = S.gam[0];
+        }
+        return GM_CONVERGED;
       }
-      return GM_CONVERGED;
-    }
-    if (lead) g.st->gmres_restarts += 1;
-    S.sigma[0] = 1.0 / S.gam[0];
+      if (lead) g.st->gmres_restarts += 1;
+      S.sigma[0] = 1.0 / S.gam[0];
 
-    // ---- Av0 = M^-1 A V0 (unnormalised), H[0][0]
-    wacc_clear(S.acc);
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
-      const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+      // ---- Av0 = M^-1 A V0 (unnormalised), H[0][0]
+      wacc_clear(S.acc);
+      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
-        for (int r = 0; r < FQ; ++r)
+          for (int r = 0; r < FQ; ++r)
 #pragma unroll
-          for (int m = 0; m < M; ++m) v[r][m] = ldcg(Vp(0) + m * N + c[r]);
-      });
-      double va = 0.0;
+            for (int m = 0; m < M; ++m) v[r][m] = (VT)ldv(Vp(0) + m * N + c[r]);
+        });
+        double va = 0.0;
 #pragma unroll
-      for (int r = 0; r < CPT; ++r) {
-        const Cell k = tile_cell(T, x0, y0, r);
-        if (!k.in) continue;
-        double aw[M];
-        op.matvec(tb, k.lx, k.ly, k.c, aw);
-        op.precond(k.c, aw);
-        const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
+        for (int r = 0; r < CPT; ++r) {
+          const Cell k = tile_cell(T, x0, y0, r);
+          if (!k.in) continue;
+          VT aw[M];
+          op.matvec(tb, k.lx, k.ly, k.c, aw);
+          op.precond(k.c, aw);
+          const int o = (k.ly + Op::HALO) * TB::SX + k.lx + Op::HALO;
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
-          AVp(0)[m * N + k.c] = aw[m];
-          va += tb.s[m * TB::SN + o] * aw[m];
+          for (int m = 0; m < M; ++m) {
+            AVp(0)[m * N + k.c] = (TS)aw[m];
+            va += (double)tb.s[m * TB::SN + o] * (double)aw[m];
+          }
         }
+        wacc_add(S.acc, 0, va);
+        __syncthreads();
       }
-      wacc_add(S.acc, 0, va);
+      wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+      if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
+      grid_reduce(part(), g.nblk, 1, S.red, S.acc);
+      ++phase;
+      count(2 * M, coef);
+      for (int r = threadIdx.x; r < (KCAP + 2) * (KCAP + 2); r += NT) (&S.H[0][0])[r] = 0.0;
       __syncthreads();
-    }
-    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
-    if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    grid_reduce(part(), g.nblk, 1, S.red, S.acc);
-    ++phase;
-    count(2 * M + coef);
-    for (int r = threadIdx.x; r < (KCAP + 2) * (KCAP + 2); r += NT) (&S.H[0][0])[r] = 0.0;
-    __syncthreads();
-    if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[0];
-    __syncthreads();
+      if (threadIdx.x == 0) S.H[0][0] = S.sigma[0] * S.sigma[0] * S.red[0];
+      __syncthreads();
     }
 
     int jend = -1;  // last Arnoldi index used in the update
     bool converged = false;
     for (int j = 0; j < kmax; ++j) {
       // ---- fused pass: w = Av_j - sum_i H[i][j] v_i ; V_{j+1} = w ; AV_{j+1} = M^-1 A w ; dots
+      // (the combination is formed in FP64 whatever the storage type)
       wacc_clear(S.acc);
       const double sj = S.sigma[j];
       for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[M]) {
-          const double* AVj = AVp(j);
+        fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
+          const TS* AVj = AVp(j);
+          double wv[FQ][M];
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
 #pragma unroll
-            for (int m = 0; m < M; ++m) v[r][m] = sj * ldcg(AVj + m * N + c[r]);
+            for (int m = 0; m < M; ++m) wv[r][m] = sj * ldv(AVj + m * N + c[r]);
 #pragma unroll 2
           for (int i = 0; i <= j; ++i) {
             const double hij = S.H[i][j], si = S.sigma[i];
-            const double* Vi = Vp(i);
+            const TS* Vi = Vp(i);
 #pragma unroll
             for (int r = 0; r < FQ; ++r)
 #pragma unroll
-              for (int m = 0; m < M; ++m) v[r][m] = v[r][m] - hij * (si * ldcg(Vi + m * N + c[r]));
+              for (int m = 0; m < M; ++m) wv[r][m] = wv[r][m] - hij * (si * ldv(Vi + m * N + c[r]));
           }
+#pragma unroll
+          for (int r = 0; r < FQ; ++r)
+#pragma unroll
+            for (int m = 0; m < M; ++m) v[r][m] = (VT)wv[r][m];
         });
-        double aw[CPT][M], wc[CPT][M];
+        VT aw[CPT][M], wc[CPT][M];
         long long cc[CPT];
         bool in[CPT];
 #pragma unroll
@@ -784,12 +843,12 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
 #pragma unroll
             for (int m = 0; m < M; ++m) {
               wc[r][m] = tb.s[m * TB::SN + o];
-              Vp(j + 1)[m * N + k.c] = wc[r][m];
-              AVp(j + 1)[m * N + k.c] = aw[r][m];
+              Vp(j + 1)[m * N + k.c] = (TS)wc[r][m];
+              AVp(j + 1)[m * N + k.c] = (TS)aw[r][m];
             }
           } else {
 #pragma unroll
-            for (int m = 0; m < M; ++m) aw[r][m] = wc[r][m] = 0.0;
+            for (int m = 0; m < M; ++m) aw[r][m] = wc[r][m] = VT(0);
           }
         }
         // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2; four basis vectors at a time
@@ -802,7 +861,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
 #pragma unroll
               for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int m = 0; m < M; ++m) d[u] += ldcg(Vp(i + u) + m * N + cc[r]) * aw[r][m];
+                for (int m = 0; m < M; ++m) d[u] += ldv(Vp(i + u) + m * N + cc[r]) * (double)aw[r][m];
             }
           wacc_add4(S.acc, i, d);
         }
@@ -812,7 +871,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
           for (int r = 0; r < CPT; ++r)
             if (in[r]) {
 #pragma unroll
-              for (int m = 0; m < M; ++m) d += ldcg(Vp(i) + m * N + cc[r]) * aw[r][m];
+              for (int m = 0; m < M; ++m) d += ldv(Vp(i) + m * N + cc[r]) * (double)aw[r][m];
             }
           wacc_add(S.acc, i, d);
         }
@@ -821,8 +880,8 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
         for (int r = 0; r < CPT; ++r)
 #pragma unroll
           for (int m = 0; m < M; ++m) {
-            wa += wc[r][m] * aw[r][m];
-            ww += wc[r][m] * wc[r][m];
+            wa += (double)wc[r][m] * (double)aw[r][m];
+            ww += (double)wc[r][m] * (double)wc[r][m];
           }
         wacc_add(S.acc, j + 1, wa);
         wacc_add(S.acc, j + 2, ww);
@@ -833,7 +892,7 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       grid_reduce(part(), g.nblk, j + 3, S.red, S.acc);
       ++phase;
       ++iters;
-      count((j + 4) * M + coef);
+      count((j + 4) * M, coef);
       if (threadIdx.x == 0) {
         // H[j+1][j] = |w|; Givens on column j (implicit_operators.cpp:857-873)
         const double beta_w = sqrt(S.red[j + 2]);
@@ -876,26 +935,26 @@ __device__ int gmres_device(const Op& op, const GmresWork& g, double* x, const d
       }
     }
     __syncthreads();
-    if (converged && defer) {
+    if (defer && (converged || last_cycle)) {
       if (threadIdx.x == 0) S.nalpha = jend + 1;
       __syncthreads();
       if (lead) {
         g.st->gmres_iters += iters;
         g.st->last_residual = S.gam[jend + 1];
       }
-      return GM_CONVERGED;
+      return converged ? GM_CONVERGED : GM_MAXIT;
     }
     for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         double xv = from_zero ? 0.0 : ldcg(x + m * N + c);
-        for (int i = 0; i <= jend; ++i) xv = xv + S.alpha[i] * (S.sigma[i] * ldcg(Vp(i) + m * N + c));
+        for (int i = 0; i <= jend; ++i) xv = xv + S.alpha[i] * (S.sigma[i] * ldv(Vp(i) + m * N + c));
         x[m * N + c] = xv;
       }
     }
     x_written = true;
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
-    count((jend + (from_zero ? 2 : 3)) * M);
+    count((jend + 1) * M, (from_zero ? 1 : 2) * M);
     if (converged) {
       if (threadIdx.x == 0 && blockIdx.x == 0) {
         g.st->gmres_iters += iters;
@@ -939,6 +998,138 @@ __global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g
   record_status(g.st, code);
 }
 
+// ------------------------------------------------------------------ mixed-precision GMRES
+// The mixed form of GMRES_Solver: FP64 iterative refinement around FP32 inner solves.
+//   each sweep, one FP64 pass: x <- x + (pending inner update), s = b - A x and |M^-1 s|
+//     in FP64 arithmetic with FP64 coefficients; stop at |M^-1 s| <= GMREStol |r_0| + GMREStol,
+//     the stopping rule of the plain form, or when the FP64 residual has reached its rounding
+//     floor: an inner cycle met its tolerance and yet the true residual fell by less than half
+//     (the plain form tests the recursive GMRES estimate, which keeps falling below that floor);
+//   then one FP32 inner GMRES cycle on M^-1 A d = M^-1 s from d = 0 (operator and preconditioner
+//     in FP32, basis stored in FP32, Gram-Schmidt dots and the Hessenberg solve in FP64), stopped
+//     at a relative residual of g.tol or after g.kmax steps; its update sum_i alpha_i v_i is
+//     added to x inside the next FP64 pass.
+// x is double buffered between x and xalt (the FP64 pass reads the old iterate on the tile
+// halo); the result ends in x.
+template <class Op64>
+struct MixedSmem {
+  using Op32 = decltype(Op64().template as<float>());
+  GmresShared S;
+  union {
+    TileBuf<Op64> d;
+    TileBuf<Op32> f;
+  } tb;
+};
+
+template <class Op64>
+__global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
+    k_gmres_mixed(Op64 op, GmresWorkT<float> g, double* x, double* xalt, double* sres, const double* b,
+                  int max_sweeps, double tol) {
+  using Op32 = typename MixedSmem<Op64>::Op32;
+  using TB = TileBuf<Op64>;
+  constexpr int M = Op64::M, FQ = FillQ<Op64>;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  MixedSmem<Op64>& sm = *reinterpret_cast<MixedSmem<Op64>*>(dsm);
+  GmresShared& S = sm.S;
+  op.bind();
+  const Op32 op32 = op.template as<float>();
+  const Tiling& T = g.T;
+  const long long N = T.N;
+  unsigned phase = 0;
+  auto part = [&]() { return g.partial + (long long)(phase & 1) * g.nblk * NP; };
+  const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
+  const int coef = Op64::COEF + (op_uses_vdiag(op) ? 1 : 0);
+  if (lead) g.st->gmres_solves += 1;
+  double* x_cur = x;
+  double* x_nxt = xalt;
+  bool pending = false, inner_ok = false;
+  double tol_eff = 0.0, prev = INFINITY;
+  int code = GM_MAXIT;
+  for (int sweep = 0;; ++sweep) {
+    // ---- FP64: x += pending update; s = b - A x; |M^-1 s|^2
+    wacc_clear(S.acc);
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+      const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+      fill_tile(op, sm.tb.d, T, x0, y0, [&](const long long* c, double (*v)[M]) {
+#pragma unroll
+        for (int r = 0; r < FQ; ++r)
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            double xv = ldcg(x_cur + m * N + c[r]);
+            if (pending)
+              for (int i = 0; i < S.nalpha; ++i)
+                xv = xv + S.alpha[i] * (S.sigma[i] * ldv(g.V + (long long)i * M * N + m * N + c[r]));
+            v[r][m] = xv;
+          }
+      });
+      double rr = 0.0;
+#pragma unroll
+      for (int r = 0; r < CPT; ++r) {
+        const Cell k = tile_cell(T, x0, y0, r);
+        if (!k.in) continue;
+        double ax[M], res[M];
+        op.matvec(sm.tb.d, k.lx, k.ly, k.c, ax);
+        const int o = (k.ly + Op64::HALO) * TB::SX + k.lx + Op64::HALO;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          if (pending) x_nxt[m * N + k.c] = sm.tb.d.s[m * TB::SN + o];
+          res[m] = ldcg(b + m * N + k.c) - ax[m];
+          sres[m * N + k.c] = res[m];
+        }
+        op.precond(k.c, res);
+#pragma unroll
+        for (int m = 0; m < M; ++m) rr += res[m] * res[m];
+      }
+      wacc_add(S.acc, 0, rr);
+      __syncthreads();
+    }
+    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+    if (!grid_barrier(g.sync, g.nblk)) {
+      record_status(g.st, GM_SYNC);
+      return;
+    }
+    grid_reduce(part(), g.nblk, 1, S.red, S.acc);
+    ++phase;
+    if (lead)
+      g.st->alg_bytes[g.fam] += ((double)((pending ? 3 : 2) * M + M + coef) * 8.0 +
+                                 (pending ? (double)S.nalpha * M * sizeof(float) : 0.0)) * (double)N;
+    if (pending) {
+      double* t = x_cur;
+      x_cur = x_nxt;
+      x_nxt = t;
+      pending = false;
+    }
+    const double res = sqrt(S.red[0]);
+    if (sweep == 0) tol_eff = tol * res + tol;
+    if (!isfinite(res)) {
+      code = GM_NONFINITE;
+      break;
+    }
+    if (lead) g.st->last_residual = res;
+    if (res <= tol_eff || (inner_ok && res > 0.5 * prev)) {
+      code = GM_CONVERGED;
+      break;
+    }
+    prev = res;
+    if (sweep >= max_sweeps) break;
+    // ---- FP32 inner cycle on M^-1 A d = M^-1 s, update deferred
+    if (lead) g.st->refine_sweeps += 1;
+    bool written = false;
+    int c2 = gmres_device(op32, g, x_nxt, sres, S, sm.tb.f, phase, true, true, written);
+    if (c2 == GM_SYNC || c2 == GM_NONFINITE) {
+      record_status(g.st, c2);
+      return;
+    }
+    inner_ok = c2 == GM_CONVERGED;
+    pending = true;
+  }
+  // the result ends in x
+  if (x_cur != x)
+    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)gridDim.x * NT)
+      x[c] = ldcg(x_cur + c);
+  if (code != GM_CONVERGED) record_status(g.st, code);
+}
+
 // ------------------------------------------------------------------ nested Newton
 // Pressure_NestedNewton (implicit_operators.cpp:625-738) on the device.
 struct NewtonArgs {
@@ -947,12 +1138,28 @@ struct NewtonArgs {
   DevScalars* sc;
 };
 
-__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWork gw, NewtonArgs na) {
+// Shared memory of the nested Newton: the FP64 tile of the residual passes and the
+// tile of the Jacobian solves (FP64, or FP32 in the mixed form) share one buffer.
+template <class TS>
+struct NewtonSmem {
+  GmresShared S;
+  union {
+    TileBuf<PressureOp> l;
+    TileBuf<PressureOpT<TS>> j;
+  } tb;
+};
+
+// The Jacobian solves store their Krylov basis as TS and apply the operator in TS
+// arithmetic (double: the plain form; float: the mixed form).  The residual, the
+// Newton convergence test and the iterate stay FP64 in both.  Only the floored or
+// Redlich-Kwong case comes here; the linear case is a plain GMRES launch.
+template <class TS>
+__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
   op.bind();
   extern __shared__ __align__(16) unsigned char dsm[];
-  SolveSmem<PressureOp>& sm = *reinterpret_cast<SolveSmem<PressureOp>*>(dsm);
+  NewtonSmem<TS>& sm = *reinterpret_cast<NewtonSmem<TS>*>(dsm);
   GmresShared& S = sm.S;
-  TileBuf<PressureOp>& tb = sm.tb;
+  TileBuf<PressureOp>& tb = sm.tb.l;
   using TB = TileBuf<PressureOp>;
   const DevParams& P = op.P;
   const Tiling& T = gw.T;
@@ -961,16 +1168,6 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   auto part = [&]() { return gw.partial + (long long)(phase & 1) * gw.nblk * NP; };
   const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
 
-  if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS) {
-    // single linear GMRES with the carrier operator L (implicit_operators.cpp:664-668)
-    PressureOp L = op;
-    L.jac = 0;
-    if (lead) gw.st->gmres_solves += 1;
-    bool written = false;
-    int code = gmres_device(L, gw, na.p, na.b, S, tb, phase, false, false, written);
-    record_status(gw.st, code);
-    return;
-  }
   // ---- Cor. 1 slope Mbig (implicit_operators.cpp:670-686)
   double Mbig = na.sc->Mbig;
   if (P.floor_on) {
@@ -1021,8 +1218,9 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       gw.st->alg_bytes[gw.fam] += (P.eos_type != IMEX_IDEAL_GAS ? 2.0 : 1.0) * 8.0 * (double)N;
     }
   }
-  PressureOp L = op, J = op;
+  PressureOp L = op;
   L.jac = 0;
+  PressureOpT<TS> J = op.as<TS>();
   J.jac = 1;
   J.vdiag = na.vdiag;
   const double a = op.a;
@@ -1038,7 +1236,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   bool dp_live = false;  // dp holds the part of that update written by restart cycles
   auto pf_update = [&](long long c) {
     double d = dp_live ? ldcg(na.dp + c) : 0.0;
-    for (int i = 0; i < S.nalpha; ++i) d = d + S.alpha[i] * (S.sigma[i] * ldcg(gw.V + (long long)i * N + c));
+    for (int i = 0; i < S.nalpha; ++i) d = d + S.alpha[i] * (S.sigma[i] * ldv(gw.V + (long long)i * N + c));
     return ldcg(pf_cur + c) + d;
   };
   int it;
@@ -1083,7 +1281,8 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
     ++phase;
     if (lead)
       gw.st->alg_bytes[gw.fam] +=
-          (double)(PressureOp::COEF + 4 + (pending ? 1 + S.nalpha + (dp_live ? 1 : 0) : 0)) * 8.0 * (double)N;
+          ((double)(PressureOp::COEF + 4 + (pending ? 1 + (dp_live ? 1 : 0) : 0)) * 8.0 +
+           (pending ? (double)S.nalpha * sizeof(TS) : 0.0)) * (double)N;
     if (pending) {
       double* t = pf_cur;
       pf_cur = pf_nxt;
@@ -1102,7 +1301,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       gw.st->gmres_solves += 1;
       gw.st->newton_iters += 1;
     }
-    int code = gmres_device(J, gw, na.dp, na.g, S, tb, phase, true, true, dp_live);
+    int code = gmres_device(J, gw, na.dp, na.g, S, sm.tb.j, phase, true, true, dp_live);
     if (code != GM_CONVERGED) {
       record_status(gw.st, code);
       if (code == GM_SYNC || code == GM_NONFINITE) return;
@@ -1110,7 +1309,9 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
     pending = true;
   }
   if (it == P.Pnewton_max && lead) atomicMax(&gw.st->status, (int)IMEX_NEWTON_MAXIT);
-  if (lead) gw.st->alg_bytes[gw.fam] += (double)(2 + (pending ? S.nalpha + (dp_live ? 1 : 0) : 0)) * 8.0 * (double)N;
+  if (lead)
+    gw.st->alg_bytes[gw.fam] += ((double)(2 + (pending && dp_live ? 1 : 0)) * 8.0 +
+                                 (pending ? (double)S.nalpha * sizeof(TS) : 0.0)) * (double)N;
   // ---- p = pf (+ an update still pending after Pnewton_max), floored-cell count and min p
   // (implicit_operators.cpp:722-737)
   double st2[2] = {0.0, INFINITY};
@@ -1493,10 +1694,9 @@ __global__ void k_barrier_selftest(SyncState* sync, unsigned phantom, int iters,
 
 namespace {
 
-template <class Op>
-int coop_blocks(imex_ctx* ctx, const void* kernel, const Tiling& T) {
+// CTAs of a cooperative launch of `kernel` with `smem` bytes of dynamic shared memory
+int coop_blocks_smem(imex_ctx* ctx, const void* kernel, const Tiling& T, size_t smem) {
   int per_sm = 0;
-  const size_t smem = sizeof(SolveSmem<Op>);
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1506,6 +1706,10 @@ int coop_blocks(imex_ctx* ctx, const void* kernel, const Tiling& T) {
   if (nb > ctx->max_blocks) nb = ctx->max_blocks;
   if (nb < 1) nb = 1;
   return nb;
+}
+template <class Op>
+int coop_blocks(imex_ctx* ctx, const void* kernel, const Tiling& T) {
+  return coop_blocks_smem(ctx, kernel, T, sizeof(SolveSmem<Op>));
 }
 
 GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
@@ -1522,8 +1726,33 @@ GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
                                                    : (int)(dim3x > 2000000000LL ? 2000000000LL : dim3x);
   g.nblk = nblk;
   g.tol = ctx->P.GMREStol;
+  g.tol_abs = ctx->P.GMREStol;
   g.T = T;
   return g;
+}
+// FP32 Krylov workspace of the mixed form; inner solves stop at a relative residual of
+// mixed_inner_tol (plus `tol_abs`), after at most `max_restarts` cycles
+GmresWorkT<float> make_work_mixed(imex_ctx* ctx, const Tiling& T, int nblk, int fam, int max_restarts,
+                                  double tol_abs) {
+  const GmresWork d = make_work(ctx, T, nblk, fam);
+  GmresWorkT<float> g{};
+  g.V = ctx->Vf;
+  g.AV = ctx->AVf;
+  g.partial = d.partial;
+  g.sync = d.sync;
+  g.st = d.st;
+  g.kmax = d.kmax;
+  g.max_restarts = max_restarts;
+  g.nblk = nblk;
+  g.fam = fam;
+  g.tol = ctx->cfg.mixed_inner_tol;
+  g.tol_abs = tol_abs;
+  g.T = T;
+  return g;
+}
+// whether solves of the given kind (IMEX_MIXED_*) take the mixed form
+bool mixed(const imex_ctx* ctx, int kind) {
+  return ctx->cfg.precision == IMEX_PRECISION_MIXED && (ctx->cfg.mixed_solves & kind) != 0;
 }
 
 }  // namespace
@@ -1545,14 +1774,17 @@ imex_status reset_sync(imex_ctx* ctx) {
   return cuda_check(ctx, cudaGetLastError(), "sync reset");
 }
 
-template <class Op, class K, class... Args>
-imex_status launch_coop(imex_ctx* ctx, K kernel, int nblk, Args... args) {
+template <class K, class... Args>
+imex_status launch_coop_smem(imex_ctx* ctx, K kernel, int nblk, size_t smem, Args... args) {
   imex_status s = reset_sync(ctx);
   if (s != IMEX_OK) return s;
   void* params[] = {(void*)&args...};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(nblk), dim3(NT), params,
-                                              sizeof(SolveSmem<Op>), ctx->stream);
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(nblk), dim3(NT), params, smem, ctx->stream);
   return cuda_check(ctx, e, "cooperative launch");
+}
+template <class Op, class K, class... Args>
+imex_status launch_coop(imex_ctx* ctx, K kernel, int nblk, Args... args) {
+  return launch_coop_smem(ctx, kernel, nblk, sizeof(SolveSmem<Op>), args...);
 }
 
 PressureOp make_pressure_op(imex_ctx* ctx) {
@@ -1608,36 +1840,40 @@ imex_status pressure_setup(imex_ctx* ctx) {
   return launch_shock(ctx, ctx->Qe, ctx->eta);
 }
 
+// One GMRES solve with operator o: the plain FP64 kernel, or in the mixed form the FP64
+// refinement kernel around FP32 inner cycles.
+template <class Op>
+imex_status gmres_run(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, int kind) {
+  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  if (!mixed(ctx, kind)) {
+    auto kern = k_gmres<Op>;
+    const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
+    GmresWork g = make_work(ctx, T, nb, fam);
+    prof_begin(ctx);
+    imex_status s = launch_coop<Op>(ctx, kern, nb, o, g, x, b);
+    prof_end(ctx, fam, 0.0, 1);
+    return s;
+  }
+  auto kern = k_gmres_mixed<Op>;
+  const size_t smem = sizeof(MixedSmem<Op>);
+  const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
+  GmresWorkT<float> g = make_work_mixed(ctx, T, nb, fam, 1, 0.0);
+  prof_begin(ctx);
+  imex_status s = launch_coop_smem(ctx, kern, nb, smem, o, g, x, ctx->mcor, ctx->mres, b, ctx->cfg.mixed_max_refine,
+                                   ctx->P.GMREStol);
+  prof_end(ctx, fam, 0.0, 1);
+  return s;
+}
+
 imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
-  Tiling T = make_tiling(ctx->nx, ctx->ny);
   if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
     PressureOp o = make_pressure_op(ctx);
     o.jac = op == IMEX_OP_PRESSURE_J;
-    auto kern = k_gmres<PressureOp>;
-    int nb = coop_blocks<PressureOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb, F_GMRES_PRES);
-    prof_begin(ctx);
-    imex_status s = launch_coop<PressureOp>(ctx, kern, nb, o, g, x, b);
-    prof_end(ctx, F_GMRES_PRES, 0.0, 1);
-    return s;
+    return gmres_run(ctx, o, F_GMRES_PRES, x, b, IMEX_MIXED_PRESSURE);
   } else if (op == IMEX_OP_MAGNETIC_B) {
-    MagneticBOp o = make_magB_op(ctx);
-    auto kern = k_gmres<MagneticBOp>;
-    int nb = coop_blocks<MagneticBOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb, F_GMRES_MAG_B);
-    prof_begin(ctx);
-    imex_status s = launch_coop<MagneticBOp>(ctx, kern, nb, o, g, x, b);
-    prof_end(ctx, F_GMRES_MAG_B, 0.0, 1);
-    return s;
+    return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC);
   } else if (op == IMEX_OP_MAGNETIC_A) {
-    MagneticAOp o = make_magA_op(ctx);
-    auto kern = k_gmres<MagneticAOp>;
-    int nb = coop_blocks<MagneticAOp>(ctx, (const void*)kern, T);
-    GmresWork g = make_work(ctx, T, nb, F_GMRES_MAG_A);
-    prof_begin(ctx);
-    imex_status s = launch_coop<MagneticAOp>(ctx, kern, nb, o, g, x, b);
-    prof_end(ctx, F_GMRES_MAG_A, 0.0, 1);
-    return s;
+    return gmres_run(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, IMEX_MIXED_MAGNETIC);
   }
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
 }
@@ -1707,11 +1943,11 @@ imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, con
 }
 
 imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
-  Tiling T = make_tiling(ctx->nx, ctx->ny);
+  const DevParams& P = ctx->P;
   PressureOp o = make_pressure_op(ctx);
-  auto kern = k_nested_newton;
-  int nb = coop_blocks<PressureOp>(ctx, (const void*)kern, T);
-  GmresWork g = make_work(ctx, T, nb, F_NEWTON);
+  if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS)  // a single linear GMRES with L (implicit_operators.cpp:664-668)
+    return gmres_run(ctx, o, F_NEWTON, p, b, IMEX_MIXED_PRESSURE);
+  const Tiling T = make_tiling(ctx->nx, ctx->ny);
   NewtonArgs na{};
   na.p = p;
   na.pf = ctx->pf;
@@ -1720,8 +1956,22 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   na.vdiag = ctx->vdiag;
   na.b = b;
   na.sc = ctx->sc;
+  imex_status s;
   prof_begin(ctx);
-  imex_status s = launch_coop<PressureOp>(ctx, kern, nb, o, g, na);
+  if (!mixed(ctx, IMEX_MIXED_PRESSURE)) {
+    auto kern = k_nested_newton<double>;
+    const size_t smem = sizeof(NewtonSmem<double>);
+    const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
+    GmresWork g = make_work(ctx, T, nb, F_NEWTON);
+    s = launch_coop_smem(ctx, kern, nb, smem, o, g, na);
+  } else {
+    auto kern = k_nested_newton<float>;
+    const size_t smem = sizeof(NewtonSmem<float>);
+    const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
+    GmresWorkT<float> g = make_work_mixed(ctx, T, nb, F_NEWTON, make_work(ctx, T, nb, F_NEWTON).max_restarts,
+                                          ctx->P.GMREStol);
+    s = launch_coop_smem(ctx, kern, nb, smem, o, g, na);
+  }
   prof_end(ctx, F_NEWTON, 0.0, 1);
   return s;
 }

@@ -71,8 +71,17 @@ typedef enum { IMEX_IDEAL_GAS = 0, IMEX_REDLICH_KWONG = 1 } imex_eos_type;
 /* Arithmetic of the implicit solves. */
 typedef enum {
   IMEX_PRECISION_FP64 = 0,  /* everything in FP64 (the plain form) */
-  IMEX_PRECISION_MIXED = 1  /* FP32 operator + Krylov vectors inside FP64 iterative refinement */
+  IMEX_PRECISION_MIXED = 1  /* FP32 operator + Krylov vectors inside FP64 iterative refinement: every
+                               GMRES solve refines in FP64 around FP32 inner cycles; the nested
+                               Newton keeps its FP64 residual and convergence test and solves its
+                               Jacobian systems in FP32 */
 } imex_precision;
+/* Solves of the mixed form (imex_config.mixed_solves).  The pressure solves (the nested
+ * Newton's Jacobian systems, or the single linear GMRES without the floor) gain from FP32:
+ * the Newton iteration is their FP64 refinement.  The magnetic systems converge in a few
+ * FP64 GMRES steps on the smooth fields of a stage; FP32 rounding noise then costs several
+ * refinement sweeps, so they stay FP64 unless IMEX_MIXED_MAGNETIC is set. */
+enum { IMEX_MIXED_PRESSURE = 1, IMEX_MIXED_MAGNETIC = 2 };
 
 /* Run-time form of the reference's compile-time configuration
  * (include/config.hpp:43-125 and the per-test settings of main.cpp:9-224).
@@ -114,6 +123,7 @@ typedef struct imex_config {
   int precision;          /* imex_precision */
   double mixed_inner_tol; /* relative tolerance of each FP32 inner solve in mixed mode */
   int mixed_max_refine;   /* cap on FP64 refinement sweeps in mixed mode */
+  int mixed_solves;       /* which solves take the mixed form: IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC */
 } imex_config;
 
 /* Scalars that the reference keeps in hidden globals and that one stage consumes
@@ -245,7 +255,8 @@ imex_status imex_gmres(imex_ctx* ctx, int op, double* x, const double* b, imex_s
  * basis, the AV ring, the per-CTA partial sums, the barrier state and the staged
  * host vectors all live in one fixed device array of IMEX_NOALLOC_SCRATCH_BYTES
  * (16 MiB) per device; no cudaMalloc, cudaFree or other allocating call is made.
- * Same kernel, same arithmetic and same results as imex_gmres.
+ * Same kernel, same arithmetic and same results as imex_gmres in the FP64 form
+ * (it always solves in FP64, whatever the context's precision).
  *
  * Limit: the solve needs about (gmres_restart + 3) x unknowns x 8 bytes, plus
  * 2 x unknowns x 8 bytes when x or b are host pointers.  For restart 25 that is
