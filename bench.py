@@ -41,6 +41,8 @@ METRIC = "cell-updates/s per IMEX stage"
 CFG1 = dict(recon="WENO5", magfield="PotentialA", floor_on=1, p_floor=1e-8, theta=0.5,
             GMREStol=1e-14, CFL=0.8)
 CFG0 = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12, CFL=0.8)
+CFG2 = dict(recon="Minmod", magfield="StaggerCT", floor_on=1, eos_type="REDLICH_KWONG", m_alfa=0.4275,
+            m_b=0.0866, CFL=0.8)
 WORKLOADS = {
     "vortex_sheet_1024": dict(problem="vortex_sheet", n=1024, rks=3, settings=CFG1,
                               desc="vortex-sheet MHD 1024^2, WENO5, A-form CT, floor on, RK3"),
@@ -48,12 +50,17 @@ WORKLOADS = {
                               desc="vortex-sheet MHD 2048^2, WENO5, A-form CT, floor on, RK3"),
     "vortex_64": dict(problem="vortex", n=64, rks=2, settings=CFG0,
                       desc="smooth MHD vortex 64^2, VanLeer, staggered CT, RK2"),
+    "random_field_2048": dict(problem="random_field", n=2048, rks=2, settings=CFG2,
+                              desc="seeded low-Mach random field 2048^2 (seed 2026, beta 0.1), Redlich-Kwong, "
+                                   "Minmod, EMF-consistent staggered CT, floor on, RK2"),
 }
 REF_SAMPLE_N = 256
 
 
 def make_problem(kind: str, n: int):
-    from imex_b200.problems import vortex, vortex_sheet
+    from imex_b200.problems import random_field, vortex, vortex_sheet
+    if kind == "random_field":
+        return random_field(n)
     return vortex(n) if kind == "vortex" else vortex_sheet(n)
 
 

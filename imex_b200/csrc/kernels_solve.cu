@@ -1003,8 +1003,9 @@ __global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g
 //   each sweep, one FP64 pass: x <- x + (pending inner update), s = b - A x and |M^-1 s|
 //     in FP64 arithmetic with FP64 coefficients; stop at |M^-1 s| <= GMREStol |r_0| + GMREStol,
 //     the stopping rule of the plain form, or when the FP64 residual has reached its rounding
-//     floor: an inner cycle met its tolerance and yet the true residual fell by less than half
-//     (the plain form tests the recursive GMRES estimate, which keeps falling below that floor);
+//     floor: an inner cycle met its tolerance and yet the true residual fell by less than half,
+//     or two sweeps in a row fell by less than half (the plain form tests the recursive GMRES
+//     estimate, which keeps falling below that floor);
 //   then one FP32 inner GMRES cycle on M^-1 A d = M^-1 s from d = 0 (operator and preconditioner
 //     in FP32, basis stored in FP32, Gram-Schmidt dots and the Hessenberg solve in FP64), stopped
 //     at a relative residual of g.tol or after g.kmax steps; its update sum_i alpha_i v_i is
@@ -1043,6 +1044,7 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
   double* x_cur = x;
   double* x_nxt = xalt;
   bool pending = false, inner_ok = false;
+  int stalls = 0;
   double tol_eff = 0.0, prev = INFINITY;
   int code = GM_MAXIT;
   for (int sweep = 0;; ++sweep) {
@@ -1106,7 +1108,8 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
       break;
     }
     if (lead) g.st->last_residual = res;
-    if (res <= tol_eff || (inner_ok && res > 0.5 * prev)) {
+    stalls = res > 0.5 * prev ? stalls + 1 : 0;
+    if (res <= tol_eff || (inner_ok && res > 0.5 * prev) || stalls >= 2) {
       code = GM_CONVERGED;
       break;
     }

@@ -15,7 +15,9 @@ Formulas follow the reference's initial conditions:
     (1,1) and the kappa/mu amplitudes of the vortex workload;
   * vortex sheet: the Orszag-Tang field of initial_conditions.cpp:426-435 in
     [0, 2*pi]^2 form, faces = average of neighbouring cell B as in
-    initial_conditions.cpp:720-726, A_z = cos y + cos(2x)/2.
+    initial_conditions.cpp:720-726, A_z = cos y + cos(2x)/2;
+  * random field: seeded low-Mach, magnetic-pressure-dominated Redlich-Kwong gas on
+    the unit square (random Fourier sums; faces from a corner A_z as for the vortex).
 """
 from __future__ import annotations
 
@@ -113,3 +115,79 @@ def vortex_sheet(n: int = 1024, ny: int | None = None, gamma: float = 5.0 / 3.0)
     A[2] = np.cos(Y) + 0.5 * np.cos(2.0 * X)
     return Problem("vortex_sheet", nx, ny, x0, x1, y0, y1, prim, bx, by, A,
                    settings=dict(gamma=gamma, vortex_test=0))
+
+
+class _FourierModes:
+    """Random Fourier sum f(x, y) = sum_{0<|k|<=kmax} a_k |k|^-2 cos(2 pi k.x + phi_k)
+    on the unit square, a_k ~ N(0, 1), phi_k ~ U[0, 2 pi).  Evaluated separably as
+    Re(Ey^T C Ex) with C[ky, kx] = a_k |k|^-2 e^{i phi_k}; derivatives scale C by 2 pi i k."""
+
+    def __init__(self, rng: np.random.Generator, kmax: int):
+        n = 2 * kmax + 1
+        self.kmax = kmax
+        self.C = np.zeros((n, n), dtype=np.complex128)
+        for ky in range(-kmax, kmax + 1):
+            for kx in range(-kmax, kmax + 1):
+                k2 = kx * kx + ky * ky
+                if k2 == 0 or k2 > kmax * kmax:
+                    continue
+                a = rng.standard_normal()
+                phi = rng.uniform(0.0, 2.0 * math.pi)
+                self.C[ky + kmax, kx + kmax] = a / k2 * np.exp(1j * phi)
+
+    def eval(self, x: np.ndarray, y: np.ndarray, dx: int = 0, dy: int = 0) -> np.ndarray:
+        """f (or its derivative d^dx/dx^dx d^dy/dy^dy) on the grid y[:, None], x[None, :]."""
+        k = np.arange(-self.kmax, self.kmax + 1)
+        C = self.C * (2j * math.pi * k[None, :]) ** dx * (2j * math.pi * k[:, None]) ** dy
+        Ex = np.exp(2j * math.pi * k[:, None] * x[None, :])
+        Ey = np.exp(2j * math.pi * k[:, None] * y[None, :])
+        return np.real(Ey.T @ C @ Ex)
+
+
+def random_field(n: int = 2048, seed: int = 2026, p0: float = 1.0, mach: float = 1e-3, beta: float = 0.1,
+                 kmax: int = 8, gamma: float = 5.0 / 3.0, m_alfa: float = 0.4275, m_b: float = 0.0866) -> Problem:
+    """Low-Mach, magnetic-pressure-dominated random field on the periodic unit square,
+    Redlich-Kwong gas.  From the seed: rho = 1 + 0.1 f1 and p = p0 (1 + 0.05 f2), with
+    f1, f2 random Fourier sums normalised to max |f| = 1; v = curl(psi) of a random
+    streamfunction scaled to max |v| = mach * sqrt(gamma p0 / rho0) (the ideal-gas sound
+    speed at the mean state is the Mach reference); B from a random vector potential A_z
+    on cell corners (faces = its exact differences, so div B = 0 to round-off; cell B =
+    face average), scaled to beta = 2 p0 / max|B|^2.  The modes are drawn in a fixed order
+    (f1, f2, psi, A_z) from numpy's default generator with this seed.
+
+    The default beta is 0.1 (magnetic pressure ten times the gas pressure): with the
+    Redlich-Kwong gas the reference scheme itself turns the state non-finite within two
+    steps at beta <= 0.03 on this field, so stronger fields have no reference result to
+    match."""
+    rng = np.random.default_rng(seed)
+    f1, f2, psi, az = (_FourierModes(rng, kmax) for _ in range(4))
+    nx = ny = n
+    h = 1.0 / n
+    xc = (np.arange(n) + 0.5) * h
+    xf = (np.arange(n) + 1.0) * h  # corners (i+1/2, j+1/2)
+    prim = np.zeros((8, ny, nx))
+    g1 = f1.eval(xc, xc)
+    g2 = f2.eval(xc, xc)
+    prim[0] = 1.0 + 0.1 * g1 / np.abs(g1).max()
+    prim[4] = p0 * (1.0 + 0.05 * g2 / np.abs(g2).max())
+    vx = psi.eval(xc, xc, dy=1)
+    vy = -psi.eval(xc, xc, dx=1)
+    vmax = np.sqrt(vx * vx + vy * vy).max()
+    vscale = mach * math.sqrt(gamma * p0 / 1.0) / vmax
+    prim[1] = vx * vscale
+    prim[2] = vy * vscale
+    a_corner = az.eval(xf, xf)
+    bx = (a_corner - np.roll(a_corner, 1, axis=0)) / h
+    by = -(a_corner - np.roll(a_corner, 1, axis=1)) / h
+    cbx = 0.5 * (np.roll(bx, 1, axis=1) + bx)
+    cby = 0.5 * (np.roll(by, 1, axis=0) + by)
+    bscale = math.sqrt(2.0 * p0 / beta) / np.sqrt(cbx * cbx + cby * cby).max()
+    bx *= bscale
+    by *= bscale
+    prim[5] = cbx * bscale
+    prim[6] = cby * bscale
+    A = np.zeros((3, ny, nx))
+    A[2] = az.eval(xc, xc) * bscale
+    return Problem("random_field", nx, ny, 0.0, 1.0, 0.0, 1.0, prim, np.ascontiguousarray(bx),
+                   np.ascontiguousarray(by), A,
+                   settings=dict(gamma=gamma, vortex_test=0, eos_type="REDLICH_KWONG", m_alfa=m_alfa, m_b=m_b))

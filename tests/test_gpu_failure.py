@@ -69,3 +69,18 @@ def test_barrier_wait_times_out_and_reports_sync_error():
     dt = sv.step()                          # the solver still works afterwards
     assert dt > 0 and sv.divergence()["face_l2"] < 1e-12
     sv.close()
+
+
+def test_strong_field_redlich_kwong_is_reported_like_the_reference_fails():
+    """At beta = 1e-4 the reference scheme itself goes non-finite within two steps on the
+    Redlich-Kwong random field; the GPU path must report that as a status, not carry on."""
+    from imex_b200.problems import random_field
+    prob = random_field(32, beta=1e-4)
+    settings = dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866)
+    sv = ix.Solver.for_problem(prob, 2, settings)
+    with pytest.raises(ix.ImexError) as err:
+        for _ in range(2):
+            sv.step()
+    assert err.value.status in (5, 6, 7, 9)  # Newton cap, non-finite, positivity or EOS iteration cap
+    sv.scalars()  # the context still answers after the error
+    sv.close()

@@ -10,7 +10,7 @@ import pytest
 
 import imex_b200 as ix
 from conftest import rel
-from imex_b200.problems import vortex, vortex_sheet
+from imex_b200.problems import random_field, vortex, vortex_sheet
 from oracle.bindings import make_solver
 
 pytestmark = pytest.mark.gpu
@@ -25,6 +25,8 @@ CASES = [
     ("vortex_nofloor", lambda: vortex(40, 36), 2, dict(recon="Minmod", magfield="UnStaggerCT", floor_on=0), 4),
     ("vortex_rkeos", lambda: vortex(32), 2,
      dict(recon="VanLeer", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 3),
+    ("random_field", lambda: random_field(48), 2,
+     dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 4),
 ]
 
 

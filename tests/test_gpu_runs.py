@@ -102,3 +102,36 @@ def test_staggered_ct_keeps_face_divergence_at_roundoff_large():
         assert gpu.divergence()["face_l2"] <= 1e-12
         assert gpu.min_pressure() > 0.0
     gpu.close()
+
+
+def test_random_field_redlich_kwong_matches_oracle():
+    """Seeded low-Mach random field (Redlich-Kwong gas, beta 0.1) at 48^2, RK2.
+
+    Before each step the GPU gets the oracle's state (the primitive state a reference step
+    starts from, main.cpp:356-358), so the comparison after the step is the error of that
+    one step.  On this field the reference's own result moves by ~5e-10 over 5 steps when
+    only its GMRES tolerance changes (1e-14 -> 1e-16, see test_oracle.py), so two correct
+    implementations that sum in different orders differ at that level: each step is held
+    to 1e-9 and the free-running comparison after 6 steps to 5e-9."""
+    from imex_b200.problems import random_field
+    prob = random_field(48)
+    settings = dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866)
+    gpu = ix.Solver.for_problem(prob, 2, settings)
+    free = ix.Solver.for_problem(prob, 2, settings)
+    cpu = make_solver("port", prob, 2, settings)
+    for _ in range(6):
+        bx, by = cpu.faces()
+        gpu.upload_state(cpu.prim(), bx, by, cpu.vector_potential())
+        dt_c = cpu.step()
+        assert gpu.step() == pytest.approx(dt_c, rel=1e-12)
+        free.step()
+        a, b = gpu.cons(), cpu.cons()
+        for k in range(8):
+            assert rel(a[k], b[k]) <= 1e-9, k
+        assert gpu.divergence()["face_l2"] <= 1e-12
+        assert gpu.min_pressure() > 0.0
+    a, b = free.cons(), cpu.cons()
+    for k in range(8):
+        assert rel(a[k], b[k]) <= 5e-9, k
+    gpu.close()
+    free.close()

@@ -115,3 +115,39 @@ def test_port_rejects_unsupported_configurations():
         make_solver("port", prob, 2, dict(formula="EnergyFormula"))
     with pytest.raises(RuntimeError):
         make_solver("port", prob, 2, dict(GLF=0))
+
+
+RK_RANDOM = dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866)
+
+
+def test_strong_field_redlich_kwong_is_not_finite_in_the_reference():
+    """The reference scheme (its C restatement, bit-identical to it) turns the Redlich-Kwong
+    random field non-finite within two steps at beta = 1e-4, and stays finite at beta = 0.1."""
+    from imex_b200.problems import random_field
+    bad = make_solver("port", random_field(32, beta=1e-4), 2, RK_RANDOM)
+    finite = True
+    for _ in range(2):
+        bad.step()
+        finite = finite and bool(np.isfinite(bad.cons()).all())
+    assert not finite
+    good = make_solver("port", random_field(32), 2, RK_RANDOM)
+    for _ in range(4):
+        good.step()
+    assert np.isfinite(good.cons()).all()
+
+
+def test_random_field_reference_is_sensitive_to_its_gmres_tolerance():
+    """On the random field the magnetic systems are stiff (about a hundred GMRES steps per
+    solve): the reference's own result moves by ~1e-10 when only GMREStol changes from
+    1e-14 to 1e-16.  This is the noise floor of any comparison between two correct
+    implementations that sum in different orders on this workload."""
+    from imex_b200.problems import random_field
+    p = random_field(48)
+    runs = []
+    for tol in (1e-14, 1e-16):
+        o = make_solver("port", p, 2, dict(RK_RANDOM, GMREStol=tol))
+        for _ in range(5):
+            o.step()
+        runs.append(o.cons())
+    worst = max(rel(runs[0][k], runs[1][k]) for k in range(8))
+    assert 1e-11 < worst < 5e-9

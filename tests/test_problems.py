@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import numpy as np
+import pytest
 
 from imex_b200.problems import vortex, vortex_sheet
 
@@ -40,3 +41,23 @@ def test_rectangular_grids():
     p = vortex(17, 23)
     assert p.prim.shape == (8, 23, 17) and p.bx.shape == (23, 17)
     assert np.max(np.abs(face_div(p))) < 1e-12
+
+
+def test_random_field_is_seeded_divergence_free_and_scaled():
+    from imex_b200.problems import random_field
+    a = random_field(64, seed=5)
+    b = random_field(64, seed=5)
+    c = random_field(64, seed=6)
+    np.testing.assert_array_equal(a.prim, b.prim)
+    assert not np.array_equal(a.prim, c.prim)
+    h = 1.0 / 64
+    div = (a.bx - np.roll(a.bx, 1, axis=1)) / h + (a.by - np.roll(a.by, 1, axis=0)) / h
+    assert np.abs(div).max() <= 1e-12 * np.abs(a.bx).max() / h
+    rho, p = a.prim[0], a.prim[4]
+    assert abs(np.abs(rho - 1.0).max() - 0.1) < 1e-12
+    assert abs(np.abs(p - 1.0).max() - 0.05) < 1e-12
+    vmax = np.sqrt(a.prim[1] ** 2 + a.prim[2] ** 2).max()
+    assert vmax == pytest.approx(1e-3 * np.sqrt(5.0 / 3.0), rel=1e-12)
+    bmax2 = (a.prim[5] ** 2 + a.prim[6] ** 2).max()
+    assert 2.0 / bmax2 == pytest.approx(0.1, rel=1e-12)
+    assert a.settings["eos_type"] == "REDLICH_KWONG"
