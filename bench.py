@@ -73,12 +73,16 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def ncu_traffic(family: str) -> float | None:
-    """Per-launch DRAM bytes of `family` at this workload from the committed ncu summary."""
+def ncu_traffic(family: str, workload: str, n: int) -> float | None:
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of `family`
+    from the committed ncu summary, when it was captured on this workload and grid."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
-            return float(json.load(f)[family]["dram_bytes_per_launch"])
+            d = json.load(f)
+        if d["workload"] != workload or int(d["n"]) != n:
+            return None
+        return float(d["families"][family]["dram_bytes_per_launch"])
     except Exception:
         return None
 
@@ -284,7 +288,7 @@ def main() -> int:
     peak, peak_kind = measured_peaks()
     dom = max(prof, key=lambda r: r["total_ms"])
     achieved = dom["alg_bytes"] / (dom["total_ms"] / 1e3) / 1e9
-    traffic = ncu_traffic(dom["name"])
+    traffic = ncu_traffic(dom["name"], args.workload, prob.nx)
     total_prof_ms = sum(r["total_ms"] for r in prof)
     roofline = {"kernel": dom["name"], "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak,
