@@ -88,6 +88,10 @@ class SolveStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double)]
+
+
 class KernelProfile(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double),
                 ("alg_bytes", C.c_double)]
@@ -133,6 +137,15 @@ _SIGS = {
     "imex_apply_operator": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "imex_gmres": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
     "imex_gmres_noalloc": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
+    "imex_batch_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_void_p)]),
+    "imex_batch_destroy": (C.c_int, [C.c_void_p]),
+    "imex_batch_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "imex_batch_configure": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "imex_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "imex_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(BatchTuning)]),
+    "imex_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "imex_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "imex_pressure_nested_newton": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(SolveStats)]),
     "imex_shock_detector": (C.c_int, [C.c_void_p, _D, _D]),
     "imex_get_stats": (C.c_int, [C.c_void_p, C.POINTER(SolveStats)]),
@@ -229,9 +242,17 @@ class Solver:
         sv.load(prob)
         return sv
 
+    @classmethod
+    def _view(cls, lib, ctx, nx: int, ny: int) -> "Solver":
+        """A Solver on a context owned elsewhere (an ensemble member); close() leaves it alive."""
+        sv = cls.__new__(cls)
+        sv.lib, sv.ctx, sv.nx, sv.ny, sv.N, sv._owns = lib, ctx, nx, ny, nx * ny, False
+        return sv
+
     def close(self) -> None:
         if getattr(self, "ctx", None):
-            self.lib.imex_destroy(self.ctx)
+            if getattr(self, "_owns", True):
+                self.lib.imex_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):
@@ -455,3 +476,69 @@ class Solver:
         v = C.c_double()
         self._check(self.lib.imex_min_pressure(self.ctx, C.byref(v)))
         return v.value
+
+
+class Batch:
+    """An ensemble (imex_batch): independent runs of one configuration on uneven grids,
+    advanced together.  ``members[m]`` is a Solver view on member m's context (state I/O
+    and diagnostics); the batch owns the members."""
+
+    def __init__(self, problems, rks: int, settings: dict | None = None, streams: int = 8, graph: bool = True):
+        self.lib = load_library()
+        p0 = problems[0]
+        s = dict(p0.settings)
+        s.update(settings or {})
+        self.cfg = make_config(s, (p0.x0, p0.x1, p0.y0, p0.y1), rks)
+        n = len(problems)
+        nx = (C.c_int * n)(*[p.nx for p in problems])
+        ny = (C.c_int * n)(*[p.ny for p in problems])
+        h = C.c_void_p()
+        rc = self.lib.imex_batch_create(C.byref(self.cfg), n, nx, ny, C.byref(h))
+        if rc != 0:
+            raise ImexError(rc, "imex_batch_create failed")
+        self.b = h
+        self.members = []
+        for m, p in enumerate(problems):
+            c = C.c_void_p()
+            self._check(self.lib.imex_batch_member(self.b, m, C.byref(c)))
+            sv = Solver._view(self.lib, c, p.nx, p.ny)
+            sv.load(p)
+            self.members.append(sv)
+        if streams != 8 or not graph:
+            self._check(self.lib.imex_batch_configure(self.b, streams, 1 if graph else 0))
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            msg = self.lib.imex_batch_last_error(self.b)
+            raise ImexError(rc, msg.decode() if msg else "")
+
+    def step(self, steps: int = 1) -> float:
+        """Advance every member `steps` steps; returns the device time in ms."""
+        ms = C.c_double()
+        self._check(self.lib.imex_batch_step(self.b, steps, C.byref(ms)))
+        return ms.value
+
+    def autotune(self, trial_steps: int = 2) -> dict:
+        t = BatchTuning()
+        self._check(self.lib.imex_batch_autotune(self.b, trial_steps, C.byref(t)))
+        return dict(streams=t.streams, gmres_restart=t.gmres_restart, ms_per_step=t.ms_per_step)
+
+    def info(self) -> dict:
+        a, g, n = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.imex_batch_info(self.b, C.byref(a), C.byref(g), C.byref(n)))
+        msg = self.lib.imex_batch_last_error(self.b)
+        return dict(streams=a.value, graph=bool(g.value), solve_launches_per_step=n.value,
+                    note=msg.decode() if msg else "")
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            for sv in self.members:
+                sv.ctx = None
+            self.lib.imex_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,398 @@
+// Ensembles: many independent runs of uneven grid sizes advanced together.
+//
+// Each member is an ordinary context (its own grid, data, dt and statistics).  One step of
+// the ensemble enqueues, for every member, the same sub-steps as imex_step, with two
+// changes:
+//   - the explicit sub-steps of the members run on a pool of streams, so small members
+//     fill the GPU together;
+//   - each implicit solve of a stage (the magnetic system, the one or two pressure solves)
+//     is ONE cooperative launch for all members, in which every member owns a contiguous
+//     range of CTAs with its own barrier and reductions (see batch_solve_build).  Members
+//     never wait on one another, and no two cooperative kernels run at the same time.
+// The whole step is captured once into a CUDA graph and replayed; if capture fails the
+// same step is launched directly and the reason is kept (imex_batch_last_error).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "imex_internal.h"
+
+struct imex_batch {
+  std::vector<imex_ctx*> members;
+  std::vector<cudaStream_t> streams;  // streams of the explicit sub-steps
+  cudaStream_t origin = nullptr;      // joins the members around the batched solves
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  imex::BatchSolvePlan* mag = nullptr;
+  imex::BatchSolvePlan* pres = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int nstreams = 8;
+  bool use_graph = true;
+  bool prepared = false;
+  bool graph_ok = false;
+  std::string last_error;
+};
+
+namespace {
+
+using namespace imex;
+
+imex_status berr(imex_batch* b, imex_status s, const std::string& msg) {
+  if (b) b->last_error = msg;
+  return s;
+}
+imex_status bcheck(imex_batch* b, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return IMEX_OK;
+  return berr(b, IMEX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+// a member's failure, with its message
+imex_status merr(imex_batch* b, size_t m, imex_status s) {
+  if (s != IMEX_OK) b->last_error = "member " + std::to_string(m) + ": " + b->members[m]->last_error;
+  return s;
+}
+
+// Drop the streams, plans and graph.  Members that are still alive first get a stream of
+// their own again: they must never hold a handle to a destroyed batch stream.
+void release_plans(imex_batch* b, bool members_alive) {
+  if (members_alive && !b->streams.empty())
+    for (imex_ctx* c : b->members) imex_set_stream(c, nullptr);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  batch_solve_free(b->mag);
+  batch_solve_free(b->pres);
+  b->mag = b->pres = nullptr;
+  for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
+  b->streams.clear();
+  b->ev_join.clear();
+  b->prepared = false;
+  b->graph_ok = false;
+}
+
+// one step of every member (main.cpp:335-561 per member), enqueued without a host wait
+imex_status enqueue_step(imex_batch* b) {
+  cudaError_t e = cudaSuccess;
+  auto fork = [&]() {
+    e = cudaEventRecord(b->ev_fork, b->origin);
+    for (cudaStream_t s : b->streams)
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->ev_fork, 0);
+    return bcheck(b, e, "batch fork");
+  };
+  auto join = [&]() {
+    for (size_t k = 0; k < b->streams.size(); ++k) {
+      if (e == cudaSuccess) e = cudaEventRecord(b->ev_join[k], b->streams[k]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->origin, b->ev_join[k], 0);
+    }
+    return bcheck(b, e, "batch join");
+  };
+  auto each = [&](auto f) {
+    for (size_t m = 0; m < b->members.size(); ++m) {
+      imex_status s = f(b->members[m]);
+      if (s != IMEX_OK) return merr(b, m, s);
+    }
+    return IMEX_OK;
+  };
+  imex_ctx* c0 = b->members[0];
+  const DevParams& P = c0->P;
+  imex_status s;
+  if ((s = fork()) != IMEX_OK) return s;
+  if ((s = each([](imex_ctx* c) { return launch_step_prologue(c); })) != IMEX_OK) return s;
+  for (int r = 0; r < P.RKs; ++r) {
+    s = each([r](imex_ctx* c) {
+      imex_status t = launch_stage_combine(c, r);
+      if (t == IMEX_OK) t = launch_reconstruct(c, false);
+      if (t == IMEX_OK) t = launch_flux_update(c, 0);
+      if (t == IMEX_OK) t = mag_rhs(c);
+      return t;
+    });
+    if (s != IMEX_OK) return s;
+    if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->mag, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
+      return s == IMEX_OK ? s : berr(b, s, b->last_error.empty() ? c0->last_error : b->last_error);
+    s = each([](imex_ctx* c) {
+      imex_status t = mag_out(c);
+      if (t == IMEX_OK && c->P.Energy_Modify) {
+        cudaError_t e2 = cudaMemcpyAsync(c->Bsave, c->cons + 5 * c->N, 3 * c->N * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, c->stream);
+        t = cuda_check(c, e2, "Bsave");
+      }
+      if (t == IMEX_OK) t = launch_flux_update(c, 1);
+      if (t == IMEX_OK) t = pres_part1(c);
+      return t;
+    });
+    if (s != IMEX_OK) return s;
+    if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->pres, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
+      return s;
+    bool second = false;
+    s = each([r, &second](imex_ctx* c) { return pres_part2(c, r, &second); });
+    if (s != IMEX_OK) return s;
+    if (second) {
+      if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->pres, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
+        return s;
+    }
+    s = each([r](imex_ctx* c) {
+      imex_status t = pres_part3(c);
+      if (t == IMEX_OK && c->P.magfield == IMEX_StaggerCT) t = launch_ct(c, 0);
+      else if (t == IMEX_OK && c->P.magfield == IMEX_UnStaggerCT) t = launch_ct(c, 1);
+      if (t == IMEX_OK) t = launch_stage_derivative(c, r);
+      return t;
+    });
+    if (s != IMEX_OK) return s;
+  }
+  return join();
+}
+
+// streams, batched-solve plans and (if asked) the captured step
+imex_status prepare(imex_batch* b) {
+  if (b->prepared) return IMEX_OK;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < b->nstreams && e == cudaSuccess; ++k) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (s) b->streams.push_back(s);
+    if (ev) b->ev_join.push_back(ev);
+  }
+  if (e != cudaSuccess) return bcheck(b, e, "batch streams");
+  for (size_t m = 0; m < b->members.size(); ++m) {
+    imex_status s = imex_set_stream(b->members[m], b->streams[m % b->streams.size()]);
+    if (s != IMEX_OK) return merr(b, m, s);
+    b->members[m]->prof_on = false;
+  }
+  imex_status s = batch_solve_build(b->members, BATCH_MAGNETIC, &b->mag);
+  if (s == IMEX_OK) s = batch_solve_build(b->members, BATCH_PRESSURE, &b->pres);
+  if (s != IMEX_OK) return berr(b, s, "batched solve set-up: " + b->members[0]->last_error);
+  b->prepared = true;
+  b->graph_ok = false;
+  if (!b->use_graph) return IMEX_OK;
+  // capture one step; on failure keep the reason and launch directly instead
+  e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    b->last_error = std::string("graph capture unavailable: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    return IMEX_OK;
+  }
+  imex_status cs = enqueue_step(b);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->origin, &g);
+  if (cs == IMEX_OK && e == cudaSuccess && g) e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (cs != IMEX_OK || e != cudaSuccess || !g) {
+    // no graph: start again from fresh streams (a failed capture can leave them unusable)
+    const std::string why = cs != IMEX_OK ? b->last_error : std::string(cudaGetErrorString(e));
+    if (g) cudaGraphDestroy(g);
+    b->exec = nullptr;
+    cudaGetLastError();
+    release_plans(b, true);
+    b->use_graph = false;
+    imex_status r = prepare(b);
+    b->last_error = "graph capture failed, launching directly: " + why;
+    return r;
+  }
+  b->graph = g;
+  b->graph_ok = true;
+  return IMEX_OK;
+}
+
+// worst status of the members since the last check (synchronises)
+imex_status members_status(imex_batch* b) {
+  cudaError_t e = cudaStreamSynchronize(b->origin);
+  if (e != cudaSuccess) return bcheck(b, e, "batch step");
+  imex_status worst = IMEX_OK;
+  for (size_t m = 0; m < b->members.size(); ++m) {
+    imex_solve_stats st;
+    imex_status s = imex_get_stats(b->members[m], &st);
+    if (s != IMEX_OK) return merr(b, m, s);
+    if (st.status != IMEX_OK && worst == IMEX_OK) {
+      worst = (imex_status)st.status;
+      b->last_error = "member " + std::to_string(m) + ": " + imex_status_string(worst);
+    }
+  }
+  if (worst != IMEX_OK)
+    for (imex_ctx* c : b->members) imex_reset_stats(c);
+  return worst;
+}
+
+// device copies of every member's step state, to run trial steps and come back
+struct Snapshot {
+  std::vector<double*> planes;
+  std::vector<std::vector<unsigned char>> scalars;
+};
+imex_status take_snapshot(imex_batch* b, Snapshot& snap, bool restore) {
+  for (size_t m = 0; m < b->members.size(); ++m) {
+    imex_ctx* c = b->members[m];
+    const size_t N = c->N;
+    if (!restore) {
+      double* p = nullptr;
+      cudaError_t e = cudaMalloc(&p, 13 * N * sizeof(double));
+      if (e != cudaSuccess) return bcheck(b, e, "autotune snapshot");
+      snap.planes.push_back(p);
+      snap.scalars.emplace_back(sizeof(DevScalars));
+    }
+    double* p = snap.planes[m];
+    auto cp = [&](double* dst, const double* src, size_t n) {
+      return cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, b->origin);
+    };
+    cudaError_t e;
+    if (!restore) {
+      e = cp(p, c->prim, 8 * N);
+      if (e == cudaSuccess) e = cp(p + 8 * N, c->bx, N);
+      if (e == cudaSuccess) e = cp(p + 9 * N, c->by, N);
+      if (e == cudaSuccess) e = cp(p + 10 * N, c->A, 3 * N);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(snap.scalars[m].data(), c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->origin);
+    } else {
+      e = cp(c->prim, p, 8 * N);
+      if (e == cudaSuccess) e = cp(c->bx, p + 8 * N, N);
+      if (e == cudaSuccess) e = cp(c->by, p + 9 * N, N);
+      if (e == cudaSuccess) e = cp(c->A, p + 10 * N, 3 * N);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->sc, snap.scalars[m].data(), sizeof(DevScalars), cudaMemcpyHostToDevice, b->origin);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->origin);
+    if (e != cudaSuccess) return bcheck(b, e, "autotune snapshot copy");
+  }
+  return IMEX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx, const int* ny,
+                              imex_batch** out) {
+  if (!cfg || members < 1 || !nx || !ny || !out) return IMEX_ERR_INVALID;
+  *out = nullptr;
+  imex_batch* b = new (std::nothrow) imex_batch();
+  if (!b) return IMEX_ERR_CUDA;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    imex_batch_destroy(b);
+    return IMEX_ERR_CUDA;
+  }
+  for (int m = 0; m < members; ++m) {
+    imex_ctx* c = nullptr;
+    imex_status s = imex_create(cfg, nx[m], ny[m], &c);
+    if (s != IMEX_OK) {
+      imex_batch_destroy(b);
+      return s;
+    }
+    b->members.push_back(c);
+  }
+  *out = b;
+  return IMEX_OK;
+}
+
+imex_status imex_batch_destroy(imex_batch* b) {
+  if (!b) return IMEX_ERR_INVALID;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  for (imex_ctx* c : b->members) imex_destroy(c);
+  b->members.clear();
+  release_plans(b, false);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+  return IMEX_OK;
+}
+
+imex_status imex_batch_member(imex_batch* b, int m, imex_ctx** ctx) {
+  if (!b || !ctx || m < 0 || m >= (int)b->members.size()) return IMEX_ERR_INVALID;
+  *ctx = b->members[m];
+  return IMEX_OK;
+}
+
+const char* imex_batch_last_error(const imex_batch* b) { return b ? b->last_error.c_str() : "no batch"; }
+
+imex_status imex_batch_configure(imex_batch* b, int streams, int use_graph) {
+  if (!b || streams < 1 || streams > 64) return IMEX_ERR_INVALID;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  release_plans(b, true);
+  b->nstreams = streams;
+  b->use_graph = use_graph != 0;
+  return IMEX_OK;
+}
+
+imex_status imex_batch_step(imex_batch* b, int steps, double* device_ms) {
+  if (!b || steps < 0) return IMEX_ERR_INVALID;
+  for (imex_ctx* c : b->members)
+    if (c->P.RKs != b->members[0]->P.RKs || c->P.magfield != b->members[0]->P.magfield)
+      return berr(b, IMEX_ERR_INVALID, "members differ in RK stages or magnetic form");
+  imex_status s = prepare(b);
+  if (s != IMEX_OK) return s;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaError_t e = cudaEventCreate(&t0);
+  if (e == cudaSuccess) e = cudaEventCreate(&t1);
+  if (e == cudaSuccess) e = cudaEventRecord(t0, b->origin);
+  for (int k = 0; k < steps && e == cudaSuccess && s == IMEX_OK; ++k) {
+    if (b->graph_ok) e = cudaGraphLaunch(b->exec, b->origin);
+    else s = enqueue_step(b);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(t1, b->origin);
+  if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  if (s != IMEX_OK) return s;
+  if (e != cudaSuccess) return bcheck(b, e, "batch step");
+  if (device_ms) *device_ms = ms;
+  return members_status(b);
+}
+
+imex_status imex_batch_info(imex_batch* b, int* streams, int* graph_used, int* solve_launches_per_step) {
+  if (!b) return IMEX_ERR_INVALID;
+  if (streams) *streams = b->nstreams;
+  if (graph_used) *graph_used = b->graph_ok ? 1 : 0;
+  if (solve_launches_per_step) {
+    int n = 0;
+    if (b->mag) n += (int)b->mag->chunks.size();
+    if (b->pres) n += (int)b->pres->chunks.size();
+    *solve_launches_per_step = n;
+  }
+  return IMEX_OK;
+}
+
+imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out) {
+  if (!b || trial_steps < 1) return IMEX_ERR_INVALID;
+  const int restart0 = b->members[0]->cfg.gmres_restart;
+  const int stream_cands[] = {4, 8, 16};
+  const int restart_cands[] = {restart0 < 15 ? restart0 : 15, restart0};
+  Snapshot snap;
+  imex_status s = take_snapshot(b, snap, false);
+  double best = 1e300;
+  int best_streams = b->nstreams, best_restart = restart0;
+  for (int sc : stream_cands) {
+    for (int rc : restart_cands) {
+      for (imex_ctx* c : b->members) c->cfg.gmres_restart = rc;
+      if (s == IMEX_OK) s = imex_batch_configure(b, sc, b->use_graph ? 1 : 0);
+      double ms = 0.0;
+      if (s == IMEX_OK) s = imex_batch_step(b, 1, nullptr);  // warm-up (and graph capture)
+      if (s == IMEX_OK) s = imex_batch_step(b, trial_steps, &ms);
+      if (s == IMEX_OK) s = take_snapshot(b, snap, true);
+      if (s != IMEX_OK) break;
+      if (ms < best) {
+        best = ms;
+        best_streams = sc;
+        best_restart = rc;
+      }
+    }
+    if (s != IMEX_OK) break;
+  }
+  for (double* p : snap.planes) cudaFree(p);
+  for (imex_ctx* c : b->members) c->cfg.gmres_restart = best_restart;
+  imex_status s2 = imex_batch_configure(b, best_streams, b->use_graph ? 1 : 0);
+  if (s != IMEX_OK) return s;
+  if (s2 != IMEX_OK) return s2;
+  if (out) {
+    out->streams = best_streams;
+    out->gmres_restart = best_restart;
+    out->ms_per_step = best / trial_steps;
+  }
+  return IMEX_OK;
+}
+
+}  // extern "C"

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -158,6 +159,13 @@ imex_status set_h(imex_ctx* ctx, double h);
 imex_status run_mag_subsystem_B(imex_ctx* ctx);
 imex_status run_mag_subsystem_A(imex_ctx* ctx);
 imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks);
+// the same sub-systems in parts around their solves (the batched stage drives these)
+imex_status mag_rhs(imex_ctx* ctx);
+void mag_system(imex_ctx* ctx, int* op, double** x, const double** b);
+imex_status mag_out(imex_ctx* ctx);
+imex_status pres_part1(imex_ctx* ctx);
+imex_status pres_part2(imex_ctx* ctx, int rks, bool* second);
+imex_status pres_part3(imex_ctx* ctx);
 imex_status prepare_operator(imex_ctx* ctx, int op, double h);
 imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax);
 imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b);
@@ -165,6 +173,21 @@ imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b);
 imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig);
 imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                  double* us_per_barrier);
+
+// batched solves of an ensemble (kernels_solve.cu): one kind of solve for every member, run
+// as cooperative launches in which each member owns a contiguous range of CTAs
+enum { BATCH_MAGNETIC = 0, BATCH_PRESSURE = 1 };
+struct BatchChunk {
+  std::function<cudaError_t(cudaStream_t)> launch;  // barrier reset + the cooperative launch
+  int ctas = 0, members = 0;
+};
+struct BatchSolvePlan {
+  std::vector<BatchChunk> chunks;
+  std::vector<void*> dev;  // device arrays of the plan (jobs, CTA map, barrier pointers)
+};
+imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out);
+imex_status batch_solve_run(BatchSolvePlan* plan, cudaStream_t stream, imex_ctx* err_ctx);
+void batch_solve_free(BatchSolvePlan* plan);
 
 // fixed device scratch of imex_gmres_noalloc (noalloc.cu) and the solve that uses it
 constexpr size_t kStaticScratchBytes = IMEX_NOALLOC_SCRATCH_BYTES;

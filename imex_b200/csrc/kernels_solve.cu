@@ -17,6 +17,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <vector>
 
 #include "device_common.cuh"
 
@@ -534,12 +536,19 @@ struct GmresWorkT {
   double* partial;
   SyncState* sync;
   DevStats* st;
-  int kmax, max_restarts, nblk;
+  int kmax, max_restarts;
+  int nblk, first;  // the solve's CTAs: [first, first + nblk) of the launch (the whole grid unless batched)
   int fam;  // profile family whose algorithmic bytes this solve accumulates
   double tol, tol_abs;  // stop when |r| <= tol * |r0| + tol_abs
   Tiling T;
 };
 using GmresWork = GmresWorkT<double>;
+
+// rank of this CTA within the CTAs of its solve
+template <class W>
+__device__ __forceinline__ int grank(const W& g) {
+  return (int)blockIdx.x - g.first;
+}
 
 struct GmresShared {
   double H[KCAP + 2][KCAP + 2];
@@ -634,7 +643,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
   auto Vp = [&](int i) { return g.V + (long long)i * M * N; };
   auto AVp = [&](int i) { return g.AV + (long long)(i & 1) * M * N; };
   auto part = [&]() { return g.partial + (long long)(phase & 1) * g.nblk * NP; };
-  const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
+  const bool lead = threadIdx.x == 0 && grank(g) == 0;
   const int coef = Op::COEF + (op_uses_vdiag(op) ? 1 : 0);
   // algorithmic bytes of a pass that moves `vals` vector values (of type TS) and `cvals`
   // doubles per cell
@@ -651,7 +660,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
     if (from_zero) {
       // ---- r0 = M^-1 b -> V0 and Av0 = M^-1 A V0 in one pass; |r0|^2 and r0.Av0
       wacc_clear(S.acc);
-      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+      for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
@@ -683,7 +692,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         wacc_add(S.acc, 1, va);
         __syncthreads();
       }
-      wacc_store(S.acc, 2, part() + (long long)blockIdx.x * NP);
+      wacc_store(S.acc, 2, part() + (long long)grank(g) * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_reduce(part(), g.nblk, 2, S.red, S.acc);
       ++phase;
@@ -697,7 +706,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
           g.st->last_residual = S.gam[0];
         }
         if (!defer) {  // x = 0
-          for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)gridDim.x * NT)
+          for (long long c = grank(g) * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)g.nblk * NT)
             x[c] = 0.0;
           x_written = true;
         }
@@ -712,7 +721,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
     } else {
       // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
       wacc_clear(S.acc);
-      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+      for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
@@ -741,7 +750,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         wacc_add(S.acc, 0, rr);
         __syncthreads();
       }
-      wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+      wacc_store(S.acc, 1, part() + (long long)grank(g) * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_reduce(part(), g.nblk, 1, S.red, S.acc);
       ++phase;
@@ -761,7 +770,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
 
       // ---- Av0 = M^-1 A V0 (unnormalised), H[0][0]
       wacc_clear(S.acc);
-      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+      for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
@@ -787,7 +796,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         wacc_add(S.acc, 0, va);
         __syncthreads();
       }
-      wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+      wacc_store(S.acc, 1, part() + (long long)grank(g) * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_reduce(part(), g.nblk, 1, S.red, S.acc);
       ++phase;
@@ -805,7 +814,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       // (the combination is formed in FP64 whatever the storage type)
       wacc_clear(S.acc);
       const double sj = S.sigma[j];
-      for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+      for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
           const TS* AVj = AVp(j);
@@ -887,7 +896,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         wacc_add(S.acc, j + 2, ww);
         __syncthreads();
       }
-      wacc_store(S.acc, j + 3, part() + (long long)blockIdx.x * NP);
+      wacc_store(S.acc, j + 3, part() + (long long)grank(g) * NP);
       if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
       grid_reduce(part(), g.nblk, j + 3, S.red, S.acc);
       ++phase;
@@ -944,7 +953,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       }
       return converged ? GM_CONVERGED : GM_MAXIT;
     }
-    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
+    for (long long c = grank(g) * (long long)NT + threadIdx.x; c < N; c += (long long)g.nblk * NT) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         double xv = from_zero ? 0.0 : ldcg(x + m * N + c);
@@ -956,19 +965,22 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
     if (!grid_barrier(g.sync, g.nblk)) return GM_SYNC;
     count((jend + 1) * M, (from_zero ? 1 : 2) * M);
     if (converged) {
-      if (threadIdx.x == 0 && blockIdx.x == 0) {
+      if (threadIdx.x == 0 && grank(g) == 0) {
         g.st->gmres_iters += iters;
         g.st->last_residual = S.gam[jend + 1];
       }
       return GM_CONVERGED;
     }
   }
-  if (threadIdx.x == 0 && blockIdx.x == 0) g.st->gmres_iters += iters;
+  if (threadIdx.x == 0 && grank(g) == 0) g.st->gmres_iters += iters;
   return GM_MAXIT;
 }
 
-__device__ __forceinline__ void record_status(DevStats* st, int code) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
+// the worst status of a solve, recorded once (by the solve's first CTA)
+template <class W>
+__device__ __forceinline__ void record_status(const W& g, int code) {
+  DevStats* st = g.st;
+  if (threadIdx.x == 0 && grank(g) == 0) {
     int s = IMEX_OK;
     if (code == GM_MAXIT) s = IMEX_GMRES_MAXIT;
     else if (code == GM_NONFINITE) s = IMEX_NONFINITE;
@@ -985,17 +997,38 @@ struct SolveSmem {
 };
 
 template <class Op>
-__global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g, double* x, const double* b) {
+__device__ __forceinline__ void gmres_solve(Op op, GmresWork g, double* x, const double* b) {
   extern __shared__ __align__(16) unsigned char dsm[];
   SolveSmem<Op>& sm = *reinterpret_cast<SolveSmem<Op>*>(dsm);
   GmresShared& S = sm.S;
   TileBuf<Op>& tb = sm.tb;
   unsigned phase = 0;
   op.bind();
-  if (threadIdx.x == 0 && blockIdx.x == 0) g.st->gmres_solves += 1;
+  if (threadIdx.x == 0 && grank(g) == 0) g.st->gmres_solves += 1;
   bool written = false;
   int code = gmres_device(op, g, x, b, S, tb, phase, false, false, written);
-  record_status(g.st, code);
+  record_status(g, code);
+}
+template <class Op>
+__global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres(Op op, GmresWork g, double* x, const double* b) {
+  gmres_solve(op, g, x, b);
+}
+
+// Batched solves: one cooperative launch runs many independent solves (the members of an
+// ensemble).  Solve m owns the contiguous CTAs [g.first, g.first + g.nblk) of the launch,
+// with its own barrier state, partial sums and statistics, so solves never wait on one
+// another; cta_job maps each CTA to its solve.
+template <class Op>
+struct GmresJob {
+  Op op;
+  GmresWork g;
+  double* x;
+  const double* b;
+};
+template <class Op>
+__global__ void __launch_bounds__(NT, Op::MIN_BLOCKS) k_gmres_jobs(const GmresJob<Op>* jobs, const int* cta_job) {
+  const GmresJob<Op>& j = jobs[cta_job[blockIdx.x]];
+  gmres_solve(j.op, j.g, j.x, j.b);
 }
 
 // ------------------------------------------------------------------ mixed-precision GMRES
@@ -1023,9 +1056,8 @@ struct MixedSmem {
 };
 
 template <class Op64>
-__global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
-    k_gmres_mixed(Op64 op, GmresWorkT<float> g, double* x, double* xalt, double* sres, const double* b,
-                  int max_sweeps, double tol) {
+__device__ __forceinline__ void mixed_solve(Op64 op, GmresWorkT<float> g, double* x, double* xalt, double* sres,
+                                            const double* b, int max_sweeps, double tol) {
   using Op32 = typename MixedSmem<Op64>::Op32;
   using TB = TileBuf<Op64>;
   constexpr int M = Op64::M, FQ = FillQ<Op64>;
@@ -1038,7 +1070,7 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
   const long long N = T.N;
   unsigned phase = 0;
   auto part = [&]() { return g.partial + (long long)(phase & 1) * g.nblk * NP; };
-  const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
+  const bool lead = threadIdx.x == 0 && grank(g) == 0;
   const int coef = Op64::COEF + (op_uses_vdiag(op) ? 1 : 0);
   if (lead) g.st->gmres_solves += 1;
   double* x_cur = x;
@@ -1050,7 +1082,7 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
   for (int sweep = 0;; ++sweep) {
     // ---- FP64: x += pending update; s = b - A x; |M^-1 s|^2
     wacc_clear(S.acc);
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    for (int t = grank(g); t < T.ntiles; t += g.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
       fill_tile(op, sm.tb.d, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
@@ -1085,9 +1117,9 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
       wacc_add(S.acc, 0, rr);
       __syncthreads();
     }
-    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+    wacc_store(S.acc, 1, part() + (long long)grank(g) * NP);
     if (!grid_barrier(g.sync, g.nblk)) {
-      record_status(g.st, GM_SYNC);
+      record_status(g, GM_SYNC);
       return;
     }
     grid_reduce(part(), g.nblk, 1, S.red, S.acc);
@@ -1120,7 +1152,7 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
     bool written = false;
     int c2 = gmres_device(op32, g, x_nxt, sres, S, sm.tb.f, phase, true, true, written);
     if (c2 == GM_SYNC || c2 == GM_NONFINITE) {
-      record_status(g.st, c2);
+      record_status(g, c2);
       return;
     }
     inner_ok = c2 == GM_CONVERGED;
@@ -1128,9 +1160,30 @@ __global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
   }
   // the result ends in x
   if (x_cur != x)
-    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)gridDim.x * NT)
+    for (long long c = grank(g) * (long long)NT + threadIdx.x; c < (long long)M * N; c += (long long)g.nblk * NT)
       x[c] = ldcg(x_cur + c);
-  if (code != GM_CONVERGED) record_status(g.st, code);
+  if (code != GM_CONVERGED) record_status(g, code);
+}
+template <class Op64>
+__global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS)
+    k_gmres_mixed(Op64 op, GmresWorkT<float> g, double* x, double* xalt, double* sres, const double* b,
+                  int max_sweeps, double tol) {
+  mixed_solve(op, g, x, xalt, sres, b, max_sweeps, tol);
+}
+template <class Op64>
+struct MixedJob {
+  Op64 op;
+  GmresWorkT<float> g;
+  double *x, *xalt, *sres;
+  const double* b;
+  int max_sweeps;
+  double tol;
+};
+template <class Op64>
+__global__ void __launch_bounds__(NT, Op64::MIN_BLOCKS) k_gmres_mixed_jobs(const MixedJob<Op64>* jobs,
+                                                                          const int* cta_job) {
+  const MixedJob<Op64>& j = jobs[cta_job[blockIdx.x]];
+  mixed_solve(j.op, j.g, j.x, j.xalt, j.sres, j.b, j.max_sweeps, j.tol);
 }
 
 // ------------------------------------------------------------------ nested Newton
@@ -1157,7 +1210,7 @@ struct NewtonSmem {
 // Newton convergence test and the iterate stay FP64 in both.  Only the floored or
 // Redlich-Kwong case comes here; the linear case is a plain GMRES launch.
 template <class TS>
-__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
+__device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
   op.bind();
   extern __shared__ __align__(16) unsigned char dsm[];
   NewtonSmem<TS>& sm = *reinterpret_cast<NewtonSmem<TS>*>(dsm);
@@ -1169,13 +1222,13 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   const long long N = T.N;
   unsigned phase = 0;
   auto part = [&]() { return gw.partial + (long long)(phase & 1) * gw.nblk * NP; };
-  const bool lead = threadIdx.x == 0 && blockIdx.x == 0;
+  const bool lead = threadIdx.x == 0 && grank(gw) == 0;
 
   // ---- Cor. 1 slope Mbig (implicit_operators.cpp:670-686)
   double Mbig = na.sc->Mbig;
   if (P.floor_on) {
     double mn = INFINITY, vpe = -INFINITY;
-    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
+    for (long long c = grank(gw) * (long long)NT + threadIdx.x; c < N; c += (long long)gw.nblk * NT) {
       mn = fmin(mn, na.b[c]);
       if (P.eos_type != IMEX_IDEAL_GAS) {
         double v = Vbase(P, P.p_floor, __ldg(op.rho + c));
@@ -1200,11 +1253,11 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
         m0 = fmin(m0, shm[0][w]);
         m1 = fmax(m1, shm[1][w]);
       }
-      part()[(long long)blockIdx.x * NP + 0] = m0;
-      part()[(long long)blockIdx.x * NP + 1] = m1;
+      part()[(long long)grank(gw) * NP + 0] = m0;
+      part()[(long long)grank(gw) * NP + 1] = m1;
     }
     if (!grid_barrier(gw.sync, gw.nblk)) {
-      record_status(gw.st, GM_SYNC);
+      record_status(gw, GM_SYNC);
       return;
     }
     grid_reduce(part(), gw.nblk, 2, S.red, S.acc, RED_MIN | (RED_MAX << 2));
@@ -1246,7 +1299,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   for (it = 0; it < P.Pnewton_max; it++) {
     // ---- pf += pending update; residual g = L pf - a pf + V_mod(pf) - b -> na.g = -g; vdiag = V_slope(pf)
     wacc_clear(S.acc);
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    for (int t = grank(gw); t < T.ntiles; t += gw.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
       fill_tile(L, tb, T, x0, y0, [&](const long long* c, double (*v)[1]) {
         if (pending) {
@@ -1275,9 +1328,9 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       wacc_add(S.acc, 0, gg);
       __syncthreads();
     }
-    wacc_store(S.acc, 1, part() + (long long)blockIdx.x * NP);
+    wacc_store(S.acc, 1, part() + (long long)grank(gw) * NP);
     if (!grid_barrier(gw.sync, gw.nblk)) {
-      record_status(gw.st, GM_SYNC);
+      record_status(gw, GM_SYNC);
       return;
     }
     grid_reduce(part(), gw.nblk, 1, S.red, S.acc);
@@ -1295,7 +1348,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
     const double res = sqrt(S.red[0]);
     if (it == 0) res0 = res;
     if (!isfinite(res)) {
-      record_status(gw.st, GM_NONFINITE);
+      record_status(gw, GM_NONFINITE);
       break;
     }
     if (res < P.Pnewton_tol * res0 + P.Pnewton_tol) break;
@@ -1306,7 +1359,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
     }
     int code = gmres_device(J, gw, na.dp, na.g, S, sm.tb.j, phase, true, true, dp_live);
     if (code != GM_CONVERGED) {
-      record_status(gw.st, code);
+      record_status(gw, code);
       if (code == GM_SYNC || code == GM_NONFINITE) return;
     }
     pending = true;
@@ -1318,7 +1371,7 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
   // ---- p = pf (+ an update still pending after Pnewton_max), floored-cell count and min p
   // (implicit_operators.cpp:722-737)
   double st2[2] = {0.0, INFINITY};
-  for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < N; c += (long long)gridDim.x * NT) {
+  for (long long c = grank(gw) * (long long)NT + threadIdx.x; c < N; c += (long long)gw.nblk * NT) {
     const double pv = pending ? pf_update(c) : ldcg(pf_cur + c);
     na.p[c] = pv;
     if (pv < P.p_floor) st2[0] += 1.0;
@@ -1341,11 +1394,11 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
         s0 += sh2[0][w];
         s1 = fmin(s1, sh2[1][w]);
       }
-      part()[(long long)blockIdx.x * NP + 0] = s0;
-      part()[(long long)blockIdx.x * NP + 1] = s1;
+      part()[(long long)grank(gw) * NP + 0] = s0;
+      part()[(long long)grank(gw) * NP + 1] = s1;
     }
     if (!grid_barrier(gw.sync, gw.nblk)) {
-      record_status(gw.st, GM_SYNC);
+      record_status(gw, GM_SYNC);
       return;
     }
     grid_reduce(part(), gw.nblk, 2, S.red, S.acc, RED_SUM | (RED_MIN << 2));
@@ -1355,6 +1408,32 @@ __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWor
       if (pmin < gw.st->min_p) gw.st->min_p = pmin;
       if (pmin < P.theta * P.p_floor - 1e-14) atomicMax(&gw.st->status, (int)IMEX_POSITIVITY);
     }
+  }
+}
+
+template <class TS>
+__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
+  newton_solve(op, gw, na);
+}
+template <class TS>
+struct NewtonJob {
+  PressureOp op;
+  GmresWorkT<TS> gw;
+  NewtonArgs na;
+};
+template <class TS>
+__global__ void __launch_bounds__(NT, 2) k_nested_newton_jobs(const NewtonJob<TS>* jobs, const int* cta_job) {
+  const NewtonJob<TS>& j = jobs[cta_job[blockIdx.x]];
+  newton_solve(j.op, j.gw, j.na);
+}
+
+// the barrier states of the solves of one batched launch start at zero
+__global__ void k_reset_syncs(SyncState* const* syncs, int n, long long limit) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    syncs[i]->count = 0;
+    syncs[i]->abort = 0;
+    syncs[i]->wait_cycles = limit;
   }
 }
 
@@ -1979,6 +2058,197 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   return s;
 }
 
+// ---- batched solves (host side)
+// One chunk = one cooperative launch over consecutive members: every member gets at least
+// one CTA and at most one per tile, the rest in proportion to its tiles, within the
+// co-resident capacity of the kernel (its occupancy, capped at 4 CTAs per SM, times the SMs).
+template <class Job, class K, class Make>
+imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members, K kernel, size_t smem,
+                       Make make_job) {
+  imex_ctx* c0 = members[0];
+  cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kernel, NT, smem);
+  if (per_sm > 4) per_sm = 4;
+  if (per_sm < 1) return set_error(c0, IMEX_ERR_CUDA, "batched solve kernel does not fit on an SM");
+  const int cap = per_sm * c0->num_sms;
+  const long long limit = wait_cycles(c0);
+  for (size_t i = 0; i < members.size();) {
+    size_t j = i;
+    double tiles_sum = 0.0;
+    while (j < members.size() && (int)(j - i) < cap) {
+      tiles_sum += make_tiling(members[j]->nx, members[j]->ny).ntiles;
+      ++j;
+    }
+    const int n = (int)(j - i);
+    std::vector<int> alloc(n, 1);
+    const int left = cap - n;
+    for (int k = 0; k < n; ++k) {
+      const int nt = make_tiling(members[i + k]->nx, members[i + k]->ny).ntiles;
+      int extra = (int)((double)left * nt / tiles_sum);
+      if (extra > nt - 1) extra = nt - 1;
+      alloc[k] += extra;
+    }
+    std::vector<Job> jobs;
+    std::vector<int> map;
+    std::vector<SyncState*> syncs;
+    int first = 0;
+    for (int k = 0; k < n; ++k) {
+      imex_ctx* m = members[i + k];
+      jobs.push_back(make_job(m, make_tiling(m->nx, m->ny), first, alloc[k]));
+      for (int q = 0; q < alloc[k]; ++q) map.push_back(k);
+      syncs.push_back(m->sync);
+      first += alloc[k];
+    }
+    Job* d_jobs = nullptr;
+    int* d_map = nullptr;
+    SyncState** d_syncs = nullptr;
+    cudaError_t e = cudaMalloc(&d_jobs, jobs.size() * sizeof(Job));
+    if (e == cudaSuccess) e = cudaMalloc(&d_map, map.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&d_syncs, syncs.size() * sizeof(SyncState*));
+    if (d_jobs) plan->dev.push_back(d_jobs);
+    if (d_map) plan->dev.push_back(d_map);
+    if (d_syncs) plan->dev.push_back(d_syncs);
+    if (e == cudaSuccess) e = cudaMemcpy(d_jobs, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_map, map.data(), map.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d_syncs, syncs.data(), syncs.size() * sizeof(SyncState*), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_check(c0, e, "batched solve set-up");
+    const int nctas = first;
+    BatchChunk ch;
+    ch.ctas = nctas;
+    ch.members = n;
+    ch.launch = [=](cudaStream_t st) {
+      k_reset_syncs<<<(n + 255) / 256, 256, 0, st>>>(d_syncs, n, limit);
+      cudaError_t e2 = cudaGetLastError();
+      if (e2 != cudaSuccess) return e2;
+      const Job* dj = d_jobs;
+      const int* dm = d_map;
+      void* params[] = {(void*)&dj, (void*)&dm};
+      return cudaLaunchCooperativeKernel((const void*)kernel, dim3(nctas), dim3(NT), params, smem, st);
+    };
+    plan->chunks.push_back(ch);
+    i = j;
+  }
+  return IMEX_OK;
+}
+
+template <class Op>
+GmresWork job_work(imex_ctx* m, const Tiling& T, int first, int nblk, int fam) {
+  GmresWork g = make_work(m, T, nblk, fam);
+  g.first = first;
+  return g;
+}
+GmresWorkT<float> job_work_mixed(imex_ctx* m, const Tiling& T, int first, int nblk, int fam, int max_restarts,
+                                 double tol_abs) {
+  GmresWorkT<float> g = make_work_mixed(m, T, nblk, fam, max_restarts, tol_abs);
+  g.first = first;
+  return g;
+}
+
+// one GMRES per member with operator make_op(member), plain or mixed
+template <class Op, class MakeOp, class Sys>
+imex_status add_gmres_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members, int kind, int fam,
+                             MakeOp make_op, Sys system) {
+  if (!mixed(members[0], kind)) {
+    return add_chunks<GmresJob<Op>>(plan, members, k_gmres_jobs<Op>, sizeof(SolveSmem<Op>),
+                                    [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
+                                      GmresJob<Op> j{};
+                                      j.op = make_op(m);
+                                      j.g = job_work<Op>(m, T, first, nblk, fam);
+                                      system(m, &j.x, &j.b);
+                                      return j;
+                                    });
+  }
+  return add_chunks<MixedJob<Op>>(plan, members, k_gmres_mixed_jobs<Op>, sizeof(MixedSmem<Op>),
+                                  [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
+                                    MixedJob<Op> j{};
+                                    j.op = make_op(m);
+                                    j.g = job_work_mixed(m, T, first, nblk, fam, 1, 0.0);
+                                    system(m, &j.x, &j.b);
+                                    j.xalt = m->mcor;
+                                    j.sres = m->mres;
+                                    j.max_sweeps = m->cfg.mixed_max_refine;
+                                    j.tol = m->P.GMREStol;
+                                    return j;
+                                  });
+}
+
+template <class TS>
+imex_status add_newton_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members) {
+  return add_chunks<NewtonJob<TS>>(
+      plan, members, k_nested_newton_jobs<TS>, sizeof(NewtonSmem<TS>),
+      [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
+        NewtonJob<TS> j{};
+        j.op = make_pressure_op(m);
+        if constexpr (std::is_same<TS, double>::value) {
+          j.gw = job_work<PressureOp>(m, T, first, nblk, F_NEWTON);
+        } else {
+          j.gw = job_work_mixed(m, T, first, nblk, F_NEWTON, make_work(m, T, nblk, F_NEWTON).max_restarts,
+                                m->P.GMREStol);
+        }
+        j.na.p = m->pp;
+        j.na.pf = m->pf;
+        j.na.g = m->pg;
+        j.na.dp = m->pdp;
+        j.na.vdiag = m->vdiag;
+        j.na.b = m->pb;
+        j.na.sc = m->sc;
+        return j;
+      });
+}
+
+}  // namespace
+
+// The batched solve of one kind for every member (all members share the configuration
+// flags that select the solve; each has its own grid, data and restart length).
+imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out) {
+  if (members.empty()) return IMEX_ERR_INVALID;
+  BatchSolvePlan* plan = new BatchSolvePlan();
+  imex_ctx* c0 = members[0];
+  const DevParams& P = c0->P;
+  imex_status s;
+  if (kind == BATCH_MAGNETIC) {
+    auto sys = [](imex_ctx* m, double** x, const double** b) {
+      int op;
+      mag_system(m, &op, x, b);
+    };
+    if (P.magfield == IMEX_PotentialA)
+      s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op, sys);
+    else
+      s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_B, make_magB_op, sys);
+  } else if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS) {  // linear pressure solve
+    s = add_gmres_chunks<PressureOp>(plan, members, IMEX_MIXED_PRESSURE, F_NEWTON, make_pressure_op,
+                                     [](imex_ctx* m, double** x, const double** b) {
+                                       *x = m->pp;
+                                       *b = m->pb;
+                                     });
+  } else if (!mixed(c0, IMEX_MIXED_PRESSURE)) {
+    s = add_newton_chunks<double>(plan, members);
+  } else {
+    s = add_newton_chunks<float>(plan, members);
+  }
+  if (s != IMEX_OK) {
+    batch_solve_free(plan);
+    return s;
+  }
+  *out = plan;
+  return IMEX_OK;
+}
+imex_status batch_solve_run(BatchSolvePlan* plan, cudaStream_t stream, imex_ctx* err_ctx) {
+  for (const BatchChunk& ch : plan->chunks) {
+    cudaError_t e = ch.launch(stream);
+    if (e != cudaSuccess) return cuda_check(err_ctx, e, "batched solve launch");
+  }
+  return IMEX_OK;
+}
+void batch_solve_free(BatchSolvePlan* plan) {
+  if (!plan) return;
+  for (void* p : plan->dev) cudaFree(p);
+  delete plan;
+}
+
+namespace {
 }  // namespace
 __global__ void k_set_h(DevScalars* sc, double h) { sc->h = h; }
 imex_status set_h(imex_ctx* ctx, double h) {
@@ -1990,11 +2260,29 @@ namespace {
 
 }  // namespace
 
-// MagSubsystem_UpdateB (imex_subsystems.cpp:537-628): RHS, GMRES, cell B, CollectMagFluxes.
-imex_status run_mag_subsystem_B(imex_ctx* ctx) {
+// The magnetic and pressure sub-systems in parts around their solves.  The single-context
+// stage runs each part and then its solve; the batched stage runs a part for every member,
+// then one batched solve for all of them.
+
+// MagSubsystem_UpdateB (imex_subsystems.cpp:537-628) / MagSubsystem_UpdateA
+// (imex_subsystems.cpp:5-74): right-hand side (and the A-form's global viscosity).
+imex_status mag_rhs(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
-  imex_status s;
   int nb = blocks_for(P.N);
+  if (P.magfield == IMEX_PotentialA) {
+    int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
+    prof_begin(ctx);
+    k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
+    LAUNCH_CHECK(ctx, "k_gmax");
+    k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
+    LAUNCH_CHECK(ctx, "k_gmax_finalize");
+    prof_end(ctx, F_GMAX, BYTES(8), 2);
+    prof_begin(ctx);
+    k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
+    LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
+    prof_end(ctx, F_MAG_RHS, BYTES(14), 1);
+    return IMEX_OK;
+  }
   prof_begin(ctx);
   // the initial guess Qe B goes straight into the cell B planes of u_con (planes 5-7; the
   // kernel reads only planes 0-3 of u_con), which GMRES then overwrites with the solution
@@ -2002,41 +2290,49 @@ imex_status run_mag_subsystem_B(imex_ctx* ctx) {
                                                     ctx->cons + 5 * P.N);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_B");
   prof_end(ctx, F_MAG_RHS, BYTES(17), 1);
-  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_B, ctx->cons + 5 * P.N, ctx->mb)) != IMEX_OK) return s;
-  prof_begin(ctx);
-  k_collect_mag_fluxes<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
-  LAUNCH_CHECK(ctx, "k_collect_mag_fluxes");
-  prof_end(ctx, F_COLLECT_FLUX, BYTES(12), 1);
   return IMEX_OK;
 }
-
-// MagSubsystem_UpdateA (imex_subsystems.cpp:5-74): RHS, global viscosity, GMRES, B = curl A.
-imex_status run_mag_subsystem_A(imex_ctx* ctx) {
+// the magnetic system of the current stage: operator, solution (in/out) and right-hand side.
+// The A form is solved in place on A (the initial guess is the current A,
+// imex_subsystems.cpp:46-60), the B form in the cell B planes of u_con.
+void mag_system(imex_ctx* ctx, int* op, double** x, const double** b) {
+  const bool a_form = ctx->P.magfield == IMEX_PotentialA;
+  *op = a_form ? IMEX_OP_MAGNETIC_A : IMEX_OP_MAGNETIC_B;
+  *x = a_form ? ctx->A : ctx->cons + 5 * ctx->P.N;
+  *b = ctx->mb;
+}
+// after the solve: B = curl A, or the face fluxes of the B form (CollectMagFluxes)
+imex_status mag_out(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
-  imex_status s;
   int nb = blocks_for(P.N);
-  int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
   prof_begin(ctx);
-  k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
-  LAUNCH_CHECK(ctx, "k_gmax");
-  k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
-  LAUNCH_CHECK(ctx, "k_gmax_finalize");
-  prof_end(ctx, F_GMAX, BYTES(8), 2);
-  prof_begin(ctx);
-  k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
-  LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
-  prof_end(ctx, F_MAG_RHS, BYTES(14), 1);
-  // solved in place: the initial guess is the current A (imex_subsystems.cpp:46-60)
-  if ((s = gmres_launch(ctx, IMEX_OP_MAGNETIC_A, ctx->A, ctx->mb)) != IMEX_OK) return s;
-  prof_begin(ctx);
-  k_curl_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->A, ctx->cons);
-  LAUNCH_CHECK(ctx, "k_curl_A");
-  prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
+  if (P.magfield == IMEX_PotentialA) {
+    k_curl_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->A, ctx->cons);
+    LAUNCH_CHECK(ctx, "k_curl_A");
+    prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
+  } else {
+    k_collect_mag_fluxes<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
+    LAUNCH_CHECK(ctx, "k_collect_mag_fluxes");
+    prof_end(ctx, F_COLLECT_FLUX, BYTES(12), 1);
+  }
   return IMEX_OK;
 }
+imex_status run_mag_subsystem(imex_ctx* ctx) {
+  imex_status s;
+  if ((s = mag_rhs(ctx)) != IMEX_OK) return s;
+  int op;
+  double* x;
+  const double* b;
+  mag_system(ctx, &op, &x, &b);
+  if ((s = gmres_launch(ctx, op, x, b)) != IMEX_OK) return s;
+  return mag_out(ctx);
+}
+imex_status run_mag_subsystem_B(imex_ctx* ctx) { return run_mag_subsystem(ctx); }
+imex_status run_mag_subsystem_A(imex_ctx* ctx) { return run_mag_subsystem(ctx); }
 
-// PreSubsystem_Pressure (imex_subsystems.cpp:76-413), DefinitionofU energy.
-imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
+// PreSubsystem_Pressure (imex_subsystems.cpp:76-413), DefinitionofU energy, in three
+// parts around its one or two nested-Newton solves of p (pp) with right-hand side pb.
+imex_status pres_part1(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   imex_status s;
   if ((s = pressure_setup(ctx)) != IMEX_OK) return s;
@@ -2046,24 +2342,43 @@ imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
                                                   ctx->pp);
   LAUNCH_CHECK(ctx, "k_pressure_rhs");
   prof_end(ctx, F_PRES_RHS, BYTES(14), 1);
-  if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  return IMEX_OK;
+}
+// momentum from the first solve; *second tells whether a second solve follows
+imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
   prof_begin(ctx);
   k_momentum<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->rv, ctx->cons);
   LAUNCH_CHECK(ctx, "k_momentum");
   prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
-  if (P.PressureSolver == IMEX_all_correction || (P.PressureSolver == IMEX_once_correction && rks == P.RKs - 1)) {
+  *second = P.PressureSolver == IMEX_all_correction || (P.PressureSolver == IMEX_once_correction && rks == P.RKs - 1);
+  if (*second) {
     prof_begin(ctx);
     k_pressure_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->cons + P.N, ctx->pb,
                                                     nullptr, nullptr);
     LAUNCH_CHECK(ctx, "k_pressure_rhs(2)");
     prof_end(ctx, F_PRES_RHS, BYTES(15), 1);
-    if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
   }
+  return IMEX_OK;
+}
+imex_status pres_part3(imex_ctx* ctx) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
   prof_begin(ctx);
   k_energy_define<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->pp, ctx->cons);
   LAUNCH_CHECK(ctx, "k_energy_define");
   prof_end(ctx, F_ENERGY, BYTES(9), 1);
   return IMEX_OK;
+}
+imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
+  imex_status s;
+  bool second = false;
+  if ((s = pres_part1(ctx)) != IMEX_OK) return s;
+  if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  if ((s = pres_part2(ctx, rks, &second)) != IMEX_OK) return s;
+  if (second && (s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  return pres_part3(ctx);
 }
 
 imex_status prepare_operator(imex_ctx* ctx, int op, double h) {

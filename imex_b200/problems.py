@@ -191,3 +191,17 @@ def random_field(n: int = 2048, seed: int = 2026, p0: float = 1.0, mach: float =
     return Problem("random_field", nx, ny, 0.0, 1.0, 0.0, 1.0, prim, np.ascontiguousarray(bx),
                    np.ascontiguousarray(by), A,
                    settings=dict(gamma=gamma, vortex_test=0, eos_type="REDLICH_KWONG", m_alfa=m_alfa, m_b=m_b))
+
+
+def vortex_ensemble(members: int = 256, seed: int = 2026, smin: int = 64, smax: int = 512) -> list[Problem]:
+    """Independent vortex runs (the vortex formulas above): per member kappa, mu ~ U[0.5, 1.5]
+    and a square grid whose side is drawn log-uniformly from [smin, smax] and made even."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(members):
+        kappa = rng.uniform(0.5, 1.5)
+        mu = rng.uniform(0.5, 1.5)
+        side = int(round(math.exp(rng.uniform(math.log(smin), math.log(smax)))))
+        side += side % 2
+        out.append(vortex(side, kappa=kappa, mu=mu))
+    return out

@@ -276,6 +276,39 @@ imex_status imex_pressure_nested_newton(imex_ctx* ctx, double* p, const double* 
 /* ShockDetector (flux.cpp:5) of 8 conserved planes into one plane. */
 imex_status imex_shock_detector(imex_ctx* ctx, const double* Q8, double* eta);
 
+/* Ensembles ------------------------------------------------------------------
+ * Many independent runs of the same configuration on uneven grids, advanced together
+ * (no counterpart in the reference, which runs one grid per process).  Member m is an
+ * ordinary context of nx[m] x ny[m] cells: its data go in and out through the usual
+ * entry points (imex_upload_prim, imex_download_state, imex_divergence, ...) on the
+ * handle from imex_batch_member, and it keeps its own dt, time and statistics.
+ * imex_batch_step advances every member by `steps` time steps: the explicit sub-steps
+ * of the members run on a pool of streams, and each implicit solve of a stage is one
+ * cooperative launch for all members, in which each member owns a range of CTAs.  The
+ * step is captured once into a CUDA graph and replayed.  Members must share the RK
+ * order and the magnetic form; imex_batch_step synchronises and returns the worst
+ * member status (imex_batch_last_error names the member). */
+typedef struct imex_batch imex_batch;
+typedef struct imex_batch_tuning {
+  int streams;          /* streams of the explicit sub-steps */
+  int gmres_restart;    /* Krylov vectors per cycle of every member */
+  double ms_per_step;   /* device time of one ensemble step at that choice */
+} imex_batch_tuning;
+imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx, const int* ny, imex_batch** out);
+imex_status imex_batch_destroy(imex_batch* b);
+imex_status imex_batch_member(imex_batch* b, int m, imex_ctx** ctx);
+/* streams of the explicit sub-steps (default 8) and graph capture (default on) */
+imex_status imex_batch_configure(imex_batch* b, int streams, int use_graph);
+/* advance every member `steps` steps; *device_ms (optional) = device time of those steps */
+imex_status imex_batch_step(imex_batch* b, int steps, double* device_ms);
+/* time `trial_steps` ensemble steps for each candidate (streams 4 / 8 / 16, restart
+ * length 15 or the configured one), restore every member's state after each trial, and
+ * keep the fastest choice */
+imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out);
+/* streams in use, whether the step runs as a captured graph, batched solve launches per step */
+imex_status imex_batch_info(imex_batch* b, int* streams, int* graph_used, int* solve_launches_per_step);
+const char* imex_batch_last_error(const imex_batch* b);
+
 /* Statistics and diagnostics ---------------------------------------------- */
 imex_status imex_get_stats(imex_ctx* ctx, imex_solve_stats* stats);
 imex_status imex_reset_stats(imex_ctx* ctx);
