@@ -10,7 +10,12 @@ benchmark step = one full time step = 3 IMEX stages.  Inputs are analytic
 larger than the 126 MB L2, so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl imex|reference]
-                    [--workload vortex_sheet_1024|vortex_64] [--precision fp64|mixed]
+                    [--workload vortex_sheet_1024|vortex_sheet_2048|vortex_64|random_field_2048|
+                                vortex_ensemble_256] [--precision fp64|mixed]
+
+vortex_ensemble_256 is the batched form: 256 independent vortex runs (seeded kappa, mu and
+grid sides 64..512) advanced together through imex_batch (batched solves, CUDA graph,
+autotuned streams and restart length).
 
 Multi-GPU: the path does not shard (one 2D domain per GPU, "replicas only"):
 N ranks each run an independent copy of the workload; value = total
@@ -50,6 +55,9 @@ WORKLOADS = {
                               desc="vortex-sheet MHD 2048^2, WENO5, A-form CT, floor on, RK3"),
     "vortex_64": dict(problem="vortex", n=64, rks=2, settings=CFG0,
                       desc="smooth MHD vortex 64^2, VanLeer, staggered CT, RK2"),
+    "vortex_ensemble_256": dict(problem="vortex_ensemble", n=0, rks=2, settings=CFG0, members=256,
+                                desc="256 independent vortex runs (seed 2026: kappa, mu ~ U[0.5,1.5], square "
+                                     "sides log-uniform 64..512), VanLeer, staggered CT, RK2, one ensemble"),
     "random_field_2048": dict(problem="random_field", n=2048, rks=2, settings=CFG2,
                               desc="seeded low-Mach random field 2048^2 (seed 2026, beta 0.1), Redlich-Kwong, "
                                    "Minmod, EMF-consistent staggered CT, floor on, RK2"),
@@ -224,6 +232,132 @@ def run_reference(args, world: int, rank: int) -> None:
     print(json.dumps(line))
 
 
+def run_ensemble(args, world: int, rank: int, local: int) -> None:
+    """The batched form: all members of the ensemble advance together through imex_batch.
+    value = cell-stage updates of all members (all ranks) / the timed span (max over ranks)."""
+    import torch
+    import imex_b200 as ix
+    from imex_b200.problems import vortex_ensemble
+
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    probs = vortex_ensemble(wl["members"], seed=2026)
+    settings = dict(wl["settings"])
+    settings["precision"] = args.precision
+    batch = ix.Batch(probs, wl["rks"], settings)
+    tuned = batch.autotune(trial_steps=1)
+    launches0 = sum(m.kernel_launches() for m in batch.members)
+    batch.step(1)  # captures the step (launch count of one step) and runs it
+    info = batch.info()
+    launches_per_step = sum(m.kernel_launches() for m in batch.members) - launches0 + 2 * info["solve_launches_per_step"]
+    for _ in range(max(args.warmup - 1, 2)):
+        batch.step(1)
+    cells_per_step = sum(p.nx * p.ny for p in probs) * wl["rks"]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ms = batch.step(args.steps)
+    barrier(world)
+    t_max = reduce_max(ms, world)
+    value = world * cells_per_step * args.steps / (t_max / 1e3)
+
+    # end to end: every member's state from pinned host memory in, the ensemble step, out
+    e2e = None
+    if not args.no_e2e:
+        bufs = []
+        for p in probs:
+            n = p.nx * p.ny
+            bufs.append([torch.empty(k * n, dtype=torch.float64, pin_memory=True) for k in (8, 1, 1, 3)])
+        for m, sv in enumerate(batch.members):
+            sv.download_state_ptr(*(t.data_ptr() for t in bufs[m]))
+        e2e_steps = min(args.steps, 3)
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for m, sv in enumerate(batch.members):
+                sv.upload_state_ptr(*(t.data_ptr() for t in bufs[m]))
+            batch.step(1)
+            for m, sv in enumerate(batch.members):
+                sv.download_state_ptr(*(t.data_ptr() for t in bufs[m]))
+        torch.cuda.synchronize()
+        wall = reduce_max((time.perf_counter() - t0) * 1e3, world)
+        nbytes = sum(13 * p.nx * p.ny * 8 for p in probs)
+        e2e = {"value": world * cells_per_step * e2e_steps / (wall / 1e3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+               "path": "imex_upload_state + imex_batch_step + imex_download_state per member, pinned host buffers"}
+    stats = [m.stats() for m in batch.members]
+    batch.close()
+
+    # roofline: the largest member alone, with the live kernel profile
+    big = max(probs, key=lambda p: p.nx * p.ny)
+    sv = ix.Solver.for_problem(big, wl["rks"], settings)
+    for _ in range(2):
+        sv.step()
+    sv.profile_enable(True)
+    for _ in range(2):
+        sv.step()
+    prof = sv.profile()
+    sv.close()
+    peak, peak_kind = measured_peaks()
+    dom = max(prof, key=lambda r: r["total_ms"])
+    achieved = dom["alg_bytes"] / (dom["total_ms"] / 1e3) / 1e9
+    roofline = {"kernel": dom["name"], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "alg_bytes_per_launch": dom["alg_bytes"] / dom["launches"],
+                "launches": dom["launches"], "ms_per_launch": dom["total_ms"] / dom["launches"],
+                "measured_on": f"the largest member ({big.nx}x{big.ny}) run alone with the live profile",
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = ensemble_cpu_rate(probs, wl, max_seconds=12.0)
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded vortex ensemble, no dataset)",
+            "config": {"workload": args.workload, "description": wl["desc"], "members": len(probs),
+                       "cells": sum(p.nx * p.ny for p in probs),
+                       "sides": [min(p.nx for p in probs), max(p.nx for p in probs)],
+                       "stages_per_step": wl["rks"], "precision": args.precision,
+                       "parallelism": f"replicas x{world}", "autotuned": tuned, "batch": info,
+                       "l2": "working set ~40 GB >> 126 MB L2; no flush"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks.summary(),
+            "solver": {"gmres_iters": sum(s["gmres_iters"] for s in stats),
+                       "newton_iters": sum(s["newton_iters"] for s in stats),
+                       "status": max(s["status"] for s in stats)},
+        }
+        print(json.dumps(line))
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                json.dump(line, f, indent=1)
+
+
+def ensemble_cpu_rate(probs, wl, max_seconds: float) -> dict:
+    """The reference CPU solver on the ensemble's members, smallest first, one step each,
+    until about max_seconds of CPU time: cell-stage updates per second on one core."""
+    from oracle.bindings import RefSolver, make_solver
+    kind = "reference" if RefSolver.available() else "port"
+    cells, t_total, done = 0, 0.0, 0
+    for p in sorted(probs, key=lambda q: q.nx * q.ny):
+        solver = make_solver("ref" if kind == "reference" else "port", p, wl["rks"], wl["settings"])
+        t0 = time.perf_counter()
+        solver.step()
+        t_total += time.perf_counter() - t0
+        cells += p.nx * p.ny * wl["rks"]
+        done += 1
+        if t_total > max_seconds:
+            break
+    return dict(value=cells / t_total, unit="cell-updates/s", cores=1, kind=kind,
+                sample=f"one time step of each of the {done} smallest members, one core")
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -241,6 +375,12 @@ def main() -> int:
         args.warmup = 3
 
     world, rank, local = dist_setup()
+    if args.impl == "imex" and WORKLOADS[args.workload]["problem"] == "vortex_ensemble":
+        run_ensemble(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:

@@ -15,6 +15,7 @@
 // sigma_i = 1/|w_{i-1}| kept in shared memory.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -2059,9 +2060,12 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
 }
 
 // ---- batched solves (host side)
-// One chunk = one cooperative launch over consecutive members: every member gets at least
-// one CTA and at most one per tile, the rest in proportion to its tiles, within the
-// co-resident capacity of the kernel (its occupancy, capped at 4 CTAs per SM, times the SMs).
+// The members are spread over one or more cooperative launches (chunks) of the kernel's
+// co-resident capacity C (its occupancy, capped at 4 CTAs per SM, times the SMs).  Members
+// are sorted by work (tiles) and dealt to L chunks in snake order, with L large enough that
+// no chunk holds more than C/2 members, so every chunk carries about the same work and has
+// room to give large members many CTAs.  Within a chunk every member gets at least one CTA
+// and at most one per tile, the rest in proportion to its tiles.
 template <class Job, class K, class Make>
 imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members, K kernel, size_t smem,
                        Make make_job) {
@@ -2073,18 +2077,27 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
   if (per_sm < 1) return set_error(c0, IMEX_ERR_CUDA, "batched solve kernel does not fit on an SM");
   const int cap = per_sm * c0->num_sms;
   const long long limit = wait_cycles(c0);
-  for (size_t i = 0; i < members.size();) {
-    size_t j = i;
+  const int nm = (int)members.size();
+  auto tiles = [&](int m) { return make_tiling(members[m]->nx, members[m]->ny).ntiles; };
+  std::vector<int> order(nm);
+  for (int m = 0; m < nm; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tiles(a) > tiles(b); });
+  const int per_chunk = cap / 2 > 0 ? cap / 2 : 1;
+  const int L = (nm + per_chunk - 1) / per_chunk;
+  std::vector<std::vector<int>> groups(L);
+  for (int i = 0; i < nm; ++i) {
+    const int r = i % (2 * L);
+    groups[r < L ? r : 2 * L - 1 - r].push_back(order[i]);
+  }
+  for (const std::vector<int>& grp : groups) {
+    if (grp.empty()) continue;
+    const int n = (int)grp.size();
     double tiles_sum = 0.0;
-    while (j < members.size() && (int)(j - i) < cap) {
-      tiles_sum += make_tiling(members[j]->nx, members[j]->ny).ntiles;
-      ++j;
-    }
-    const int n = (int)(j - i);
+    for (int m : grp) tiles_sum += tiles(m);
     std::vector<int> alloc(n, 1);
     const int left = cap - n;
     for (int k = 0; k < n; ++k) {
-      const int nt = make_tiling(members[i + k]->nx, members[i + k]->ny).ntiles;
+      const int nt = tiles(grp[k]);
       int extra = (int)((double)left * nt / tiles_sum);
       if (extra > nt - 1) extra = nt - 1;
       alloc[k] += extra;
@@ -2094,7 +2107,7 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
     std::vector<SyncState*> syncs;
     int first = 0;
     for (int k = 0; k < n; ++k) {
-      imex_ctx* m = members[i + k];
+      imex_ctx* m = members[grp[k]];
       jobs.push_back(make_job(m, make_tiling(m->nx, m->ny), first, alloc[k]));
       for (int q = 0; q < alloc[k]; ++q) map.push_back(k);
       syncs.push_back(m->sync);
@@ -2128,7 +2141,6 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
       return cudaLaunchCooperativeKernel((const void*)kernel, dim3(nctas), dim3(NT), params, smem, st);
     };
     plan->chunks.push_back(ch);
-    i = j;
   }
   return IMEX_OK;
 }
