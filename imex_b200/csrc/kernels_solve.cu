@@ -1572,12 +1572,6 @@ __global__ void k_magnetic_rhs_B(DevParams P, const DevScalars* __restrict__ sc,
   x0[N + n] = Q(6, n);
   x0[2 * N + n] = Q(7, n);
 }
-// cell B of u_con = solution (imex_subsystems.cpp:618-624)
-__global__ void k_copy3(long long N, const double* __restrict__ src, double* __restrict__ dst) {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= 3 * N) return;
-  dst[n] = src[n];
-}
 // CollectMagFluxes (ct_flux.cpp:5-130), GLF
 __global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon, const double* __restrict__ Qe,
                                      const double* __restrict__ pe, double* __restrict__ Fx,
