@@ -124,6 +124,7 @@ _SIGS = {
     "imex_Pressure_flux_Update": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "imex_PreSubsystem_Pressure": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "imex_PreSubsystem_Energy": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "imex_Energy_flux_Update": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "imex_Staggered_CT_Consistent": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "imex_Unstaggered_CT_Consistent": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "imex_Staggered_CT": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
@@ -408,6 +409,12 @@ class Solver:
 
     def PreSubsystem_Pressure(self, h: float, rks: int = 0) -> None:
         self._check(self.lib.imex_PreSubsystem_Pressure(self.ctx, h, rks))
+
+    def Energy_flux_Update(self, h: float, rks: int = 0) -> None:
+        self._check(self.lib.imex_Energy_flux_Update(self.ctx, h, rks))
+
+    def PreSubsystem_Energy(self, h: float, rks: int = 0) -> None:
+        self._check(self.lib.imex_PreSubsystem_Energy(self.ctx, h, rks))
 
     def Staggered_CT_Consistent(self, h: float, rks: int = 0) -> None:
         self._check(self.lib.imex_Staggered_CT_Consistent(self.ctx, h, rks))

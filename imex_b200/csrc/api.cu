@@ -23,7 +23,8 @@ static const char* kFamilyNames[NFAM] = {
     "step_reduce", "cons_from_prim", "stage_combine", "reconstruct", "flux_convective", "flux_pressure",
     "magnetic_rhs", "gmres_magnetic_B", "gmres_magnetic_A", "magnetic_out", "collect_mag_fluxes",
     "pressure_setup", "shock_detector", "pressure_rhs", "nested_newton", "momentum", "energy_define",
-    "constrained_transport", "stage_derivative", "gmax", "gmres_pressure", "apply_operator", "mixed_refine"};
+    "constrained_transport", "stage_derivative", "gmax", "gmres_pressure", "apply_operator", "mixed_refine",
+    "gmres_energy"};
 const char* family_name(int fam) { return fam >= 0 && fam < NFAM ? kFamilyNames[fam] : "?"; }
 
 static cudaEvent_t prof_event(imex_ctx* ctx) {
@@ -79,7 +80,7 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if (c->RKs < 1 || c->RKs > kMaxRK) return why = "RKs must be 1, 2 or 3", IMEX_ERR_INVALID;
   if (c->x_bc != IMEX_x_Periodic || c->y_bc != IMEX_y_Periodic)
     return why = "only periodic boundaries are implemented", IMEX_ERR_UNSUPPORTED;
-  if (c->formula != IMEX_PressureFormula) return why = "only the pressure formula is implemented", IMEX_ERR_UNSUPPORTED;
+  if (c->formula != IMEX_PressureFormula && c->formula != IMEX_EnergyFormula) return why = "bad formula", IMEX_ERR_INVALID;
   if (!c->GLF) return why = "only the global Lax-Friedrichs dissipation (GLF) is implemented", IMEX_ERR_UNSUPPORTED;
   if (c->U_update != IMEX_DefinitionofU) return why = "only DefinitionofU is implemented", IMEX_ERR_UNSUPPORTED;
   if (c->recon < IMEX_NoRecon || c->recon > IMEX_WENO5) return why = "bad recon", IMEX_ERR_INVALID;
@@ -193,8 +194,10 @@ imex_status stage_body(imex_ctx* ctx, int rks) {
                                     cudaMemcpyDeviceToDevice, ctx->stream);
     if (e != cudaSuccess) return cuda_check(ctx, e, "Bsave");
   }
-  if ((s = launch_flux_update(ctx, 1)) != IMEX_OK) return s;
-  if ((s = run_pre_subsystem_pressure(ctx, rks)) != IMEX_OK) return s;
+  if ((s = launch_flux_update(ctx, second_flux_form(ctx))) != IMEX_OK) return s;
+  if (P.formula == IMEX_EnergyFormula) s = run_pre_subsystem_energy(ctx);
+  else s = run_pre_subsystem_pressure(ctx, rks);
+  if (s != IMEX_OK) return s;
   if (P.magfield == IMEX_StaggerCT) s = launch_ct(ctx, 0);
   else if (P.magfield == IMEX_UnStaggerCT) s = launch_ct(ctx, 1);
   if (s != IMEX_OK) return s;
@@ -630,8 +633,18 @@ imex_status imex_PreSubsystem_Pressure(imex_ctx* ctx, double h, int rks) {
   if (s == IMEX_OK) s = run_pre_subsystem_pressure(ctx, rks);
   return s != IMEX_OK ? s : device_status(ctx);
 }
-imex_status imex_PreSubsystem_Energy(imex_ctx* ctx, double, int) {
-  return set_error(ctx, IMEX_ERR_UNSUPPORTED, "the energy-formula sub-system is not implemented");
+imex_status imex_Energy_flux_Update(imex_ctx* ctx, double h, int rks) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  (void)rks;
+  imex_status s = set_h(ctx, h);
+  return s != IMEX_OK ? s : launch_flux_update(ctx, 2);
+}
+imex_status imex_PreSubsystem_Energy(imex_ctx* ctx, double h, int rks) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  (void)rks;
+  imex_status s = set_h(ctx, h);
+  if (s == IMEX_OK) s = run_pre_subsystem_energy(ctx);
+  return s != IMEX_OK ? s : device_status(ctx);
 }
 imex_status imex_Staggered_CT_Consistent(imex_ctx* ctx, double h, int) { return ct_entry(ctx, h, 0, IMEX_StaggerCT); }
 imex_status imex_Unstaggered_CT_Consistent(imex_ctx* ctx, double h, int) {

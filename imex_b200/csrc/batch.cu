@@ -119,7 +119,7 @@ imex_status enqueue_step(imex_batch* b) {
                                          cudaMemcpyDeviceToDevice, c->stream);
         t = cuda_check(c, e2, "Bsave");
       }
-      if (t == IMEX_OK) t = launch_flux_update(c, 1);
+      if (t == IMEX_OK) t = launch_flux_update(c, second_flux_form(c));
       if (t == IMEX_OK) t = pres_part1(c);
       return t;
     });

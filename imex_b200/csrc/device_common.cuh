@@ -272,14 +272,53 @@ __device__ __forceinline__ void magflux_p(const double* Q, int dir, double* f) {
     f[4] = Q[2] / Q[0] * B2 - Q[6] * vB;
   }
 }
-// Rusanov face flux of RusanovC_x/y (flux.cpp:329-406) or Pressure_flux_x/y (flux.cpp:202-287)
-template <bool kPressureForm>
+// magnetic flux of the energy formula, MagneticFlux_x/y (state.cpp:272-296)
+__device__ __forceinline__ void magflux_e(const DevParams& P, const double* Q, int dir, double* f) {
+  double B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
+  double vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
+  f[0] = 0;
+  if (dir == 0) {
+    f[1] = (2 - P.gamma) * B2 * 0.5 - Q[5] * Q[5];
+    f[2] = -Q[5] * Q[6];
+    f[3] = -Q[5] * Q[7];
+    f[4] = Q[1] / Q[0] * B2 * 0.5 - Q[5] * vB;
+  } else {
+    f[1] = -Q[5] * Q[6];
+    f[2] = (2 - P.gamma) * B2 * 0.5 - Q[6] * Q[6];
+    f[3] = -Q[6] * Q[7];
+    f[4] = Q[2] / Q[0] * B2 * 0.5 - Q[6] * vB;
+  }
+}
+// the non-zero component (1 + dir) of f/g_KineticEnergyFlux (state.cpp:325-345)
+__device__ __forceinline__ double keflux(const DevParams& P, const double* Q) {
+  return -(P.gamma - 1) * 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
+}
+// total enthalpy (E + p) / rho, caltotalenthalpy (timestep.cpp:232-237)
+__device__ __forceinline__ double caltotalenthalpy(const DevParams& P, const double* c) {
+  double pri[8];
+  con2pri(P, pri, c);
+  return (c[4] + pri[4]) / pri[0];
+}
+// Rusanov face flux of RusanovC_x/y (flux.cpp:329-406), Pressure_flux_x/y (flux.cpp:202-287)
+// or Energy_flux_x/y (flux.cpp:78-200): kForm 0, 1, 2
+template <int kForm>
 __device__ __forceinline__ void face_flux(const DevParams& P, const double* QL, const double* QR, int dir,
                                           double a_max, double* F) {
   double fL[5], fR[5];
   f_conv(QL, dir, fL);
   f_conv(QR, dir, fR);
-  if (kPressureForm) {
+  if (kForm == 2) {  // convective (energy zeroed) + magnetic + kinetic-energy fluxes
+    fL[4] = 0;
+    fR[4] = 0;
+    double fb[5];
+    const double kl = keflux(P, QL), kr = keflux(P, QR);
+    magflux_e(P, QL, dir, fb);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fL[k] = fL[k] + fb[k] + (k == 1 + dir ? kl : 0.0);
+    magflux_e(P, QR, dir, fb);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fR[k] = fR[k] + fb[k] + (k == 1 + dir ? kr : 0.0);
+  } else if (kForm == 1) {
     double fb[5];
     magflux_p(QL, dir, fb);
 #pragma unroll

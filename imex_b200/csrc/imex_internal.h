@@ -40,7 +40,7 @@ struct DevScalars {
 enum Family {
   F_PROLOGUE_REDUCE, F_CONS_FROM_PRIM, F_COMBINE, F_RECON, F_FLUX_CONV, F_FLUX_PRES, F_MAG_RHS,
   F_GMRES_MAG_B, F_GMRES_MAG_A, F_MAG_OUT, F_COLLECT_FLUX, F_PRES_SETUP, F_SHOCK, F_PRES_RHS, F_NEWTON,
-  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, NFAM
+  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, F_GMRES_ENERGY, NFAM
 };
 
 // Device-side counters and status of the implicit solves.
@@ -142,7 +142,8 @@ imex_status cuda_check(imex_ctx* ctx, cudaError_t e, const char* what);
 imex_status launch_step_prologue(imex_ctx* ctx);
 imex_status launch_stage_combine(imex_ctx* ctx, int rks);
 imex_status launch_reconstruct(imex_ctx* ctx, bool full);
-imex_status launch_flux_update(imex_ctx* ctx, int pressure_form);
+imex_status launch_flux_update(imex_ctx* ctx, int form);
+int second_flux_form(const imex_ctx* ctx);
 imex_status launch_stage_derivative(imex_ctx* ctx, int rks);
 imex_status launch_ct(imex_ctx* ctx, int variant);
 imex_status launch_prim_from_cons(imex_ctx* ctx);
@@ -159,7 +160,9 @@ imex_status set_h(imex_ctx* ctx, double h);
 imex_status run_mag_subsystem_B(imex_ctx* ctx);
 imex_status run_mag_subsystem_A(imex_ctx* ctx);
 imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks);
-// the same sub-systems in parts around their solves (the batched stage drives these)
+imex_status run_pre_subsystem_energy(imex_ctx* ctx);
+// the same sub-systems in parts around their solves (the batched stage drives these); in the
+// energy formula the pres_part* functions run PreSubsystem_Energy around its one solve
 imex_status mag_rhs(imex_ctx* ctx);
 void mag_system(imex_ctx* ctx, int* op, double** x, const double** b);
 imex_status mag_out(imex_ctx* ctx);

@@ -288,6 +288,57 @@ struct PressureOpT : PressureCoef {
 };
 using PressureOp = PressureOpT<double>;
 
+// Energy_Subsystem_AX (implicit_operators.cpp:741-795), periodic, on the total energy E:
+//   A E = (E - (g-1) h^2 div(hh grad E)) dx dy,  hh = h(Qe) rho_e / rho frozen per solve;
+// precE (imex_subsystems.cpp:487-505) divides by the staged diag dx dy.
+struct EnergyCoef {
+  DevParams P;
+  const DevScalars* sc;
+  const double *hh, *tdiag;
+  double gh2, idx2, idy2, dx, dy;
+  __device__ __forceinline__ void bind() {
+    const double h = sc->h;
+    gh2 = (P.gamma - 1) * h * h;
+    idx2 = 1.0 / (P.dx * P.dx);
+    idy2 = 1.0 / (P.dy * P.dy);
+    dx = P.dx;
+    dy = P.dy;
+  }
+};
+template <class T>
+struct EnergyOpT : EnergyCoef {
+  using value_type = T;
+  static constexpr int M = 1, HALO = 1;
+  static constexpr int COEF = 2;  // hh, tdiag
+  static constexpr int QT = 1;    // staged: hh
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 2;
+  template <class U>
+  __device__ __forceinline__ EnergyOpT<U> as() const {
+    EnergyOpT<U> o;
+    static_cast<EnergyCoef&>(o) = *this;
+    return o;
+  }
+  __device__ __forceinline__ void coef(long long c, T* q) const { q[0] = (T)__ldg(hh + c); }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB&, int, int) const {}
+  template <class TB>
+  __device__ __forceinline__ void matvec(const TB& tb, int lx, int ly, long long, T* out) const {
+    const int sx = TB::SX, o = (ly + 1) * sx + lx + 1;
+    const T hf = T(0.5);
+    const T* x = tb.s;
+    const T* hq = tb.c;
+    const T Ei = x[o], xe = x[o + 1], xw = x[o - 1], xn = x[o + sx], xs = x[o - sx];
+    const T h00 = hq[o];
+    const T hpx = hf * (h00 + hq[o + 1]), hmx = hf * (h00 + hq[o - 1]);
+    const T hpy = hf * (h00 + hq[o + sx]), hmy = hf * (h00 + hq[o - sx]);
+    const T r = Ei - (T)gh2 * ((T)idx2 * (hpx * (xe - Ei) - hmx * (Ei - xw)) + (T)idy2 * (hpy * (xn - Ei) - hmy * (Ei - xs)));
+    out[0] = r * (T)dx * (T)dy;
+  }
+  __device__ __forceinline__ void precond(long long c, T* v) const { v[0] = v[0] / (T)__ldg(tdiag + c); }
+};
+using EnergyOp = EnergyOpT<double>;
+
 // Magnetic_Subsystem_AX (implicit_operators.cpp:141-353), GLF viscosity, periodic.
 struct MagneticBCoef {
   DevParams P;
@@ -1516,6 +1567,49 @@ __global__ void k_energy_define(DevParams P, const double* __restrict__ p, doubl
   ucon[4 * N + n] = Vbase(P, p[n], r) + 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / r + 0.5 * (b5 * b5 + b6 * b6 + b7 * b7);
 }
 
+// total-enthalpy ratio hh = caltotalenthalpy(Qe) rho_e / rho (imex_subsystems.cpp:442-446)
+__global__ void k_energy_coeffs(DevParams P, const double* __restrict__ Qe, const double* __restrict__ ucon,
+                                double* __restrict__ hh) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double c[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c[k] = Qe[k * N + n];
+  hh[n] = caltotalenthalpy(P, c) * c[0] / ucon[n];
+}
+// right-hand side b = U* dx dy (imex_subsystems.cpp:448-452) and the Jacobi scale diag dx dy
+// of precE (imex_subsystems.cpp:499-503); the initial guess is E of u_con (solved in place)
+__global__ void k_energy_rhs(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                             const double* __restrict__ hh, double* __restrict__ b, double* __restrict__ tdiag) {
+  const long long N = P.N;
+  const double h = sc->h;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const long long e = cid(P, i + 1, j), w = cid(P, i - 1, j), no = cid(P, i, j + 1), s = cid(P, i, j - 1);
+  const double h00 = hh[n], hp0 = hh[e], hm0 = hh[w], h0p = hh[no], h0m = hh[s];
+  const double U_star = ucon[4 * N + n] - 0.5 * h / P.dx * (hp0 * ucon[N + e] - hm0 * ucon[N + w]) -
+                        0.5 * h / P.dy * (h0p * ucon[2 * N + no] - h0m * ucon[2 * N + s]);
+  b[n] = U_star * P.dx * P.dy;
+  const double hhp_x = 0.5 * (h00 + hp0), hhm_x = 0.5 * (h00 + hm0);
+  const double hhp_y = 0.5 * (h00 + h0p), hhm_y = 0.5 * (h00 + h0m);
+  const double diag =
+      1.0 + (P.gamma - 1.0) * h * h * ((hhp_x + hhm_x) / (P.dx * P.dx) + (hhp_y + hhm_y) / (P.dy * P.dy));
+  tdiag[n] = diag * P.dx * P.dy;
+}
+// momentum correction rho v -= h (g-1) grad E (imex_subsystems.cpp:514-519)
+__global__ void k_energy_momentum(DevParams P, const DevScalars* __restrict__ sc, double* __restrict__ ucon) {
+  const long long N = P.N;
+  const double h = sc->h;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double* E = ucon + 4 * N;
+  ucon[N + n] -= h * (1 / (2 * P.dx)) * (P.gamma - 1) * (E[cid(P, i + 1, j)] - E[cid(P, i - 1, j)]);
+  ucon[2 * N + n] -= h * (1 / (2 * P.dy)) * (P.gamma - 1) * (E[cid(P, i, j + 1)] - E[cid(P, i, j - 1)]);
+}
+
 // B* right-hand side (imex_subsystems.cpp:549-615) and initial guess x0 = Qe B
 __global__ void k_magnetic_rhs_B(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                  const double* __restrict__ Qe, const double* __restrict__ Qs,
@@ -1877,6 +1971,14 @@ PressureOp make_pressure_op(imex_ctx* ctx) {
   op.jac = 0;
   return op;
 }
+EnergyOp make_energy_op(imex_ctx* ctx) {
+  EnergyOp op{};
+  op.P = ctx->P;
+  op.sc = ctx->sc;
+  op.hh = ctx->hh;
+  op.tdiag = ctx->tdiag;
+  return op;
+}
 MagneticBOp make_magB_op(imex_ctx* ctx) {
   MagneticBOp op{};
   op.P = ctx->P;
@@ -1904,6 +2006,28 @@ void launch_apply(imex_ctx* ctx, const Op& o, int nb, const Tiling& T, const dou
   prof_end(ctx, F_APPLY, (double)(2 * Op::M + Op::COEF) * 8.0 * (double)T.N, 1);
 }
 
+// hh and the right-hand side / Jacobi scale of the energy solve
+imex_status energy_setup(imex_ctx* ctx) {
+  const DevParams& P = ctx->P;
+  int nb = blocks_for(P.N);
+  prof_begin(ctx);
+  k_energy_coeffs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->Qe, ctx->cons, ctx->hh);
+  LAUNCH_CHECK(ctx, "k_energy_coeffs");
+  prof_end(ctx, F_PRES_SETUP, BYTES(10), 1);
+  prof_begin(ctx);
+  k_energy_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->pb, ctx->tdiag);
+  LAUNCH_CHECK(ctx, "k_energy_rhs");
+  prof_end(ctx, F_PRES_RHS, BYTES(6), 1);
+  return IMEX_OK;
+}
+imex_status energy_momentum(imex_ctx* ctx) {
+  int nb = blocks_for(ctx->P.N);
+  prof_begin(ctx);
+  k_energy_momentum<<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->cons);
+  LAUNCH_CHECK(ctx, "k_energy_momentum");
+  prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
+  return IMEX_OK;
+}
 imex_status pressure_setup(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
@@ -1951,6 +2075,8 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
     return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     return gmres_run(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, IMEX_MIXED_MAGNETIC);
+  } else if (op == IMEX_OP_ENERGY) {
+    return gmres_run(ctx, make_energy_op(ctx), F_GMRES_ENERGY, x, b, IMEX_MIXED_PRESSURE);
   }
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
 }
@@ -2223,6 +2349,12 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
       s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op, sys);
     else
       s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_B, make_magB_op, sys);
+  } else if (P.formula == IMEX_EnergyFormula) {  // the energy solve, in place on E
+    s = add_gmres_chunks<EnergyOp>(plan, members, IMEX_MIXED_PRESSURE, F_GMRES_ENERGY, make_energy_op,
+                                   [](imex_ctx* m, double** x, const double** b) {
+                                     *x = m->cons + 4 * m->N;
+                                     *b = m->pb;
+                                   });
   } else if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS) {  // linear pressure solve
     s = add_gmres_chunks<PressureOp>(plan, members, IMEX_MIXED_PRESSURE, F_NEWTON, make_pressure_op,
                                      [](imex_ctx* m, double** x, const double** b) {
@@ -2340,6 +2472,7 @@ imex_status run_mag_subsystem_A(imex_ctx* ctx) { return run_mag_subsystem(ctx); 
 // parts around its one or two nested-Newton solves of p (pp) with right-hand side pb.
 imex_status pres_part1(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
+  if (P.formula == IMEX_EnergyFormula) return energy_setup(ctx);
   imex_status s;
   if ((s = pressure_setup(ctx)) != IMEX_OK) return s;
   int nb = blocks_for(P.N);
@@ -2354,6 +2487,10 @@ imex_status pres_part1(imex_ctx* ctx) {
 imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
+  if (P.formula == IMEX_EnergyFormula) {
+    *second = false;
+    return energy_momentum(ctx);
+  }
   prof_begin(ctx);
   k_momentum<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->rv, ctx->cons);
   LAUNCH_CHECK(ctx, "k_momentum");
@@ -2370,6 +2507,7 @@ imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
 }
 imex_status pres_part3(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
+  if (P.formula == IMEX_EnergyFormula) return IMEX_OK;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
   k_energy_define<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->pp, ctx->cons);
@@ -2385,6 +2523,15 @@ imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
   if ((s = pres_part2(ctx, rks, &second)) != IMEX_OK) return s;
   if (second && (s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
   return pres_part3(ctx);
+}
+// PreSubsystem_Energy (imex_subsystems.cpp:415-534), periodic: one GMRES on E in place
+imex_status run_pre_subsystem_energy(imex_ctx* ctx) {
+  imex_status s;
+  if ((s = energy_setup(ctx)) != IMEX_OK) return s;
+  if ((s = gmres_run(ctx, make_energy_op(ctx), F_GMRES_ENERGY, ctx->cons + 4 * ctx->N, ctx->pb,
+                     IMEX_MIXED_PRESSURE)) != IMEX_OK)
+    return s;
+  return energy_momentum(ctx);
 }
 
 imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
@@ -2403,6 +2550,7 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
     if ((s = launch_qe_derived(ctx)) != IMEX_OK) return s;
     return pressure_setup(ctx);
   }
+  if (op == IMEX_OP_ENERGY) return energy_setup(ctx);
   return IMEX_OK;
 }
 
@@ -2427,6 +2575,8 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
     launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     launch_apply(ctx, make_magA_op(ctx), nb, T, x, Ax);
+  } else if (op == IMEX_OP_ENERGY) {
+    launch_apply(ctx, make_energy_op(ctx), nb, T, x, Ax);
   } else {
     return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
   }
@@ -2446,6 +2596,8 @@ imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b,
     return gmres_noalloc_op(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, base, capacity);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     return gmres_noalloc_op(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, base, capacity);
+  } else if (op == IMEX_OP_ENERGY) {
+    return gmres_noalloc_op(ctx, make_energy_op(ctx), F_GMRES_ENERGY, x, b, base, capacity);
   }
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, "operator not available");
 }

@@ -275,7 +275,7 @@ __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double*
 // ---------------------------------------------------------------- flux updates
 // RusanovC_Update (flux.cpp:409-455) or Pressure_flux_Update (flux.cpp:290-326) with the
 // B slots of the face states taken from cell B of u_con (main.cpp:447-467).
-template <bool kPressureForm>
+template <int kForm>
 __global__ void __launch_bounds__(kThreads, 2) k_flux_update(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ w,
                               const double* __restrict__ Qs, double* __restrict__ ucon) {
   const long long N = P.N;
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_flux_update(DevParams P, const 
   auto state = [&](const double* wq, long long m, double* Q) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) Q[k] = __ldg(wq + k * N + m);
-    if (kPressureForm) {
+    if (kForm != 0) {
 #pragma unroll
       for (int k = 5; k < 8; ++k) Q[k] = __ldg(ucon + k * N + m);
     } else {
@@ -301,16 +301,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_flux_update(DevParams P, const 
   double QL[8], QR[8], fp[5], fm[5], gp[5], gm[5];
   state(wxR, n, QL);
   state(wxL, ip, QR);
-  face_flux<kPressureForm>(P, QL, QR, 0, a_max, fp);
+  face_flux<kForm>(P, QL, QR, 0, a_max, fp);
   state(wyR, n, QL);
   state(wyL, jp, QR);
-  face_flux<kPressureForm>(P, QL, QR, 1, a_max, gp);
+  face_flux<kForm>(P, QL, QR, 1, a_max, gp);
   state(wxR, im, QL);
   state(wxL, n, QR);
-  face_flux<kPressureForm>(P, QL, QR, 0, a_max, fm);
+  face_flux<kForm>(P, QL, QR, 0, a_max, fm);
   state(wyR, jm, QL);
   state(wyL, n, QR);
-  face_flux<kPressureForm>(P, QL, QR, 1, a_max, gm);
+  face_flux<kForm>(P, QL, QR, 1, a_max, gm);
 #pragma unroll
   for (int k = 0; k < 5; ++k)
     ucon[k * N + n] = Qs[k * N + n] - h / P.dx * (fp[k] - fm[k]) - h / P.dy * (gp[k] - gm[k]);
@@ -696,17 +696,22 @@ imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
   return IMEX_OK;
 }
 
-imex_status launch_flux_update(imex_ctx* ctx, int pressure_form) {
+// form 0: RusanovC_Update; 1: Pressure_flux_Update; 2: Energy_flux_Update (flux.cpp:186-200)
+imex_status launch_flux_update(imex_ctx* ctx, int form) {
   int nb = blocks_for(ctx->P.N);
   prof_begin(ctx);
-  if (pressure_form)
-    k_flux_update<true><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  if (form == 1)
+    k_flux_update<1><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  else if (form == 2)
+    k_flux_update<2><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else
-    k_flux_update<false><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    k_flux_update<0><<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   LAUNCH_CHECK(ctx, "k_flux_update");
-  prof_end(ctx, pressure_form ? F_FLUX_PRES : F_FLUX_CONV, BYTES(pressure_form ? 33 : 30), 1);
+  prof_end(ctx, form ? F_FLUX_PRES : F_FLUX_CONV, BYTES(form ? 33 : 30), 1);
   return IMEX_OK;
 }
+// the flux of the implicit formula of this context (main.cpp:469-476)
+int second_flux_form(const imex_ctx* ctx) { return ctx->P.formula == IMEX_EnergyFormula ? 2 : 1; }
 
 // variant: 0 Staggered_CT_Consistent, 1 Unstaggered_CT_Consistent, 2 Staggered_CT, 3 Unstaggered_CT
 imex_status launch_ct(imex_ctx* ctx, int variant) {

@@ -192,6 +192,7 @@ imex_status imex_MagSubsystem_UpdateB(imex_ctx* ctx, double h, int rks);      /*
 imex_status imex_MagSubsystem_UpdateA(imex_ctx* ctx, double h, int rks);      /* imex_subsystems.cpp:5 */
 imex_status imex_Pressure_flux_Update(imex_ctx* ctx, double h, int rks);      /* flux.cpp:290 + main.cpp:447-467 */
 imex_status imex_PreSubsystem_Pressure(imex_ctx* ctx, double h, int rks);     /* imex_subsystems.cpp:76 */
+imex_status imex_Energy_flux_Update(imex_ctx* ctx, double h, int rks);        /* flux.cpp:163 + main.cpp:447-467 */
 imex_status imex_PreSubsystem_Energy(imex_ctx* ctx, double h, int rks);       /* imex_subsystems.cpp:415 */
 imex_status imex_Staggered_CT_Consistent(imex_ctx* ctx, double h, int rks);   /* ct_flux.cpp:150 */
 imex_status imex_Unstaggered_CT_Consistent(imex_ctx* ctx, double h, int rks); /* constrained_transport.cpp:500 */

@@ -405,6 +405,41 @@ static void pressure_flux(const double* QL, const double* QR, double* F, int dir
   double s = smax_of(QL, QR, dir);
   for (int k = 0; k < 5; ++k) F[k] = 0.5 * (fL[k] + fR[k]) - 0.5 * s * (QR[k] - QL[k]);
 }
+/* state.cpp:272-296 MagneticFlux_x/y (energy formula) */
+static void magflux_e(double* f, const double* Q, int dir) {
+  const double g = PP.gamma_plasma;
+  double B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
+  double vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
+  f[0] = 0;
+  if (dir == 0) {
+    f[1] = (2 - g) * B2 * 0.5 - Q[5] * Q[5];
+    f[2] = -Q[5] * Q[6];
+    f[3] = -Q[5] * Q[7];
+    f[4] = Q[1] / Q[0] * B2 * 0.5 - Q[5] * vB;
+  } else {
+    f[1] = -Q[5] * Q[6];
+    f[2] = (2 - g) * B2 * 0.5 - Q[6] * Q[6];
+    f[3] = -Q[6] * Q[7];
+    f[4] = Q[2] / Q[0] * B2 * 0.5 - Q[6] * vB;
+  }
+}
+/* flux.cpp:78-161 Energy_flux_x / Energy_flux_y: convective (energy slot zeroed) +
+   magnetic + kinetic-energy flux f/g_KineticEnergyFlux (state.cpp:325-345) */
+static void energy_flux(const double* QL, const double* QR, double* F, int dir) {
+  double fC[5], fB[5], fK[5], fL[5], fR[5];
+  const double* Q[2] = {QL, QR};
+  double* out[2] = {fL, fR};
+  for (int s = 0; s < 2; ++s) {
+    f_conv(fC, Q[s], dir);
+    fC[4] = 0;
+    magflux_e(fB, Q[s], dir);
+    for (int k = 0; k < 5; ++k) fK[k] = 0;
+    fK[1 + dir] = -(PP.gamma_plasma - 1) * 0.5 * (Q[s][1] * Q[s][1] + Q[s][2] * Q[s][2] + Q[s][3] * Q[s][3]) / Q[s][0];
+    for (int k = 0; k < 5; ++k) out[s][k] = fC[k] + fB[k] + fK[k];
+  }
+  double s = smax_of(QL, QR, dir);
+  for (int k = 0; k < 5; ++k) F[k] = 0.5 * (fL[k] + fR[k]) - 0.5 * s * (QR[k] - QL[k]);
+}
 typedef void (*flux_fn)(const double*, const double*, double*, int);
 
 /* flux.cpp:409-455 / 290-326: u_con[0..4] = Qs - h/dx (fp - fm) - h/dy (gp - gm) */
@@ -774,6 +809,86 @@ static void pre_subsystem_pressure(double* ucon, const double* Qs, const double*
     }
   }
   free(rvx); free(rvy); free(rvz); free(b); free(p);
+}
+
+/* ------------------------------------------------------------------ */
+/* energy sub-system, PreSubsystem_Energy imex_subsystems.cpp:415-534 */
+/* with Energy_Subsystem_AX implicit_operators.cpp:741-795 (periodic) */
+/* ------------------------------------------------------------------ */
+/* total enthalpy (E + p) / rho, caltotalenthalpy timestep.cpp:232-237 */
+static double caltotalenthalpy(const double* c) {
+  double pri[8];
+  con2pri(pri, c);
+  return (c[4] + pri[4]) / pri[0];
+}
+static void energy_ax(const double* x, double* Ax) {
+  const double h = OP.h, dx = G.dx, dy = G.dy, g = PP.gamma_plasma;
+  for (int i = 0; i < G.nx; i++)
+    for (int j = 0; j < G.ny; j++) {
+      size_t c = ID(i, j), e = ID(i + 1, j), w = ID(i - 1, j), n = ID(i, j + 1), s = ID(i, j - 1);
+      double h00 = OP.hh[c], hp0 = OP.hh[e], hm0 = OP.hh[w], h0p = OP.hh[n], h0m = OP.hh[s];
+      double hhp_x = 0.5 * (h00 + hp0), hhm_x = 0.5 * (h00 + hm0);
+      double hhp_y = 0.5 * (h00 + h0p), hhm_y = 0.5 * (h00 + h0m);
+      double Ei = x[c];
+      double r = Ei - (g - 1) * h * h *
+                          (1.0 / (dx * dx) * (hhp_x * (x[e] - Ei) - hhm_x * (Ei - x[w])) +
+                           1.0 / (dy * dy) * (hhp_y * (x[n] - Ei) - hhm_y * (Ei - x[s])));
+      Ax[c] = r * dx * dy;
+    }
+}
+/* precE, imex_subsystems.cpp:487-505: in / (diag dx dy) */
+static void energy_pc(const double* in, double* out) {
+  for (size_t n = 0; n < G.N; ++n) out[n] = in[n] / OP.tdiag[n];
+}
+/* the cell enthalpy ratio h(Qe) rho_e / rho of the operator and the Jacobi scale diag dx dy */
+static void energy_setup(const double* ucon, const double* Qe, double h) {
+  const size_t N = G.N;
+  const double dx = G.dx, dy = G.dy, g = PP.gamma_plasma;
+  OP.ucon = ucon;
+  OP.Qe = Qe;
+  OP.h = h;
+  free(OP.hh); free(OP.tdiag);
+  OP.hh = alloc(N);
+  OP.tdiag = alloc(N);
+  double c[8];
+  for (size_t n = 0; n < N; ++n) {
+    load8(Qe, n, c);
+    OP.hh[n] = caltotalenthalpy(c) * c[0] / ucon[n];
+  }
+  for (int i = 0; i < G.nx; i++)
+    for (int j = 0; j < G.ny; j++) {
+      size_t o = ID(i, j);
+      double h00 = OP.hh[o], hp0 = OP.hh[ID(i + 1, j)], hm0 = OP.hh[ID(i - 1, j)];
+      double h0p = OP.hh[ID(i, j + 1)], h0m = OP.hh[ID(i, j - 1)];
+      double hhp_x = 0.5 * (h00 + hp0), hhm_x = 0.5 * (h00 + hm0);
+      double hhp_y = 0.5 * (h00 + h0p), hhm_y = 0.5 * (h00 + h0m);
+      double diag = 1.0 + (g - 1.0) * h * h * ((hhp_x + hhm_x) / (dx * dx) + (hhp_y + hhm_y) / (dy * dy));
+      OP.tdiag[o] = diag * dx * dy;
+    }
+}
+static void pre_subsystem_energy(double* ucon, const double* Qe, double h) {
+  const size_t N = G.N;
+  const double dx = G.dx, dy = G.dy, g = PP.gamma_plasma;
+  energy_setup(ucon, Qe, h);
+  double *b = alloc(N), *E = alloc(N);
+  for (int i = 0; i < G.nx; i++)
+    for (int j = 0; j < G.ny; j++) {
+      size_t o = ID(i, j), e = ID(i + 1, j), w = ID(i - 1, j), n = ID(i, j + 1), s = ID(i, j - 1);
+      double hp0 = OP.hh[e], hm0 = OP.hh[w], h0p = OP.hh[n], h0m = OP.hh[s];
+      double U_star = ucon[4 * N + o] - 0.5 * h / dx * (hp0 * ucon[N + e] - hm0 * ucon[N + w]) -
+                      0.5 * h / dy * (h0p * ucon[2 * N + n] - h0m * ucon[2 * N + s]);
+      b[o] = U_star * dx * dy;
+      E[o] = ucon[4 * N + o];
+    }
+  gmres(E, b, energy_ax, energy_pc, (int)N);
+  memcpy(PL(ucon, 4), E, N * sizeof(double));
+  for (int i = 0; i < G.nx; i++)
+    for (int j = 0; j < G.ny; j++) {
+      size_t o = ID(i, j);
+      ucon[N + o] -= h * (1 / (2 * dx)) * (g - 1) * (E[ID(i + 1, j)] - E[ID(i - 1, j)]);
+      ucon[2 * N + o] -= h * (1 / (2 * dy)) * (g - 1) * (E[ID(i, j + 1)] - E[ID(i, j - 1)]);
+    }
+  free(b); free(E);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1440,10 +1555,13 @@ static void stage(int rks) {
   memcpy(G.Bsave, PL(G.cons, 5), 3 * N * sizeof(double));
   double* ws[4] = {G.wxL, G.wxR, G.wyL, G.wyR};
   for (int q = 0; q < 4; ++q) memcpy(PL(ws[q], 5), PL(G.cons, 5), 3 * N * sizeof(double));
-  flux_update(pressure_flux, G.cons, G.Qs, G.wxL, G.wxR, G.wyL, G.wyR, adt);
+  /* main.cpp:469-485 */
+  flux_update(PP.formula == EnergyFormula ? energy_flux : pressure_flux, G.cons, G.Qs, G.wxL, G.wxR, G.wyL, G.wyR,
+              adt);
   snapshot(SUB_PFLUX, rks);
 
-  pre_subsystem_pressure(G.cons, G.Qs, G.Qe, adt, rks);
+  if (PP.formula == EnergyFormula) pre_subsystem_energy(G.cons, G.Qe, adt);
+  else pre_subsystem_pressure(G.cons, G.Qs, G.Qe, adt, rks);
   snapshot(SUB_PRESSURE, rks);
 
   if (PP.magfield == StaggerCT) {
@@ -1498,7 +1616,8 @@ static void free_all(void) {
 
 int ora_setup(int nx, int ny, int rks, const ora_params* p) {
   if (nx < 4 || ny < 4 || rks < 1 || rks > MAXRK) return 1;
-  if (p->formula != PressureFormula || !p->GLF || p->U_update != DefinitionofU) return 2;
+  if ((p->formula != PressureFormula && p->formula != EnergyFormula) || !p->GLF || p->U_update != DefinitionofU)
+    return 2;
   free_all();
   G.nx = nx;
   G.ny = ny;
@@ -1667,6 +1786,9 @@ void ora_fn_operator(int op, const double* ucon8, const double* Qe8, const doubl
     OP.h = h;
     potential_gmax(Qs8);
     potential_ax(x, Ax);
+  } else if (op == 4) {
+    energy_setup(ucon8, Qe8, h);
+    energy_ax(x, Ax);
   }
 }
 
@@ -1693,11 +1815,13 @@ void ora_fn_substep(int sub, double h, int rks, double* ucon8, const double* Qe8
       reconstruct(Qe8, G.wxL, G.wxR, G.wyL, G.wyR);
       double* ws[4] = {G.wxL, G.wxR, G.wyL, G.wyR};
       for (int q = 0; q < 4; ++q) memcpy(PL(ws[q], 5), PL(ucon8, 5), 3 * N * sizeof(double));
-      flux_update(pressure_flux, ucon8, Qs8, G.wxL, G.wxR, G.wyL, G.wyR, h);
+      flux_update(PP.formula == EnergyFormula ? energy_flux : pressure_flux, ucon8, Qs8, G.wxL, G.wxR, G.wyL, G.wyR,
+                  h);
       break;
     }
     case 4:
-      pre_subsystem_pressure(ucon8, Qs8, Qe8, h, rks);
+      if (PP.formula == EnergyFormula) pre_subsystem_energy(ucon8, Qe8, h);
+      else pre_subsystem_pressure(ucon8, Qs8, Qe8, h, rks);
       break;
     case 5:
       if (PP.magfield == StaggerCT) staggered_ct_consistent(ucon8, bx, by, bxQs, byQs, Fx, Fy, h);

@@ -10,7 +10,8 @@ the reference sources by `make -C oracle ref`) on small analytic inputs:
                      TVDReconstruction, ShockDetector and the four matrix-free
                      operators of implicit_operators.cpp.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [case ...]
+(no arguments: every case; otherwise only the named step cases and/or "fn").
 """
 from __future__ import annotations
 
@@ -43,6 +44,12 @@ STEP_CASES = {
                             m_alfa=0.4275, m_b=0.0866), 1),
     "vortex16_energy_modify": (lambda: vortex(16), 2,
                                dict(recon="WENO5", magfield="StaggerCT", Energy_modify=1), 1),
+    # the energy formula: Energy_flux_Update + PreSubsystem_Energy (main.cpp:469-485)
+    "vortex16_energyformula": (lambda: vortex(16), 2, dict(CFG0, formula="EnergyFormula"), 2),
+    "sheet16_energyformula_rk3": (lambda: vortex_sheet(16), 3, dict(CFG1, formula="EnergyFormula"), 1),
+    "vortex14x12_energyformula_unstag_rk1": (lambda: vortex(14, 12), 1,
+                                             dict(recon="Minmod", magfield="UnStaggerCT",
+                                                  formula="EnergyFormula"), 2),
 }
 
 
@@ -93,6 +100,7 @@ def fn_case() -> None:
     out["op_pressure_L"] = s.operator(0, ucon, Qp, Q, h, x1)
     out["op_pressure_J"] = s.operator(1, ucon, Qp, Q, h, x1, pfreeze=pf, mbig=1.5e6)
     out["op_magnetic_B"] = s.operator(2, ucon, Qp, Q, h, x3)
+    out["op_energy"] = s.operator(4, ucon, Qp, Q, h, x1)
     sa = make_solver("ref", prob, 2, dict(CFG1))
     sa.set_scalars(0.02, h, 1.3, 1.1, 0.9, 0.8, 1.5)
     out["op_magnetic_A"] = sa.operator(3, ucon, Qp, Q, h, x3)
@@ -102,11 +110,15 @@ def fn_case() -> None:
 def main() -> None:
     if not RefSolver.available():
         raise SystemExit("oracle/_ref/libimexref.so missing: run `make -C oracle ref` first")
+    only = set(sys.argv[1:])
     for name, (factory, rks, settings, steps) in STEP_CASES.items():
+        if only and name not in only:
+            continue
         step_case(name, factory, rks, settings, steps)
         print("wrote", name)
-    fn_case()
-    print("wrote fn_vortex16x12")
+    if not only or "fn" in only:
+        fn_case()
+        print("wrote fn_vortex16x12")
 
 
 if __name__ == "__main__":

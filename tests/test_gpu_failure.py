@@ -41,10 +41,6 @@ def test_ct_variant_must_match_magfield():
     with pytest.raises(ix.ImexError) as err:
         sv.Staggered_CT_Consistent(0.01, 0)
     assert err.value.status == 1
-    with pytest.raises(ix.ImexError) as err:
-        sv.lib_energy = sv.lib.imex_PreSubsystem_Energy(sv.ctx, 0.01, 0)
-        sv._check(sv.lib_energy)
-    assert err.value.status == 2
     sv.close()
 
 

@@ -27,6 +27,8 @@ CASES = [
      dict(recon="VanLeer", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 3),
     ("random_field", lambda: random_field(48), 2,
      dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 4),
+    ("vortex_energy", lambda: vortex(48), 2,
+     dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula", GMREStol=1e-12), 5),
 ]
 
 

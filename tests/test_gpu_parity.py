@@ -67,6 +67,7 @@ def test_gpu_reconstruction_and_shock_detector_bit_exact():
     ("pressure_J", dict(recon="VanLeer", magfield="StaggerCT")),
     ("magnetic_B", dict(recon="VanLeer", magfield="StaggerCT")),
     ("magnetic_A", dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+    ("energy", dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula")),
 ])
 def test_gpu_operators_bit_exact(op, settings):
     g = load_golden("fn_vortex16x12.npz")
@@ -91,6 +92,8 @@ SUB_CASES = [
     ("vortex", (16, 16), 2, dict(recon="ENO3", magfield="StaggerCT", reconstate="PrimState")),
     ("vortex", (16, 16), 2, dict(recon="VanLeer", magfield="StaggerCT", eos_type="REDLICH_KWONG",
                                   m_alfa=0.4275, m_b=0.0866)),
+    ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula", GMREStol=1e-12)),
+    ("sheet", (24, 20), 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, formula="EnergyFormula")),
 ]
 
 
@@ -130,10 +133,11 @@ def test_gpu_substeps_match_oracle(kind, shape, rks, settings):
             assert rel(g.get_buffer("Fy"), S("magnetic", "Fy")) < 1e-12
         assert rel(g.get_buffer("cons")[5:], S("magnetic", "u_con")[5:]) < 1e-12
         g.set_buffer("cons", S("magnetic", "u_con"))
-        g.Pressure_flux_Update(adt, k)
-        exact(g.get_buffer("cons")[:5], S("pflux", "u_con")[:5], f"Pressure_flux stage {k}")
+        energy = settings.get("formula") == "EnergyFormula"
+        (g.Energy_flux_Update if energy else g.Pressure_flux_Update)(adt, k)
+        exact(g.get_buffer("cons")[:5], S("pflux", "u_con")[:5], f"second flux stage {k}")
         g.set_buffer("cons", S("pflux", "u_con"))
-        g.PreSubsystem_Pressure(adt, k)
+        (g.PreSubsystem_Energy if energy else g.PreSubsystem_Pressure)(adt, k)
         out = g.get_buffer("cons")
         for q in (1, 2, 4):
             assert rel(out[q], S("pressure", "u_con")[q]) < 1e-12, (k, q)

@@ -56,6 +56,7 @@ def test_port_reproduces_reference_golden_functions():
         s.operator(1, g["ucon"], g["Q"], g["Qs"], h, g["x1"], pfreeze=g["pfreeze"], mbig=float(g["mbig"])),
         g["op_pressure_J"])
     np.testing.assert_array_equal(s.operator(2, g["ucon"], g["Q"], g["Qs"], h, g["x3"]), g["op_magnetic_B"])
+    np.testing.assert_array_equal(s.operator(4, g["ucon"], g["Q"], g["Qs"], h, g["x1"]), g["op_energy"])
     np.testing.assert_array_equal(s.operator(3, g["ucon"], g["Q"], g["Qs"], h, g["x3"]), g["op_magnetic_A"])
 
 
@@ -67,6 +68,8 @@ LIVE_CASES = [
     ("sheet", 18, 2, dict(recon="WENO5", magfield="PotentialA", add_bvisc=0, PressureSolver="no_correction"), 1),
     ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", caltimestep="Fullydt"), 2),
     ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", add_pvisc="AlfvenSpeedp"), 1),
+    ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula"), 2),
+    ("sheet", 18, 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, formula="EnergyFormula"), 1),
 ]
 
 
@@ -112,7 +115,7 @@ def test_port_matches_live_reference_legacy_ct():
 def test_port_rejects_unsupported_configurations():
     prob = vortex(8)
     with pytest.raises(RuntimeError):
-        make_solver("port", prob, 2, dict(formula="EnergyFormula"))
+        make_solver("port", prob, 2, dict(U_update="ConservationofU"))
     with pytest.raises(RuntimeError):
         make_solver("port", prob, 2, dict(GLF=0))
 
