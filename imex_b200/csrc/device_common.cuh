@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include "dual.cuh"
 #include "imex_internal.h"
 
 namespace imex {
@@ -27,102 +28,119 @@ __device__ __forceinline__ long long cid(const DevParams& P, int i, int j) {
 }
 
 // ---------------------------------------------------------------- EOS
+// The per-cell physics below is templated on its scalar type S: double in the
+// forward kernels (the operations and their order are the reference's), Dual<L>
+// (dual.cuh) when the adjoint differentiates a cell function.
 // Redlich-Kwong thermal/caloric EOS and its Newton inversions, config.hpp:130-173.
-__device__ inline double rk_T_from_rho_p(const DevParams& P, double rho, double p) {
-  const double v = 1.0 / rho;
-  double T_old, T_new = (1.0 / rho - P.m_b) * (p + P.m_alfa * rho * rho) / P.m_R;
+template <class S>
+__device__ inline S rk_T_from_rho_p(const DevParams& P, S rho, S p) {
+  const S v = 1.0 / rho;
+  S T_old, T_new = (1.0 / rho - P.m_b) * (p + P.m_alfa * rho * rho) / P.m_R;
   int it = 0;
   do {
     T_old = T_new;
-    double f = P.m_R * T_old / (v - P.m_b) - P.m_alfa / sqrt(T_old) / v / (v + P.m_b) - p;
-    double df = P.m_R / (v - P.m_b) + 0.5 * P.m_alfa / T_old / sqrt(T_old) / v / (v + P.m_b);
+    S f = P.m_R * T_old / (v - P.m_b) - P.m_alfa / sqrt(T_old) / v / (v + P.m_b) - p;
+    S df = P.m_R / (v - P.m_b) + 0.5 * P.m_alfa / T_old / sqrt(T_old) / v / (v + P.m_b);
     T_new = T_old - f / df;
   } while (fabs(T_new - T_old) / fabs(T_old) > 1e-14 && ++it < kEosNewtonCap);
   if (it >= kEosNewtonCap) d_eos_flag = 1;
   return T_new;
 }
-__device__ inline double rk_e_from_rho_p(const DevParams& P, double rho, double p) {
-  const double v = 1.0 / rho;
-  double T = rk_T_from_rho_p(P, rho, p);
-  double U = log(v / (v + P.m_b));
+template <class S>
+__device__ inline S rk_e_from_rho_p(const DevParams& P, S rho, S p) {
+  const S v = 1.0 / rho;
+  S T = rk_T_from_rho_p(P, rho, p);
+  S U = log(v / (v + P.m_b));
   return P.m_cv * T + 1.5 * P.m_alfa / P.m_b * U / sqrt(T);
 }
-__device__ inline double rk_p_from_rho_e(const DevParams& P, double rho, double e) {
-  const double v = 1.0 / rho;
-  double T_old, T_new = (e + rho * P.m_alfa) / P.m_cv;
+template <class S>
+__device__ inline S rk_p_from_rho_e(const DevParams& P, S rho, S e) {
+  const S v = 1.0 / rho;
+  S T_old, T_new = (e + rho * P.m_alfa) / P.m_cv;
   int it = 0;
-  const double U = log(v / (v + P.m_b));
+  const S U = log(v / (v + P.m_b));
   do {
     T_old = T_new;
-    double f = P.m_cv * T_old + 1.5 * P.m_alfa / P.m_b * U / sqrt(T_old) - e;
-    double df = P.m_cv - 0.75 * P.m_alfa / P.m_b * U / T_old / sqrt(T_old);
+    S f = P.m_cv * T_old + 1.5 * P.m_alfa / P.m_b * U / sqrt(T_old) - e;
+    S df = P.m_cv - 0.75 * P.m_alfa / P.m_b * U / T_old / sqrt(T_old);
     T_new = T_old - f / df;
   } while (fabs(T_new - T_old) / fabs(T_old) > 1e-14 && ++it < kEosNewtonCap);
   if (it >= kEosNewtonCap) d_eos_flag = 1;
-  double a = P.m_alfa / sqrt(T_new);
+  S a = P.m_alfa / sqrt(T_new);
   return P.m_R * T_new / (v - P.m_b) - a / v / (v + P.m_b);
 }
-__device__ inline double rk_sound(const DevParams& P, double rho, double p) {
-  const double v = 1.0 / rho;
-  double T = rk_T_from_rho_p(P, rho, p);
-  double U = log(v / (v + P.m_b));
-  double p_T = P.m_R / (v - P.m_b) + P.m_alfa / (2.0 * T * sqrt(T) * v * (v + P.m_b));
-  double e_T = P.m_cv - 0.75 * P.m_alfa / P.m_b * U / (T * sqrt(T));
-  double vmb = v - P.m_b, vpb = v + P.m_b;
-  double p_v = -P.m_R * T / (vmb * vmb) + P.m_alfa * (2.0 * v + P.m_b) / (sqrt(T) * v * v * (vpb * vpb));
-  double e_v = 1.5 * P.m_alfa / P.m_b * (1.0 / v - 1.0 / (v + P.m_b)) / sqrt(T);
-  double a2 = p / (rho * rho) * (p_T / e_T) + v * v * (e_v - e_T * (p_v / p_T));
+template <class S>
+__device__ inline S rk_sound(const DevParams& P, S rho, S p) {
+  const S v = 1.0 / rho;
+  S T = rk_T_from_rho_p(P, rho, p);
+  S U = log(v / (v + P.m_b));
+  S p_T = P.m_R / (v - P.m_b) + P.m_alfa / (2.0 * T * sqrt(T) * v * (v + P.m_b));
+  S e_T = P.m_cv - 0.75 * P.m_alfa / P.m_b * U / (T * sqrt(T));
+  S vmb = v - P.m_b, vpb = v + P.m_b;
+  S p_v = -P.m_R * T / (vmb * vmb) + P.m_alfa * (2.0 * v + P.m_b) / (sqrt(T) * v * v * (vpb * vpb));
+  S e_v = 1.5 * P.m_alfa / P.m_b * (1.0 / v - 1.0 / (v + P.m_b)) / sqrt(T);
+  S a2 = p / (rho * rho) * (p_T / e_T) + v * v * (e_v - e_T * (p_v / p_T));
   return sqrt(a2);
 }
 // unified EOS interface, config.hpp:176-198
-__device__ __forceinline__ double eos_p(const DevParams& P, double rho, double e) {
+template <class S>
+__device__ __forceinline__ S eos_p(const DevParams& P, S rho, S e) {
   return P.eos_type == IMEX_IDEAL_GAS ? (P.gamma - 1.0) * rho * e : rk_p_from_rho_e(P, rho, e);
 }
-__device__ __forceinline__ double eos_e(const DevParams& P, double rho, double p) {
+template <class S>
+__device__ __forceinline__ S eos_e(const DevParams& P, S rho, S p) {
   return P.eos_type == IMEX_IDEAL_GAS ? p / ((P.gamma - 1.0) * rho) : rk_e_from_rho_p(P, rho, p);
 }
-__device__ __forceinline__ double eos_a2(const DevParams& P, double rho, double p) {
-  double a = P.eos_type == IMEX_IDEAL_GAS ? sqrt(P.gamma * p / rho) : rk_sound(P, rho, p);
+template <class S>
+__device__ __forceinline__ S eos_a2(const DevParams& P, S rho, S p) {
+  S a = P.eos_type == IMEX_IDEAL_GAS ? sqrt(P.gamma * p / rho) : rk_sound(P, rho, p);
   return a * a;
 }
-__device__ __forceinline__ double eos_fast(const DevParams& P, double rho, double p, double Bn, double B2) {
-  double a2 = eos_a2(P, rho, p);
-  double t = a2 + B2 / rho;
-  double disc = t * t - 4.0 * a2 * Bn * Bn / rho;
+template <class S>
+__device__ __forceinline__ S eos_fast(const DevParams& P, S rho, S p, S Bn, S B2) {
+  S a2 = eos_a2(P, rho, p);
+  S t = a2 + B2 / rho;
+  S disc = t * t - 4.0 * a2 * Bn * Bn / rho;
   if (disc < 0) disc = 0;
   return sqrt(0.5 * (t + sqrt(disc)));
 }
 // V(p) = rho e(rho, p) and its slopes, config.hpp:206-239
-__device__ __forceinline__ double Vbase(const DevParams& P, double p, double rho) {
+template <class S>
+__device__ __forceinline__ S Vbase(const DevParams& P, S p, S rho) {
   return P.eos_type == IMEX_IDEAL_GAS ? p / (P.gamma - 1.0) : rho * rk_e_from_rho_p(P, rho, p);
 }
-__device__ __forceinline__ double Vbase_slope(const DevParams& P, double p, double rho) {
-  if (P.eos_type == IMEX_IDEAL_GAS) return 1.0 / (P.gamma - 1.0);
+template <class S>
+__device__ __forceinline__ S Vbase_slope(const DevParams& P, S p, S rho) {
+  if (P.eos_type == IMEX_IDEAL_GAS) return S(1.0 / (P.gamma - 1.0));
   const double d = 1e-8;
-  double ep = rk_e_from_rho_p(P, rho, p + d);
-  double em = rk_e_from_rho_p(P, rho, p - d);
+  S ep = rk_e_from_rho_p(P, rho, p + d);
+  S em = rk_e_from_rho_p(P, rho, p - d);
   return rho * (ep - em) / (2.0 * d);
 }
-__device__ __forceinline__ double V_mod(const DevParams& P, double Mbig, double p, double rho) {
+template <class S>
+__device__ __forceinline__ S V_mod(const DevParams& P, double Mbig, S p, S rho) {
   if (!P.floor_on) return Vbase(P, p, rho);
-  return (p >= P.p_floor) ? Vbase(P, p, rho) : Vbase(P, P.p_floor, rho) + Mbig * (p - P.p_floor);
+  return (p >= P.p_floor) ? Vbase(P, p, rho) : Vbase(P, S(P.p_floor), rho) + Mbig * (p - P.p_floor);
 }
-__device__ __forceinline__ double V_slope(const DevParams& P, double Mbig, double p, double rho) {
+template <class S>
+__device__ __forceinline__ S V_slope(const DevParams& P, double Mbig, S p, S rho) {
   if (!P.floor_on) return Vbase_slope(P, p, rho);
-  return (p >= P.p_floor) ? Vbase_slope(P, p, rho) : Mbig;
+  return (p >= P.p_floor) ? Vbase_slope(P, p, rho) : S(Mbig);
 }
 
 // ---------------------------------------------------------------- state
 // specific internal energy of a conserved state, reconstruction.cpp:291-304
-__device__ __forceinline__ double calecon(const double* c) {
-  double rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
-  double B2 = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
-  double v2 = vx * vx + vy * vy + vz * vz;
+template <class S>
+__device__ __forceinline__ S calecon(const S* c) {
+  S rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
+  S B2 = c[5] * c[5] + c[6] * c[6] + c[7] * c[7];
+  S v2 = vx * vx + vy * vy + vz * vz;
   return (c[4] - 0.5 * rho * v2 - 0.5 * B2) / rho;
 }
 // ini_con2pri, state.cpp:206-218
-__device__ __forceinline__ void con2pri(const DevParams& P, double* pri, const double* con) {
-  double e = calecon(con);
+template <class S>
+__device__ __forceinline__ void con2pri(const DevParams& P, S* pri, const S* con) {
+  S e = calecon(con);
   pri[0] = con[0];
   pri[1] = con[1] / con[0];
   pri[2] = con[2] / con[0];
@@ -133,15 +151,17 @@ __device__ __forceinline__ void con2pri(const DevParams& P, double* pri, const d
   pri[7] = con[7];
 }
 // pressure of a conserved state (pri[4] of con2pri)
-__device__ __forceinline__ double pressure_of(const DevParams& P, const double* con) {
+template <class S>
+__device__ __forceinline__ S pressure_of(const DevParams& P, const S* con) {
   return eos_p(P, con[0], calecon(con));
 }
 // ini_pri2con, state.cpp:220-240
-__device__ __forceinline__ void pri2con(const DevParams& P, double* con, const double* pri) {
-  double e = eos_e(P, pri[0], pri[4]);
-  double B2 = pri[5] * pri[5] + pri[6] * pri[6] + pri[7] * pri[7];
-  double v2 = pri[1] * pri[1] + pri[2] * pri[2] + pri[3] * pri[3];
-  double r = pri[0];
+template <class S>
+__device__ __forceinline__ void pri2con(const DevParams& P, S* con, const S* pri) {
+  S e = eos_e(P, pri[0], pri[4]);
+  S B2 = pri[5] * pri[5] + pri[6] * pri[6] + pri[7] * pri[7];
+  S v2 = pri[1] * pri[1] + pri[2] * pri[2] + pri[3] * pri[3];
+  S r = pri[0];
   con[0] = r;
   con[1] = r * pri[1];
   con[2] = r * pri[2];
@@ -152,14 +172,16 @@ __device__ __forceinline__ void pri2con(const DevParams& P, double* con, const d
   con[7] = pri[7];
 }
 // calenthalpy, timestep.cpp:224-230: e + p / rho
-__device__ __forceinline__ double calenthalpy(const DevParams& P, const double* c) {
-  double e = calecon(c);
-  double p = eos_p(P, c[0], e);
+template <class S>
+__device__ __forceinline__ S calenthalpy(const DevParams& P, const S* c) {
+  S e = calecon(c);
+  S p = eos_p(P, c[0], e);
   return e + p / c[0];
 }
 // calkinetic, timestep.cpp:239-247
-__device__ __forceinline__ double calkinetic(const double* c) {
-  double rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
+template <class S>
+__device__ __forceinline__ S calkinetic(const S* c) {
+  S rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
   return 0.5 * rho * (vx * vx + vy * vy + vz * vz);
 }
 
@@ -172,9 +194,9 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ a, long lon
 // ---------------------------------------------------------------- reconstruction
 // One variable along one direction from the 5-point stencil (um2 .. up2):
 // left and right face values of the cell, reconstruction.cpp:38-266.
-__device__ inline void recon_1d(int scheme, double um2, double um1, double u0, double up1, double up2,
-                                double& wL, double& wR, bool vortex_central) {
-  double sR = up1 - u0, sL = u0 - um1, c = 0.0;
+template <class S>
+__device__ inline void recon_1d(int scheme, S um2, S um1, S u0, S up1, S up2, S& wL, S& wR, bool vortex_central) {
+  S sR = up1 - u0, sL = u0 - um1, c = 0.0;
   switch (scheme) {
     case IMEX_NoRecon:
       wL = u0;
@@ -191,44 +213,44 @@ __device__ inline void recon_1d(int scheme, double um2, double um1, double u0, d
     case IMEX_VanLeer:
       if (fabs(sR) < 1e-16) c = 0;
       else {
-        double r = sL / sR;
-        c = (r < 0) ? 0.0 : fmin(2 / (1 + r), (2 * r) / (1 + r));
+        S r = sL / sR;
+        c = (r < 0) ? S(0.0) : fmin(2 / (1 + r), (2 * r) / (1 + r));
       }
       wL = u0 - 0.5 * c * sL;
       wR = u0 + 0.5 * c * sR;
       break;
     case IMEX_ENO3: {
-      double q0L = -1.0 / 6.0 * um2 + 5.0 / 6.0 * um1 + 1.0 / 3.0 * u0;
-      double q1L = 1.0 / 3.0 * um1 + 5.0 / 6.0 * u0 - 1.0 / 6.0 * up1;
-      double q2L = 11.0 / 6.0 * u0 - 7.0 / 6.0 * up1 + 1.0 / 3.0 * up2;
-      double q0R = 1.0 / 3.0 * um2 - 7.0 / 6.0 * um1 + 11.0 / 6.0 * u0;
-      double q1R = -1.0 / 6.0 * um1 + 5.0 / 6.0 * u0 + 1.0 / 3.0 * up1;
-      double q2R = 1.0 / 3.0 * u0 + 5.0 / 6.0 * up1 - 1.0 / 6.0 * up2;
-      double d1 = fabs(u0 - um1), d2 = fabs(up1 - u0);
+      S q0L = -1.0 / 6.0 * um2 + 5.0 / 6.0 * um1 + 1.0 / 3.0 * u0;
+      S q1L = 1.0 / 3.0 * um1 + 5.0 / 6.0 * u0 - 1.0 / 6.0 * up1;
+      S q2L = 11.0 / 6.0 * u0 - 7.0 / 6.0 * up1 + 1.0 / 3.0 * up2;
+      S q0R = 1.0 / 3.0 * um2 - 7.0 / 6.0 * um1 + 11.0 / 6.0 * u0;
+      S q1R = -1.0 / 6.0 * um1 + 5.0 / 6.0 * u0 + 1.0 / 3.0 * up1;
+      S q2R = 1.0 / 3.0 * u0 + 5.0 / 6.0 * up1 - 1.0 / 6.0 * up2;
+      S d1 = fabs(u0 - um1), d2 = fabs(up1 - u0);
       if (d1 >= d2) {
-        double d3 = fabs(fabs(up2 - up1) - fabs(up1 - u0));
-        double d4 = fabs(fabs(up1 - u0) - fabs(u0 - um1));
+        S d3 = fabs(fabs(up2 - up1) - fabs(up1 - u0));
+        S d4 = fabs(fabs(up1 - u0) - fabs(u0 - um1));
         if (d3 >= d4) { wL = q1L; wR = q1R; } else { wL = q2L; wR = q2R; }
       } else {
-        double d3 = fabs(fabs(u0 - um1) - fabs(um1 - um2));
-        double d4 = fabs(fabs(up1 - u0) - fabs(u0 - um1));
+        S d3 = fabs(fabs(u0 - um1) - fabs(um1 - um2));
+        S d4 = fabs(fabs(up1 - u0) - fabs(u0 - um1));
         if (d4 >= d3) { wL = q0L; wR = q0R; } else { wL = q1L; wR = q1R; }
       }
       break;
     }
     default: {  // WENO5
-      double a0 = um2 - 2 * um1 + u0, b0 = um2 - 4 * um1 + 3 * u0;
-      double a1 = um1 - 2 * u0 + up1, b1 = um1 - up1;
-      double a2 = u0 - 2 * up1 + up2, b2 = 3 * u0 - 4 * up1 + up2;
-      double e0 = 1e-6 + (13.0 / 12.0 * (a0 * a0) + 1.0 / 4.0 * (b0 * b0));
-      double e1 = 1e-6 + (13.0 / 12.0 * (a1 * a1) + 1.0 / 4.0 * (b1 * b1));
-      double e2 = 1e-6 + (13.0 / 12.0 * (a2 * a2) + 1.0 / 4.0 * (b2 * b2));
-      double s0 = e0 * e0, s1 = e1 * e1, s2 = e2 * e2;
-      double q0 = -1.0 / 6.0 * um2 + 5.0 / 6.0 * um1 + 1.0 / 3.0 * u0;
-      double q1 = 1.0 / 3.0 * um1 + 5.0 / 6.0 * u0 - 1.0 / 6.0 * up1;
-      double q2 = 11.0 / 6.0 * u0 - 7.0 / 6.0 * up1 + 1.0 / 3.0 * up2;
-      double w0b = 3.0 / 10.0 / s0, w1b = 6.0 / 10.0 / s1, w2b = 1.0 / 10.0 / s2;
-      double sum = w0b + w1b + w2b;
+      S a0 = um2 - 2 * um1 + u0, b0 = um2 - 4 * um1 + 3 * u0;
+      S a1 = um1 - 2 * u0 + up1, b1 = um1 - up1;
+      S a2 = u0 - 2 * up1 + up2, b2 = 3 * u0 - 4 * up1 + up2;
+      S e0 = 1e-6 + (13.0 / 12.0 * (a0 * a0) + 1.0 / 4.0 * (b0 * b0));
+      S e1 = 1e-6 + (13.0 / 12.0 * (a1 * a1) + 1.0 / 4.0 * (b1 * b1));
+      S e2 = 1e-6 + (13.0 / 12.0 * (a2 * a2) + 1.0 / 4.0 * (b2 * b2));
+      S s0 = e0 * e0, s1 = e1 * e1, s2 = e2 * e2;
+      S q0 = -1.0 / 6.0 * um2 + 5.0 / 6.0 * um1 + 1.0 / 3.0 * u0;
+      S q1 = 1.0 / 3.0 * um1 + 5.0 / 6.0 * u0 - 1.0 / 6.0 * up1;
+      S q2 = 11.0 / 6.0 * u0 - 7.0 / 6.0 * up1 + 1.0 / 3.0 * up2;
+      S w0b = 3.0 / 10.0 / s0, w1b = 6.0 / 10.0 / s1, w2b = 1.0 / 10.0 / s2;
+      S sum = w0b + w1b + w2b;
       wL = w0b / sum * q0 + w1b / sum * q1 + w2b / sum * q2;
       q0 = 1.0 / 3.0 * um2 - 7.0 / 6.0 * um1 + 11.0 / 6.0 * u0;
       q1 = -1.0 / 6.0 * um1 + 5.0 / 6.0 * u0 + 1.0 / 3.0 * up1;
@@ -245,10 +267,11 @@ __device__ inline void recon_1d(int scheme, double um2, double um1, double u0, d
 
 // ---------------------------------------------------------------- explicit fluxes
 // convective flux along dir (0 = x, 1 = y), state.cpp:27-44 / 86-106
-__device__ __forceinline__ void f_conv(const double* c, int dir, double* f) {
-  double rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
-  double k = calkinetic(c);
-  double vn = dir == 0 ? vx : vy;
+template <class S>
+__device__ __forceinline__ void f_conv(const S* c, int dir, S* f) {
+  S rho = c[0], vx = c[1] / c[0], vy = c[2] / c[0], vz = c[3] / c[0];
+  S k = calkinetic(c);
+  S vn = dir == 0 ? vx : vy;
   f[0] = rho * vn;
   f[1] = rho * vx * vn;
   f[2] = rho * vy * vn;
@@ -256,9 +279,10 @@ __device__ __forceinline__ void f_conv(const double* c, int dir, double* f) {
   f[4] = k * vn;
 }
 // magnetic flux of the pressure formula, state.cpp:298-322
-__device__ __forceinline__ void magflux_p(const double* Q, int dir, double* f) {
-  double B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
-  double vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
+template <class S>
+__device__ __forceinline__ void magflux_p(const S* Q, int dir, S* f) {
+  S B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
+  S vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
   f[0] = 0;
   if (dir == 0) {
     f[1] = B2 * 0.5 - Q[5] * Q[5];
@@ -273,9 +297,10 @@ __device__ __forceinline__ void magflux_p(const double* Q, int dir, double* f) {
   }
 }
 // magnetic flux of the energy formula, MagneticFlux_x/y (state.cpp:272-296)
-__device__ __forceinline__ void magflux_e(const DevParams& P, const double* Q, int dir, double* f) {
-  double B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
-  double vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
+template <class S>
+__device__ __forceinline__ void magflux_e(const DevParams& P, const S* Q, int dir, S* f) {
+  S B2 = Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7];
+  S vB = (Q[1] * Q[5] + Q[2] * Q[6] + Q[3] * Q[7]) / Q[0];
   f[0] = 0;
   if (dir == 0) {
     f[1] = (2 - P.gamma) * B2 * 0.5 - Q[5] * Q[5];
@@ -290,36 +315,37 @@ __device__ __forceinline__ void magflux_e(const DevParams& P, const double* Q, i
   }
 }
 // the non-zero component (1 + dir) of f/g_KineticEnergyFlux (state.cpp:325-345)
-__device__ __forceinline__ double keflux(const DevParams& P, const double* Q) {
+template <class S>
+__device__ __forceinline__ S keflux(const DevParams& P, const S* Q) {
   return -(P.gamma - 1) * 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0];
 }
 // total enthalpy (E + p) / rho, caltotalenthalpy (timestep.cpp:232-237)
-__device__ __forceinline__ double caltotalenthalpy(const DevParams& P, const double* c) {
-  double pri[8];
+template <class S>
+__device__ __forceinline__ S caltotalenthalpy(const DevParams& P, const S* c) {
+  S pri[8];
   con2pri(P, pri, c);
   return (c[4] + pri[4]) / pri[0];
 }
 // Rusanov face flux of RusanovC_x/y (flux.cpp:329-406), Pressure_flux_x/y (flux.cpp:202-287)
 // or Energy_flux_x/y (flux.cpp:78-200): kForm 0, 1, 2
-template <int kForm>
-__device__ __forceinline__ void face_flux(const DevParams& P, const double* QL, const double* QR, int dir,
-                                          double a_max, double* F) {
-  double fL[5], fR[5];
+template <int kForm, class S>
+__device__ __forceinline__ void face_flux(const DevParams& P, const S* QL, const S* QR, int dir, S a_max, S* F) {
+  S fL[5], fR[5];
   f_conv(QL, dir, fL);
   f_conv(QR, dir, fR);
   if (kForm == 2) {  // convective (energy zeroed) + magnetic + kinetic-energy fluxes
     fL[4] = 0;
     fR[4] = 0;
-    double fb[5];
-    const double kl = keflux(P, QL), kr = keflux(P, QR);
+    S fb[5];
+    const S kl = keflux(P, QL), kr = keflux(P, QR);
     magflux_e(P, QL, dir, fb);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) fL[k] = fL[k] + fb[k] + (k == 1 + dir ? kl : 0.0);
+    for (int k = 0; k < 5; ++k) fL[k] = fL[k] + fb[k] + (k == 1 + dir ? kl : S(0.0));
     magflux_e(P, QR, dir, fb);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) fR[k] = fR[k] + fb[k] + (k == 1 + dir ? kr : 0.0);
+    for (int k = 0; k < 5; ++k) fR[k] = fR[k] + fb[k] + (k == 1 + dir ? kr : S(0.0));
   } else if (kForm == 1) {
-    double fb[5];
+    S fb[5];
     magflux_p(QL, dir, fb);
 #pragma unroll
     for (int k = 0; k < 5; ++k) fL[k] = fL[k] + fb[k];
@@ -330,7 +356,7 @@ __device__ __forceinline__ void face_flux(const DevParams& P, const double* QL, 
     fL[4] = 0;
     fR[4] = 0;
   }
-  double s = P.GLF ? a_max : fmax(fabs(QL[1 + dir] / QL[0]), fabs(QR[1 + dir] / QR[0]));
+  S s = P.GLF ? a_max : fmax(fabs(QL[1 + dir] / QL[0]), fabs(QR[1 + dir] / QR[0]));
 #pragma unroll
   for (int k = 0; k < 5; ++k) F[k] = 0.5 * (fL[k] + fR[k]) - 0.5 * s * (QR[k] - QL[k]);
 }

@@ -21,7 +21,7 @@
 #include <functional>
 #include <vector>
 
-#include "device_common.cuh"
+#include "cells.cuh"
 
 namespace imex {
 namespace {
@@ -1529,18 +1529,13 @@ __global__ void k_pressure_rhs(DevParams P, const DevScalars* __restrict__ sc, c
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const long long e = cid(P, i + 1, j), w = cid(P, i - 1, j), no = cid(P, i, j + 1), s = cid(P, i, j - 1);
-  const double u5 = ucon[5 * N + n], u6 = ucon[6 * N + n], u7 = ucon[7 * N + n];
-  const double B2 = u5 * u5 + u6 * u6 + u7 * u7;
-  const double h00 = hh[n], hp0 = hh[e], hm0 = hh[w], h0p = hh[no], h0m = hh[s];
-  const double p_star = ucon[4 * N + n] - 0.5 * B2;
-  const double kx = kin[n], ky = kin[N + n], kz = kin[2 * N + n];
-  const double* rvx = rv;
-  const double* rvy = rv + N;
-  b[n] = p_star - 0.5 * (kx * kx + ky * ky + kz * kz) / ucon[n] -
-         h * (1 / P.dx * (0.5 * (hp0 + h00) * 0.5 * (rvx[e] + rvx[n]) - 0.5 * (hm0 + h00) * 0.5 * (rvx[w] + rvx[n])) +
-              (1 / P.dy * (0.5 * (h0p + h00) * 0.5 * (rvy[no] + rvy[n]) - 0.5 * (h0m + h00) * 0.5 * (rvy[s] + rvy[n]))));
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[4] = {ucon, hh, rv, kin};
+  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+  double out[1];
+  pressure_rhs_cell<double>(P, h, nb, ld, out);
+  b[n] = out[0];
   if (p0) p0[n] = p0src[n];
 }
 // momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)
@@ -1550,21 +1545,27 @@ __global__ void k_momentum(DevParams P, const DevScalars* __restrict__ sc, const
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double pc = p[n];
-  double flux_xm = 0.5 * (p[cid(P, i - 1, j)] + pc), flux_xp = 0.5 * (pc + p[cid(P, i + 1, j)]);
-  ucon[N + n] = rv[n] - h / P.dx * (flux_xp - flux_xm);
-  double flux_ym = 0.5 * (p[cid(P, i, j - 1)] + pc), flux_yp = 0.5 * (pc + p[cid(P, i, j + 1)]);
-  ucon[2 * N + n] = rv[N + n] - h / P.dy * (flux_yp - flux_ym);
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[2] = {p, rv};
+  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+  double out[2];
+  momentum_cell<double>(P, h, nb, ld, out);
+  ucon[N + n] = out[0];
+  ucon[2 * N + n] = out[1];
 }
 // E = V(p) + KE + ME (DefinitionofU, imex_subsystems.cpp:286-302)
 __global__ void k_energy_define(DevParams P, const double* __restrict__ p, double* __restrict__ ucon) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const double r = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
-  const double b5 = ucon[5 * N + n], b6 = ucon[6 * N + n], b7 = ucon[7 * N + n];
-  ucon[4 * N + n] = Vbase(P, p[n], r) + 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / r + 0.5 * (b5 * b5 + b6 * b6 + b7 * b7);
+  long long nb[9];
+  nb[NB_C] = n;
+  const double* arr[2] = {p, ucon};
+  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+  double out[1];
+  energy_define_cell<double>(P, nb, ld, out);
+  ucon[4 * N + n] = out[0];
 }
 
 // total-enthalpy ratio hh = caltotalenthalpy(Qe) rho_e / rho (imex_subsystems.cpp:442-446)
@@ -1618,110 +1619,35 @@ __global__ void k_magnetic_rhs_B(DevParams P, const DevScalars* __restrict__ sc,
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double dx = P.dx, dy = P.dy;
-  const long long E = cid(P, i + 1, j), W = cid(P, i - 1, j), No = cid(P, i, j + 1), S = cid(P, i, j - 1);
-  const long long NE = cid(P, i + 1, j + 1), SE = cid(P, i + 1, j - 1), NW = cid(P, i - 1, j + 1),
-                  SW = cid(P, i - 1, j - 1);
-  auto U = [&](int k, long long m) { return __ldg(ucon + k * N + m); };
-  auto Q = [&](int k, long long m) { return __ldg(Qe + k * N + m); };
-  auto PE = [&](long long m) { return __ldg(pe + m); };
-  const double rho_p0 = 0.5 * (U(0, n) + U(0, E)), rho_m0 = 0.5 * (U(0, n) + U(0, W));
-  const double rho_0p = 0.5 * (U(0, n) + U(0, No)), rho_0m = 0.5 * (U(0, n) + U(0, S));
-  const double rvx_p0 = 0.5 * (U(1, n) + U(1, E)), rvx_m0 = 0.5 * (U(1, n) + U(1, W));
-  const double rvx_0p = 0.5 * (U(1, n) + U(1, No)), rvx_0m = 0.5 * (U(1, n) + U(1, S));
-  const double rvy_p0 = 0.5 * (U(2, n) + U(2, E)), rvy_m0 = 0.5 * (U(2, n) + U(2, W));
-  const double rvy_0p = 0.5 * (U(2, n) + U(2, No)), rvy_0m = 0.5 * (U(2, n) + U(2, S));
-  const double rvz_p0 = 0.5 * (U(3, n) + U(3, E)), rvz_m0 = 0.5 * (U(3, n) + U(3, W));
-  const double rvz_0p = 0.5 * (U(3, n) + U(3, No)), rvz_0m = 0.5 * (U(3, n) + U(3, S));
-  const double p_pp = 0.25 * (PE(n) + PE(E) + PE(No) + PE(NE));
-  const double p_pm = 0.25 * (PE(n) + PE(E) + PE(S) + PE(SE));
-  const double p_mp = 0.25 * (PE(n) + PE(W) + PE(No) + PE(NW));
-  const double p_mm = 0.25 * (PE(n) + PE(W) + PE(S) + PE(SW));
-  const double Bxn_p0 = 0.5 * (Q(5, n) + Q(5, E)), Bxn_m0 = 0.5 * (Q(5, n) + Q(5, W));
-  const double Bxn_0p = 0.5 * (Q(5, n) + Q(5, No)), Bxn_0m = 0.5 * (Q(5, n) + Q(5, S));
-  const double Byn_p0 = 0.5 * (Q(6, n) + Q(6, E)), Byn_m0 = 0.5 * (Q(6, n) + Q(6, W));
-  const double Byn_0p = 0.5 * (Q(6, n) + Q(6, No)), Byn_0m = 0.5 * (Q(6, n) + Q(6, S));
-  const double Bzn_p0 = 0.5 * (Q(7, n) + Q(7, E)), Bzn_m0 = 0.5 * (Q(7, n) + Q(7, W));
-  const double Bzn_0p = 0.5 * (Q(7, n) + Q(7, No)), Bzn_0m = 0.5 * (Q(7, n) + Q(7, S));
-  const double Bx_star =
-      Qs[5 * N + n] - (h / dy) * ((Bxn_0p / rho_0p * (rvy_0p - (h / dy) * (PE(No) - PE(n))) -
-                                   Byn_0p / rho_0p * (rvx_0p - h / dx * (p_pp - p_mp))) -
-                                  (Bxn_0m / rho_0m * (rvy_0m - (h / dy) * (PE(n) - PE(S))) -
-                                   Byn_0m / rho_0m * (rvx_0m - h / dx * (p_pm - p_mm))));
-  const double By_star =
-      Qs[6 * N + n] - (h / dx) * ((Byn_p0 / rho_p0 * (rvx_p0 - (h / dx) * (PE(E) - PE(n))) -
-                                   Bxn_p0 / rho_p0 * (rvy_p0 - h / dy * (p_pp - p_pm))) -
-                                  (Byn_m0 / rho_m0 * (rvx_m0 - (h / dx) * (PE(n) - PE(W))) -
-                                   Bxn_m0 / rho_m0 * (rvy_m0 - h / dy * (p_mp - p_mm))));
-  const double Bz1 = ((Bzn_p0 / rho_p0 * (rvx_p0 - h / dx * (PE(E) - PE(n))) - Bxn_p0 / rho_p0 * (rvz_p0)) -
-                      (Bzn_m0 / rho_m0 * (rvx_m0 - h / dx * (PE(n) - PE(W))) - Bxn_m0 / rho_m0 * (rvz_m0)));
-  const double Bz2 = ((Bzn_0p / rho_0p * (rvy_0p - h / dy * (PE(No) - PE(n))) - Byn_0p / rho_0p * (rvz_0p)) -
-                      (Bzn_0m / rho_0m * (rvy_0m - h / dy * (PE(n) - PE(S))) - Byn_0m / rho_0m * (rvz_0m)));
-  const double Bz_star = Qs[7 * N + n] - (h / dx) * Bz1 - (h / dy) * Bz2;
-  b[n] = Bx_star;
-  b[N + n] = By_star;
-  b[2 * N + n] = Bz_star;
-  x0[n] = Q(5, n);
-  x0[N + n] = Q(6, n);
-  x0[2 * N + n] = Q(7, n);
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[4] = {ucon, Qe, pe, Qs};
+  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+  double out[3];
+  mag_rhs_B_cell<double>(P, h, nb, ld, out);
+  b[n] = out[0];
+  b[N + n] = out[1];
+  b[2 * N + n] = out[2];
+  x0[n] = Qe[5 * N + n];
+  x0[N + n] = Qe[6 * N + n];
+  x0[2 * N + n] = Qe[7 * N + n];
 }
-// CollectMagFluxes (ct_flux.cpp:5-130), GLF
-__global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon, const double* __restrict__ Qe,
-                                     const double* __restrict__ pe, double* __restrict__ Fx,
-                                     double* __restrict__ Fy) {
+// CollectMagFluxes (ct_flux.cpp:5-130), GLF (collect_cell)
+__global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                                     const double* __restrict__ Qe, const double* __restrict__ pe,
+                                     double* __restrict__ Fx, double* __restrict__ Fy) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const double h = sc->h;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double dx = P.dx, dy = P.dy;
-  const long long E = cid(P, i + 1, j), W = cid(P, i - 1, j), No = cid(P, i, j + 1), S = cid(P, i, j - 1);
-  const long long NE = cid(P, i + 1, j + 1), SE = cid(P, i + 1, j - 1), NW = cid(P, i - 1, j + 1);
-  auto U = [&](int k, long long m) { return __ldg(ucon + k * N + m); };
-  auto Q = [&](int k, long long m) { return __ldg(Qe + k * N + m); };
-  auto PE = [&](long long m) { return __ldg(pe + m); };
-  const double rho_p0 = 0.5 * (U(0, n) + U(0, E)), rho_0p = 0.5 * (U(0, n) + U(0, No));
-  const double rvx_p0 = 0.5 * (U(1, n) + U(1, E)), rvy_p0 = 0.5 * (U(2, n) + U(2, E));
-  const double rvx_0p = 0.5 * (U(1, n) + U(1, No)), rvy_0p = 0.5 * (U(2, n) + U(2, No));
-  const double p_pp = 0.25 * (PE(n) + PE(E) + PE(No) + PE(NE));
-  const double p_pm = 0.25 * (PE(n) + PE(E) + PE(S) + PE(SE));
-  const double p_mp = 0.25 * (PE(n) + PE(W) + PE(No) + PE(NW));
-  const double Bxn_p0 = 0.5 * (Q(5, n) + Q(5, E)), Byn_p0 = 0.5 * (Q(6, n) + Q(6, E));
-  const double Bxn_0p = 0.5 * (Q(5, n) + Q(5, No)), Byn_0p = 0.5 * (Q(6, n) + Q(6, No));
-#define C4(f, k, a, b2, c) (0.25 * (f(k, n) + f(k, a) + f(k, b2) + f(k, c)))
-  const double Bxn_pp = C4(Q, 5, E, No, NE), Bxn_pm = C4(Q, 5, E, S, SE), Bxn_mp = C4(Q, 5, W, No, NW);
-  const double Byn_pp = C4(Q, 6, E, No, NE), Byn_pm = C4(Q, 6, E, S, SE), Byn_mp = C4(Q, 6, W, No, NW);
-  const double Bzn_pp = C4(Q, 7, E, No, NE), Bzn_pm = C4(Q, 7, E, S, SE), Bzn_mp = C4(Q, 7, W, No, NW);
-  const double Bx1_pp = C4(U, 5, E, No, NE), Bx1_pm = C4(U, 5, E, S, SE), Bx1_mp = C4(U, 5, W, No, NW);
-  const double By1_pp = C4(U, 6, E, No, NE), By1_pm = C4(U, 6, E, S, SE), By1_mp = C4(U, 6, W, No, NW);
-  const double Bz1_pp = C4(U, 7, E, No, NE), Bz1_pm = C4(U, 7, E, S, SE), Bz1_mp = C4(U, 7, W, No, NW);
-#undef C4
-  auto QU = [&](long long m) { return 0.5 * (Q(5, m) * U(5, m) + Q(6, m) * U(6, m) + Q(7, m) * U(7, m)); };
-  const double Fn_x = Byn_p0 / rho_p0 * (rvx_p0 - (h / dx) * (PE(E) - PE(n))) -
-                      Bxn_p0 / rho_p0 * (rvy_p0 - (h / dy) * (p_pp - p_pm));
-  const double By_1 = Byn_p0 / rho_p0 *
-                      (-1.0 / dx * ((QU(E) - Q(5, E) * U(5, E)) - (QU(n) - Q(5, n) * U(5, n))) +
-                       1.0 / dy * (Bxn_pp * By1_pp - Bxn_pm * By1_pm));
-  const double By_2 = Bxn_p0 / rho_p0 *
-                      (-1.0 / dx * (Q(5, E) * U(6, E) - Q(5, n) * U(6, n)) +
-                       1.0 / dy * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Byn_pp * By1_pp) -
-                                   (0.5 * (Bxn_pm * Bx1_pm + Byn_pm * By1_pm + Bzn_pm * Bz1_pm) - Byn_pm * By1_pm)));
-  const double nu_x = sc->B_max_x * dx;
-  const double Fdiff_x = -nu_x * (U(6, E) - U(6, n)) / dx;
-  Fx[n] = Fn_x + h * (By_1 + By_2) + Fdiff_x;
-  const double Fn_y = Bxn_0p / rho_0p * (rvy_0p - (h / dy) * (PE(No) - PE(n))) -
-                      Byn_0p / rho_0p * (rvx_0p - (h / dx) * (p_pp - p_mp));
-  const double Bx_1 = Bxn_0p / rho_0p *
-                      (1.0 / dx * (Bxn_pp * By1_pp - Bxn_mp * By1_mp) -
-                       1.0 / dy * ((QU(No) - Q(6, No) * U(6, No)) - (QU(n) - Q(6, n) * U(6, n))));
-  const double Bx_2 = Byn_0p / rho_0p *
-                      (1.0 / dx * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Bxn_pp * Bx1_pp) -
-                                   (0.5 * (Bxn_mp * Bx1_mp + Byn_mp * By1_mp + Bzn_mp * Bz1_mp) - Bxn_mp * Bx1_mp)) -
-                       1.0 / dy * (Q(6, No) * U(5, No) - Q(6, n) * U(5, n)));
-  const double nu_y = sc->B_max_y * dy;
-  const double Fdiff_y = -nu_y * (U(5, No) - U(5, n)) / dy;
-  Fy[n] = Fn_y + h * (Bx_1 + Bx_2) + Fdiff_y;
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[3] = {ucon, Qe, pe};
+  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+  const double bmax[2] = {sc->B_max_x, sc->B_max_y};
+  double out[2];
+  collect_cell<double>(P, sc->h, bmax, nb, ld, out);
+  Fx[n] = out[0];
+  Fy[n] = out[1];
 }
 
 // A** right-hand side (imex_subsystems.cpp:18-51), x0 = A

@@ -8,7 +8,7 @@
 #include <cstdio>
 #include <cstring>
 
-#include "device_common.cuh"
+#include "cells.cuh"
 
 namespace imex {
 
@@ -317,30 +317,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_flux_update(DevParams P, const 
 }
 
 // ---------------------------------------------------------------- constrained transport
-__device__ __forceinline__ double cell_ez(const double* __restrict__ u, long long N, long long m) {
-  double r = __ldg(u + m);
-  return __ldg(u + 2 * N + m) / r * __ldg(u + 5 * N + m) - __ldg(u + N + m) / r * __ldg(u + 6 * N + m);
-}
-// Corner EMF: CT_CornerAssemble (constrained_transport.cpp:147-164) of the face EMFs
-// ep0 = sx * fx, e0p = sy * fy and the cell EMF of u_con (ct_flux.cpp:165-168).
+// Corner EMF of u_con and the collected face fluxes (ct_corner_cell).
 __global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
                             double sy, const double* __restrict__ ucon, double* __restrict__ Epp) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const long long c00 = n, c10 = cid(P, i + 1, j), c01 = cid(P, i, j + 1), c11 = cid(P, i + 1, j + 1);
-  const double dx = P.dx, dy = P.dy;
-  double Ep0_00 = sx * __ldg(fx + c00), Ep0_01 = sx * __ldg(fx + c01);
-  double E0p_00 = sy * __ldg(fy + c00), E0p_10 = sy * __ldg(fy + c10);
-  double Et00 = cell_ez(ucon, N, c00), Et10 = cell_ez(ucon, N, c10), Et01 = cell_ez(ucon, N, c01),
-         Et11 = cell_ez(ucon, N, c11);
-  double bar = 0.25 * (Ep0_00 + Ep0_01 + E0p_00 + E0p_10);
-  double t1 = 0.5 * ((Ep0_00 - Et00) / (dx / 2.0) + (Ep0_01 - Et01) / (dx / 2.0));
-  double t2 = 0.5 * ((Et10 - Ep0_00) / (dx / 2.0) + (Et11 - Ep0_01) / (dx / 2.0));
-  double t3 = 0.5 * ((E0p_00 - Et00) / (dy / 2.0) + (E0p_10 - Et10) / (dy / 2.0));
-  double t4 = 0.5 * ((Et01 - E0p_00) / (dy / 2.0) + (Et11 - E0p_10) / (dy / 2.0));
-  Epp[n] = bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[3] = {fx, fy, ucon};
+  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+  double out[1];
+  ct_corner_cell<double>(P, sx, sy, nb, ld, out);
+  Epp[n] = out[0];
 }
 // Face update from the corner EMF and cell B = face average
 // (ct_flux.cpp:174-189, constrained_transport.cpp:128-141).  The neighbour faces
