@@ -92,6 +92,10 @@ class BatchTuning(C.Structure):
     _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double)]
 
 
+class AdjointOpts(C.Structure):
+    _fields_ = [("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("gmres_tol", C.c_double)]
+
+
 class KernelProfile(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double),
                 ("alg_bytes", C.c_double)]
@@ -137,6 +141,8 @@ _SIGS = {
     "imex_set_newton_state": (C.c_int, [C.c_void_p, _D, C.c_double]),
     "imex_apply_operator": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "imex_gmres": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
+    "imex_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(AdjointOpts), _D, _D, _D, _D, _D, _D]),
+    "imex_adjoint_vjp": (C.c_int, [C.c_void_p, C.POINTER(AdjointOpts), _D, _D, _D, _D, _D, _D]),
     "imex_gmres_noalloc": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
     "imex_batch_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.POINTER(C.c_void_p)]),
@@ -459,6 +465,32 @@ class Solver:
         st = SolveStats()
         self._check(self.lib.imex_gmres_noalloc(self.ctx, OP[op], _dp(x), _dp(b), C.byref(st)))
         return x, st.as_dict()
+
+    # ---- discrete adjoint
+    def adjoint_run(self, nsteps: int, rho_target, B_target, checkpoint_every: int = 10,
+                    gmres_tol: float = 0.0) -> tuple[float, np.ndarray, np.ndarray, np.ndarray]:
+        """Run nsteps from the current state and return J = 1/2|rho - rho_t|^2 + 1/2|B - B_t|^2
+        at the end with its gradient w.r.t. the initial primitive planes and face fields."""
+        o = AdjointOpts(nsteps, checkpoint_every, gmres_tol)
+        rt, Bt = _c(rho_target), _c(B_target)
+        J = C.c_double()
+        gp, gx, gy = self._planes(8), self._planes(1), self._planes(1)
+        self._check(self.lib.imex_adjoint_run(self.ctx, C.byref(o), _dp(rt), _dp(Bt), C.byref(J), _dp(gp),
+                                              _dp(gx), _dp(gy)))
+        return J.value, gp, gx, gy
+
+    def adjoint_vjp(self, nsteps: int, lam_cons, lam_bx=None, lam_by=None, checkpoint_every: int = 10,
+                    gmres_tol: float = 0.0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Run nsteps and pull the cotangent (lam_cons, lam_bx, lam_by) of the final state back
+        to the initial primitive planes and face fields."""
+        o = AdjointOpts(nsteps, checkpoint_every, gmres_tol)
+        lc = _c(lam_cons)
+        lx = _c(lam_bx) if lam_bx is not None else None
+        ly = _c(lam_by) if lam_by is not None else None
+        gp, gx, gy = self._planes(8), self._planes(1), self._planes(1)
+        self._check(self.lib.imex_adjoint_vjp(self.ctx, C.byref(o), _dp(lc), _dp(lx) if lx is not None else None,
+                                              _dp(ly) if ly is not None else None, _dp(gp), _dp(gx), _dp(gy)))
+        return gp, gx, gy
 
     def nested_newton(self, p0, b) -> tuple[np.ndarray, dict]:
         p = np.array(p0, dtype=np.float64, copy=True)

@@ -40,7 +40,7 @@ struct DevScalars {
 enum Family {
   F_PROLOGUE_REDUCE, F_CONS_FROM_PRIM, F_COMBINE, F_RECON, F_FLUX_CONV, F_FLUX_PRES, F_MAG_RHS,
   F_GMRES_MAG_B, F_GMRES_MAG_A, F_MAG_OUT, F_COLLECT_FLUX, F_PRES_SETUP, F_SHOCK, F_PRES_RHS, F_NEWTON,
-  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, F_GMRES_ENERGY, NFAM
+  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, F_GMRES_ENERGY, F_ADJOINT, NFAM
 };
 
 // Device-side counters and status of the implicit solves.
@@ -153,6 +153,8 @@ imex_status launch_divergence(imex_ctx* ctx, double* out4);
 imex_status launch_min_pressure(imex_ctx* ctx, double* pmin);
 imex_status launch_qe_derived(imex_ctx* ctx);
 imex_status launch_vslope(imex_ctx* ctx);
+// Butcher tableaux Ae, Ai of the IMEX-RK scheme (main.cpp:269-319)
+void tableau(int RKs, double ae[kMaxRK][kMaxRK], double ai[kMaxRK][kMaxRK]);
 
 // launchers implemented in kernels_solve.cu
 // the implicit step h of these sub-steps is read from device scalars (set_h or the stage combination)
@@ -191,6 +193,21 @@ struct BatchSolvePlan {
 imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out);
 imex_status batch_solve_run(BatchSolvePlan* plan, cudaStream_t stream, imex_ctx* err_ctx);
 void batch_solve_free(BatchSolvePlan* plan);
+
+// adjoint building blocks (kernels_solve.cu): the operators of one solve on explicit planes
+enum { ADJ_OP_PRESSURE_L = 0, ADJ_OP_PRESSURE_J = 1, ADJ_OP_MAGNETIC_B = 2 };
+struct AdjOp {
+  int kind;
+  const double *Qe, *rho;                  // magnetic B: Qe (8 planes), rho (one plane)
+  const double *hh, *eta, *vscale, *vdiag;  // pressure (vdiag: J mode)
+};
+// mu = A^{-T} lam by GMRES on the assembled transposed stencil AT (9 M^2 planes of scratch)
+imex_status adj_transpose_solve(imex_ctx* ctx, const AdjOp& a, double* AT, double* mu, const double* lam, double tol);
+// lam_q[q](cells) -= mu^T d(A x)/d coef_q for the staged coefficients (magnetic B: Qe Bx, By,
+// Bz, rho; pressure: hh, eta) and, if lam_visc, lam_visc[0..1] -= mu^T d(A x)/d (viscosity scalars)
+imex_status adj_coef_vjp(imex_ctx* ctx, const AdjOp& a, const double* x, const double* mu, double* const* lam_q,
+                         double* lam_visc);
+imex_status adj_apply(imex_ctx* ctx, const AdjOp& a, const double* x, double* Ax);
 
 // fixed device scratch of imex_gmres_noalloc (noalloc.cu) and the solve that uses it
 constexpr size_t kStaticScratchBytes = IMEX_NOALLOC_SCRATCH_BYTES;

@@ -16,6 +16,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -2553,6 +2554,272 @@ imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_bloc
 }
 imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b) { return newton_launch(ctx, p, b); }
 
+
+// ================================================================== adjoint building blocks
+// The operators evaluated on the 3x3 local tile of one cell, through the same tile-buffer
+// interface the solver kernels stage (halo 1), in any scalar type: with Dual<L> they give
+// columns of the operator's stencil (transposed solves) or of its dependence on the frozen
+// coefficients (coefficient adjoints).
+namespace {
+template <class Op, class T>
+struct LocalTile {
+  static constexpr int SX = 3, SY = 3, SN = 9;
+  T s[Op::M * SN];
+  T c[(Op::QT > 0 ? Op::QT : 1) * SN];
+  T p[1];
+};
+// coefficients of the nine cells around nb[4]; the vector from x (planes of N) or zero
+template <class Op, class T>
+__device__ __forceinline__ void local_fill(const Op& od, LocalTile<Op, T>& t, const long long* nb, const double* x,
+                                           long long N) {
+  constexpr int QC = Op::QT > 0 ? Op::QT : 1;
+  for (int q = 0; q < 9; ++q) {
+    T cq[QC];
+    od.coef(nb[q], cq);
+    for (int k = 0; k < Op::QT; ++k) t.c[k * 9 + q] = cq[k];
+    for (int k = 0; k < Op::M; ++k) t.s[k * 9 + q] = x ? T(x[k * N + nb[q]]) : T(0.0);
+  }
+}
+// viscosity scalars of the operators (cx, cy: magnetic; cvx, cvy: pressure)
+__device__ __forceinline__ void set_visc(MagneticBCoef& c, double a, double b) {
+  c.cx = a;
+  c.cy = b;
+}
+__device__ __forceinline__ void set_visc(PressureCoef& c, double a, double b) {
+  c.cvx = a;
+  c.cvy = b;
+}
+
+// Transposed stencil of a linear operator: AT[(o M + k') M + k] at cell c' = c + offset(o)
+// holds d(A x)[k](c) / d x[k'](c'), so (A^T mu)[k'](c') = sum_o sum_k AT[..](c') mu[k](c' - o).
+template <class Op>
+__global__ void k_adj_assemble_T(Op op, DevParams P, double* __restrict__ AT) {
+  constexpr int M = Op::M;
+  using D = Dual<M>;
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  op.bind();
+  const auto od = op.template as<D>();
+  using OD = typename std::remove_const<decltype(od)>::type;
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  LocalTile<OD, D> t;
+  local_fill(od, t, nb, nullptr, N);
+  for (int o = 0; o < 9; ++o) {
+    for (int kk = 0; kk < M; ++kk) t.s[kk * 9 + o].d[kk] = 1.0;
+    D out[M];
+    od.matvec(t, 0, 0, n, out);
+    for (int kk = 0; kk < M; ++kk)
+      for (int k = 0; k < M; ++k) AT[((long long)(o * M + kk) * M + k) * N + nb[o]] = out[k].d[kk];
+    for (int kk = 0; kk < M; ++kk) t.s[kk * 9 + o].d[kk] = 0.0;
+  }
+}
+
+// The assembled transposed operator in the solver-kernel interface (FP64 only), with the
+// Jacobi preconditioner of its diagonal.
+template <int M_>
+struct AssembledTOp {
+  using value_type = double;
+  static constexpr int M = M_, HALO = 1;
+  static constexpr int COEF = 9 * M_ * M_;
+  static constexpr int QT = 1;  // nothing staged; one dummy plane keeps the tile layout
+  static constexpr int PT = 0;
+  static constexpr int MIN_BLOCKS = 2;
+  const double* AT;
+  long long N;
+  __device__ __forceinline__ void bind() {}
+  template <class U>
+  __device__ __forceinline__ AssembledTOp as() const {
+    return *this;
+  }
+  __device__ __forceinline__ void coef(long long, double* q) const { q[0] = 0.0; }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB&, int, int) const {}
+  template <class TB>
+  __device__ __forceinline__ void matvec(const TB& tb, int lx, int ly, long long c, double* out) const {
+    const int o0 = (ly + 1) * TB::SX + lx + 1;
+#pragma unroll
+    for (int kk = 0; kk < M; ++kk) out[kk] = 0.0;
+#pragma unroll
+    for (int o = 0; o < 9; ++o) {
+      const int src = o0 - (o % 3 - 1) - (o / 3 - 1) * TB::SX;
+#pragma unroll
+      for (int kk = 0; kk < M; ++kk)
+#pragma unroll
+        for (int k = 0; k < M; ++k) out[kk] += __ldg(AT + ((long long)(o * M + kk) * M + k) * N + c) * tb.s[k * TB::SN + src];
+    }
+  }
+  __device__ __forceinline__ void precond(long long c, double* v) const {
+#pragma unroll
+    for (int k = 0; k < M; ++k) v[k] = v[k] / __ldg(AT + ((long long)(4 * M + k) * M + k) * N + c);
+  }
+};
+
+// coefficient adjoint: lam_q(c + o) -= sum_k mu[k](c) d(A x)[k](c) / d coef_q(c + o), at fixed x
+struct LamPlanes {
+  double* p[4];
+};
+template <class Op>
+__global__ void k_adj_coef_vjp(Op op, DevParams P, const double* __restrict__ x, const double* __restrict__ mu,
+                               LamPlanes lam) {
+  constexpr int M = Op::M, QT = Op::QT;
+  using D = Dual<QT>;
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  op.bind();
+  const auto od = op.template as<D>();
+  using OD = typename std::remove_const<decltype(od)>::type;
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  LocalTile<OD, D> t;
+  local_fill(od, t, nb, x, N);
+  double m[M];
+  for (int k = 0; k < M; ++k) m[k] = mu[k * N + n];
+  for (int o = 0; o < 9; ++o) {
+    for (int q = 0; q < QT; ++q) t.c[q * 9 + o].d[q] = 1.0;
+    D out[M];
+    od.matvec(t, 0, 0, n, out);
+    for (int q = 0; q < QT; ++q) {
+      double s = 0.0;
+      for (int k = 0; k < M; ++k) s += m[k] * out[k].d[q];
+      if (s != 0.0 && lam.p[q]) atomicAdd(lam.p[q] + nb[o], -s);
+    }
+    for (int q = 0; q < QT; ++q) t.c[q * 9 + o].d[q] = 0.0;
+  }
+}
+// viscosity-scalar adjoint: the operators are affine in their two viscosity scalars, so
+// d(A x)/d c = A x |(c=1) - A x |(c=0); lam2[0..1] -= sum_cells mu . d(A x)/d c
+template <class Op>
+__global__ void k_adj_visc_vjp(Op op, DevParams P, const double* __restrict__ x, const double* __restrict__ mu,
+                               double* __restrict__ lam2) {
+  constexpr int M = Op::M;
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double sx = 0.0, sy = 0.0;
+  if (n < N) {
+    op.bind();
+    long long nb[9];
+    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    LocalTile<Op, double> t;
+    local_fill(op, t, nb, x, N);
+    Op o0 = op, ox = op, oy = op;
+    set_visc(o0, 0.0, 0.0);
+    set_visc(ox, 1.0, 0.0);
+    set_visc(oy, 0.0, 1.0);
+    double a0[M], ax[M], ay[M];
+    o0.matvec(t, 0, 0, n, a0);
+    ox.matvec(t, 0, 0, n, ax);
+    oy.matvec(t, 0, 0, n, ay);
+    for (int k = 0; k < M; ++k) {
+      const double m = mu[k * N + n];
+      sx += m * (ax[k] - a0[k]);
+      sy += m * (ay[k] - a0[k]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (sx != 0.0) atomicAdd(lam2, -sx);
+    if (sy != 0.0) atomicAdd(lam2 + 1, -sy);
+  }
+}
+
+template <class Op>
+imex_status adj_op_dispatch(imex_ctx* ctx, const AdjOp& a, Op* out);
+template <>
+imex_status adj_op_dispatch(imex_ctx* ctx, const AdjOp& a, MagneticBOp* out) {
+  MagneticBOp o = make_magB_op(ctx);
+  o.Qe = a.Qe;
+  o.rho = a.rho;
+  *out = o;
+  return IMEX_OK;
+}
+template <>
+imex_status adj_op_dispatch(imex_ctx* ctx, const AdjOp& a, PressureOp* out) {
+  PressureOp o = make_pressure_op(ctx);
+  o.hh = a.hh;
+  o.eta = a.eta;
+  o.rho = a.rho;
+  o.vscale = a.vscale;
+  o.vdiag = a.vdiag;
+  o.jac = a.kind == ADJ_OP_PRESSURE_J;
+  *out = o;
+  return IMEX_OK;
+}
+
+template <class Op, int M>
+imex_status adj_transpose_solve_op(imex_ctx* ctx, const AdjOp& a, double* AT, double* mu, const double* lam,
+                                   double tol) {
+  Op op;
+  adj_op_dispatch(ctx, a, &op);
+  const DevParams& P = ctx->P;
+  const int nb = blocks_for(P.N);
+  k_adj_assemble_T<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, AT);
+  LAUNCH_CHECK(ctx, "k_adj_assemble_T");
+  cudaError_t e = cudaMemsetAsync(mu, 0, (size_t)M * P.N * sizeof(double), ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "adjoint initial guess");
+  AssembledTOp<M> T{};
+  T.AT = AT;
+  T.N = P.N;
+  const Tiling TL = make_tiling(ctx->nx, ctx->ny);
+  auto kern = k_gmres<AssembledTOp<M>>;
+  const int nblk = coop_blocks<AssembledTOp<M>>(ctx, (const void*)kern, TL);
+  GmresWork g = make_work(ctx, TL, nblk, F_ADJOINT);
+  g.tol = tol;
+  g.tol_abs = 0.0;
+  prof_begin(ctx);
+  imex_status s = launch_coop<AssembledTOp<M>>(ctx, kern, nblk, T, g, mu, lam);
+  prof_end(ctx, F_ADJOINT, 0.0, 3);
+  return s;
+}
+template <class Op>
+imex_status adj_coef_vjp_op(imex_ctx* ctx, const AdjOp& a, const double* x, const double* mu, double* const* lam_q,
+                            double* lam_visc) {
+  Op op;
+  adj_op_dispatch(ctx, a, &op);
+  const DevParams& P = ctx->P;
+  const int nb = blocks_for(P.N);
+  LamPlanes L{};
+  for (int q = 0; q < Op::QT && q < 4; ++q) L.p[q] = lam_q[q];
+  k_adj_coef_vjp<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, x, mu, L);
+  LAUNCH_CHECK(ctx, "k_adj_coef_vjp");
+  if (lam_visc) {
+    k_adj_visc_vjp<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, x, mu, lam_visc);
+    LAUNCH_CHECK(ctx, "k_adj_visc_vjp");
+  }
+  ctx->kernel_launches += lam_visc ? 2 : 1;
+  return IMEX_OK;
+}
+}  // namespace
+
+imex_status adj_transpose_solve(imex_ctx* ctx, const AdjOp& a, double* AT, double* mu, const double* lam, double tol) {
+  if (a.kind == ADJ_OP_MAGNETIC_B) return adj_transpose_solve_op<MagneticBOp, 3>(ctx, a, AT, mu, lam, tol);
+  return adj_transpose_solve_op<PressureOp, 1>(ctx, a, AT, mu, lam, tol);
+}
+imex_status adj_coef_vjp(imex_ctx* ctx, const AdjOp& a, const double* x, const double* mu, double* const* lam_q,
+                         double* lam_visc) {
+  if (a.kind == ADJ_OP_MAGNETIC_B) return adj_coef_vjp_op<MagneticBOp>(ctx, a, x, mu, lam_q, lam_visc);
+  return adj_coef_vjp_op<PressureOp>(ctx, a, x, mu, lam_q, lam_visc);
+}
+imex_status adj_apply(imex_ctx* ctx, const AdjOp& a, const double* x, double* Ax) {
+  Tiling T = make_tiling(ctx->nx, ctx->ny);
+  int nb = T.ntiles < ctx->max_blocks ? T.ntiles : ctx->max_blocks;
+  if (a.kind == ADJ_OP_MAGNETIC_B) {
+    MagneticBOp o;
+    adj_op_dispatch(ctx, a, &o);
+    launch_apply(ctx, o, nb, T, x, Ax);
+  } else {
+    PressureOp o;
+    adj_op_dispatch(ctx, a, &o);
+    launch_apply(ctx, o, nb, T, x, Ax);
+  }
+  LAUNCH_CHECK(ctx, "k_apply");
+  return IMEX_OK;
+}
 
 imex_status eos_flag_solve(imex_ctx* ctx, int* flag, bool reset) {
   cudaError_t e = cudaMemcpyFromSymbolAsync(&ctx->h_red[0], d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,

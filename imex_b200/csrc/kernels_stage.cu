@@ -629,7 +629,7 @@ imex_status launch_prim_from_cons(imex_ctx* ctx) {
 }
 
 // Butcher tableaux of main.cpp:269-319
-static void tableau(int RKs, double ae[kMaxRK][kMaxRK], double ai[kMaxRK][kMaxRK]) {
+void tableau(int RKs, double ae[kMaxRK][kMaxRK], double ai[kMaxRK][kMaxRK]) {
   for (int r = 0; r < kMaxRK; ++r)
     for (int c = 0; c < kMaxRK; ++c) ae[r][c] = ai[r][c] = 0.0;
   if (RKs == 1) {

@@ -289,6 +289,31 @@ imex_status imex_shock_detector(imex_ctx* ctx, const double* Q8, double* eta);
  * step is captured once into a CUDA graph and replayed.  Members must share the RK
  * order and the magnetic form; imex_batch_step synchronises and returns the worst
  * member status (imex_batch_last_error names the member). */
+/* ---- discrete adjoint
+ * Gradients of the final state of an nsteps run with respect to the initial fields, by the
+ * hand-written discrete adjoint of the step: every sub-step of main.cpp:335-561 in reverse,
+ * each implicit solve as a transposed matrix-free GMRES solve on the assembled transposed
+ * stencil, the nested Newton differentiated at its converged pressure through its active set
+ * (with the Cor.1 slope Mbig), the GLF maxima through the cells attaining them.  Checkpoints
+ * every `checkpoint_every` steps; each segment and each step are recomputed from them.
+ * Supported: PressureFormula, StaggerCT, ConsState, ideal gas, GLF, MaterialSpeedp or
+ * Noaddvisp, fixed_dt > 0, FP64, Energy_Modify off (else IMEX_ERR_UNSUPPORTED).
+ * The run starts from the context's current state and leaves it at the final state. */
+typedef struct imex_adjoint_opts {
+  int nsteps;            /* steps of the forward run (>= 1) */
+  int checkpoint_every;  /* steps between checkpoints (>= 1) */
+  double gmres_tol;      /* relative tolerance of the transposed solves (<= 0: 1e-13) */
+} imex_adjoint_opts;
+/* J = 1/2 |rho(T) - rho_target|^2 + 1/2 |B(T) - B_target|^2 (cell values, B_target three
+ * planes) and its gradient with respect to the initial primitive planes (8) and face fields.
+ * Host or device pointers; J, g_prim, g_bx, g_by may be NULL. */
+imex_status imex_adjoint_run(imex_ctx* ctx, const imex_adjoint_opts* opts, const double* rho_target,
+                             const double* B_target, double* J, double* g_prim, double* g_bx, double* g_by);
+/* The vector-Jacobian product for a given cotangent of the final conserved planes (8) and
+ * faces (lam_bx, lam_by may be NULL). */
+imex_status imex_adjoint_vjp(imex_ctx* ctx, const imex_adjoint_opts* opts, const double* lam_cons,
+                             const double* lam_bx, const double* lam_by, double* g_prim, double* g_bx, double* g_by);
+
 typedef struct imex_batch imex_batch;
 typedef struct imex_batch_tuning {
   int streams;          /* streams of the explicit sub-steps */
