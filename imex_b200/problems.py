@@ -205,3 +205,69 @@ def vortex_ensemble(members: int = 256, seed: int = 2026, smin: int = 64, smax: 
         side += side % 2
         out.append(vortex(side, kappa=kappa, mu=mu))
     return out
+
+
+@dataclass
+class PerturbedVortex:
+    """The vortex with a seeded smooth perturbation of v and A_z: 32 Fourier modes, the first
+    16 a streamfunction of the velocity (divergence-free), the last 16 the corner potential A_z
+    (faces from its exact differences, cell B = face average).  The initial fields are linear
+    in the mode amplitudes a: prim = base.prim + sum_m a_m dprim[m], likewise bx, by."""
+    base: Problem
+    dprim: np.ndarray  # (32, 4, ny, nx): the perturbed primitive planes PLANES = vx, vy, Bx, By
+    dbx: np.ndarray    # (32, ny, nx)
+    dby: np.ndarray
+    amplitudes: np.ndarray  # (32,) the nominal amplitudes
+    PLANES = (1, 2, 5, 6)
+
+    def problem(self, a: np.ndarray | None = None) -> Problem:
+        a = self.amplitudes if a is None else np.asarray(a, dtype=np.float64)
+        b = self.base
+        prim = b.prim.copy()
+        prim[list(self.PLANES)] += np.tensordot(a, self.dprim, axes=1)
+        bx = b.bx + np.tensordot(a, self.dbx, axes=1)
+        by = b.by + np.tensordot(a, self.dby, axes=1)
+        return Problem("perturbed_vortex", b.nx, b.ny, b.x0, b.x1, b.y0, b.y1, prim, np.ascontiguousarray(bx),
+                       np.ascontiguousarray(by), b.A.copy(), settings=dict(b.settings))
+
+
+def perturbed_vortex(n: int = 512, seed: int = 2026, amplitude: float = 1e-2, modes: int = 32,
+                     kmax: int = 3) -> PerturbedVortex:
+    """Adjoint workload: vortex(n) plus `modes` seeded Fourier modes (integer wavenumbers
+    |k_x|, |k_y| <= kmax on the periodic square, uniform phases) of the velocity streamfunction
+    (first half) and of A_z (second half), nominal amplitudes `amplitude` times N(0, 1)."""
+    base = vortex(n)
+    nx = ny = n
+    L = base.x1 - base.x0
+    dx, dy = base.dx, base.dy
+    rng = np.random.default_rng(seed)
+    xc = base.x0 + (np.arange(nx) + 0.5) * dx
+    yc = base.y0 + (np.arange(ny) + 0.5) * dy
+    X, Y = np.meshgrid(xc, yc)
+    XF, YF = np.meshgrid(base.x0 + (np.arange(nx) + 1.0) * dx, base.y0 + (np.arange(ny) + 1.0) * dy)
+    dprim = np.zeros((modes, 4, ny, nx))
+    dbx = np.zeros((modes, ny, nx))
+    dby = np.zeros((modes, ny, nx))
+    for m in range(modes):
+        while True:
+            kx, ky = rng.integers(-kmax, kmax + 1, size=2)
+            if kx or ky:
+                break
+        phase = rng.uniform(0.0, 2.0 * math.pi)
+        wx, wy = 2.0 * math.pi * kx / L, 2.0 * math.pi * ky / L
+        knorm = math.hypot(wx, wy)
+        if m < modes // 2:
+            # psi = cos(w.x + phase) / |w|: v = (d psi / dy, -d psi / dx)
+            s = -np.sin(wx * X + wy * Y + phase) / knorm
+            dprim[m, 0] = wy * s
+            dprim[m, 1] = -wx * s
+        else:
+            az = np.cos(wx * XF + wy * YF + phase) / (knorm * knorm)
+            bxm = (az - np.roll(az, 1, axis=0)) / dy
+            bym = -(az - np.roll(az, 1, axis=1)) / dx
+            dbx[m] = bxm
+            dby[m] = bym
+            dprim[m, 2] = 0.5 * (np.roll(bxm, 1, axis=1) + bxm)
+            dprim[m, 3] = 0.5 * (np.roll(bym, 1, axis=0) + bym)
+    amps = amplitude * rng.standard_normal(modes)
+    return PerturbedVortex(base, dprim, dbx, dby, amps)

@@ -1,0 +1,106 @@
+"""The adjoint workload: the vortex with a seeded 32-mode perturbation of v and A_z,
+J = 1/2 |rho(T) - rho_t|^2 + 1/2 |B(T) - B_t|^2 with targets from the unperturbed run,
+gradient with respect to the 32 amplitudes through the torch.autograd.Function of the test
+binding (tests/adjoint_torch.py), checked against central finite differences (h = 1e-6) of
+the GPU forward map and of the reference solver's own FP64 forward map at 64 x 64."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import imex_b200 as ix
+from adjoint_torch import ImexRun, RunSpec, initial_fields, misfit
+from imex_b200.problems import perturbed_vortex
+from oracle.bindings import RefSolver, make_solver
+
+pytestmark = pytest.mark.gpu
+
+SETTINGS = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-14, fixed_dt=0.02)
+H = 1e-6
+
+
+def _setup(n, nsteps, ckpt):
+    pv = perturbed_vortex(n)
+    spec = RunSpec(pv.base, 2, SETTINGS, nsteps, ckpt)
+    sv = ix.Solver.for_problem(pv.base, 2, SETTINGS)  # unperturbed run -> targets
+    for _ in range(nsteps):
+        sv.step()
+    c = sv.cons()
+    sv.close()
+    return pv, spec, c[0], c[5:8]
+
+
+def _gradient(pv, spec, rho_t, B_t):
+    a = torch.tensor(pv.amplitudes, requires_grad=True)
+    J = misfit(ImexRun.apply(*initial_fields(pv, a), spec), rho_t, B_t)
+    J.backward()
+    return J.detach().item(), a.grad.numpy().copy()
+
+
+def _J_gpu(pv, spec, rho_t, B_t, a):
+    with torch.no_grad():
+        return float(misfit(ImexRun.apply(*initial_fields(pv, torch.tensor(a)), spec), rho_t, B_t))
+
+
+def test_amplitude_gradient_matches_gpu_finite_differences():
+    pv, spec, rho_t, B_t = _setup(64, 10, 4)
+    J, g = _gradient(pv, spec, rho_t, B_t)
+    assert J > 0
+    fd = np.empty_like(g)
+    for m in range(len(g)):
+        e = np.zeros_like(g)
+        e[m] = H
+        fd[m] = (_J_gpu(pv, spec, rho_t, B_t, pv.amplitudes + e) - _J_gpu(pv, spec, rho_t, B_t, pv.amplitudes - e)) / (2 * H)
+    err = np.abs(g - fd)
+    print("J", J, "max |g|", np.abs(g).max(), "max rel err", (err / np.abs(fd).max()).max())
+    assert err.max() <= 1e-6 * np.abs(fd).max()
+    big = np.abs(fd) > 1e-2 * np.abs(fd).max()
+    assert (err[big] <= 1e-5 * np.abs(fd[big])).all()
+
+
+def test_full_size_gradient_matches_gpu_finite_differences():
+    """512 x 512, 50 steps, checkpoints every 10: the three largest amplitude derivatives."""
+    pv = perturbed_vortex(512)
+    settings = dict(SETTINGS, GMREStol=1e-14, fixed_dt=0.0025)
+    spec = RunSpec(pv.base, 2, settings, 50, 10)
+    sv = ix.Solver.for_problem(pv.base, 2, settings)
+    for _ in range(spec.nsteps):
+        sv.step()
+    c = sv.cons()
+    sv.close()
+    rho_t, B_t = c[0], c[5:8]
+    J, g = _gradient(pv, spec, rho_t, B_t)
+    for m in np.argsort(-np.abs(g))[:3]:
+        e = np.zeros_like(g)
+        e[m] = H
+        fd = (_J_gpu(pv, spec, rho_t, B_t, pv.amplitudes + e) - _J_gpu(pv, spec, rho_t, B_t, pv.amplitudes - e)) / (2 * H)
+        print(f"512^2 mode {m}: adjoint {g[m]:.12e} FD {fd:.12e} rel {abs(g[m] - fd) / abs(fd):.2e}")
+        assert abs(g[m] - fd) <= 1e-6 * abs(fd)
+
+
+@pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
+def test_amplitude_gradient_matches_reference_finite_differences():
+    """The reference's own FP64 solver (oracle/_ref) at 64 x 64: central differences of its J."""
+    pv, spec, _, _ = _setup(64, 6, 3)
+    ref0 = make_solver("ref", pv.base, 2, SETTINGS)
+    for _ in range(spec.nsteps):
+        ref0.step()
+    c = ref0.cons()
+    rho_t, B_t = c[0], c[5:8]
+    J, g = _gradient(pv, spec, rho_t, B_t)
+
+    def J_ref(a):
+        r = make_solver("ref", pv.problem(a), 2, SETTINGS)
+        for _ in range(spec.nsteps):
+            r.step()
+        cc = r.cons()
+        return 0.5 * np.sum((cc[0] - rho_t) ** 2) + 0.5 * np.sum((cc[5:8] - B_t) ** 2)
+
+    assert J == pytest.approx(J_ref(pv.amplitudes), rel=1e-9)
+    for m in np.argsort(-np.abs(g))[:4]:
+        e = np.zeros_like(g)
+        e[m] = H
+        fd = (J_ref(pv.amplitudes + e) - J_ref(pv.amplitudes - e)) / (2 * H)
+        print(f"mode {m}: adjoint {g[m]:.12e} reference FD {fd:.12e} rel {abs(g[m] - fd) / abs(fd):.2e}")
+        assert abs(g[m] - fd) <= 1e-6 * abs(fd)
