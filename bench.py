@@ -358,6 +358,49 @@ def ensemble_cpu_rate(probs, wl, max_seconds: float) -> dict:
                 sample=f"one time step of each of the {done} smallest members, one core")
 
 
+def adjoint_measure(n: int = 512, steps: int = 50, checkpoint_every: int = 10) -> dict:
+    """The differentiation form on its own workload: the 32-mode perturbed vortex, J = misfit
+    of rho and B against the unperturbed run, gradient w.r.t. the initial fields by the
+    checkpointed discrete adjoint; the forward run is timed beside it (device time), the
+    adjoint by wall clock (it includes its recomputations and host synchronisations)."""
+    import numpy as np
+    import torch
+    import imex_b200 as ix
+    from imex_b200.problems import perturbed_vortex
+
+    pv = perturbed_vortex(n)
+    settings = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12, fixed_dt=0.0025)
+    sv = ix.Solver.for_problem(pv.base, 2, settings)
+    for _ in range(steps):
+        sv.step()
+    c = sv.cons()
+    sv.close()
+    sv = ix.Solver.for_problem(pv.problem(), 2, settings)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sv.step()
+    torch.cuda.synchronize()
+    fwd = time.perf_counter() - t0
+    sv.close()
+    sv = ix.Solver.for_problem(pv.problem(), 2, settings)
+    sv.profile_enable(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, gp, gx, gy = sv.adjoint_run(steps, c[0], c[5:8], checkpoint_every=checkpoint_every)
+    adj = time.perf_counter() - t0
+    prof = sv.profile()
+    sv.close()
+    g = np.array([np.sum(gp[list(pv.PLANES)] * pv.dprim[m]) + np.sum(gx * pv.dbx[m]) + np.sum(gy * pv.dby[m])
+                  for m in range(len(pv.amplitudes))])
+    tot = sum(r["total_ms"] for r in prof) or 1.0
+    return {"workload": f"perturbed_vortex_{n} (32 modes of v and A_z, amplitude 1e-2)", "steps": steps,
+            "checkpoint_every": checkpoint_every, "forward_s": fwd, "adjoint_s": adj,
+            "adjoint_over_forward": adj / fwd, "J": J, "grad_amplitudes_norm": float(np.linalg.norm(g)),
+            "kernels": sorted(({"name": r["name"], "share": r["total_ms"] / tot} for r in prof),
+                              key=lambda r: -r["share"])[:8]}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,6 +411,7 @@ def main() -> int:
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-form measurement")
     ap.add_argument("--n", type=int, default=None, help="override the grid side (profiling cases)")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()
@@ -484,6 +528,12 @@ def main() -> int:
                     "max_rel_l2_per_field": max(errs), "rel_l2_per_field": errs}
 
     line = None
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            adjoint = adjoint_measure()
+        except Exception as exc:
+            adjoint = {"error": str(exc)}
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
@@ -508,6 +558,7 @@ def main() -> int:
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "accuracy": accuracy,
+            "adjoint": adjoint,
             "solver": {"gmres_iters": stats["gmres_iters"], "gmres_solves": stats["gmres_solves"],
                        "newton_iters": stats["newton_iters"], "refine_sweeps": stats["refine_sweeps"],
                        "status": stats["status"],

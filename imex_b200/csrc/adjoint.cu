@@ -256,9 +256,10 @@ void cv_arr(CellVjp& A, int a, const double* in, double* lam, int k0, int nk, in
 template <int L, class Fn>
 imex_status run_cell_vjp(imex_ctx* ctx, const CellVjp& A, Fn fn) {
   // unused arrays still need a readable base pointer for the value loads of the cell function
+  prof_begin(ctx);
   k_cell_vjp<L, Fn><<<ablocks(ctx->P.N), kAT, 0, ctx->stream>>>(ctx->P, A, fn);
-  ctx->kernel_launches += 1;
   ACHECK(ctx, "k_cell_vjp");
+  prof_end(ctx, F_ADJ_CELLS, 0.0, 1);
   return IMEX_OK;
 }
 
@@ -918,6 +919,7 @@ imex_status reverse_step(Adj& W) {
     const double h = S.sc.h, adt = S.sc.adt;
     const bool last = r == W.R - 1;
     // (1) stage derivative
+    prof_begin(ctx);
     k_adj_derivative<<<nb, kAT, 0, st>>>(P, r, adt, last ? W.lam_u : nullptr, last ? W.lam_bx : nullptr,
                                           last ? W.lam_by : nullptr, W.lam_Hs, W.lam_HsB, W.l5, W.lQs, W.lbx5, W.lby5,
                                           W.lbxQs, W.lbyQs);
@@ -925,6 +927,7 @@ imex_status reverse_step(Adj& W) {
     k_adj_ct_faces1<<<nb, kAT, 0, st>>>(P, W.l5, W.lbx5, W.lby5, W.lbxt, W.lbyt, W.lbxQs, W.lbyQs, W.l4);
     k_adj_ct_faces2<<<nb, kAT, 0, st>>>(P, h, W.lbxt, W.lbyt, W.lE);
     ACHECK(ctx, "adjoint CT faces");
+    prof_end(ctx, F_ADJ_LINEAR, 0.0, 3);
     // (3) CT corner EMF: inputs Fx, Fy, u_con after the pressure sub-system (= um with E of p)
     // u4 is not kept: its planes other than E equal um, and the corner reads none of E
     zero(W, W.lFx, N);
@@ -1024,9 +1027,11 @@ imex_status reverse_step(Adj& W) {
     if ((s = copy(W, ctx->Qe, S.Qe, 8 * N)) != IMEX_OK) return s;
     if ((s = launch_reconstruct(ctx, false)) != IMEX_OK) return s;
     if ((s = copy(W, W.w, ctx->w, 32 * N)) != IMEX_OK) return s;
+    prof_begin(ctx);
     k_adj_flux<1><<<nb, kAT, 0, st>>>(P, h, S.sc.a_max, W.w, S.u2, W.l3, W.lw, W.l2, W.lQs, W.dscal + 0);
     k_adj_recon<<<nb, kAT, 0, st>>>(P, S.Qe, W.lw, W.lQe, 5);
     ACHECK(ctx, "adjoint pressure flux");
+    prof_end(ctx, F_ADJ_FLUX, 0.0, 2);
     for (int k = 5; k < 8; ++k) k_axpy_planes<<<ablocks(N), kAT, 0, st>>>((long long)N, W.l2 + k * N, W.l3 + k * N, 1.0);
     // (6) CollectMagFluxes
     {
@@ -1070,9 +1075,11 @@ imex_status reverse_step(Adj& W) {
     k_axpy_planes<<<ablocks(3 * N), kAT, 0, st>>>((long long)(3 * N), W.lQs + 5 * N, W.mu, 1.0);
     // (9) convective flux: u1[0..4] = Qs - h div F(w(Qe), a_max)
     zero(W, W.lw, 32 * N);
+    prof_begin(ctx);
     k_adj_flux<0><<<nb, kAT, 0, st>>>(P, h, S.sc.a_max, W.w, S.u1, W.l1, W.lw, nullptr, W.lQs, W.dscal + 0);
     k_adj_recon<<<nb, kAT, 0, st>>>(P, S.Qe, W.lw, W.lQe, 5);
     ACHECK(ctx, "adjoint convective flux");
+    prof_end(ctx, F_ADJ_FLUX, 0.0, 2);
     // (10) p(Qe) of the combination
     {
       CellVjp A = cv_empty();
@@ -1089,7 +1096,7 @@ imex_status reverse_step(Adj& W) {
     k_adj_combine<<<nb, kAT, 0, st>>>(P, T, r, dt, W.lQe, W.lQs, W.lbxQs, W.lbyQs, W.lam_cons_n, W.lam_Hs, W.lam_bx_n,
                                        W.lam_by_n, W.lam_HsB);
     ACHECK(ctx, "adjoint combination");
-    ctx->kernel_launches += 40;
+    ctx->kernel_launches += 20;  // the linear helpers (axpy, shock, combine) outside the profiled families
   }
   // GLF maxima of the step prologue, from prim = con2pri(cons_n)
   {

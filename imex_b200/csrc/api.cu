@@ -24,7 +24,8 @@ static const char* kFamilyNames[NFAM] = {
     "magnetic_rhs", "gmres_magnetic_B", "gmres_magnetic_A", "magnetic_out", "collect_mag_fluxes",
     "pressure_setup", "shock_detector", "pressure_rhs", "nested_newton", "momentum", "energy_define",
     "constrained_transport", "stage_derivative", "gmax", "gmres_pressure", "apply_operator", "mixed_refine",
-    "gmres_energy", "adjoint"};
+    "gmres_energy", "adjoint_transposed_gmres", "adjoint_cells", "adjoint_flux", "adjoint_linear",
+    "adjoint_assemble"};
 const char* family_name(int fam) { return fam >= 0 && fam < NFAM ? kFamilyNames[fam] : "?"; }
 
 static cudaEvent_t prof_event(imex_ctx* ctx) {

@@ -40,7 +40,7 @@ struct DevScalars {
 enum Family {
   F_PROLOGUE_REDUCE, F_CONS_FROM_PRIM, F_COMBINE, F_RECON, F_FLUX_CONV, F_FLUX_PRES, F_MAG_RHS,
   F_GMRES_MAG_B, F_GMRES_MAG_A, F_MAG_OUT, F_COLLECT_FLUX, F_PRES_SETUP, F_SHOCK, F_PRES_RHS, F_NEWTON,
-  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, F_GMRES_ENERGY, F_ADJOINT, NFAM
+  F_MOMENTUM, F_ENERGY, F_CT, F_DERIVATIVE, F_GMAX, F_GMRES_PRES, F_APPLY, F_MIXED, F_GMRES_ENERGY, F_ADJOINT, F_ADJ_CELLS, F_ADJ_FLUX, F_ADJ_LINEAR, F_ADJ_ASSEMBLE, NFAM
 };
 
 // Device-side counters and status of the implicit solves.

@@ -2758,8 +2758,10 @@ imex_status adj_transpose_solve_op(imex_ctx* ctx, const AdjOp& a, double* AT, do
   adj_op_dispatch(ctx, a, &op);
   const DevParams& P = ctx->P;
   const int nb = blocks_for(P.N);
+  prof_begin(ctx);
   k_adj_assemble_T<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, AT);
   LAUNCH_CHECK(ctx, "k_adj_assemble_T");
+  prof_end(ctx, F_ADJ_ASSEMBLE, 0.0, 1);
   cudaError_t e = cudaMemsetAsync(mu, 0, (size_t)M * P.N * sizeof(double), ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "adjoint initial guess");
   AssembledTOp<M> T{};
@@ -2773,7 +2775,7 @@ imex_status adj_transpose_solve_op(imex_ctx* ctx, const AdjOp& a, double* AT, do
   g.tol_abs = 0.0;
   prof_begin(ctx);
   imex_status s = launch_coop<AssembledTOp<M>>(ctx, kern, nblk, T, g, mu, lam);
-  prof_end(ctx, F_ADJOINT, 0.0, 3);
+  prof_end(ctx, F_ADJOINT, 0.0, 2);
   return s;
 }
 template <class Op>
@@ -2785,13 +2787,14 @@ imex_status adj_coef_vjp_op(imex_ctx* ctx, const AdjOp& a, const double* x, cons
   const int nb = blocks_for(P.N);
   LamPlanes L{};
   for (int q = 0; q < Op::QT && q < 4; ++q) L.p[q] = lam_q[q];
+  prof_begin(ctx);
   k_adj_coef_vjp<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, x, mu, L);
   LAUNCH_CHECK(ctx, "k_adj_coef_vjp");
   if (lam_visc) {
     k_adj_visc_vjp<Op><<<nb, kThreads, 0, ctx->stream>>>(op, P, x, mu, lam_visc);
     LAUNCH_CHECK(ctx, "k_adj_visc_vjp");
   }
-  ctx->kernel_launches += lam_visc ? 2 : 1;
+  prof_end(ctx, F_ADJ_ASSEMBLE, 0.0, lam_visc ? 2 : 1);
   return IMEX_OK;
 }
 }  // namespace
