@@ -92,6 +92,15 @@ class BatchTuning(C.Structure):
     _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double)]
 
 
+class Diagnostics(C.Structure):
+    _fields_ = [("timestep", C.c_int), ("t", C.c_double), ("dt", C.c_double), ("div_error", C.c_double),
+                ("B_inf", C.c_double), ("dt_comp", C.c_double), ("emin", C.c_double), ("emin_x", C.c_double),
+                ("emin_y", C.c_double), ("mass", C.c_double), ("intE", C.c_double), ("magE_max", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class AdjointOpts(C.Structure):
     _fields_ = [("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("gmres_tol", C.c_double)]
 
@@ -141,6 +150,16 @@ _SIGS = {
     "imex_set_newton_state": (C.c_int, [C.c_void_p, _D, C.c_double]),
     "imex_apply_operator": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "imex_gmres": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
+    "imex_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diagnostics)]),
+    "imex_write_vtk": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "imex_write_fields_dat": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "imex_save_state_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "imex_load_state_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "imex_vtk_write_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_int, _D, _D]),
+    "imex_dat_write_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, _D]),
+    "imex_history_write_host": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int), _D]),
     "imex_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(AdjointOpts), _D, _D, _D, _D, _D, _D]),
     "imex_adjoint_vjp": (C.c_int, [C.c_void_p, C.POINTER(AdjointOpts), _D, _D, _D, _D, _D, _D]),
     "imex_gmres_noalloc": (C.c_int, [C.c_void_p, C.c_int, _D, _D, C.POINTER(SolveStats)]),
@@ -465,6 +484,25 @@ class Solver:
         st = SolveStats()
         self._check(self.lib.imex_gmres_noalloc(self.ctx, OP[op], _dp(x), _dp(b), C.byref(st)))
         return x, st.as_dict()
+
+    # ---- output formats and diagnostics
+    def diagnostics(self) -> dict:
+        """The per-step quantities of the reference's console and history files."""
+        d = Diagnostics()
+        self._check(self.lib.imex_diagnostics(self.ctx, C.byref(d)))
+        return d.as_dict()
+
+    def write_vtk(self, path: str, cycle: int = 0) -> None:
+        self._check(self.lib.imex_write_vtk(self.ctx, str(path).encode(), cycle))
+
+    def write_fields_dat(self, directory: str) -> None:
+        self._check(self.lib.imex_write_fields_dat(self.ctx, str(directory).encode()))
+
+    def save_state_file(self, path: str) -> None:
+        self._check(self.lib.imex_save_state_file(self.ctx, str(path).encode()))
+
+    def load_state_file(self, path: str) -> None:
+        self._check(self.lib.imex_load_state_file(self.ctx, str(path).encode()))
 
     # ---- discrete adjoint
     def adjoint_run(self, nsteps: int, rho_target, B_target, checkpoint_every: int = 10,

@@ -68,6 +68,20 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+DRIVER_SRC = os.path.join(HERE, "driver", "imex_run.cpp")
+DRIVER = os.path.join(HERE, "imex_run")
+
+
+def build_driver(force: bool = False) -> str:
+    """The time-marching driver executable (C++ over the C ABI), linked to the in-tree library."""
+    if not force and not _stale(DRIVER, [DRIVER_SRC, LIB, os.path.join(ROOT, "include", "imex_b200.h")]):
+        return DRIVER
+    cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), DRIVER_SRC,
+           "-L", HERE, "-limex_b200", "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build_oracles() -> None:
     """Build oracle/liboracle.so always, oracle/_ref when the reference sources exist."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "port"], check=True)
@@ -77,4 +91,5 @@ def build_oracles() -> None:
 
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose=True)
+    build_driver(force="--force" in sys.argv)
     build_oracles()

@@ -271,3 +271,43 @@ def perturbed_vortex(n: int = 512, seed: int = 2026, amplitude: float = 1e-2, mo
             dprim[m, 3] = 0.5 * (np.roll(bym, 1, axis=0) + bym)
     amps = amplitude * rng.standard_normal(modes)
     return PerturbedVortex(base, dprim, dbx, dby, amps)
+
+
+# ---- state files (the layout of imex_save_state_file / imex_load_state_file)
+# header: 8-byte magic, int32 version, nx, ny, timestep, then float64 t, prev_dt, dt, x0, x1,
+# y0, y1; then float64 planes prim (8), bx, by, A (3), each ny x nx with x fastest.
+STATE_MAGIC = b"IMEXSTAT"
+_STATE_HEADER = np.dtype([("magic", "S8"), ("version", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
+                          ("timestep", "<i4"), ("t", "<f8"), ("prev_dt", "<f8"), ("dt", "<f8"),
+                          ("x0", "<f8"), ("x1", "<f8"), ("y0", "<f8"), ("y1", "<f8")])
+
+
+def write_state_file(prob: Problem, path: str, t: float = 0.0, timestep: int = 0, prev_dt: float = 0.0) -> None:
+    """The initial state of a problem as a state file (the input of the imex_run driver)."""
+    h = np.zeros((), dtype=_STATE_HEADER)
+    h["magic"], h["version"], h["nx"], h["ny"], h["timestep"] = STATE_MAGIC, 1, prob.nx, prob.ny, timestep
+    h["t"], h["prev_dt"], h["dt"] = t, prev_dt, 0.0
+    h["x0"], h["x1"], h["y0"], h["y1"] = prob.x0, prob.x1, prob.y0, prob.y1
+    with open(path, "wb") as f:
+        f.write(h.tobytes())
+        for a in (prob.prim, prob.bx, prob.by, prob.A):
+            f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+
+
+def read_state_file(path: str) -> tuple[dict, np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+    """(header, prim, bx, by, A) of a state file."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    h = np.frombuffer(raw[:_STATE_HEADER.itemsize], dtype=_STATE_HEADER)[0]
+    if bytes(h["magic"]) != STATE_MAGIC:
+        raise ValueError(f"{path} is not a state file")
+    nx, ny = int(h["nx"]), int(h["ny"])
+    d = np.frombuffer(raw[_STATE_HEADER.itemsize:], dtype="<f8")
+    N = nx * ny
+    if d.size != 13 * N:
+        raise ValueError(f"{path}: expected {13 * N} values, found {d.size}")
+    prim = d[:8 * N].reshape(8, ny, nx)
+    bx, by = d[8 * N:9 * N].reshape(ny, nx), d[9 * N:10 * N].reshape(ny, nx)
+    A = d[10 * N:].reshape(3, ny, nx)
+    header = {n: (h[n].item() if n != "magic" else bytes(h[n])) for n in _STATE_HEADER.names}
+    return header, prim.copy(), bx.copy(), by.copy(), A.copy()

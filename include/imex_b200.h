@@ -289,6 +289,37 @@ imex_status imex_shock_detector(imex_ctx* ctx, const double* Q8, double* eta);
  * step is captured once into a CUDA graph and replayed.  Members must share the RK
  * order and the magnetic form; imex_batch_step synchronises and returns the worst
  * member status (imex_batch_last_error names the member). */
+/* ---- output formats and run diagnostics (main.cpp:560-721, output.cpp)
+ * The per-step quantities the reference prints and records after every step. */
+typedef struct imex_diagnostics_t {
+  int timestep;
+  double t, dt;
+  double div_error;  /* cal_divergence_error (imex_subsystems.cpp:630): face FV L2 for StaggerCT, else cell L2 */
+  double B_inf;      /* max |central div of cell B| (main.cpp:578-589) */
+  double dt_comp;    /* imex_dt / fully_dt (timestep.cpp:56-57) */
+  double emin, emin_x, emin_y;  /* min internal energy and its cell centre (main.cpp:562-573) */
+  double mass, intE;            /* integrals of rho and of the internal energy over the domain */
+  double magE_max;              /* max |B|^2 / 2 */
+} imex_diagnostics_t;
+imex_status imex_diagnostics(imex_ctx* ctx, imex_diagnostics_t* d);
+/* Legacy-VTK rectilinear grid of the current state: the reference's 13 cell fields (rho,
+ * mom_X/Y/Z, U, B_X/Y/Z, velX/Y/Z, p, B), node coordinates on the nx + 1 / ny + 1 cell faces,
+ * interior cells only, 17 significant digits. */
+imex_status imex_write_vtk(imex_ctx* ctx, const char* path, int cycle);
+/* The final-state field files RK_rho/vx/vy/E/p/Bx/By/Bz/v_mag.dat (and RK_T.dat for the
+ * Redlich-Kwong EOS) into `dir`: "x y value" per cell, x outer, full precision. */
+imex_status imex_write_fields_dat(imex_ctx* ctx, const char* dir);
+/* Binary state (primitive planes, faces, A, t, step counter, previous dt): a run loaded from
+ * it continues bit for bit. */
+imex_status imex_save_state_file(imex_ctx* ctx, const char* path);
+imex_status imex_load_state_file(imex_ctx* ctx, const char* path);
+/* The writers on host arrays (no GPU needed); "timestep value" lines for the histories. */
+int imex_vtk_write_host(const char* path, int nx, int ny, double x0, double y0, double dx, double dy, double t,
+                        int cycle, const double* cons8, const double* prim8);
+int imex_dat_write_host(const char* path, int nx, int ny, double x0, double y0, double dx, double dy,
+                        const double* plane);
+int imex_history_write_host(const char* path, int n, const int* steps, const double* values);
+
 /* ---- discrete adjoint
  * Gradients of the final state of an nsteps run with respect to the initial fields, by the
  * hand-written discrete adjoint of the step: every sub-step of main.cpp:335-561 in reverse,
