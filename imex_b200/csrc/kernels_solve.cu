@@ -876,7 +876,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
           for (int r = 0; r < FQ; ++r)
 #pragma unroll
             for (int m = 0; m < M; ++m) wv[r][m] = sj * ldv(AVj + m * N + c[r]);
-#pragma unroll 2
+#pragma unroll 4
           for (int i = 0; i <= j; ++i) {
             const double hij = S.H[i][j], si = S.sigma[i];
             const TS* Vi = Vp(i);
@@ -913,8 +913,22 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
             for (int m = 0; m < M; ++m) aw[r][m] = wc[r][m] = VT(0);
           }
         }
-        // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2; four basis vectors at a time
+        // slots: v_i.Aw -> i (i <= j), w.Aw -> j+1, w.w -> j+2; eight, then four basis vectors
+        // at a time (independent loads in flight)
         int i = 0;
+        for (; i + 7 <= j; i += 8) {
+          double d[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int r = 0; r < CPT; ++r)
+            if (in[r]) {
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int m = 0; m < M; ++m) d[u] += ldv(Vp(i + u) + m * N + cc[r]) * (double)aw[r][m];
+            }
+          wacc_add4(S.acc, i, *reinterpret_cast<double(*)[4]>(&d[0]));
+          wacc_add4(S.acc, i + 4, *reinterpret_cast<double(*)[4]>(&d[4]));
+        }
         for (; i + 3 <= j; i += 4) {
           double d[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
