@@ -217,10 +217,10 @@ __global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc,
 }
 
 // ---------------------------------------------------------------- reconstruction
-// TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes.
+// TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes,
+// PrimState (the ConsState form is k_reconstruct_var below).
 // nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
-template <bool kPrim>
-__global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
+__global__ void k_reconstruct_prim(DevParams P, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -232,21 +232,6 @@ __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double*
     iy[d] = cid(P, i, j + d - 2);
   }
   const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
-  if (!kPrim) {
-    for (int k = 0; k < nstore; ++k) {
-      const double* a = Q + k * N;
-      double xl, xr, yl, yr;
-      recon_1d(P.recon, __ldg(a + ix[0]), __ldg(a + ix[1]), __ldg(a + ix[2]), __ldg(a + ix[3]), __ldg(a + ix[4]), xl,
-               xr, false);
-      recon_1d(P.recon, __ldg(a + iy[0]), __ldg(a + iy[1]), __ldg(a + iy[2]), __ldg(a + iy[3]), __ldg(a + iy[4]), yl,
-               yr, vortex);
-      w[(0 * 8 + k) * N + n] = xl;
-      w[(1 * 8 + k) * N + n] = xr;
-      w[(2 * 8 + k) * N + n] = yl;
-      w[(3 * 8 + k) * N + n] = yr;
-    }
-    return;
-  }
   // PrimState: reconstruct primitive variables, convert each face state back (reconstruction.cpp:272-281)
   double px[5][8], py[5][8];
 #pragma unroll
@@ -270,6 +255,32 @@ __global__ void k_reconstruct(DevParams P, const double* __restrict__ Q, double*
     pri2con(P, c, outs[q]);
     for (int k = 0; k < nstore; ++k) w[(q * 8 + k) * N + n] = c[k];
   }
+}
+
+// ConsState reconstructs every conserved variable on its own (reconstruction.cpp:5-266), so
+// one thread per (cell, variable) pair: variable k = blockIdx.y.  The same recon_1d calls as a
+// per-cell loop over the variables, with a small per-thread working set and 5-8x the threads.
+__global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams P, const double* __restrict__ Q,
+                                                               double* __restrict__ w) {
+  const long long N = P.N;
+  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int k = blockIdx.y;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
+  const double* a = Q + k * N;
+  double v[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i + d - 2, j));
+  double xl, xr, yl, yr;
+  recon_1d(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
+#pragma unroll
+  for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i, j + d - 2));
+  recon_1d(P.recon, v[0], v[1], v[2], v[3], v[4], yl, yr, vortex);
+  w[(0 * 8 + k) * N + n] = xl;
+  w[(1 * 8 + k) * N + n] = xr;
+  w[(2 * 8 + k) * N + n] = yl;
+  w[(3 * 8 + k) * N + n] = yr;
 }
 
 // ---------------------------------------------------------------- flux updates
@@ -677,9 +688,9 @@ imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
   const int nread = ctx->P.reconstate == IMEX_PrimState ? 8 : nstore;
   prof_begin(ctx);
   if (ctx->P.reconstate == IMEX_PrimState)
-    k_reconstruct<true><<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
+    k_reconstruct_prim<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
   else
-    k_reconstruct<false><<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
+    k_reconstruct_var<<<dim3(blocks_for(ctx->P.N), nstore), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w);
   LAUNCH_CHECK(ctx, "k_reconstruct");
   prof_end(ctx, F_RECON, BYTES(nread + 4 * nstore), 1);
   return IMEX_OK;
@@ -712,8 +723,8 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
     k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
-    if (P.reconstate == IMEX_PrimState) k_reconstruct<true><<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
-    else k_reconstruct<false><<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
+    if (P.reconstate == IMEX_PrimState) k_reconstruct_prim<<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
+    else k_reconstruct_var<<<dim3(nb, 8), kThreads, 0, s>>>(P, ctx->cons, ctx->w);
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
     k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
