@@ -42,14 +42,21 @@ inline int ablocks(long long n) { return (int)((n + kAT - 1) / kAT); }
   } while (0)
 
 // ------------------------------------------------------------------ generic cell VJP
-// A cell function reads arrays a < kMaxArr through ld(a, k, m).  Array a is seeded on
-// planes [k0, k0 + nk) at the 3x3 neighbourhood (nofs = 9) or the cell itself (nofs = 1);
-// its adjoint accumulates into lam[a].  Scalars (at most 2) are seeded after the arrays.
-constexpr int kMaxArr = 4;
+// A cell function reads arrays a < kMaxArr through ld(a, k, m).  Array a is seeded on the
+// planes whose bits are set in pmask[a] and at the neighbours of the 3x3 neighbourhood whose
+// bits are set in mask[a] (bit o = neighbour nb[o]); its adjoint accumulates into lam[a].
+// The masks must cover every plane and neighbour the cell function reads of that array.
+// Scalars (at most 2) are seeded after the arrays.
+constexpr int kMaxArr = 5;
+constexpr unsigned OFS_C = 1u << NB_C;
+constexpr unsigned OFS_CROSS = OFS_C | (1u << NB_E) | (1u << NB_W) | (1u << NB_N) | (1u << NB_S);
+constexpr unsigned OFS_ALL = 0x1FFu;
+constexpr unsigned OFS_NO_SW = OFS_ALL & ~(1u << NB_SW);
 struct CellVjp {
   const double* in[kMaxArr];
   double* lam[kMaxArr];
-  int k0[kMaxArr], nk[kMaxArr], nofs[kMaxArr];
+  unsigned pmask[kMaxArr];  // seeded planes
+  unsigned mask[kMaxArr];   // seeded neighbours
   const double* lam_out[8];  // adjoint of each output (one plane each)
   double sval[2];
   double* lam_s;
@@ -65,18 +72,15 @@ struct SeedLoad {
   int q0;
   __device__ __forceinline__ Dual<L> operator()(int a, int k, long long m) const {
     Dual<L> r(__ldg(A.in[a] + (long long)k * N + m));
-    const int kk = k - A.k0[a];
-    if (kk >= 0 && kk < A.nk[a]) {
+    if ((A.pmask[a] >> k) & 1u) {
+      const int kk = __popc(A.pmask[a] & ((1u << k) - 1u));
+      const unsigned mask = A.mask[a];
       int oi = -1;
-      if (A.nofs[a] == 1) {
-        if (m == nb[NB_C]) oi = 0;
-      } else {
 #pragma unroll
-        for (int o = 0; o < 9; ++o)
-          if (nb[o] == m) oi = o;
-      }
+      for (int o = 0; o < 9; ++o)
+        if (((mask >> o) & 1u) && nb[o] == m) oi = o;
       if (oi >= 0) {
-        const int l = base[a] + kk * A.nofs[a] + oi - q0;
+        const int l = base[a] + kk * __popc(mask) + __popc(mask & ((1u << oi) - 1u)) - q0;
 #pragma unroll
         for (int ll = 0; ll < L; ++ll)
           if (ll == l) r.d[ll] = 1.0;
@@ -104,11 +108,11 @@ __global__ void __launch_bounds__(kAT) k_cell_vjp(DevParams P, CellVjp A, Fn fn)
     if (any) {
       long long nb[9];
       neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-      SeedLoad<L> ld{A, nb, N, {0, 0, 0, 0}, 0};
+      SeedLoad<L> ld{A, nb, N, {0, 0, 0, 0, 0}, 0};
       int nin = 0;
       for (int a = 0; a < kMaxArr; ++a) {
         ld.base[a] = nin;
-        nin += A.nk[a] * A.nofs[a];
+        nin += __popc(A.pmask[a]) * __popc(A.mask[a]);
       }
       const int ntot = nin + Fn::NS;
       for (int q0 = 0; q0 < ntot; q0 += L) {
@@ -138,9 +142,20 @@ __global__ void __launch_bounds__(kAT) k_cell_vjp(DevParams P, CellVjp A, Fn fn)
           }
           int a = 0;
           while (a + 1 < kMaxArr && q >= ld.base[a + 1]) ++a;
-          const int r = q - ld.base[a], kk = r / A.nofs[a], oi = r % A.nofs[a];
-          const long long m = A.nofs[a] == 1 ? nb[NB_C] : nb[oi];
-          atomicAdd(A.lam[a] + (long long)(A.k0[a] + kk) * N + m, c);
+          const unsigned mask = A.mask[a], pmask = A.pmask[a];
+          const int cnt = __popc(mask), r = q - ld.base[a];
+          int kr = r / cnt, rank = r % cnt, o = 0, k = 0;
+          for (; o < 9; ++o)
+            if ((mask >> o) & 1u) {
+              if (rank == 0) break;
+              --rank;
+            }
+          for (; k < 8; ++k)
+            if ((pmask >> k) & 1u) {
+              if (kr == 0) break;
+              --kr;
+            }
+          atomicAdd(A.lam[a] + (long long)k * N + nb[o], c);
         }
       }
     }
@@ -246,12 +261,19 @@ CellVjp cv_empty() {
   memset(&A, 0, sizeof(A));
   return A;
 }
-void cv_arr(CellVjp& A, int a, const double* in, double* lam, int k0, int nk, int nofs) {
+// array a seeded on planes [k0, k0 + nk) at the neighbours in `mask`
+void cv_arr(CellVjp& A, int a, const double* in, double* lam, int k0, int nk, unsigned mask) {
   A.in[a] = in;
   A.lam[a] = lam;
-  A.k0[a] = k0;
-  A.nk[a] = lam ? nk : 0;
-  A.nofs[a] = nofs;
+  A.pmask[a] = lam ? ((1u << nk) - 1u) << k0 : 0u;
+  A.mask[a] = mask;
+}
+// array a seeded on the planes in `pmask`
+void cv_arr_planes(CellVjp& A, int a, const double* in, double* lam, unsigned pmask, unsigned mask) {
+  A.in[a] = in;
+  A.lam[a] = lam;
+  A.pmask[a] = lam ? pmask : 0u;
+  A.mask[a] = mask;
 }
 template <int L, class Fn>
 imex_status run_cell_vjp(imex_ctx* ctx, const CellVjp& A, Fn fn) {
@@ -934,9 +956,10 @@ imex_status reverse_step(Adj& W) {
     zero(W, W.lFy, N);
     {
       CellVjp A = cv_empty();
-      cv_arr(A, CC_FX, S.Fx, W.lFx, 0, 1, 9);
-      cv_arr(A, CC_FY, S.Fy, W.lFy, 0, 1, 9);
-      cv_arr(A, CC_UCON, S.um, W.l4, 0, 7, 9);
+      const unsigned cN = 1u << NB_N, cE = 1u << NB_E, cNE = 1u << NB_NE;
+      cv_arr(A, CC_FX, S.Fx, W.lFx, 0, 1, OFS_C | cN);
+      cv_arr(A, CC_FY, S.Fy, W.lFy, 0, 1, OFS_C | cE);
+      cv_arr_planes(A, CC_UCON, S.um, W.l4, 0x67u, OFS_C | cE | cN | cNE);  // rho, mx, my, Bx, By
       A.lam_out[0] = W.lE;
       A.sx = -1.0;
       A.sy = 1.0;
@@ -954,8 +977,8 @@ imex_status reverse_step(Adj& W) {
     const double* pE = S.second ? S.p2 : S.p1;
     {  // DefinitionofU at the final pressure, on um
       CellVjp A = cv_empty();
-      cv_arr(A, ED_P, pE, W.lp, 0, 1, 1);
-      cv_arr(A, ED_UCON, S.um, W.lum, 0, 8, 1);
+      cv_arr(A, ED_P, pE, W.lp, 0, 1, OFS_C);
+      cv_arr(A, ED_UCON, S.um, W.lum, 0, 8, OFS_C);
       A.lam_out[0] = W.l4 + 4 * N;
       if ((s = run_cell_vjp<8>(ctx, A, FnEnergyDef{})) != IMEX_OK) return s;
     }
@@ -965,10 +988,10 @@ imex_status reverse_step(Adj& W) {
     if (S.second) {
       if ((s = newton_adjoint(W, S, S.p2, S.b2, S.mbig2, W.lp, W.mu)) != IMEX_OK) return s;
       CellVjp A = cv_empty();  // b2 = rhs(um, hh, rv, kin = um momentum)
-      cv_arr(A, PR_UCON, S.um, W.lum, 0, 8, 1);
-      cv_arr(A, PR_HH, S.hh, W.lhh, 0, 1, 9);
-      cv_arr(A, PR_RV, S.u3 + N, W.lrv, 0, 2, 9);
-      cv_arr(A, PR_KIN, S.um + N, W.lum + N, 0, 3, 1);
+      cv_arr(A, PR_UCON, S.um, W.lum, 0, 8, OFS_C);
+      cv_arr(A, PR_HH, S.hh, W.lhh, 0, 1, OFS_CROSS);
+      cv_arr(A, PR_RV, S.u3 + N, W.lrv, 0, 2, OFS_CROSS);
+      cv_arr(A, PR_KIN, S.um + N, W.lum + N, 0, 3, OFS_C);
       A.lam_out[0] = W.mu;
       A.h = h;
       if ((s = run_cell_vjp<8>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
@@ -976,8 +999,8 @@ imex_status reverse_step(Adj& W) {
     }
     {  // momentum: um[1..2] = rv - h grad p1
       CellVjp A = cv_empty();
-      cv_arr(A, MO_P, S.p1, W.lp, 0, 1, 9);
-      cv_arr(A, MO_RV, S.u3 + N, W.lrv, 0, 2, 1);
+      cv_arr(A, MO_P, S.p1, W.lp, 0, 1, OFS_CROSS);
+      cv_arr(A, MO_RV, S.u3 + N, W.lrv, 0, 2, OFS_C);
       A.lam_out[0] = W.lum + N;
       A.lam_out[1] = W.lum + 2 * N;
       A.h = h;
@@ -992,10 +1015,10 @@ imex_status reverse_step(Adj& W) {
     if ((s = newton_adjoint(W, S, S.p1, S.b1, S.mbig1, W.lp, W.mu)) != IMEX_OK) return s;
     {  // b1 = rhs(u3, hh, rv, kin = rv)
       CellVjp A = cv_empty();
-      cv_arr(A, PR_UCON, S.u3, W.l3, 0, 8, 1);
-      cv_arr(A, PR_HH, S.hh, W.lhh, 0, 1, 9);
-      cv_arr(A, PR_RV, S.u3 + N, W.lrv, 0, 2, 9);
-      cv_arr(A, PR_KIN, S.u3 + N, W.lrv, 0, 3, 1);
+      cv_arr(A, PR_UCON, S.u3, W.l3, 0, 8, OFS_C);
+      cv_arr(A, PR_HH, S.hh, W.lhh, 0, 1, OFS_CROSS);
+      cv_arr(A, PR_RV, S.u3 + N, W.lrv, 0, 2, OFS_CROSS);
+      cv_arr(A, PR_KIN, S.u3 + N, W.lrv, 0, 3, OFS_C);
       A.lam_out[0] = W.mu;
       A.h = h;
       if ((s = run_cell_vjp<8>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
@@ -1003,8 +1026,8 @@ imex_status reverse_step(Adj& W) {
     k_axpy_planes<<<ablocks(3 * N), kAT, 0, st>>>((long long)(3 * N), W.l3 + N, W.lrv, 1.0);
     {  // hh = h(Qe) rho_e / rho
       CellVjp A = cv_empty();
-      cv_arr(A, HH_QE, S.Qe, W.lQe, 0, 8, 1);
-      cv_arr(A, HH_UCON, S.u3, W.l3, 0, 1, 1);
+      cv_arr(A, HH_QE, S.Qe, W.lQe, 0, 8, OFS_C);
+      cv_arr(A, HH_UCON, S.u3, W.l3, 0, 1, OFS_C);
       A.lam_out[0] = W.lhh;
       if ((s = run_cell_vjp<8>(ctx, A, FnHh{})) != IMEX_OK) return s;
     }
@@ -1017,7 +1040,7 @@ imex_status reverse_step(Adj& W) {
     ACHECK(ctx, "adjoint shock detector");
     {
       CellVjp A = cv_empty();
-      cv_arr(A, 0, S.Qe, W.lQe, 0, 8, 1);
+      cv_arr(A, 0, S.Qe, W.lQe, 0, 8, OFS_C);
       A.lam_out[0] = W.lcf;
       if ((s = run_cell_vjp<8>(ctx, A, FnShockCf{})) != IMEX_OK) return s;
     }
@@ -1036,9 +1059,9 @@ imex_status reverse_step(Adj& W) {
     // (6) CollectMagFluxes
     {
       CellVjp A = cv_empty();
-      cv_arr(A, CF_UCON, S.u2, W.l2, 0, 8, 9);
-      cv_arr(A, CF_QE, S.Qe, W.lQe, 5, 3, 9);
-      cv_arr(A, CF_PE, S.pe, W.lpe, 0, 1, 9);
+      cv_arr_planes(A, CF_UCON, S.u2, W.l2, 0xE7u, OFS_NO_SW);  // rho, mx, my, B
+      cv_arr(A, CF_QE, S.Qe, W.lQe, 5, 3, OFS_NO_SW);
+      cv_arr(A, CF_PE, S.pe, W.lpe, 0, 1, OFS_NO_SW);
       A.lam_out[0] = W.lFx;
       A.lam_out[1] = W.lFy;
       A.sval[0] = S.sc.B_max_x;
@@ -1062,10 +1085,10 @@ imex_status reverse_step(Adj& W) {
     // (8) magnetic right-hand side b(u1, Qe, pe, Qs)
     {
       CellVjp A = cv_empty();
-      cv_arr(A, MR_UCON, S.u1, W.l1, 0, 4, 9);
-      cv_arr(A, MR_QE, S.Qe, W.lQe, 5, 3, 9);
-      cv_arr(A, MR_PE, S.pe, W.lpe, 0, 1, 9);
-      cv_arr(A, MR_QS, S.Qs, nullptr, 0, 0, 1);
+      cv_arr(A, MR_UCON, S.u1, W.l1, 0, 4, OFS_CROSS);
+      cv_arr(A, MR_QE, S.Qe, W.lQe, 5, 3, OFS_CROSS);
+      cv_arr(A, MR_PE, S.pe, W.lpe, 0, 1, OFS_ALL);
+      cv_arr(A, MR_QS, S.Qs, nullptr, 0, 0, OFS_C);
       A.lam_out[0] = W.mu;
       A.lam_out[1] = W.mu + N;
       A.lam_out[2] = W.mu + 2 * N;
@@ -1083,7 +1106,7 @@ imex_status reverse_step(Adj& W) {
     // (10) p(Qe) of the combination
     {
       CellVjp A = cv_empty();
-      cv_arr(A, 0, S.Qe, W.lQe, 0, 8, 1);
+      cv_arr(A, 0, S.Qe, W.lQe, 0, 8, OFS_C);
       A.lam_out[0] = W.lpe;
       if ((s = run_cell_vjp<8>(ctx, A, FnPe{})) != IMEX_OK) return s;
     }
@@ -1196,7 +1219,7 @@ imex_status adjoint_core(imex_ctx* ctx, const imex_adjoint_opts* o, const std::f
       double* gp;
       if ((t = amalloc(W, &gp, 8 * N)) != IMEX_OK || (t = zero(W, gp, 8 * N)) != IMEX_OK) return t;
       CellVjp A = cv_empty();
-      cv_arr(A, 0, start.prim, gp, 0, 8, 1);
+      cv_arr(A, 0, start.prim, gp, 0, 8, OFS_C);
       for (int k = 0; k < 8; ++k) A.lam_out[k] = W.lam_u + k * N;
       if ((t = run_cell_vjp<8>(ctx, A, FnPri2Con{})) != IMEX_OK) return t;
       cudaError_t e = cudaMemcpyAsync(g_prim, gp, 8 * N * sizeof(double), cudaMemcpyDefault, ctx->stream);
