@@ -963,7 +963,7 @@ imex_status reverse_step(Adj& W) {
       A.lam_out[0] = W.lE;
       A.sx = -1.0;
       A.sy = 1.0;
-      if ((s = run_cell_vjp<8>(ctx, A, FnCtCorner{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnCtCorner{})) != IMEX_OK) return s;
     }
     // (4) pressure sub-system
     zero(W, W.lum, 8 * N);
@@ -980,7 +980,7 @@ imex_status reverse_step(Adj& W) {
       cv_arr(A, ED_P, pE, W.lp, 0, 1, OFS_C);
       cv_arr(A, ED_UCON, S.um, W.lum, 0, 8, OFS_C);
       A.lam_out[0] = W.l4 + 4 * N;
-      if ((s = run_cell_vjp<8>(ctx, A, FnEnergyDef{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnEnergyDef{})) != IMEX_OK) return s;
     }
     // passthrough of the planes other than E
     for (int k = 0; k < 8; ++k)
@@ -994,7 +994,7 @@ imex_status reverse_step(Adj& W) {
       cv_arr(A, PR_KIN, S.um + N, W.lum + N, 0, 3, OFS_C);
       A.lam_out[0] = W.mu;
       A.h = h;
-      if ((s = run_cell_vjp<8>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
       zero(W, W.lp, N);
     }
     {  // momentum: um[1..2] = rv - h grad p1
@@ -1004,7 +1004,7 @@ imex_status reverse_step(Adj& W) {
       A.lam_out[0] = W.lum + N;
       A.lam_out[1] = W.lum + 2 * N;
       A.h = h;
-      if ((s = run_cell_vjp<8>(ctx, A, FnMomentum{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnMomentum{})) != IMEX_OK) return s;
     }
     // um = u3 except momentum x, y
     for (int k = 0; k < 8; ++k)
@@ -1021,7 +1021,7 @@ imex_status reverse_step(Adj& W) {
       cv_arr(A, PR_KIN, S.u3 + N, W.lrv, 0, 3, OFS_C);
       A.lam_out[0] = W.mu;
       A.h = h;
-      if ((s = run_cell_vjp<8>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnPresRhs{})) != IMEX_OK) return s;
     }
     k_axpy_planes<<<ablocks(3 * N), kAT, 0, st>>>((long long)(3 * N), W.l3 + N, W.lrv, 1.0);
     {  // hh = h(Qe) rho_e / rho
@@ -1029,7 +1029,7 @@ imex_status reverse_step(Adj& W) {
       cv_arr(A, HH_QE, S.Qe, W.lQe, 0, 8, OFS_C);
       cv_arr(A, HH_UCON, S.u3, W.l3, 0, 1, OFS_C);
       A.lam_out[0] = W.lhh;
-      if ((s = run_cell_vjp<8>(ctx, A, FnHh{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnHh{})) != IMEX_OK) return s;
     }
     // shock detector eta(Qe)
     zero(W, W.lchit, N);
@@ -1042,7 +1042,7 @@ imex_status reverse_step(Adj& W) {
       CellVjp A = cv_empty();
       cv_arr(A, 0, S.Qe, W.lQe, 0, 8, OFS_C);
       A.lam_out[0] = W.lcf;
-      if ((s = run_cell_vjp<8>(ctx, A, FnShockCf{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnShockCf{})) != IMEX_OK) return s;
     }
     // (5) pressure-form flux: u3[0..4] = Qs - h div F(w(Qe), B of u2, a_max)
     zero(W, W.l2, 8 * N);
@@ -1068,7 +1068,7 @@ imex_status reverse_step(Adj& W) {
       A.sval[1] = S.sc.B_max_y;
       A.lam_s = W.dscal + 1;
       A.h = h;
-      if ((s = run_cell_vjp<8>(ctx, A, FnCollect{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnCollect{})) != IMEX_OK) return s;
     }
     // (7) magnetic solve A(Qe B, rho) x = b with x = B of u2
     {
@@ -1093,7 +1093,7 @@ imex_status reverse_step(Adj& W) {
       A.lam_out[1] = W.mu + N;
       A.lam_out[2] = W.mu + 2 * N;
       A.h = h;
-      if ((s = run_cell_vjp<8>(ctx, A, FnMagRhs{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnMagRhs{})) != IMEX_OK) return s;
     }
     k_axpy_planes<<<ablocks(3 * N), kAT, 0, st>>>((long long)(3 * N), W.lQs + 5 * N, W.mu, 1.0);
     // (9) convective flux: u1[0..4] = Qs - h div F(w(Qe), a_max)
@@ -1108,7 +1108,7 @@ imex_status reverse_step(Adj& W) {
       CellVjp A = cv_empty();
       cv_arr(A, 0, S.Qe, W.lQe, 0, 8, OFS_C);
       A.lam_out[0] = W.lpe;
-      if ((s = run_cell_vjp<8>(ctx, A, FnPe{})) != IMEX_OK) return s;
+      if ((s = run_cell_vjp<4>(ctx, A, FnPe{})) != IMEX_OK) return s;
     }
     // (11) stage combination
     Coefs T{};
@@ -1221,7 +1221,7 @@ imex_status adjoint_core(imex_ctx* ctx, const imex_adjoint_opts* o, const std::f
       CellVjp A = cv_empty();
       cv_arr(A, 0, start.prim, gp, 0, 8, OFS_C);
       for (int k = 0; k < 8; ++k) A.lam_out[k] = W.lam_u + k * N;
-      if ((t = run_cell_vjp<8>(ctx, A, FnPri2Con{})) != IMEX_OK) return t;
+      if ((t = run_cell_vjp<4>(ctx, A, FnPri2Con{})) != IMEX_OK) return t;
       cudaError_t e = cudaMemcpyAsync(g_prim, gp, 8 * N * sizeof(double), cudaMemcpyDefault, ctx->stream);
       if (e != cudaSuccess) return cuda_check(ctx, e, "gradient download");
     }
