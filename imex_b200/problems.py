@@ -7,6 +7,9 @@ Every field is returned as interior-only SoA planes of shape (ny, nx), index
     bx    (ny, nx)   : Bx on the x-face (i+1/2, j)
     by    (ny, nx)   : By on the y-face (i, j+1/2)
     A     (3, ny, nx): vector potential at cell centres
+    bx_x0 (ny,), by_y0 (nx,): only for a transmissive direction, the boundary normal
+                       faces Bx(x_0, j) and By(i, y_0), which a periodic direction
+                       identifies with the faces at x_1 / y_1
 
 Formulas follow the reference's initial conditions:
   * vortex:  initial_conditions.cpp:641-669 (cell state) and :698-717 (faces
@@ -17,7 +20,10 @@ Formulas follow the reference's initial conditions:
     [0, 2*pi]^2 form, faces = average of neighbouring cell B as in
     initial_conditions.cpp:720-726, A_z = cos y + cos(2x)/2;
   * random field: seeded low-Mach, magnetic-pressure-dominated Redlich-Kwong gas on
-    the unit square (random Fourier sums; faces from a corner A_z as for the vortex).
+    the unit square (random Fourier sums; faces from a corner A_z as for the vortex);
+  * open blast: a smooth pressure pulse in an oblique field with a shearing flow on the
+    open unit square (x_Transmissive, y_Transmissive as the reference's blast and
+    shock-tube tests, main.cpp:9-60), with every field varying across the boundaries.
 """
 from __future__ import annotations
 
@@ -41,6 +47,8 @@ class Problem:
     by: np.ndarray
     A: np.ndarray
     settings: dict = field(default_factory=dict)
+    bx_x0: np.ndarray | None = None
+    by_y0: np.ndarray | None = None
 
     @property
     def dx(self) -> float:
@@ -191,6 +199,47 @@ def random_field(n: int = 2048, seed: int = 2026, p0: float = 1.0, mach: float =
     return Problem("random_field", nx, ny, 0.0, 1.0, 0.0, 1.0, prim, np.ascontiguousarray(bx),
                    np.ascontiguousarray(by), A,
                    settings=dict(gamma=gamma, vortex_test=0, eos_type="REDLICH_KWONG", m_alfa=m_alfa, m_b=m_b))
+
+
+def open_blast(n: int = 64, ny: int | None = None, b0: float = 0.5, angle: float = 0.3) -> Problem:
+    """Smooth blast in an oblique field on the open square [-1/2, 1/2]^2 (transmissive in x
+    and y, gamma = 5/3).  rho = 1 + 0.3 g(r, 0.15) + 0.1 x, p = 0.5 + 2 g(r, 0.1) with
+    g(r, s) = exp(-r^2 / s^2); v = (0.3 + 0.2 y, -0.2 + 0.1 sin(2 pi x), 0.05 x); A_z on the
+    (nx + 1) x (ny + 1) corners = b0 (y cos a - x sin a) + 0.05 g(r, 0.2), so the faces
+    (boundary faces included) are its exact differences and div B = 0 to round-off; cell B
+    = face average; B_z = 0.1 (1 + y)."""
+    nx = n
+    ny = n if ny is None else ny
+    x0, x1, y0, y1 = -0.5, 0.5, -0.5, 0.5
+    dx, dy = (x1 - x0) / nx, (y1 - y0) / ny
+    xc = x0 + (np.arange(nx) + 0.5) * dx
+    yc = y0 + (np.arange(ny) + 0.5) * dy
+    X, Y = np.meshgrid(xc, yc)
+    g = lambda x, y, s: np.exp(-(x * x + y * y) / (s * s))
+    prim = np.zeros((8, ny, nx))
+    prim[0] = 1.0 + 0.3 * g(X, Y, 0.15) + 0.1 * X
+    prim[1] = 0.3 + 0.2 * Y
+    prim[2] = -0.2 + 0.1 * np.sin(2.0 * math.pi * X)
+    prim[3] = 0.05 * X
+    prim[4] = 0.5 + 2.0 * g(X, Y, 0.1)
+    ca, sa = math.cos(angle), math.sin(angle)
+    az = lambda x, y: b0 * (y * ca - x * sa) + 0.05 * g(x, y, 0.2)
+    xf = x0 + np.arange(nx + 1) * dx  # corners (i - 1/2) for i = 0..nx
+    yf = y0 + np.arange(ny + 1) * dy
+    XF, YF = np.meshgrid(xf, yf)  # (ny + 1, nx + 1)
+    ac = az(XF, YF)
+    bx_all = (ac[1:, :] - ac[:-1, :]) / dy  # (ny, nx + 1): Bx at x-faces i - 1/2, i = 0..nx
+    by_all = -(ac[:, 1:] - ac[:, :-1]) / dx  # (ny + 1, nx): By at y-faces j - 1/2
+    bx, bx_x0 = bx_all[:, 1:], bx_all[:, 0]
+    by, by_y0 = by_all[1:, :], by_all[0, :]
+    prim[5] = 0.5 * (bx_all[:, :-1] + bx_all[:, 1:])
+    prim[6] = 0.5 * (by_all[:-1, :] + by_all[1:, :])
+    prim[7] = 0.1 * (1.0 + Y)
+    A = np.zeros((3, ny, nx))
+    A[2] = az(X, Y)
+    return Problem("open_blast", nx, ny, x0, x1, y0, y1, prim, np.ascontiguousarray(bx), np.ascontiguousarray(by),
+                   A, settings=dict(gamma=5.0 / 3.0, vortex_test=0, x_bc="x_Transmissive", y_bc="y_Transmissive"),
+                   bx_x0=np.ascontiguousarray(bx_x0), by_y0=np.ascontiguousarray(by_y0))
 
 
 def vortex_ensemble(members: int = 256, seed: int = 2026, smin: int = 64, smax: int = 512) -> list[Problem]:

@@ -30,6 +30,8 @@ PVISC = {"MaterialSpeedp": 0, "AlfvenSpeedp": 1, "Noaddvisp": 2}
 UUPDATE = {"ConservationofU": 0, "DefinitionofU": 1}
 PSOLVER = {"no_correction": 0, "once_correction": 1, "all_correction": 2}
 EOS = {"IDEAL_GAS": 0, "REDLICH_KWONG": 1}
+XBC = {"x_Transmissive": 0, "x_Reflective": 1, "x_Periodic": 2, "x_Dirichlet": 3}
+YBC = {"y_Transmissive": 0, "y_Reflective": 1, "y_Periodic": 2, "y_Dirichlet": 3, "y_JetInflow": 4}
 
 # reference defaults, include/config.hpp:43-125
 DEFAULTS = dict(
@@ -128,6 +130,9 @@ class _Solver:
                 "fn_substep": (None, [C.c_int, C.c_double, C.c_int, D, D, D, D, D, D, D, D, D,
                                       D, D]),
                 "div_error": (C.c_double, []),
+                "set_bc": (C.c_int, [C.c_int, C.c_int]),
+                "set_boundary_faces": (None, [D, D]), "get_boundary_faces": (None, [D, D]),
+                "get_snapshot_boundary": (C.c_int, [C.c_int, C.c_int, C.c_int, D]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(lib, p + name)
@@ -138,6 +143,31 @@ class _Solver:
 
     def _f(self, name):
         return getattr(self.lib, self.prefix + name)
+
+    # ---- boundaries ----------------------------------------------------
+    def set_bc(self, x_bc, y_bc) -> None:
+        """x_bc / y_bc as names or ordinals (config.hpp:36-37); call before load()."""
+        xb = XBC[x_bc] if isinstance(x_bc, str) else int(x_bc)
+        yb = YBC[y_bc] if isinstance(y_bc, str) else int(y_bc)
+        if self._f("set_bc")(xb, yb) != 0:
+            raise RuntimeError(f"{self.prefix}set_bc({x_bc}, {y_bc}) refused")
+
+    def set_boundary_faces(self, bx_x0, by_y0) -> None:
+        """Bx on x = x_0 (ny values) and By on y = y_0 (nx values)."""
+        bx0, by0 = _c(bx_x0), _c(by_y0)
+        assert bx0.size == self.ny and by0.size == self.nx
+        self._f("set_boundary_faces")(_dp(bx0), _dp(by0))
+
+    def boundary_faces(self) -> tuple[np.ndarray, np.ndarray]:
+        bx0, by0 = np.empty(self.ny), np.empty(self.nx)
+        self._f("get_boundary_faces")(_dp(bx0), _dp(by0))
+        return bx0, by0
+
+    def snapshot_boundary(self, rks: int, sub: str, which: str) -> np.ndarray | None:
+        w = SNAP[which]
+        out = np.zeros(self.ny if w in (3, 5) else self.nx)
+        rc = self._f("get_snapshot_boundary")(rks, SUB[sub], w, _dp(out))
+        return None if rc != 0 else out
 
     # ---- whole steps -------------------------------------------------
     def load(self, prob) -> None:
@@ -263,5 +293,9 @@ def make_solver(kind: str, prob, rks: int, settings: dict):
     s = dict(prob.settings)
     s.update(settings)
     solver = cls(prob.nx, prob.ny, rks, s, (prob.x0, prob.x1, prob.y0, prob.y1))
+    if "x_bc" in s or "y_bc" in s:
+        solver.set_bc(s.get("x_bc", "x_Periodic"), s.get("y_bc", "y_Periodic"))
     solver.load(prob)
+    if getattr(prob, "bx_x0", None) is not None:
+        solver.set_boundary_faces(prob.bx_x0, prob.by_y0)
     return solver

@@ -7,9 +7,20 @@
  * with the reference bit for bit; implicit solves agree to solver tolerance
  * because reductions are summed serially in index order here.
  *
- * Periodic boundaries only: ghost cells are replaced by wrap-around indexing,
- * which reproduces the reference's periodic ghost fills (boundary.cpp:46,118,
- * timestep.cpp:184,213, constrained_transport.cpp:13,32) exactly.
+ * Periodic and transmissive boundaries (per direction, ora_set_bc): ghost cells
+ * are replaced by index maps.  Periodic wraps, which reproduces the reference's
+ * periodic ghost fills (boundary.cpp:46,118, timestep.cpp:184,213,
+ * constrained_transport.cpp:13,32) exactly.  Transmissive clamps to the nearest
+ * interior cell, which is what bound_cond_u, bound_cond_array, M_P / M_B and the
+ * operators' max/min neighbour indices do for x_Transmissive / y_Transmissive
+ * (boundary.cpp:7-16, timestep.cpp:168-175,195-204, implicit_operators.cpp:12-14,
+ * 150-153).  Two things are not a clamp there and are restated explicitly:
+ *   - the boundary normal faces (Bx at x = x_0, By at y = y_0) are degrees of
+ *     freedom that CT evolves (constrained_transport.cpp:5-30); every face array
+ *     carries them after its nx*ny interior values (bx: ny values, by: nx values);
+ *   - the corner EMF at x_0 / y_0: its averaged part Ez_bar is clamped by
+ *     bound_cond_array while its correction terms are evaluated at the boundary
+ *     corner itself (constrained_transport.cpp:147-164).
  */
 #include "imex_oracle.h"
 
@@ -38,7 +49,8 @@ typedef struct {
 
 static struct {
   int ready, nx, ny, R;
-  size_t N;
+  int xclamp, yclamp; /* transmissive (clamped) directions; periodic otherwise */
+  size_t N, NF;       /* cells; entries of a face array (N + nx + ny) */
   ora_params P;
   double dx, dy;
   double *prim, *cons, *cons_n, *Qe, *Qs, *wxL, *wxR, *wyL, *wyR;
@@ -54,13 +66,26 @@ static struct {
 /* ------------------------------------------------------------------ */
 /* indexing                                                           */
 /* ------------------------------------------------------------------ */
-static inline size_t ID(int i, int j) {
-  int nx = G.nx, ny = G.ny;
+static inline int CI(int i) {
+  int nx = G.nx;
+  if (G.xclamp) return i < 0 ? 0 : (i >= nx ? nx - 1 : i);
   i %= nx;
-  if (i < 0) i += nx;
+  return i < 0 ? i + nx : i;
+}
+static inline int CJ(int j) {
+  int ny = G.ny;
+  if (G.yclamp) return j < 0 ? 0 : (j >= ny ? ny - 1 : j);
   j %= ny;
-  if (j < 0) j += ny;
-  return (size_t)i + (size_t)nx * (size_t)j;
+  return j < 0 ? j + ny : j;
+}
+static inline size_t ID(int i, int j) { return (size_t)CI(i) + (size_t)G.nx * (size_t)CJ(j); }
+/* x-face (i+1/2, j) and y-face (i, j+1/2) of a face array: left of x_0 / below y_0 a
+ * transmissive direction reads the boundary face (bound_cond_staggered's normal rule) */
+static inline double BXF(const double* a, int i, int j) {
+  return (i < 0 && G.xclamp) ? a[G.N + (size_t)CJ(j)] : a[ID(i, j)];
+}
+static inline double BYF(const double* a, int i, int j) {
+  return (j < 0 && G.yclamp) ? a[G.N + (size_t)CI(i)] : a[ID(i, j)];
 }
 #define PL(a, k) ((a) + (size_t)(k)*G.N)
 #define AT(a, k, i, j) ((a)[(size_t)(k)*G.N + ID(i, j)])
@@ -1268,51 +1293,67 @@ static void mag_subsystem_A(double* ucon, const double* Qs, const double* Qe, do
 /* ------------------------------------------------------------------ */
 /* constrained transport                                              */
 /* ------------------------------------------------------------------ */
-/* CT_CornerAssemble, constrained_transport.cpp:147-164 */
-static void corner_assemble(double* Epp, const double* Ep0, const double* E0p, const double* Et) {
+/* CT_CornerAssemble, constrained_transport.cpp:147-164: the corner (i+1/2, j+1/2) for
+ * i, j >= -1.  Ez_bar holds its ghost corners by bound_cond_array (a clamp or a wrap of the
+ * corner index), the correction terms read the edge and cell EMFs at the corner itself. */
+static double corner_at(int i, int j, const double* Ep0, const double* E0p, const double* Et) {
   const double dx = G.dx, dy = G.dy;
-  for (int j = 0; j < G.ny; j++)
-    for (int i = 0; i < G.nx; i++) {
+  const int bi = i < 0 ? (G.xclamp ? 0 : G.nx + i) : i, bj = j < 0 ? (G.yclamp ? 0 : G.ny + j) : j;
 #define E(a, ii, jj) a[ID(ii, jj)]
-      double bar = 0.25 * (E(Ep0, i, j) + E(Ep0, i, j + 1) + E(E0p, i, j) + E(E0p, i + 1, j));
-      double t1 = 0.5 * ((E(Ep0, i, j) - E(Et, i, j)) / (dx / 2.0) + (E(Ep0, i, j + 1) - E(Et, i, j + 1)) / (dx / 2.0));
-      double t2 = 0.5 * ((E(Et, i + 1, j) - E(Ep0, i, j)) / (dx / 2.0) + (E(Et, i + 1, j + 1) - E(Ep0, i, j + 1)) / (dx / 2.0));
-      double t3 = 0.5 * ((E(E0p, i, j) - E(Et, i, j)) / (dy / 2.0) + (E(E0p, i + 1, j) - E(Et, i + 1, j)) / (dy / 2.0));
-      double t4 = 0.5 * ((E(Et, i, j + 1) - E(E0p, i, j)) / (dy / 2.0) + (E(Et, i + 1, j + 1) - E(E0p, i + 1, j)) / (dy / 2.0));
+  double bar = 0.25 * (E(Ep0, bi, bj) + E(Ep0, bi, bj + 1) + E(E0p, bi, bj) + E(E0p, bi + 1, bj));
+  double t1 = 0.5 * ((E(Ep0, i, j) - E(Et, i, j)) / (dx / 2.0) + (E(Ep0, i, j + 1) - E(Et, i, j + 1)) / (dx / 2.0));
+  double t2 = 0.5 * ((E(Et, i + 1, j) - E(Ep0, i, j)) / (dx / 2.0) + (E(Et, i + 1, j + 1) - E(Ep0, i, j + 1)) / (dx / 2.0));
+  double t3 = 0.5 * ((E(E0p, i, j) - E(Et, i, j)) / (dy / 2.0) + (E(E0p, i + 1, j) - E(Et, i + 1, j)) / (dy / 2.0));
+  double t4 = 0.5 * ((E(Et, i, j + 1) - E(E0p, i, j)) / (dy / 2.0) + (E(Et, i + 1, j + 1) - E(E0p, i + 1, j)) / (dy / 2.0));
 #undef E
-      Epp[ID(i, j)] = bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
-    }
+  return bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
+}
+static void corner_assemble(double* Epp, const double* Ep0, const double* E0p, const double* Et) {
+  for (int j = 0; j < G.ny; j++)
+    for (int i = 0; i < G.nx; i++) Epp[ID(i, j)] = corner_at(i, j, Ep0, E0p, Et);
 }
 static void cell_ez(double* Et, const double* ucon) {
   const size_t N = G.N;
   for (size_t c = 0; c < N; ++c)
     Et[c] = ucon[2 * N + c] / ucon[c] * ucon[5 * N + c] - ucon[N + c] / ucon[c] * ucon[6 * N + c];
 }
+/* eq (39) face update and eq (46) cell average, ct_flux.cpp:176-189.  Epp is the corner
+ * grid of (nx+1)(ny+1) corners from (-1/2, -1/2): EC(i, j) = corner (i+1/2, j+1/2). */
+#define EC(i, j) Epp[(size_t)((i) + 1) + (size_t)(G.nx + 1) * (size_t)((j) + 1)]
 static void face_update(double* bx, double* by, const double* bxQs, const double* byQs, const double* Epp, double h,
                         double* ucon) {
   const size_t N = G.N;
   for (int j = 0; j < G.ny; j++)
     for (int i = 0; i < G.nx; i++) {
-      bx[ID(i, j)] = bxQs[ID(i, j)] - h / G.dy * (Epp[ID(i, j)] - Epp[ID(i, j - 1)]);
-      by[ID(i, j)] = byQs[ID(i, j)] + h / G.dx * (Epp[ID(i, j)] - Epp[ID(i - 1, j)]);
+      bx[ID(i, j)] = bxQs[ID(i, j)] - h / G.dy * (EC(i, j) - EC(i, j - 1));
+      by[ID(i, j)] = byQs[ID(i, j)] + h / G.dx * (EC(i, j) - EC(i - 1, j));
     }
+  if (G.xclamp)
+    for (int j = 0; j < G.ny; j++) bx[N + j] = bxQs[N + j] - h / G.dy * (EC(-1, j) - EC(-1, j - 1));
+  if (G.yclamp)
+    for (int i = 0; i < G.nx; i++) by[N + i] = byQs[N + i] + h / G.dx * (EC(i, -1) - EC(i - 1, -1));
   for (int j = 0; j < G.ny; j++)
     for (int i = 0; i < G.nx; i++) {
-      ucon[5 * N + ID(i, j)] = 0.5 * (bx[ID(i - 1, j)] + bx[ID(i, j)]);
-      ucon[6 * N + ID(i, j)] = 0.5 * (by[ID(i, j - 1)] + by[ID(i, j)]);
+      ucon[5 * N + ID(i, j)] = 0.5 * (BXF(bx, i - 1, j) + bx[ID(i, j)]);
+      ucon[6 * N + ID(i, j)] = 0.5 * (BYF(by, i, j - 1) + by[ID(i, j)]);
     }
 }
+static void corner_grid(double* Epp, const double* Ep0, const double* E0p, const double* Et) {
+  for (int j = -1; j < G.ny; j++)
+    for (int i = -1; i < G.nx; i++) EC(i, j) = corner_at(i, j, Ep0, E0p, Et);
+}
+#undef EC
 /* Staggered_CT_Consistent, ct_flux.cpp:150-191 */
 static void staggered_ct_consistent(double* ucon, double* bx, double* by, const double* bxQs, const double* byQs,
                                     const double* Fx, const double* Fy, double h) {
   const size_t N = G.N;
-  double *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc(N);
+  double *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc((size_t)(G.nx + 1) * (G.ny + 1));
   for (size_t c = 0; c < N; ++c) {
     Ep0[c] = -Fx[c];
     E0p[c] = +Fy[c];
   }
   cell_ez(Et, ucon);
-  corner_assemble(Epp, Ep0, E0p, Et);
+  corner_grid(Epp, Ep0, E0p, Et);
   face_update(bx, by, bxQs, byQs, Epp, h, ucon);
   free(Ep0); free(E0p); free(Et); free(Epp);
 }
@@ -1342,7 +1383,8 @@ static void unstaggered_ct_consistent(double* ucon, double* A, const double* A_s
 /* Staggered_CT (legacy), constrained_transport.cpp:66-143 */
 static void staggered_ct_legacy(double* ucon, double* bx, double* by, const double* bxQs, const double* byQs, double h) {
   const size_t N = G.N;
-  double *w = alloc(32 * N), *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc(N);
+  double *w = alloc(32 * N), *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N);
+  double* Epp = alloc((size_t)(G.nx + 1) * (G.ny + 1));
   double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
   reconstruct(ucon, wxL, wxR, wyL, wyR);
   double QL[8], QR[8];
@@ -1360,7 +1402,7 @@ static void staggered_ct_legacy(double* ucon, double* bx, double* by, const doub
       E0p[ID(i, j)] = (0.5 * (gL5 + gR5));
     }
   cell_ez(Et, ucon);
-  corner_assemble(Epp, Ep0, E0p, Et);
+  corner_grid(Epp, Ep0, E0p, Et);
   face_update(bx, by, bxQs, byQs, Epp, h, ucon);
   free(w); free(Ep0); free(E0p); free(Et); free(Epp);
 }
@@ -1493,10 +1535,10 @@ static void snapshot(int sub, int rks) {
   keep(&s->u_con, G.cons, 8 * N);
   keep(&s->Qe, G.Qe, 8 * N);
   keep(&s->Qs, G.Qs, 8 * N);
-  keep(&s->bx, G.bx, N);
-  keep(&s->by, G.by, N);
-  keep(&s->bxQs, G.bxQs, N);
-  keep(&s->byQs, G.byQs, N);
+  keep(&s->bx, G.bx, G.NF);
+  keep(&s->by, G.by, G.NF);
+  keep(&s->bxQs, G.bxQs, G.NF);
+  keep(&s->byQs, G.byQs, G.NF);
   keep(&s->A, G.A, 3 * N);
   keep(&s->A_s, G.A_s, 3 * N);
   keep(&s->Fx, G.Fx, N);
@@ -1514,10 +1556,11 @@ static void stage(int rks) {
   memcpy(G.Qs, G.cons_n, 8 * N * sizeof(double));
   memcpy(G.A_s, G.A_snap, 3 * N * sizeof(double));
   memcpy(G.A_e, G.A_snap, 3 * N * sizeof(double));
-  memcpy(G.bxQe, G.bx_n, N * sizeof(double));
-  memcpy(G.byQe, G.by_n, N * sizeof(double));
-  memcpy(G.bxQs, G.bx_n, N * sizeof(double));
-  memcpy(G.byQs, G.by_n, N * sizeof(double));
+  const size_t NF = G.NF;
+  memcpy(G.bxQe, G.bx_n, NF * sizeof(double));
+  memcpy(G.byQe, G.by_n, NF * sizeof(double));
+  memcpy(G.bxQs, G.bx_n, NF * sizeof(double));
+  memcpy(G.byQs, G.by_n, NF * sizeof(double));
   for (int r = 0; r < rks; r++) {
     const double* H = G.Hs + (size_t)r * 8 * N;
     for (size_t n = 0; n < 8 * N; ++n) {
@@ -1527,16 +1570,16 @@ static void stage(int rks) {
   }
   for (int r = 0; r < rks; r++) {
     const double* HA = G.HsA + (size_t)r * 3 * N;
-    const double* HB = G.HsB + (size_t)r * 2 * N;
+    const double* HB = G.HsB + (size_t)r * 2 * NF;
     for (size_t n = 0; n < 3 * N; ++n) {
       G.A_e[n] += G.Ae[rks][r] * dt * HA[n];
       G.A_s[n] += G.Ai[rks][r] * dt * HA[n];
     }
-    for (size_t n = 0; n < N; ++n) {
+    for (size_t n = 0; n < NF; ++n) {
       G.bxQe[n] += G.Ae[rks][r] * dt * HB[n];
-      G.byQe[n] += G.Ae[rks][r] * dt * HB[N + n];
+      G.byQe[n] += G.Ae[rks][r] * dt * HB[NF + n];
       G.bxQs[n] += G.Ai[rks][r] * dt * HB[n];
-      G.byQs[n] += G.Ai[rks][r] * dt * HB[N + n];
+      G.byQs[n] += G.Ai[rks][r] * dt * HB[NF + n];
     }
   }
   memcpy(G.A, G.A_s, 3 * N * sizeof(double));
@@ -1583,10 +1626,10 @@ static void stage(int rks) {
   for (size_t n = 0; n < 8 * N; ++n) H[n] = (G.cons[n] - G.Qs[n]) / adt;
   double* HA = G.HsA + (size_t)rks * 3 * N;
   for (size_t n = 0; n < 3 * N; ++n) HA[n] = (G.A[n] - G.A_s[n]) / adt;
-  double* HB = G.HsB + (size_t)rks * 2 * N;
-  for (size_t n = 0; n < N; ++n) {
+  double* HB = G.HsB + (size_t)rks * 2 * G.NF;
+  for (size_t n = 0; n < G.NF; ++n) {
     HB[n] = (G.bx[n] - G.bxQs[n]) / adt;
-    HB[N + n] = (G.by[n] - G.byQs[n]) / adt;
+    HB[G.NF + n] = (G.by[n] - G.byQs[n]) / adt;
   }
 }
 
@@ -1623,16 +1666,19 @@ int ora_setup(int nx, int ny, int rks, const ora_params* p) {
   G.ny = ny;
   G.R = rks;
   G.N = (size_t)nx * ny;
+  G.NF = G.N + (size_t)nx + (size_t)ny;
+  G.xclamp = G.yclamp = 0;
   G.P = *p;
   G.dx = (p->x1 - p->x0) / nx;
   G.dy = (p->y1 - p->y0) / ny;
   size_t N = G.N;
   G.prim = alloc(8 * N); G.cons = alloc(8 * N); G.cons_n = alloc(8 * N); G.Qe = alloc(8 * N); G.Qs = alloc(8 * N);
   G.wxL = alloc(8 * N); G.wxR = alloc(8 * N); G.wyL = alloc(8 * N); G.wyR = alloc(8 * N);
-  G.bx = alloc(N); G.by = alloc(N); G.bx_n = alloc(N); G.by_n = alloc(N); G.bxQe = alloc(N); G.byQe = alloc(N);
-  G.bxQs = alloc(N); G.byQs = alloc(N); G.Fx = alloc(N); G.Fy = alloc(N);
+  const size_t NF = G.NF;
+  G.bx = alloc(NF); G.by = alloc(NF); G.bx_n = alloc(NF); G.by_n = alloc(NF); G.bxQe = alloc(NF); G.byQe = alloc(NF);
+  G.bxQs = alloc(NF); G.byQs = alloc(NF); G.Fx = alloc(N); G.Fy = alloc(N);
   G.A = alloc(3 * N); G.A_s = alloc(3 * N); G.A_e = alloc(3 * N); G.A_snap = alloc(3 * N);
-  G.Hs = alloc((size_t)rks * 8 * N); G.HsA = alloc((size_t)rks * 3 * N); G.HsB = alloc((size_t)rks * 2 * N);
+  G.Hs = alloc((size_t)rks * 8 * N); G.HsA = alloc((size_t)rks * 3 * N); G.HsB = alloc((size_t)rks * 2 * NF);
   G.Bsave = alloc(3 * N);
   memset(G.Ae, 0, sizeof G.Ae);
   memset(G.Ai, 0, sizeof G.Ai);
@@ -1699,8 +1745,8 @@ double ora_step(int snapshots) {
   G.t = G.t + G.dt;
   grid_pri2con(G.cons, G.prim);
   memcpy(G.cons_n, G.cons, 8 * N * sizeof(double));
-  memcpy(G.bx_n, G.bx, N * sizeof(double));
-  memcpy(G.by_n, G.by, N * sizeof(double));
+  memcpy(G.bx_n, G.bx, G.NF * sizeof(double));
+  memcpy(G.by_n, G.by, G.NF * sizeof(double));
   for (int r = 0; r < G.R; ++r) stage(r);
   grid_con2pri(G.prim, G.cons);
   return G.dt;
@@ -1717,7 +1763,8 @@ void ora_get_Hs(int r, double* c8, double* a3, double* b2) {
   size_t N = G.N;
   memcpy(c8, G.Hs + (size_t)r * 8 * N, 8 * N * sizeof(double));
   memcpy(a3, G.HsA + (size_t)r * 3 * N, 3 * N * sizeof(double));
-  memcpy(b2, G.HsB + (size_t)r * 2 * N, 2 * N * sizeof(double));
+  memcpy(b2, G.HsB + (size_t)r * 2 * G.NF, N * sizeof(double));
+  memcpy(b2 + N, G.HsB + (size_t)r * 2 * G.NF + G.NF, N * sizeof(double));
 }
 void ora_get_scalars(double* o) {
   o[0] = G.dt; o[1] = G.adt; o[2] = G.B_max_x; o[3] = G.B_max_y; o[4] = G.vx_max; o[5] = G.vy_max;
@@ -1824,13 +1871,27 @@ void ora_fn_substep(int sub, double h, int rks, double* ucon8, const double* Qe8
       else pre_subsystem_pressure(ucon8, Qs8, Qe8, h, rks);
       break;
     case 5:
-      if (PP.magfield == StaggerCT) staggered_ct_consistent(ucon8, bx, by, bxQs, byQs, Fx, Fy, h);
-      else if (PP.magfield == UnStaggerCT) unstaggered_ct_consistent(ucon8, A3, As3, Fx, Fy, h);
+    case 6: {
+      /* the caller's face planes are interior-only; the boundary lines of a transmissive
+       * direction come from (and go back to) the solver's own face arrays */
+      const size_t NF = G.NF, L = NF - N;
+      double *fx = alloc(NF), *fy = alloc(NF), *fxs = alloc(NF), *fys = alloc(NF);
+      memcpy(fx, bx, N * sizeof(double)); memcpy(fx + N, G.bx + N, L * sizeof(double));
+      memcpy(fy, by, N * sizeof(double)); memcpy(fy + N, G.by + N, L * sizeof(double));
+      memcpy(fxs, bxQs, N * sizeof(double)); memcpy(fxs + N, G.bxQs + N, L * sizeof(double));
+      memcpy(fys, byQs, N * sizeof(double)); memcpy(fys + N, G.byQs + N, L * sizeof(double));
+      if (sub == 5) {
+        if (PP.magfield == StaggerCT) staggered_ct_consistent(ucon8, fx, fy, fxs, fys, Fx, Fy, h);
+        else if (PP.magfield == UnStaggerCT) unstaggered_ct_consistent(ucon8, A3, As3, Fx, Fy, h);
+      } else {
+        if (PP.magfield == StaggerCT) staggered_ct_legacy(ucon8, fx, fy, fxs, fys, h);
+        else if (PP.magfield == UnStaggerCT) unstaggered_ct_legacy(ucon8, A3, As3, h);
+      }
+      memcpy(bx, fx, N * sizeof(double)); memcpy(G.bx + N, fx + N, L * sizeof(double));
+      memcpy(by, fy, N * sizeof(double)); memcpy(G.by + N, fy + N, L * sizeof(double));
+      free(fx); free(fy); free(fxs); free(fys);
       break;
-    case 6:
-      if (PP.magfield == StaggerCT) staggered_ct_legacy(ucon8, bx, by, bxQs, byQs, h);
-      else if (PP.magfield == UnStaggerCT) unstaggered_ct_legacy(ucon8, A3, As3, h);
-      break;
+    }
     default:
       break;
   }
@@ -1844,7 +1905,7 @@ double ora_div_error(void) {
     for (int j = 0; j < G.ny; j++) {
       double d;
       if (PP.magfield == StaggerCT) {
-        d = (G.bx[ID(i, j)] - G.bx[ID(i - 1, j)]) / G.dx + (G.by[ID(i, j)] - G.by[ID(i, j - 1)]) / G.dy;
+        d = (G.bx[ID(i, j)] - BXF(G.bx, i - 1, j)) / G.dx + (G.by[ID(i, j)] - BYF(G.by, i, j - 1)) / G.dy;
       } else {
         double dBxdx, dBydy;
         const double* B5 = G.cons + 5 * N;
@@ -1860,4 +1921,39 @@ double ora_div_error(void) {
       err += G.dx * G.dy * d * d;
     }
   return sqrt(err);
+}
+
+/* Boundary conditions per direction (config.hpp:36-37 ordinals): 0 Transmissive or
+ * 2 Periodic.  Call after ora_setup and before ora_load_prim.  Transmissive runs are
+ * restated for the face-based and the divergence-cleaning-free magnetic forms. */
+int ora_set_bc(int x_bc, int y_bc) {
+  if (!G.ready) return 1;
+  if ((x_bc != 0 && x_bc != 2) || (y_bc != 0 && y_bc != 2)) return 2;
+  if ((x_bc == 0 || y_bc == 0) && PP.magfield != StaggerCT && PP.magfield != NoDivFree) return 2;
+  G.xclamp = x_bc == 0;
+  G.yclamp = y_bc == 0;
+  return 0;
+}
+/* boundary normal faces: Bx on x = x_0 (ny values), By on y = y_0 (nx values) */
+void ora_set_boundary_faces(const double* bx_x0, const double* by_y0) {
+  memcpy(G.bx + G.N, bx_x0, (size_t)G.ny * sizeof(double));
+  memcpy(G.by + G.N, by_y0, (size_t)G.nx * sizeof(double));
+}
+/* a periodic direction reports the face it identifies with x_0 / y_0 (the one at x_1 / y_1) */
+static void boundary_lines(const double* bxa, const double* bya, double* bx_x0, double* by_y0) {
+  if (bx_x0)
+    for (int j = 0; j < G.ny; ++j) bx_x0[j] = BXF(bxa, -1, j);
+  if (by_y0)
+    for (int i = 0; i < G.nx; ++i) by_y0[i] = BYF(bya, i, -1);
+}
+void ora_get_boundary_faces(double* bx_x0, double* by_y0) { boundary_lines(G.bx, G.by, bx_x0, by_y0); }
+int ora_get_snapshot_boundary(int rks, int sub, int which, double* out) {
+  if (rks < 0 || rks >= MAXRK || sub < 0 || sub >= NSUB) return 1;
+  snap_t* s = &G.snaps[rks][sub];
+  if (!s->valid) return 2;
+  const double* v = which == 3 ? s->bx : which == 4 ? s->by : which == 5 ? s->bxQs : which == 6 ? s->byQs : NULL;
+  if (!v) return 3;
+  if (which == 3 || which == 5) boundary_lines(v, NULL, out, NULL);
+  else boundary_lines(NULL, v, NULL, out);
+  return 0;
 }

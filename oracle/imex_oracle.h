@@ -56,6 +56,10 @@ void ora_fn_substep(int sub, double h, int rks, double* ucon8, const double* Qe8
                     double* bx, double* by, const double* bxQs, const double* byQs, double* A3,
                     const double* As3, double* Fx, double* Fy);
 double ora_div_error(void);
+int ora_set_bc(int x_bc, int y_bc);
+void ora_set_boundary_faces(const double* bx_x0, const double* by_y0);
+void ora_get_boundary_faces(double* bx_x0, double* by_y0);
+int ora_get_snapshot_boundary(int rks, int sub, int which, double* out);
 
 #ifdef __cplusplus
 }

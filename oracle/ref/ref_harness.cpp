@@ -308,6 +308,29 @@ void ref_get_faces(double* bx, double* by) {
   array_to_plane(*S.By_0p, by);
 }
 void ref_get_A(double* A3) { grid_to_planes(*S.A, A3, 3); }
+
+// Boundary conditions (config.hpp:63-64, the x_bc / y_bc globals that main.cpp:9-233
+// sets per test).  Call before ref_load_prim so that the initial ghost fills use them.
+int ref_set_bc(int xbc, int ybc) {
+  if (xbc < 0 || xbc > 3 || ybc < 0 || ybc > 4) return 1;
+  x_bc = (x_boundary_condition)xbc;
+  y_bc = (y_boundary_condition)ybc;
+  return 0;
+}
+// The boundary normal faces that a non-periodic direction carries as degrees of freedom
+// (constrained_transport.cpp:5-30): Bx_p0 at x = x_0 (index ghost_cells - 1), one value per
+// row j, and By_0p at y = y_0, one per column i.  Periodic runs identify them with the
+// faces at x_1 / y_1.
+void ref_set_boundary_faces(const double* bx_x0, const double* by_y0) {
+  for (int j = 0; j < nyCells; ++j) (*S.Bx_p0)(ghost_cells - 1, j + ghost_cells) = bx_x0[j];
+  for (int i = 0; i < nxCells; ++i) (*S.By_0p)(i + ghost_cells, ghost_cells - 1) = by_y0[i];
+  bound_cond_staggered(*S.Bx_p0, 0);
+  bound_cond_staggered(*S.By_0p, 1);
+}
+void ref_get_boundary_faces(double* bx_x0, double* by_y0) {
+  for (int j = 0; j < nyCells; ++j) bx_x0[j] = (*S.Bx_p0)(ghost_cells - 1, j + ghost_cells);
+  for (int i = 0; i < nxCells; ++i) by_y0[i] = (*S.By_0p)(i + ghost_cells, ghost_cells - 1);
+}
 void ref_get_Hs(int r, double* cons8, double* hsa3, double* hsb2) {
   const int nx = nxCells, ny = nyCells;
   for (int j = 0; j < ny; ++j)
@@ -369,6 +392,22 @@ int ref_get_snapshot(int rks, int sub, int which, double* out) {
     case 10: arr_plane(s.Fy); break;
     default: return 3;
   }
+  return 0;
+}
+// The boundary-face line of a face snapshot (which = 3 Bx_p0, 5 Bx_p0_Qs: ny values at
+// x = x_0; 4 By_0p, 6 By_0p_Qs: nx values at y = y_0), as ref_get_boundary_faces.
+int ref_get_snapshot_boundary(int rks, int sub, int which, double* out) {
+  if (rks < 0 || rks >= MAXRK || sub < 0 || sub >= NSUB) return 1;
+  Snap& s = S.snaps[rks][sub];
+  if (!s.valid) return 2;
+  const int P = PX();
+  const std::vector<double>* v = which == 3 ? &s.bx : which == 4 ? &s.by : which == 5 ? &s.bxQs
+                                 : which == 6 ? &s.byQs : nullptr;
+  if (!v) return 3;
+  if (which == 3 || which == 5)
+    for (int j = 0; j < nyCells; ++j) out[j] = (*v)[(ghost_cells - 1) + (size_t)(j + ghost_cells) * P];
+  else
+    for (int i = 0; i < nxCells; ++i) out[i] = (*v)[(i + ghost_cells) + (size_t)(ghost_cells - 1) * P];
   return 0;
 }
 

@@ -58,6 +58,8 @@ def golden_problem(g):
     x0, x1, y0, y1 = g["domain"]
     settings = eval(str(g["settings"]))  # the repr of a plain dict of literals written by make_golden.py
     p = Problem("golden", nx, ny, x0, x1, y0, y1, prim, g["bx0"], g["by0"], g["A0"], settings=settings)
+    if "bx_x00" in g.files:
+        p.bx_x0, p.by_y0 = g["bx_x00"], g["by_y00"]
     return p, int(g["rks"]), settings
 
 

@@ -5,7 +5,9 @@ are outputs of the reference's own code (oracle/_ref/libimexref.so, built from
 the reference sources by `make -C oracle ref`) on small analytic inputs:
 
   step_<case>.npz  - initial data + state after a few full time steps
-                     (main.cpp:335-561) and the dt of each step;
+                     (main.cpp:335-561) and the dt of each step; the open-blast
+                     cases run x_Transmissive / y_Transmissive and also store the
+                     boundary normal faces (Bx at x_0, By at y_0);
   fn_<case>.npz    - single reference functions on fixed inputs:
                      TVDReconstruction, ShockDetector and the four matrix-free
                      operators of implicit_operators.cpp.
@@ -24,7 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from imex_b200.problems import vortex, vortex_sheet  # noqa: E402
+from imex_b200.problems import open_blast, vortex, vortex_sheet  # noqa: E402
 from oracle.bindings import RefSolver, make_solver  # noqa: E402
 
 CFG0 = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12)
@@ -50,13 +52,27 @@ STEP_CASES = {
     "vortex14x12_energyformula_unstag_rk1": (lambda: vortex(14, 12), 1,
                                              dict(recon="Minmod", magfield="UnStaggerCT",
                                                   formula="EnergyFormula"), 2),
+    # transmissive boundaries (open_blast sets x_Transmissive / y_Transmissive)
+    "blast16x14_minmod_open": (lambda: open_blast(16, 14), 2, dict(recon="Minmod", magfield="StaggerCT"), 3),
+    "blast16_weno5_open_rk3": (lambda: open_blast(16), 3,
+                               dict(recon="WENO5", magfield="StaggerCT", p_floor=1e-8), 2),
+    "blast14x12_eno3_nodivfree_open": (lambda: open_blast(14, 12), 2, dict(recon="ENO3", magfield="NoDivFree"), 2),
+    "blast16_primstate_rkeos_open": (lambda: open_blast(16), 2,
+                                     dict(recon="VanLeer", reconstate="PrimState", magfield="StaggerCT",
+                                          eos_type="REDLICH_KWONG", m_alfa=0.05, m_b=0.1), 2),
+    "blast16_energyformula_open": (lambda: open_blast(16), 2,
+                                   dict(recon="Minmod", magfield="StaggerCT", formula="EnergyFormula",
+                                        GMREStol=1e-12), 2),
+    "blast16x12_xperiodic_open_y": (lambda: open_blast(16, 12), 2,
+                                    dict(recon="VanLeer", magfield="StaggerCT", x_bc="x_Periodic",
+                                         floor_on=0, PressureSolver="once_correction"), 2),
 }
 
 
 def step_case(name: str, factory, rks: int, settings: dict, steps: int) -> None:
     prob = factory()
     ref = make_solver("ref", prob, rks, settings)
-    dts, cons, faces_x, faces_y, As = [], [], [], [], []
+    dts, cons, faces_x, faces_y, As, lines_x, lines_y = [], [], [], [], [], [], []
     for _ in range(steps):
         dts.append(ref.step())
         cons.append(ref.cons())
@@ -64,13 +80,19 @@ def step_case(name: str, factory, rks: int, settings: dict, steps: int) -> None:
         faces_x.append(bx)
         faces_y.append(by)
         As.append(ref.vector_potential())
+        bxb, byb = ref.boundary_faces()
+        lines_x.append(bxb)
+        lines_y.append(byb)
+    extra = {}
+    if prob.bx_x0 is not None:
+        extra = dict(bx_x00=prob.bx_x0, by_y00=prob.by_y0, bx_x0=np.array(lines_x), by_y0=np.array(lines_y))
     np.savez_compressed(
         os.path.join(HERE, f"step_{name}.npz"),
         prim0=prob.prim, bx0=prob.bx, by0=prob.by, A0=prob.A, rks=rks,
         domain=np.array([prob.x0, prob.x1, prob.y0, prob.y1]),
         settings=np.array(repr(dict(prob.settings, **settings))),
         dt=np.array(dts), cons=np.array(cons), bx=np.array(faces_x), by=np.array(faces_y),
-        A=np.array(As), div=np.array(ref.div_error()))
+        A=np.array(As), div=np.array(ref.div_error()), **extra)
 
 
 def fn_case() -> None:

@@ -35,6 +35,10 @@ def test_port_reproduces_reference_golden_steps(case):
             np.testing.assert_array_equal(port.vector_potential(), g["A"][s])
         else:
             assert rel(cons, g["cons"][s]) < 1e-13
+        if "bx_x0" in g.files:  # boundary normal faces of the transmissive directions
+            bxb, byb = port.boundary_faces()
+            np.testing.assert_allclose(bxb, g["bx_x0"][s], rtol=0 if exact else 1e-13, atol=0)
+            np.testing.assert_allclose(byb, g["by_y0"][s], rtol=0 if exact else 1e-13, atol=0)
     assert port.div_error() == pytest.approx(float(g["div"]), rel=1e-10, abs=1e-14)
 
 
@@ -88,6 +92,45 @@ def test_port_matches_live_reference(kind, n, rks, settings, steps):
                 if a is not None:
                     np.testing.assert_array_equal(b, a, err_msg=f"stage {k} after {sub}")
     np.testing.assert_array_equal(port.cons(), ref.cons())
+
+
+@pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("rks,settings", [
+    (2, dict(recon="VanLeer", magfield="StaggerCT")),
+    (3, dict(recon="WENO5", magfield="StaggerCT", p_floor=1e-8, y_bc="y_Periodic")),
+    (2, dict(recon="Minmod", magfield="NoDivFree", formula="EnergyFormula", GMREStol=1e-12)),
+], ids=["vanleer_ct", "weno5_ct_yperiodic", "minmod_nodivfree_energy"])
+def test_port_matches_live_reference_transmissive(rks, settings):
+    """Transmissive boundaries: every sub-step of every stage, boundary faces included."""
+    from imex_b200.problems import open_blast
+    prob = open_blast(18, 14)
+    ref = make_solver("ref", prob, rks, settings)
+    port = make_solver("port", prob, rks, settings)
+    for _ in range(2):
+        assert ref.step(snapshots=True) == port.step(snapshots=True)
+        for k in range(rks):
+            for sub in ("combine", "convective", "magnetic", "pflux", "pressure", "ct"):
+                a, b = ref.snapshot(k, sub, "u_con"), port.snapshot(k, sub, "u_con")
+                assert (a is None) == (b is None)
+                if a is None:
+                    continue
+                np.testing.assert_array_equal(b, a, err_msg=f"stage {k} after {sub}")
+                for w in ("bx", "by", "bxQs", "byQs"):
+                    np.testing.assert_array_equal(port.snapshot(k, sub, w), ref.snapshot(k, sub, w))
+                    np.testing.assert_array_equal(port.snapshot_boundary(k, sub, w),
+                                                  ref.snapshot_boundary(k, sub, w), err_msg=f"{w} line")
+    np.testing.assert_array_equal(port.cons(), ref.cons())
+    assert port.div_error() == ref.div_error()
+
+
+def test_port_refuses_unsupported_boundaries():
+    from imex_b200.problems import open_blast
+    prob = open_blast(12)
+    for bc, magfield in ((("x_Reflective", "y_Periodic"), "StaggerCT"), (("x_Dirichlet", "y_Periodic"), "StaggerCT"),
+                         (("x_Periodic", "y_JetInflow"), "StaggerCT"), (("x_Transmissive", "y_Periodic"), "PotentialA"),
+                         (("x_Periodic", "y_Transmissive"), "UnStaggerCT")):
+        with pytest.raises(RuntimeError):
+            make_solver("port", prob, 2, dict(magfield=magfield, x_bc=bc[0], y_bc=bc[1]))
 
 
 @pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
