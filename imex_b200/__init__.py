@@ -31,14 +31,16 @@ UUPDATE = {"ConservationofU": 0, "DefinitionofU": 1}
 PSOLVER = {"no_correction": 0, "once_correction": 1, "all_correction": 2}
 EOS = {"IDEAL_GAS": 0, "REDLICH_KWONG": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
+XBC = {"x_Transmissive": 0, "x_Reflective": 1, "x_Periodic": 2, "x_Dirichlet": 3}
+YBC = {"y_Transmissive": 0, "y_Reflective": 1, "y_Periodic": 2, "y_Dirichlet": 3, "y_JetInflow": 4}
 ENUMS = dict(formula=FORMULA, magfield=MAGFIELD, recon=RECON, reconstate=RECONSTATE,
              caltimestep=DTCALC, add_pvisc=PVISC, U_update=UUPDATE, PressureSolver=PSOLVER,
-             eos_type=EOS, precision=PRECISION)
+             eos_type=EOS, precision=PRECISION, x_bc=XBC, y_bc=YBC)
 
 OP = {"pressure_L": 0, "pressure_J": 1, "magnetic_B": 2, "magnetic_A": 3, "energy": 4}
 BUF = {"cons": 0, "prim": 1, "cons_n": 2, "Qe": 3, "Qs": 4, "bx": 5, "by": 6, "bxQs": 7,
        "byQs": 8, "A": 9, "A_s": 10, "Fx": 11, "Fy": 12, "w": 13, "Hs": 14, "HsA": 15,
-       "HsB": 16, "eta": 17}
+       "HsB": 16, "eta": 17, "bx_x0": 18, "by_y0": 19, "bxQs_x0": 20, "byQs_y0": 21}
 BUF_PLANES = {"cons": 8, "prim": 8, "cons_n": 8, "Qe": 8, "Qs": 8, "bx": 1, "by": 1, "bxQs": 1,
               "byQs": 1, "A": 3, "A_s": 3, "Fx": 1, "Fy": 1, "w": 32, "Hs": 8, "HsA": 3,
               "HsB": 2, "eta": 1}
@@ -123,6 +125,8 @@ _SIGS = {
     "imex_upload_prim": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "imex_upload_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "imex_download_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D]),
+    "imex_set_boundary_faces": (C.c_int, [C.c_void_p, _D, _D]),
+    "imex_get_boundary_faces": (C.c_int, [C.c_void_p, _D, _D]),
     "imex_step": (C.c_int, [C.c_void_p, _D]),
     "imex_begin_step": (C.c_int, [C.c_void_p]),
     "imex_stage": (C.c_int, [C.c_void_p, C.c_int]),
@@ -246,7 +250,8 @@ def _c(a) -> np.ndarray:
 
 
 class Solver:
-    """One imex_ctx: the state of one 2D periodic MHD run on the current GPU."""
+    """One imex_ctx: the state of one 2D MHD run (periodic or transmissive per direction) on the
+    current GPU."""
 
     def __init__(self, nx: int, ny: int, settings: dict | None = None, domain=None,
                  rks: int | None = None, config: Config | None = None):
@@ -296,6 +301,20 @@ class Solver:
     def load(self, prob) -> None:
         prim, bx, by, A = _c(prob.prim), _c(prob.bx), _c(prob.by), _c(prob.A)
         self._check(self.lib.imex_upload_prim(self.ctx, _dp(prim), _dp(bx), _dp(by), _dp(A)))
+        if getattr(prob, "bx_x0", None) is not None:
+            self.set_boundary_faces(prob.bx_x0, prob.by_y0)
+
+    def set_boundary_faces(self, bx_x0, by_y0) -> None:
+        """Bx on x = x_0 (ny values) and By on y = y_0 (nx values) of the transmissive
+        directions (imex_set_boundary_faces); a periodic direction ignores its line."""
+        bx0, by0 = _c(bx_x0).reshape(self.ny), _c(by_y0).reshape(self.nx)
+        self._check(self.lib.imex_set_boundary_faces(self.ctx, _dp(bx0), _dp(by0)))
+
+    def boundary_faces(self) -> tuple[np.ndarray, np.ndarray]:
+        """(Bx on x = x_0, By on y = y_0); a periodic direction gives the faces at x_1 / y_1."""
+        bx0, by0 = np.empty(self.ny), np.empty(self.nx)
+        self._check(self.lib.imex_get_boundary_faces(self.ctx, _dp(bx0), _dp(by0)))
+        return bx0, by0
 
     def _planes(self, k):
         return np.empty((k, self.ny, self.nx)) if k > 1 else np.empty((self.ny, self.nx))
@@ -401,16 +420,21 @@ class Solver:
         self._check(self.lib.imex_reset_stats(self.ctx))
 
     # ---- buffers
+    def _line(self, name: str) -> int | None:
+        """Length of a boundary-face line buffer (ny for an x_0 line, nx for a y_0 line)."""
+        return {"bx_x0": self.ny, "bxQs_x0": self.ny, "by_y0": self.nx, "byQs_y0": self.nx}.get(name)
+
     def get_buffer(self, name: str, index: int = 0) -> np.ndarray:
-        k = BUF_PLANES[name]
-        out = self._planes(k)
+        n = self._line(name)
+        out = np.empty(n) if n else self._planes(BUF_PLANES[name])
         self._check(self.lib.imex_get_buffer(self.ctx, BUF[name], index, _dp(out)))
         return out
 
     def set_buffer(self, name: str, data, index: int = 0) -> None:
         a = _c(data)
-        if a.size != BUF_PLANES[name] * self.N:
-            raise ValueError(f"{name}: expected {BUF_PLANES[name] * self.N} values, got {a.size}")
+        want = self._line(name) or BUF_PLANES[name] * self.N
+        if a.size != want:
+            raise ValueError(f"{name}: expected {want} values, got {a.size}")
         self._check(self.lib.imex_set_buffer(self.ctx, BUF[name], index, _dp(a)))
 
     # ---- sub-steps (reference function names)

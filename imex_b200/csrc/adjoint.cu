@@ -1166,6 +1166,7 @@ imex_status supported(imex_ctx* ctx) {
   else if (!(P.fixed_dt > 0.0)) why = "a fixed time step (fixed_dt > 0)";
   else if (P.Energy_Modify) why = "Energy_Modify off";
   else if (ctx->cfg.precision != IMEX_PRECISION_FP64) why = "FP64 precision";
+  else if (P.xclamp || P.yclamp) why = "periodic boundaries";
   if (!why) return IMEX_OK;
   return set_error(ctx, IMEX_ERR_UNSUPPORTED, std::string("the adjoint needs ") + why);
 }

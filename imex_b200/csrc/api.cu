@@ -79,8 +79,12 @@ constexpr int NPSLOTS = 32;
 imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if (nx < 4 || ny < 4) return why = "grid must be at least 4 x 4", IMEX_ERR_INVALID;
   if (c->RKs < 1 || c->RKs > kMaxRK) return why = "RKs must be 1, 2 or 3", IMEX_ERR_INVALID;
-  if (c->x_bc != IMEX_x_Periodic || c->y_bc != IMEX_y_Periodic)
-    return why = "only periodic boundaries are implemented", IMEX_ERR_UNSUPPORTED;
+  if ((c->x_bc != IMEX_x_Periodic && c->x_bc != IMEX_x_Transmissive) ||
+      (c->y_bc != IMEX_y_Periodic && c->y_bc != IMEX_y_Transmissive))
+    return why = "only periodic and transmissive boundaries are implemented", IMEX_ERR_UNSUPPORTED;
+  if ((c->x_bc == IMEX_x_Transmissive || c->y_bc == IMEX_y_Transmissive) && c->magfield != IMEX_StaggerCT &&
+      c->magfield != IMEX_NoDivFree)
+    return why = "transmissive boundaries are implemented for StaggerCT and NoDivFree", IMEX_ERR_UNSUPPORTED;
   if (c->formula != IMEX_PressureFormula && c->formula != IMEX_EnergyFormula) return why = "bad formula", IMEX_ERR_INVALID;
   if (!c->GLF) return why = "only the global Lax-Friedrichs dissipation (GLF) is implemented", IMEX_ERR_UNSUPPORTED;
   if (c->U_update != IMEX_DefinitionofU) return why = "only DefinitionofU is implemented", IMEX_ERR_UNSUPPORTED;
@@ -146,6 +150,10 @@ double* buffer_ptr(imex_ctx* ctx, int which, int index, size_t* count) {
       *count = 2 * N;
       return ctx->HsB + (size_t)index * 2 * N;
     case IMEX_BUF_SHOCK: *count = N; return ctx->eta;
+    case IMEX_BUF_BX_X0: *count = (size_t)ctx->ny; return ctx->bl.bx;
+    case IMEX_BUF_BY_Y0: *count = (size_t)ctx->nx; return ctx->bl.by;
+    case IMEX_BUF_BX_QS_X0: *count = (size_t)ctx->ny; return ctx->bl.bxQs;
+    case IMEX_BUF_BY_QS_Y0: *count = (size_t)ctx->nx; return ctx->bl.byQs;
     default: return nullptr;
   }
 }
@@ -256,6 +264,8 @@ imex_status ct_entry(imex_ctx* ctx, double h, int variant, int needed_magfield) 
   if (!ctx) return IMEX_ERR_INVALID;
   if (ctx->P.magfield != needed_magfield)
     return set_error(ctx, IMEX_ERR_INVALID, "CT variant does not match the configured magfield");
+  if (variant >= 2 && (ctx->P.xclamp || ctx->P.yclamp))
+    return set_error(ctx, IMEX_ERR_UNSUPPORTED, "the legacy CT variants are implemented for periodic boundaries");
   imex_status s = set_h(ctx, h);
   return s != IMEX_OK ? s : launch_ct(ctx, variant);
 }
@@ -391,6 +401,8 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   P.CFL = cfg->CFL;
   P.time_stop = cfg->time_stop;
   P.fixed_dt = cfg->fixed_dt;
+  P.xclamp = cfg->x_bc == IMEX_x_Transmissive;
+  P.yclamp = cfg->y_bc == IMEX_y_Transmissive;
 
   const size_t N = ctx->N;
   const size_t R = (size_t)cfg->RKs;
@@ -409,6 +421,8 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   A_(pb, N); A_(pp, N); A_(pf, N); A_(pg, N); A_(pdp, N);
   A_(mx, 3 * N); A_(mb, 3 * N);
   A_(chit, N); A_(Epp, N); A_(Et, N);
+  const size_t lx = (size_t)ny, ly = (size_t)nx;
+  A_(bline, (4 + R) * (lx + ly) + (lx + 1) + (ly + 1));
   A_(V, kv * 3 * N); A_(AV, 2 * 3 * N);
   if (cfg->precision == IMEX_PRECISION_MIXED) {
     A_(Vf, kv * 3 * N); A_(AVf, 2 * 3 * N); A_(mres, 3 * N); A_(mcor, 3 * N);
@@ -422,6 +436,16 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_st, sizeof(DevStats));
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_red, 64 * sizeof(double));
     if (e != cudaSuccess) s = cuda_check(ctx, e, "cudaMallocHost");
+  }
+  if (s == IMEX_OK) {
+    BoundaryLines& L = ctx->bl;
+    double* q = ctx->bline;
+    L.bx = q; q += lx; L.bx_n = q; q += lx; L.bxQe = q; q += lx; L.bxQs = q; q += lx; L.hsbx = q; q += R * lx;
+    L.by = q; q += ly; L.by_n = q; q += ly; L.byQe = q; q += ly; L.byQs = q; q += ly; L.hsby = q; q += R * ly;
+    L.ex = q; q += lx + 1;
+    L.ey = q;
+    e = cudaMemsetAsync(ctx->bline, 0, ((4 + R) * (lx + ly) + (lx + 1) + (ly + 1)) * sizeof(double), ctx->stream);
+    if (e != cudaSuccess) s = cuda_check(ctx, e, "boundary lines");
   }
   if (s == IMEX_OK) {
     std::memset(ctx->h_sc, 0, sizeof(DevScalars));
@@ -485,6 +509,13 @@ imex_status imex_upload_prim(imex_ctx* ctx, const double* prim8, const double* b
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->bx, bx, pl, cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by, by, pl, cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A, A3, 3 * pl, cudaMemcpyDefault, ctx->stream);
+  // boundary faces of a transmissive direction until imex_set_boundary_faces sets them: the
+  // first interior face of the row / column (Bx(1/2, j), By(i, 1/2))
+  if (e == cudaSuccess && ctx->P.xclamp)
+    e = cudaMemcpy2DAsync(ctx->bl.bx, sizeof(double), ctx->bx, ctx->nx * sizeof(double), sizeof(double), ctx->ny,
+                          cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess && ctx->P.yclamp)
+    e = cudaMemcpyAsync(ctx->bl.by, ctx->by, ctx->nx * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "state upload");
   imex_status s = launch_cons_from_prim(ctx);
   if (s != IMEX_OK) return s;
@@ -518,6 +549,31 @@ imex_status imex_download_state(imex_ctx* ctx, double* cons8, double* prim8, dou
   if (A3 && e == cudaSuccess) e = cudaMemcpyAsync(A3, ctx->A, 3 * pl, cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   return cuda_check(ctx, e, "state download");
+}
+
+imex_status imex_set_boundary_faces(imex_ctx* ctx, const double* bx_x0, const double* by_y0) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  cudaError_t e = cudaSuccess;
+  if (bx_x0 && ctx->P.xclamp) e = cudaMemcpyAsync(ctx->bl.bx, bx_x0, ctx->ny * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (by_y0 && ctx->P.yclamp && e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->bl.by, by_y0, ctx->nx * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_check(ctx, e, "boundary faces upload");
+}
+
+imex_status imex_get_boundary_faces(imex_ctx* ctx, double* bx_x0, double* by_y0) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  cudaError_t e = cudaSuccess;
+  const size_t d = sizeof(double);
+  if (bx_x0)  // a periodic x reports Bx(x_1, j), the face it identifies with x_0
+    e = ctx->P.xclamp ? cudaMemcpyAsync(bx_x0, ctx->bl.bx, ctx->ny * d, cudaMemcpyDefault, ctx->stream)
+                      : cudaMemcpy2DAsync(bx_x0, d, ctx->bx + (ctx->nx - 1), ctx->nx * d, d, ctx->ny, cudaMemcpyDefault,
+                                          ctx->stream);
+  if (by_y0 && e == cudaSuccess)
+    e = cudaMemcpyAsync(by_y0, ctx->P.yclamp ? ctx->bl.by : ctx->by + (ctx->N - ctx->nx), ctx->nx * d, cudaMemcpyDefault,
+                        ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_check(ctx, e, "boundary faces download");
 }
 
 imex_status imex_begin_step(imex_ctx* ctx) {

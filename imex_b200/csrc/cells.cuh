@@ -9,7 +9,7 @@
 
 namespace imex {
 
-// the 3x3 neighbourhood of cell (i, j), periodic: nb[(dj + 1) * 3 + (di + 1)]
+// the 3x3 neighbourhood of cell (i, j) (periodic images or clamped cells, cid): nb[(dj + 1) * 3 + (di + 1)]
 enum { NB_SW = 0, NB_S, NB_SE, NB_W, NB_C, NB_E, NB_NW, NB_N, NB_NE };
 __device__ __forceinline__ void neighbours(const DevParams& P, int i, int j, long long* nb) {
 #pragma unroll
@@ -164,20 +164,30 @@ __device__ __forceinline__ S cell_ez(Ld& ld, long long m) {
   const S r = ld(CC_UCON, 0, m);
   return ld(CC_UCON, 2, m) / r * ld(CC_UCON, 5, m) - ld(CC_UCON, 1, m) / r * ld(CC_UCON, 6, m);
 }
+// bnb: the neighbourhood Ez_bar is evaluated on.  It is nb itself except at a corner on
+// x = x_0 or y = y_0 of a transmissive direction, where bound_cond_array has replaced
+// Ez_bar by its value at the nearest interior corner (constrained_transport.cpp:150-155)
+// while the correction terms still read the corner's own neighbourhood.
 template <class S, class Ld>
-__device__ __forceinline__ void ct_corner_cell(const DevParams& P, double sx, double sy, const long long* nb, Ld& ld,
-                                               S* out) {
+__device__ __forceinline__ void ct_corner_at(const DevParams& P, double sx, double sy, const long long* nb,
+                                             const long long* bnb, Ld& ld, S* out) {
   const long long c00 = nb[NB_C], c10 = nb[NB_E], c01 = nb[NB_N], c11 = nb[NB_NE];
   const double dx = P.dx, dy = P.dy;
   const S Ep0_00 = sx * ld(CC_FX, 0, c00), Ep0_01 = sx * ld(CC_FX, 0, c01);
   const S E0p_00 = sy * ld(CC_FY, 0, c00), E0p_10 = sy * ld(CC_FY, 0, c10);
   const S Et00 = cell_ez<S>(ld, c00), Et10 = cell_ez<S>(ld, c10), Et01 = cell_ez<S>(ld, c01), Et11 = cell_ez<S>(ld, c11);
-  const S bar = 0.25 * (Ep0_00 + Ep0_01 + E0p_00 + E0p_10);
+  const S bar = 0.25 * (sx * ld(CC_FX, 0, bnb[NB_C]) + sx * ld(CC_FX, 0, bnb[NB_N]) + sy * ld(CC_FY, 0, bnb[NB_C]) +
+                        sy * ld(CC_FY, 0, bnb[NB_E]));
   const S t1 = 0.5 * ((Ep0_00 - Et00) / (dx / 2.0) + (Ep0_01 - Et01) / (dx / 2.0));
   const S t2 = 0.5 * ((Et10 - Ep0_00) / (dx / 2.0) + (Et11 - Ep0_01) / (dx / 2.0));
   const S t3 = 0.5 * ((E0p_00 - Et00) / (dy / 2.0) + (E0p_10 - Et10) / (dy / 2.0));
   const S t4 = 0.5 * ((Et01 - E0p_00) / (dy / 2.0) + (Et11 - E0p_10) / (dy / 2.0));
   out[0] = bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
+}
+template <class S, class Ld>
+__device__ __forceinline__ void ct_corner_cell(const DevParams& P, double sx, double sy, const long long* nb, Ld& ld,
+                                               S* out) {
+  ct_corner_at<S>(P, sx, sy, nb, nb, ld, out);
 }
 
 // ---- frozen pressure-operator coefficient hh = h(Qe) rho_e / rho (imex_subsystems.cpp:92-104)

@@ -23,8 +23,13 @@ __device__ __forceinline__ int wrap(int i, int n) {
 }
 // neighbour index with |offset| < n
 __device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+__device__ __forceinline__ int clamp1(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+// the cell a neighbour index (|offset| < n) reads: the periodic image, or the nearest
+// interior cell of a transmissive direction
+__device__ __forceinline__ int cix(const DevParams& P, int i) { return P.xclamp ? clamp1(i, P.nx) : wrap1(i, P.nx); }
+__device__ __forceinline__ int cjy(const DevParams& P, int j) { return P.yclamp ? clamp1(j, P.ny) : wrap1(j, P.ny); }
 __device__ __forceinline__ long long cid(const DevParams& P, int i, int j) {
-  return (long long)wrap1(i, P.nx) + (long long)P.nx * wrap1(j, P.ny);
+  return (long long)cix(P, i) + (long long)P.nx * cjy(P, j);
 }
 
 // ---------------------------------------------------------------- EOS

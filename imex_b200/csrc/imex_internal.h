@@ -24,6 +24,22 @@ struct DevParams {
   int U_update, PressureSolver, Energy_Modify, floor_on, Pnewton_max, eos_type, caltimestep, RKs;
   double gamma, m_alfa, m_b, m_R, m_cv;
   double p_floor, Mbig_fac, theta, Pnewton_tol, shock_kappa1, GMREStol, CFL, time_stop, fixed_dt;
+  // 1 where the direction is transmissive: neighbour indices clamp to the nearest interior
+  // cell (bound_cond_u / bound_cond_array / M_P / M_B, boundary.cpp:7-16,
+  // timestep.cpp:168-204, implicit_operators.cpp:12-14); 0 where it is periodic (wrap)
+  int xclamp, yclamp;
+};
+
+// Boundary normal faces of the transmissive directions.  The reference keeps Bx_p0 at
+// x = x_0 and By_0p at y = y_0 as degrees of freedom that CT evolves and that the cell
+// average of the first row / column reads (constrained_transport.cpp:5-30,
+// ct_flux.cpp:176-189); a periodic direction identifies them with the faces at x_1 / y_1.
+// One line of ny values per Bx array, nx per By array; ex / ey hold the corner EMFs on
+// x = x_0 (corners j - 1/2 for j = 0..ny) and on y = y_0 (corners i - 1/2 for i = 0..nx).
+struct BoundaryLines {
+  double *bx, *bx_n, *bxQe, *bxQs, *hsbx;  // hsbx: RKs lines (the HsB of each stage)
+  double *by, *by_n, *byQe, *byQs, *hsby;
+  double *ex, *ey;
 };
 
 // Scalars living in device memory (the reference's hidden globals).
@@ -96,6 +112,8 @@ struct imex_ctx {
   double *pb = nullptr, *pp = nullptr, *pf = nullptr, *pg = nullptr, *pdp = nullptr;  // pressure vectors
   double *mx = nullptr, *mb = nullptr;  // magnetic solution / rhs (3 planes each)
   double *chit = nullptr, *Epp = nullptr, *Et = nullptr;
+  double* bline = nullptr;  // storage of the boundary lines
+  imex::BoundaryLines bl{};
   // GMRES workspace
   double* V = nullptr;      // (restart + 1) * 3 planes
   double* AV = nullptr;     // 2 * 3 planes

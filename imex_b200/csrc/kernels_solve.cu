@@ -92,11 +92,14 @@ __device__ bool grid_barrier(SyncState* s, unsigned nblk) {
 struct Tiling {
   int nx, ny, tiles_x, ntiles;
   long long N;
+  int xclamp, yclamp;  // transmissive directions: the halo clamps instead of wrapping
 };
-__host__ __device__ inline Tiling make_tiling(int nx, int ny) {
+__host__ __device__ inline Tiling make_tiling(int nx, int ny, int xclamp = 0, int yclamp = 0) {
   Tiling t;
   t.nx = nx;
   t.ny = ny;
+  t.xclamp = xclamp;
+  t.yclamp = yclamp;
   t.N = (long long)nx * ny;
   t.tiles_x = (nx + TX - 1) / TX;
   t.ntiles = t.tiles_x * ((ny + TY - 1) / TY);
@@ -630,7 +633,9 @@ __device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const T
     int q = threadIdx.x + r * NT;
     if (q >= TB::SN) q = TB::SN - 1;  // an already staged cell: loaded again, never stored
     const int sxq = q % TB::SX, syq = q / TB::SX;
-    const int gi = wrapc(x0 + sxq - Op::HALO, T.nx), gj = wrapc(y0 + syq - Op::HALO, T.ny);
+    const int xi = x0 + sxq - Op::HALO, yj = y0 + syq - Op::HALO;
+    const int gi = T.xclamp ? (xi < 0 ? 0 : (xi >= T.nx ? T.nx - 1 : xi)) : wrapc(xi, T.nx);
+    const int gj = T.yclamp ? (yj < 0 ? 0 : (yj >= T.ny ? T.ny - 1 : yj)) : wrapc(yj, T.ny);
     c[r] = (long long)gi + (long long)T.nx * gj;
   }
   VT qv[Q][QC];
@@ -1986,7 +1991,7 @@ imex_status pressure_setup(imex_ctx* ctx) {
 // refinement kernel around FP32 inner cycles.
 template <class Op>
 imex_status gmres_run(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, int kind) {
-  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   if (!mixed(ctx, kind)) {
     auto kern = k_gmres<Op>;
     const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
@@ -2038,7 +2043,7 @@ bool on_device(const void* p) {
 template <class Op>
 imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, unsigned char* base,
                              size_t capacity) {
-  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   auto kern = k_gmres<Op>;
   const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
   const size_t n = (size_t)Op::M * (size_t)T.N;
@@ -2091,7 +2096,7 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   PressureOp o = make_pressure_op(ctx);
   if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS)  // a single linear GMRES with L (implicit_operators.cpp:664-668)
     return gmres_run(ctx, o, F_NEWTON, p, b, IMEX_MIXED_PRESSURE);
-  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   NewtonArgs na{};
   na.p = p;
   na.pf = ctx->pf;
@@ -2506,7 +2511,7 @@ imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig) {
 }
 
 imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
-  Tiling T = make_tiling(ctx->nx, ctx->ny);
+  Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   int nb = T.ntiles < ctx->max_blocks ? T.ntiles : ctx->max_blocks;
   if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
     PressureOp o = make_pressure_op(ctx);
@@ -2545,7 +2550,7 @@ imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b,
 
 imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                  double* us_per_barrier) {
-  const Tiling T = make_tiling(ctx->nx, ctx->ny);
+  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   int nb = coop_blocks<MagneticAOp>(ctx, (const void*)k_gmres<MagneticAOp>, T);
   const double saved = ctx->barrier_timeout_s;
   ctx->barrier_timeout_s = timeout_s;
@@ -2781,7 +2786,7 @@ imex_status adj_transpose_solve_op(imex_ctx* ctx, const AdjOp& a, double* AT, do
   AssembledTOp<M> T{};
   T.AT = AT;
   T.N = P.N;
-  const Tiling TL = make_tiling(ctx->nx, ctx->ny);
+  const Tiling TL = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   auto kern = k_gmres<AssembledTOp<M>>;
   const int nblk = coop_blocks<AssembledTOp<M>>(ctx, (const void*)kern, TL);
   GmresWork g = make_work(ctx, TL, nblk, F_ADJOINT);
@@ -2823,7 +2828,7 @@ imex_status adj_coef_vjp(imex_ctx* ctx, const AdjOp& a, const double* x, const d
   return adj_coef_vjp_op<PressureOp>(ctx, a, x, mu, lam_q, lam_visc);
 }
 imex_status adj_apply(imex_ctx* ctx, const AdjOp& a, const double* x, double* Ax) {
-  Tiling T = make_tiling(ctx->nx, ctx->ny);
+  Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
   int nb = T.ntiles < ctx->max_blocks ? T.ntiles : ctx->max_blocks;
   if (a.kind == ADJ_OP_MAGNETIC_B) {
     MagneticBOp o;

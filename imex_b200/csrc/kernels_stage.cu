@@ -3,7 +3,7 @@
 // constrained transport, stage derivative, and diagnostics.
 //
 // Every kernel here is a memory-bound stencil over interior-only SoA planes
-// with periodic wrap-around (no ghost cells): one thread per cell, loads
+// with periodic or clamped neighbour indices (no ghost cells): one thread per cell, loads
 // through the read-only path so the stencil neighbours hit L1.
 #include <cstdio>
 #include <cstring>
@@ -362,41 +362,110 @@ __global__ void __launch_bounds__(FNT, 3) k_flux_mag(DevParams P, const DevScala
 }
 
 // ---------------------------------------------------------------- constrained transport
-// Corner EMF of u_con and the collected face fluxes (ct_corner_cell).
+// corner EMF (ci + 1/2, cj + 1/2) for ci, cj >= -1 (ct_corner_at): Ez_bar on the corner
+// index as bound_cond_array leaves it (clamped to 0 on x_0 / y_0 of a transmissive
+// direction, the periodic image otherwise), the correction terms on the corner itself
+template <class Ld>
+__device__ __forceinline__ double corner_emf(const DevParams& P, double sx, double sy, int ci, int cj, Ld& ld) {
+  long long nb[9], bnb[9];
+  neighbours(P, ci, cj, nb);
+  const int bi = ci < 0 ? (P.xclamp ? 0 : P.nx + ci) : ci, bj = cj < 0 ? (P.yclamp ? 0 : P.ny + cj) : cj;
+  neighbours(P, bi, bj, bnb);
+  double out[1];
+  ct_corner_at<double>(P, sx, sy, nb, bnb, ld, out);
+  return out[0];
+}
+// Corner EMF of u_con and the collected face fluxes (ct_corner_cell); on a transmissive
+// direction the first column / row of threads also writes the boundary corners (-1/2).
 __global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
-                            double sy, const double* __restrict__ ucon, double* __restrict__ Epp) {
+                            double sy, const double* __restrict__ ucon, double* __restrict__ Epp, BoundaryLines L) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
   long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  neighbours(P, i, j, nb);
   const double* arr[3] = {fx, fy, ucon};
   auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
   double out[1];
   ct_corner_cell<double>(P, sx, sy, nb, ld, out);
   Epp[n] = out[0];
+  if (P.xclamp && i == 0) {
+    L.ex[j + 1] = corner_emf(P, sx, sy, -1, j, ld);
+    if (j == 0) L.ex[0] = corner_emf(P, sx, sy, -1, -1, ld);
+  }
+  if (P.yclamp && j == 0) {
+    L.ey[i + 1] = corner_emf(P, sx, sy, i, -1, ld);
+    if (i == 0) L.ey[0] = corner_emf(P, sx, sy, -1, -1, ld);
+  }
+}
+// corner (ci + 1/2, cj + 1/2), ci, cj >= -1, from the corner plane and the boundary lines
+__device__ __forceinline__ double corner_read(const DevParams& P, const double* __restrict__ Epp,
+                                              const BoundaryLines& L, int ci, int cj) {
+  if (ci < 0 && P.xclamp) return L.ex[cj + 1];
+  if (cj < 0 && P.yclamp) return L.ey[cix(P, ci) + 1];
+  return __ldg(Epp + cid(P, ci, cj));
 }
 // Face update from the corner EMF and cell B = face average
 // (ct_flux.cpp:174-189, constrained_transport.cpp:128-141).  The neighbour faces
 // are recomputed with the same arithmetic rather than re-read.
+// On a transmissive direction the faces left of / below the first column / row are the
+// boundary faces (their own lines, corner EMFs from the boundary corners), which the
+// first column / row of threads also stores.
 __global__ void k_ct_faces(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
                            const double* __restrict__ bxQs, const double* __restrict__ byQs, double* __restrict__ bx,
-                           double* __restrict__ by, double* __restrict__ ucon) {
+                           double* __restrict__ by, double* __restrict__ ucon, BoundaryLines L) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
   const double h = sc->h;
-  const long long im = cid(P, i - 1, j), jm = cid(P, i, j - 1), imjm = cid(P, i - 1, j - 1);
-  double e00 = __ldg(Epp + n), em0 = __ldg(Epp + im), e0m = __ldg(Epp + jm), emm = __ldg(Epp + imjm);
+  const bool xb = P.xclamp && i == 0, yb = P.yclamp && j == 0;
+  double e00 = __ldg(Epp + n), em0 = corner_read(P, Epp, L, i - 1, j), e0m = corner_read(P, Epp, L, i, j - 1);
+  double emm = corner_read(P, Epp, L, i - 1, j - 1);
   double fx = __ldg(bxQs + n) - h / P.dy * (e00 - e0m);
   double fy = __ldg(byQs + n) + h / P.dx * (e00 - em0);
-  double fxm = __ldg(bxQs + im) - h / P.dy * (em0 - emm);
-  double fym = __ldg(byQs + jm) + h / P.dx * (e0m - emm);
+  double fxm = (xb ? L.bxQs[j] : __ldg(bxQs + cid(P, i - 1, j))) - h / P.dy * (em0 - emm);
+  double fym = (yb ? L.byQs[i] : __ldg(byQs + cid(P, i, j - 1))) + h / P.dx * (e0m - emm);
   bx[n] = fx;
   by[n] = fy;
+  if (xb) L.bx[j] = fxm;
+  if (yb) L.by[i] = fym;
   ucon[5 * N + n] = 0.5 * (fxm + fx);
   ucon[6 * N + n] = 0.5 * (fym + fy);
+}
+// Stage combination (main.cpp:397-407) and stage derivative (main.cpp:550-551) of the
+// boundary-face lines of the transmissive directions; thread q handles row q of the x_0
+// line and column q of the y_0 line.
+__global__ void k_bline_combine(DevParams P, Tableau T, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = sc->dt;
+  if (P.xclamp && q < P.ny) {
+    double fe = L.bx_n[q], fs = fe;
+    for (int r = 0; r < rks; ++r) {
+      const double h0 = L.hsbx[(long long)r * P.ny + q];
+      fe += T.ae[r] * dt * h0;
+      fs += T.ai[r] * dt * h0;
+    }
+    L.bxQe[q] = fe;
+    L.bxQs[q] = fs;
+  }
+  if (P.yclamp && q < P.nx) {
+    double fe = L.by_n[q], fs = fe;
+    for (int r = 0; r < rks; ++r) {
+      const double h1 = L.hsby[(long long)r * P.nx + q];
+      fe += T.ae[r] * dt * h1;
+      fs += T.ai[r] * dt * h1;
+    }
+    L.byQe[q] = fe;
+    L.byQs[q] = fs;
+  }
+}
+__global__ void k_bline_derivative(DevParams P, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const double adt = sc->adt;
+  if (P.xclamp && q < P.ny) L.hsbx[(long long)rks * P.ny + q] = (L.bx[q] - L.bxQs[q]) / adt;
+  if (P.yclamp && q < P.nx) L.hsby[(long long)rks * P.nx + q] = (L.by[q] - L.byQs[q]) / adt;
 }
 // Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:523-529)
 __global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
@@ -556,13 +625,15 @@ __global__ void k_shock_max(DevParams P, const double* __restrict__ chit, double
 // face FV div (StaggerCT), wrapped central div of cell B, reference cell metric
 // (imex_subsystems.cpp:646-654), max |central div|
 __global__ void k_divergence(DevParams P, const double* __restrict__ ucon, const double* __restrict__ bx,
-                             const double* __restrict__ by, double* __restrict__ partial) {
+                             const double* __restrict__ by, BoundaryLines L, double* __restrict__ partial) {
   const long long N = P.N;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   double m = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-    double d = (bx[n] - bx[cid(P, i - 1, j)]) / P.dx + (by[n] - by[cid(P, i, j - 1)]) / P.dy;
+    const double bxm = (P.xclamp && i == 0) ? L.bx[j] : bx[cid(P, i - 1, j)];
+    const double bym = (P.yclamp && j == 0) ? L.by[i] : by[cid(P, i, j - 1)];
+    double d = (bx[n] - bxm) / P.dx + (by[n] - bym) / P.dy;
     v[0] += P.dx * P.dy * d * d;
     const double* B5 = ucon + 5 * N;
     const double* B6 = ucon + 6 * N;
@@ -645,6 +716,10 @@ imex_status launch_step_prologue(imex_ctx* ctx) {
   cudaError_t e = cudaMemcpyAsync(ctx->bx_n, ctx->bx, plane, cudaMemcpyDeviceToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by_n, ctx->by, plane, cudaMemcpyDeviceToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A_snap, ctx->A, 3 * plane, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess && P.xclamp)
+    e = cudaMemcpyAsync(ctx->bl.bx_n, ctx->bl.bx, P.ny * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess && P.yclamp)
+    e = cudaMemcpyAsync(ctx->bl.by_n, ctx->bl.by, P.nx * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
   prof_end(ctx, F_CONS_FROM_PRIM, BYTES(24 + 10), 1);
   return cuda_check(ctx, e, "step snapshot copies");
 }
@@ -712,6 +787,11 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
       ctx->P, T, rks, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
       ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe);
   LAUNCH_CHECK(ctx, "k_stage_combine");
+  if (ctx->P.xclamp || ctx->P.yclamp) {
+    k_bline_combine<<<blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream>>>(ctx->P, T, rks,
+                                                                                                   ctx->sc, ctx->bl);
+    LAUNCH_CHECK(ctx, "k_bline_combine");
+  }
   prof_end(ctx, F_COMBINE, BYTES(44 + 13 * rks), 1);
   return IMEX_OK;
 }
@@ -754,7 +834,7 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
   cudaStream_t s = ctx->stream;
   prof_begin(ctx);
   if (variant == 0 || variant == 1) {
-    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp);
+    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
     if (P.reconstate == IMEX_PrimState) k_reconstruct_prim<<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
@@ -762,11 +842,12 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
     k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
-    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->chit, 1.0, ctx->Et, 1.0, ctx->cons, ctx->Epp);
+    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->chit, 1.0, ctx->Et, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   }
   if (variant == 0 || variant == 2) {
-    k_ct_faces<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->bxQs, ctx->byQs, ctx->bx, ctx->by, ctx->cons);
+    k_ct_faces<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->bxQs, ctx->byQs, ctx->bx, ctx->by, ctx->cons,
+                                       ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_faces");
   } else {
     if (variant == 1) k_ct_unstag_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A);
@@ -786,6 +867,11 @@ imex_status launch_stage_derivative(imex_ctx* ctx, int rks) {
       ctx->P, rks, ctx->sc, ctx->cons, ctx->Qs, ctx->A, ctx->A_s, ctx->bx, ctx->bxQs, ctx->by, ctx->byQs, ctx->Bsave,
       ctx->Hs, ctx->HsA, ctx->HsB, ctx->prim);
   LAUNCH_CHECK(ctx, "k_stage_derivative");
+  if (ctx->P.xclamp || ctx->P.yclamp) {
+    k_bline_derivative<<<blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream>>>(
+        ctx->P, rks, ctx->sc, ctx->bl);
+    LAUNCH_CHECK(ctx, "k_bline_derivative");
+  }
   prof_end(ctx, F_DERIVATIVE, BYTES(47), 1);
   return IMEX_OK;
 }
@@ -806,7 +892,7 @@ imex_status launch_divergence(imex_ctx* ctx, double* out4) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
   if (nb > ctx->max_blocks) nb = ctx->max_blocks;
-  k_divergence<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->cons, ctx->bx, ctx->by, ctx->partial);
+  k_divergence<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->cons, ctx->bx, ctx->by, ctx->bl, ctx->partial);
   LAUNCH_CHECK(ctx, "k_divergence");
   std::vector<double> h((size_t)nb * 4);
   cudaError_t e = cudaMemcpyAsync(h.data(), ctx->partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);

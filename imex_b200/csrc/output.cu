@@ -300,9 +300,17 @@ imex_status imex_save_state_file(imex_ctx* ctx, const char* path) {
   cudaError_t e = cudaMemcpyAsync(ctx->h_sc, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "state scalars");
+  // a transmissive run appends its boundary normal faces (ny values of Bx on x_0, nx of By
+  // on y_0) and marks the file version 2
+  const bool lines = ctx->P.xclamp || ctx->P.yclamp;
+  if (lines) {
+    buf.resize(buf.size() + ctx->ny + ctx->nx);
+    s = imex_get_boundary_faces(ctx, buf.data() + 13 * N, buf.data() + 13 * N + ctx->ny);
+    if (s != IMEX_OK) return s;
+  }
   StateHeader h{};
   memcpy(h.magic, kMagic, 8);
-  h.version = 1;
+  h.version = lines ? 2 : 1;
   h.nx = ctx->nx;
   h.ny = ctx->ny;
   h.timestep = ctx->h_sc->timestep;
@@ -328,14 +336,18 @@ imex_status imex_load_state_file(imex_ctx* ctx, const char* path) {
   const size_t N = ctx->N;
   std::vector<double> buf((8 + 1 + 1 + 3) * N);
   bool ok = fread(&h, sizeof(h), 1, f) == 1;
-  if (ok && (memcmp(h.magic, kMagic, 8) != 0 || h.version != 1 || h.nx != ctx->nx || h.ny != ctx->ny)) {
+  if (ok && (memcmp(h.magic, kMagic, 8) != 0 || (h.version != 1 && h.version != 2) || h.nx != ctx->nx ||
+             h.ny != ctx->ny)) {
     fclose(f);
     return set_error(ctx, IMEX_ERR_INVALID, std::string("'") + path + "' is not a state file of this grid");
   }
+  if (h.version == 2) buf.resize(buf.size() + ctx->ny + ctx->nx);
   ok = ok && fread(buf.data(), sizeof(double), buf.size(), f) == buf.size();
   fclose(f);
   if (!ok) return set_error(ctx, IMEX_ERR_INVALID, std::string("short state file '") + path + "'");
   imex_status s = imex_upload_prim(ctx, buf.data(), buf.data() + 8 * N, buf.data() + 9 * N, buf.data() + 10 * N);
+  if (s == IMEX_OK && h.version == 2)
+    s = imex_set_boundary_faces(ctx, buf.data() + 13 * N, buf.data() + 13 * N + ctx->ny);
   if (s != IMEX_OK) return s;
   cudaError_t e = cudaMemcpyAsync(ctx->h_sc, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

@@ -332,19 +332,22 @@ _STATE_HEADER = np.dtype([("magic", "S8"), ("version", "<i4"), ("nx", "<i4"), ("
 
 
 def write_state_file(prob: Problem, path: str, t: float = 0.0, timestep: int = 0, prev_dt: float = 0.0) -> None:
-    """The initial state of a problem as a state file (the input of the imex_run driver)."""
+    """The initial state of a problem as a state file (the input of the imex_run driver).  A
+    problem with boundary normal faces (transmissive) writes version 2, which appends them."""
+    lines = prob.bx_x0 is not None
     h = np.zeros((), dtype=_STATE_HEADER)
-    h["magic"], h["version"], h["nx"], h["ny"], h["timestep"] = STATE_MAGIC, 1, prob.nx, prob.ny, timestep
+    h["magic"], h["version"], h["nx"], h["ny"], h["timestep"] = STATE_MAGIC, 2 if lines else 1, prob.nx, prob.ny, timestep
     h["t"], h["prev_dt"], h["dt"] = t, prev_dt, 0.0
     h["x0"], h["x1"], h["y0"], h["y1"] = prob.x0, prob.x1, prob.y0, prob.y1
     with open(path, "wb") as f:
         f.write(h.tobytes())
-        for a in (prob.prim, prob.bx, prob.by, prob.A):
+        for a in (prob.prim, prob.bx, prob.by, prob.A) + ((prob.bx_x0, prob.by_y0) if lines else ()):
             f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
 
 
 def read_state_file(path: str) -> tuple[dict, np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
-    """(header, prim, bx, by, A) of a state file."""
+    """(header, prim, bx, by, A) of a state file; a version-2 file's boundary normal faces are
+    in header["bx_x0"] / header["by_y0"]."""
     with open(path, "rb") as f:
         raw = f.read()
     h = np.frombuffer(raw[:_STATE_HEADER.itemsize], dtype=_STATE_HEADER)[0]
@@ -353,10 +356,13 @@ def read_state_file(path: str) -> tuple[dict, np.ndarray, np.ndarray, np.ndarray
     nx, ny = int(h["nx"]), int(h["ny"])
     d = np.frombuffer(raw[_STATE_HEADER.itemsize:], dtype="<f8")
     N = nx * ny
-    if d.size != 13 * N:
-        raise ValueError(f"{path}: expected {13 * N} values, found {d.size}")
+    extra = nx + ny if int(h["version"]) == 2 else 0
+    if d.size != 13 * N + extra:
+        raise ValueError(f"{path}: expected {13 * N + extra} values, found {d.size}")
     prim = d[:8 * N].reshape(8, ny, nx)
     bx, by = d[8 * N:9 * N].reshape(ny, nx), d[9 * N:10 * N].reshape(ny, nx)
-    A = d[10 * N:].reshape(3, ny, nx)
+    A = d[10 * N:13 * N].reshape(3, ny, nx)
     header = {n: (h[n].item() if n != "magic" else bytes(h[n])) for n in _STATE_HEADER.names}
+    if extra:
+        header["bx_x0"], header["by_y0"] = d[13 * N:13 * N + ny].copy(), d[13 * N + ny:].copy()
     return header, prim.copy(), bx.copy(), by.copy(), A.copy()

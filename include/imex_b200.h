@@ -100,7 +100,8 @@ typedef struct imex_config {
   double CFL;          /* (config.hpp:57) */
   int recon;           /* imex_reconstruction      (config.hpp:60) */
   int reconstate;      /* imex_recon_state         (config.hpp:61) */
-  int x_bc, y_bc;      /* boundary conditions; only periodic is implemented */
+  int x_bc, y_bc;      /* imex_x_bc / imex_y_bc (config.hpp:63-64): Periodic, or Transmissive with
+                          StaggerCT or NoDivFree; the other kinds return IMEX_ERR_UNSUPPORTED */
   int PressureSolver;  /* imex_solve_pressure      (config.hpp:65) */
   int Energy_Modify;   /* (config.hpp:69) */
   double GMREStol;     /* (config.hpp:71) */
@@ -169,6 +170,17 @@ imex_status imex_upload_state(imex_ctx* ctx, const double* prim8, const double* 
                               const double* A3);
 /* Current state; any pointer may be NULL. */
 imex_status imex_download_state(imex_ctx* ctx, double* cons8, double* prim8, double* bx, double* by, double* A3);
+/* Boundary normal faces of a transmissive direction: Bx on x = x_0 (ny values, one per row)
+ * and By on y = y_0 (nx values, one per column).  The reference carries them as the faces
+ * at ghost index ghost_cells - 1 of Bx_p0 / By_0p, which bound_cond_staggered preserves and
+ * Staggered_CT_Consistent evolves (constrained_transport.cpp:5-30, ct_flux.cpp:176-189);
+ * the bx / by planes above hold the faces at i + 1/2 and j + 1/2 of the interior cells only.
+ * imex_upload_prim sets them to the first interior face of their row / column (Bx(1/2, j),
+ * By(i, 1/2)); set them after it to the initial condition's own values.  A NULL pointer or a
+ * periodic direction leaves that line alone.  Reading a periodic direction returns the
+ * faces it identifies with x_0 / y_0, those at x_1 / y_1.  Host or device pointers. */
+imex_status imex_set_boundary_faces(imex_ctx* ctx, const double* bx_x0, const double* by_y0);
+imex_status imex_get_boundary_faces(imex_ctx* ctx, double* bx_x0, double* by_y0);
 
 /* Time stepping ------------------------------------------------------------ */
 /* One full time step of main.cpp:335-561: global wave-speed maxima, dt, every stage. */
@@ -219,7 +231,11 @@ typedef enum imex_buffer {
   IMEX_BUF_HS = 14,   /* Hs[index], 8 planes */
   IMEX_BUF_HSA = 15,  /* HsA[index], 3 planes */
   IMEX_BUF_HSB = 16,  /* HsB[index], 2 planes */
-  IMEX_BUF_SHOCK = 17 /* shock detector eta of the last pressure solve, 1 plane */
+  IMEX_BUF_SHOCK = 17, /* shock detector eta of the last pressure solve, 1 plane */
+  IMEX_BUF_BX_X0 = 18,    /* transmissive x: Bx_p0 on x = x_0, ny values */
+  IMEX_BUF_BY_Y0 = 19,    /* transmissive y: By_0p on y = y_0, nx values */
+  IMEX_BUF_BX_QS_X0 = 20, /* the same lines of Bx_p0_Qs / By_0p_Qs */
+  IMEX_BUF_BY_QS_Y0 = 21
 } imex_buffer;
 imex_status imex_buffer_count(const imex_ctx* ctx, int buffer, size_t* ndoubles);
 imex_status imex_set_buffer(imex_ctx* ctx, int buffer, int index, const double* src);
@@ -309,8 +325,8 @@ imex_status imex_write_vtk(imex_ctx* ctx, const char* path, int cycle);
 /* The final-state field files RK_rho/vx/vy/E/p/Bx/By/Bz/v_mag.dat (and RK_T.dat for the
  * Redlich-Kwong EOS) into `dir`: "x y value" per cell, x outer, full precision. */
 imex_status imex_write_fields_dat(imex_ctx* ctx, const char* dir);
-/* Binary state (primitive planes, faces, A, t, step counter, previous dt): a run loaded from
- * it continues bit for bit. */
+/* Binary state (primitive planes, faces, A, t, step counter, previous dt; a transmissive run
+ * also its boundary normal faces, file version 2): a run loaded from it continues bit for bit. */
 imex_status imex_save_state_file(imex_ctx* ctx, const char* path);
 imex_status imex_load_state_file(imex_ctx* ctx, const char* path);
 /* The writers on host arrays (no GPU needed); "timestep value" lines for the histories. */

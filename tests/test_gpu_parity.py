@@ -24,7 +24,11 @@ pytestmark = pytest.mark.gpu
 def test_gpu_steps_match_reference_golden(case):
     g = load_golden(f"step_{case}.npz")
     prob, rks, settings = golden_problem(g)
-    tol = 1e-11 if settings.get("eos_type") == "REDLICH_KWONG" else 1e-12
+    # The Redlich-Kwong EOS inverts T(rho, p) by Newton with log and 1/(v - b): CUDA's log and the
+    # host's differ in the last ulp, which that inversion amplifies where v approaches b (the
+    # open-blast case reaches 3.9e-11 after one step), so those cases are held to the per-step
+    # bound of 1e-10; ideal-gas steps differ only by the solves' reduction order (1e-12).
+    tol = 1e-10 if settings.get("eos_type") == "REDLICH_KWONG" else 1e-12
     gpu = ix.Solver.for_problem(prob, rks, settings)
     for s in range(len(g["dt"])):
         dt = gpu.step()
@@ -35,6 +39,9 @@ def test_gpu_steps_match_reference_golden(case):
         bx, by = gpu.faces()
         assert rel(bx, g["bx"][s]) <= tol and rel(by, g["by"][s]) <= tol
         assert rel(gpu.vector_potential(), g["A"][s]) <= tol
+        if "bx_x0" in g.files:  # transmissive cases: the boundary normal faces
+            bxb, byb = gpu.boundary_faces()
+            assert rel(bxb, g["bx_x0"][s]) <= tol and rel(byb, g["by_y0"][s]) <= tol
     gpu.close()
 
 
