@@ -11,7 +11,7 @@ larger than the 126 MB L2, so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl imex|reference]
                     [--workload vortex_sheet_1024|vortex_sheet_2048|vortex_64|random_field_2048|
-                                vortex_ensemble_256] [--precision fp64|mixed]
+                                open_blast_1024|vortex_ensemble_256] [--precision fp64|mixed]
 
 vortex_ensemble_256 is the batched form: 256 independent vortex runs (seeded kappa, mu and
 grid sides 64..512) advanced together through imex_batch (batched solves, CUDA graph,
@@ -62,13 +62,19 @@ WORKLOADS = {
                               desc="seeded low-Mach random field 2048^2 (seed 2026, beta 0.1), Redlich-Kwong, "
                                    "Minmod, EMF-consistent staggered CT, floor on, RK2"),
 }
+CFG3 = dict(recon="WENO5", magfield="StaggerCT", floor_on=1, p_floor=1e-8, theta=0.5, GMREStol=1e-14, CFL=0.8)
+WORKLOADS["open_blast_1024"] = dict(problem="open_blast", n=1024, rks=3, settings=CFG3,
+                                    desc="smooth blast in an oblique field on the open unit square 1024^2 "
+                                         "(transmissive x and y), WENO5, EMF-consistent staggered CT, floor on, RK3")
 REF_SAMPLE_N = 256
 
 
 def make_problem(kind: str, n: int):
-    from imex_b200.problems import random_field, vortex, vortex_sheet
+    from imex_b200.problems import open_blast, random_field, vortex, vortex_sheet
     if kind == "random_field":
         return random_field(n)
+    if kind == "open_blast":
+        return open_blast(n)
     return vortex(n) if kind == "vortex" else vortex_sheet(n)
 
 
@@ -173,11 +179,11 @@ def barrier(world: int) -> None:
         dist.barrier()
 
 
-def cpu_reference_rate(steps: int, max_seconds: float) -> dict:
+def cpu_reference_rate(steps: int, max_seconds: float, workload: str = "vortex_sheet_1024") -> dict:
     """Reference CPU solver on the sample: cell-stage updates per second over `steps` steps."""
     from oracle.bindings import RefSolver, make_solver, PortSolver
     kind = "reference" if RefSolver.available() else "port"
-    wl = WORKLOADS["vortex_sheet_1024"]
+    wl = WORKLOADS[workload]
     prob = make_problem(wl["problem"], REF_SAMPLE_N)
     solver = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
     done, t_total = 0, 0.0
@@ -538,7 +544,7 @@ def main() -> int:
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(steps=3, max_seconds=12.0)
+                cpu = cpu_reference_rate(steps=3, max_seconds=12.0, workload=args.workload)
                 cpu.pop("seconds", None)
             except Exception as exc:
                 cpu = {"value": None, "error": str(exc)}
