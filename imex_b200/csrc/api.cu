@@ -82,9 +82,6 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if ((c->x_bc != IMEX_x_Periodic && c->x_bc != IMEX_x_Transmissive) ||
       (c->y_bc != IMEX_y_Periodic && c->y_bc != IMEX_y_Transmissive))
     return why = "only periodic and transmissive boundaries are implemented", IMEX_ERR_UNSUPPORTED;
-  if ((c->x_bc == IMEX_x_Transmissive || c->y_bc == IMEX_y_Transmissive) && c->magfield != IMEX_StaggerCT &&
-      c->magfield != IMEX_NoDivFree)
-    return why = "transmissive boundaries are implemented for StaggerCT and NoDivFree", IMEX_ERR_UNSUPPORTED;
   if (c->formula != IMEX_PressureFormula && c->formula != IMEX_EnergyFormula) return why = "bad formula", IMEX_ERR_INVALID;
   if (!c->GLF) return why = "only the global Lax-Friedrichs dissipation (GLF) is implemented", IMEX_ERR_UNSUPPORTED;
   if (c->U_update != IMEX_DefinitionofU) return why = "only DefinitionofU is implemented", IMEX_ERR_UNSUPPORTED;
@@ -403,6 +400,12 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   P.fixed_dt = cfg->fixed_dt;
   P.xclamp = cfg->x_bc == IMEX_x_Transmissive;
   P.yclamp = cfg->y_bc == IMEX_y_Transmissive;
+  P.xm = P.xclamp ? 0 : 1;
+  P.xlo = P.xclamp ? 0 : nx;
+  P.xhi = P.xclamp ? nx - 1 : -nx;
+  P.ym = P.yclamp ? 0 : 1;
+  P.ylo = P.yclamp ? 0 : ny;
+  P.yhi = P.yclamp ? ny - 1 : -ny;
 
   const size_t N = ctx->N;
   const size_t R = (size_t)cfg->RKs;

@@ -21,15 +21,59 @@ __device__ __forceinline__ int wrap(int i, int n) {
   i %= n;
   return i < 0 ? i + n : i;
 }
-// neighbour index with |offset| < n
-__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
-__device__ __forceinline__ int clamp1(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
 // the cell a neighbour index (|offset| < n) reads: the periodic image, or the nearest
 // interior cell of a transmissive direction
-__device__ __forceinline__ int cix(const DevParams& P, int i) { return P.xclamp ? clamp1(i, P.nx) : wrap1(i, P.nx); }
-__device__ __forceinline__ int cjy(const DevParams& P, int j) { return P.yclamp ? clamp1(j, P.ny) : wrap1(j, P.ny); }
+__device__ __forceinline__ int cix(const DevParams& P, int i) {
+  return i < 0 ? i * P.xm + P.xlo : (i >= P.nx ? i * P.xm + P.xhi : i);
+}
+__device__ __forceinline__ int cjy(const DevParams& P, int j) {
+  return j < 0 ? j * P.ym + P.ylo : (j >= P.ny ? j * P.ym + P.yhi : j);
+}
 __device__ __forceinline__ long long cid(const DevParams& P, int i, int j) {
   return (long long)cix(P, i) + (long long)P.nx * cjy(P, j);
+}
+// The parameters a kernel instantiated for periodic (kOpen = false) or transmissive
+// (kOpen = true) neighbour maps works with: the periodic instance has the wrap as
+// compile-time constants, so its index arithmetic is the plain wrap.
+template <bool kOpen>
+__device__ __forceinline__ DevParams bc_params(const DevParams& P) {
+  DevParams Q = P;
+  if (!kOpen) {
+    Q.xclamp = Q.yclamp = 0;
+    Q.xm = Q.ym = 1;
+    Q.xlo = P.nx;
+    Q.xhi = -P.nx;
+    Q.ylo = P.ny;
+    Q.yhi = -P.ny;
+  }
+  return Q;
+}
+// Plane a of A at (i, j) with the ghosts of bound_cond_A (boundary.cpp:177-292): a
+// transmissive direction extrapolates linearly from its two nearest interior cells, x first
+// and then y on the x-extrapolated rows; a periodic direction wraps.
+__device__ __forceinline__ double a_row(const DevParams& P, const double* __restrict__ a, int i, int j) {
+  const double* r = a + (long long)P.nx * j;
+  if (P.xclamp && i < 0) {
+    const double slope = r[1] - r[0];
+    return r[0] - (double)(-i) * slope;
+  }
+  if (P.xclamp && i >= P.nx) {
+    const double slope = r[P.nx - 1] - r[P.nx - 2];
+    return r[P.nx - 1] + (double)(i - P.nx + 1) * slope;
+  }
+  return r[cix(P, i)];
+}
+__device__ __forceinline__ double a_ghost(const DevParams& P, const double* __restrict__ a, int i, int j) {
+  if (!P.xclamp && !P.yclamp) return a[cid(P, i, j)];
+  if (P.yclamp && j < 0) {
+    const double a0 = a_row(P, a, i, 0), slope = a_row(P, a, i, 1) - a0;
+    return a0 - (double)(-j) * slope;
+  }
+  if (P.yclamp && j >= P.ny) {
+    const double aT = a_row(P, a, i, P.ny - 1), slope = aT - a_row(P, a, i, P.ny - 2);
+    return aT + (double)(j - P.ny + 1) * slope;
+  }
+  return a_row(P, a, i, cjy(P, j));
 }
 
 // ---------------------------------------------------------------- EOS

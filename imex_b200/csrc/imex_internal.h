@@ -28,6 +28,9 @@ struct DevParams {
   // cell (bound_cond_u / bound_cond_array / M_P / M_B, boundary.cpp:7-16,
   // timestep.cpp:168-204, implicit_operators.cpp:12-14); 0 where it is periodic (wrap)
   int xclamp, yclamp;
+  // the index map as one multiply-add per side: i < 0 -> i * xm + xlo, i >= nx -> i * xm + xhi
+  // (periodic: xm = 1, xlo = nx, xhi = -nx; transmissive: xm = 0, xlo = 0, xhi = nx - 1)
+  int xm, xlo, xhi, ym, ylo, yhi;
 };
 
 // Boundary normal faces of the transmissive directions.  The reference keeps Bx_p0 at
@@ -143,6 +146,14 @@ struct imex_ctx {
   long long kernel_launches = 0;  // every kernel this context launched
   double barrier_timeout_s = 2.0;  // bound on any single device-wide wait
 };
+
+// Launch kernel template kern<kOpen> with the instance for this context's boundaries
+// (bc_params): transmissive in x or y, or periodic in both.
+#define IMEX_LAUNCH_BC(P, kern, grid, block, smem, stream, ...)                    \
+  do {                                                                             \
+    if ((P).xclamp || (P).yclamp) kern<true><<<grid, block, smem, stream>>>(__VA_ARGS__); \
+    else kern<false><<<grid, block, smem, stream>>>(__VA_ARGS__);                  \
+  } while (0)
 
 namespace imex {
 

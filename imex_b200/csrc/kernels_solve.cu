@@ -505,7 +505,9 @@ struct MagneticACoef {
     cy = nu_y / (P.dy * P.dy);
   }
 };
-template <class T>
+// kOpen: an instance for runs with a transmissive direction, whose tiles extrapolate A
+// past the domain (extrapolate); the periodic instance carries none of that code.
+template <class T, bool kOpen = false>
 struct MagneticAOpT : MagneticACoef {
   using value_type = T;
   static constexpr int M = 3, HALO = 2;
@@ -514,8 +516,8 @@ struct MagneticAOpT : MagneticACoef {
   static constexpr int PT = 6;    // Txx, Tyx, Tzx, Txy, Tyy, Tzy on the halo-1 region
   static constexpr int MIN_BLOCKS = 2;
   template <class U>
-  __device__ __forceinline__ MagneticAOpT<U> as() const {
-    MagneticAOpT<U> o;
+  __device__ __forceinline__ MagneticAOpT<U, kOpen> as() const {
+    MagneticAOpT<U, kOpen> o;
     static_cast<MagneticACoef&>(o) = *this;
     return o;
   }
@@ -525,10 +527,58 @@ struct MagneticAOpT : MagneticACoef {
     q[2] = (T)__ldg(Qe + 7 * P.N + c);
   }
   __device__ __forceinline__ void precond(long long, T*) const {}
+  // bound_cond_A on the staged vector: the operator reads AG = bound_cond_A(x)
+  // (implicit_operators.cpp:377-384).  In a transmissive direction the staged cells outside
+  // the domain get linear extrapolations of the two nearest interior cells (boundary.cpp:
+  // 181-195, 233-246), x first, then y on the x-extrapolated rows; the fill left the
+  // clamped values there.  Tiles away from such a boundary have nothing to do.
   template <class TB>
-  __device__ __forceinline__ void prepass(TB& tb, int, int) const {
+  __device__ __forceinline__ void extrapolate(TB& tb, int x0, int y0) const {
+    constexpr int SX = TB::SX, SY = TB::SY, SN = TB::SN, H = HALO;
+    if (P.xclamp && (x0 - H < 0 || x0 - H + SX > P.nx)) {
+      const int sa = H - x0, sr = P.nx - 1 - x0 + H;  // staged columns of i = 0 and i = nx - 1
+      for (int q = threadIdx.x; q < SN; q += NT) {
+        const int sx = q % SX, gi = x0 - H + sx;
+        if (gi >= 0 && gi < P.nx) continue;
+        T* r = tb.s + (q - sx);
+#pragma unroll
+        for (int m = 0; m < M; ++m, r += SN) {
+          if (gi < 0) {
+            const T slope = r[sa + 1] - r[sa];
+            r[sx] = r[sa] - (T)(-gi) * slope;
+          } else {
+            const T slope = r[sr] - r[sr - 1];
+            r[sx] = r[sr] + (T)(gi - P.nx + 1) * slope;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (P.yclamp && (y0 - H < 0 || y0 - H + SY > P.ny)) {
+      const int ra = H - y0, rt = P.ny - 1 - y0 + H;  // staged rows of j = 0 and j = ny - 1
+      for (int q = threadIdx.x; q < SN; q += NT) {
+        const int sx = q % SX, sy = q / SX, gj = y0 - H + sy;
+        if (gj >= 0 && gj < P.ny) continue;
+        T* c = tb.s + sx;
+#pragma unroll
+        for (int m = 0; m < M; ++m, c += SN) {
+          if (gj < 0) {
+            const T slope = c[(ra + 1) * SX] - c[ra * SX];
+            c[sy * SX] = c[ra * SX] - (T)(-gj) * slope;
+          } else {
+            const T slope = c[rt * SX] - c[(rt - 1) * SX];
+            c[sy * SX] = c[rt * SX] + (T)(gj - P.ny + 1) * slope;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB& tb, int x0, int y0) const {
     constexpr int SX = TB::SX, SN = TB::SN;
     const T dx = (T)P.dx, dy = (T)P.dy, two = T(2);
+    if constexpr (kOpen) extrapolate(tb, x0, y0);
     for (int q = threadIdx.x; q < TB::PN; q += NT) {
       const int px = q % TB::PX, py = q / TB::PX;
       const int o = (py + 1) * SX + (px + 1);  // same cell in the halo-2 tile
@@ -579,6 +629,7 @@ struct MagneticAOpT : MagneticACoef {
   }
 };
 using MagneticAOp = MagneticAOpT<double>;
+using MagneticAOpOpen = MagneticAOpT<double, true>;
 
 template <class Op>
 __device__ __forceinline__ bool op_uses_vdiag(const Op&) { return false; }
@@ -633,9 +684,9 @@ __device__ __forceinline__ void fill_tile(const Op& op, TileBuf<Op>& tb, const T
     int q = threadIdx.x + r * NT;
     if (q >= TB::SN) q = TB::SN - 1;  // an already staged cell: loaded again, never stored
     const int sxq = q % TB::SX, syq = q / TB::SX;
-    const int xi = x0 + sxq - Op::HALO, yj = y0 + syq - Op::HALO;
-    const int gi = T.xclamp ? (xi < 0 ? 0 : (xi >= T.nx ? T.nx - 1 : xi)) : wrapc(xi, T.nx);
-    const int gj = T.yclamp ? (yj < 0 ? 0 : (yj >= T.ny ? T.ny - 1 : yj)) : wrapc(yj, T.ny);
+    int gi = x0 + sxq - Op::HALO, gj = y0 + syq - Op::HALO;
+    if (gi < 0 || gi >= T.nx) gi = T.xclamp ? (gi < 0 ? 0 : T.nx - 1) : wrapc(gi, T.nx);
+    if (gj < 0 || gj >= T.ny) gj = T.yclamp ? (gj < 0 ? 0 : T.ny - 1) : wrapc(gj, T.ny);
     c[r] = (long long)gi + (long long)T.nx * gj;
   }
   VT qv[Q][QC];
@@ -1514,9 +1565,11 @@ constexpr int kThreads = 256;
 inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
 
 // enthalpy ratio h(Qe) rho_e / rho, V slope at p(Qe), rho v* snapshot (imex_subsystems.cpp:92-147)
-__global__ void k_pressure_coeffs(DevParams P, const double* __restrict__ Qe, const double* __restrict__ ucon,
+template <bool kOpen>
+__global__ void k_pressure_coeffs(DevParams Pin, const double* __restrict__ Qe, const double* __restrict__ ucon,
                                   const double* __restrict__ hQe, const double* __restrict__ pe,
                                   double* __restrict__ hh, double* __restrict__ vscale, double* __restrict__ rv) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -1528,8 +1581,10 @@ __global__ void k_pressure_coeffs(DevParams P, const double* __restrict__ Qe, co
   rv[2 * N + n] = ucon[3 * N + n];
 }
 // Jacobi diagonal Tdiag (implicit_operators.cpp:631-649)
-__global__ void k_pressure_tdiag(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ hh,
+template <bool kOpen>
+__global__ void k_pressure_tdiag(DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ hh,
                                  double* __restrict__ tdiag) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= P.N) return;
@@ -1541,10 +1596,12 @@ __global__ void k_pressure_tdiag(DevParams P, const DevScalars* __restrict__ sc,
 }
 // pressure RHS b (imex_subsystems.cpp:123-169 first, 226-269 second); kin = momentum used in
 // the kinetic term, rv = rho v* used in the enthalpy-flux divergence; p0 = initial guess.
-__global__ void k_pressure_rhs(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+template <bool kOpen>
+__global__ void k_pressure_rhs(DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                const double* __restrict__ hh, const double* __restrict__ rv,
                                const double* __restrict__ kin, double* __restrict__ b,
                                const double* __restrict__ p0src, double* __restrict__ p0) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1745,12 +1802,14 @@ __global__ void k_gmax_finalize(const double* __restrict__ partial, int nblk, De
   }
 }
 // B = curl A after the A solve (imex_subsystems.cpp:65-72)
-__global__ void k_curl_A(DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
+template <bool kOpen>
+__global__ void k_curl_A(DevParams Pin, const double* __restrict__ A, double* __restrict__ ucon) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  auto Ak = [&](int k, int di, int dj) { return A[k * N + cid(P, i + di, j + dj)]; };
+  auto Ak = [&](int k, int di, int dj) { return a_ghost(P, A + k * N, i + di, j + dj); };
   ucon[5 * N + n] = 1 / (2.0 * P.dy) * (Ak(2, 0, 1) - Ak(2, 0, -1));
   ucon[6 * N + n] = -1 / (2.0 * P.dx) * (Ak(2, 1, 0) - Ak(2, -1, 0));
   ucon[7 * N + n] = 1 / (2.0 * P.dx) * (Ak(1, 1, 0) - Ak(1, -1, 0)) - 1 / (2.0 * P.dy) * (Ak(0, 0, 1) - Ak(0, 0, -1));
@@ -1933,8 +1992,9 @@ MagneticBOp make_magB_op(imex_ctx* ctx) {
   op.rho = ctx->cons;
   return op;
 }
-MagneticAOp make_magA_op(imex_ctx* ctx) {
-  MagneticAOp op{};
+template <bool kOpen = false>
+MagneticAOpT<double, kOpen> make_magA_op(imex_ctx* ctx) {
+  MagneticAOpT<double, kOpen> op{};
   op.P = ctx->P;
   op.sc = ctx->sc;
   op.Qe = ctx->Qe;
@@ -1978,10 +2038,10 @@ imex_status pressure_setup(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
-  k_pressure_coeffs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->Qe, ctx->cons, ctx->hQe, ctx->pe, ctx->hh, ctx->vscale,
-                                                     ctx->rv);
+  IMEX_LAUNCH_BC(P, k_pressure_coeffs, nb, kThreads, 0, ctx->stream, P, ctx->Qe, ctx->cons, ctx->hQe, ctx->pe, ctx->hh,
+                 ctx->vscale, ctx->rv);
   LAUNCH_CHECK(ctx, "k_pressure_coeffs");
-  k_pressure_tdiag<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->hh, ctx->tdiag);
+  IMEX_LAUNCH_BC(P, k_pressure_tdiag, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->hh, ctx->tdiag);
   LAUNCH_CHECK(ctx, "k_pressure_tdiag");
   prof_end(ctx, F_PRES_SETUP, BYTES(12 + 2), 2);
   return launch_shock(ctx, ctx->Qe, ctx->eta);
@@ -2020,6 +2080,8 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
   } else if (op == IMEX_OP_MAGNETIC_B) {
     return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC);
   } else if (op == IMEX_OP_MAGNETIC_A) {
+    if (ctx->P.xclamp || ctx->P.yclamp)
+      return gmres_run(ctx, make_magA_op<true>(ctx), F_GMRES_MAG_A, x, b, IMEX_MIXED_MAGNETIC);
     return gmres_run(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, IMEX_MIXED_MAGNETIC);
   } else if (op == IMEX_OP_ENERGY) {
     return gmres_run(ctx, make_energy_op(ctx), F_GMRES_ENERGY, x, b, IMEX_MIXED_PRESSURE);
@@ -2292,7 +2354,7 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
       mag_system(m, &op, x, b);
     };
     if (P.magfield == IMEX_PotentialA)
-      s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op, sys);
+      s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<false>, sys);
     else
       s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_B, make_magB_op, sys);
   } else if (P.formula == IMEX_EnergyFormula) {  // the energy solve, in place on E
@@ -2391,7 +2453,7 @@ imex_status mag_out(imex_ctx* ctx) {
   int nb = blocks_for(P.N);
   prof_begin(ctx);
   if (P.magfield == IMEX_PotentialA) {
-    k_curl_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->A, ctx->cons);
+    IMEX_LAUNCH_BC(P, k_curl_A, nb, kThreads, 0, ctx->stream, P, ctx->A, ctx->cons);
     LAUNCH_CHECK(ctx, "k_curl_A");
     prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
   } else {
@@ -2423,8 +2485,8 @@ imex_status pres_part1(imex_ctx* ctx) {
   if ((s = pressure_setup(ctx)) != IMEX_OK) return s;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
-  k_pressure_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->rv, ctx->pb, ctx->pe,
-                                                  ctx->pp);
+  IMEX_LAUNCH_BC(P, k_pressure_rhs, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->rv,
+                 ctx->pb, ctx->pe, ctx->pp);
   LAUNCH_CHECK(ctx, "k_pressure_rhs");
   prof_end(ctx, F_PRES_RHS, BYTES(14), 1);
   return IMEX_OK;
@@ -2444,8 +2506,8 @@ imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
   *second = P.PressureSolver == IMEX_all_correction || (P.PressureSolver == IMEX_once_correction && rks == P.RKs - 1);
   if (*second) {
     prof_begin(ctx);
-    k_pressure_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->cons + P.N, ctx->pb,
-                                                    nullptr, nullptr);
+    IMEX_LAUNCH_BC(P, k_pressure_rhs, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->hh, ctx->rv,
+                   ctx->cons + P.N, ctx->pb, nullptr, nullptr);
     LAUNCH_CHECK(ctx, "k_pressure_rhs(2)");
     prof_end(ctx, F_PRES_RHS, BYTES(15), 1);
   }
@@ -2520,7 +2582,8 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
   } else if (op == IMEX_OP_MAGNETIC_B) {
     launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_A) {
-    launch_apply(ctx, make_magA_op(ctx), nb, T, x, Ax);
+    if (ctx->P.xclamp || ctx->P.yclamp) launch_apply(ctx, make_magA_op<true>(ctx), nb, T, x, Ax);
+    else launch_apply(ctx, make_magA_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_ENERGY) {
     launch_apply(ctx, make_energy_op(ctx), nb, T, x, Ax);
   } else {
@@ -2541,6 +2604,8 @@ imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b,
   } else if (op == IMEX_OP_MAGNETIC_B) {
     return gmres_noalloc_op(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, base, capacity);
   } else if (op == IMEX_OP_MAGNETIC_A) {
+    if (ctx->P.xclamp || ctx->P.yclamp)
+      return gmres_noalloc_op(ctx, make_magA_op<true>(ctx), F_GMRES_MAG_A, x, b, base, capacity);
     return gmres_noalloc_op(ctx, make_magA_op(ctx), F_GMRES_MAG_A, x, b, base, capacity);
   } else if (op == IMEX_OP_ENERGY) {
     return gmres_noalloc_op(ctx, make_energy_op(ctx), F_GMRES_ENERGY, x, b, base, capacity);

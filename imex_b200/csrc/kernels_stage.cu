@@ -220,7 +220,9 @@ __global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc,
 // TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes,
 // PrimState (the ConsState form is k_reconstruct_var below).
 // nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
-__global__ void k_reconstruct_prim(DevParams P, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
+template <bool kOpen>
+__global__ void k_reconstruct_prim(DevParams Pin, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -260,8 +262,10 @@ __global__ void k_reconstruct_prim(DevParams P, const double* __restrict__ Q, do
 // ConsState reconstructs every conserved variable on its own (reconstruction.cpp:5-266), so
 // one thread per (cell, variable) pair: variable k = blockIdx.y.  The same recon_1d calls as a
 // per-cell loop over the variables, with a small per-thread working set and 5-8x the threads.
-__global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams P, const double* __restrict__ Q,
+template <bool kOpen>
+__global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, const double* __restrict__ Q,
                                                                double* __restrict__ w) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -349,15 +353,18 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* 
 }
 // The register budgets were measured: the convective form runs fastest as the compiler
 // chooses, the pressure and energy forms at three CTAs per SM.
-__global__ void __launch_bounds__(FNT) k_flux_conv(DevParams P, const DevScalars* __restrict__ sc,
+template <bool kOpen>
+__global__ void __launch_bounds__(FNT) k_flux_conv(DevParams Pin, const DevScalars* __restrict__ sc,
                                                    const double* __restrict__ w, const double* __restrict__ Qs,
                                                    double* __restrict__ ucon) {
+  const DevParams P = bc_params<kOpen>(Pin);
   flux_tile<0>(P, sc, w, Qs, ucon);
 }
-template <int kForm>
-__global__ void __launch_bounds__(FNT, 3) k_flux_mag(DevParams P, const DevScalars* __restrict__ sc,
+template <int kForm, bool kOpen>
+__global__ void __launch_bounds__(FNT, 3) k_flux_mag(DevParams Pin, const DevScalars* __restrict__ sc,
                                                      const double* __restrict__ w, const double* __restrict__ Qs,
                                                      double* __restrict__ ucon) {
+  const DevParams P = bc_params<kOpen>(Pin);
   flux_tile<kForm>(P, sc, w, Qs, ucon);
 }
 
@@ -469,13 +476,13 @@ __global__ void k_bline_derivative(DevParams P, int rks, const DevScalars* __res
 }
 // Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:523-529)
 __global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
-                              const double* __restrict__ A_s, double* __restrict__ A) {
+                              const double* __restrict__ A_s, double* __restrict__ A, BoundaryLines L) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  double Ec = 0.25 * (__ldg(Epp + n) + __ldg(Epp + cid(P, i - 1, j)) + __ldg(Epp + cid(P, i, j - 1)) +
-                      __ldg(Epp + cid(P, i - 1, j - 1)));
+  double Ec = 0.25 * (__ldg(Epp + n) + corner_read(P, Epp, L, i - 1, j) + corner_read(P, Epp, L, i, j - 1) +
+                      corner_read(P, Epp, L, i - 1, j - 1));
   A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
 }
 // Unstaggered_CT upwind A_z advection (constrained_transport.cpp:436-488)
@@ -516,8 +523,8 @@ __global__ void k_curl_Az(DevParams P, const double* __restrict__ A, double* __r
   if (n >= N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
   const double* Az = A + 2 * N;
-  ucon[5 * N + n] = (__ldg(Az + cid(P, i, j + 1)) - __ldg(Az + cid(P, i, j - 1))) / (2.0 * P.dy);
-  ucon[6 * N + n] = -(__ldg(Az + cid(P, i + 1, j)) - __ldg(Az + cid(P, i - 1, j))) / (2.0 * P.dx);
+  ucon[5 * N + n] = (a_ghost(P, Az, i, j + 1) - a_ghost(P, Az, i, j - 1)) / (2.0 * P.dy);
+  ucon[6 * N + n] = -(a_ghost(P, Az, i + 1, j) - a_ghost(P, Az, i - 1, j)) / (2.0 * P.dx);
 }
 // Face EMFs of the legacy Staggered_CT from the reconstruction of u_con
 // (constrained_transport.cpp:73-97): Ez_p0 = -(f6_L + f6_R)/2, Ez_0p = (g5_L + g5_R)/2.
@@ -577,7 +584,9 @@ __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __res
 
 // ---------------------------------------------------------------- shock detector
 // ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41).
-__global__ void k_shock_cf(DevParams P, const double* __restrict__ Q, double* __restrict__ cf) {
+template <bool kOpen>
+__global__ void k_shock_cf(DevParams Pin, const double* __restrict__ Q, double* __restrict__ cf) {
+  const DevParams P = bc_params<kOpen>(Pin);
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= P.N) return;
   double c[8];
@@ -587,8 +596,10 @@ __global__ void k_shock_cf(DevParams P, const double* __restrict__ Q, double* __
   double cA2 = (c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) / c[0];
   cf[n] = sqrt(a2 + cA2);
 }
-__global__ void k_shock_tilde(DevParams P, const double* __restrict__ Q, const double* __restrict__ cf,
+template <bool kOpen>
+__global__ void k_shock_tilde(DevParams Pin, const double* __restrict__ Q, const double* __restrict__ cf,
                               double* __restrict__ chit) {
+  const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -608,7 +619,9 @@ __global__ void k_shock_tilde(DevParams P, const double* __restrict__ Q, const d
   double mx = (0.0 < q) ? q : 0.0;
   chit[n] = (mx < 1.0) ? mx : 1.0;
 }
-__global__ void k_shock_max(DevParams P, const double* __restrict__ chit, double* __restrict__ eta) {
+template <bool kOpen>
+__global__ void k_shock_max(DevParams Pin, const double* __restrict__ chit, double* __restrict__ eta) {
+  const DevParams P = bc_params<kOpen>(Pin);
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= P.N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
@@ -802,9 +815,11 @@ imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
   const int nread = ctx->P.reconstate == IMEX_PrimState ? 8 : nstore;
   prof_begin(ctx);
   if (ctx->P.reconstate == IMEX_PrimState)
-    k_reconstruct_prim<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w, nstore);
+    IMEX_LAUNCH_BC(ctx->P, k_reconstruct_prim, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, ctx->P, ctx->Qe, ctx->w,
+                   nstore);
   else
-    k_reconstruct_var<<<dim3(blocks_for(ctx->P.N), nstore), kThreads, 0, ctx->stream>>>(ctx->P, ctx->Qe, ctx->w);
+    IMEX_LAUNCH_BC(ctx->P, k_reconstruct_var, (dim3(blocks_for(ctx->P.N), nstore)), kThreads, 0, ctx->stream, ctx->P,
+                   ctx->Qe, ctx->w);
   LAUNCH_CHECK(ctx, "k_reconstruct");
   prof_end(ctx, F_RECON, BYTES(nread + 4 * nstore), 1);
   return IMEX_OK;
@@ -814,12 +829,17 @@ imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
 imex_status launch_flux_update(imex_ctx* ctx, int form) {
   const dim3 nb((ctx->nx + FTX - 1) / FTX, (ctx->ny + FTY - 1) / FTY);
   prof_begin(ctx);
-  if (form == 1)
-    k_flux_mag<1><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  const bool open = ctx->P.xclamp || ctx->P.yclamp;
+  if (form == 1 && open)
+    k_flux_mag<1, true><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  else if (form == 1)
+    k_flux_mag<1, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  else if (form == 2 && open)
+    k_flux_mag<2, true><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else if (form == 2)
-    k_flux_mag<2><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    k_flux_mag<2, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else
-    k_flux_conv<<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    IMEX_LAUNCH_BC(ctx->P, k_flux_conv, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   LAUNCH_CHECK(ctx, "flux update");
   prof_end(ctx, form ? F_FLUX_PRES : F_FLUX_CONV, BYTES(form ? 33 : 30), 1);
   return IMEX_OK;
@@ -837,8 +857,8 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
     k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
-    if (P.reconstate == IMEX_PrimState) k_reconstruct_prim<<<nb, kThreads, 0, s>>>(P, ctx->cons, ctx->w, 8);
-    else k_reconstruct_var<<<dim3(nb, 8), kThreads, 0, s>>>(P, ctx->cons, ctx->w);
+    if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
+    else IMEX_LAUNCH_BC(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
     k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
@@ -850,7 +870,7 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
                                        ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_faces");
   } else {
-    if (variant == 1) k_ct_unstag_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A);
+    if (variant == 1) k_ct_unstag_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A, ctx->bl);
     else k_ct_unstag_legacy_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->cons, ctx->A_s, ctx->A);
     LAUNCH_CHECK(ctx, "k_ct_unstag_A");
     k_curl_Az<<<nb, kThreads, 0, s>>>(P, ctx->A, ctx->cons);
@@ -880,9 +900,9 @@ imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
-  k_shock_cf<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et);
-  k_shock_tilde<<<nb, kThreads, 0, ctx->stream>>>(P, Q, ctx->Et, ctx->chit);
-  k_shock_max<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->chit, eta);
+  IMEX_LAUNCH_BC(P, k_shock_cf, nb, kThreads, 0, ctx->stream, P, Q, ctx->Et);
+  IMEX_LAUNCH_BC(P, k_shock_tilde, nb, kThreads, 0, ctx->stream, P, Q, ctx->Et, ctx->chit);
+  IMEX_LAUNCH_BC(P, k_shock_max, nb, kThreads, 0, ctx->stream, P, ctx->chit, eta);
   LAUNCH_CHECK(ctx, "shock detector");
   prof_end(ctx, F_SHOCK, BYTES(16), 3);
   return IMEX_OK;

@@ -100,8 +100,8 @@ typedef struct imex_config {
   double CFL;          /* (config.hpp:57) */
   int recon;           /* imex_reconstruction      (config.hpp:60) */
   int reconstate;      /* imex_recon_state         (config.hpp:61) */
-  int x_bc, y_bc;      /* imex_x_bc / imex_y_bc (config.hpp:63-64): Periodic, or Transmissive with
-                          StaggerCT or NoDivFree; the other kinds return IMEX_ERR_UNSUPPORTED */
+  int x_bc, y_bc;      /* imex_x_bc / imex_y_bc (config.hpp:63-64): Periodic or Transmissive, per
+                          direction; the other kinds return IMEX_ERR_UNSUPPORTED */
   int PressureSolver;  /* imex_solve_pressure      (config.hpp:65) */
   int Energy_Modify;   /* (config.hpp:69) */
   double GMREStol;     /* (config.hpp:71) */

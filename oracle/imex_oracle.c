@@ -87,6 +87,34 @@ static inline double BXF(const double* a, int i, int j) {
 static inline double BYF(const double* a, int i, int j) {
   return (j < 0 && G.yclamp) ? a[G.N + (size_t)CI(i)] : a[ID(i, j)];
 }
+/* a plane of A (or of the A-form operator's vector) with the ghosts of bound_cond_A,
+ * boundary.cpp:177-292: a transmissive direction extrapolates linearly from its two nearest
+ * interior cells, x first and then y on the x-extrapolated rows; a periodic one wraps */
+static double agh_row(const double* a, int i, int j) {
+  const int nx = G.nx;
+  const double* r = a + (size_t)nx * (size_t)j;
+  if (G.xclamp && i < 0) {
+    double slope = r[1] - r[0];
+    return r[0] - (double)(-i) * slope;
+  }
+  if (G.xclamp && i >= nx) {
+    double slope = r[nx - 1] - r[nx - 2];
+    return r[nx - 1] + (double)(i - nx + 1) * slope;
+  }
+  return r[CI(i)];
+}
+static double agh(const double* a, int i, int j) {
+  const int ny = G.ny;
+  if (G.yclamp && j < 0) {
+    double a0 = agh_row(a, i, 0), slope = agh_row(a, i, 1) - a0;
+    return a0 - (double)(-j) * slope;
+  }
+  if (G.yclamp && j >= ny) {
+    double aT = agh_row(a, i, ny - 1), slope = aT - agh_row(a, i, ny - 2);
+    return aT + (double)(j - ny + 1) * slope;
+  }
+  return agh_row(a, i, CJ(j));
+}
 #define PL(a, k) ((a) + (size_t)(k)*G.N)
 #define AT(a, k, i, j) ((a)[(size_t)(k)*G.N + ID(i, j)])
 
@@ -1185,7 +1213,7 @@ static void mag_subsystem_B(double* ucon, const double* Qs, const double* Qe, do
 static void potential_ax(const double* x, double* Ax) {
   const double h = OP.h, dx = G.dx, dy = G.dy;
   const size_t N = G.N;
-#define AG(ii, jj, k) x[(size_t)(k)*N + ID(ii, jj)]
+#define AG(ii, jj, k) agh(x + (size_t)(k)*N, ii, jj)
 #define Q(k, ii, jj) AT(OP.Qe, k, ii, jj)
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
@@ -1282,10 +1310,11 @@ static void mag_subsystem_A(double* ucon, const double* Qs, const double* Qe, do
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
       size_t c = ID(i, j);
-      ucon[5 * N + c] = 1 / (2.0 * dy) * (AT(A, 2, i, j + 1) - AT(A, 2, i, j - 1));
-      ucon[6 * N + c] = -1 / (2.0 * dx) * (AT(A, 2, i + 1, j) - AT(A, 2, i - 1, j));
-      ucon[7 * N + c] = 1 / (2.0 * dx) * (AT(A, 1, i + 1, j) - AT(A, 1, i - 1, j)) -
-                        1 / (2.0 * dy) * (AT(A, 0, i, j + 1) - AT(A, 0, i, j - 1));
+      const double *A0 = A, *A1 = A + N, *A2 = A + 2 * N;
+      ucon[5 * N + c] = 1 / (2.0 * dy) * (agh(A2, i, j + 1) - agh(A2, i, j - 1));
+      ucon[6 * N + c] = -1 / (2.0 * dx) * (agh(A2, i + 1, j) - agh(A2, i - 1, j));
+      ucon[7 * N + c] = 1 / (2.0 * dx) * (agh(A1, i + 1, j) - agh(A1, i - 1, j)) -
+                        1 / (2.0 * dy) * (agh(A0, i, j + 1) - agh(A0, i, j - 1));
     }
   free(pri); free(b); free(x);
 }
@@ -1307,10 +1336,6 @@ static double corner_at(int i, int j, const double* Ep0, const double* E0p, cons
   double t4 = 0.5 * ((E(Et, i, j + 1) - E(E0p, i, j)) / (dy / 2.0) + (E(Et, i + 1, j + 1) - E(E0p, i + 1, j)) / (dy / 2.0));
 #undef E
   return bar + dx / 8.0 * (t1 - t2) + dy / 8.0 * (t3 - t4);
-}
-static void corner_assemble(double* Epp, const double* Ep0, const double* E0p, const double* Et) {
-  for (int j = 0; j < G.ny; j++)
-    for (int i = 0; i < G.nx; i++) Epp[ID(i, j)] = corner_at(i, j, Ep0, E0p, Et);
 }
 static void cell_ez(double* Et, const double* ucon) {
   const size_t N = G.N;
@@ -1361,22 +1386,25 @@ static void staggered_ct_consistent(double* ucon, double* bx, double* by, const 
 static void unstaggered_ct_consistent(double* ucon, double* A, const double* A_s, const double* Fx, const double* Fy,
                                       double h) {
   const size_t N = G.N;
-  double *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc(N);
+  double *Ep0 = alloc(N), *E0p = alloc(N), *Et = alloc(N), *Epp = alloc((size_t)(G.nx + 1) * (G.ny + 1));
   for (size_t c = 0; c < N; ++c) {
     Ep0[c] = -Fx[c];
     E0p[c] = +Fy[c];
   }
   cell_ez(Et, ucon);
-  corner_assemble(Epp, Ep0, E0p, Et);
+  corner_grid(Epp, Ep0, E0p, Et);
+#define EC(i, j) Epp[(size_t)((i) + 1) + (size_t)(G.nx + 1) * (size_t)((j) + 1)]
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
-      double Ec = 0.25 * (Epp[ID(i, j)] + Epp[ID(i - 1, j)] + Epp[ID(i, j - 1)] + Epp[ID(i - 1, j - 1)]);
+      double Ec = 0.25 * (EC(i, j) + EC(i - 1, j) + EC(i, j - 1) + EC(i - 1, j - 1));
       A[2 * N + ID(i, j)] = A_s[2 * N + ID(i, j)] - h * Ec;
     }
+#undef EC
+  const double* A2 = A + 2 * N;
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
-      ucon[5 * N + ID(i, j)] = (AT(A, 2, i, j + 1) - AT(A, 2, i, j - 1)) / (2.0 * G.dy);
-      ucon[6 * N + ID(i, j)] = -(AT(A, 2, i + 1, j) - AT(A, 2, i - 1, j)) / (2.0 * G.dx);
+      ucon[5 * N + ID(i, j)] = (agh(A2, i, j + 1) - agh(A2, i, j - 1)) / (2.0 * G.dy);
+      ucon[6 * N + ID(i, j)] = -(agh(A2, i + 1, j) - agh(A2, i - 1, j)) / (2.0 * G.dx);
     }
   free(Ep0); free(E0p); free(Et); free(Epp);
 }
@@ -1924,12 +1952,11 @@ double ora_div_error(void) {
 }
 
 /* Boundary conditions per direction (config.hpp:36-37 ordinals): 0 Transmissive or
- * 2 Periodic.  Call after ora_setup and before ora_load_prim.  Transmissive runs are
- * restated for the face-based and the divergence-cleaning-free magnetic forms. */
+ * 2 Periodic.  Call after ora_setup and before ora_load_prim.  Every magnetic form runs
+ * with either; the legacy CT variants (fn_substep 6) are restated for periodic runs. */
 int ora_set_bc(int x_bc, int y_bc) {
   if (!G.ready) return 1;
   if ((x_bc != 0 && x_bc != 2) || (y_bc != 0 && y_bc != 2)) return 2;
-  if ((x_bc == 0 || y_bc == 0) && PP.magfield != StaggerCT && PP.magfield != NoDivFree) return 2;
   G.xclamp = x_bc == 0;
   G.yclamp = y_bc == 0;
   return 0;

@@ -63,6 +63,9 @@ STEP_CASES = {
     "blast16_energyformula_open": (lambda: open_blast(16), 2,
                                    dict(recon="Minmod", magfield="StaggerCT", formula="EnergyFormula",
                                         GMREStol=1e-12), 2),
+    "blast16_potentialA_weno5_open_rk3": (lambda: open_blast(16), 3,
+                                          dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5), 2),
+    "blast14x12_unstag_minmod_open": (lambda: open_blast(14, 12), 2, dict(recon="Minmod", magfield="UnStaggerCT"), 2),
     "blast16x12_xperiodic_open_y": (lambda: open_blast(16, 12), 2,
                                     dict(recon="VanLeer", magfield="StaggerCT", x_bc="x_Periodic",
                                          floor_on=0, PressureSolver="once_correction"), 2),

@@ -99,7 +99,9 @@ def test_port_matches_live_reference(kind, n, rks, settings, steps):
     (2, dict(recon="VanLeer", magfield="StaggerCT")),
     (3, dict(recon="WENO5", magfield="StaggerCT", p_floor=1e-8, y_bc="y_Periodic")),
     (2, dict(recon="Minmod", magfield="NoDivFree", formula="EnergyFormula", GMREStol=1e-12)),
-], ids=["vanleer_ct", "weno5_ct_yperiodic", "minmod_nodivfree_energy"])
+    (3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+    (2, dict(recon="VanLeer", magfield="UnStaggerCT", x_bc="x_Periodic")),
+], ids=["vanleer_ct", "weno5_ct_yperiodic", "minmod_nodivfree_energy", "weno5_potentialA", "unstag_xperiodic"])
 def test_port_matches_live_reference_transmissive(rks, settings):
     """Transmissive boundaries: every sub-step of every stage, boundary faces included."""
     from imex_b200.problems import open_blast
@@ -115,6 +117,7 @@ def test_port_matches_live_reference_transmissive(rks, settings):
                 if a is None:
                     continue
                 np.testing.assert_array_equal(b, a, err_msg=f"stage {k} after {sub}")
+                np.testing.assert_array_equal(port.snapshot(k, sub, "A"), ref.snapshot(k, sub, "A"))
                 for w in ("bx", "by", "bxQs", "byQs"):
                     np.testing.assert_array_equal(port.snapshot(k, sub, w), ref.snapshot(k, sub, w))
                     np.testing.assert_array_equal(port.snapshot_boundary(k, sub, w),
@@ -127,8 +130,7 @@ def test_port_refuses_unsupported_boundaries():
     from imex_b200.problems import open_blast
     prob = open_blast(12)
     for bc, magfield in ((("x_Reflective", "y_Periodic"), "StaggerCT"), (("x_Dirichlet", "y_Periodic"), "StaggerCT"),
-                         (("x_Periodic", "y_JetInflow"), "StaggerCT"), (("x_Transmissive", "y_Periodic"), "PotentialA"),
-                         (("x_Periodic", "y_Transmissive"), "UnStaggerCT")):
+                         (("x_Periodic", "y_JetInflow"), "StaggerCT"), (("x_Transmissive", "y_Reflective"), "PotentialA")):
         with pytest.raises(RuntimeError):
             make_solver("port", prob, 2, dict(magfield=magfield, x_bc=bc[0], y_bc=bc[1]))
 
