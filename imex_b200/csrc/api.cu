@@ -71,6 +71,8 @@ void prof_harvest(imex_ctx* ctx) {
 // EOS iteration-cap flags of the two kernel translation units
 imex_status eos_flag_stage(imex_ctx* ctx, int* flag, bool reset);
 imex_status eos_flag_solve(imex_ctx* ctx, int* flag, bool reset);
+imex_status eos_flag_stage_enqueue(imex_ctx* ctx, int* host_flag);
+imex_status eos_flag_solve_enqueue(imex_ctx* ctx, int* host_flag);
 
 namespace {
 
@@ -167,14 +169,23 @@ imex_status write_scalars(imex_ctx* ctx) {
 }
 
 // worst status recorded on the device since the last call (resets it)
-imex_status device_status(imex_ctx* ctx) {
+// The status of the work queued so far, with one wait: the solve statistics, both EOS
+// flags and (with_scalars) the step scalars come back in one round trip.
+imex_status device_status(imex_ctx* ctx, bool with_scalars = false) {
+  int* flags = reinterpret_cast<int*>(ctx->h_red);
   cudaError_t e = cudaMemcpyAsync(ctx->h_st, ctx->st, sizeof(DevStats), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess && with_scalars)
+    e = cudaMemcpyAsync(ctx->h_sc, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "status readback");
+  imex_status q = eos_flag_stage_enqueue(ctx, &flags[0]);
+  if (q == IMEX_OK) q = eos_flag_solve_enqueue(ctx, &flags[1]);
+  if (q != IMEX_OK) return q;
+  e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "status readback");
   int s = ctx->h_st->status;
-  int f1 = 0, f2 = 0;
-  eos_flag_stage(ctx, &f1, true);
-  eos_flag_solve(ctx, &f2, true);
+  int f1 = flags[0], f2 = flags[1];
+  if (f1) eos_flag_stage(ctx, &f1, true);  // clears it
+  if (f2) eos_flag_solve(ctx, &f2, true);
   if ((f1 || f2) && s < IMEX_ERR_EOS) s = IMEX_ERR_EOS;
   if (s != IMEX_OK) {
     int zero = 0;
@@ -599,11 +610,9 @@ imex_status imex_step(imex_ctx* ctx, double* dt_out) {
   imex_status s = launch_step_prologue(ctx);
   for (int r = 0; s == IMEX_OK && r < ctx->P.RKs; ++r) s = stage_body(ctx, r);
   if (s != IMEX_OK) return s;
-  if (dt_out) {
-    if ((s = read_scalars(ctx)) != IMEX_OK) return s;
-    *dt_out = ctx->h_sc->dt;
-  }
-  return device_status(ctx);
+  s = device_status(ctx, dt_out != nullptr);
+  if (dt_out && ctx->h_sc) *dt_out = ctx->h_sc->dt;
+  return s;
 }
 
 imex_status imex_set_step_scalars(imex_ctx* ctx, const imex_step_scalars* in) {

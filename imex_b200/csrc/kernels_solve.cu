@@ -2908,6 +2908,12 @@ imex_status adj_apply(imex_ctx* ctx, const AdjOp& a, const double* x, double* Ax
   return IMEX_OK;
 }
 
+// queue the copy of this translation unit's EOS flag into pinned host memory (no wait)
+imex_status eos_flag_solve_enqueue(imex_ctx* ctx, int* host_flag) {
+  return cuda_check(ctx, cudaMemcpyFromSymbolAsync(host_flag, d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,
+                                                   ctx->stream),
+                    "eos flag");
+}
 imex_status eos_flag_solve(imex_ctx* ctx, int* flag, bool reset) {
   cudaError_t e = cudaMemcpyFromSymbolAsync(&ctx->h_red[0], d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,
                                             ctx->stream);

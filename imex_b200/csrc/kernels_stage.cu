@@ -949,6 +949,12 @@ imex_status launch_min_pressure(imex_ctx* ctx, double* pmin) {
 }
 
 
+// queue the copy of this translation unit's EOS flag into pinned host memory (no wait)
+imex_status eos_flag_stage_enqueue(imex_ctx* ctx, int* host_flag) {
+  return cuda_check(ctx, cudaMemcpyFromSymbolAsync(host_flag, d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,
+                                                   ctx->stream),
+                    "eos flag");
+}
 imex_status eos_flag_stage(imex_ctx* ctx, int* flag, bool reset) {
   cudaError_t e = cudaMemcpyFromSymbolAsync(&ctx->h_red[0], d_eos_flag, sizeof(int), 0, cudaMemcpyDeviceToHost,
                                             ctx->stream);
