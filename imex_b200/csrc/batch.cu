@@ -266,8 +266,6 @@ imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx
                               imex_batch** out) {
   if (!cfg || members < 1 || !nx || !ny || !out) return IMEX_ERR_INVALID;
   *out = nullptr;
-  // ensemble members share the fused cross-member launches, written for periodic members
-  if (cfg->x_bc != IMEX_x_Periodic || cfg->y_bc != IMEX_y_Periodic) return IMEX_ERR_UNSUPPORTED;
   imex_batch* b = new (std::nothrow) imex_batch();
   if (!b) return IMEX_ERR_CUDA;
   cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);

@@ -2206,7 +2206,7 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
   const int cap = per_sm * c0->num_sms;
   const long long limit = wait_cycles(c0);
   const int nm = (int)members.size();
-  auto tiles = [&](int m) { return make_tiling(members[m]->nx, members[m]->ny).ntiles; };
+  auto tiles = [&](int m) { return make_tiling(members[m]->nx, members[m]->ny).ntiles; };  // work only
   std::vector<int> order(nm);
   for (int m = 0; m < nm; ++m) order[m] = m;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tiles(a) > tiles(b); });
@@ -2236,7 +2236,7 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
     int first = 0;
     for (int k = 0; k < n; ++k) {
       imex_ctx* m = members[grp[k]];
-      jobs.push_back(make_job(m, make_tiling(m->nx, m->ny), first, alloc[k]));
+      jobs.push_back(make_job(m, make_tiling(m->nx, m->ny, m->P.xclamp, m->P.yclamp), first, alloc[k]));
       for (int q = 0; q < alloc[k]; ++q) map.push_back(k);
       syncs.push_back(m->sync);
       first += alloc[k];
@@ -2353,7 +2353,10 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
       int op;
       mag_system(m, &op, x, b);
     };
-    if (P.magfield == IMEX_PotentialA)
+    if (P.magfield == IMEX_PotentialA && (P.xclamp || P.yclamp))  // members share the configuration
+      s = add_gmres_chunks<MagneticAOpOpen>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<true>,
+                                            sys);
+    else if (P.magfield == IMEX_PotentialA)
       s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<false>, sys);
     else
       s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_B, make_magB_op, sys);

@@ -12,11 +12,10 @@ corner EMF on x_0 / y_0 (constrained_transport.cpp:5-30,147-164).  The checks he
 * at 256^2: face div B at round-off, p > 0, bit-identical repeat runs;
 * restart files carry the boundary faces (version 2) and continue bit for bit;
 * mixed precision against FP64 at the north-star tolerance;
+* ensembles of transmissive members match their single runs;
 * what is not built for these boundaries is refused, not run.
 """
 from __future__ import annotations
-
-import ctypes as C
 
 import numpy as np
 import pytest
@@ -199,12 +198,29 @@ def test_gpu_unbuilt_boundary_paths_are_refused():
         sv.adjoint_run(1, prob.prim[0], prob.prim[5:8])
     assert err.value.status == 2
     sv.close()
-    lib = ix.load_library()
-    cfg = ix.make_config(dict(prob.settings, magfield="StaggerCT"), (prob.x0, prob.x1, prob.y0, prob.y1), 2)
-    nx = (C.c_int * 2)(16, 16)
-    h = C.c_void_p()
-    assert lib.imex_batch_create(C.byref(cfg), 2, nx, nx, C.byref(h)) == 2
-    assert not h.value
+
+
+@pytest.mark.parametrize("rks,settings", [
+    (2, dict(recon="VanLeer", magfield="StaggerCT")),
+    (3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GMREStol=1e-12)),
+], ids=["staggered", "potentialA"])
+def test_gpu_batch_of_open_members_matches_single_runs(rks, settings):
+    """An ensemble of transmissive members on uneven grids: each member's batched solves (its
+    own CTA range, tiles clamped at its own boundaries) against the same run alone."""
+    probs = [open_blast(40, 32), open_blast(64), open_blast(24, 48)]
+    batch = ix.Batch(probs, rks, settings)
+    batch.step(3)
+    for m, p in enumerate(probs):
+        single = ix.Solver.for_problem(p, rks, settings)
+        for _ in range(3):
+            single.step()
+        a, b = batch.members[m].cons(), single.cons()
+        for k in range(8):
+            assert rel(a[k], b[k]) <= 1e-11, (m, k, rel(a[k], b[k]))
+        for u, v in zip(batch.members[m].boundary_faces(), single.boundary_faces()):
+            assert rel(u, v) <= 1e-11
+        single.close()
+    batch.close()
 
 
 def test_imex_run_driver_transmissive_matches_the_binding(tmp_path):
