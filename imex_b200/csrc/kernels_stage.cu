@@ -635,7 +635,8 @@ __global__ void k_shock_max(DevParams Pin, const double* __restrict__ chit, doub
 }
 
 // ---------------------------------------------------------------- diagnostics
-// face FV div (StaggerCT), wrapped central div of cell B, reference cell metric
+// face FV div (StaggerCT; a transmissive direction's first column / row differences against
+// its boundary face), central div of cell B over the neighbour map, reference cell metric
 // (imex_subsystems.cpp:646-654), max |central div|
 __global__ void k_divergence(DevParams P, const double* __restrict__ ucon, const double* __restrict__ bx,
                              const double* __restrict__ by, BoundaryLines L, double* __restrict__ partial) {

@@ -257,3 +257,27 @@ def test_imex_run_driver_transmissive_matches_the_binding(tmp_path):
     np.testing.assert_array_equal(h["bx_x0"], bxb)
     np.testing.assert_array_equal(h["by_y0"], byb)
     sv.close()
+
+
+def test_gpu_boundary_face_lines_follow_each_directions_kind():
+    """A transmissive direction stores the line it is given; a periodic direction ignores it and
+    reports the faces it identifies with x_0 / y_0, those at x_1 / y_1."""
+    prob = open_blast(20, 16)
+    sv = ix.Solver.for_problem(prob, 2, dict(magfield="StaggerCT", x_bc="x_Periodic"))
+    bxb, byb = sv.boundary_faces()
+    bx, by = sv.faces()
+    np.testing.assert_array_equal(bxb, bx[:, -1])       # periodic x: Bx at x_1 of each row
+    np.testing.assert_array_equal(byb, prob.by_y0)      # transmissive y: the line that was set
+    sv.set_boundary_faces(np.full(16, 7.0), np.full(20, 3.0))
+    bxb2, byb2 = sv.boundary_faces()
+    np.testing.assert_array_equal(bxb2, bx[:, -1])
+    np.testing.assert_array_equal(byb2, np.full(20, 3.0))
+    sv.close()
+    # without set_boundary_faces, the line defaults to the first interior face of its row / column
+    q = open_blast(20, 16)
+    q.bx_x0 = q.by_y0 = None
+    sv = ix.Solver.for_problem(q, 2, dict(magfield="StaggerCT"))
+    bxb, byb = sv.boundary_faces()
+    np.testing.assert_array_equal(bxb, q.bx[:, 0])
+    np.testing.assert_array_equal(byb, q.by[0, :])
+    sv.close()
