@@ -1534,8 +1534,12 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
   }
 }
 
-template <class TS>
+// kRK = false: the ideal-gas instance.  Its EOS branches fold at compile time, so it carries
+// none of the Redlich-Kwong Newton iterations and its code stays small (this persistent
+// kernel is large enough for instruction fetch to stall it).
+template <class TS, bool kRK = true>
 __global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
+  if (!kRK) op.P.eos_type = IMEX_IDEAL_GAS;
   newton_solve(op, gw, na);
 }
 template <class TS>
@@ -2170,13 +2174,13 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   imex_status s;
   prof_begin(ctx);
   if (!mixed(ctx, IMEX_MIXED_PRESSURE)) {
-    auto kern = k_nested_newton<double>;
+    auto kern = P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton<double, false> : k_nested_newton<double, true>;
     const size_t smem = sizeof(NewtonSmem<double>);
     const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
     GmresWork g = make_work(ctx, T, nb, F_NEWTON);
     s = launch_coop_smem(ctx, kern, nb, smem, o, g, na);
   } else {
-    auto kern = k_nested_newton<float>;
+    auto kern = P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton<float, false> : k_nested_newton<float, true>;
     const size_t smem = sizeof(NewtonSmem<float>);
     const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
     GmresWorkT<float> g = make_work_mixed(ctx, T, nb, F_NEWTON, make_work(ctx, T, nb, F_NEWTON).max_restarts,
