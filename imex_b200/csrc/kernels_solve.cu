@@ -1548,10 +1548,12 @@ struct NewtonJob {
   GmresWorkT<TS> gw;
   NewtonArgs na;
 };
-template <class TS>
+template <class TS, bool kRK = true>  // kRK as for k_nested_newton
 __global__ void __launch_bounds__(NT, 2) k_nested_newton_jobs(const NewtonJob<TS>* jobs, const int* cta_job) {
   const NewtonJob<TS>& j = jobs[cta_job[blockIdx.x]];
-  newton_solve(j.op, j.gw, j.na);
+  PressureOp op = j.op;
+  if (!kRK) op.P.eos_type = IMEX_IDEAL_GAS;
+  newton_solve(op, j.gw, j.na);
 }
 
 // the barrier states of the solves of one batched launch start at zero
@@ -2320,8 +2322,10 @@ imex_status add_gmres_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>&
 
 template <class TS>
 imex_status add_newton_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members) {
+  // members share the configuration, so one instance serves all of them
+  auto kern = members[0]->P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton_jobs<TS, false> : k_nested_newton_jobs<TS, true>;
   return add_chunks<NewtonJob<TS>>(
-      plan, members, k_nested_newton_jobs<TS>, sizeof(NewtonSmem<TS>),
+      plan, members, kern, sizeof(NewtonSmem<TS>),
       [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
         NewtonJob<TS> j{};
         j.op = make_pressure_op(m);
