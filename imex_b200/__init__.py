@@ -126,6 +126,7 @@ _SIGS = {
     "imex_upload_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "imex_download_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D]),
     "imex_set_boundary_faces": (C.c_int, [C.c_void_p, _D, _D]),
+    "imex_ct_emf_diagnostics": (C.c_int, [C.c_void_p, _D]),
     "imex_get_boundary_faces": (C.c_int, [C.c_void_p, _D, _D]),
     "imex_step": (C.c_int, [C.c_void_p, _D]),
     "imex_begin_step": (C.c_int, [C.c_void_p]),
@@ -515,6 +516,15 @@ class Solver:
         d = Diagnostics()
         self._check(self.lib.imex_diagnostics(self.ctx, C.byref(d)))
         return d.as_dict()
+
+    CT_DIAG_PARTS = ("central", "rusanov", "tilde", "TOTAL")
+
+    def ct_emf_diagnostics(self) -> dict:
+        """The reference's per-step [CT-DIAG] figures (Diagnose_CT_EMF): for each part of the
+        corner EMF, (L2 of Ez, max |Ez|, L2 of |dB/dt|, max |dB/dt|)."""
+        out = np.zeros(16)
+        self._check(self.lib.imex_ct_emf_diagnostics(self.ctx, _dp(out)))
+        return {name: tuple(out[4 * c:4 * c + 4].tolist()) for c, name in enumerate(self.CT_DIAG_PARTS)}
 
     def write_vtk(self, path: str, cycle: int = 0) -> None:
         self._check(self.lib.imex_write_vtk(self.ctx, str(path).encode(), cycle))

@@ -179,6 +179,7 @@ imex_status launch_prim_from_cons(imex_ctx* ctx);
 imex_status launch_cons_from_prim(imex_ctx* ctx);
 imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta);
 imex_status launch_divergence(imex_ctx* ctx, double* out4);
+imex_status launch_ct_diag(imex_ctx* ctx, double* out16);
 imex_status launch_min_pressure(imex_ctx* ctx, double* pmin);
 imex_status launch_qe_derived(imex_ctx* ctx);
 imex_status launch_vslope(imex_ctx* ctx);

@@ -547,6 +547,82 @@ __global__ void k_ct_legacy_faces(DevParams P, const double* __restrict__ w, dou
   e0p[n] = (0.5 * (g5(wyR, n) + g5(wyL, cid(P, i, j + 1))));
 }
 
+// ---------------------------------------------------------------- CT EMF diagnostics
+// Diagnose_CT_EMF (constrained_transport.cpp:183-222), printed by the reference's driver after
+// every step (main.cpp:594).  The face EMFs of the reconstructed u_con split into their central
+// average (C: -(f6_L + f6_R)/2 and (g5_L + g5_R)/2) and their Rusanov dissipation (R), plus the
+// cell EMF Ez~ (T); CT_CornerAssemble turns each into corner EMFs with the other inputs zero.
+__global__ void k_ct_diag_faces(DevParams P, const double* __restrict__ w, double* __restrict__ cp0,
+                                double* __restrict__ c0p, double* __restrict__ rp0, double* __restrict__ r0p) {
+  const long long N = P.N;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
+  auto f6 = [&](const double* q, long long m) {  // f_full_con[6], state.cpp:152-175
+    double r = __ldg(q + m);
+    return __ldg(q + 6 * N + m) * (__ldg(q + N + m) / r) - (__ldg(q + 2 * N + m) / r) * __ldg(q + 5 * N + m);
+  };
+  auto g5 = [&](const double* q, long long m) {  // g_full_con[5], state.cpp:179-200
+    double r = __ldg(q + m);
+    return __ldg(q + 5 * N + m) * (__ldg(q + 2 * N + m) / r) - (__ldg(q + N + m) / r) * __ldg(q + 6 * N + m);
+  };
+  auto q = [&](const double* a, int k, long long m) { return __ldg(a + k * N + m); };
+  const long long xp = cid(P, i + 1, j), yp = cid(P, i, j + 1);
+  cp0[n] = -(0.5 * (f6(wxR, n) + f6(wxL, xp)));
+  rp0[n] = 0.5 * fmax(fabs(q(wxR, 1, n) / q(wxR, 0, n)), fabs(q(wxL, 1, xp) / q(wxL, 0, xp))) *
+           (q(wxL, 6, xp) - q(wxR, 6, n));
+  c0p[n] = 0.5 * (g5(wyR, n) + g5(wyL, yp));
+  r0p[n] = -0.5 * fmax(fabs(q(wyR, 2, n) / q(wyR, 0, n)), fabs(q(wyL, 2, yp) / q(wyL, 0, yp))) *
+           (q(wyL, 5, yp) - q(wyR, 5, n));
+}
+// CT_EMF_Stats (constrained_transport.cpp:166-181) of C, R, T and their sum: per block the
+// sums of dx dy Ez^2 and dx dy |dB/dt|^2 (slots 0-7) and the maxima of |Ez| and |dB/dt|
+// (slots 8-15), where dB/dt = (-(E(i,j) - E(i,j-1))/dy, (E(i,j) - E(i-1,j))/dx) on the faces.
+__global__ void k_ct_diag_stats(DevParams P, const double* __restrict__ cp0, const double* __restrict__ c0p,
+                                const double* __restrict__ rp0, const double* __restrict__ r0p,
+                                const double* __restrict__ ucon, double* __restrict__ partial) {
+  const long long N = P.N;
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0}, mx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const double* fx[3] = {cp0, rp0, nullptr};
+  const double* fy[3] = {c0p, r0p, nullptr};
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    double e[4][3];  // component (C, R, T, total) x corner ((i, j), (i, j-1), (i-1, j))
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      // C and R: their face EMFs and a zero cell EMF (rho 1, B 0); T: zero face EMFs and Ez~(u_con)
+      auto ld = [&](int a, int k, long long m) -> double {
+        if (a == CC_UCON) return c == 2 ? __ldg(ucon + k * N + m) : (k == 0 ? 1.0 : 0.0);
+        if (c == 2) return 0.0;
+        return __ldg((a == CC_FX ? fx[c] : fy[c]) + m);
+      };
+      e[c][0] = corner_emf(P, 1.0, 1.0, i, j, ld);
+      e[c][1] = corner_emf(P, 1.0, 1.0, i, j - 1, ld);
+      e[c][2] = corner_emf(P, 1.0, 1.0, i - 1, j, ld);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[3][k] = e[0][k] + e[1][k] + e[2][k];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double ez = e[c][0];
+      sum[c] += P.dx * P.dy * ez * ez;
+      mx[c] = fmax(mx[c], fabs(ez));
+      const double dBx = -(e[c][0] - e[c][1]) / P.dy, dBy = (e[c][0] - e[c][2]) / P.dx;
+      const double m2 = dBx * dBx + dBy * dBy;
+      sum[4 + c] += P.dx * P.dy * m2;
+      mx[4 + c] = fmax(mx[4 + c], sqrt(m2));
+    }
+  }
+  block_reduce(sum, FSum(), 0.0);
+  block_reduce(mx, FMax(), 0.0);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 8; ++k) {
+      partial[blockIdx.x * 16 + k] = sum[k];
+      partial[blockIdx.x * 16 + 8 + k] = mx[k];
+    }
+}
+
 // ---------------------------------------------------------------- stage derivative
 // Energy_Modify (main.cpp:528-534), Hs / HsA / HsB (main.cpp:539-555), u_pri (main.cpp:537).
 __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __restrict__ sc, double* __restrict__ cons,
@@ -930,6 +1006,39 @@ imex_status launch_divergence(imex_ctx* ctx, double* out4) {
   out4[1] = sqrt(s1);
   out4[2] = sqrt(s2);
   out4[3] = m;
+  return IMEX_OK;
+}
+
+// out[4 c + q] for component c = central, rusanov, tilde, total and q = L2(Ez), max|Ez|,
+// L2(dB/dt), max|dB/dt| (the four [CT-DIAG] lines).  Uses the reconstruction buffer and
+// stage work planes, which only the inside of a stage reads.
+imex_status launch_ct_diag(imex_ctx* ctx, double* out16) {
+  const DevParams& P = ctx->P;
+  const int nb = blocks_for(P.N);
+  cudaStream_t s = ctx->stream;
+  double *cp0 = ctx->chit, *c0p = ctx->Et, *rp0 = ctx->Epp, *r0p = ctx->vscale;
+  if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
+  else IMEX_LAUNCH_BC(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
+  k_ct_diag_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, cp0, c0p, rp0, r0p);
+  int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
+  k_ct_diag_stats<<<nred, kThreads, 0, s>>>(P, cp0, c0p, rp0, r0p, ctx->cons, ctx->partial);
+  LAUNCH_CHECK(ctx, "CT EMF diagnostics");
+  std::vector<double> h((size_t)nred * 16);
+  cudaError_t e = cudaMemcpyAsync(h.data(), ctx->partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "CT EMF diagnostics readback");
+  double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0}, mx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nred; ++b)
+    for (int k = 0; k < 8; ++k) {
+      sum[k] += h[(size_t)b * 16 + k];
+      mx[k] = fmax(mx[k], h[(size_t)b * 16 + 8 + k]);
+    }
+  for (int c = 0; c < 4; ++c) {
+    out16[4 * c + 0] = sqrt(sum[c]);
+    out16[4 * c + 1] = mx[c];
+    out16[4 * c + 2] = sqrt(sum[4 + c]);
+    out16[4 * c + 3] = mx[4 + c];
+  }
   return IMEX_OK;
 }
 

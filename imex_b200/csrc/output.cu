@@ -170,6 +170,11 @@ int imex_history_write_host(const char* path, int n, const int* steps, const dou
 }
 
 // ---- on a context
+imex_status imex_ct_emf_diagnostics(imex_ctx* ctx, double* out16) {
+  if (!ctx || !out16) return IMEX_ERR_INVALID;
+  return launch_ct_diag(ctx, out16);
+}
+
 imex_status imex_diagnostics(imex_ctx* ctx, imex_diagnostics_t* d) {
   if (!ctx || !d) return IMEX_ERR_INVALID;
   const DevParams& P = ctx->P;

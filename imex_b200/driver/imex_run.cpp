@@ -11,7 +11,8 @@
 //   name           prefix of the VTK files (plt_<name>_<step>.vtk)
 // The initial state is a state file (imex_save_state_file; the Python problems write them).
 // Per step the reference's console lines are printed ("[timestep, dt, time] = ...,
-// Divergence Error: ..." and "DIAG ts=..."), and after the run the output directory holds
+// Divergence Error: ...", "DIAG ts=..." and the four "[CT-DIAG]" lines of its EMF
+// decomposition, main.cpp:562-594), and after the run the output directory holds
 // the VTK files, the histories RK_div_error.dat, RK_B_inf.dat, RK_dt_comp.dat, the field
 // files RK_*.dat and final_state.bin.
 #include <cstddef>
@@ -157,6 +158,12 @@ int main(int argc, char** argv) {
     std::printf("[timestep, dt, time] = %d %.17g %.17g, Divergence Error: %.17g\n", d.timestep, dt, d.t, d.div_error);
     std::printf("DIAG ts=%d t=%.17g emin=%.17g at(%.17g,%.17g) mass=%.17g intE=%.17g magE_max=%.17g\n", d.timestep,
                 d.t, d.emin, d.emin_x, d.emin_y, d.mass, d.intE, d.magE_max);
+    double ct[16];
+    if ((s = imex_ct_emf_diagnostics(ctx, ct)) != IMEX_OK) return fail(ctx, s, "CT EMF diagnostics");
+    static const char* parts[4] = {"central", "rusanov", "tilde", "TOTAL"};
+    for (int c = 0; c < 4; ++c)
+      std::printf("[CT-DIAG] %-8s  Ez: L2=%.3e max=%.3e | dB/dt: L2=%.3e max=%.3e\n", parts[c], ct[4 * c],
+                  ct[4 * c + 1], ct[4 * c + 2], ct[4 * c + 3]);
     steps.push_back(d.timestep);
     div.push_back(d.div_error);
     binf.push_back(d.B_inf);

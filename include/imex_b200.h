@@ -318,6 +318,13 @@ typedef struct imex_diagnostics_t {
   double magE_max;              /* max |B|^2 / 2 */
 } imex_diagnostics_t;
 imex_status imex_diagnostics(imex_ctx* ctx, imex_diagnostics_t* d);
+/* Diagnose_CT_EMF (constrained_transport.cpp:166-222), which the reference's driver prints
+ * after every step (main.cpp:594): the corner EMF of the current state split into its parts
+ * from the central face average, the Rusanov dissipation and the cell EMF Ez~, and their sum.
+ * out[4 c + q] for c = central, rusanov, tilde, total and q = L2 of Ez, max |Ez|, L2 of the
+ * face injection rate |dB/dt|, its max.  Overwrites the reconstruction buffer (IMEX_BUF_W)
+ * and the stage work planes, which only the inside of a stage reads. */
+imex_status imex_ct_emf_diagnostics(imex_ctx* ctx, double* out16);
 /* Legacy-VTK rectilinear grid of the current state: the reference's 13 cell fields (rho,
  * mom_X/Y/Z, U, B_X/Y/Z, velX/Y/Z, p, B), node coordinates on the nx + 1 / ny + 1 cell faces,
  * interior cells only, 17 significant digits. */

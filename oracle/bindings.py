@@ -235,6 +235,33 @@ class _Solver:
     def div_error(self) -> float:
         return self._f("div_error")()
 
+    CT_DIAG_PARTS = ("central", "rusanov", "tilde", "TOTAL")
+
+    def ct_diag(self) -> dict:
+        """Diagnose_CT_EMF's figures on the current state: {part: (L2 Ez, max|Ez|, L2 dB/dt,
+        max|dB/dt|)}.  The C restatement returns them at full precision; the reference's own
+        function prints them (%.3e), and those printed lines are parsed."""
+        if self.prefix == "ora_":
+            out = np.zeros(16)
+            fn = self.lib.ora_ct_diag
+            fn.restype, fn.argtypes = None, [C.POINTER(C.c_double)]
+            fn(_dp(out))
+            return {name: tuple(out[4 * c:4 * c + 4].tolist()) for c, name in enumerate(self.CT_DIAG_PARTS)}
+        import re
+        import tempfile
+        fn = self.lib.ref_ct_diag_print
+        fn.restype, fn.argtypes = C.c_int, [C.c_char_p]
+        with tempfile.NamedTemporaryFile("r", suffix=".txt") as f:
+            if fn(f.name.encode()) != 0:
+                raise RuntimeError("ref_ct_diag_print failed")
+            text = open(f.name).read()
+        out = {}
+        for line in text.splitlines():
+            m = re.match(r"\[CT-DIAG\]\s+(\S+)\s+Ez: L2=(\S+) max=(\S+) \| dB/dt: L2=(\S+) max=(\S+)", line)
+            if m:
+                out[m.group(1)] = tuple(float(v) for v in m.groups()[1:])
+        return out
+
     # ---- single functions on caller-supplied state -------------------
     def reconstruct(self, Q: np.ndarray) -> np.ndarray:
         Q = _c(Q)

@@ -1984,3 +1984,64 @@ int ora_get_snapshot_boundary(int rks, int sub, int which, double* out) {
   else boundary_lines(NULL, v, NULL, out);
   return 0;
 }
+
+/* Diagnose_CT_EMF with CT_EMF_Stats, constrained_transport.cpp:166-222 (printed by the
+ * reference's driver after every step, main.cpp:594): the statistics it prints, returned.
+ * out[4 c + q]: c = central, rusanov, tilde, total; q = L2(Ez), max|Ez|, L2(dB/dt), max|dB/dt|. */
+void ora_ct_diag(double* out) {
+  const size_t N = G.N;
+  const double dx = G.dx, dy = G.dy;
+  double* w = alloc(32 * N);
+  double *cp0 = alloc(N), *c0p = alloc(N), *rp0 = alloc(N), *r0p = alloc(N), *zero = alloc(N), *et = alloc(N);
+  double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
+  reconstruct(G.cons, wxL, wxR, wyL, wyR);
+  double QL[8], QR[8];
+  for (int i = 0; i < G.nx; i++)
+    for (int j = 0; j < G.ny; j++) {
+      const size_t c = ID(i, j);
+      load8(wxR, c, QL);
+      load8(wxL, ID(i + 1, j), QR);
+      double fL6 = QL[6] * (QL[1] / QL[0]) - (QL[2] / QL[0]) * QL[5];
+      double fR6 = QR[6] * (QR[1] / QR[0]) - (QR[2] / QR[0]) * QR[5];
+      cp0[c] = -(0.5 * (fL6 + fR6));
+      rp0[c] = 0.5 * fmax(fabs(QL[1] / QL[0]), fabs(QR[1] / QR[0])) * (QR[6] - QL[6]);
+      load8(wyR, c, QL);
+      load8(wyL, ID(i, j + 1), QR);
+      double gL5 = QL[5] * (QL[2] / QL[0]) - (QL[1] / QL[0]) * QL[6];
+      double gR5 = QR[5] * (QR[2] / QR[0]) - (QR[1] / QR[0]) * QR[6];
+      c0p[c] = 0.5 * (gL5 + gR5);
+      r0p[c] = -0.5 * fmax(fabs(QL[2] / QL[0]), fabs(QR[2] / QR[0])) * (QR[5] - QL[5]);
+    }
+  cell_ez(et, G.cons);
+  const double* ep[3] = {cp0, rp0, zero};
+  const double* eq[3] = {c0p, r0p, zero};
+  const double* tt[3] = {zero, zero, et};
+  double l2E[4] = {0, 0, 0, 0}, mxE[4] = {0, 0, 0, 0}, l2B[4] = {0, 0, 0, 0}, mxB[4] = {0, 0, 0, 0};
+  for (int j = 0; j < G.ny; j++)
+    for (int i = 0; i < G.nx; i++) {
+      double e[4][3];
+      for (int k = 0; k < 3; ++k) {
+        e[k][0] = corner_at(i, j, ep[k], eq[k], tt[k]);
+        e[k][1] = corner_at(i, j - 1, ep[k], eq[k], tt[k]);
+        e[k][2] = corner_at(i - 1, j, ep[k], eq[k], tt[k]);
+      }
+      for (int q = 0; q < 3; ++q) e[3][q] = e[0][q] + e[1][q] + e[2][q];
+      for (int k = 0; k < 4; ++k) {
+        double v = e[k][0];
+        l2E[k] += dx * dy * v * v;
+        if (fabs(v) > mxE[k]) mxE[k] = fabs(v);
+        double dBx = -(e[k][0] - e[k][1]) / dy;
+        double dBy = (e[k][0] - e[k][2]) / dx;
+        double m2 = dBx * dBx + dBy * dBy;
+        l2B[k] += dx * dy * m2;
+        if (sqrt(m2) > mxB[k]) mxB[k] = sqrt(m2);
+      }
+    }
+  for (int k = 0; k < 4; ++k) {
+    out[4 * k + 0] = sqrt(l2E[k]);
+    out[4 * k + 1] = mxE[k];
+    out[4 * k + 2] = sqrt(l2B[k]);
+    out[4 * k + 3] = mxB[k];
+  }
+  free(w); free(cp0); free(c0p); free(rp0); free(r0p); free(zero); free(et);
+}

@@ -60,6 +60,7 @@ int ora_set_bc(int x_bc, int y_bc);
 void ora_set_boundary_faces(const double* bx_x0, const double* by_y0);
 void ora_get_boundary_faces(double* bx_x0, double* by_y0);
 int ora_get_snapshot_boundary(int rks, int sub, int which, double* out);
+void ora_ct_diag(double* out16);
 
 #ifdef __cplusplus
 }

@@ -25,8 +25,12 @@
 
 #include "declarations.hpp"
 
+#include <cstdio>
 #include <cstring>
 #include <vector>
+
+#include <fcntl.h>
+#include <unistd.h>
 
 namespace {
 
@@ -576,5 +580,21 @@ void ref_fn_substep(int sub, double h, int rks, double* ucon8, const double* Qe8
 
 // Divergence diagnostic cal_divergence_error (imex_subsystems.cpp:630).
 double ref_div_error() { return cal_divergence_error(*S.u_con, *S.Bx_p0, *S.By_0p); }
+
+// The reference's own per-step EMF decomposition (Diagnose_CT_EMF, constrained_transport.cpp:
+// 183-222, called by main.cpp:594) on the current state, its printed lines sent to `path`.
+int ref_ct_diag_print(const char* path) {
+  std::fflush(stdout);
+  const int saved = dup(1);
+  const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  if (saved < 0 || fd < 0) return 1;
+  dup2(fd, 1);
+  Diagnose_CT_EMF(*S.u_con);
+  std::fflush(stdout);
+  dup2(saved, 1);
+  close(saved);
+  close(fd);
+  return 0;
+}
 
 }  // extern "C"

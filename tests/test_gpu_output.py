@@ -108,6 +108,7 @@ def test_imex_run_driver_matches_the_binding(tmp_path):
     diag_lines = [l for l in r.stdout.splitlines() if l.startswith("DIAG ts=")]
     n = len(step_lines)
     assert n >= 2 and len(diag_lines) == n
+    assert len([l for l in r.stdout.splitlines() if l.startswith("[CT-DIAG] ")]) == 4 * n
     # the same run through the binding
     sv = ix.Solver.for_problem(p, 2, dict(CFG, time_stop=0.5))
     for _ in range(n):
@@ -124,4 +125,27 @@ def test_imex_run_driver_matches_the_binding(tmp_path):
     want = {0} | {s for s in range(1, n + 1) if s % 4 == 0} | {n}
     assert vtks == sorted(f"plt_vortex_{s}.vtk" for s in want)
     assert np.loadtxt(out / "RK_rho.dat").shape == (32 * 32, 3)
+    sv.close()
+
+
+@pytest.mark.parametrize("kind", ["vortex", "open_blast", "sheet_primstate"])
+def test_ct_emf_diagnostics_match_the_oracle(kind):
+    """The reference driver's per-step [CT-DIAG] figures (Diagnose_CT_EMF) on the device against
+    the oracle's restatement, which prints exactly the reference's lines."""
+    from imex_b200.problems import open_blast, vortex_sheet
+    if kind == "vortex":
+        prob, st = vortex(24, 20), dict(recon="VanLeer", magfield="StaggerCT")
+    elif kind == "open_blast":
+        prob, st = open_blast(40, 36), dict(recon="WENO5", magfield="StaggerCT", p_floor=1e-8)
+    else:
+        prob, st = vortex_sheet(48), dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5,
+                                          reconstate="PrimState")
+    sv = ix.Solver.for_problem(prob, 2, st)
+    cpu = make_solver("port", prob, 2, st)
+    for _ in range(2):
+        sv.step()
+        cpu.step()
+    g, c = sv.ct_emf_diagnostics(), cpu.ct_diag()
+    for name in c:
+        np.testing.assert_allclose(g[name], c[name], rtol=1e-9, atol=1e-14, err_msg=name)
     sv.close()

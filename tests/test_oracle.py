@@ -199,3 +199,26 @@ def test_random_field_reference_is_sensitive_to_its_gmres_tolerance():
         runs.append(o.cons())
     worst = max(rel(runs[0][k], runs[1][k]) for k in range(8))
     assert 1e-11 < worst < 5e-9
+
+
+@pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kind", ["vortex", "open_blast", "sheet_primstate"])
+def test_port_ct_emf_diagnostics_print_as_the_reference(kind):
+    """Diagnose_CT_EMF (constrained_transport.cpp:166-222): the restatement's figures, printed
+    the reference's way (%.3e), are the reference's own printed lines."""
+    from imex_b200.problems import open_blast
+    if kind == "vortex":
+        prob, st = vortex(24, 20), dict(recon="VanLeer", magfield="StaggerCT")
+    elif kind == "open_blast":
+        prob, st = open_blast(24, 20), dict(recon="WENO5", magfield="StaggerCT", p_floor=1e-8)
+    else:
+        prob, st = vortex_sheet(32), dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5,
+                                          reconstate="PrimState")
+    ref, port = make_solver("ref", prob, 2, st), make_solver("port", prob, 2, st)
+    for _ in range(2):
+        ref.step()
+        port.step()
+    r, p = ref.ct_diag(), port.ct_diag()
+    assert set(r) == set(p) == {"central", "rusanov", "tilde", "TOTAL"}
+    for name in r:
+        assert ["%.3e" % v for v in p[name]] == ["%.3e" % v for v in r[name]], name
