@@ -242,6 +242,104 @@ def open_blast(n: int = 64, ny: int | None = None, b0: float = 0.5, angle: float
                    bx_x0=np.ascontiguousarray(bx_x0), by_y0=np.ascontiguousarray(by_y0))
 
 
+# The 2D problems of the reference's test catalogue: the settings main.cpp:124-178 gives each
+# (domain, gamma, boundaries, end time), the cell states of u_initialization
+# (initial_conditions.cpp:426-594), the faces it averages from neighbouring cells under those
+# boundaries (initial_conditions.cpp:716-722) and the A_z of A_initial
+# (constrained_transport.cpp:233-260).  A0 is the reference's amplitude constant (config.hpp:59).
+_A0 = 1e-3
+_S4P = math.sqrt(4.0 * math.pi)
+REFERENCE_TESTS = {
+    # name: (enum ordinal in config.hpp:29, domain, gamma, x_bc, y_bc, time_stop)
+    "Orszag_Tang": (15, (0.0, 1.0, 0.0, 1.0), 1.4, "x_Periodic", "y_Periodic", 1.0),
+    "blastwave": (16, (-0.5, 0.5, -0.5, 0.5), 1.4, "x_Transmissive", "y_Transmissive", 0.01),
+    "Rotor": (18, (-0.5, 0.5, -0.5, 0.5), 1.4, "x_Transmissive", "y_Transmissive", 0.25),
+    "FieldLoop": (19, (-1.0, 1.0, -0.5, 0.5), 5.0 / 3.0, "x_Periodic", "y_Periodic", 1.0),
+    "KHInstability": (20, (0.0, 2.0, -0.5, 0.5), 1.4, "x_Periodic", "y_Periodic", (4.8 / _A0) / 6.0),
+    "blastwave2": (26, (-0.5, 0.5, -0.5, 0.5), 1.4, "x_Transmissive", "y_Transmissive", 0.001),
+}
+
+
+def reference_test(name: str, n: int = 128, ny: int | None = None) -> Problem:
+    """One of the reference's 2D test problems (REFERENCE_TESTS) on an n x ny grid."""
+    _, (x0, x1, y0, y1), gamma, xbc, ybc, t_end = REFERENCE_TESTS[name]
+    nx = n
+    ny = n if ny is None else ny
+    dx, dy = (x1 - x0) / nx, (y1 - y0) / ny
+    X, Y = np.meshgrid(x0 + (np.arange(nx) + 0.5) * dx, y0 + (np.arange(ny) + 0.5) * dy)
+    prim = np.zeros((8, ny, nx))
+    az = np.zeros((ny, nx))
+    pi = math.pi
+    if name == "Orszag_Tang":
+        prim[0] = gamma * gamma
+        prim[1] = -np.sin(2 * pi * Y)
+        prim[2] = np.sin(2 * pi * X)
+        prim[4] = gamma
+        prim[5] = -np.sin(2 * pi * Y)
+        prim[6] = np.sin(4 * pi * X)
+        az = np.cos(2.0 * pi * Y) / (2.0 * pi) + np.cos(4.0 * pi * X) / (4.0 * pi)
+    elif name in ("blastwave", "blastwave2"):
+        p_in, b0 = (1000.0, 70.0) if name == "blastwave" else (10000.0, 1000.0)
+        rad = np.sqrt(X * X + Y * Y)
+        eps = 1 * math.sqrt(dx * dx + dy * dy)
+        erf = np.vectorize(math.erf)
+        prim[0] = 1.0
+        prim[4] = 0.5 * (0.1 + p_in) + 0.5 * (0.1 - p_in) * erf((rad - 0.1) / eps)
+        prim[5] = b0 / math.sqrt(4.0 * pi)
+        az = (1.0 / math.sqrt(4.0 * pi) * b0) * Y
+    elif name == "Rotor":
+        disc = np.sqrt(X * X + Y * Y) <= 0.1
+        prim[0] = np.where(disc, 10.0, 1.0)
+        prim[1] = np.where(disc, -10 * Y, 0.0)
+        prim[2] = np.where(disc, 10 * X, 0.0)
+        prim[4] = 1.0
+        prim[5] = 2.5 / math.sqrt(4 * pi)
+        az = (2.5 / math.sqrt(4.0 * pi)) * Y
+    elif name == "FieldLoop":
+        r = np.sqrt(X * X + Y * Y)
+        loop = r < 0.3
+        prim[0] = 1.0
+        prim[1] = 2.0
+        prim[2] = 1.0
+        prim[4] = 1e5
+        with np.errstate(divide="ignore", invalid="ignore"):
+            prim[5] = np.where(loop, (-_A0 * Y / r) / math.sqrt(4 * pi), 0.0)
+            prim[6] = np.where(loop, (_A0 * X / r) / math.sqrt(4 * pi), 0.0)
+        az = np.where(r < 0.3, (_A0 / math.sqrt(4.0 * pi)) * (0.3 - r), 0.0)
+    elif name == "KHInstability":
+        Mx = _A0
+        eta = np.where((Y >= -9.0 / 32.0) & (Y < -7.0 / 32.0), 0.5 * (1.0 + np.sin(16.0 * pi * (Y + 0.25))),
+              np.where((Y >= -7.0 / 32.0) & (Y < 7.0 / 32.0), 1.0,
+              np.where((Y >= 7.0 / 32.0) & (Y < 9.0 / 32.0), 0.5 * (1.0 - np.sin(16.0 * pi * (Y - 0.25))), 0.0)))
+        prim[0] = 1.4
+        prim[1] = Mx * (1.0 - 2.0 * eta)
+        prim[2] = 0.1 * Mx * np.sin(2.0 * pi * X)
+        prim[4] = 1.0
+        prim[5] = 0.1 * Mx
+        az = 0.1 * _A0 * Y
+    else:
+        raise KeyError(name)
+    # faces: the average of the two cells beside each face, the outer cell by the boundary rule
+    def beside(a, axis, periodic):
+        nxt = np.roll(a, -1, axis=axis)
+        if not periodic:  # transmissive: the cell past the last one is the last one
+            idx = [slice(None)] * 2
+            idx[axis] = -1
+            nxt[tuple(idx)] = a[tuple(idx)]
+        return 0.5 * (a + nxt)
+    bx = beside(prim[5], 1, xbc == "x_Periodic")
+    by = beside(prim[6], 0, ybc == "y_Periodic")
+    A = np.zeros((3, ny, nx))
+    A[2] = az
+    settings = dict(gamma=gamma, vortex_test=0, x_bc=xbc, y_bc=ybc, time_stop=t_end)
+    lines = {}
+    if xbc == "x_Transmissive" or ybc == "y_Transmissive":  # the boundary face averages its cell twice
+        lines = dict(bx_x0=np.ascontiguousarray(0.5 * (prim[5][:, 0] + prim[5][:, 0])),
+                     by_y0=np.ascontiguousarray(0.5 * (prim[6][0, :] + prim[6][0, :])))
+    return Problem(name, nx, ny, x0, x1, y0, y1, prim, np.ascontiguousarray(bx), np.ascontiguousarray(by), A,
+                   settings=settings, **lines)
+
+
 def vortex_ensemble(members: int = 256, seed: int = 2026, smin: int = 64, smax: int = 512) -> list[Problem]:
     """Independent vortex runs (the vortex formulas above): per member kappa, mu ~ U[0.5, 1.5]
     and a square grid whose side is drawn log-uniformly from [smin, smax] and made even."""

@@ -235,6 +235,19 @@ class _Solver:
     def div_error(self) -> float:
         return self._f("div_error")()
 
+    def init_test(self, test_id: int) -> dict:
+        """The reference's own initial data of catalogue test `test_id` (reference library only)."""
+        fn = self.lib.ref_init_test
+        D = C.POINTER(C.c_double)
+        fn.restype, fn.argtypes = C.c_int, [C.c_int, D, D, D, D, D, D]
+        nx, ny = self.nx, self.ny
+        out = dict(prim=np.empty((8, ny, nx)), bx=np.empty((ny, nx)), by=np.empty((ny, nx)), bx_x0=np.empty(ny),
+                   by_y0=np.empty(nx), A=np.empty((3, ny, nx)))
+        rc = fn(test_id, *(_dp(out[k]) for k in ("prim", "bx", "by", "bx_x0", "by_y0", "A")))
+        if rc != 0:
+            raise RuntimeError("ref_init_test failed")
+        return out
+
     CT_DIAG_PARTS = ("central", "rusanov", "tilde", "TOTAL")
 
     def ct_diag(self) -> dict:

@@ -581,6 +581,25 @@ void ref_fn_substep(int sub, double h, int rks, double* ucon8, const double* Qe8
 // Divergence diagnostic cal_divergence_error (imex_subsystems.cpp:630).
 double ref_div_error() { return cal_divergence_error(*S.u_con, *S.Bx_p0, *S.By_0p); }
 
+// The reference's own initial data for catalogue test `test_id` (the Test ordinal of
+// config.hpp:29): u_initialization (initial_conditions.cpp:5-740) and A_initial
+// (constrained_transport.cpp), on the grid, domain, gamma and boundaries of ref_setup /
+// ref_set_bc.  Planes as ref_get_prim / ref_get_faces / ref_get_boundary_faces / ref_get_A.
+int ref_init_test(int test_id, double* prim8, double* bx, double* by, double* bx_x0, double* by_y0, double* A3) {
+  if (!S.ready) return 1;
+  const Test saved = test;
+  test = (Test)test_id;
+  u_initialization(*S.u_pri, *S.Bx_p0, *S.By_0p);
+  A_initial(*S.A);
+  test = saved;
+  grid_to_planes(*S.u_pri, prim8, NUM_VARS);
+  array_to_plane(*S.Bx_p0, bx);
+  array_to_plane(*S.By_0p, by);
+  ref_get_boundary_faces(bx_x0, by_y0);
+  grid_to_planes(*S.A, A3, 3);
+  return 0;
+}
+
 // The reference's own per-step EMF decomposition (Diagnose_CT_EMF, constrained_transport.cpp:
 // 183-222, called by main.cpp:594) on the current state, its printed lines sent to `path`.
 int ref_ct_diag_print(const char* path) {

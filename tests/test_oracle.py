@@ -222,3 +222,21 @@ def test_port_ct_emf_diagnostics_print_as_the_reference(kind):
     assert set(r) == set(p) == {"central", "rusanov", "tilde", "TOTAL"}
     for name in r:
         assert ["%.3e" % v for v in p[name]] == ["%.3e" % v for v in r[name]], name
+
+
+@pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["Orszag_Tang", "blastwave", "blastwave2", "Rotor", "FieldLoop", "KHInstability"])
+def test_reference_test_problems_are_the_references_initial_data(name):
+    """imex_b200.problems.reference_test restates the reference's own u_initialization and
+    A_initial for its 2D catalogue: the same cell states, faces, boundary faces and A_z."""
+    from imex_b200.problems import REFERENCE_TESTS, reference_test
+    tid, _, _, xbc, ybc, _ = REFERENCE_TESTS[name]
+    p = reference_test(name, 24, 20)
+    ref = RefSolver(p.nx, p.ny, 2, dict(p.settings), (p.x0, p.x1, p.y0, p.y1))
+    ref.set_bc(xbc, ybc)
+    got = ref.init_test(tid)
+    for k in ("prim", "bx", "by", "A"):
+        np.testing.assert_array_equal(getattr(p, k), got[k], err_msg=k)
+    if p.bx_x0 is not None:
+        np.testing.assert_array_equal(p.bx_x0, got["bx_x0"])
+        np.testing.assert_array_equal(p.by_y0, got["by_y0"])
