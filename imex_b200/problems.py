@@ -244,7 +244,7 @@ def open_blast(n: int = 64, ny: int | None = None, b0: float = 0.5, angle: float
 
 # The 2D problems of the reference's test catalogue: the settings main.cpp:124-178 gives each
 # (domain, gamma, boundaries, end time), the cell states of u_initialization
-# (initial_conditions.cpp:426-594), the faces it averages from neighbouring cells under those
+# (initial_conditions.cpp:426-594, the shock-cloud at :464-484), the faces it averages from neighbouring cells under those
 # boundaries (initial_conditions.cpp:716-722) and the A_z of A_initial
 # (constrained_transport.cpp:233-260).  A0 is the reference's amplitude constant (config.hpp:59).
 _A0 = 1e-3
@@ -257,6 +257,7 @@ REFERENCE_TESTS = {
     "FieldLoop": (19, (-1.0, 1.0, -0.5, 0.5), 5.0 / 3.0, "x_Periodic", "y_Periodic", 1.0),
     "KHInstability": (20, (0.0, 2.0, -0.5, 0.5), 1.4, "x_Periodic", "y_Periodic", (4.8 / _A0) / 6.0),
     "blastwave2": (26, (-0.5, 0.5, -0.5, 0.5), 1.4, "x_Transmissive", "y_Transmissive", 0.001),
+    "ShockCloud": (27, (0.0, 1.0, 0.0, 1.0), 5.0 / 3.0, "x_Transmissive", "y_Transmissive", 0.06),
 }
 
 
@@ -317,6 +318,16 @@ def reference_test(name: str, n: int = 128, ny: int | None = None) -> Problem:
         prim[4] = 1.0
         prim[5] = 0.1 * Mx
         az = 0.1 * _A0 * Y
+    elif name == "ShockCloud":
+        post = X < 0.6  # the shocked gas left of x = 0.6; the cloud of radius 0.15 at (0.8, 0.5)
+        cloud = np.sqrt((X - 0.8) * (X - 0.8) + (Y - 0.5) * (Y - 0.5)) < 0.15
+        prim[0] = np.where(post, 3.86859, np.where(cloud, 10.0, 1.0))
+        prim[1] = np.where(post, 0.0, -11.2536)
+        prim[4] = np.where(post, 167.345, 1.0)
+        prim[6] = np.where(post, 2.1826182, 0.56418958)
+        prim[7] = np.where(post, -2.1826182, 0.56418958)
+        az = np.where(post, -2.1826182 * X, -1.30957092 - 0.56418958 * (X - 0.6))
+        ay = np.where(post, -2.1826182 * X, -1.30957092 + 0.56418958 * (X - 0.6))
     else:
         raise KeyError(name)
     # faces: the average of the two cells beside each face, the outer cell by the boundary rule
@@ -331,6 +342,8 @@ def reference_test(name: str, n: int = 128, ny: int | None = None) -> Problem:
     by = beside(prim[6], 0, ybc == "y_Periodic")
     A = np.zeros((3, ny, nx))
     A[2] = az
+    if name == "ShockCloud":
+        A[1] = ay
     settings = dict(gamma=gamma, vortex_test=0, x_bc=xbc, y_bc=ybc, time_stop=t_end)
     lines = {}
     if xbc == "x_Transmissive" or ybc == "y_Transmissive":  # the boundary face averages its cell twice

@@ -15,7 +15,8 @@ from oracle.bindings import make_solver
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["Orszag_Tang", "blastwave", "blastwave2", "Rotor", "FieldLoop", "KHInstability"])
+@pytest.mark.parametrize("name", ["Orszag_Tang", "blastwave", "blastwave2", "Rotor", "FieldLoop", "KHInstability",
+                                  "ShockCloud"])
 @pytest.mark.parametrize("settings", [dict(), dict(magfield="StaggerCT", recon="VanLeer")], ids=["defaults", "ct"])
 def test_reference_test_problem_steps_match_oracle(name, settings):
     prob = reference_test(name, 40, 36)

@@ -225,7 +225,8 @@ def test_port_ct_emf_diagnostics_print_as_the_reference(kind):
 
 
 @pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("name", ["Orszag_Tang", "blastwave", "blastwave2", "Rotor", "FieldLoop", "KHInstability"])
+@pytest.mark.parametrize("name", ["Orszag_Tang", "blastwave", "blastwave2", "Rotor", "FieldLoop", "KHInstability",
+                                  "ShockCloud"])
 def test_reference_test_problems_are_the_references_initial_data(name):
     """imex_b200.problems.reference_test restates the reference's own u_initialization and
     A_initial for its 2D catalogue: the same cell states, faces, boundary faces and A_z."""
