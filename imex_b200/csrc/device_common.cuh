@@ -32,6 +32,15 @@ __device__ __forceinline__ int cjy(const DevParams& P, int j) {
 __device__ __forceinline__ long long cid(const DevParams& P, int i, int j) {
   return (long long)cix(P, i) + (long long)P.nx * cjy(P, j);
 }
+// Order key of a double: unsigned comparison of keys is numeric comparison of the values.
+__device__ __forceinline__ unsigned long long dkey(double d) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_value(unsigned long long k) {
+  return __longlong_as_double((long long)((k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k));
+}
+
 // The parameters a kernel instantiated for periodic (kOpen = false) or transmissive
 // (kOpen = true) neighbour maps works with: the periodic instance has the wrap as
 // compile-time constants, so its index arithmetic is the plain wrap.

@@ -53,6 +53,10 @@ struct DevScalars {
   double h;                 // implicit step of the current sub-step
   int timestep;
   int pad;
+  // order keys (dkey) of min b and of ~max V(p_floor, rho) over the cells, from the pressure
+  // right-hand sides of a stage (slot 0: the first solve, slot 1: the second) for the nested
+  // Newton's floor slope Mbig; k_pressure_coeffs resets them at the start of the sub-system
+  unsigned long long bkey[2][2];
 };
 
 // Kernel launch families of the live profile.

@@ -1315,6 +1315,7 @@ struct NewtonArgs {
   double *p, *pf, *g, *dp, *vdiag;
   const double* b;
   DevScalars* sc;
+  const unsigned long long* bkeys;  // min b / max V keys from k_pressure_rhs, or null: reduce here
 };
 
 // Shared memory of the nested Newton: the FP64 tile of the residual passes and the
@@ -1349,7 +1350,18 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
 
   // ---- Cor. 1 slope Mbig (implicit_operators.cpp:670-686)
   double Mbig = na.sc->Mbig;
-  if (P.floor_on) {
+  if (P.floor_on && na.bkeys) {
+    // min b and max V(p_floor, rho) came with the right-hand side (k_pressure_rhs)
+    const unsigned long long kb = na.bkeys[0], kv = ~na.bkeys[1];
+    const double bmin = kb == ~0ull ? INFINITY : dkey_value(kb);
+    double Vpe = P.p_floor / (P.gamma - 1.0);
+    if (P.eos_type != IMEX_IDEAL_GAS && kv != 0ull && dkey_value(kv) > Vpe) Vpe = dkey_value(kv);
+    double q = Vpe - bmin;
+    double M_cor = ((0.0 < q) ? q : 0.0) / ((1.0 - P.theta) * P.p_floor);
+    double M_base = P.Mbig_fac / (P.gamma - 1.0);
+    Mbig = (M_base < M_cor) ? M_cor : M_base;
+    if (lead) na.sc->Mbig = Mbig;
+  } else if (P.floor_on) {
     double mn = INFINITY, vpe = -INFINITY;
     for (long long c = grank(gw) * (long long)NT + threadIdx.x; c < N; c += (long long)gw.nblk * NT) {
       mn = fmin(mn, na.b[c]);
@@ -1574,10 +1586,12 @@ inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads)
 template <bool kOpen>
 __global__ void k_pressure_coeffs(DevParams Pin, const double* __restrict__ Qe, const double* __restrict__ ucon,
                                   const double* __restrict__ hQe, const double* __restrict__ pe,
-                                  double* __restrict__ hh, double* __restrict__ vscale, double* __restrict__ rv) {
+                                  double* __restrict__ hh, double* __restrict__ vscale, double* __restrict__ rv,
+                                  unsigned long long* __restrict__ bkeys) {
   const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n < 4) bkeys[n] = ~0ull;  // the identities of the min keys k_pressure_rhs forms next
   if (n >= N) return;
   const double r = ucon[n];
   hh[n] = hQe[n] * Qe[n] / r;
@@ -1606,20 +1620,51 @@ template <bool kOpen>
 __global__ void k_pressure_rhs(DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                const double* __restrict__ hh, const double* __restrict__ rv,
                                const double* __restrict__ kin, double* __restrict__ b,
-                               const double* __restrict__ p0src, double* __restrict__ p0) {
+                               const double* __restrict__ p0src, double* __restrict__ p0,
+                               unsigned long long* __restrict__ bkeys) {
   const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   const double h = sc->h;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-  const double* arr[4] = {ucon, hh, rv, kin};
-  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
-  double out[1];
-  pressure_rhs_cell<double>(P, h, nb, ld, out);
-  b[n] = out[0];
-  if (p0) p0[n] = p0src[n];
+  unsigned long long kb = ~0ull, kv = ~0ull;  // identities of min
+  if (n < N) {
+    long long nb[9];
+    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    const double* arr[4] = {ucon, hh, rv, kin};
+    auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+    double out[1];
+    pressure_rhs_cell<double>(P, h, nb, ld, out);
+    b[n] = out[0];
+    if (p0) p0[n] = p0src[n];
+    if (out[0] == out[0]) kb = dkey(out[0]);
+    if (P.floor_on && P.eos_type != IMEX_IDEAL_GAS) {
+      const double v = Vbase(P, P.p_floor, ucon[n]);
+      if (isfinite(v)) kv = ~dkey(v);
+    }
+  }
+  // the nested Newton's Cor.1 inputs (implicit_operators.cpp:670-686): min b and max V(p_floor,
+  // rho), as exact order-key minima, so that the solve needs no reduction pass of its own
+  if (bkeys) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long ob = __shfl_xor_sync(0xffffffffu, kb, o), ov = __shfl_xor_sync(0xffffffffu, kv, o);
+      kb = ob < kb ? ob : kb;
+      kv = ov < kv ? ov : kv;
+    }
+    __shared__ unsigned long long sk[2][kThreads / 32];
+    if ((threadIdx.x & 31) == 0) {
+      sk[0][threadIdx.x >> 5] = kb;
+      sk[1][threadIdx.x >> 5] = kv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        kb = sk[0][w] < kb ? sk[0][w] : kb;
+        kv = sk[1][w] < kv ? sk[1][w] : kv;
+      }
+      if (kb < *(volatile unsigned long long*)&bkeys[0]) atomicMin(&bkeys[0], kb);
+      if (kv < *(volatile unsigned long long*)&bkeys[1]) atomicMin(&bkeys[1], kv);
+    }
+  }
 }
 // momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)
 __global__ void k_momentum(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
@@ -2045,7 +2090,7 @@ imex_status pressure_setup(imex_ctx* ctx) {
   int nb = blocks_for(P.N);
   prof_begin(ctx);
   IMEX_LAUNCH_BC(P, k_pressure_coeffs, nb, kThreads, 0, ctx->stream, P, ctx->Qe, ctx->cons, ctx->hQe, ctx->pe, ctx->hh,
-                 ctx->vscale, ctx->rv);
+                 ctx->vscale, ctx->rv, &ctx->sc->bkey[0][0]);
   LAUNCH_CHECK(ctx, "k_pressure_coeffs");
   IMEX_LAUNCH_BC(P, k_pressure_tdiag, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->hh, ctx->tdiag);
   LAUNCH_CHECK(ctx, "k_pressure_tdiag");
@@ -2159,7 +2204,9 @@ imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, con
   return cuda_check(ctx, e, "imex_gmres_noalloc: solve");
 }
 
-imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
+// keys: b is this context's pb just written by k_pressure_rhs into key slot `keys` - 1 (the
+// floor slope's inputs min b, max V); 0: the solve reduces them itself
+imex_status newton_launch(imex_ctx* ctx, double* p, const double* b, int keys = 0) {
   const DevParams& P = ctx->P;
   PressureOp o = make_pressure_op(ctx);
   if (!P.floor_on && P.eos_type == IMEX_IDEAL_GAS)  // a single linear GMRES with L (implicit_operators.cpp:664-668)
@@ -2173,6 +2220,7 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b) {
   na.vdiag = ctx->vdiag;
   na.b = b;
   na.sc = ctx->sc;
+  na.bkeys = keys ? ctx->sc->bkey[keys - 1] : nullptr;
   imex_status s;
   prof_begin(ctx);
   if (!mixed(ctx, IMEX_MIXED_PRESSURE)) {
@@ -2342,6 +2390,7 @@ imex_status add_newton_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>
         j.na.vdiag = m->vdiag;
         j.na.b = m->pb;
         j.na.sc = m->sc;
+        j.na.bkeys = nullptr;  // one plan serves both pressure solves of a stage: reduce in the kernel
         return j;
       });
 }
@@ -2497,7 +2546,7 @@ imex_status pres_part1(imex_ctx* ctx) {
   int nb = blocks_for(P.N);
   prof_begin(ctx);
   IMEX_LAUNCH_BC(P, k_pressure_rhs, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->hh, ctx->rv, ctx->rv,
-                 ctx->pb, ctx->pe, ctx->pp);
+                 ctx->pb, ctx->pe, ctx->pp, P.floor_on ? ctx->sc->bkey[0] : nullptr);
   LAUNCH_CHECK(ctx, "k_pressure_rhs");
   prof_end(ctx, F_PRES_RHS, BYTES(14), 1);
   return IMEX_OK;
@@ -2518,7 +2567,7 @@ imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
   if (*second) {
     prof_begin(ctx);
     IMEX_LAUNCH_BC(P, k_pressure_rhs, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->hh, ctx->rv,
-                   ctx->cons + P.N, ctx->pb, nullptr, nullptr);
+                   ctx->cons + P.N, ctx->pb, nullptr, nullptr, P.floor_on ? ctx->sc->bkey[1] : nullptr);
     LAUNCH_CHECK(ctx, "k_pressure_rhs(2)");
     prof_end(ctx, F_PRES_RHS, BYTES(15), 1);
   }
@@ -2538,9 +2587,9 @@ imex_status run_pre_subsystem_pressure(imex_ctx* ctx, int rks) {
   imex_status s;
   bool second = false;
   if ((s = pres_part1(ctx)) != IMEX_OK) return s;
-  if ((s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  if ((s = newton_launch(ctx, ctx->pp, ctx->pb, 1)) != IMEX_OK) return s;
   if ((s = pres_part2(ctx, rks, &second)) != IMEX_OK) return s;
-  if (second && (s = newton_launch(ctx, ctx->pp, ctx->pb)) != IMEX_OK) return s;
+  if (second && (s = newton_launch(ctx, ctx->pp, ctx->pb, 2)) != IMEX_OK) return s;
   return pres_part3(ctx);
 }
 // PreSubsystem_Energy (imex_subsystems.cpp:415-534), periodic: one GMRES on E in place
