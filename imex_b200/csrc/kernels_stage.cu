@@ -157,7 +157,10 @@ struct Tableau {
 };
 // Qe, Qs, face and A stage states (main.cpp:368-414), plus the pressure and
 // enthalpy of Qe that the implicit sub-systems freeze for the stage.
-__global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc, const double* __restrict__ cons_n,
+// R = rks: the stage count is a template parameter so that every load of a thread is
+// issued before the first is used.
+template <int R>
+__global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const double* __restrict__ cons_n,
                                 const double* __restrict__ Hs, const double* __restrict__ bx_n,
                                 const double* __restrict__ by_n, const double* __restrict__ HsB,
                                 const double* __restrict__ A_snap, const double* __restrict__ HsA,
@@ -173,14 +176,29 @@ __global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc,
     sc->h = T.aii * dt;
   }
   if (n >= N) return;
+  constexpr int RR = R > 0 ? R : 1;
+  double u[8], h[RR][8], a[3], ha[RR][3], fx = bx_n[n], fy = by_n[n], hb[RR][2];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) u[k] = cons_n[k * N + n];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) a[k] = A_snap[k * N + n];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) h[r][k] = Hs[((long long)r * 8 + k) * N + n];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ha[r][k] = HsA[((long long)r * 3 + k) * N + n];
+    hb[r][0] = HsB[((long long)r * 2 + 0) * N + n];
+    hb[r][1] = HsB[((long long)r * 2 + 1) * N + n];
+  }
   double qe[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    double e = cons_n[k * N + n], s = e;
-    for (int r = 0; r < rks; ++r) {
-      double h = Hs[((long long)r * 8 + k) * N + n];
-      e = e + T.ae[r] * dt * h;
-      s = s + T.ai[r] * dt * h;
+    double e = u[k], s = e;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      e = e + T.ae[r] * dt * h[r][k];
+      s = s + T.ai[r] * dt * h[r][k];
     }
     qe[k] = e;
     Qe[k * N + n] = e;
@@ -188,23 +206,23 @@ __global__ void k_stage_combine(DevParams P, Tableau T, int rks, DevScalars* sc,
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    double e = A_snap[k * N + n], s = e;
-    for (int r = 0; r < rks; ++r) {
-      double h = HsA[((long long)r * 3 + k) * N + n];
-      e += T.ae[r] * dt * h;
-      s += T.ai[r] * dt * h;
+    double e = a[k], s = e;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      e += T.ae[r] * dt * ha[r][k];
+      s += T.ai[r] * dt * ha[r][k];
     }
     A_e[k * N + n] = e;
     A_s[k * N + n] = s;
     A[k * N + n] = s;
   }
-  double fxe = bx_n[n], fxs = fxe, fye = by_n[n], fys = fye;
-  for (int r = 0; r < rks; ++r) {
-    double h0 = HsB[((long long)r * 2 + 0) * N + n], h1 = HsB[((long long)r * 2 + 1) * N + n];
-    fxe += T.ae[r] * dt * h0;
-    fye += T.ae[r] * dt * h1;
-    fxs += T.ai[r] * dt * h0;
-    fys += T.ai[r] * dt * h1;
+  double fxe = fx, fxs = fxe, fye = fy, fys = fye;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    fxe += T.ae[r] * dt * hb[r][0];
+    fye += T.ae[r] * dt * hb[r][1];
+    fxs += T.ai[r] * dt * hb[r][0];
+    fys += T.ai[r] * dt * hb[r][1];
   }
   bxQe[n] = fxe;
   byQe[n] = fye;
@@ -636,22 +654,32 @@ __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __res
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const double adt = sc->adt;
-  double c[8];
+  // every input first, so that the divisions below do not serialise the loads
+  double c[8], qs[8], a[3], as[3], o[3];
   load_cell<8>(cons, N, n, c);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) qs[k] = Qs[k * N + n];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    a[k] = A[k * N + n];
+    as[k] = A_s[k * N + n];
+  }
+  const double fx = bx[n], fxs = bxQs[n], fy = by[n], fys = byQs[n];
   if (P.Energy_Modify) {
-    double o5 = Bsave[n], o6 = Bsave[N + n], o7 = Bsave[2 * N + n];
-    c[4] = c[4] + ((c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) - (o5 * o5 + o6 * o6 + o7 * o7)) / 2.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[k] = Bsave[k * N + n];
+    c[4] = c[4] + ((c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) - (o[0] * o[0] + o[1] * o[1] + o[2] * o[2])) / 2.0;
     cons[4 * N + n] = c[4];
   }
   double* H = Hs + (long long)rks * 8 * N;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) H[k * N + n] = (c[k] - Qs[k * N + n]) / adt;
+  for (int k = 0; k < 8; ++k) H[k * N + n] = (c[k] - qs[k]) / adt;
   double* HA = HsA + (long long)rks * 3 * N;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) HA[k * N + n] = (A[k * N + n] - A_s[k * N + n]) / adt;
+  for (int k = 0; k < 3; ++k) HA[k * N + n] = (a[k] - as[k]) / adt;
   double* HB = HsB + (long long)rks * 2 * N;
-  HB[n] = (bx[n] - bxQs[n]) / adt;
-  HB[N + n] = (by[n] - byQs[n]) / adt;
+  HB[n] = (fx - fxs) / adt;
+  HB[N + n] = (fy - fys) / adt;
   double p[8];
   con2pri(P, p, c);
 #pragma unroll
@@ -873,8 +901,10 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
   }
   T.aii = ai[rks][rks];
   prof_begin(ctx);
-  k_stage_combine<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
-      ctx->P, T, rks, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
+  static_assert(kMaxRK == 3, "one k_stage_combine instance per stage index");
+  auto kern = rks == 0 ? k_stage_combine<0> : (rks == 1 ? k_stage_combine<1> : k_stage_combine<2>);
+  kern<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
+      ctx->P, T, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
       ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe);
   LAUNCH_CHECK(ctx, "k_stage_combine");
   if (ctx->P.xclamp || ctx->P.yclamp) {
