@@ -127,11 +127,13 @@ __device__ __forceinline__ void pressure_rhs_cell(const DevParams& P, double h, 
           h0m = ld(PR_HH, 0, s);
   const S p_star = ld(PR_UCON, 4, n) - 0.5 * B2;
   const S kx = ld(PR_KIN, 0, n), ky = ld(PR_KIN, 1, n), kz = ld(PR_KIN, 2, n);
-  auto rvx = [&](long long m) { return ld(PR_RV, 0, m); };
-  auto rvy = [&](long long m) { return ld(PR_RV, 1, m); };
-  out[0] = p_star - 0.5 * (kx * kx + ky * ky + kz * kz) / ld(PR_UCON, 0, n) -
-           h * (1 / P.dx * (0.5 * (hp0 + h00) * 0.5 * (rvx(e) + rvx(n)) - 0.5 * (hm0 + h00) * 0.5 * (rvx(w) + rvx(n))) +
-                (1 / P.dy * (0.5 * (h0p + h00) * 0.5 * (rvy(no) + rvy(n)) - 0.5 * (h0m + h00) * 0.5 * (rvy(s) + rvy(n)))));
+  // every input before the first division, so that the loads are all in flight together
+  const S rho = ld(PR_UCON, 0, n);
+  const S rxe = ld(PR_RV, 0, e), rxn = ld(PR_RV, 0, n), rxw = ld(PR_RV, 0, w);
+  const S ryo = ld(PR_RV, 1, no), ryn = ld(PR_RV, 1, n), rys = ld(PR_RV, 1, s);
+  out[0] = p_star - 0.5 * (kx * kx + ky * ky + kz * kz) / rho -
+           h * (1 / P.dx * (0.5 * (hp0 + h00) * 0.5 * (rxe + rxn) - 0.5 * (hm0 + h00) * 0.5 * (rxw + rxn)) +
+                (1 / P.dy * (0.5 * (h0p + h00) * 0.5 * (ryo + ryn) - 0.5 * (h0m + h00) * 0.5 * (rys + ryn))));
 }
 
 // ---- momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)

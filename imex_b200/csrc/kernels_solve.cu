@@ -1593,12 +1593,13 @@ __global__ void k_pressure_coeffs(DevParams Pin, const double* __restrict__ Qe, 
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n < 4) bkeys[n] = ~0ull;  // the identities of the min keys k_pressure_rhs forms next
   if (n >= N) return;
-  const double r = ucon[n];
-  hh[n] = hQe[n] * Qe[n] / r;
-  vscale[n] = Vbase_slope(P, pe[n], r);
-  rv[n] = ucon[N + n];
-  rv[N + n] = ucon[2 * N + n];
-  rv[2 * N + n] = ucon[3 * N + n];
+  const double r = ucon[n], hq = hQe[n], q = Qe[n], pn = pe[n];
+  const double m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
+  rv[n] = m1;
+  rv[N + n] = m2;
+  rv[2 * N + n] = m3;
+  hh[n] = hq * q / r;
+  vscale[n] = Vbase_slope(P, pn, r);
 }
 // Jacobi diagonal Tdiag (implicit_operators.cpp:631-649)
 template <bool kOpen>
@@ -1787,25 +1788,40 @@ __global__ void k_magnetic_rhs_A(DevParams P, const DevScalars* __restrict__ sc,
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  // every input first, so that the divisions do not serialise the loads
   const double Bxn = Qe[5 * N + n], Byn = Qe[6 * N + n], Bzn = Qe[7 * N + n];
-  const double rho = ucon[n];
-  const double Sx = ucon[N + n] / rho - h / rho * (pe[cid(P, i + 1, j)] - pe[cid(P, i - 1, j)]) / (2.0 * P.dx);
-  const double Sy = ucon[2 * N + n] / rho - h / rho * (pe[cid(P, i, j + 1)] - pe[cid(P, i, j - 1)]) / (2.0 * P.dy);
-  const double Sz = ucon[3 * N + n] / rho;
-  b[n] = A_s[n] - h * (Byn * Sz - Bzn * Sy);
-  b[N + n] = A_s[N + n] - h * (Bzn * Sx - Bxn * Sz);
-  b[2 * N + n] = A_s[2 * N + n] - h * (Bxn * Sy - Byn * Sx);
+  const double rho = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
+  const double pxp = pe[cid(P, i + 1, j)], pxm = pe[cid(P, i - 1, j)], pyp = pe[cid(P, i, j + 1)],
+               pym = pe[cid(P, i, j - 1)];
+  const double a0 = A_s[n], a1 = A_s[N + n], a2 = A_s[2 * N + n];
+  const double Sx = m1 / rho - h / rho * (pxp - pxm) / (2.0 * P.dx);
+  const double Sy = m2 / rho - h / rho * (pyp - pym) / (2.0 * P.dy);
+  const double Sz = m3 / rho;
+  b[n] = a0 - h * (Byn * Sz - Bzn * Sy);
+  b[N + n] = a1 - h * (Bzn * Sx - Bxn * Sz);
+  b[2 * N + n] = a2 - h * (Bxn * Sy - Byn * Sx);
 }
 // global A-viscosity maxima of prim(Qs) over real cells (implicit_operators.cpp:364-374)
 __global__ void k_gmax(DevParams P, const double* __restrict__ Qs, double* __restrict__ partial) {
   double m0 = 0.0, m1 = 0.0;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < P.N; n += (long long)gridDim.x * blockDim.x) {
-    double c[8], p[8];
-    load_cell<8>(Qs, P.N, n, c);
-    con2pri(P, p, c);
-    double Bsq = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
-    m0 = fmax(m0, 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4.0 * Bsq / p[0])));
-    m1 = fmax(m1, 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4.0 * Bsq / p[0])));
+  // four cells per round, all loaded before the first division (the maxima do not depend
+  // on the order cells are visited in)
+  constexpr int kU = 4;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long n0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; n0 < P.N; n0 += kU * stride) {
+    double c[kU][8];
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (n0 + u * stride < P.N) load_cell<8>(Qs, P.N, n0 + u * stride, c[u]);
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      if (n0 + u * stride >= P.N) break;
+      double p[8];
+      con2pri(P, p, c[u]);
+      double Bsq = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
+      m0 = fmax(m0, 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4.0 * Bsq / p[0])));
+      m1 = fmax(m1, 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4.0 * Bsq / p[0])));
+    }
   }
   __shared__ double sh[2][kThreads / 32];
   for (int o = 16; o > 0; o >>= 1) {

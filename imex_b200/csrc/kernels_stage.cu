@@ -715,8 +715,10 @@ __global__ void k_shock_tilde(DevParams Pin, const double* __restrict__ Q, const
       if (v < m) m = v;
     }
   long long xp = cid(P, i + 1, j), xm = cid(P, i - 1, j), yp = cid(P, i, j + 1), ym = cid(P, i, j - 1);
-  double div_u = (__ldg(Q + N + xp) / __ldg(Q + xp) - __ldg(Q + N + xm) / __ldg(Q + xm)) / (2.0 * P.dx) +
-                 (__ldg(Q + 2 * N + yp) / __ldg(Q + yp) - __ldg(Q + 2 * N + ym) / __ldg(Q + ym)) / (2.0 * P.dy);
+  // every load before the first division
+  const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
+  const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
+  double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
   double num = P.hmin * div_u + P.shock_kappa1 * m;
   double den = P.shock_kappa1 * m;
   double q = -num / den;
