@@ -442,6 +442,7 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
     A_(Vf, kv * 3 * N); A_(AVf, 2 * 3 * N); A_(mres, 3 * N); A_(mcor, 3 * N);
   }
   A_(partial, 2 * (size_t)ctx->max_blocks * NPSLOTS);
+  ctx->partial_len = 2LL * ctx->max_blocks * NPSLOTS;
   A_(red, 64);
   A_(sc, 1); A_(st, 1); A_(sync, 1);
 #undef A_
@@ -686,6 +687,7 @@ imex_status imex_MagSubsystem_UpdateA(imex_ctx* ctx, double h, int rks) {
   (void)rks;
   imex_status s = set_h(ctx, h);
   if (s == IMEX_OK) s = launch_qe_derived(ctx);
+  ctx->gmax_ready = false;  // Qs is the caller's: take its maxima
   if (s == IMEX_OK) s = run_mag_subsystem_A(ctx);
   return s != IMEX_OK ? s : device_status(ctx);
 }

@@ -125,7 +125,9 @@ struct imex_ctx {
   double* V = nullptr;      // (restart + 1) * 3 planes
   double* AV = nullptr;     // 2 * 3 planes
   double* partial = nullptr;
+  long long partial_len = 0;  // doubles in partial
   int max_blocks = 0;
+  bool gmax_ready = false;  // gmax_bx / gmax_by already hold the maxima of the current Qs
   float* Vf = nullptr;      // FP32 basis (mixed precision)
   float* AVf = nullptr;
   double* mres = nullptr;   // refinement residual (3 planes)
@@ -174,6 +176,7 @@ imex_status cuda_check(imex_ctx* ctx, cudaError_t e, const char* what);
 // launchers implemented in kernels_stage.cu
 imex_status launch_step_prologue(imex_ctx* ctx);
 imex_status launch_stage_combine(imex_ctx* ctx, int rks);
+imex_status gmax_finalize(imex_ctx* ctx, int nblk);
 imex_status launch_reconstruct(imex_ctx* ctx, bool full);
 imex_status launch_flux_update(imex_ctx* ctx, int form);
 int second_flux_form(const imex_ctx* ctx);

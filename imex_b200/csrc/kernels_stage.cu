@@ -158,16 +158,20 @@ struct Tableau {
 // Qe, Qs, face and A stage states (main.cpp:368-414), plus the pressure and
 // enthalpy of Qe that the implicit sub-systems freeze for the stage.
 // R = rks: the stage count is a template parameter so that every load of a thread is
-// issued before the first is used.
-template <int R>
-__global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const double* __restrict__ cons_n,
+// issued before the first is used.  kG: the A form also takes the global A-viscosity
+// maxima of prim(Qs) (implicit_operators.cpp:364-374, the k_gmax expression) from the Qs
+// it has just formed, one fmax pair per CTA into partial[2 * block], which saves the
+// separate pass over Qs.
+template <int R, bool kG>
+__global__ void __launch_bounds__(kThreads) k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const double* __restrict__ cons_n,
                                 const double* __restrict__ Hs, const double* __restrict__ bx_n,
                                 const double* __restrict__ by_n, const double* __restrict__ HsB,
                                 const double* __restrict__ A_snap, const double* __restrict__ HsA,
                                 double* __restrict__ Qe, double* __restrict__ Qs, double* __restrict__ bxQe,
                                 double* __restrict__ byQe, double* __restrict__ bxQs, double* __restrict__ byQs,
                                 double* __restrict__ A_s, double* __restrict__ A_e, double* __restrict__ A,
-                                double* __restrict__ pe, double* __restrict__ hQe) {
+                                double* __restrict__ pe, double* __restrict__ hQe,
+                                double* __restrict__ partial) {
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const double dt = sc->dt;
@@ -175,7 +179,8 @@ __global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const do
     sc->adt = T.aii * dt;
     sc->h = T.aii * dt;
   }
-  if (n >= N) return;
+  double g0 = 0.0, g1 = 0.0;
+  if (n < N) {
   constexpr int RR = R > 0 ? R : 1;
   double u[8], h[RR][8], a[3], ha[RR][3], fx = bx_n[n], fy = by_n[n], hb[RR][2];
 #pragma unroll
@@ -191,7 +196,7 @@ __global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const do
     hb[r][0] = HsB[((long long)r * 2 + 0) * N + n];
     hb[r][1] = HsB[((long long)r * 2 + 1) * N + n];
   }
-  double qe[8];
+  double qe[8], qs[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     double e = u[k], s = e;
@@ -201,6 +206,7 @@ __global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const do
       s = s + T.ai[r] * dt * h[r][k];
     }
     qe[k] = e;
+    qs[k] = s;
     Qe[k * N + n] = e;
     Qs[k * N + n] = s;
   }
@@ -232,6 +238,33 @@ __global__ void k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const do
   double p = eos_p(P, qe[0], e);
   pe[n] = p;
   hQe[n] = e + p / qe[0];
+  if constexpr (kG) {
+    const double vx = qs[1] / qs[0], vy = qs[2] / qs[0];
+    const double Bsq = qs[5] * qs[5] + qs[6] * qs[6] + qs[7] * qs[7];
+    g0 = fmax(g0, 0.5 * (fabs(vx) + sqrt(vx * vx + 4.0 * Bsq / qs[0])));
+    g1 = fmax(g1, 0.5 * (fabs(vy) + sqrt(vy * vy + 4.0 * Bsq / qs[0])));
+  }
+  }
+  if constexpr (kG) {
+    __shared__ double sh[2][kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+      g0 = fmax(g0, __shfl_xor_sync(0xffffffffu, g0, o));
+      g1 = fmax(g1, __shfl_xor_sync(0xffffffffu, g1, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sh[0][threadIdx.x >> 5] = g0;
+      sh[1][threadIdx.x >> 5] = g1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < kThreads / 32; ++w) {
+        g0 = fmax(g0, sh[0][w]);
+        g1 = fmax(g1, sh[1][w]);
+      }
+      partial[2 * blockIdx.x] = g0;
+      partial[2 * blockIdx.x + 1] = g1;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- reconstruction
@@ -291,14 +324,14 @@ __global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, con
   const int i = (int)(n % P.nx), j = (int)(n / P.nx);
   const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
   const double* a = Q + k * N;
-  double v[5];
+  double v[5], u[5];  // both stencils loaded before the divisions of the first reconstruction
 #pragma unroll
   for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i + d - 2, j));
+#pragma unroll
+  for (int d = 0; d < 5; ++d) u[d] = __ldg(a + cid(P, i, j + d - 2));
   double xl, xr, yl, yr;
   recon_1d(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
-#pragma unroll
-  for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i, j + d - 2));
-  recon_1d(P.recon, v[0], v[1], v[2], v[3], v[4], yl, yr, vortex);
+  recon_1d(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
   w[(0 * 8 + k) * N + n] = xl;
   w[(1 * 8 + k) * N + n] = xr;
   w[(2 * 8 + k) * N + n] = yl;
@@ -904,17 +937,29 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
   T.aii = ai[rks][rks];
   prof_begin(ctx);
   static_assert(kMaxRK == 3, "one k_stage_combine instance per stage index");
-  auto kern = rks == 0 ? k_stage_combine<0> : (rks == 1 ? k_stage_combine<1> : k_stage_combine<2>);
-  kern<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
+  const int nb = blocks_for(ctx->P.N);
+  // the A form's viscosity maxima come with the combination while one pair per CTA fits
+  // the partial buffer; otherwise the magnetic sub-system takes them in its own pass
+  const bool g = ctx->P.magfield == IMEX_PotentialA && 2LL * nb <= ctx->partial_len;
+  auto kern = g ? (rks == 0 ? k_stage_combine<0, true> : (rks == 1 ? k_stage_combine<1, true> : k_stage_combine<2, true>))
+                : (rks == 0 ? k_stage_combine<0, false> : (rks == 1 ? k_stage_combine<1, false> : k_stage_combine<2, false>));
+  kern<<<nb, kThreads, 0, ctx->stream>>>(
       ctx->P, T, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
-      ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe);
+      ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe,
+      ctx->partial);
   LAUNCH_CHECK(ctx, "k_stage_combine");
+  ctx->gmax_ready = false;
+  if (g) {
+    imex_status s = gmax_finalize(ctx, nb);
+    if (s != IMEX_OK) return s;
+    ctx->gmax_ready = true;
+  }
   if (ctx->P.xclamp || ctx->P.yclamp) {
     k_bline_combine<<<blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream>>>(ctx->P, T, rks,
                                                                                                    ctx->sc, ctx->bl);
     LAUNCH_CHECK(ctx, "k_bline_combine");
   }
-  prof_end(ctx, F_COMBINE, BYTES(44 + 13 * rks), 1);
+  prof_end(ctx, F_COMBINE, BYTES(44 + 13 * rks), g ? 2 : 1);
   return IMEX_OK;
 }
 
