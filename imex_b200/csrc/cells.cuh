@@ -141,11 +141,14 @@ enum { MO_P = 0, MO_RV = 1 };
 template <class S, class Ld>
 __device__ __forceinline__ void momentum_cell(const DevParams& P, double h, const long long* nb, Ld& ld, S* out) {
   const long long n = nb[NB_C];
-  const S pc = ld(MO_P, 0, n);
-  const S flux_xm = 0.5 * (ld(MO_P, 0, nb[NB_W]) + pc), flux_xp = 0.5 * (pc + ld(MO_P, 0, nb[NB_E]));
-  out[0] = ld(MO_RV, 0, n) - h / P.dx * (flux_xp - flux_xm);
-  const S flux_ym = 0.5 * (ld(MO_P, 0, nb[NB_S]) + pc), flux_yp = 0.5 * (pc + ld(MO_P, 0, nb[NB_N]));
-  out[1] = ld(MO_RV, 1, n) - h / P.dy * (flux_yp - flux_ym);
+  // every input before the divisions h / dx, h / dy
+  const S pc = ld(MO_P, 0, n), pw = ld(MO_P, 0, nb[NB_W]), pe = ld(MO_P, 0, nb[NB_E]);
+  const S ps = ld(MO_P, 0, nb[NB_S]), pn = ld(MO_P, 0, nb[NB_N]);
+  const S r0 = ld(MO_RV, 0, n), r1 = ld(MO_RV, 1, n);
+  const S flux_xm = 0.5 * (pw + pc), flux_xp = 0.5 * (pc + pe);
+  out[0] = r0 - h / P.dx * (flux_xp - flux_xm);
+  const S flux_ym = 0.5 * (ps + pc), flux_yp = 0.5 * (pc + pn);
+  out[1] = r1 - h / P.dy * (flux_yp - flux_ym);
 }
 
 // ---- E = V(p) + KE + ME (DefinitionofU, imex_subsystems.cpp:286-302)
