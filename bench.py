@@ -23,9 +23,19 @@ cell-stage updates of all ranks / max over ranks of the timed span.
 
 --impl reference times the reference solver's own CPU code (oracle/_ref,
 built from the reference sources; else the C restatement) on the host with
-the threads it can use (it is single-threaded), on a bounded sample of the
-same physics: the same problem on a 256 x 256 grid, one time step per
-benchmark step.
+the threads it can use (it is single-threaded), on the same workload and
+grid as the GPU arm.  One of its benchmark steps is one IMEX stage of that
+run (the metric is per stage, and one stage of the 1024^2 vortex sheet takes
+the reference about 13 s on one core), so `--steps K --warmup W` runs W + K
+consecutive stages.
+
+The default line also carries a `mixed` object: the same workload in the
+mixed-precision form (FP32 operator applications and Krylov updates inside
+FP64 refinement), its speed against the FP64 line, and its relative L2 error
+per field against the FP64 oracle on a small grid of the same physics.
+The FP64 headline is timed with the live per-kernel profile off; the
+per-kernel list and the roofline come from a second, profiled pass of the
+same steps.
 """
 from __future__ import annotations
 
@@ -66,7 +76,6 @@ CFG3 = dict(recon="WENO5", magfield="StaggerCT", floor_on=1, p_floor=1e-8, theta
 WORKLOADS["open_blast_1024"] = dict(problem="open_blast", n=1024, rks=3, settings=CFG3,
                                     desc="smooth blast in an oblique field on the open unit square 1024^2 "
                                          "(transmissive x and y), WENO5, EMF-consistent staggered CT, floor on, RK3")
-REF_SAMPLE_N = 256
 
 
 def make_problem(kind: str, n: int):
@@ -179,63 +188,151 @@ def barrier(world: int) -> None:
         dist.barrier()
 
 
-def cpu_reference_rate(steps: int, max_seconds: float, workload: str = "vortex_sheet_1024") -> dict:
-    """Reference CPU solver on the sample: cell-stage updates per second over `steps` steps."""
-    from oracle.bindings import RefSolver, make_solver, PortSolver
-    kind = "reference" if RefSolver.available() else "port"
-    wl = WORKLOADS[workload]
-    prob = make_problem(wl["problem"], REF_SAMPLE_N)
-    solver = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
+def host_info() -> dict:
+    """CPU model and core counts of the host the CPU legs run on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except Exception:
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_cores": usable}
+
+
+def arm_config(args, wl: dict, nx: int, ny: int, world: int) -> dict:
+    """The `config` object both arms print for the same workload (so the lines compare)."""
+    return {"workload": args.workload, "description": wl["desc"], "grid": f"{nx}x{ny}",
+            "stages_per_step": wl["rks"], "precision": args.precision,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (working set >> 126 MB); no flush"}
+
+
+class _RefStages:
+    """The reference CPU solver advanced one IMEX stage at a time (oracle/_ref's
+    ref_stage), or one whole time step at a time when only the C restatement exists."""
+
+    def __init__(self, prob, wl: dict):
+        import ctypes as C
+        from oracle.bindings import RefSolver, make_solver
+        self.kind = "reference" if RefSolver.available() else "port"
+        self.solver = make_solver("ref" if self.kind == "reference" else "port", prob, wl["rks"],
+                                  wl["settings"])
+        self.cells = prob.nx * prob.ny
+        self.rks = wl["rks"]
+        self._stage = None
+        if self.kind == "reference":
+            self._stage = self.solver.lib.ref_stage
+            self._stage.restype, self._stage.argtypes = C.c_int, []
+
+    @property
+    def unit_stages(self) -> int:
+        """IMEX stages one advance() runs."""
+        return 1 if self._stage is not None else self.rks
+
+    def advance(self) -> None:
+        if self._stage is not None:
+            if self._stage() < 0:
+                raise RuntimeError("ref_stage failed")
+        else:
+            self.solver.step()
+
+
+def cpu_reference_rate(prob, wl: dict, max_seconds: float, max_units: int = 4) -> dict:
+    """The reference CPU solver on the workload's own grid, from t = 0: cell-stage updates
+    per second over the first stages, stopping once `max_seconds` are spent (at least one)."""
+    ref = _RefStages(prob, wl)
     done, t_total = 0, 0.0
-    while done < steps:
+    while done < max_units:
         t0 = time.perf_counter()
-        solver.step()
+        ref.advance()
         t_total += time.perf_counter() - t0
         done += 1
         if t_total > max_seconds:
             break
-    cells = prob.nx * prob.ny * wl["rks"] * done
-    return dict(value=cells / t_total, unit="cell-updates/s", cores=1, kind=kind,
-                sample=(f"{done} time step(s) x {wl['rks']} stages of the same physics on a "
-                        f"{REF_SAMPLE_N}x{REF_SAMPLE_N} grid, from t=0, one core"),
-                seconds=t_total)
+    stages = done * ref.unit_stages
+    info = host_info()
+    return dict(value=ref.cells * stages / t_total, unit="cell-updates/s", cores=1, kind=ref.kind,
+                sample=(f"the first {stages} IMEX stage(s) of the same run ({prob.nx}x{prob.ny}, from t=0) "
+                        f"on one core of a {info['nproc']}-core host ({info['cpu_model']})"),
+                host=info, seconds=t_total)
 
 
 def run_reference(args, world: int, rank: int) -> None:
+    """The reference's own CPU solver on the same workload and grid as the GPU arm: W warm-up
+    and K timed benchmark steps of one IMEX stage each (rank 0 only)."""
     if rank != 0:
         return
     try:
-        from oracle.bindings import RefSolver, make_solver
+        import oracle.bindings  # noqa: F401
     except Exception as exc:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle import failed: {exc}"}))
         return
-    kind = "reference" if RefSolver.available() else "port"
     wl = WORKLOADS[args.workload]
-    prob = make_problem(wl["problem"], REF_SAMPLE_N)
-    solver = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
-    for _ in range(args.warmup):
-        solver.step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        solver.step()
-    t = time.perf_counter() - t0
-    cells = prob.nx * prob.ny * wl["rks"] * args.steps
-    value = cells / t
+    info = host_info()
+    if wl["problem"] == "vortex_ensemble":
+        # the reference has no batching: its members run one after another, one time step of
+        # the next member (in ensemble order, smallest first) per benchmark step
+        from imex_b200.problems import vortex_ensemble
+        probs = sorted(vortex_ensemble(wl["members"], seed=2026), key=lambda q: q.nx * q.ny)
+        runs = [_RefStages(p, wl) for p in probs[:args.warmup + args.steps]]
+        for r in runs[:args.warmup]:
+            for _ in range(r.rks // r.unit_stages):
+                r.advance()
+        t0 = time.perf_counter()
+        cells = 0
+        for r in runs[args.warmup:]:
+            for _ in range(r.rks // r.unit_stages):
+                r.advance()
+            cells += r.cells * r.rks
+        t = time.perf_counter() - t0
+        value = cells / t
+        ref = runs[0]
+        nx = ny = 0
+        config = arm_config(args, wl, nx, ny, world)
+        config.pop("grid")
+        unit_desc = "one time step of one member"
+        sample = (f"{args.steps} members (the smallest, after {args.warmup} warm-up members), one time step "
+                  f"each; single-threaded reference on one core of a {info['nproc']}-core host "
+                  f"({info['cpu_model']})")
+    else:
+        prob = make_problem(wl["problem"], args.n or wl["n"])
+        ref = _RefStages(prob, wl)
+        for _ in range(args.warmup):
+            ref.advance()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ref.advance()
+        t = time.perf_counter() - t0
+        stages = args.steps * ref.unit_stages
+        value = ref.cells * stages / t
+        config = arm_config(args, wl, prob.nx, prob.ny, world)
+        unit_desc = "one IMEX stage" if ref.unit_stages == 1 else f"one time step ({ref.unit_stages} stages)"
+        sample = (f"{args.steps} consecutive benchmark steps of {unit_desc} each, after {args.warmup} warm-up, "
+                  f"of the {prob.nx}x{prob.ny} run; single-threaded reference on one core of a "
+                  f"{info['nproc']}-core host ({info['cpu_model']})")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial data)",
-        "config": {"workload": args.workload, "description": wl["desc"],
-                   "grid": f"{REF_SAMPLE_N}x{REF_SAMPLE_N} sample", "stages_per_step": wl["rks"],
-                   "parallelism": "single-threaded reference"},
-        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} timed time steps (after {args.warmup} warm-up) "
-                                   f"on a {REF_SAMPLE_N}x{REF_SAMPLE_N} grid of the same physics"},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial data, no dataset)",
+        "config": config,
+        "step_unit": unit_desc,
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": ref.kind,
+                         "sample": sample, "host": info},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+    if args.json_out:
+        with open(args.json_out, "w") as f:
+            json.dump(line, f, indent=1)
 
 
 def run_ensemble(args, world: int, rank: int, local: int) -> None:
@@ -360,8 +457,10 @@ def ensemble_cpu_rate(probs, wl, max_seconds: float) -> dict:
         done += 1
         if t_total > max_seconds:
             break
+    info = host_info()
     return dict(value=cells / t_total, unit="cell-updates/s", cores=1, kind=kind,
-                sample=f"one time step of each of the {done} smallest members, one core")
+                sample=(f"one time step of each of the {done} smallest members, one core of a "
+                        f"{info['nproc']}-core host ({info['cpu_model']})"), host=info)
 
 
 def adjoint_measure(n: int = 512, steps: int = 50, checkpoint_every: int = 10) -> dict:
@@ -418,6 +517,7 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-form measurement")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision pair")
     ap.add_argument("--n", type=int, default=None, help="override the grid side (profiling cases)")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()
@@ -444,96 +544,72 @@ def main() -> int:
     torch.cuda.set_device(local)
     wl = WORKLOADS[args.workload]
     prob = make_problem(wl["problem"], args.n or wl["n"])
-    settings = dict(wl["settings"])
-    settings["precision"] = args.precision
-    solver = ix.Solver.for_problem(prob, wl["rks"], settings)
+    cells_per_step = prob.nx * prob.ny * wl["rks"]
     stream = torch.cuda.Stream()
-    solver.set_stream(stream.cuda_stream)
+    peak, peak_kind = measured_peaks()
 
-    for _ in range(args.warmup):
-        solver.step()
+    # ---- headline: K timed steps, live profile off
+    run = timed_run(ix, prob, wl, args.precision, stream, args.steps, args.warmup, world, local,
+                    clocks=True)
+    solver = run.pop("solver")
+    t_max = run["t_max_ms"]
+    value = world * cells_per_step * args.steps / (t_max / 1e3)
+
+    # ---- second pass of the same K steps with the per-kernel profile (CUDA events per family)
     solver.reset_stats()
     solver.profile_enable(True)
-    k0 = solver.kernel_launches()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(world)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            solver.step()
-        stop.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    t_ms = start.elapsed_time(stop)
-    launches = solver.kernel_launches() - k0
+    start.record(stream)
+    for _ in range(args.steps):
+        solver.step()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    prof_ms = start.elapsed_time(stop)
     prof = solver.profile()
     solver.profile_enable(False)
     stats = solver.stats()
-    t_max = reduce_max(t_ms, world)
-    cells_per_step = prob.nx * prob.ny * wl["rks"]
-    value = world * cells_per_step * args.steps / (t_max / 1e3)
-
-    # roofline of the dominant kernel family (largest share of the timed region)
-    peak, peak_kind = measured_peaks()
     dom = max(prof, key=lambda r: r["total_ms"])
     achieved = dom["alg_bytes"] / (dom["total_ms"] / 1e3) / 1e9
     traffic = ncu_traffic(dom["name"], args.workload, prob.nx)
     total_prof_ms = sum(r["total_ms"] for r in prof)
     roofline = {"kernel": dom["name"], "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic if traffic is None else traffic,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "alg_bytes_per_launch": dom["alg_bytes"] / dom["launches"],
                 "launches": dom["launches"], "ms_per_launch": dom["total_ms"] / dom["launches"],
                 "share_of_step": dom["total_ms"] / total_prof_ms if total_prof_ms else None,
-                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                "timing": "CUDA events around each launch family, in a profiled pass of the same steps",
+                "peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                 else "fallback 6650 GB/s"}
     step_bytes = sum(r["alg_bytes"] for r in prof)
 
-    # end to end through the C ABI: pinned host state in, step, state out, every step
+    # ---- the device's FP64 rates (denominators of the FP64-bound stencil kernels)
+    fp64 = solver.selftest_fp64()
+
+    # ---- end to end through the C ABI: pinned host state in, step, state out, every step
     e2e = None
     if not args.no_e2e:
-        N = prob.nx * prob.ny
-        h_prim = torch.empty(8 * N, dtype=torch.float64, pin_memory=True)
-        h_bx = torch.empty(N, dtype=torch.float64, pin_memory=True)
-        h_by = torch.empty(N, dtype=torch.float64, pin_memory=True)
-        h_A = torch.empty(3 * N, dtype=torch.float64, pin_memory=True)
-        ptrs = (h_prim.data_ptr(), h_bx.data_ptr(), h_by.data_ptr(), h_A.data_ptr())
-        solver.download_state_ptr(*ptrs)
-        barrier(world)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        start.record(stream)
-        for _ in range(args.steps):
-            solver.upload_state_ptr(*ptrs)
-            solver.step()
-            solver.download_state_ptr(*ptrs)
-        stop.record(stream)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        e2e_ms = reduce_max(max(start.elapsed_time(stop), wall * 1e3), world)
-        nbytes = (8 + 1 + 1 + 3) * N * 8
-        e2e = {"value": world * cells_per_step * args.steps / (e2e_ms / 1e3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "path": "imex_upload_state + imex_step + imex_download_state, pinned host buffers"}
+        e2e = e2e_run(solver, prob, stream, args.steps, world, cells_per_step)
 
-    # accuracy of the mixed form: the same two steps in FP64 and in the mixed form
-    accuracy = None
-    if args.precision == "mixed" and rank == 0:
-        import numpy as np
-        res = []
-        for prec in ("fp64", "mixed"):
-            sv = ix.Solver.for_problem(prob, wl["rks"], dict(wl["settings"], precision=prec))
-            for _ in range(2):
-                sv.step()
-            res.append(sv.cons())
-            sv.close()
-        errs = [float(np.linalg.norm(res[1][k] - res[0][k]) / max(np.linalg.norm(res[0][k]), 1e-300))
-                for k in range(8)]
-        accuracy = {"reference": "FP64 GPU path (parity-tested against the FP64 oracle)", "steps": 2,
-                    "max_rel_l2_per_field": max(errs), "rel_l2_per_field": errs}
+    # ---- the mixed-precision form on the same workload, and its error against the FP64 oracle
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        solver.close()
+        solver = None
+        mrun = timed_run(ix, prob, wl, "mixed", stream, args.steps, args.warmup, world, local, clocks=False)
+        msv = mrun.pop("solver")
+        mstats = msv.stats()
+        m_ms = mrun["t_max_ms"]
+        mixed = {"value": world * cells_per_step * args.steps / (m_ms / 1e3),
+                 "ms_per_step": m_ms / args.steps, "speedup_vs_fp64": t_max / m_ms,
+                 "solver": {"gmres_iters": mstats["gmres_iters"], "newton_iters": mstats["newton_iters"],
+                            "refine_sweeps": mstats["refine_sweeps"], "status": mstats["status"]}}
+        msv.close()
+        if rank == 0:
+            mixed["accuracy"] = mixed_accuracy(ix, wl, args.workload)
+    elif args.precision == "mixed" and rank == 0:
+        mixed = {"accuracy": mixed_accuracy(ix, wl, args.workload)}
 
-    line = None
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         try:
@@ -544,7 +620,7 @@ def main() -> int:
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(steps=3, max_seconds=12.0, workload=args.workload)
+                cpu = cpu_reference_rate(prob, wl, max_seconds=20.0)
                 cpu.pop("seconds", None)
             except Exception as exc:
                 cpu = {"value": None, "error": str(exc)}
@@ -554,22 +630,22 @@ def main() -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (analytic initial data, no dataset)",
-            "config": {"workload": args.workload, "description": wl["desc"],
-                       "grid": f"{prob.nx}x{prob.ny}", "stages_per_step": wl["rks"],
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "working set ~2 GB >> 126 MB L2; no flush"},
+            "config": arm_config(args, wl, prob.nx, prob.ny, world),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clocks.summary(),
-            "accuracy": accuracy,
+            "gpu_launches": run["launches"],
+            "clocks": run["clocks"],
+            "mixed": mixed,
+            "fp64_peak": {"dfma_tflops": fp64["dfma_tflops"], "ddiv_per_s": fp64["ddiv_per_s"],
+                          "source": "imex_selftest_fp64 on this GPU, in this run"},
             "adjoint": adjoint,
             "solver": {"gmres_iters": stats["gmres_iters"], "gmres_solves": stats["gmres_solves"],
                        "newton_iters": stats["newton_iters"], "refine_sweeps": stats["refine_sweeps"],
                        "status": stats["status"],
                        "alg_bytes_per_step": step_bytes / args.steps,
-                       "stage_hbm_frac": step_bytes / (t_ms / 1e3) / 1e9 / peak},
+                       "stage_hbm_frac": step_bytes / (prof_ms / 1e3) / 1e9 / peak,
+                       "profiled_pass_ms_per_step": prof_ms / args.steps},
             "kernels": sorted(({"name": r["name"], "share": r["total_ms"] / total_prof_ms,
                                 "launches": r["launches"],
                                 "GBps": r["alg_bytes"] / (r["total_ms"] / 1e3) / 1e9 if r["total_ms"] else 0}
@@ -579,11 +655,104 @@ def main() -> int:
         if args.json_out:
             with open(args.json_out, "w") as f:
                 json.dump(line, f, indent=1)
-    solver.close()
+    if solver is not None:
+        solver.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def timed_run(ix, prob, wl: dict, precision: str, stream, steps: int, warmup: int, world: int, local: int,
+              clocks: bool) -> dict:
+    """W warm-up steps, then K steps timed with CUDA events on the solver's stream between
+    barriers and synchronisations; returns the solver and the max over ranks of the span."""
+    import torch
+    settings = dict(wl["settings"])
+    settings["precision"] = precision
+    solver = ix.Solver.for_problem(prob, wl["rks"], settings)
+    solver.set_stream(stream.cuda_stream)
+    for _ in range(warmup):
+        solver.step()
+    solver.reset_stats()
+    k0 = solver.kernel_launches()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    start.record(stream)
+    for _ in range(steps):
+        solver.step()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    barrier(world)
+    t_ms = start.elapsed_time(stop)
+    return {"solver": solver, "t_ms": t_ms, "t_max_ms": reduce_max(t_ms, world),
+            "launches": solver.kernel_launches() - k0, "clocks": sampler.summary() if sampler else None}
+
+
+def e2e_run(solver, prob, stream, steps: int, world: int, cells_per_step: int) -> dict:
+    """The metric through the public API with host buffers: every step uploads the state from
+    pinned host memory, steps, and downloads it (copies inside the timed region)."""
+    import torch
+    N = prob.nx * prob.ny
+    h_prim = torch.empty(8 * N, dtype=torch.float64, pin_memory=True)
+    h_bx = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    h_by = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    h_A = torch.empty(3 * N, dtype=torch.float64, pin_memory=True)
+    ptrs = (h_prim.data_ptr(), h_bx.data_ptr(), h_by.data_ptr(), h_A.data_ptr())
+    solver.download_state_ptr(*ptrs)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    start.record(stream)
+    for _ in range(steps):
+        solver.upload_state_ptr(*ptrs)
+        solver.step()
+        solver.download_state_ptr(*ptrs)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = reduce_max(max(start.elapsed_time(stop), wall * 1e3), world)
+    nbytes = (8 + 1 + 1 + 3) * N * 8
+    return {"value": world * cells_per_step * steps / (e2e_ms / 1e3), "unit": "cell-updates/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "path": "imex_upload_state + imex_step + imex_download_state, pinned host buffers"}
+
+
+ACCURACY_N = 64
+ACCURACY_STEPS = 20
+
+
+def mixed_accuracy(ix, wl: dict, workload: str, n: int = ACCURACY_N, steps: int = ACCURACY_STEPS) -> dict:
+    """Relative L2 error per field of the mixed form, and of the FP64 GPU path, against the FP64
+    oracle (the reference's own solver when built, else its C restatement) after `steps` time
+    steps of the same physics on an n x n grid."""
+    import numpy as np
+    from oracle.bindings import RefSolver, make_solver
+    prob = make_problem(wl["problem"], n)
+    kind = "reference" if RefSolver.available() else "port"
+    ora = make_solver("ref" if kind == "reference" else "port", prob, wl["rks"], wl["settings"])
+    for _ in range(steps):
+        ora.step()
+    want = ora.cons()
+    out = {"oracle": f"FP64 {kind} solver on the CPU", "grid": f"{n}x{n}", "steps": steps}
+    for prec in ("mixed", "fp64"):
+        sv = ix.Solver.for_problem(prob, wl["rks"], dict(wl["settings"], precision=prec))
+        for _ in range(steps):
+            sv.step()
+        got = sv.cons()
+        sv.close()
+        errs = [float(np.linalg.norm(got[k] - want[k]) / max(np.linalg.norm(want[k]), 1e-300))
+                for k in range(8)]
+        out[f"{prec}_max_rel_l2_per_field"] = max(errs)
+        out[f"{prec}_rel_l2_per_field"] = errs
+    return out
 
 
 if __name__ == "__main__":

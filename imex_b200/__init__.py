@@ -189,6 +189,7 @@ _SIGS = {
     "imex_kernel_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "imex_set_barrier_timeout": (C.c_int, [C.c_void_p, C.c_double]),
     "imex_selftest_barrier": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, _D]),
+    "imex_selftest_fp64": (C.c_int, [C.c_void_p, _D, _D]),
 }
 
 _lib = None
@@ -369,6 +370,12 @@ class Solver:
 
     def set_barrier_timeout(self, seconds: float) -> None:
         self._check(self.lib.imex_set_barrier_timeout(self.ctx, seconds))
+
+    def selftest_fp64(self) -> dict:
+        """Measured FP64 rates of this device: fused multiply-adds and divisions per second."""
+        fma, div = C.c_double(), C.c_double()
+        self._check(self.lib.imex_selftest_fp64(self.ctx, C.byref(fma), C.byref(div)))
+        return {"dfma_per_s": fma.value, "dfma_tflops": 2e-12 * fma.value, "ddiv_per_s": div.value}
 
     def selftest_barrier(self, iterations: int, phantom_blocks: int = 0, timeout_s: float = 1.0) -> float:
         """Mean microseconds per device-wide barrier (raises ImexError on a timeout)."""

@@ -83,10 +83,13 @@ def build_driver(force: bool = False) -> str:
 
 
 def build_oracles() -> None:
-    """Build oracle/liboracle.so always, oracle/_ref when the reference sources exist."""
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "port"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    """Build oracle/liboracle.so always, oracle/_ref when the reference sources exist
+    (oracle/Makefile knows where they lie; `make have-ref` says whether they are there)."""
+    oracle = os.path.join(ROOT, "oracle")
+    subprocess.run(["make", "-s", "-C", oracle, "port"], check=True)
+    if subprocess.run(["make", "-s", "-C", oracle, "have-ref"], stdout=subprocess.DEVNULL,
+                      stderr=subprocess.DEVNULL).returncode == 0:
+        subprocess.run(["make", "-s", "-C", oracle, "ref"], check=True)
 
 
 if __name__ == "__main__":

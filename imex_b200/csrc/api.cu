@@ -363,6 +363,8 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   ctx->N = (size_t)nx * ny;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
+  ctx->device = dev;
+  if (e == cudaSuccess) forget_static_scratch(dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->clock_khz, cudaDevAttrClockRate, dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
@@ -893,6 +895,10 @@ imex_status imex_selftest_barrier(imex_ctx* ctx, int iterations, int phantom_blo
   if (!ctx || iterations < 0 || phantom_blocks < 0 || !(timeout_s > 0.0) || timeout_s > 60.0) return IMEX_ERR_INVALID;
   imex_status s = run_barrier_selftest(ctx, iterations, phantom_blocks, timeout_s, us_per_barrier);
   return s != IMEX_OK ? s : device_status(ctx);
+}
+imex_status imex_selftest_fp64(imex_ctx* ctx, double* dfma_per_s, double* ddiv_per_s) {
+  if (!ctx) return IMEX_ERR_INVALID;
+  return run_fp64_selftest(ctx, dfma_per_s, ddiv_per_s);
 }
 imex_status imex_set_barrier_timeout(imex_ctx* ctx, double seconds) {
   if (!ctx || !(seconds > 0.0) || seconds > 600.0) return IMEX_ERR_INVALID;

@@ -84,8 +84,7 @@ struct ProfRec {
 
 // Grid-barrier and reduction workspace of the persistent solver kernels.
 struct SyncState {
-  unsigned int count;   // barrier arrivals since the launch started (monotonic)
-  unsigned int pad0;
+  unsigned long long count;  // barrier arrivals since the launch started (monotonic, 64-bit: never wraps)
   int abort;
   int pad1;
   long long wait_cycles;  // bound of any single barrier wait, in SM clock cycles
@@ -103,6 +102,7 @@ struct imex_ctx {
   std::string last_error;
   int num_sms = 0;
   int clock_khz = 0;  // maximum SM clock, read once at creation (bounds of device-side waits)
+  int device = -1;    // the device that was current at imex_create; all its memory lives there
 
   // device state (interior planes)
   double *prim = nullptr, *cons = nullptr, *cons_n = nullptr, *Qe = nullptr, *Qs = nullptr;
@@ -213,6 +213,7 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax);
 imex_status run_gmres(imex_ctx* ctx, int op, double* x, const double* b);
 imex_status run_nested_newton(imex_ctx* ctx, double* p, const double* b);
 imex_status set_newton_state(imex_ctx* ctx, const double* pf, double mbig);
+imex_status run_fp64_selftest(imex_ctx* ctx, double* dfma_per_s, double* ddiv_per_s);
 imex_status run_barrier_selftest(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                  double* us_per_barrier);
 
@@ -249,6 +250,7 @@ imex_status adj_apply(imex_ctx* ctx, const AdjOp& a, const double* x, double* Ax
 // fixed device scratch of imex_gmres_noalloc (noalloc.cu) and the solve that uses it
 constexpr size_t kStaticScratchBytes = IMEX_NOALLOC_SCRATCH_BYTES;
 imex_status static_scratch(imex_ctx* ctx, unsigned char** base);
+void forget_static_scratch(int dev);  // drop the cached address (imex_create)
 imex_status run_gmres_noalloc(imex_ctx* ctx, int op, double* x, const double* b, unsigned char* base,
                               size_t capacity);
 

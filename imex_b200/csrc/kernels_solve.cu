@@ -40,22 +40,24 @@ __device__ __forceinline__ double ldv(const float* p) { return (double)__ldcg(p)
 // Bounded barrier over a cooperative launch (all CTAs co-resident).  The arrival
 // counter only ever grows: barrier number g is complete once it reaches
 // (g + 1) * nblk, so the last CTA to arrive releases everyone with its own
-// arrival (no reset, no second counter).  Arrival is a release atomic and the
-// wait ends with an acquire fence, so the CTA's writes before the barrier are
-// visible to every CTA after it.  The wait polls with relaxed loads: an acquire
-// load per poll would invalidate the SM's L1 on every poll, under the feet of
-// the other CTA working on the same SM.  A wait
+// arrival (no reset, no second counter).  The counter is 64-bit, so it cannot wrap
+// within a launch (a 32-bit one would after 2^32 / nblk barriers, and the target
+// computed from a wrapped count would be wrong when nblk is not a power of two).
+// Arrival is a release atomic and the wait ends with an acquire fence, so the
+// CTA's writes before the barrier are visible to every CTA after it.  The wait
+// polls with relaxed loads: an acquire load per poll would invalidate the SM's L1
+// on every poll, under the feet of the other CTA working on the same SM.  A wait
 // longer than s->wait_cycles SM cycles sets the abort flag; every CTA then
 // returns false and the caller leaves the kernel.
-__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_relaxed_gpu(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-__device__ __forceinline__ unsigned atom_add_release_gpu(unsigned* p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long atom_add_release_gpu(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.release.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
   return old;
 }
 __device__ bool grid_barrier(SyncState* s, unsigned nblk) {
@@ -63,12 +65,12 @@ __device__ bool grid_barrier(SyncState* s, unsigned nblk) {
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    const unsigned old = atom_add_release_gpu(&s->count, 1u);
-    const unsigned target = (old / nblk + 1u) * nblk;
+    const unsigned long long old = atom_add_release_gpu(&s->count, 1ull);
+    const unsigned long long target = (old / nblk + 1ull) * nblk;
     const long long limit = s->wait_cycles;
     const long long t0 = clock64();
     for (unsigned spin = 0;; ++spin) {
-      if ((int)(ld_relaxed_gpu(&s->count) - target) >= 0) break;
+      if (ld_relaxed_gpu(&s->count) >= target) break;
       __nanosleep(32);
       if ((spin & 15u) == 15u) {
         if (*((volatile int*)&s->abort)) {
@@ -1964,9 +1966,12 @@ GmresWork make_work(imex_ctx* ctx, const Tiling& T, int nblk, int fam) {
   g.sync = ctx->sync;
   g.st = ctx->st;
   g.kmax = ctx->cfg.gmres_restart;
-  long long dim3x = 3 * T.N;
+  // 0 = the system's dimension, as the reference's outmax = dim (implicit_operators.cpp:802):
+  // 3N for the magnetic systems and the adjoint's, N for the pressure and energy systems
+  const long long width = (fam == F_GMRES_MAG_B || fam == F_GMRES_MAG_A || fam == F_ADJOINT) ? 3 : 1;
+  const long long dim = width * T.N;
   g.max_restarts = ctx->cfg.gmres_max_restarts > 0 ? ctx->cfg.gmres_max_restarts
-                                                   : (int)(dim3x > 2000000000LL ? 2000000000LL : dim3x);
+                                                   : (int)(dim > 2000000000LL ? 2000000000LL : dim);
   g.nblk = nblk;
   g.tol = ctx->P.GMREStol;
   g.tol_abs = ctx->P.GMREStol;

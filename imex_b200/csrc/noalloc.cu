@@ -24,13 +24,27 @@ unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 }  // namespace
 
-// Device address of the scratch array on the current device.  The first call on a
-// device resolves it with cudaGetSymbolAddress (with that device current); later
-// calls return the cached pointer.
+// Device address of the scratch array on the context's device.  The context's device
+// must be the current one (its memory and the kernel launch live there); a mismatch is
+// refused with IMEX_ERR_INVALID rather than handing the solve another device's array.
+// The first call on a device resolves the address with cudaGetSymbolAddress (with that
+// device current) and later calls reuse it.  A cudaDeviceReset unloads the module and
+// with it the array, and every context of that device dies with it; so imex_create
+// drops the cached address of its device (forget_static_scratch), and the first call
+// through a context created after a reset resolves the address again.  Without a
+// reset the address resolved again is the same one.
 imex_status static_scratch(imex_ctx* ctx, unsigned char** base) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_check(ctx, e, "cudaGetDevice");
+  if (dev != ctx->device) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "imex_gmres_noalloc: device %d is current but the context lives on device %d; "
+             "make the context's device current first",
+             dev, ctx->device);
+    return set_error(ctx, IMEX_ERR_INVALID, msg);
+  }
   if (dev < 0 || dev >= kMaxDevices) return set_error(ctx, IMEX_ERR_UNSUPPORTED, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   if (!g_scratch_ptr[dev]) {
@@ -41,6 +55,12 @@ imex_status static_scratch(imex_ctx* ctx, unsigned char** base) {
   }
   *base = g_scratch_ptr[dev];
   return IMEX_OK;
+}
+
+void forget_static_scratch(int dev) {
+  if (dev < 0 || dev >= kMaxDevices) return;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  g_scratch_ptr[dev] = nullptr;
 }
 
 }  // namespace imex

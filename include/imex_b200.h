@@ -408,6 +408,11 @@ imex_status imex_set_barrier_timeout(imex_ctx* ctx, double seconds);
  * call must return IMEX_ERR_SYNC (a self-test of the failure path). */
 imex_status imex_selftest_barrier(imex_ctx* ctx, int iterations, int phantom_blocks, double timeout_s,
                                   double* us_per_barrier);
+/* FP64 throughput of the context's device, measured (no counterpart in the reference):
+ * fused multiply-adds per second and IEEE double divisions per second, each from a
+ * kernel of independent dependency chains over every SM with no memory traffic.  These
+ * are the denominators against which a stencil kernel is called FP64 bound. */
+imex_status imex_selftest_fp64(imex_ctx* ctx, double* dfma_per_s, double* ddiv_per_s);
 /* Minimum pressure of the current primitive state. */
 imex_status imex_min_pressure(imex_ctx* ctx, double* pmin);
 

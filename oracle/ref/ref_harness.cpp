@@ -11,6 +11,13 @@
 //   ref_step_body.inc = main.cpp:335-561  (one time step: BCs, calch/caldt,
 //                        eigenvalues, con<->prim, the IMEX stage loop
 //                        main.cpp:367-559, final con->prim)
+// and the same time step once more in three pieces, so that a caller can advance
+// the reference one IMEX stage at a time (ref_stage):
+//   ref_step_pre.inc   = main.cpp:335-366  (the part before the stage loop; its
+//                        local `Grid A_n_snapshot` becomes a reference to a grid
+//                        held here, because it must outlive the call)
+//   ref_stage_body.inc = main.cpp:368-558  (the body of the stage loop)
+//   ref_step_post.inc  = main.cpp:561      (final con->prim)
 // Every other reference .cpp except main.cpp is compiled unchanged and linked
 // in.  This file supplies what main() would: allocation, initial-data
 // injection, and read-back.  Sub-step calls inside the stage loop are wrapped
@@ -45,12 +52,14 @@ const int MAXRK = 3;
 struct State {
   bool ready = false;
   Grid *u_pri = nullptr, *u_con = nullptr, *u_con_n = nullptr, *Qe = nullptr, *Qe_pri = nullptr,
-       *Qs = nullptr, *w_xL = nullptr, *w_xR = nullptr, *w_yL = nullptr, *w_yR = nullptr, *A = nullptr;
+       *Qs = nullptr, *w_xL = nullptr, *w_xR = nullptr, *w_yL = nullptr, *w_yR = nullptr, *A = nullptr,
+       *A_n_snapshot = nullptr;
   Tensor *HsA = nullptr, *HsB = nullptr, *Hs = nullptr;
   Array *Bx_p0 = nullptr, *By_0p = nullptr, *Bx_p0_n = nullptr, *By_0p_n = nullptr, *Bx = nullptr,
         *By = nullptr, *Bz = nullptr, *Bx_p0_Qe = nullptr, *By_0p_Qe = nullptr, *Bx_p0_Qs = nullptr,
         *By_0p_Qs = nullptr, *Ae = nullptr, *Ai = nullptr;
   bool snap_on = false;
+  int next_stage = 0;  // ref_stage: the stage the next call runs (0 = a new time step)
   Snap snaps[MAXRK][NSUB];
 };
 State S;
@@ -62,7 +71,7 @@ template <class T> void del(T*& p) {
 
 void free_all() {
   del(S.u_pri); del(S.u_con); del(S.u_con_n); del(S.Qe); del(S.Qe_pri); del(S.Qs);
-  del(S.w_xL); del(S.w_xR); del(S.w_yL); del(S.w_yR); del(S.A);
+  del(S.w_xL); del(S.w_xR); del(S.w_yL); del(S.w_yR); del(S.A); del(S.A_n_snapshot);
   del(S.HsA); del(S.HsB); del(S.Hs);
   del(S.Bx_p0); del(S.By_0p); del(S.Bx_p0_n); del(S.By_0p_n); del(S.Bx); del(S.By); del(S.Bz);
   del(S.Bx_p0_Qe); del(S.By_0p_Qe); del(S.Bx_p0_Qs); del(S.By_0p_Qs); del(S.Ae); del(S.Ai);
@@ -129,35 +138,39 @@ void set_tableau() {
   (void)bRK;
 }
 
+// The names main() gives the solver state, bound to the grids held here.
+#define BIND_STATE \
+  Grid& u_pri = *S.u_pri; \
+  Grid& u_con = *S.u_con; \
+  Grid& u_con_n = *S.u_con_n; \
+  Grid& Qe = *S.Qe; \
+  Grid& Qe_pri = *S.Qe_pri; \
+  Grid& Qs = *S.Qs; \
+  Grid& w_xL = *S.w_xL; \
+  Grid& w_xR = *S.w_xR; \
+  Grid& w_yL = *S.w_yL; \
+  Grid& w_yR = *S.w_yR; \
+  Grid& A = *S.A; \
+  Tensor& HsA = *S.HsA; \
+  Tensor& HsB = *S.HsB; \
+  Tensor& Hs = *S.Hs; \
+  Array& Bx_p0 = *S.Bx_p0; \
+  Array& By_0p = *S.By_0p; \
+  Array& Bx_p0_n = *S.Bx_p0_n; \
+  Array& By_0p_n = *S.By_0p_n; \
+  Array& Bx = *S.Bx; \
+  Array& By = *S.By; \
+  Array& Bz = *S.Bz; \
+  Array& Bx_p0_Qe = *S.Bx_p0_Qe; \
+  Array& By_0p_Qe = *S.By_0p_Qe; \
+  Array& Bx_p0_Qs = *S.Bx_p0_Qs; \
+  Array& By_0p_Qs = *S.By_0p_Qs; \
+  Array& Ae = *S.Ae; \
+  Array& Ai = *S.Ai;
+
 // One time step of the reference driver, main.cpp:335-561, with sub-step hooks.
 void run_step_body() {
-  Grid& u_pri = *S.u_pri;
-  Grid& u_con = *S.u_con;
-  Grid& u_con_n = *S.u_con_n;
-  Grid& Qe = *S.Qe;
-  Grid& Qe_pri = *S.Qe_pri;
-  Grid& Qs = *S.Qs;
-  Grid& w_xL = *S.w_xL;
-  Grid& w_xR = *S.w_xR;
-  Grid& w_yL = *S.w_yL;
-  Grid& w_yR = *S.w_yR;
-  Grid& A = *S.A;
-  Tensor& HsA = *S.HsA;
-  Tensor& HsB = *S.HsB;
-  Tensor& Hs = *S.Hs;
-  Array& Bx_p0 = *S.Bx_p0;
-  Array& By_0p = *S.By_0p;
-  Array& Bx_p0_n = *S.Bx_p0_n;
-  Array& By_0p_n = *S.By_0p_n;
-  Array& Bx = *S.Bx;
-  Array& By = *S.By;
-  Array& Bz = *S.Bz;
-  Array& Bx_p0_Qe = *S.Bx_p0_Qe;
-  Array& By_0p_Qe = *S.By_0p_Qe;
-  Array& Bx_p0_Qs = *S.Bx_p0_Qs;
-  Array& By_0p_Qs = *S.By_0p_Qs;
-  Array& Ae = *S.Ae;
-  Array& Ai = *S.Ai;
+  BIND_STATE
   bool isFinalTime = false;
 
 #define HOOK_(sub) snapshot(sub, rks, u_con, Qe, Qs, Bx_p0, By_0p, Bx_p0_Qs, By_0p_Qs, A, A_s)
@@ -186,6 +199,35 @@ void run_step_body() {
 #undef Unstaggered_CT_Consistent
 #undef HOOK_
   (void)isFinalTime;
+}
+
+// The same time step in three pieces (ref_stage): before the stage loop, one
+// pass of the stage loop's body for stage `rks`, and after the loop.  Run in
+// order pre, stage 0 .. RKs-1, post, they execute the statements of
+// run_step_body() in the same order on the same state (no snapshots).
+void run_step_pre() {
+  BIND_STATE
+  bool isFinalTime = false;
+#include "ref_step_pre.inc"
+  (void)isFinalTime;
+  (void)Qe; (void)Qe_pri; (void)Qs; (void)w_xL; (void)w_xR; (void)w_yL; (void)w_yR;
+  (void)HsA; (void)HsB; (void)Hs; (void)Bx; (void)By; (void)Bz; (void)Bx_p0_Qe; (void)By_0p_Qe;
+  (void)Bx_p0_Qs; (void)By_0p_Qs; (void)Ae; (void)Ai;
+}
+
+void run_stage_body(int rks) {
+  BIND_STATE
+  Grid& A_n_snapshot = *S.A_n_snapshot;
+  bool isFinalTime = false;
+#include "ref_stage_body.inc"
+  (void)isFinalTime;
+  (void)Bx_p0_n; (void)By_0p_n;
+}
+
+void run_step_post() {
+  Grid& u_pri = *S.u_pri;
+  Grid& u_con = *S.u_con;
+#include "ref_step_post.inc"
 }
 
 }  // namespace
@@ -254,7 +296,7 @@ int ref_setup(int nx, int ny, int rk, const ref_params* p) {
   S.u_pri = new Grid(nx, ny); S.u_con = new Grid(nx, ny); S.u_con_n = new Grid(nx, ny);
   S.Qe = new Grid(nx, ny); S.Qe_pri = new Grid(nx, ny); S.Qs = new Grid(nx, ny);
   S.w_xL = new Grid(nx, ny); S.w_xR = new Grid(nx, ny); S.w_yL = new Grid(nx, ny);
-  S.w_yR = new Grid(nx, ny); S.A = new Grid(nx, ny);
+  S.w_yR = new Grid(nx, ny); S.A = new Grid(nx, ny); S.A_n_snapshot = new Grid(nx, ny);
   S.HsA = new Tensor(RKs, nx, ny); S.HsB = new Tensor(RKs, nx, ny); S.Hs = new Tensor(RKs, nx, ny);
   S.Bx_p0 = new Array(nx, ny); S.By_0p = new Array(nx, ny); S.Bx_p0_n = new Array(nx, ny);
   S.By_0p_n = new Array(nx, ny); S.Bx = new Array(nx, ny); S.By = new Array(nx, ny);
@@ -263,7 +305,8 @@ int ref_setup(int nx, int ny, int rk, const ref_params* p) {
   S.Ae = new Array(RKs, RKs); S.Ai = new Array(RKs, RKs);
   gFluxBy_p0 = new Array(nx, ny);
   gFluxBx_0p = new Array(nx, ny);
-  for (Grid* g : {S.u_pri, S.u_con, S.u_con_n, S.Qe, S.Qe_pri, S.Qs, S.w_xL, S.w_xR, S.w_yL, S.w_yR, S.A})
+  for (Grid* g : {S.u_pri, S.u_con, S.u_con_n, S.Qe, S.Qe_pri, S.Qs, S.w_xL, S.w_xR, S.w_yL, S.w_yR, S.A,
+                  S.A_n_snapshot})
     zero_grid(*g);
   for (Array* a : {S.Bx_p0, S.By_0p, S.Bx_p0_n, S.By_0p_n, S.Bx, S.By, S.Bz, S.Bx_p0_Qe, S.By_0p_Qe,
                    S.Bx_p0_Qs, S.By_0p_Qs, gFluxBy_p0, gFluxBx_0p})
@@ -271,6 +314,7 @@ int ref_setup(int nx, int ny, int rk, const ref_params* p) {
   set_tableau();
   for (auto& row : S.snaps)
     for (auto& s : row) s.valid = false;
+  S.next_stage = 0;
   S.ready = true;
   return 0;
 }
@@ -292,17 +336,36 @@ int ref_load_prim(const double* prim, const double* bx_face, const double* by_fa
   bound_cond_A(*S.A);
   t = 0;
   timestep = 0;
+  S.next_stage = 0;
   return 0;
 }
 
 // One reference time step (main.cpp:335-561).  Returns the dt it used.
 double ref_step(int snapshots) {
-  if (!S.ready) return -1.0;
+  if (!S.ready || S.next_stage != 0) return -1.0;
   S.snap_on = snapshots != 0;
   for (auto& row : S.snaps)
     for (auto& s : row) s.valid = false;
   run_step_body();
   return dt;
+}
+
+// One IMEX stage of the reference time step: the first call of a time step also
+// runs the part before the stage loop (BCs, dt, GLF maxima, con<->prim), the last
+// also the final con->prim.  Returns the stage index it ran, or -1 if not set up.
+// RKs calls in a row give the same state as one ref_step(0).
+int ref_stage(void) {
+  if (!S.ready) return -1;
+  const int r = S.next_stage;
+  if (r == 0) run_step_pre();
+  run_stage_body(r);
+  if (r + 1 == RKs) {
+    run_step_post();
+    S.next_stage = 0;
+  } else {
+    S.next_stage = r + 1;
+  }
+  return r;
 }
 
 void ref_get_cons(double* cons8) { grid_to_planes(*S.u_con, cons8, NUM_VARS); }

@@ -49,3 +49,36 @@ def test_workloads_and_peaks():
     assert bench.WORKLOADS["vortex_sheet_1024"]["rks"] == 3
     peak, kind = bench.measured_peaks()
     assert peak > 1000 and kind in ("measured", "fallback")
+
+
+def test_reference_arm_config_matches_the_imex_arm():
+    """Both arms print the same `config` object for the same workload and grid."""
+    import argparse
+    args = argparse.Namespace(workload="vortex_sheet_1024", precision="fp64")
+    wl = bench.WORKLOADS["vortex_sheet_1024"]
+    a = bench.arm_config(args, wl, 1024, 1024, 1)
+    assert a["grid"] == "1024x1024" and a["workload"] == "vortex_sheet_1024"
+    assert a == bench.arm_config(args, wl, 1024, 1024, 1)
+    info = bench.host_info()
+    assert info["nproc"] >= 1 and info["usable_cores"] >= 1
+
+
+def test_reference_stage_stepping_matches_whole_steps():
+    """The reference arm advances the reference one IMEX stage at a time (ref_stage); RKs
+    stages in a row leave exactly the state of one whole reference time step."""
+    import numpy as np
+    from oracle.bindings import RefSolver, make_solver
+    if not RefSolver.available():
+        pytest.skip("oracle/_ref not built")
+    wl = bench.WORKLOADS["vortex_sheet_1024"]
+    prob = bench.make_problem(wl["problem"], 16)
+    whole = make_solver("ref", prob, wl["rks"], wl["settings"])
+    staged = bench._RefStages(prob, wl)
+    assert staged.kind == "reference" and staged.unit_stages == 1
+    for _ in range(2):
+        whole.step()
+        for _ in range(wl["rks"]):
+            staged.advance()
+    assert np.array_equal(whole.cons(), staged.solver.cons())
+    assert np.array_equal(whole.vector_potential(), staged.solver.vector_potential())
+    assert whole.scalars() == staged.solver.scalars()
