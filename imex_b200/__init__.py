@@ -31,11 +31,12 @@ UUPDATE = {"ConservationofU": 0, "DefinitionofU": 1}
 PSOLVER = {"no_correction": 0, "once_correction": 1, "all_correction": 2}
 EOS = {"IDEAL_GAS": 0, "REDLICH_KWONG": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
+ARITH = {"exact": 0, "fast": 1}
 XBC = {"x_Transmissive": 0, "x_Reflective": 1, "x_Periodic": 2, "x_Dirichlet": 3}
 YBC = {"y_Transmissive": 0, "y_Reflective": 1, "y_Periodic": 2, "y_Dirichlet": 3, "y_JetInflow": 4}
 ENUMS = dict(formula=FORMULA, magfield=MAGFIELD, recon=RECON, reconstate=RECONSTATE,
              caltimestep=DTCALC, add_pvisc=PVISC, U_update=UUPDATE, PressureSolver=PSOLVER,
-             eos_type=EOS, precision=PRECISION, x_bc=XBC, y_bc=YBC)
+             eos_type=EOS, precision=PRECISION, x_bc=XBC, y_bc=YBC, arith=ARITH)
 
 OP = {"pressure_L": 0, "pressure_J": 1, "magnetic_B": 2, "magnetic_A": 3, "energy": 4}
 BUF = {"cons": 0, "prim": 1, "cons_n": 2, "Qe": 3, "Qs": 4, "bx": 5, "by": 6, "bxQs": 7,
@@ -71,7 +72,8 @@ class Config(C.Structure):
         ("x_0", C.c_double), ("x_1", C.c_double), ("y_0", C.c_double), ("y_1", C.c_double),
         ("time_stop", C.c_double), ("fixed_dt", C.c_double), ("gmres_restart", C.c_int),
         ("gmres_max_restarts", C.c_int), ("precision", C.c_int), ("mixed_inner_tol", C.c_double),
-        ("mixed_max_refine", C.c_int), ("mixed_solves", C.c_int),
+        ("mixed_max_refine", C.c_int), ("mixed_solves", C.c_int), ("mixed_outer_tol", C.c_double),
+        ("arith", C.c_int),
     ]
 
 

@@ -1165,6 +1165,7 @@ imex_status supported(imex_ctx* ctx) {
   else if (P.add_pvisc == IMEX_AlfvenSpeedp) why = "MaterialSpeedp or Noaddvisp pressure viscosity";
   else if (!(P.fixed_dt > 0.0)) why = "a fixed time step (fixed_dt > 0)";
   else if (P.Energy_Modify) why = "Energy_Modify off";
+  else if (P.U_update != IMEX_DefinitionofU) why = "DefinitionofU";
   else if (ctx->cfg.precision != IMEX_PRECISION_FP64) why = "FP64 precision";
   else if (P.xclamp || P.yclamp) why = "periodic boundaries";
   if (!why) return IMEX_OK;

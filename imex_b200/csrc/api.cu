@@ -86,8 +86,10 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
     return why = "only periodic and transmissive boundaries are implemented", IMEX_ERR_UNSUPPORTED;
   if (c->formula != IMEX_PressureFormula && c->formula != IMEX_EnergyFormula) return why = "bad formula", IMEX_ERR_INVALID;
   if (!c->GLF) return why = "only the global Lax-Friedrichs dissipation (GLF) is implemented", IMEX_ERR_UNSUPPORTED;
-  if (c->U_update != IMEX_DefinitionofU) return why = "only DefinitionofU is implemented", IMEX_ERR_UNSUPPORTED;
+  if (c->U_update != IMEX_DefinitionofU && c->U_update != IMEX_ConservationofU)
+    return why = "U_update must be DefinitionofU or ConservationofU", IMEX_ERR_INVALID;
   if (c->recon < IMEX_NoRecon || c->recon > IMEX_WENO5) return why = "bad recon", IMEX_ERR_INVALID;
+  if (c->arith != IMEX_ARITH_EXACT && c->arith != IMEX_ARITH_FAST) return why = "bad arith", IMEX_ERR_INVALID;
   if (c->magfield < IMEX_StaggerCT || c->magfield > IMEX_NoDivFree) return why = "bad magfield", IMEX_ERR_INVALID;
   if (c->gmres_restart < 1 || c->gmres_restart > 30) return why = "gmres_restart must be in 1..30", IMEX_ERR_INVALID;
   if (c->precision != IMEX_PRECISION_FP64 && c->precision != IMEX_PRECISION_MIXED)
@@ -96,6 +98,8 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
     if (!(c->mixed_inner_tol > 0.0 && c->mixed_inner_tol < 1.0))
       return why = "mixed_inner_tol must be in (0, 1)", IMEX_ERR_INVALID;
     if (c->mixed_max_refine < 1) return why = "mixed_max_refine must be at least 1", IMEX_ERR_INVALID;
+    if (!(c->mixed_outer_tol >= 0.0 && c->mixed_outer_tol < 1.0))
+      return why = "mixed_outer_tol must be in [0, 1)", IMEX_ERR_INVALID;
     if (c->mixed_solves & ~(IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC))
       return why = "bad mixed_solves", IMEX_ERR_INVALID;
   }
@@ -344,6 +348,8 @@ void imex_config_default(imex_config* c) {
   c->mixed_inner_tol = 1e-6;
   c->mixed_max_refine = 50;
   c->mixed_solves = IMEX_MIXED_PRESSURE;
+  c->mixed_outer_tol = 1e-10;
+  c->arith = IMEX_ARITH_FAST;
 }
 
 imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) {
@@ -390,6 +396,7 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   P.add_bvisc = cfg->add_bvisc;
   P.add_pvisc = cfg->add_pvisc;
   P.U_update = cfg->U_update;
+  P.fast = cfg->arith == IMEX_ARITH_FAST;
   P.PressureSolver = cfg->PressureSolver;
   P.Energy_Modify = cfg->Energy_Modify;
   P.floor_on = cfg->floor_on;

@@ -161,6 +161,32 @@ __device__ __forceinline__ void energy_define_cell(const DevParams& P, const lon
   out[0] = Vbase(P, ld(ED_P, 0, n), r) + 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / r + 0.5 * (b5 * b5 + b6 * b6 + b7 * b7);
 }
 
+// ---- E -= h div(h_e rho v) (ConservationofU, imex_subsystems.cpp:303-392): the energy is
+// advanced by the central flux of the specific enthalpy h = e(rho, p) + p / rho carried by
+// the corrected momentum, with p the pressure the solve returned (ghosts by index map)
+enum { EC_P = 0, EC_UCON = 1 };
+template <class S, class Ld>
+__device__ __forceinline__ void energy_conservation_cell(const DevParams& P, double h, const long long* nb, Ld& ld,
+                                                         S* out) {
+  const long long n = nb[NB_C], E = nb[NB_E], W = nb[NB_W], No = nb[NB_N], S_ = nb[NB_S];
+  const S p00 = ld(EC_P, 0, n), pp0 = ld(EC_P, 0, E), pm0 = ld(EC_P, 0, W), p0p = ld(EC_P, 0, No), p0m = ld(EC_P, 0, S_);
+  const S r00 = ld(EC_UCON, 0, n), rp0 = ld(EC_UCON, 0, E), rm0 = ld(EC_UCON, 0, W);
+  const S r0p = ld(EC_UCON, 0, No), r0m = ld(EC_UCON, 0, S_);
+  const S mx00 = ld(EC_UCON, 1, n), mxp0 = ld(EC_UCON, 1, E), mxm0 = ld(EC_UCON, 1, W);
+  const S my00 = ld(EC_UCON, 2, n), my0p = ld(EC_UCON, 2, No), my0m = ld(EC_UCON, 2, S_);
+  const S E00 = ld(EC_UCON, 4, n);
+  const S h_00 = eos_e(P, r00, p00) + p00 / r00;
+  const S h_p0 = eos_e(P, rp0, pp0) + pp0 / rp0;
+  const S h_m0 = eos_e(P, rm0, pm0) + pm0 / rm0;
+  const S h_0p = eos_e(P, r0p, p0p) + p0p / r0p;
+  const S h_0m = eos_e(P, r0m, p0m) + p0m / r0m;
+  const S flux_xm = 0.5 * (h_m0 * mxm0 + h_00 * mx00);
+  const S flux_xp = 0.5 * (h_00 * mx00 + h_p0 * mxp0);
+  const S flux_ym = 0.5 * (h_0m * my0m + h_00 * my00);
+  const S flux_yp = 0.5 * (h_00 * my00 + h_0p * my0p);
+  out[0] = E00 - h / (P.dx) * (flux_xp - flux_xm) - h / (P.dy) * (flux_yp - flux_ym);
+}
+
 // ---- corner EMF: CT_CornerAssemble (constrained_transport.cpp:147-164) of the face EMFs
 // ep0 = sx fx, e0p = sy fy and the cell EMF vy Bx - vx By of u_con (ct_flux.cpp:165-168)
 enum { CC_FX = 0, CC_FY = 1, CC_UCON = 2 };

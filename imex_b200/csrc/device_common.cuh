@@ -252,9 +252,53 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ a, long lon
 // ---------------------------------------------------------------- reconstruction
 // One variable along one direction from the 5-point stencil (um2 .. up2):
 // left and right face values of the cell, reconstruction.cpp:38-266.
+// kFast (imex_config.arith = fast): WENO5 forms its normalised weights with one division per
+// face (w_k / sum w = d_k P_k / sum_i d_i P_i, P_k the product of the other two smoothness
+// terms) and its polynomials with fused multiply-adds; VanLeer takes 1 / (1 + r) once.
 template <class S>
+__device__ inline void weno5_fast(S um2, S um1, S u0, S up1, S up2, S& wL, S& wR) {
+  const S a0 = um2 - 2 * um1 + u0, b0 = fma(S(3), u0, um2 - 4 * um1);
+  const S a1 = um1 - 2 * u0 + up1, b1 = um1 - up1;
+  const S a2 = u0 - 2 * up1 + up2, b2 = fma(S(3), u0, up2 - 4 * up1);
+  const S e0 = fma(13.0 / 12.0 * a0, a0, fma(0.25 * b0, b0, S(1e-6)));
+  const S e1 = fma(13.0 / 12.0 * a1, a1, fma(0.25 * b1, b1, S(1e-6)));
+  const S e2 = fma(13.0 / 12.0 * a2, a2, fma(0.25 * b2, b2, S(1e-6)));
+  const S s0 = e0 * e0, s1 = e1 * e1, s2 = e2 * e2;
+  const S t0 = s1 * s2, t1 = s0 * s2, t2 = s0 * s1;
+  {
+    const S q0 = fma(-1.0 / 6.0, um2, fma(5.0 / 6.0, um1, 1.0 / 3.0 * u0));
+    const S q1 = fma(1.0 / 3.0, um1, fma(5.0 / 6.0, u0, -1.0 / 6.0 * up1));
+    const S q2 = fma(11.0 / 6.0, u0, fma(-7.0 / 6.0, up1, 1.0 / 3.0 * up2));
+    const S a = 0.3 * t0, b = 0.6 * t1, c = 0.1 * t2;
+    wL = fma(a, q0, fma(b, q1, c * q2)) / (a + b + c);
+  }
+  {
+    const S q0 = fma(1.0 / 3.0, um2, fma(-7.0 / 6.0, um1, 11.0 / 6.0 * u0));
+    const S q1 = fma(-1.0 / 6.0, um1, fma(5.0 / 6.0, u0, 1.0 / 3.0 * up1));
+    const S q2 = fma(1.0 / 3.0, u0, fma(5.0 / 6.0, up1, -1.0 / 6.0 * up2));
+    const S a = 0.1 * t0, b = 0.6 * t1, c = 0.3 * t2;
+    wR = fma(a, q0, fma(b, q1, c * q2)) / (a + b + c);
+  }
+}
+template <bool kFast = false, class S>
 __device__ inline void recon_1d(int scheme, S um2, S um1, S u0, S up1, S up2, S& wL, S& wR, bool vortex_central) {
   S sR = up1 - u0, sL = u0 - um1, c = 0.0;
+  if constexpr (kFast) {
+    if (scheme == IMEX_WENO5) {
+      weno5_fast(um2, um1, u0, up1, up2, wL, wR);
+      return;
+    }
+    if (scheme == IMEX_VanLeer) {
+      if (fabs(sR) < 1e-16) c = 0;
+      else {
+        const S r = sL / sR;
+        c = (r < 0) ? S(0.0) : 2 * fmin(S(1), r) / (1 + r);
+      }
+      wL = fma(-0.5 * c, sL, u0);
+      wR = fma(0.5 * c, sR, u0);
+      return;
+    }
+  }
   switch (scheme) {
     case IMEX_NoRecon:
       wL = u0;
@@ -324,6 +368,30 @@ __device__ inline void recon_1d(int scheme, S um2, S um1, S u0, S up1, S up2, S&
 }
 
 // ---------------------------------------------------------------- explicit fluxes
+// The fast forms (kFast) take 1 / rho once where the reference divides by rho per term.
+template <class S>
+__device__ __forceinline__ void f_conv_fast(const S* c, int dir, S ir, S* f) {
+  const S vx = c[1] * ir, vy = c[2] * ir, vz = c[3] * ir;
+  const S k = 0.5 * c[0] * fma(vx, vx, fma(vy, vy, vz * vz));
+  const S vn = dir == 0 ? vx : vy;
+  const S mn = c[0] * vn;
+  f[0] = mn;
+  f[1] = mn * vx;
+  f[2] = mn * vy;
+  f[3] = mn * vz;
+  f[4] = k * vn;
+}
+template <class S>
+__device__ __forceinline__ void magflux_p_fast(const S* Q, int dir, S ir, S* f) {
+  const S B2 = fma(Q[5], Q[5], fma(Q[6], Q[6], Q[7] * Q[7]));
+  const S vB = fma(Q[1], Q[5], fma(Q[2], Q[6], Q[3] * Q[7])) * ir;
+  const S Bn = dir == 0 ? Q[5] : Q[6];
+  f[0] = 0;
+  f[1] = dir == 0 ? fma(B2, S(0.5), -Q[5] * Q[5]) : -Q[5] * Q[6];
+  f[2] = dir == 0 ? -Q[5] * Q[6] : fma(B2, S(0.5), -Q[6] * Q[6]);
+  f[3] = -Bn * Q[7];
+  f[4] = fma(Q[1 + dir] * ir, B2, -Bn * vB);
+}
 // convective flux along dir (0 = x, 1 = y), state.cpp:27-44 / 86-106
 template <class S>
 __device__ __forceinline__ void f_conv(const S* c, int dir, S* f) {
@@ -386,9 +454,31 @@ __device__ __forceinline__ S caltotalenthalpy(const DevParams& P, const S* c) {
 }
 // Rusanov face flux of RusanovC_x/y (flux.cpp:329-406), Pressure_flux_x/y (flux.cpp:202-287)
 // or Energy_flux_x/y (flux.cpp:78-200): kForm 0, 1, 2
-template <int kForm, class S>
+template <int kForm, bool kFast = false, class S>
 __device__ __forceinline__ void face_flux(const DevParams& P, const S* QL, const S* QR, int dir, S a_max, S* F) {
   S fL[5], fR[5];
+  if constexpr (kFast && kForm != 2) {
+    const S irL = 1 / QL[0], irR = 1 / QR[0];
+    f_conv_fast(QL, dir, irL, fL);
+    f_conv_fast(QR, dir, irR, fR);
+    if (kForm == 1) {
+      S fb[5];
+      magflux_p_fast(QL, dir, irL, fb);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) fL[k] = fL[k] + fb[k];
+      magflux_p_fast(QR, dir, irR, fb);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) fR[k] = fR[k] + fb[k];
+    } else if (P.formula == IMEX_EnergyFormula) {
+      fL[4] = 0;
+      fR[4] = 0;
+    }
+    const S s = P.GLF ? a_max : fmax(fabs(QL[1 + dir] * irL), fabs(QR[1 + dir] * irR));
+    const S hs = 0.5 * s;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[k] = fma(S(0.5), fL[k] + fR[k], -hs * (QR[k] - QL[k]));
+    return;
+  }
   f_conv(QL, dir, fL);
   f_conv(QR, dir, fR);
   if (kForm == 2) {  // convective (energy zeroed) + magnetic + kinetic-energy fluxes

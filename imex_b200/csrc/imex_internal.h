@@ -31,6 +31,7 @@ struct DevParams {
   // the index map as one multiply-add per side: i < 0 -> i * xm + xlo, i >= nx -> i * xm + xhi
   // (periodic: xm = 1, xlo = nx, xhi = -nx; transmissive: xm = 0, xlo = 0, xhi = nx - 1)
   int xm, xlo, xhi, ym, ylo, yhi;
+  int fast;  // imex_config.arith == IMEX_ARITH_FAST (explicit stencil kernels)
 };
 
 // Boundary normal faces of the transmissive directions.  The reference keeps Bx_p0 at
@@ -159,6 +160,15 @@ struct imex_ctx {
   do {                                                                             \
     if ((P).xclamp || (P).yclamp) kern<true><<<grid, block, smem, stream>>>(__VA_ARGS__); \
     else kern<false><<<grid, block, smem, stream>>>(__VA_ARGS__);                  \
+  } while (0)
+// the same over the boundary kind and the arithmetic of the explicit stencils (kern<kOpen, kFast>)
+#define IMEX_LAUNCH_BC_ARITH(P, kern, grid, block, smem, stream, ...)                              \
+  do {                                                                                             \
+    const bool open_ = (P).xclamp || (P).yclamp;                                                   \
+    if (open_ && (P).fast) kern<true, true><<<grid, block, smem, stream>>>(__VA_ARGS__);            \
+    else if (open_) kern<true, false><<<grid, block, smem, stream>>>(__VA_ARGS__);                 \
+    else if ((P).fast) kern<false, true><<<grid, block, smem, stream>>>(__VA_ARGS__);              \
+    else kern<false, false><<<grid, block, smem, stream>>>(__VA_ARGS__);                           \
   } while (0)
 
 namespace imex {

@@ -1699,6 +1699,23 @@ __global__ void k_energy_define(DevParams P, const double* __restrict__ p, doubl
   ucon[4 * N + n] = out[0];
 }
 
+// E -= h div(h_e rho v) (ConservationofU, imex_subsystems.cpp:303-392).  Reads only the
+// density and momentum planes of the neighbours, so E is updated in place.
+__global__ void k_energy_conservation(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
+                                      double* __restrict__ ucon) {
+  const long long N = P.N;
+  const double h = sc->h;
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  long long nb[9];
+  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  const double* arr[2] = {p, ucon};
+  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+  double out[1];
+  energy_conservation_cell<double>(P, h, nb, ld, out);
+  ucon[4 * N + n] = out[0];
+}
+
 // total-enthalpy ratio hh = caltotalenthalpy(Qe) rho_e / rho (imex_subsystems.cpp:442-446)
 __global__ void k_energy_coeffs(DevParams P, const double* __restrict__ Qe, const double* __restrict__ ucon,
                                 double* __restrict__ hh) {
@@ -2002,6 +2019,10 @@ GmresWorkT<float> make_work_mixed(imex_ctx* ctx, const Tiling& T, int nblk, int 
 bool mixed(const imex_ctx* ctx, int kind) {
   return ctx->cfg.precision == IMEX_PRECISION_MIXED && (ctx->cfg.mixed_solves & kind) != 0;
 }
+// tolerance of the FP64 refinement of a mixed solve: mixed_outer_tol, or GMREStol when that is 0
+double mixed_outer_tol(const imex_ctx* ctx) {
+  return ctx->cfg.mixed_outer_tol > 0.0 ? ctx->cfg.mixed_outer_tol : ctx->P.GMREStol;
+}
 
 }  // namespace
 __global__ void k_reset_sync(SyncState* s, long long limit) {
@@ -2139,7 +2160,7 @@ imex_status gmres_run(imex_ctx* ctx, const Op& o, int fam, double* x, const doub
   GmresWorkT<float> g = make_work_mixed(ctx, T, nb, fam, 1, 0.0);
   prof_begin(ctx);
   imex_status s = launch_coop_smem(ctx, kern, nb, smem, o, g, x, ctx->mcor, ctx->mres, b, ctx->cfg.mixed_max_refine,
-                                   ctx->P.GMREStol);
+                                   mixed_outer_tol(ctx));
   prof_end(ctx, fam, 0.0, 1);
   return s;
 }
@@ -2384,7 +2405,7 @@ imex_status add_gmres_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>&
                                     j.xalt = m->mcor;
                                     j.sres = m->mres;
                                     j.max_sweeps = m->cfg.mixed_max_refine;
-                                    j.tol = m->P.GMREStol;
+                                    j.tol = mixed_outer_tol(m);
                                     return j;
                                   });
 }
@@ -2608,6 +2629,12 @@ imex_status pres_part3(imex_ctx* ctx) {
   if (P.formula == IMEX_EnergyFormula) return IMEX_OK;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
+  if (P.U_update == IMEX_ConservationofU) {
+    k_energy_conservation<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->cons);
+    LAUNCH_CHECK(ctx, "k_energy_conservation");
+    prof_end(ctx, F_ENERGY, BYTES(6), 1);  // p, rho, rho vx, rho vy, E in; E out
+    return IMEX_OK;
+  }
   k_energy_define<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->pp, ctx->cons);
   LAUNCH_CHECK(ctx, "k_energy_define");
   prof_end(ctx, F_ENERGY, BYTES(9), 1);

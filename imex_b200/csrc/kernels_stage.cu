@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kThreads) k_stage_combine(DevParams P, Tableau
 // TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes,
 // PrimState (the ConsState form is k_reconstruct_var below).
 // nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
-template <bool kOpen>
+template <bool kOpen, bool kFast>
 __global__ void k_reconstruct_prim(DevParams Pin, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
   const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
@@ -298,8 +298,8 @@ __global__ void k_reconstruct_prim(DevParams Pin, const double* __restrict__ Q, 
   double wxl[8], wxr[8], wyl[8], wyr[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    recon_1d(P.recon, px[0][k], px[1][k], px[2][k], px[3][k], px[4][k], wxl[k], wxr[k], false);
-    recon_1d(P.recon, py[0][k], py[1][k], py[2][k], py[3][k], py[4][k], wyl[k], wyr[k], vortex);
+    recon_1d<kFast>(P.recon, px[0][k], px[1][k], px[2][k], px[3][k], px[4][k], wxl[k], wxr[k], false);
+    recon_1d<kFast>(P.recon, py[0][k], py[1][k], py[2][k], py[3][k], py[4][k], wyl[k], wyr[k], vortex);
   }
   double c[8];
   double* outs[4] = {wxl, wxr, wyl, wyr};
@@ -313,7 +313,7 @@ __global__ void k_reconstruct_prim(DevParams Pin, const double* __restrict__ Q, 
 // ConsState reconstructs every conserved variable on its own (reconstruction.cpp:5-266), so
 // one thread per (cell, variable) pair: variable k = blockIdx.y.  The same recon_1d calls as a
 // per-cell loop over the variables, with a small per-thread working set and 5-8x the threads.
-template <bool kOpen>
+template <bool kOpen, bool kFast>
 __global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, const double* __restrict__ Q,
                                                                double* __restrict__ w) {
   const DevParams P = bc_params<kOpen>(Pin);
@@ -330,8 +330,8 @@ __global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, con
 #pragma unroll
   for (int d = 0; d < 5; ++d) u[d] = __ldg(a + cid(P, i, j + d - 2));
   double xl, xr, yl, yr;
-  recon_1d(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
-  recon_1d(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
+  recon_1d<kFast>(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
+  recon_1d<kFast>(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
   w[(0 * 8 + k) * N + n] = xl;
   w[(1 * 8 + k) * N + n] = xr;
   w[(2 * 8 + k) * N + n] = yl;
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, con
 // own), kept in shared memory, then each cell is updated with the reference's expression:
 // fp / fm are the fluxes of the faces at i +- 1/2, gp / gm those at j +- 1/2.
 constexpr int FTX = 32, FTY = 8, FNT = FTX * FTY;
-template <int kForm>
+template <int kForm, bool kFast>
 __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* __restrict__ sc,
                                           const double* __restrict__ w, const double* __restrict__ Qs,
                                           double* __restrict__ ucon) {
@@ -379,7 +379,7 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* 
       const int j = y0 + ly;
       state(wxR, cid(P, x0 + fi - 1, j), QL);
       state(wxL, cid(P, x0 + fi, j), QR);
-      face_flux<kForm>(P, QL, QR, 0, a_max, F);
+      face_flux<kForm, kFast>(P, QL, QR, 0, a_max, F);
 #pragma unroll
       for (int k = 0; k < 5; ++k) fx[k][ly][fi] = F[k];
     } else {
@@ -388,7 +388,7 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* 
       const int i = x0 + lx;
       state(wyR, cid(P, i, y0 + fj - 1), QL);
       state(wyL, cid(P, i, y0 + fj), QR);
-      face_flux<kForm>(P, QL, QR, 1, a_max, F);
+      face_flux<kForm, kFast>(P, QL, QR, 1, a_max, F);
 #pragma unroll
       for (int k = 0; k < 5; ++k) fy[k][fj][lx] = F[k];
     }
@@ -404,19 +404,26 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* 
 }
 // The register budgets were measured: the convective form runs fastest as the compiler
 // chooses, the pressure and energy forms at three CTAs per SM.
-template <bool kOpen>
+template <bool kOpen, bool kFast>
 __global__ void __launch_bounds__(FNT) k_flux_conv(DevParams Pin, const DevScalars* __restrict__ sc,
                                                    const double* __restrict__ w, const double* __restrict__ Qs,
                                                    double* __restrict__ ucon) {
   const DevParams P = bc_params<kOpen>(Pin);
-  flux_tile<0>(P, sc, w, Qs, ucon);
+  flux_tile<0, kFast>(P, sc, w, Qs, ucon);
 }
-template <int kForm, bool kOpen>
+template <int kForm, bool kOpen, bool kFast>
 __global__ void __launch_bounds__(FNT, 3) k_flux_mag(DevParams Pin, const DevScalars* __restrict__ sc,
                                                      const double* __restrict__ w, const double* __restrict__ Qs,
                                                      double* __restrict__ ucon) {
   const DevParams P = bc_params<kOpen>(Pin);
-  flux_tile<kForm>(P, sc, w, Qs, ucon);
+  flux_tile<kForm, kFast>(P, sc, w, Qs, ucon);
+}
+template <bool kOpen, bool kFast>
+__global__ void __launch_bounds__(FNT, 3) k_flux_pres(DevParams Pin, const DevScalars* __restrict__ sc,
+                                                      const double* __restrict__ w, const double* __restrict__ Qs,
+                                                      double* __restrict__ ucon) {
+  const DevParams P = bc_params<kOpen>(Pin);
+  flux_tile<1, kFast>(P, sc, w, Qs, ucon);
 }
 
 // ---------------------------------------------------------------- constrained transport
@@ -969,11 +976,11 @@ imex_status launch_reconstruct(imex_ctx* ctx, bool full) {
   const int nread = ctx->P.reconstate == IMEX_PrimState ? 8 : nstore;
   prof_begin(ctx);
   if (ctx->P.reconstate == IMEX_PrimState)
-    IMEX_LAUNCH_BC(ctx->P, k_reconstruct_prim, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, ctx->P, ctx->Qe, ctx->w,
-                   nstore);
+    IMEX_LAUNCH_BC_ARITH(ctx->P, k_reconstruct_prim, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, ctx->P, ctx->Qe,
+                         ctx->w, nstore);
   else
-    IMEX_LAUNCH_BC(ctx->P, k_reconstruct_var, (dim3(blocks_for(ctx->P.N), nstore)), kThreads, 0, ctx->stream, ctx->P,
-                   ctx->Qe, ctx->w);
+    IMEX_LAUNCH_BC_ARITH(ctx->P, k_reconstruct_var, (dim3(blocks_for(ctx->P.N), nstore)), kThreads, 0, ctx->stream,
+                         ctx->P, ctx->Qe, ctx->w);
   LAUNCH_CHECK(ctx, "k_reconstruct");
   prof_end(ctx, F_RECON, BYTES(nread + 4 * nstore), 1);
   return IMEX_OK;
@@ -984,16 +991,14 @@ imex_status launch_flux_update(imex_ctx* ctx, int form) {
   const dim3 nb((ctx->nx + FTX - 1) / FTX, (ctx->ny + FTY - 1) / FTY);
   prof_begin(ctx);
   const bool open = ctx->P.xclamp || ctx->P.yclamp;
-  if (form == 1 && open)
-    k_flux_mag<1, true><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
-  else if (form == 1)
-    k_flux_mag<1, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
-  else if (form == 2 && open)
-    k_flux_mag<2, true><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  if (form == 1)
+    IMEX_LAUNCH_BC_ARITH(ctx->P, k_flux_pres, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+  else if (form == 2 && open)  // the energy formula's flux keeps the reference's operation order
+    k_flux_mag<2, true, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else if (form == 2)
-    k_flux_mag<2, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    k_flux_mag<2, false, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else
-    IMEX_LAUNCH_BC(ctx->P, k_flux_conv, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    IMEX_LAUNCH_BC_ARITH(ctx->P, k_flux_conv, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   LAUNCH_CHECK(ctx, "flux update");
   prof_end(ctx, form ? F_FLUX_PRES : F_FLUX_CONV, BYTES(form ? 33 : 30), 1);
   return IMEX_OK;
@@ -1011,8 +1016,8 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
     k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
-    if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
-    else IMEX_LAUNCH_BC(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
+    if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
+    else IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
     k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
@@ -1094,8 +1099,8 @@ imex_status launch_ct_diag(imex_ctx* ctx, double* out16) {
   const int nb = blocks_for(P.N);
   cudaStream_t s = ctx->stream;
   double *cp0 = ctx->chit, *c0p = ctx->Et, *rp0 = ctx->Epp, *r0p = ctx->vscale;
-  if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
-  else IMEX_LAUNCH_BC(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
+  if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
+  else IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
   k_ct_diag_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, cp0, c0p, rp0, r0p);
   int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
   k_ct_diag_stats<<<nred, kThreads, 0, s>>>(P, cp0, c0p, rp0, r0p, ctx->cons, ctx->partial);

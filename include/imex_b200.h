@@ -20,8 +20,11 @@
  *   - a GMRES vector of the pressure system is one plane; of the magnetic
  *     systems three planes, in the order of the reference's M_P / M_B maps
  *     (implicit_operators.cpp:5-139).
- * Ghost cells do not exist: boundaries are periodic in both directions and
- * handled by wrap-around indexing inside the kernels.
+ * Ghost cells do not exist: each direction is periodic or transmissive
+ * (imex_config.x_bc / y_bc), and the kernels read a neighbour past the edge
+ * through an index map (wrap-around for periodic, the nearest interior cell
+ * for transmissive).  The boundary normal faces of a transmissive direction
+ * are extra degrees of freedom (imex_set_boundary_faces).
  *
  * Conventions: every function returns imex_status (0 = OK).  Non-convergence
  * and non-finite values found on the device are reported through the status
@@ -76,6 +79,17 @@ typedef enum {
                                Newton keeps its FP64 residual and convergence test and solves its
                                Jacobian systems in FP32 */
 } imex_precision;
+/* Operation order of the explicit stencil kernels (reconstruction and the Rusanov face
+ * fluxes), imex_config.arith.  The exact order is the reference's, operand for operand,
+ * without fused multiply-adds, so those sub-steps match the reference bit for bit.  The
+ * fast order hoists the divisions that the reference repeats (WENO5 forms its three
+ * nonlinear weights with one division instead of six; the fluxes take 1/rho once) and
+ * fuses multiply-adds; a sub-step then differs from the reference by a few units in the
+ * last place.  The implicit solves are not affected. */
+typedef enum {
+  IMEX_ARITH_EXACT = 0,
+  IMEX_ARITH_FAST = 1
+} imex_arith;
 /* Solves of the mixed form (imex_config.mixed_solves).  The pressure solves (the nested
  * Newton's Jacobian systems, or the single linear GMRES without the floor) gain from FP32:
  * the Newton iteration is their FP64 refinement.  The magnetic systems converge in a few
@@ -125,6 +139,10 @@ typedef struct imex_config {
   double mixed_inner_tol; /* relative tolerance of each FP32 inner solve in mixed mode */
   int mixed_max_refine;   /* cap on FP64 refinement sweeps in mixed mode */
   int mixed_solves;       /* which solves take the mixed form: IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC */
+  double mixed_outer_tol; /* relative residual at which the FP64 refinement of a mixed GMRES solve stops
+                             (plus the same value absolute, as GMREStol); the plain form's GMREStol when
+                             0.  The default, 1e-10, spends part of the mixed form's 1e-8 error budget. */
+  int arith;              /* imex_arith of the explicit stencil kernels; default IMEX_ARITH_FAST */
 } imex_config;
 
 /* Scalars that the reference keeps in hidden globals and that one stage consumes

@@ -860,6 +860,23 @@ static void pre_subsystem_pressure(double* ucon, const double* Qs, const double*
       double b5 = ucon[5 * N + c], b6 = ucon[6 * N + c], b7 = ucon[7 * N + c];
       ucon[4 * N + c] = Vbase(p[c], r) + 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / r + 0.5 * (b5 * b5 + b6 * b6 + b7 * b7);
     }
+  } else {
+    /* ConservationofU, imex_subsystems.cpp:303-392: E -= h div(h_e rho v), h_e = e(rho, p) + p / rho
+       of the final pressure (ghosts as bound_cond_array) and the corrected momentum */
+    for (int i = 0; i < G.nx; i++)
+      for (int j = 0; j < G.ny; j++) {
+        size_t c = ID(i, j), e = ID(i + 1, j), w = ID(i - 1, j), n = ID(i, j + 1), s = ID(i, j - 1);
+        double h_00 = eos_e(ucon[c], p[c]) + p[c] / ucon[c];
+        double h_p0 = eos_e(ucon[e], p[e]) + p[e] / ucon[e];
+        double h_m0 = eos_e(ucon[w], p[w]) + p[w] / ucon[w];
+        double h_0p = eos_e(ucon[n], p[n]) + p[n] / ucon[n];
+        double h_0m = eos_e(ucon[s], p[s]) + p[s] / ucon[s];
+        double flux_xm = 0.5 * (h_m0 * ucon[N + w] + h_00 * ucon[N + c]);
+        double flux_xp = 0.5 * (h_00 * ucon[N + c] + h_p0 * ucon[N + e]);
+        double flux_ym = 0.5 * (h_0m * ucon[2 * N + s] + h_00 * ucon[2 * N + c]);
+        double flux_yp = 0.5 * (h_00 * ucon[2 * N + c] + h_0p * ucon[2 * N + n]);
+        ucon[4 * N + c] = ucon[4 * N + c] - h / (dx) * (flux_xp - flux_xm) - h / (dy) * (flux_yp - flux_ym);
+      }
   }
   free(rvx); free(rvy); free(rvz); free(b); free(p);
 }
@@ -1687,7 +1704,8 @@ static void free_all(void) {
 
 int ora_setup(int nx, int ny, int rks, const ora_params* p) {
   if (nx < 4 || ny < 4 || rks < 1 || rks > MAXRK) return 1;
-  if ((p->formula != PressureFormula && p->formula != EnergyFormula) || !p->GLF || p->U_update != DefinitionofU)
+  if ((p->formula != PressureFormula && p->formula != EnergyFormula) || !p->GLF ||
+      (p->U_update != DefinitionofU && p->U_update != ConservationofU))
     return 2;
   free_all();
   G.nx = nx;

@@ -69,6 +69,13 @@ STEP_CASES = {
     "blast16x12_xperiodic_open_y": (lambda: open_blast(16, 12), 2,
                                     dict(recon="VanLeer", magfield="StaggerCT", x_bc="x_Periodic",
                                          floor_on=0, PressureSolver="once_correction"), 2),
+    # ConservationofU: E advanced by the enthalpy flux of the corrected momentum (imex_subsystems.cpp:303-392)
+    "vortex16_conservationofU": (lambda: vortex(16), 2, dict(CFG0, U_update="ConservationofU"), 2),
+    "blast16_conservationofU_open": (lambda: open_blast(16), 2,
+                                     dict(recon="Minmod", magfield="StaggerCT", U_update="ConservationofU"), 2),
+    "vortex16_conservationofU_rkeos": (lambda: vortex(16), 2,
+                                       dict(recon="VanLeer", magfield="StaggerCT", U_update="ConservationofU",
+                                            eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 1),
 }
 
 

@@ -47,7 +47,7 @@ def test_gpu_substeps_match_oracle_transmissive(rks, settings):
     sc = o.scalars()
     ae, ai = o.tableau()
     exact = lambda a, b, msg: np.testing.assert_array_equal(a, b, err_msg=msg)
-    g = ix.Solver.for_problem(prob, rks, settings)
+    g = ix.Solver.for_problem(prob, rks, dict(settings, arith="exact"))
     energy = settings.get("formula") == "EnergyFormula"
     for k in range(rks):
         S = lambda sub, w: o.snapshot(k, sub, w)

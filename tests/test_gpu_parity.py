@@ -1,7 +1,10 @@
 """CUDA path vs the oracle on identical inputs, through the C ABI.
 
-Explicit sub-steps and the matrix-free operators use the reference's operand
-order and no FMA contraction, so they must be bit-identical.  Implicit solves
+With arith = "exact", the explicit sub-steps and the matrix-free operators use
+the reference's operand order and no FMA contraction, so they must be
+bit-identical.  The default arith = "fast" hoists repeated divisions and fuses
+multiply-adds in the reconstruction and the face fluxes: those sub-steps are
+held to 1e-13 relative L2 per field.  Implicit solves
 reduce dot products in a different (parallel, fixed) order than the
 reference's serial loop, so GMRES/Newton results agree to round-off of the
 solve, asserted at 1e-12 relative L2 (the per-step target of the north star
@@ -45,6 +48,22 @@ def test_gpu_steps_match_reference_golden(case):
     gpu.close()
 
 
+@pytest.mark.parametrize("scheme", ["VanLeer", "WENO5", "Minmod", "ENO3"])
+def test_gpu_fast_reconstruction_within_round_off(scheme):
+    """The fast WENO5 (one division per face for the normalised weights) and VanLeer forms
+    against the reference's output: every face state within 1e-13 relative L2 per variable."""
+    g = load_golden("fn_vortex16x12.npz")
+    sv = _fn_solver(dict(recon=scheme, magfield="StaggerCT", arith="fast"))
+    sv.set_buffer("Qe", g["Q"])
+    sv.TVDReconstruction()
+    w = sv.get_buffer("w").reshape(4, 8, 12, 16)
+    want = g[f"recon_{scheme}"]
+    for q in range(4):
+        for k in range(8):
+            assert rel(w[q, k], want[q, k]) <= 1e-13, (scheme, q, k, rel(w[q, k], want[q, k]))
+    sv.close()
+
+
 def _fn_solver(settings):
     prob = vortex(16, 12)
     s = dict(prob.settings)
@@ -55,13 +74,13 @@ def _fn_solver(settings):
 def test_gpu_reconstruction_and_shock_detector_bit_exact():
     g = load_golden("fn_vortex16x12.npz")
     for scheme in ("NoRecon", "Minmod", "VanLeer", "ENO3", "WENO5"):
-        sv = _fn_solver(dict(recon=scheme, magfield="StaggerCT"))
+        sv = _fn_solver(dict(recon=scheme, magfield="StaggerCT", arith="exact"))
         sv.set_buffer("Qe", g["Q"])
         sv.TVDReconstruction()
         np.testing.assert_array_equal(sv.get_buffer("w").reshape(4, 8, 12, 16), g[f"recon_{scheme}"],
                                       err_msg=scheme)
         sv.close()
-    sv = _fn_solver(dict(recon="Minmod", reconstate="PrimState", magfield="StaggerCT"))
+    sv = _fn_solver(dict(recon="Minmod", reconstate="PrimState", magfield="StaggerCT", arith="exact"))
     sv.set_buffer("Qe", g["Q"])
     sv.TVDReconstruction()
     np.testing.assert_array_equal(sv.get_buffer("w").reshape(4, 8, 12, 16), g["recon_Minmod_prim"])
@@ -101,21 +120,37 @@ SUB_CASES = [
                                   m_alfa=0.4275, m_b=0.0866)),
     ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula", GMREStol=1e-12)),
     ("sheet", (24, 20), 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, formula="EnergyFormula")),
+    ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", U_update="ConservationofU")),
 ]
 
 
+@pytest.mark.parametrize("arith", ["exact", "fast"])
 @pytest.mark.parametrize("kind,shape,rks,settings", SUB_CASES)
-def test_gpu_substeps_match_oracle(kind, shape, rks, settings):
-    """Each sub-step of each stage on the oracle's inputs of that sub-step."""
+def test_gpu_substeps_match_oracle(kind, shape, rks, settings, arith):
+    """Each sub-step of each stage on the oracle's inputs of that sub-step: bit for bit in the
+    exact arithmetic (1e-13 with the Redlich-Kwong EOS, whose log differs in the last ulp), to
+    1e-13 relative L2 per field in the fast arithmetic."""
     prob = vortex(*shape) if kind == "vortex" else vortex_sheet(*shape)
     o = make_solver("port", prob, rks, settings)
     o.step(snapshots=True)
     sc = o.scalars()
     ae, ai = o.tableau()
     rk_eos = settings.get("eos_type") == "REDLICH_KWONG"
-    exact = (lambda a, b, msg: np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-15, err_msg=msg)) if rk_eos \
-        else (lambda a, b, msg: np.testing.assert_array_equal(a, b, err_msg=msg))
-    g = ix.Solver.for_problem(prob, rks, settings)
+
+    def close_fields(a, b, msg):
+        a, b = np.asarray(a), np.asarray(b)
+        if a.ndim == 2:
+            a, b = a[None], b[None]
+        for q in range(a.shape[0]):
+            assert rel(a[q], b[q]) <= 1e-13, (msg, q, rel(a[q], b[q]))
+
+    if arith == "fast":
+        exact = close_fields
+    elif rk_eos:
+        exact = lambda a, b, msg: np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-15, err_msg=msg)
+    else:
+        exact = lambda a, b, msg: np.testing.assert_array_equal(a, b, err_msg=msg)
+    g = ix.Solver.for_problem(prob, rks, dict(settings, arith=arith))
     for k in range(rks):
         S = lambda sub, w: o.snapshot(k, sub, w)
         adt = ai[k, k] * sc["dt"]
@@ -179,7 +214,7 @@ def test_gpu_legacy_ct_bit_exact(magfield):
     bx, by = o.snapshot(0, "pressure", "bx"), o.snapshot(0, "pressure", "by")
     h = 0.01
     ref = o.substep(6, h, 0, u, Q, Qs, bx, by, bxq, byq, A, As)
-    g = ix.Solver.for_problem(prob, 2, settings)
+    g = ix.Solver.for_problem(prob, 2, dict(settings, arith="exact"))
     for name, val in (("cons", u), ("Qe", Q), ("Qs", Qs), ("bx", bx), ("by", by), ("bxQs", bxq),
                       ("byQs", byq), ("A", A), ("A_s", As)):
         g.set_buffer(name, val)

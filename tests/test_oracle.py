@@ -160,8 +160,6 @@ def test_port_matches_live_reference_legacy_ct():
 def test_port_rejects_unsupported_configurations():
     prob = vortex(8)
     with pytest.raises(RuntimeError):
-        make_solver("port", prob, 2, dict(U_update="ConservationofU"))
-    with pytest.raises(RuntimeError):
         make_solver("port", prob, 2, dict(GLF=0))
 
 
