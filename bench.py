@@ -65,7 +65,7 @@ WORKLOADS = {
                               desc="vortex-sheet MHD 2048^2, WENO5, A-form CT, floor on, RK3"),
     "vortex_64": dict(problem="vortex", n=64, rks=2, settings=CFG0,
                       desc="smooth MHD vortex 64^2, VanLeer, staggered CT, RK2"),
-    "vortex_ensemble_256": dict(problem="vortex_ensemble", n=0, rks=2, settings=CFG0, members=256,
+    "vortex_ensemble_256": dict(problem="vortex_ensemble", n=0, rks=2, settings=CFG0, members=256, precision="mixed",
                                 desc="256 independent vortex runs (seed 2026: kappa, mu ~ U[0.5,1.5], square "
                                      "sides log-uniform 64..512), VanLeer, staggered CT, RK2, one ensemble"),
     "random_field_2048": dict(problem="random_field", n=2048, rks=2, settings=CFG2,
@@ -513,7 +513,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="imex", choices=["imex", "reference"])
     ap.add_argument("--workload", default="vortex_sheet_1024", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="default: the workload's own (mixed for the ensemble, as its configuration asks; "
+                         "fp64 otherwise, with the mixed pair measured beside it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-form measurement")
@@ -523,6 +525,8 @@ def main() -> int:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.precision is None:
+        args.precision = WORKLOADS[args.workload].get("precision", "fp64")
 
     world, rank, local = dist_setup()
     if args.impl == "imex" and WORKLOADS[args.workload]["problem"] == "vortex_ensemble":

@@ -727,57 +727,69 @@ __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __res
 }
 
 // ---------------------------------------------------------------- shock detector
-// ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41).
-template <bool kOpen>
-__global__ void k_shock_cf(DevParams Pin, const double* __restrict__ Q, double* __restrict__ cf) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= P.N) return;
+// ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41), as
+// one tiled kernel: the fast speed c_f on the tile plus a halo of 2 (shared memory), chi~ on
+// the halo-1 ring, chi on the tile.  Q is read once (72 B/cell) and only eta is written.
+// A staged halo position p holds the value of its mapped cell cid(p), as the reference's
+// ghost copies do: for a periodic direction the image has the same neighbourhood, so the
+// value is evaluated at p itself; for a transmissive one it is evaluated at the clamped
+// position, which lies in the same tile.
+constexpr int STX = 32, STY = 16, SHX = STX + 4, SHY = STY + 4, SCX = STX + 2, SCY = STY + 2;
+__device__ __forceinline__ double shock_cf_at(const DevParams& P, const double* __restrict__ Q, long long m) {
   double c[8];
-  load_cell<8>(Q, P.N, n, c);
+  load_cell<8>(Q, P.N, m, c);
   double p = pressure_of(P, c);
   double a2 = eos_a2(P, c[0], p);
   double cA2 = (c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) / c[0];
-  cf[n] = sqrt(a2 + cA2);
+  return sqrt(a2 + cA2);
 }
 template <bool kOpen>
-__global__ void k_shock_tilde(DevParams Pin, const double* __restrict__ Q, const double* __restrict__ cf,
-                              double* __restrict__ chit) {
+__global__ void __launch_bounds__(kThreads) k_shock(DevParams Pin, const double* __restrict__ Q,
+                                                     double* __restrict__ eta) {
   const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  double m = 1.0e300;
-  for (int di = -1; di <= 1; di++)
-    for (int dj = -1; dj <= 1; dj++) {
-      double v = __ldg(cf + cid(P, i + di, j + dj));
-      if (v < m) m = v;
-    }
-  long long xp = cid(P, i + 1, j), xm = cid(P, i - 1, j), yp = cid(P, i, j + 1), ym = cid(P, i, j - 1);
-  // every load before the first division
-  const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
-  const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
-  double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
-  double num = P.hmin * div_u + P.shock_kappa1 * m;
-  double den = P.shock_kappa1 * m;
-  double q = -num / den;
-  double mx = (0.0 < q) ? q : 0.0;
-  chit[n] = (mx < 1.0) ? mx : 1.0;
-}
-template <bool kOpen>
-__global__ void k_shock_max(DevParams Pin, const double* __restrict__ chit, double* __restrict__ eta) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= P.N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  double m = 0.0;
-  for (int di = -1; di <= 1; di++)
-    for (int dj = -1; dj <= 1; dj++) {
-      double v = __ldg(chit + cid(P, i + di, j + dj));
-      if (v > m) m = v;
-    }
-  eta[n] = m;
+  __shared__ double cf[SHY * SHX];  // c_f at (x0 - 2 + sx, y0 - 2 + sy)
+  __shared__ double ch[SCY * SCX];  // chi~ at (x0 - 1 + px, y0 - 1 + py)
+  const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
+  for (int q = threadIdx.x; q < SHY * SHX; q += kThreads) {
+    const int gi = x0 - 2 + q % SHX, gj = y0 - 2 + q / SHX;
+    cf[q] = shock_cf_at(P, Q, cid(P, gi, gj));
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < SCY * SCX; q += kThreads) {
+    int gi = x0 - 1 + q % SCX, gj = y0 - 1 + q / SCX;
+    if (P.xclamp) gi = gi < 0 ? 0 : (gi >= P.nx ? P.nx - 1 : gi);
+    if (P.yclamp) gj = gj < 0 ? 0 : (gj >= P.ny ? P.ny - 1 : gj);
+    const int sx = gi - x0 + 2, sy = gj - y0 + 2;  // within [1, SHX - 2] x [1, SHY - 2]
+    double m = 1.0e300;
+    for (int di = -1; di <= 1; di++)
+      for (int dj = -1; dj <= 1; dj++) {
+        double v = cf[(sy + dj) * SHX + sx + di];
+        if (v < m) m = v;
+      }
+    long long xp = cid(P, gi + 1, gj), xm = cid(P, gi - 1, gj), yp = cid(P, gi, gj + 1), ym = cid(P, gi, gj - 1);
+    // every load before the first division
+    const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
+    const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
+    double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
+    double num = P.hmin * div_u + P.shock_kappa1 * m;
+    double den = P.shock_kappa1 * m;
+    double qv = -num / den;
+    double mx = (0.0 < qv) ? qv : 0.0;
+    ch[q] = (mx < 1.0) ? mx : 1.0;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < STX * STY; q += kThreads) {
+    const int lx = q % STX, ly = q / STX, i = x0 + lx, j = y0 + ly;
+    if (i >= P.nx || j >= P.ny) continue;
+    double m = 0.0;
+    for (int di = -1; di <= 1; di++)
+      for (int dj = -1; dj <= 1; dj++) {
+        double v = ch[(ly + 1 + dj) * SCX + lx + 1 + di];
+        if (v > m) m = v;
+      }
+    eta[(long long)j * P.nx + i] = m;
+  }
 }
 
 // ---------------------------------------------------------------- diagnostics
@@ -1057,13 +1069,11 @@ imex_status launch_stage_derivative(imex_ctx* ctx, int rks) {
 
 imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
   const DevParams& P = ctx->P;
-  int nb = blocks_for(P.N);
+  const dim3 nb((P.nx + STX - 1) / STX, (P.ny + STY - 1) / STY);
   prof_begin(ctx);
-  IMEX_LAUNCH_BC(P, k_shock_cf, nb, kThreads, 0, ctx->stream, P, Q, ctx->Et);
-  IMEX_LAUNCH_BC(P, k_shock_tilde, nb, kThreads, 0, ctx->stream, P, Q, ctx->Et, ctx->chit);
-  IMEX_LAUNCH_BC(P, k_shock_max, nb, kThreads, 0, ctx->stream, P, ctx->chit, eta);
+  IMEX_LAUNCH_BC(P, k_shock, nb, kThreads, 0, ctx->stream, P, Q, eta);
   LAUNCH_CHECK(ctx, "shock detector");
-  prof_end(ctx, F_SHOCK, BYTES(16), 3);
+  prof_end(ctx, F_SHOCK, BYTES(9), 1);
   return IMEX_OK;
 }
 

@@ -10,10 +10,12 @@ the reference sources by `make -C oracle ref`) on small analytic inputs:
                      boundary normal faces (Bx at x_0, By at y_0);
   fn_<case>.npz    - single reference functions on fixed inputs:
                      TVDReconstruction, ShockDetector and the four matrix-free
-                     operators of implicit_operators.cpp.
+                     operators of implicit_operators.cpp;
+  adjoint_ref_fd64.npz - central finite differences of the reference's J on the
+                     adjoint workload at 64 x 64 (50 steps, all 32 amplitudes).
 
 Run from the repository root:  python tests/golden/make_golden.py [case ...]
-(no arguments: every case; otherwise only the named step cases and/or "fn").
+(no arguments: every case; otherwise only the named step cases and/or "fn", "adjoint_fd").
 """
 from __future__ import annotations
 
@@ -139,6 +141,49 @@ def fn_case() -> None:
     np.savez_compressed(os.path.join(HERE, "fn_vortex16x12.npz"), **out)
 
 
+ADJ_SETTINGS = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-14, fixed_dt=0.02)
+ADJ_N, ADJ_STEPS, ADJ_H = 64, 50, 1e-6
+
+
+def _adj_J(args):
+    """J of the reference solver on the perturbed vortex with amplitudes a (one process each)."""
+    a, rho_t, B_t = args
+    from imex_b200.problems import perturbed_vortex
+    pv = perturbed_vortex(ADJ_N)
+    r = make_solver("ref", pv.problem(a), 2, ADJ_SETTINGS)
+    for _ in range(ADJ_STEPS):
+        r.step()
+    c = r.cons()
+    return 0.5 * np.sum((c[0] - rho_t) ** 2) + 0.5 * np.sum((c[5:8] - B_t) ** 2)
+
+
+def adjoint_fd_case() -> None:
+    """The adjoint workload's check at 64 x 64: central differences (h = 1e-6) of the reference's
+    own FP64 J over 50 fixed-dt steps, for all 32 amplitudes, with the targets from the
+    reference's unperturbed run."""
+    import multiprocessing as mp
+    from imex_b200.problems import perturbed_vortex
+    pv = perturbed_vortex(ADJ_N)
+    base = make_solver("ref", pv.base, 2, ADJ_SETTINGS)
+    for _ in range(ADJ_STEPS):
+        base.step()
+    c = base.cons()
+    rho_t, B_t = c[0], c[5:8]
+    a0 = np.array(pv.amplitudes)
+    jobs = [(a0, rho_t, B_t)]
+    for m in range(len(a0)):
+        for sgn in (1.0, -1.0):
+            a = a0.copy()
+            a[m] += sgn * ADJ_H
+            jobs.append((a, rho_t, B_t))
+    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        Js = pool.map(_adj_J, jobs)
+    fd = np.array([(Js[1 + 2 * m] - Js[2 + 2 * m]) / (2 * ADJ_H) for m in range(len(a0))])
+    np.savez_compressed(os.path.join(HERE, "adjoint_ref_fd64.npz"), amplitudes=a0, J=np.array(Js[0]),
+                        fd=fd, rho_t=rho_t, B_t=B_t, nsteps=ADJ_STEPS, h=ADJ_H,
+                        settings=np.array(repr(ADJ_SETTINGS)))
+
+
 def main() -> None:
     if not RefSolver.available():
         raise SystemExit("oracle/_ref/libimexref.so missing: run `make -C oracle ref` first")
@@ -151,6 +196,9 @@ def main() -> None:
     if not only or "fn" in only:
         fn_case()
         print("wrote fn_vortex16x12")
+    if not only or "adjoint_fd" in only:
+        adjoint_fd_case()
+        print("wrote adjoint_ref_fd64")
 
 
 if __name__ == "__main__":

@@ -2,7 +2,9 @@
 J = 1/2 |rho(T) - rho_t|^2 + 1/2 |B(T) - B_t|^2 with targets from the unperturbed run,
 gradient with respect to the 32 amplitudes through the torch.autograd.Function of the test
 binding (tests/adjoint_torch.py), checked against central finite differences (h = 1e-6) of
-the GPU forward map and of the reference solver's own FP64 forward map at 64 x 64."""
+the GPU forward map and of the reference solver's own FP64 forward map at 64 x 64 (the
+latter also over the workload's 50 steps for all 32 amplitudes, from tests/golden/
+adjoint_ref_fd64.npz, which tests/golden/make_golden.py computes with the reference)."""
 from __future__ import annotations
 
 import numpy as np
@@ -104,3 +106,22 @@ def test_amplitude_gradient_matches_reference_finite_differences():
         fd = (J_ref(pv.amplitudes + e) - J_ref(pv.amplitudes - e)) / (2 * H)
         print(f"mode {m}: adjoint {g[m]:.12e} reference FD {fd:.12e} rel {abs(g[m] - fd) / abs(fd):.2e}")
         assert abs(g[m] - fd) <= 1e-6 * abs(fd)
+
+
+def test_all_amplitudes_match_reference_finite_differences_over_50_steps():
+    """All 32 amplitude derivatives over the workload's 50 steps with checkpoints every 10,
+    against the reference's own central differences (golden fixture, same targets)."""
+    import os
+    from conftest import GOLDEN
+    g0 = np.load(os.path.join(GOLDEN, "adjoint_ref_fd64.npz"))
+    pv = perturbed_vortex(64)
+    np.testing.assert_array_equal(np.asarray(pv.amplitudes), g0["amplitudes"])
+    spec = RunSpec(pv.base, 2, SETTINGS, int(g0["nsteps"]), 10)
+    J, g = _gradient(pv, spec, g0["rho_t"], g0["B_t"])
+    fd = g0["fd"]
+    assert J == pytest.approx(float(g0["J"]), rel=1e-9)
+    err = np.abs(g - fd)
+    print("max |fd|", np.abs(fd).max(), "max rel err", (err / np.abs(fd).max()).max())
+    assert err.max() <= 1e-6 * np.abs(fd).max()
+    big = np.abs(fd) > 1e-2 * np.abs(fd).max()
+    assert (err[big] <= 1e-5 * np.abs(fd[big])).all()
