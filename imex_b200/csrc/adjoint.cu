@@ -1182,6 +1182,12 @@ imex_status adjoint_core(imex_ctx* ctx, const imex_adjoint_opts* o, const std::f
   Adj W{};
   W.ctx = ctx;
   W.N = ctx->N;
+  // the forward recomputations keep the shock detector's chi~ (its VJP follows the branches)
+  struct KeepChit {
+    imex_ctx* c;
+    ~KeepChit() { c->keep_shock_chit = false; }
+  } keep{ctx};
+  ctx->keep_shock_chit = true;
   W.R = ctx->P.RKs;
   W.tol = o->gmres_tol > 0.0 ? o->gmres_tol : 1e-13;
   const size_t N = W.N;

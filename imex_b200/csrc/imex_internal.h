@@ -104,6 +104,7 @@ struct imex_ctx {
   int num_sms = 0;
   int clock_khz = 0;  // maximum SM clock, read once at creation (bounds of device-side waits)
   int device = -1;    // the device that was current at imex_create; all its memory lives there
+  bool keep_shock_chit = false;  // the shock detector also stores chi~ in chit (the adjoint reads it)
 
   // device state (interior planes)
   double *prim = nullptr, *cons = nullptr, *cons_n = nullptr, *Qe = nullptr, *Qs = nullptr;

@@ -729,31 +729,40 @@ __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __res
 // ---------------------------------------------------------------- shock detector
 // ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41), as
 // one tiled kernel: the fast speed c_f on the tile plus a halo of 2 (shared memory), chi~ on
-// the halo-1 ring, chi on the tile.  Q is read once (72 B/cell) and only eta is written.
+// the halo-1 ring, chi on the tile.  Q is read once and only eta is written (72 B/cell);
+// the discrete adjoint also has chi~ of every cell stored (chit, 8 B/cell more).
 // A staged halo position p holds the value of its mapped cell cid(p), as the reference's
 // ghost copies do: for a periodic direction the image has the same neighbourhood, so the
 // value is evaluated at p itself; for a transmissive one it is evaluated at the clamped
 // position, which lies in the same tile.
 constexpr int STX = 32, STY = 16, SHX = STX + 4, SHY = STY + 4, SCX = STX + 2, SCY = STY + 2;
-__device__ __forceinline__ double shock_cf_at(const DevParams& P, const double* __restrict__ Q, long long m) {
-  double c[8];
-  load_cell<8>(Q, P.N, m, c);
-  double p = pressure_of(P, c);
-  double a2 = eos_a2(P, c[0], p);
-  double cA2 = (c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) / c[0];
-  return sqrt(a2 + cA2);
-}
 template <bool kOpen>
 __global__ void __launch_bounds__(kThreads) k_shock(DevParams Pin, const double* __restrict__ Q,
-                                                     double* __restrict__ eta) {
+                                                     double* __restrict__ eta, double* __restrict__ chit) {
   const DevParams P = bc_params<kOpen>(Pin);
   const long long N = P.N;
   __shared__ double cf[SHY * SHX];  // c_f at (x0 - 2 + sx, y0 - 2 + sy)
   __shared__ double ch[SCY * SCX];  // chi~ at (x0 - 1 + px, y0 - 1 + py)
   const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
-  for (int q = threadIdx.x; q < SHY * SHX; q += kThreads) {
-    const int gi = x0 - 2 + q % SHX, gj = y0 - 2 + q / SHX;
-    cf[q] = shock_cf_at(P, Q, cid(P, gi, gj));
+  {  // each thread's cells of the halo-2 tile, every load before the first division
+    constexpr int KC = (SHY * SHX + kThreads - 1) / kThreads;
+    double c[KC][8];
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      const int q = threadIdx.x + k * kThreads;
+      const int qq = q < SHY * SHX ? q : SHY * SHX - 1;  // past the end: a staged cell, loaded again
+      load_cell<8>(Q, N, cid(P, x0 - 2 + qq % SHX, y0 - 2 + qq / SHX), c[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      const int q = threadIdx.x + k * kThreads;
+      if (q < SHY * SHX) {
+        const double p = pressure_of(P, c[k]);
+        const double a2 = eos_a2(P, c[k][0], p);
+        const double cA2 = (c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7]) / c[k][0];
+        cf[q] = sqrt(a2 + cA2);
+      }
+    }
   }
   __syncthreads();
   for (int q = threadIdx.x; q < SCY * SCX; q += kThreads) {
@@ -777,6 +786,10 @@ __global__ void __launch_bounds__(kThreads) k_shock(DevParams Pin, const double*
     double qv = -num / den;
     double mx = (0.0 < qv) ? qv : 0.0;
     ch[q] = (mx < 1.0) ? mx : 1.0;
+    // chi~ of the tile's own cells, when asked for (chit != nullptr)
+    const int lx = q % SCX - 1, ly = q / SCX - 1;
+    if (chit && lx >= 0 && lx < STX && ly >= 0 && ly < STY && x0 + lx < P.nx && y0 + ly < P.ny)
+      chit[(long long)(y0 + ly) * P.nx + (x0 + lx)] = ch[q];
   }
   __syncthreads();
   for (int q = threadIdx.x; q < STX * STY; q += kThreads) {
@@ -1071,7 +1084,7 @@ imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
   const DevParams& P = ctx->P;
   const dim3 nb((P.nx + STX - 1) / STX, (P.ny + STY - 1) / STY);
   prof_begin(ctx);
-  IMEX_LAUNCH_BC(P, k_shock, nb, kThreads, 0, ctx->stream, P, Q, eta);
+  IMEX_LAUNCH_BC(P, k_shock, nb, kThreads, 0, ctx->stream, P, Q, eta, ctx->keep_shock_chit ? ctx->chit : nullptr);
   LAUNCH_CHECK(ctx, "shock detector");
   prof_end(ctx, F_SHOCK, BYTES(9), 1);
   return IMEX_OK;
