@@ -93,7 +93,8 @@ class SolveStats(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double)]
+    _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double),
+                ("mixed_solves", C.c_int)]
 
 
 class Diagnostics(C.Structure):
@@ -641,7 +642,8 @@ class Batch:
     def autotune(self, trial_steps: int = 2) -> dict:
         t = BatchTuning()
         self._check(self.lib.imex_batch_autotune(self.b, trial_steps, C.byref(t)))
-        return dict(streams=t.streams, gmres_restart=t.gmres_restart, ms_per_step=t.ms_per_step)
+        return dict(streams=t.streams, gmres_restart=t.gmres_restart, ms_per_step=t.ms_per_step,
+                    mixed_solves=t.mixed_solves)
 
     def info(self) -> dict:
         a, g, n = C.c_int(), C.c_int(), C.c_int()

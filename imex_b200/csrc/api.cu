@@ -100,7 +100,7 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
     if (c->mixed_max_refine < 1) return why = "mixed_max_refine must be at least 1", IMEX_ERR_INVALID;
     if (!(c->mixed_outer_tol >= 0.0 && c->mixed_outer_tol < 1.0))
       return why = "mixed_outer_tol must be in [0, 1)", IMEX_ERR_INVALID;
-    if (c->mixed_solves & ~(IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC))
+    if (c->mixed_solves & ~(IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B))
       return why = "bad mixed_solves", IMEX_ERR_INVALID;
   }
   if (!(c->x_1 > c->x_0) || !(c->y_1 > c->y_0)) return why = "empty domain", IMEX_ERR_INVALID;
@@ -347,7 +347,7 @@ void imex_config_default(imex_config* c) {
   c->precision = IMEX_PRECISION_FP64;
   c->mixed_inner_tol = 1e-6;
   c->mixed_max_refine = 50;
-  c->mixed_solves = IMEX_MIXED_PRESSURE;
+  c->mixed_solves = IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC_B;
   c->mixed_outer_tol = 1e-10;
   c->arith = IMEX_ARITH_FAST;
 }

@@ -361,29 +361,46 @@ imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tunin
   const int restart0 = b->members[0]->cfg.gmres_restart;
   const int stream_cands[] = {4, 8, 16};
   const int restart_cands[] = {restart0 < 15 ? restart0 : 15, restart0};
+  // in mixed precision, whether the magnetic systems take the FP32 form pays only where
+  // FP64 GMRES needs many Krylov steps: time both
+  const int solves0 = b->members[0]->cfg.mixed_solves;
+  const int mag = IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B;
+  std::vector<int> solve_cands{solves0};
+  if (b->members[0]->cfg.precision == IMEX_PRECISION_MIXED)
+    solve_cands.push_back((solves0 & mag) ? (solves0 & ~mag) : (solves0 | IMEX_MIXED_MAGNETIC_B));
   Snapshot snap;
   imex_status s = take_snapshot(b, snap, false);
   double best = 1e300;
-  int best_streams = b->nstreams, best_restart = restart0;
+  int best_streams = b->nstreams, best_restart = restart0, best_solves = solves0;
   for (int sc : stream_cands) {
     for (int rc : restart_cands) {
-      for (imex_ctx* c : b->members) c->cfg.gmres_restart = rc;
-      if (s == IMEX_OK) s = imex_batch_configure(b, sc, b->use_graph ? 1 : 0);
-      double ms = 0.0;
-      if (s == IMEX_OK) s = imex_batch_step(b, 1, nullptr);  // warm-up (and graph capture)
-      if (s == IMEX_OK) s = imex_batch_step(b, trial_steps, &ms);
-      if (s == IMEX_OK) s = take_snapshot(b, snap, true);
-      if (s != IMEX_OK) break;
-      if (ms < best) {
-        best = ms;
-        best_streams = sc;
-        best_restart = rc;
+      for (int mc : solve_cands) {
+        for (imex_ctx* c : b->members) {
+          c->cfg.gmres_restart = rc;
+          c->cfg.mixed_solves = mc;
+        }
+        if (s == IMEX_OK) s = imex_batch_configure(b, sc, b->use_graph ? 1 : 0);
+        double ms = 0.0;
+        if (s == IMEX_OK) s = imex_batch_step(b, 1, nullptr);  // warm-up (and graph capture)
+        if (s == IMEX_OK) s = imex_batch_step(b, trial_steps, &ms);
+        if (s == IMEX_OK) s = take_snapshot(b, snap, true);
+        if (s != IMEX_OK) break;
+        if (ms < best) {
+          best = ms;
+          best_streams = sc;
+          best_restart = rc;
+          best_solves = mc;
+        }
       }
+      if (s != IMEX_OK) break;
     }
     if (s != IMEX_OK) break;
   }
   for (double* p : snap.planes) cudaFree(p);
-  for (imex_ctx* c : b->members) c->cfg.gmres_restart = best_restart;
+  for (imex_ctx* c : b->members) {
+    c->cfg.gmres_restart = best_restart;
+    c->cfg.mixed_solves = best_solves;
+  }
   imex_status s2 = imex_batch_configure(b, best_streams, b->use_graph ? 1 : 0);
   if (s != IMEX_OK) return s;
   if (s2 != IMEX_OK) return s2;
@@ -391,6 +408,7 @@ imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tunin
     out->streams = best_streams;
     out->gmres_restart = best_restart;
     out->ms_per_step = best / trial_steps;
+    out->mixed_solves = best_solves;
   }
   return IMEX_OK;
 }

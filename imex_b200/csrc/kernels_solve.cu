@@ -2171,7 +2171,7 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
     o.jac = op == IMEX_OP_PRESSURE_J;
     return gmres_run(ctx, o, F_GMRES_PRES, x, b, IMEX_MIXED_PRESSURE);
   } else if (op == IMEX_OP_MAGNETIC_B) {
-    return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC);
+    return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     if (ctx->P.xclamp || ctx->P.yclamp)
       return gmres_run(ctx, make_magA_op<true>(ctx), F_GMRES_MAG_A, x, b, IMEX_MIXED_MAGNETIC);
@@ -2458,7 +2458,8 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
     else if (P.magfield == IMEX_PotentialA)
       s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<false>, sys);
     else
-      s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_B, make_magB_op, sys);
+      s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B, F_GMRES_MAG_B,
+                                        make_magB_op, sys);
   } else if (P.formula == IMEX_EnergyFormula) {  // the energy solve, in place on E
     s = add_gmres_chunks<EnergyOp>(plan, members, IMEX_MIXED_PRESSURE, F_GMRES_ENERGY, make_energy_op,
                                    [](imex_ctx* m, double** x, const double** b) {

@@ -92,10 +92,13 @@ typedef enum {
 } imex_arith;
 /* Solves of the mixed form (imex_config.mixed_solves).  The pressure solves (the nested
  * Newton's Jacobian systems, or the single linear GMRES without the floor) gain from FP32:
- * the Newton iteration is their FP64 refinement.  The magnetic systems converge in a few
- * FP64 GMRES steps on the smooth fields of a stage; FP32 rounding noise then costs several
- * refinement sweeps, so they stay FP64 unless IMEX_MIXED_MAGNETIC is set. */
-enum { IMEX_MIXED_PRESSURE = 1, IMEX_MIXED_MAGNETIC = 2 };
+ * the Newton iteration is their FP64 refinement.  The B-form magnetic system (StaggerCT,
+ * UnStaggerCT, NoDivFree) gains where it needs many Krylov steps, as on the low-beta random
+ * field; the A-form (PotentialA) system converges in a few FP64 steps on the smooth fields
+ * of a stage, where FP32 rounding noise costs more refinement sweeps than it saves.  The
+ * default is IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC_B; IMEX_MIXED_MAGNETIC takes both
+ * magnetic forms. */
+enum { IMEX_MIXED_PRESSURE = 1, IMEX_MIXED_MAGNETIC = 2, IMEX_MIXED_MAGNETIC_B = 4 };
 
 /* Run-time form of the reference's compile-time configuration
  * (include/config.hpp:43-125 and the per-test settings of main.cpp:9-224).
@@ -138,7 +141,7 @@ typedef struct imex_config {
   int precision;          /* imex_precision */
   double mixed_inner_tol; /* relative tolerance of each FP32 inner solve in mixed mode */
   int mixed_max_refine;   /* cap on FP64 refinement sweeps in mixed mode */
-  int mixed_solves;       /* which solves take the mixed form: IMEX_MIXED_PRESSURE | IMEX_MIXED_MAGNETIC */
+  int mixed_solves;       /* which solves take the mixed form: IMEX_MIXED_* flags */
   double mixed_outer_tol; /* relative residual at which the FP64 refinement of a mixed GMRES solve stops
                              (plus the same value absolute, as GMREStol); the plain form's GMREStol when
                              0.  The default, 1e-10, spends part of the mixed form's 1e-8 error budget. */
@@ -391,6 +394,7 @@ typedef struct imex_batch_tuning {
   int streams;          /* streams of the explicit sub-steps */
   int gmres_restart;    /* Krylov vectors per cycle of every member */
   double ms_per_step;   /* device time of one ensemble step at that choice */
+  int mixed_solves;     /* IMEX_MIXED_* flags of every member (mixed precision only) */
 } imex_batch_tuning;
 imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx, const int* ny, imex_batch** out);
 imex_status imex_batch_destroy(imex_batch* b);
@@ -400,8 +404,9 @@ imex_status imex_batch_configure(imex_batch* b, int streams, int use_graph);
 /* advance every member `steps` steps; *device_ms (optional) = device time of those steps */
 imex_status imex_batch_step(imex_batch* b, int steps, double* device_ms);
 /* time `trial_steps` ensemble steps for each candidate (streams 4 / 8 / 16, restart
- * length 15 or the configured one), restore every member's state after each trial, and
- * keep the fastest choice */
+ * length 15 or the configured one, and in mixed precision the configured mixed_solves or
+ * the same with the magnetic systems' FP32 form toggled), restore every member's state
+ * after each trial, and keep the fastest choice */
 imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out);
 /* streams in use, whether the step runs as a captured graph, batched solve launches per step */
 imex_status imex_batch_info(imex_batch* b, int* streams, int* graph_used, int* solve_launches_per_step);

@@ -41,17 +41,18 @@ def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "imex_b200.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(imex_config), sizeof(imex_step_scalars),'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(imex_config), sizeof(imex_step_scalars),'
         ' sizeof(imex_solve_stats), sizeof(imex_kernel_profile), offsetof(imex_config, mixed_max_refine),'
         ' offsetof(imex_config, gmres_restart), sizeof(imex_diagnostics_t), offsetof(imex_diagnostics_t, magE_max),'
-        ' sizeof(imex_adjoint_opts)); return 0;}\n')
+        ' sizeof(imex_adjoint_opts), sizeof(imex_batch_tuning), offsetof(imex_batch_tuning, mixed_solves));'
+        ' return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert vals == [C.sizeof(ix.Config), C.sizeof(ix.StepScalars), C.sizeof(ix.SolveStats),
                     C.sizeof(ix.KernelProfile), ix.Config.mixed_max_refine.offset,
                     ix.Config.gmres_restart.offset, C.sizeof(ix.Diagnostics), ix.Diagnostics.magE_max.offset,
-                    C.sizeof(ix.AdjointOpts)]
+                    C.sizeof(ix.AdjointOpts), C.sizeof(ix.BatchTuning), ix.BatchTuning.mixed_solves.offset]
 
 
 def test_defaults_are_the_reference_defaults():
