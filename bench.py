@@ -348,7 +348,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     settings = dict(wl["settings"])
     settings["precision"] = args.precision
     batch = ix.Batch(probs, wl["rks"], settings)
-    tuned = batch.autotune(trial_steps=1)
+    tuned = None if args.no_autotune else batch.autotune(trial_steps=1)
     launches0 = sum(m.kernel_launches() for m in batch.members)
     batch.step(1)  # captures the step (launch count of one step) and runs it
     info = batch.info()
@@ -520,6 +520,8 @@ def main() -> int:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-form measurement")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision pair")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="ensemble: keep the configured streams, restart length and mixed solves")
     ap.add_argument("--n", type=int, default=None, help="override the grid side (profiling cases)")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()

@@ -667,6 +667,28 @@ static struct {
   double gmax_bx, gmax_by;
 } OP;
 
+/* Local Lax-Friedrichs speed of one cell for the magnetic viscosity (GLF = false):
+   0.5 (|v| + sqrt(v^2 + 4 |B|^2 / rho)) of the primitive state of conserved state c along
+   dir (implicit_operators.cpp:324-335 and 473-480, ct_flux.cpp:81-84 and 116-119) */
+static double lf_speed(const double* c, int dir) {
+  double rho = c[0], v = c[1 + dir] / c[0];
+  return 0.5 * (fabs(v) + sqrt(v * v + 4.0 * (c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) / rho));
+}
+static double lf_speed_at(const double* Q, int i, int j, int dir) {
+  double c[8];
+  load8(Q, ID(i, j), c);
+  return lf_speed(c, dir);
+}
+/* the pressure viscosity's local speed of one cell (implicit_operators.cpp:587-598): |v_dir|
+   (MaterialSpeedp), |B_dir| / sqrt(rho) (AlfvenSpeedp), 0 (Noaddvisp) */
+static double pv_speed_at(const double* Q, int i, int j, int dir) {
+  double c[8];
+  load8(Q, ID(i, j), c);
+  if (PP.add_pvisc == MaterialSpeedp) return fabs(c[1 + dir] / c[0]);
+  if (PP.add_pvisc == AlfvenSpeedp) return fabs(c[5 + dir] / sqrt(c[0]));
+  return 0.0;
+}
+
 /* enthalpy ratio h(Qe) rho_e / rho (implicit_operators.cpp:527-531) */
 static double hhat_at(size_t n) {
   double c[8];
@@ -697,10 +719,23 @@ static void pressure_ax(const double* x, double* Ax) {
                      (1 / (dx * dx) * (0.5 * (hp0 + h00) * (x[e] - x[c]) - 0.5 * (h00 + hm0) * (x[c] - x[w])) +
                       1 / (dy * dy) * (0.5 * (h0p + h00) * (x[n] - x[c]) - 0.5 * (h0m + h00) * (x[c] - p_0m)));
       const double* et = OP.eta;
-      double lap_p = nu_x / (dx * dx) *
-                         (0.5 * (et[e] + et[c]) * (x[e] - pii) - 0.5 * (et[c] + et[w]) * (pii - x[w])) +
-                     nu_y / (dy * dy) *
-                         (0.5 * (et[n] + et[c]) * (x[n] - pii) - 0.5 * (et[c] + et[s]) * (pii - x[s]));
+      double lap_p;
+      if (PP.GLF) {
+        lap_p = nu_x / (dx * dx) *
+                    (0.5 * (et[e] + et[c]) * (x[e] - pii) - 0.5 * (et[c] + et[w]) * (pii - x[w])) +
+                nu_y / (dy * dy) *
+                    (0.5 * (et[n] + et[c]) * (x[n] - pii) - 0.5 * (et[c] + et[s]) * (pii - x[s]));
+      } else { /* implicit_operators.cpp:584-607 */
+        double sx = pv_speed_at(OP.Qe, i, j, 0), sy = pv_speed_at(OP.Qe, i, j, 1);
+        double nu_x_p = fmax(sx, pv_speed_at(OP.Qe, i + 1, j, 0)) * dx;
+        double nu_x_m = fmax(sx, pv_speed_at(OP.Qe, i - 1, j, 0)) * dx;
+        double nu_y_p = fmax(sy, pv_speed_at(OP.Qe, i, j + 1, 1)) * dy;
+        double nu_y_m = fmax(sy, pv_speed_at(OP.Qe, i, j - 1, 1)) * dy;
+        lap_p = 1 / (dx * dx) *
+                    (0.5 * (et[e] + et[c]) * nu_x_p * (x[e] - pii) - 0.5 * (et[c] + et[w]) * nu_x_m * (pii - x[w])) +
+                1 / (dy * dy) *
+                    (0.5 * (et[n] + et[c]) * nu_y_p * (x[n] - pii) - 0.5 * (et[c] + et[s]) * nu_y_m * (pii - x[s]));
+      }
       Ax[c] = r - OP.vscale[c] * h * lap_p;
     }
 }
@@ -1077,9 +1112,22 @@ static void magnetic_ax(const double* x, double* Ax) {
       double ax7 = XB(7, i, j) + h * h / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + h * h / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
 
       double nu_x = G.B_max_x * dx, nu_y = G.B_max_y * dy;
+      double nu_x_p = 0, nu_x_m = 0, nu_y_p = 0, nu_y_m = 0;
+      if (!PP.GLF) { /* implicit_operators.cpp:323-352 */
+        double b_x = lf_speed_at(OP.Qe, i, j, 0), b_y = lf_speed_at(OP.Qe, i, j, 1);
+        nu_x_p = fmax(fabs(b_x), fabs(lf_speed_at(OP.Qe, i + 1, j, 0))) * dx;
+        nu_x_m = fmax(fabs(b_x), fabs(lf_speed_at(OP.Qe, i - 1, j, 0))) * dx;
+        nu_y_p = fmax(fabs(b_y), fabs(lf_speed_at(OP.Qe, i, j + 1, 1))) * dy;
+        nu_y_m = fmax(fabs(b_y), fabs(lf_speed_at(OP.Qe, i, j - 1, 1))) * dy;
+      }
       for (int k = 5; k <= 7; ++k) {
-        double lap = nu_x / (dx * dx) * (XB(k, i - 1, j) - 2.0 * XB(k, i, j) + XB(k, i + 1, j)) +
-                     nu_y / (dy * dy) * (XB(k, i, j - 1) - 2.0 * XB(k, i, j) + XB(k, i, j + 1));
+        double lap;
+        if (PP.GLF)
+          lap = nu_x / (dx * dx) * (XB(k, i - 1, j) - 2.0 * XB(k, i, j) + XB(k, i + 1, j)) +
+                nu_y / (dy * dy) * (XB(k, i, j - 1) - 2.0 * XB(k, i, j) + XB(k, i, j + 1));
+        else
+          lap = 1 / (dx * dx) * (nu_x_p * (XB(k, i + 1, j) - XB(k, i, j)) - nu_x_m * (XB(k, i, j) - XB(k, i - 1, j))) +
+                1 / (dy * dy) * (nu_y_p * (XB(k, i, j + 1) - XB(k, i, j)) - nu_y_m * (XB(k, i, j) - XB(k, i, j - 1)));
         double base = k == 5 ? ax5 : (k == 6 ? ax6 : ax7);
         Ax[(size_t)(k - 5) * N + ID(i, j)] = base - h * lap;
       }
@@ -1185,6 +1233,7 @@ static void collect_mag_fluxes(double* Fx, double* Fy, const double* ucon, const
                      1.0 / dy * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Byn_pp * By1_pp) -
                                  (0.5 * (Bxn_pm * Bx1_pm + Byn_pm * By1_pm + Bzn_pm * Bz1_pm) - Byn_pm * By1_pm)));
       double nu_x = G.B_max_x * dx;
+      if (!PP.GLF) nu_x = fmax(fabs(lf_speed_at(Qe, i, j, 0)), fabs(lf_speed_at(Qe, i + 1, j, 0))) * dx;
       double Fdiff_x = -nu_x * (U(6, i + 1, j) - U(6, i, j)) / dx;
       Fx[ID(i, j)] = Fn_x + h * (By_1 + By_2) + Fdiff_x;
       double Fn_y = Bxn_0p / rho_0p * (rvy_0p - (h / dy) * (PE(i, j + 1) - PE(i, j))) -
@@ -1198,6 +1247,7 @@ static void collect_mag_fluxes(double* Fx, double* Fy, const double* ucon, const
                      1.0 / dy * (Q(6, i, j + 1) * U(5, i, j + 1) - Q(6, i, j) * U(5, i, j)));
 #undef QU
       double nu_y = G.B_max_y * dy;
+      if (!PP.GLF) nu_y = fmax(fabs(lf_speed_at(Qe, i, j, 1)), fabs(lf_speed_at(Qe, i, j + 1, 1))) * dy;
       double Fdiff_y = -nu_y * (U(5, i, j + 1) - U(5, i, j)) / dy;
       Fy[ID(i, j)] = Fn_y + h * (Bx_1 + Bx_2) + Fdiff_y;
     }
@@ -1268,10 +1318,21 @@ static void potential_ax(const double* x, double* Ax) {
       double cross_y = Bzn_00 * Fx - Bxn_00 * Fz;
       double cross_z = Bxn_00 * Fy - Byn_00 * Fx;
       double lap[3] = {0.0, 0.0, 0.0};
-      double nu_x = OP.gmax_bx * dx, nu_y = OP.gmax_by * dy;
-      for (int k = 0; k < 3; ++k)
-        lap[k] = nu_x / (dx * dx) * (AG(i - 1, j, k) - 2.0 * AG(i, j, k) + AG(i + 1, j, k)) +
-                 nu_y / (dy * dy) * (AG(i, j - 1, k) - 2.0 * AG(i, j, k) + AG(i, j + 1, k));
+      if (PP.GLF) {
+        double nu_x = OP.gmax_bx * dx, nu_y = OP.gmax_by * dy;
+        for (int k = 0; k < 3; ++k)
+          lap[k] = nu_x / (dx * dx) * (AG(i - 1, j, k) - 2.0 * AG(i, j, k) + AG(i + 1, j, k)) +
+                   nu_y / (dy * dy) * (AG(i, j - 1, k) - 2.0 * AG(i, j, k) + AG(i, j + 1, k));
+      } else { /* face averages of the speeds of prim(Qs), implicit_operators.cpp:472-490 */
+        double b_x = lf_speed_at(OP.Qs, i, j, 0), b_y = lf_speed_at(OP.Qs, i, j, 1);
+        double nu_xp = 0.5 * (fabs(b_x) + fabs(lf_speed_at(OP.Qs, i + 1, j, 0))) * dx;
+        double nu_xm = 0.5 * (fabs(b_x) + fabs(lf_speed_at(OP.Qs, i - 1, j, 0))) * dx;
+        double nu_yp = 0.5 * (fabs(b_y) + fabs(lf_speed_at(OP.Qs, i, j + 1, 1))) * dy;
+        double nu_ym = 0.5 * (fabs(b_y) + fabs(lf_speed_at(OP.Qs, i, j - 1, 1))) * dy;
+        for (int k = 0; k < 3; ++k)
+          lap[k] = 1.0 / (dx * dx) * (nu_xp * (AG(i + 1, j, k) - AG(i, j, k)) - nu_xm * (AG(i, j, k) - AG(i - 1, j, k))) +
+                   1.0 / (dy * dy) * (nu_yp * (AG(i, j + 1, k) - AG(i, j, k)) - nu_ym * (AG(i, j, k) - AG(i, j - 1, k)));
+      }
       if (!PP.add_bvisc) lap[0] = lap[1] = lap[2] = 0.0;
       size_t c = ID(i, j);
       Ax[c] = AG(i, j, 0) - h * cross_x - h * lap[0];
@@ -1704,7 +1765,7 @@ static void free_all(void) {
 
 int ora_setup(int nx, int ny, int rks, const ora_params* p) {
   if (nx < 4 || ny < 4 || rks < 1 || rks > MAXRK) return 1;
-  if ((p->formula != PressureFormula && p->formula != EnergyFormula) || !p->GLF ||
+  if ((p->formula != PressureFormula && p->formula != EnergyFormula) ||
       (p->U_update != DefinitionofU && p->U_update != ConservationofU))
     return 2;
   free_all();

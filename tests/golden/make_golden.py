@@ -78,6 +78,23 @@ STEP_CASES = {
     "vortex16_conservationofU_rkeos": (lambda: vortex(16), 2,
                                        dict(recon="VanLeer", magfield="StaggerCT", U_update="ConservationofU",
                                             eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 1),
+    # local Lax-Friedrichs dissipation (GLF = false): face speeds from the neighbouring cells in the
+    # explicit fluxes (flux.cpp:108-389), the magnetic and pressure viscosities
+    # (implicit_operators.cpp:311-353, 472-490, 584-607) and CollectMagFluxes (ct_flux.cpp:79-124)
+    "vortex16_local_lf": (lambda: vortex(16), 2, dict(CFG0, GLF=0), 2),
+    "sheet16_potentialA_local_lf_rk3": (lambda: vortex_sheet(16), 3, dict(CFG1, GLF=0, add_bvisc=1), 2),
+    "blast16_local_lf_alfven_open": (lambda: open_blast(16), 2,
+                                     dict(recon="Minmod", magfield="StaggerCT", GLF=0, add_pvisc="AlfvenSpeedp"), 2),
+    "blast16x14_potentialA_local_lf_open": (lambda: open_blast(16, 14), 2,
+                                            dict(recon="VanLeer", magfield="PotentialA", GLF=0, p_floor=1e-8,
+                                                 theta=0.5), 2),
+    "vortex14x12_unstag_energyformula_local_lf": (lambda: vortex(14, 12), 2,
+                                                  dict(recon="Minmod", magfield="UnStaggerCT", GLF=0,
+                                                       formula="EnergyFormula"), 2),
+    "vortex16_local_lf_rkeos_conservationofU": (lambda: vortex(16), 2,
+                                                dict(recon="VanLeer", magfield="StaggerCT", GLF=0,
+                                                     U_update="ConservationofU", eos_type="REDLICH_KWONG",
+                                                     m_alfa=0.4275, m_b=0.0866), 1),
 }
 
 

@@ -74,6 +74,9 @@ LIVE_CASES = [
     ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", add_pvisc="AlfvenSpeedp"), 1),
     ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula"), 2),
     ("sheet", 18, 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, formula="EnergyFormula"), 1),
+    ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", GLF=0), 2),
+    ("vortex", 20, 2, dict(recon="WENO5", magfield="StaggerCT", GLF=0, add_pvisc="AlfvenSpeedp"), 1),
+    ("sheet", 18, 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GLF=0), 2),
 ]
 
 
@@ -101,7 +104,10 @@ def test_port_matches_live_reference(kind, n, rks, settings, steps):
     (2, dict(recon="Minmod", magfield="NoDivFree", formula="EnergyFormula", GMREStol=1e-12)),
     (3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
     (2, dict(recon="VanLeer", magfield="UnStaggerCT", x_bc="x_Periodic")),
-], ids=["vanleer_ct", "weno5_ct_yperiodic", "minmod_nodivfree_energy", "weno5_potentialA", "unstag_xperiodic"])
+    (2, dict(recon="VanLeer", magfield="StaggerCT", GLF=0)),
+    (2, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GLF=0)),
+], ids=["vanleer_ct", "weno5_ct_yperiodic", "minmod_nodivfree_energy", "weno5_potentialA", "unstag_xperiodic",
+        "vanleer_ct_local_lf", "weno5_potentialA_local_lf"])
 def test_port_matches_live_reference_transmissive(rks, settings):
     """Transmissive boundaries: every sub-step of every stage, boundary faces included."""
     from imex_b200.problems import open_blast
@@ -159,8 +165,9 @@ def test_port_matches_live_reference_legacy_ct():
 
 def test_port_rejects_unsupported_configurations():
     prob = vortex(8)
-    with pytest.raises(RuntimeError):
-        make_solver("port", prob, 2, dict(GLF=0))
+    for bad in (dict(U_update=5), dict(formula=7)):
+        with pytest.raises(RuntimeError):
+            make_solver("port", prob, 2, bad)
 
 
 RK_RANDOM = dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866)
