@@ -347,6 +347,8 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     probs = vortex_ensemble(wl["members"], seed=2026)
     settings = dict(wl["settings"])
     settings["precision"] = args.precision
+    if args.mixed_solves is not None:
+        settings["mixed_solves"] = args.mixed_solves
     batch = ix.Batch(probs, wl["rks"], settings)
     tuned = None if args.no_autotune else batch.autotune(trial_steps=1)
     launches0 = sum(m.kernel_launches() for m in batch.members)
@@ -522,6 +524,9 @@ def main() -> int:
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision pair")
     ap.add_argument("--no-autotune", action="store_true",
                     help="ensemble: keep the configured streams, restart length and mixed solves")
+    ap.add_argument("--mixed-solves", type=int, default=None,
+                    help="ensemble: the mixed solves (imex_mixed_solves bits) to start from, e.g. the set "
+                         "an earlier autotune chose, with --no-autotune")
     ap.add_argument("--n", type=int, default=None, help="override the grid side (profiling cases)")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()

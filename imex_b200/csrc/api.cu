@@ -85,7 +85,6 @@ imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
       (c->y_bc != IMEX_y_Periodic && c->y_bc != IMEX_y_Transmissive))
     return why = "only periodic and transmissive boundaries are implemented", IMEX_ERR_UNSUPPORTED;
   if (c->formula != IMEX_PressureFormula && c->formula != IMEX_EnergyFormula) return why = "bad formula", IMEX_ERR_INVALID;
-  if (!c->GLF) return why = "only the global Lax-Friedrichs dissipation (GLF) is implemented", IMEX_ERR_UNSUPPORTED;
   if (c->U_update != IMEX_DefinitionofU && c->U_update != IMEX_ConservationofU)
     return why = "U_update must be DefinitionofU or ConservationofU", IMEX_ERR_INVALID;
   if (c->recon < IMEX_NoRecon || c->recon > IMEX_WENO5) return why = "bad recon", IMEX_ERR_INVALID;
@@ -443,6 +442,9 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   A_(hh, N); A_(eta, N); A_(vscale, N); A_(tdiag, N); A_(vdiag, N); A_(rv, 3 * N);
   A_(pb, N); A_(pp, N); A_(pf, N); A_(pg, N); A_(pdp, N);
   A_(mx, 3 * N); A_(mb, 3 * N);
+  if (!cfg->GLF) {
+    A_(lvm, 4 * N); A_(lvp, 4 * N);
+  }
   A_(chit, N); A_(Epp, N); A_(Et, N);
   const size_t lx = (size_t)ny, ly = (size_t)nx;
   A_(bline, (4 + R) * (lx + ly) + (lx + 1) + (ly + 1));

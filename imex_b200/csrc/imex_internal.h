@@ -118,6 +118,9 @@ struct imex_ctx {
   // implicit-solve planes
   double *hh = nullptr, *eta = nullptr, *vscale = nullptr, *tdiag = nullptr, *vdiag = nullptr;
   double *rv = nullptr;    // rho v* snapshot (3 planes)
+  // local Lax-Friedrichs face viscosities (GLF off, else null), 4 planes each: the magnetic
+  // operator's and the pressure operator's, built before their solves (k_local_visc)
+  double *lvm = nullptr, *lvp = nullptr;
   double *pb = nullptr, *pp = nullptr, *pf = nullptr, *pg = nullptr, *pdp = nullptr;  // pressure vectors
   double *mx = nullptr, *mb = nullptr;  // magnetic solution / rhs (3 planes each)
   double *chit = nullptr, *Epp = nullptr, *Et = nullptr;

@@ -215,18 +215,60 @@ struct TileBuf {
   T p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
 };
 
+// ------------------------------------------------------------------ L2 prefetch
+// The solver passes are bound by the latency of their global loads, not by bandwidth: a
+// CTA stages one tile at a time and each thread keeps few loads in flight.  Before a CTA
+// starts a tile it asks the L2 to fetch the rows of its next tile (plus halo) of every
+// plane that tile reads (cp.async.bulk.prefetch.L2: it holds no registers and nothing
+// waits for it), so that the next tile's loads hit the L2 instead of DRAM.  A row range
+// is trimmed inward to 16-byte boundaries (the instruction's alignment rule) and never
+// leaves its row; halo columns that wrap around a periodic edge are left out.  The rows
+// of the call are spread over the CTA's threads from a running item counter, which every
+// thread advances alike.
+struct PrefetchTile {
+  const Tiling* T;
+  int x0, y0, halo, xs, xe;
+  int item;  // the CTA-wide item counter
+  __device__ __forceinline__ PrefetchTile(const Tiling& t, int tile, int h) : T(&t), halo(h), item(0) {
+    x0 = (tile % t.tiles_x) * TX;
+    y0 = (tile / t.tiles_x) * TY;
+    xs = x0 - h < 0 ? 0 : x0 - h;
+    xe = x0 + TX + h > t.nx ? t.nx : x0 + TX + h;
+  }
+  // rows of nplanes consecutive planes of N elements of type E, starting at base
+  template <class E>
+  __device__ __forceinline__ void operator()(const E* base, int nplanes, bool interior_only = false) {
+    const int h = interior_only ? 0 : halo;
+    const int rows = TY + 2 * h, total = nplanes * rows;
+    const int a = (xs > x0 - h ? xs : x0 - h), b = (xe < x0 + TX + h ? xe : x0 + TX + h);
+    const long long N = T->N;
+    int k = (int)((threadIdx.x + NT - (unsigned)(item % NT)) % NT);
+    for (; k < total; k += NT) {
+      const int plane = k / rows, ry = k % rows;
+      int gj = y0 - h + ry;
+      if (gj < 0 || gj >= T->ny) gj = T->yclamp ? (gj < 0 ? 0 : T->ny - 1) : wrapc(gj, T->ny);
+      const E* row = base + (long long)plane * N + (long long)gj * T->nx;
+      const unsigned long long s = ((unsigned long long)(row + a) + 15ull) & ~15ull;
+      const unsigned long long e = (unsigned long long)(row + b) & ~15ull;
+      if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((unsigned)(e - s)) : "memory");
+    }
+    item += total;
+  }
+};
+
 // ------------------------------------------------------------------ operators
 // Each operator is a template on its arithmetic type T: double is the plain FP64
 // path (the same operations, in the same order, as the reference), float the
 // operator of the inner solves of the mixed-precision form.  Coefficients are
 // read from the FP64 planes and rounded to T when a tile is staged.
 //
-// Pressure_Subsystem_AX (implicit_operators.cpp:505-616), GLF viscosity, periodic,
+// Pressure_Subsystem_AX (implicit_operators.cpp:505-616), GLF or local viscosity,
 // with the frozen coefficient planes of one solve; precP (implicit_operators.cpp:650-662).
 struct PressureCoef {
   DevParams P;
   const DevScalars* sc;
   const double *hh, *eta, *rho, *vscale, *tdiag, *vdiag;
+  const double* lv;  // local dissipation (GLF off): K of the faces x+, x-, y+, y- (k_local_visc), else null
   double h, hh2, idx2, idy2, nu_x, nu_y, cvx, cvy, a;
   int jac;
   // step scalars of the current sub-step (h, GLF viscosity), read from device memory
@@ -268,6 +310,16 @@ struct PressureOpT : PressureCoef {
     q[0] = (T)__ldg(hh + c);
     q[1] = (T)__ldg(eta + c);
   }
+  // the planes a tile reads (for the L2 prefetch): staged on the halo, then per cell
+  template <class PF>
+  __device__ __forceinline__ void coef_planes(PF& pf) const {
+    pf(hh, 1);
+    pf(eta, 1);
+    pf(vscale, 1, true);
+    pf(tdiag, 1, true);
+    if (jac) pf(vdiag, 1, true);
+    if (lv) pf(lv, 4, true);
+  }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>
@@ -282,9 +334,17 @@ struct PressureOpT : PressureCoef {
     const T Vd = jac ? (T)__ldcg(vdiag + c) : (T)a;
     T r = Vd * xc - (T)hh2 * ((T)idx2 * (hf * (hp0 + h00) * (xe - xc) - hf * (h00 + hm0) * (xc - xw)) +
                               (T)idy2 * (hf * (h0p + h00) * (xn - xc) - hf * (h0m + h00) * (xc - xs)));
-    const T ec = eq[o], ee = eq[o + 1], ew = eq[o - 1], en = eq[o + sx], es = eq[o - sx];
-    T lap = (T)cvx * (hf * (ee + ec) * (xe - xc) - hf * (ec + ew) * (xc - xw)) +
+    T lap;
+    if (lv) {  // implicit_operators.cpp:584-607
+      const long long N = P.N;
+      const T kxp = (T)__ldg(lv + c), kxm = (T)__ldg(lv + N + c);
+      const T kyp = (T)__ldg(lv + 2 * N + c), kym = (T)__ldg(lv + 3 * N + c);
+      lap = (T)idx2 * (kxp * (xe - xc) - kxm * (xc - xw)) + (T)idy2 * (kyp * (xn - xc) - kym * (xc - xs));
+    } else {
+      const T ec = eq[o], ee = eq[o + 1], ew = eq[o - 1], en = eq[o + sx], es = eq[o - sx];
+      lap = (T)cvx * (hf * (ee + ec) * (xe - xc) - hf * (ec + ew) * (xc - xw)) +
             (T)cvy * (hf * (en + ec) * (xn - xc) - hf * (ec + es) * (xc - xs));
+    }
     out[0] = r - (T)__ldg(vscale + c) * (T)h * lap;
   }
   __device__ __forceinline__ void precond(long long c, T* v) const {
@@ -326,6 +386,11 @@ struct EnergyOpT : EnergyCoef {
     return o;
   }
   __device__ __forceinline__ void coef(long long c, T* q) const { q[0] = (T)__ldg(hh + c); }
+  template <class PF>
+  __device__ __forceinline__ void coef_planes(PF& pf) const {
+    pf(hh, 1);
+    pf(tdiag, 1, true);
+  }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>
@@ -345,11 +410,12 @@ struct EnergyOpT : EnergyCoef {
 };
 using EnergyOp = EnergyOpT<double>;
 
-// Magnetic_Subsystem_AX (implicit_operators.cpp:141-353), GLF viscosity, periodic.
+// Magnetic_Subsystem_AX (implicit_operators.cpp:141-353), GLF or local viscosity.
 struct MagneticBCoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
+  const double* lv;  // local dissipation (GLF off): nu of the faces x+, x-, y+, y- (k_local_visc), else null
   double h, nu_x, nu_y, cx, cy;
   __device__ __forceinline__ void bind() {
     h = sc->h;
@@ -379,11 +445,32 @@ struct MagneticBOpT : MagneticBCoef {
     q[2] = (T)__ldg(Qe + 7 * P.N + c);
     q[3] = (T)__ldg(rho + c);
   }
+  template <class PF>
+  __device__ __forceinline__ void coef_planes(PF& pf) const {
+    pf(Qe + 5 * P.N, 3);
+    pf(rho, 1);
+    if (lv) pf(lv, 4, true);
+  }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   __device__ __forceinline__ void precond(long long, T*) const {}
+  // the viscous Laplacian of one component x at staged cell o: the GLF form with the global
+  // coefficients cxT = B_max_x dx / dx^2, cyT (implicit_operators.cpp:311-320), or the face
+  // viscosities of the local form (implicit_operators.cpp:346-352)
+  __device__ __forceinline__ T visc(const T* x, long long c, int o, int sx, T cxT, T cyT) const {
+    const T two = T(2), one = T(1);
+    if (lv) {
+      const long long N = P.N;
+      const T dx = (T)P.dx, dy = (T)P.dy;
+      const T nxp = (T)__ldg(lv + c), nxm = (T)__ldg(lv + N + c);
+      const T nyp = (T)__ldg(lv + 2 * N + c), nym = (T)__ldg(lv + 3 * N + c);
+      return one / (dx * dx) * (nxp * (x[o + 1] - x[o]) - nxm * (x[o] - x[o - 1])) +
+             one / (dy * dy) * (nyp * (x[o + sx] - x[o]) - nym * (x[o] - x[o - sx]));
+    }
+    return cxT * (x[o - 1] - two * x[o] + x[o + 1]) + cyT * (x[o - sx] - two * x[o] + x[o + sx]);
+  }
   template <class TB>
-  __device__ void matvec(const TB& tb, int lx, int ly, long long, T* out) const {
+  __device__ void matvec(const TB& tb, int lx, int ly, long long c, T* out) const {
     constexpr int SX = TB::SX, SN = TB::SN;
     const T dx = (T)P.dx, dy = (T)P.dy, hT = (T)h, cxT = (T)cx, cyT = (T)cy;
     const T hf = T(0.5), qf = T(0.25), one = T(1), two = T(2);
@@ -436,7 +523,7 @@ struct MagneticBOpT : MagneticBCoef {
                      (one / dx * ((Wpm - Bxn_pm * Bx_pm) - (Wmm - Bxn_mm * Bx_mm)) -
                       one / dy * (q6[o] * x5[o] - q6[S] * x5[S]));
       const T ax5 = x5[o] + (hT * hT / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
-      out[0] = ax5 - hT * (cxT * (x5[W] - two * x5[o] + x5[E]) + cyT * (x5[S] - two * x5[o] + x5[No]));
+      out[0] = ax5 - hT * visc(x5, c, o, SX, cxT, cyT);
     }
     const T QXe = QX(E), QXw = QX(W);
     {  // y component (implicit_operators.cpp:277-285)
@@ -453,7 +540,7 @@ struct MagneticBOpT : MagneticBCoef {
                      (-one / dx * (q5[o] * x6[o] - q5[W] * x6[W]) +
                       one / dy * ((Wmp - Byn_mp * By_mp) - (Wmm - Byn_mm * By_mm)));
       const T ax6 = x6[o] + (hT * hT / dx) * ((By_1 + By_2) - (By_3 + By_4));
-      out[1] = ax6 - hT * (cxT * (x6[W] - two * x6[o] + x6[E]) + cyT * (x6[S] - two * x6[o] + x6[No]));
+      out[1] = ax6 - hT * visc(x6, c, o, SX, cxT, cyT);
     }
     {  // z component (implicit_operators.cpp:288-306)
       const T QXn = QX(No), QXs = QX(S);
@@ -479,7 +566,7 @@ struct MagneticBOpT : MagneticBCoef {
                      (-one / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - one / dy * (q6[o] * x7[o] - q6[S] * x7[S]));
       const T ax7 =
           x7[o] + hT * hT / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + hT * hT / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
-      out[2] = ax7 - hT * (cxT * (x7[W] - two * x7[o] + x7[E]) + cyT * (x7[S] - two * x7[o] + x7[No]));
+      out[2] = ax7 - hT * visc(x7, c, o, SX, cxT, cyT);
     }
 #undef FA
 #undef CA
@@ -488,7 +575,7 @@ struct MagneticBOpT : MagneticBCoef {
 };
 using MagneticBOp = MagneticBOpT<double>;
 
-// Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355-503), GLF, periodic.
+// Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355-503), GLF or local viscosity.
 // The reference evaluates B = curl A and the stress tensor T^B at the four
 // neighbours of each cell; those values are exactly curl A and T^B of the
 // neighbouring cells, so the tile pre-pass computes them once per cell (same
@@ -497,6 +584,7 @@ struct MagneticACoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
+  const double* lv;  // local dissipation (GLF off): nu of the faces x+, x-, y+, y- (k_local_visc), else null
   double h, nu_x, nu_y, cx, cy;
   int add_bvisc;
   __device__ __forceinline__ void bind() {
@@ -527,6 +615,12 @@ struct MagneticAOpT : MagneticACoef {
     q[0] = (T)__ldg(Qe + 5 * P.N + c);
     q[1] = (T)__ldg(Qe + 6 * P.N + c);
     q[2] = (T)__ldg(Qe + 7 * P.N + c);
+  }
+  template <class PF>
+  __device__ __forceinline__ void coef_planes(PF& pf) const {
+    pf(Qe + 5 * P.N, 3);
+    pf(rho, 1, true);
+    if (lv && add_bvisc) pf(lv, 4, true);
   }
   __device__ __forceinline__ void precond(long long, T*) const {}
   // bound_cond_A on the staged vector: the operator reads AG = bound_cond_A(x)
@@ -619,11 +713,22 @@ struct MagneticAOpT : MagneticACoef {
     const T cross_x = By * Fz - Bz * Fy;
     const T cross_y = Bz * Fx - Bx * Fz;
     const T cross_z = Bx * Fy - By * Fx;
+    T nxp = T(0), nxm = T(0), nyp = T(0), nym = T(0);
+    if (lv && add_bvisc) {
+      const long long N = P.N;
+      nxp = (T)__ldg(lv + c);
+      nxm = (T)__ldg(lv + N + c);
+      nyp = (T)__ldg(lv + 2 * N + c);
+      nym = (T)__ldg(lv + 3 * N + c);
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const T* A = tb.s + k * SN;
       T lap = T(0);
-      if (add_bvisc)
+      if (add_bvisc && lv)  // implicit_operators.cpp:481-490
+        lap = T(1) / (dx * dx) * (nxp * (A[o + 1] - A[o]) - nxm * (A[o] - A[o - 1])) +
+              T(1) / (dy * dy) * (nyp * (A[o + SX] - A[o]) - nym * (A[o] - A[o - SX]));
+      else if (add_bvisc)
         lap = (T)cx * (A[o - 1] - two * A[o] + A[o + 1]) + (T)cy * (A[o - SX] - two * A[o] + A[o + SX]);
       const T cr = k == 0 ? cross_x : (k == 1 ? cross_y : cross_z);
       out[k] = A[o] - hT * cr - hT * lap;
@@ -761,7 +866,15 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
   auto count = [&](int vals, int cvals) {
     if (lead) g.st->alg_bytes[g.fam] += ((double)vals * sizeof(TS) + (double)cvals * 8.0) * (double)N;
   };
-  (void)HALO;
+  // L2 prefetch of the rows of this CTA's next tile: the vectors named by vecs, then the
+  // operator's coefficient planes
+  auto prefetch_next = [&](int t, auto&& vecs) {
+    const int tn = t + g.nblk;
+    if (tn >= T.ntiles) return;
+    PrefetchTile pf(T, tn, HALO);
+    vecs(pf);
+    op.coef_planes(pf);
+  };
   x_written = false;
   if (threadIdx.x == 0) S.nalpha = 0;
 
@@ -773,6 +886,9 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        prefetch_next(t, [&](PrefetchTile& pf) {
+          pf(b, M);
+        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -834,6 +950,10 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        prefetch_next(t, [&](PrefetchTile& pf) {
+          pf(x, M);
+          pf(b, M, true);
+        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -883,6 +1003,9 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        prefetch_next(t, [&](PrefetchTile& pf) {
+          pf(Vp(0), M);
+        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -927,6 +1050,10 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       const double sj = S.sigma[j];
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        prefetch_next(t, [&](PrefetchTile& pf) {
+          pf(AVp(j), M);
+          pf(Vp(0), (j + 1) * M);
+        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
           const TS* AVj = AVp(j);
           double wv[FQ][M];
@@ -1209,6 +1336,13 @@ __device__ __forceinline__ void mixed_solve(Op64 op, GmresWorkT<float> g, double
     wacc_clear(S.acc);
     for (int t = grank(g); t < T.ntiles; t += g.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+      if (t + g.nblk < T.ntiles) {  // L2 prefetch of the next tile (PrefetchTile)
+        PrefetchTile pfx(T, t + g.nblk, Op64::HALO);
+        pfx(x_cur, M);
+        if (pending) pfx(g.V, S.nalpha * M);
+        pfx(b, M, true);
+        op.coef_planes(pfx);
+      }
       fill_tile(op, sm.tb.d, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
         for (int r = 0; r < FQ; ++r)
@@ -1438,6 +1572,17 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
     wacc_clear(S.acc);
     for (int t = grank(gw); t < T.ntiles; t += gw.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+      if (t + gw.nblk < T.ntiles) {  // L2 prefetch of the next tile (PrefetchTile)
+        PrefetchTile pfx(T, t + gw.nblk, PressureOp::HALO);
+        pfx(pf_cur, 1);
+        if (pending) {
+          if (dp_live) pfx(na.dp, 1);
+          pfx(gw.V, S.nalpha);
+        }
+        pfx(op.rho, 1, true);
+        pfx(na.b, 1, true);
+        L.coef_planes(pfx);
+      }
       fill_tile(L, tb, T, x0, y0, [&](const long long* c, double (*v)[1]) {
         if (pending) {
 #pragma unroll
@@ -1780,7 +1925,24 @@ __global__ void k_magnetic_rhs_B(DevParams P, const DevScalars* __restrict__ sc,
   x0[N + n] = Qe[6 * N + n];
   x0[2 * N + n] = Qe[7 * N + n];
 }
-// CollectMagFluxes (ct_flux.cpp:5-130), GLF (collect_cell)
+// ---- local Lax-Friedrichs dissipation (GLF off)
+// The speed of cell m along dir (0: x, 1: y) from its conserved state Q:
+// 0.5 (|v| + sqrt(v^2 + 4 |B|^2 / rho)) of prim(Q) (implicit_operators.cpp:324-335, 473-480,
+// ct_flux.cpp:81-84)
+__device__ __forceinline__ double lf_speed(const double* __restrict__ Q, long long N, long long m, int dir) {
+  const double rho = __ldg(Q + m), vm = __ldg(Q + (1 + dir) * N + m);
+  const double b5 = __ldg(Q + 5 * N + m), b6 = __ldg(Q + 6 * N + m), b7 = __ldg(Q + 7 * N + m);
+  const double v = vm / rho;
+  return 0.5 * (fabs(v) + sqrt(v * v + 4.0 * (b5 * b5 + b6 * b6 + b7 * b7) / rho));
+}
+// the pressure viscosity's speed of cell m: |v_dir| (MaterialSpeedp) or |B_dir| / sqrt(rho)
+// (AlfvenSpeedp) of prim(Q) (implicit_operators.cpp:587-597)
+__device__ __forceinline__ double pv_speed(const DevParams& P, const double* __restrict__ Q, long long N, long long m,
+                                           int dir) {
+  if (P.add_pvisc == IMEX_MaterialSpeedp) return fabs(__ldg(Q + (1 + dir) * N + m) / __ldg(Q + m));
+  return fabs(__ldg(Q + (5 + dir) * N + m) / sqrt(__ldg(Q + m)));
+}
+// CollectMagFluxes (ct_flux.cpp:5-130) (collect_cell), GLF or local dissipation
 __global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                      const double* __restrict__ Qe, const double* __restrict__ pe,
                                      double* __restrict__ Fx, double* __restrict__ Fy) {
@@ -1791,7 +1953,11 @@ __global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__
   neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
   const double* arr[3] = {ucon, Qe, pe};
   auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
-  const double bmax[2] = {sc->B_max_x, sc->B_max_y};
+  double bmax[2] = {sc->B_max_x, sc->B_max_y};
+  if (!P.GLF) {  // the larger speed of the two cells of each face (ct_flux.cpp:79-87, 114-122)
+    bmax[0] = fmax(lf_speed(Qe, N, n, 0), lf_speed(Qe, N, nb[NB_E], 0));
+    bmax[1] = fmax(lf_speed(Qe, N, n, 1), lf_speed(Qe, N, nb[NB_N], 1));
+  }
   double out[2];
   collect_cell<double>(P, sc->h, bmax, nb, ld, out);
   Fx[n] = out[0];
@@ -1886,6 +2052,46 @@ __global__ void k_gmax_finalize(const double* __restrict__ partial, int nblk, De
     sc->gmax_bx = a;
     sc->gmax_by = b;
   }
+}
+// ---- face viscosities of the local dissipation
+enum { LV_MAG_B = 0, LV_MAG_A = 1, LV_PRES = 2 };
+// The face viscosities of one solve, frozen like its other coefficients: plane f of lv holds,
+// for every cell, the face x+ (f = 0), x- (1), y+ (2) or y- (3), as the operator multiplies it.
+//   LV_MAG_B: max(b_c, b_nb) d from prim(Qe)        (implicit_operators.cpp:323-345)
+//   LV_MAG_A: (b_c + b_nb) / 2 d from prim(Qs)      (implicit_operators.cpp:472-486)
+//   LV_PRES:  (eta_nb + eta_c) / 2 max(s_c, s_nb) d (implicit_operators.cpp:584-607)
+// d is dx for the x faces and dy for the y faces; a neighbour outside a transmissive
+// direction is the nearest interior cell.
+__global__ void k_local_visc(DevParams P, int mode, const double* __restrict__ Q, const double* __restrict__ eta,
+                             double* __restrict__ lv) {
+  const long long N = P.N;
+  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  const long long nbr[4] = {cid(P, i + 1, j), cid(P, i - 1, j), cid(P, i, j + 1), cid(P, i, j - 1)};
+  double own[2], out[4];
+  if (mode == LV_PRES) {
+    own[0] = pv_speed(P, Q, N, n, 0);
+    own[1] = pv_speed(P, Q, N, n, 1);
+    const double ec = __ldg(eta + n);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const int dir = f >> 1;
+      const double nu = fmax(own[dir], pv_speed(P, Q, N, nbr[f], dir)) * (dir ? P.dy : P.dx);
+      out[f] = 0.5 * (__ldg(eta + nbr[f]) + ec) * nu;
+    }
+  } else {
+    own[0] = lf_speed(Q, N, n, 0);
+    own[1] = lf_speed(Q, N, n, 1);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const int dir = f >> 1;
+      const double b = lf_speed(Q, N, nbr[f], dir), d = dir ? P.dy : P.dx;
+      out[f] = mode == LV_MAG_B ? fmax(own[dir], b) * d : 0.5 * (own[dir] + b) * d;
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 4; ++f) lv[f * N + n] = out[f];
 }
 // B = curl A after the A solve (imex_subsystems.cpp:65-72)
 template <bool kOpen>
@@ -2066,6 +2272,7 @@ PressureOp make_pressure_op(imex_ctx* ctx) {
   op.vscale = ctx->vscale;
   op.tdiag = ctx->tdiag;
   op.vdiag = ctx->vdiag;
+  op.lv = ctx->P.add_pvisc == IMEX_Noaddvisp ? nullptr : ctx->lvp;
   op.jac = 0;
   return op;
 }
@@ -2083,6 +2290,7 @@ MagneticBOp make_magB_op(imex_ctx* ctx) {
   op.sc = ctx->sc;
   op.Qe = ctx->Qe;
   op.rho = ctx->cons;
+  op.lv = ctx->lvm;
   return op;
 }
 template <bool kOpen = false>
@@ -2092,6 +2300,7 @@ MagneticAOpT<double, kOpen> make_magA_op(imex_ctx* ctx) {
   op.sc = ctx->sc;
   op.Qe = ctx->Qe;
   op.rho = ctx->cons;
+  op.lv = ctx->lvm;
   op.add_bvisc = ctx->P.add_bvisc;
   return op;
 }
@@ -2127,6 +2336,23 @@ imex_status energy_momentum(imex_ctx* ctx) {
   prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
   return IMEX_OK;
 }
+// the face viscosities of the local dissipation (GLF off) for the magnetic solve (from Qe,
+// or Qs in the A form) or the pressure solve (from Qe and eta); nothing with GLF
+imex_status local_visc(imex_ctx* ctx, int mode) {
+  const DevParams& P = ctx->P;
+  if (P.GLF || (mode == LV_PRES && P.add_pvisc == IMEX_Noaddvisp)) return IMEX_OK;
+  const int nb = blocks_for(P.N);
+  prof_begin(ctx);
+  if (mode == LV_PRES)
+    k_local_visc<<<nb, kThreads, 0, ctx->stream>>>(P, mode, ctx->Qe, ctx->eta, ctx->lvp);
+  else
+    k_local_visc<<<nb, kThreads, 0, ctx->stream>>>(P, mode, mode == LV_MAG_A ? ctx->Qs : ctx->Qe, nullptr, ctx->lvm);
+  LAUNCH_CHECK(ctx, "k_local_visc");
+  prof_end(ctx, mode == LV_PRES ? F_PRES_SETUP : F_MAG_RHS, BYTES(mode == LV_PRES ? 8 : 10), 1);
+  return IMEX_OK;
+}
+int mag_visc_mode(const imex_ctx* ctx) { return ctx->P.magfield == IMEX_PotentialA ? LV_MAG_A : LV_MAG_B; }
+
 imex_status pressure_setup(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
@@ -2137,7 +2363,9 @@ imex_status pressure_setup(imex_ctx* ctx) {
   IMEX_LAUNCH_BC(P, k_pressure_tdiag, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->hh, ctx->tdiag);
   LAUNCH_CHECK(ctx, "k_pressure_tdiag");
   prof_end(ctx, F_PRES_SETUP, BYTES(12 + 2), 2);
-  return launch_shock(ctx, ctx->Qe, ctx->eta);
+  imex_status s = launch_shock(ctx, ctx->Qe, ctx->eta);
+  if (s != IMEX_OK) return s;
+  return local_visc(ctx, LV_PRES);
 }
 
 // One GMRES solve with operator o: the plain FP64 kernel, or in the mixed form the FP64
@@ -2524,6 +2752,8 @@ namespace {
 imex_status mag_rhs(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
+  imex_status s = local_visc(ctx, mag_visc_mode(ctx));
+  if (s != IMEX_OK) return s;
   if (P.magfield == IMEX_PotentialA) {
     if (!ctx->gmax_ready) {  // the stage combination did not take the maxima of this Qs
       int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
@@ -2669,6 +2899,9 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
     k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
     LAUNCH_CHECK(ctx, "k_gmax");
   }
+  if ((op == IMEX_OP_MAGNETIC_A || op == IMEX_OP_MAGNETIC_B) &&
+      (s = local_visc(ctx, op == IMEX_OP_MAGNETIC_A ? LV_MAG_A : LV_MAG_B)) != IMEX_OK)
+    return s;
   if ((s = set_h(ctx, h)) != IMEX_OK) return s;
   if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
     // the Qe pressure / enthalpy planes come from the stage combination; rebuild them here
@@ -2836,6 +3069,8 @@ struct AssembledTOp {
     return *this;
   }
   __device__ __forceinline__ void coef(long long, double* q) const { q[0] = 0.0; }
+  template <class PF>
+  __device__ __forceinline__ void coef_planes(PF&) const {}
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>

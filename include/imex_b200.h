@@ -109,7 +109,7 @@ typedef struct imex_config {
   int magfield;        /* imex_magfield            (config.hpp:45) */
   int add_pvisc;       /* imex_add_pvisc           (config.hpp:46) */
   int flux_diss;       /* imex_flux_diss           (config.hpp:47) */
-  int GLF;             /* global Lax-Friedrichs dissipation (config.hpp:48) */
+  int GLF;             /* 1: global Lax-Friedrichs dissipation; 0: local, per face (config.hpp:48) */
   int add_bvisc;       /* A-form numerical viscosity (config.hpp:49) */
   int U_update;        /* imex_energy_update       (config.hpp:50) */
   int vortex_test;     /* nonzero reproduces `test == testMHD_vortex` (Minmod y-slope special case) */

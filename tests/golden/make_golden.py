@@ -10,12 +10,14 @@ the reference sources by `make -C oracle ref`) on small analytic inputs:
                      boundary normal faces (Bx at x_0, By at y_0);
   fn_<case>.npz    - single reference functions on fixed inputs:
                      TVDReconstruction, ShockDetector and the four matrix-free
-                     operators of implicit_operators.cpp;
+                     operators of implicit_operators.cpp (fn_local_*: the operators
+                     with the local dissipation, on the same inputs);
   adjoint_ref_fd64.npz - central finite differences of the reference's J on the
                      adjoint workload at 64 x 64 (50 steps, all 32 amplitudes).
 
 Run from the repository root:  python tests/golden/make_golden.py [case ...]
-(no arguments: every case; otherwise only the named step cases and/or "fn", "adjoint_fd").
+(no arguments: every case; otherwise only the named step cases and/or "fn", "fn_local",
+"adjoint_fd").
 """
 from __future__ import annotations
 
@@ -162,6 +164,25 @@ ADJ_SETTINGS = dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-14, fixed
 ADJ_N, ADJ_STEPS, ADJ_H = 64, 50, 1e-6
 
 
+def fn_local_case() -> None:
+    """The matrix-free operators with the local dissipation (GLF = false) on the inputs of
+    fn_vortex16x12.npz (implicit_operators.cpp:311-353, 472-490, 584-607)."""
+    g = dict(np.load(os.path.join(HERE, "fn_vortex16x12.npz")))
+    prob = vortex(16, 12)
+    args = (g["ucon"], g["Q"], g["Qs"], float(g["h"]))
+    out = {}
+    for name, settings in (("", {}), ("_alfven", dict(add_pvisc="AlfvenSpeedp"))):
+        s = make_solver("ref", prob, 2, dict(CFG0, GLF=0, **settings))
+        s.set_scalars(*(float(v) for v in g["scalars"]))
+        out[f"op_pressure_L{name}"] = s.operator(0, *args, g["x1"])
+        out[f"op_pressure_J{name}"] = s.operator(1, *args, g["x1"], pfreeze=g["pfreeze"], mbig=float(g["mbig"]))
+    out["op_magnetic_B"] = s.operator(2, *args, g["x3"])
+    sa = make_solver("ref", prob, 2, dict(CFG1, GLF=0))
+    sa.set_scalars(*(float(v) for v in g["scalars"]))
+    out["op_magnetic_A"] = sa.operator(3, *args, g["x3"])
+    np.savez_compressed(os.path.join(HERE, "fn_local_vortex16x12.npz"), **out)
+
+
 def _adj_J(args):
     """J of the reference solver on the perturbed vortex with amplitudes a (one process each)."""
     a, rho_t, B_t = args
@@ -213,6 +234,9 @@ def main() -> None:
     if not only or "fn" in only:
         fn_case()
         print("wrote fn_vortex16x12")
+    if not only or "fn" in only or "fn_local" in only:
+        fn_local_case()
+        print("wrote fn_local_vortex16x12")
     if not only or "adjoint_fd" in only:
         adjoint_fd_case()
         print("wrote adjoint_ref_fd64")

@@ -73,7 +73,7 @@ def test_defaults_are_the_reference_defaults():
 
 @pytest.mark.parametrize("override,status", [
     (dict(x_bc=1), 2), (dict(x_bc=3), 2), (dict(y_bc=4), 2), (dict(y_bc=1), 2),
-    (dict(formula=2), 1), (dict(GLF=0), 2),
+    (dict(formula=2), 1),
     (dict(U_update=5), 1), (dict(arith=2), 1), (dict(RKs=4), 1), (dict(gmres_restart=31), 1),
     (dict(gmres_restart=0), 1), (dict(recon=7), 1), (dict(x_0=1.0, x_1=0.0), 1),
 ])

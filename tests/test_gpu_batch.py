@@ -53,6 +53,16 @@ def test_batch_members_match_single_runs_and_oracle():
     batch.close()
 
 
+def test_batch_local_dissipation_members_match_single_runs_and_oracle():
+    """GLF = false: every member builds its own face viscosities before the batched solves."""
+    probs = _members()[:3]
+    settings = dict(CFG0, GLF=0, add_pvisc="AlfvenSpeedp")
+    batch = ix.Batch(probs, 2, settings)
+    batch.step(2)
+    _check_members(batch, probs, 2, settings, 2, 1e-11, 1e-10)
+    batch.close()
+
+
 def test_batch_without_graph_matches_graph():
     probs = _members()[:3]
     a = ix.Batch(probs, 2, CFG0, streams=3, graph=True)

@@ -34,11 +34,14 @@ SUB_CASES = [
     (2, dict(recon="ENO3", magfield="NoDivFree", reconstate="PrimState")),
     (3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
     (2, dict(recon="Minmod", magfield="UnStaggerCT")),
+    (2, dict(recon="VanLeer", magfield="StaggerCT", GLF=0, add_pvisc="AlfvenSpeedp")),
+    (3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GLF=0)),
 ]
 
 
 @pytest.mark.parametrize("rks,settings", SUB_CASES, ids=["vanleer_ct", "weno5_ct_yper", "energy_xper", "eno3_nodiv",
-                                                        "weno5_potentialA", "minmod_unstag"])
+                                                        "weno5_potentialA", "minmod_unstag", "vanleer_ct_local",
+                                                        "weno5_potentialA_local"])
 def test_gpu_substeps_match_oracle_transmissive(rks, settings):
     prob = open_blast(40, 36)
     o = make_solver("port", prob, rks, settings)

@@ -29,6 +29,10 @@ CASES = [
      dict(recon="Minmod", magfield="StaggerCT", eos_type="REDLICH_KWONG", m_alfa=0.4275, m_b=0.0866), 4),
     ("vortex_energy", lambda: vortex(48), 2,
      dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula", GMREStol=1e-12), 5),
+    ("vortex_local_lf", lambda: vortex(48), 2,
+     dict(recon="VanLeer", magfield="StaggerCT", GLF=0, add_pvisc="AlfvenSpeedp", GMREStol=1e-12), 4),
+    ("sheet_local_lf", lambda: vortex_sheet(48), 3,
+     dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GLF=0, GMREStol=1e-12), 3),
 ]
 
 

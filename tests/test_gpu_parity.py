@@ -119,6 +119,34 @@ def test_gpu_operators_bit_exact(op, settings):
     sv.close()
 
 
+@pytest.mark.parametrize("op,settings", [
+    ("pressure_L", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("pressure_J", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("pressure_L_alfven", dict(recon="VanLeer", magfield="StaggerCT", add_pvisc="AlfvenSpeedp")),
+    ("pressure_J_alfven", dict(recon="VanLeer", magfield="StaggerCT", add_pvisc="AlfvenSpeedp")),
+    ("magnetic_B", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("magnetic_A", dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+])
+def test_gpu_local_dissipation_operators_bit_exact(op, settings):
+    """The operators with GLF = false (face viscosities from k_local_visc) against the
+    reference's on the inputs of the function fixture."""
+    g = load_golden("fn_vortex16x12.npz")
+    loc = load_golden("fn_local_vortex16x12.npz")
+    sv = _fn_solver(dict(settings, GLF=0))
+    dt, h, bmx, bmy, vxm, vym, amax = (float(v) for v in g["scalars"])
+    sv.set_scalars(dt=dt, adt=h, B_max_x=bmx, B_max_y=bmy, vx_max=vxm, vy_max=vym, a_max=amax)
+    sv.set_buffer("cons", g["ucon"])
+    sv.set_buffer("Qe", g["Q"])
+    sv.set_buffer("Qs", g["Qs"])
+    kind = op.replace("_alfven", "")
+    sv.prepare_operator(kind, float(g["h"]))
+    if kind == "pressure_J":
+        sv.set_newton_state(g["pfreeze"], float(g["mbig"]))
+    x = g["x3"] if op.startswith("magnetic") else g["x1"]
+    np.testing.assert_array_equal(sv.apply_operator(kind, x), loc[f"op_{op}"])
+    sv.close()
+
+
 SUB_CASES = [
     ("vortex", (32, 32), 2, dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12)),
     ("vortex", (20, 14), 2, dict(recon="Minmod", magfield="UnStaggerCT")),
@@ -129,6 +157,9 @@ SUB_CASES = [
     ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", formula="EnergyFormula", GMREStol=1e-12)),
     ("sheet", (24, 20), 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, formula="EnergyFormula")),
     ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", U_update="ConservationofU")),
+    ("vortex", (24, 20), 2, dict(recon="VanLeer", magfield="StaggerCT", GLF=0, add_pvisc="AlfvenSpeedp")),
+    ("sheet", (24, 20), 3, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5, GLF=0)),
+    ("vortex", (20, 14), 2, dict(recon="Minmod", magfield="UnStaggerCT", GLF=0, formula="EnergyFormula")),
 ]
 
 

@@ -64,6 +64,26 @@ def test_port_reproduces_reference_golden_functions():
     np.testing.assert_array_equal(s.operator(3, g["ucon"], g["Q"], g["Qs"], h, g["x3"]), g["op_magnetic_A"])
 
 
+def test_port_reproduces_reference_local_dissipation_operators():
+    """The four operators with GLF = false on the inputs of the function fixture."""
+    g = load_golden("fn_vortex16x12.npz")
+    loc = load_golden("fn_local_vortex16x12.npz")
+    from imex_b200.problems import vortex
+    prob = vortex(16, 12)
+    args = (g["ucon"], g["Q"], g["Qs"], float(g["h"]))
+    for name, extra in (("", {}), ("_alfven", dict(add_pvisc="AlfvenSpeedp"))):
+        s = make_solver("port", prob, 2, dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12, GLF=0, **extra))
+        s.set_scalars(*g["scalars"])
+        np.testing.assert_array_equal(s.operator(0, *args, g["x1"]), loc[f"op_pressure_L{name}"])
+        np.testing.assert_array_equal(s.operator(1, *args, g["x1"], pfreeze=g["pfreeze"], mbig=float(g["mbig"])),
+                                      loc[f"op_pressure_J{name}"])
+    np.testing.assert_array_equal(s.operator(2, *args, g["x3"]), loc["op_magnetic_B"])
+    sa = make_solver("port", prob, 2, dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5,
+                                           GMREStol=1e-12, GLF=0))
+    sa.set_scalars(*g["scalars"])
+    np.testing.assert_array_equal(sa.operator(3, *args, g["x3"]), loc["op_magnetic_A"])
+
+
 LIVE_CASES = [
     ("vortex", 20, 2, dict(recon="VanLeer", magfield="StaggerCT", GMREStol=1e-12), 2),
     ("vortex", 20, 2, dict(recon="Minmod", magfield="UnStaggerCT"), 2),
