@@ -215,47 +215,6 @@ struct TileBuf {
   T p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
 };
 
-// ------------------------------------------------------------------ L2 prefetch
-// The solver passes are bound by the latency of their global loads, not by bandwidth: a
-// CTA stages one tile at a time and each thread keeps few loads in flight.  Before a CTA
-// starts a tile it asks the L2 to fetch the rows of its next tile (plus halo) of every
-// plane that tile reads (cp.async.bulk.prefetch.L2: it holds no registers and nothing
-// waits for it), so that the next tile's loads hit the L2 instead of DRAM.  A row range
-// is trimmed inward to 16-byte boundaries (the instruction's alignment rule) and never
-// leaves its row; halo columns that wrap around a periodic edge are left out.  The rows
-// of the call are spread over the CTA's threads from a running item counter, which every
-// thread advances alike.
-struct PrefetchTile {
-  const Tiling* T;
-  int x0, y0, halo, xs, xe;
-  int item;  // the CTA-wide item counter
-  __device__ __forceinline__ PrefetchTile(const Tiling& t, int tile, int h) : T(&t), halo(h), item(0) {
-    x0 = (tile % t.tiles_x) * TX;
-    y0 = (tile / t.tiles_x) * TY;
-    xs = x0 - h < 0 ? 0 : x0 - h;
-    xe = x0 + TX + h > t.nx ? t.nx : x0 + TX + h;
-  }
-  // rows of nplanes consecutive planes of N elements of type E, starting at base
-  template <class E>
-  __device__ __forceinline__ void operator()(const E* base, int nplanes, bool interior_only = false) {
-    const int h = interior_only ? 0 : halo;
-    const int rows = TY + 2 * h, total = nplanes * rows;
-    const int a = (xs > x0 - h ? xs : x0 - h), b = (xe < x0 + TX + h ? xe : x0 + TX + h);
-    const long long N = T->N;
-    int k = (int)((threadIdx.x + NT - (unsigned)(item % NT)) % NT);
-    for (; k < total; k += NT) {
-      const int plane = k / rows, ry = k % rows;
-      int gj = y0 - h + ry;
-      if (gj < 0 || gj >= T->ny) gj = T->yclamp ? (gj < 0 ? 0 : T->ny - 1) : wrapc(gj, T->ny);
-      const E* row = base + (long long)plane * N + (long long)gj * T->nx;
-      const unsigned long long s = ((unsigned long long)(row + a) + 15ull) & ~15ull;
-      const unsigned long long e = (unsigned long long)(row + b) & ~15ull;
-      if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((unsigned)(e - s)) : "memory");
-    }
-    item += total;
-  }
-};
-
 // ------------------------------------------------------------------ operators
 // Each operator is a template on its arithmetic type T: double is the plain FP64
 // path (the same operations, in the same order, as the reference), float the
@@ -309,16 +268,6 @@ struct PressureOpT : PressureCoef {
   __device__ __forceinline__ void coef(long long c, T* q) const {
     q[0] = (T)__ldg(hh + c);
     q[1] = (T)__ldg(eta + c);
-  }
-  // the planes a tile reads (for the L2 prefetch): staged on the halo, then per cell
-  template <class PF>
-  __device__ __forceinline__ void coef_planes(PF& pf) const {
-    pf(hh, 1);
-    pf(eta, 1);
-    pf(vscale, 1, true);
-    pf(tdiag, 1, true);
-    if (jac) pf(vdiag, 1, true);
-    if (lv) pf(lv, 4, true);
   }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
@@ -386,11 +335,6 @@ struct EnergyOpT : EnergyCoef {
     return o;
   }
   __device__ __forceinline__ void coef(long long c, T* q) const { q[0] = (T)__ldg(hh + c); }
-  template <class PF>
-  __device__ __forceinline__ void coef_planes(PF& pf) const {
-    pf(hh, 1);
-    pf(tdiag, 1, true);
-  }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>
@@ -444,12 +388,6 @@ struct MagneticBOpT : MagneticBCoef {
     q[1] = (T)__ldg(Qe + 6 * P.N + c);
     q[2] = (T)__ldg(Qe + 7 * P.N + c);
     q[3] = (T)__ldg(rho + c);
-  }
-  template <class PF>
-  __device__ __forceinline__ void coef_planes(PF& pf) const {
-    pf(Qe + 5 * P.N, 3);
-    pf(rho, 1);
-    if (lv) pf(lv, 4, true);
   }
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
@@ -615,12 +553,6 @@ struct MagneticAOpT : MagneticACoef {
     q[0] = (T)__ldg(Qe + 5 * P.N + c);
     q[1] = (T)__ldg(Qe + 6 * P.N + c);
     q[2] = (T)__ldg(Qe + 7 * P.N + c);
-  }
-  template <class PF>
-  __device__ __forceinline__ void coef_planes(PF& pf) const {
-    pf(Qe + 5 * P.N, 3);
-    pf(rho, 1, true);
-    if (lv && add_bvisc) pf(lv, 4, true);
   }
   __device__ __forceinline__ void precond(long long, T*) const {}
   // bound_cond_A on the staged vector: the operator reads AG = bound_cond_A(x)
@@ -866,15 +798,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
   auto count = [&](int vals, int cvals) {
     if (lead) g.st->alg_bytes[g.fam] += ((double)vals * sizeof(TS) + (double)cvals * 8.0) * (double)N;
   };
-  // L2 prefetch of the rows of this CTA's next tile: the vectors named by vecs, then the
-  // operator's coefficient planes
-  auto prefetch_next = [&](int t, auto&& vecs) {
-    const int tn = t + g.nblk;
-    if (tn >= T.ntiles) return;
-    PrefetchTile pf(T, tn, HALO);
-    vecs(pf);
-    op.coef_planes(pf);
-  };
+  (void)HALO;
   x_written = false;
   if (threadIdx.x == 0) S.nalpha = 0;
 
@@ -886,9 +810,6 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        prefetch_next(t, [&](PrefetchTile& pf) {
-          pf(b, M);
-        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -950,10 +871,6 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        prefetch_next(t, [&](PrefetchTile& pf) {
-          pf(x, M);
-          pf(b, M, true);
-        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -1003,9 +920,6 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        prefetch_next(t, [&](PrefetchTile& pf) {
-          pf(Vp(0), M);
-        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -1050,10 +964,6 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       const double sj = S.sigma[j];
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
         const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-        prefetch_next(t, [&](PrefetchTile& pf) {
-          pf(AVp(j), M);
-          pf(Vp(0), (j + 1) * M);
-        });
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
           const TS* AVj = AVp(j);
           double wv[FQ][M];
@@ -1336,13 +1246,6 @@ __device__ __forceinline__ void mixed_solve(Op64 op, GmresWorkT<float> g, double
     wacc_clear(S.acc);
     for (int t = grank(g); t < T.ntiles; t += g.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      if (t + g.nblk < T.ntiles) {  // L2 prefetch of the next tile (PrefetchTile)
-        PrefetchTile pfx(T, t + g.nblk, Op64::HALO);
-        pfx(x_cur, M);
-        if (pending) pfx(g.V, S.nalpha * M);
-        pfx(b, M, true);
-        op.coef_planes(pfx);
-      }
       fill_tile(op, sm.tb.d, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
         for (int r = 0; r < FQ; ++r)
@@ -1572,17 +1475,6 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
     wacc_clear(S.acc);
     for (int t = grank(gw); t < T.ntiles; t += gw.nblk) {
       const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
-      if (t + gw.nblk < T.ntiles) {  // L2 prefetch of the next tile (PrefetchTile)
-        PrefetchTile pfx(T, t + gw.nblk, PressureOp::HALO);
-        pfx(pf_cur, 1);
-        if (pending) {
-          if (dp_live) pfx(na.dp, 1);
-          pfx(gw.V, S.nalpha);
-        }
-        pfx(op.rho, 1, true);
-        pfx(na.b, 1, true);
-        L.coef_planes(pfx);
-      }
       fill_tile(L, tb, T, x0, y0, [&](const long long* c, double (*v)[1]) {
         if (pending) {
 #pragma unroll
@@ -3069,8 +2961,6 @@ struct AssembledTOp {
     return *this;
   }
   __device__ __forceinline__ void coef(long long, double* q) const { q[0] = 0.0; }
-  template <class PF>
-  __device__ __forceinline__ void coef_planes(PF&) const {}
   template <class TB>
   __device__ __forceinline__ void prepass(TB&, int, int) const {}
   template <class TB>
