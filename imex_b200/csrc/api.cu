@@ -440,6 +440,7 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   A_(Hs, R * 8 * N); A_(HsA, R * 3 * N); A_(HsB, R * 2 * N); A_(w, 32 * N); A_(Bsave, 3 * N);
   A_(pe, N); A_(hQe, N);
   A_(hh, N); A_(eta, N); A_(vscale, N); A_(tdiag, N); A_(vdiag, N); A_(rv, 3 * N);
+  A_(irho, N);
   A_(pb, N); A_(pp, N); A_(pf, N); A_(pg, N); A_(pdp, N);
   A_(mx, 3 * N); A_(mb, 3 * N);
   if (!cfg->GLF) {

@@ -117,6 +117,7 @@ struct imex_ctx {
   double *hQe = nullptr;   // enthalpy e + p/rho of Qe
   // implicit-solve planes
   double *hh = nullptr, *eta = nullptr, *vscale = nullptr, *tdiag = nullptr, *vdiag = nullptr;
+  double* irho = nullptr;  // fast arithmetic: 1/rho of u_con for the A-form operator
   double *rv = nullptr;    // rho v* snapshot (3 planes)
   // local Lax-Friedrichs face viscosities (GLF off, else null), 4 planes each: the magnetic
   // operator's and the pressure operator's, built before their solves (k_local_visc)

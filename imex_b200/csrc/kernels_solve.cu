@@ -425,6 +425,12 @@ struct MagneticBOpT : MagneticBCoef {
     const T r0 = rr[o];
     const T rho_p0 = hf * (r0 + rr[E]), rho_m0 = hf * (r0 + rr[W]);
     const T rho_0p = hf * (r0 + rr[No]), rho_0m = hf * (r0 + rr[S]);
+    // B/rho on a face: the reference divides in every term; the fast arithmetic takes the
+    // four face reciprocals once and multiplies (a few ulp; the exact one keeps the divisions)
+    const bool fast = P.fast != 0;
+    const T ir_p0 = fast ? one / rho_p0 : T(0), ir_m0 = fast ? one / rho_m0 : T(0);
+    const T ir_0p = fast ? one / rho_0p : T(0), ir_0m = fast ? one / rho_0m : T(0);
+    auto bor = [&](T b, T rho, T ir) { return fast ? b * ir : b / rho; };
 #define FA(a, t) (hf * (a[o] + a[t]))
 #define CA(a, t1, t2, t3) (qf * (a[o] + a[t1] + a[t2] + a[t3]))
 #define QX(t) (hf * (q5[t] * x5[t] + q6[t] * x6[t] + q7[t] * x7[t]))
@@ -448,16 +454,16 @@ struct MagneticBOpT : MagneticBCoef {
     const T QXc = QX(o);
     {  // x component (implicit_operators.cpp:266-275)
       const T QXn = QX(No), QXs = QX(S);
-      const T Bx_1 = FA(q5, No) / rho_0p *
+      const T Bx_1 = bor(FA(q5, No), rho_0p, ir_0p) *
                      (one / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
                       one / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
-      const T Bx_2 = FA(q6, No) / rho_0p *
+      const T Bx_2 = bor(FA(q6, No), rho_0p, ir_0p) *
                      (one / dx * ((Wpp - Bxn_pp * Bx_pp) - (Wmp - Bxn_mp * Bx_mp)) -
                       one / dy * (q6[No] * x5[No] - q6[o] * x5[o]));
-      const T Bx_3 = FA(q5, S) / rho_0m *
+      const T Bx_3 = bor(FA(q5, S), rho_0m, ir_0m) *
                      (one / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
                       one / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
-      const T Bx_4 = FA(q6, S) / rho_0m *
+      const T Bx_4 = bor(FA(q6, S), rho_0m, ir_0m) *
                      (one / dx * ((Wpm - Bxn_pm * Bx_pm) - (Wmm - Bxn_mm * Bx_mm)) -
                       one / dy * (q6[o] * x5[o] - q6[S] * x5[S]));
       const T ax5 = x5[o] + (hT * hT / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
@@ -465,16 +471,16 @@ struct MagneticBOpT : MagneticBCoef {
     }
     const T QXe = QX(E), QXw = QX(W);
     {  // y component (implicit_operators.cpp:277-285)
-      const T By_1 = FA(q6, E) / rho_p0 *
+      const T By_1 = bor(FA(q6, E), rho_p0, ir_p0) *
                      (-one / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
                       one / dy * (Bxn_pp * By_pp - Bxn_pm * By_pm));
-      const T By_2 = FA(q5, E) / rho_p0 *
+      const T By_2 = bor(FA(q5, E), rho_p0, ir_p0) *
                      (-one / dx * (q5[E] * x6[E] - q5[o] * x6[o]) +
                       one / dy * ((Wpp - Byn_pp * By_pp) - (Wpm - Byn_pm * By_pm)));
-      const T By_3 = FA(q6, W) / rho_m0 *
+      const T By_3 = bor(FA(q6, W), rho_m0, ir_m0) *
                      (-one / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
                       one / dy * (Bxn_mp * By_mp - Bxn_mm * By_mm));
-      const T By_4 = FA(q5, W) / rho_m0 *
+      const T By_4 = bor(FA(q5, W), rho_m0, ir_m0) *
                      (-one / dx * (q5[o] * x6[o] - q5[W] * x6[W]) +
                       one / dy * ((Wmp - Byn_mp * By_mp) - (Wmm - Byn_mm * By_mm)));
       const T ax6 = x6[o] + (hT * hT / dx) * ((By_1 + By_2) - (By_3 + By_4));
@@ -482,25 +488,25 @@ struct MagneticBOpT : MagneticBCoef {
     }
     {  // z component (implicit_operators.cpp:288-306)
       const T QXn = QX(No), QXs = QX(S);
-      const T Bz_1 = FA(q7, E) / rho_p0 *
+      const T Bz_1 = bor(FA(q7, E), rho_p0, ir_p0) *
                      (-one / dx * ((QXe - q5[E] * x5[E]) - (QXc - q5[o] * x5[o])) +
                       one / dy * (Byn_pp * Bx_pp - Byn_pm * Bx_pm));
-      const T Bz_2 = FA(q5, E) / rho_p0 *
+      const T Bz_2 = bor(FA(q5, E), rho_p0, ir_p0) *
                      (-one / dx * (q5[E] * x7[E] - q5[o] * x7[o]) - one / dy * (Byn_pp * Bz_pp - Byn_pm * Bz_pm));
-      const T Bz_3 = FA(q7, W) / rho_m0 *
+      const T Bz_3 = bor(FA(q7, W), rho_m0, ir_m0) *
                      (-one / dx * ((QXc - q5[o] * x5[o]) - (QXw - q5[W] * x5[W])) +
                       one / dy * (Byn_mp * Bx_mp - Byn_mm * Bx_mm));
-      const T Bz_4 = FA(q5, W) / rho_m0 *
+      const T Bz_4 = bor(FA(q5, W), rho_m0, ir_m0) *
                      (-one / dx * (q5[o] * x7[o] - q5[W] * x7[W]) - one / dy * (Byn_mp * Bz_mp - Byn_mm * Bz_mm));
-      const T Bz_5 = FA(q7, No) / rho_0p *
+      const T Bz_5 = bor(FA(q7, No), rho_0p, ir_0p) *
                      (one / dx * (Bxn_pp * By_pp - Bxn_mp * By_mp) -
                       one / dy * ((QXn - q6[No] * x6[No]) - (QXc - q6[o] * x6[o])));
-      const T Bz_6 = FA(q6, No) / rho_0p *
+      const T Bz_6 = bor(FA(q6, No), rho_0p, ir_0p) *
                      (-one / dx * (Bxn_pp * Bz_pp - Bxn_mp * Bz_mp) - one / dy * (q6[No] * x7[No] - q6[o] * x7[o]));
-      const T Bz_7 = FA(q7, S) / rho_0m *
+      const T Bz_7 = bor(FA(q7, S), rho_0m, ir_0m) *
                      (one / dx * (Bxn_pm * By_pm - Bxn_mm * By_mm) -
                       one / dy * ((QXc - q6[o] * x6[o]) - (QXs - q6[S] * x6[S])));
-      const T Bz_8 = FA(q6, S) / rho_0m *
+      const T Bz_8 = bor(FA(q6, S), rho_0m, ir_0m) *
                      (-one / dx * (Bxn_pm * Bz_pm - Bxn_mm * Bz_mm) - one / dy * (q6[o] * x7[o] - q6[S] * x7[S]));
       const T ax7 =
           x7[o] + hT * hT / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + hT * hT / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
@@ -522,6 +528,7 @@ struct MagneticACoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
+  const double* irho;  // fast arithmetic: 1/rho (k_recip before the solve), else null
   const double* lv;  // local dissipation (GLF off): nu of the faces x+, x-, y+, y- (k_local_visc), else null
   double h, nu_x, nu_y, cx, cy;
   int add_bvisc;
@@ -606,6 +613,12 @@ struct MagneticAOpT : MagneticACoef {
   __device__ __forceinline__ void prepass(TB& tb, int x0, int y0) const {
     constexpr int SX = TB::SX, SN = TB::SN;
     const T dx = (T)P.dx, dy = (T)P.dy, two = T(2);
+    // central differences: a division by 2 dx in the reference; the fast arithmetic multiplies
+    // by the reciprocal taken once
+    const bool fast = P.fast != 0;
+    const T r2dx = T(1) / (two * dx), r2dy = T(1) / (two * dy);
+    auto cdx = [&](T d) { return fast ? d * r2dx : d / (two * dx); };
+    auto cdy = [&](T d) { return fast ? d * r2dy : d / (two * dy); };
     if constexpr (kOpen) extrapolate(tb, x0, y0);
     for (int q = threadIdx.x; q < TB::PN; q += NT) {
       const int px = q % TB::PX, py = q / TB::PX;
@@ -613,9 +626,9 @@ struct MagneticAOpT : MagneticACoef {
       const T* A0 = tb.s;
       const T* A1 = tb.s + SN;
       const T* A2 = tb.s + 2 * SN;
-      const T bx = (A2[o + SX] - A2[o - SX]) / (two * dy);
-      const T by = -(A2[o + 1] - A2[o - 1]) / (two * dx);
-      const T bz = (A1[o + 1] - A1[o - 1]) / (two * dx) - (A0[o + SX] - A0[o - SX]) / (two * dy);
+      const T bx = cdy(A2[o + SX] - A2[o - SX]);
+      const T by = cdx(-(A2[o + 1] - A2[o - 1]));
+      const T bz = cdx(A1[o + 1] - A1[o - 1]) - cdy(A0[o + SX] - A0[o - SX]);
       const T Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
       const T bdot = Bx * bx + By * by + Bz * bz;
       tb.p[0 * TB::PN + q] = bdot / two - Bx * bx;  // Txx
@@ -633,13 +646,14 @@ struct MagneticAOpT : MagneticACoef {
     const int o = (ly + 2) * SX + lx + 2;  // halo-2 tile
     const int p = (ly + 1) * PX + lx + 1;  // halo-1 pre-pass region
     const T* Tq = tb.p;
-    const T divT_x = (Tq[0 * PN + p + 1] - Tq[0 * PN + p - 1]) / (two * dx) +
-                     (Tq[3 * PN + p + PX] - Tq[3 * PN + p - PX]) / (two * dy);
-    const T divT_y = (Tq[1 * PN + p + 1] - Tq[1 * PN + p - 1]) / (two * dx) +
-                     (Tq[4 * PN + p + PX] - Tq[4 * PN + p - PX]) / (two * dy);
-    const T divT_z = (Tq[2 * PN + p + 1] - Tq[2 * PN + p - 1]) / (two * dx) +
-                     (Tq[5 * PN + p + PX] - Tq[5 * PN + p - PX]) / (two * dy);
-    const T hr = hT / (T)__ldg(rho + c);
+    const bool fast = P.fast != 0;
+    const T r2dx = T(1) / (two * dx), r2dy = T(1) / (two * dy);
+    auto cdx = [&](T d) { return fast ? d * r2dx : d / (two * dx); };
+    auto cdy = [&](T d) { return fast ? d * r2dy : d / (two * dy); };
+    const T divT_x = cdx(Tq[0 * PN + p + 1] - Tq[0 * PN + p - 1]) + cdy(Tq[3 * PN + p + PX] - Tq[3 * PN + p - PX]);
+    const T divT_y = cdx(Tq[1 * PN + p + 1] - Tq[1 * PN + p - 1]) + cdy(Tq[4 * PN + p + PX] - Tq[4 * PN + p - PX]);
+    const T divT_z = cdx(Tq[2 * PN + p + 1] - Tq[2 * PN + p - 1]) + cdy(Tq[5 * PN + p + PX] - Tq[5 * PN + p - PX]);
+    const T hr = irho ? hT * (T)__ldg(irho + c) : hT / (T)__ldg(rho + c);
     const T Fx = hr * divT_x, Fy = hr * divT_y, Fz = hr * divT_z;
     const T Bx = tb.c[o], By = tb.c[SN + o], Bz = tb.c[2 * SN + o];
     const T cross_x = By * Fz - Bz * Fy;
@@ -1588,8 +1602,11 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
 // kRK = false: the ideal-gas instance.  Its EOS branches fold at compile time, so it carries
 // none of the Redlich-Kwong Newton iterations and its code stays small (this persistent
 // kernel is large enough for instruction fetch to stall it).
-template <class TS, bool kRK = true>
-__global__ void __launch_bounds__(NT, 2) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
+// kMinB: CTAs per SM the registers are sized for.  Three (80 registers, a few hundred bytes
+// spilled) hide more load latency once a solve's planes no longer fit in the L2; two keep
+// the spills away while they do (newton_launch chooses by grid size).
+template <class TS, bool kRK = true, int kMinB = 2>
+__global__ void __launch_bounds__(NT, kMinB) k_nested_newton(PressureOp op, GmresWorkT<TS> gw, NewtonArgs na) {
   if (!kRK) op.P.eos_type = IMEX_IDEAL_GAS;
   newton_solve(op, gw, na);
 }
@@ -1599,8 +1616,9 @@ struct NewtonJob {
   GmresWorkT<TS> gw;
   NewtonArgs na;
 };
-template <class TS, bool kRK = true>  // kRK as for k_nested_newton
-__global__ void __launch_bounds__(NT, 2) k_nested_newton_jobs(const NewtonJob<TS>* jobs, const int* cta_job) {
+// kRK as for k_nested_newton; three CTAs per SM (an ensemble's members together outgrow the L2)
+template <class TS, bool kRK = true>
+__global__ void __launch_bounds__(NT, 3) k_nested_newton_jobs(const NewtonJob<TS>* jobs, const int* cta_job) {
   const NewtonJob<TS>& j = jobs[cta_job[blockIdx.x]];
   PressureOp op = j.op;
   if (!kRK) op.P.eos_type = IMEX_IDEAL_GAS;
@@ -1920,6 +1938,11 @@ __global__ void k_gmax(DevParams P, const double* __restrict__ Qs, double* __res
     partial[2 * blockIdx.x + 1] = b;
   }
 }
+// r = 1 / a over n values (the A-form operator's 1/rho in the fast arithmetic)
+__global__ void k_recip(const double* __restrict__ a, double* __restrict__ r, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) r[i] = 1.0 / a[i];
+}
 __global__ void k_gmax_finalize(const double* __restrict__ partial, int nblk, DevScalars* sc) {
   double a = 0.0, b = 0.0;
   for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
@@ -2192,6 +2215,7 @@ MagneticAOpT<double, kOpen> make_magA_op(imex_ctx* ctx) {
   op.sc = ctx->sc;
   op.Qe = ctx->Qe;
   op.rho = ctx->cons;
+  op.irho = ctx->P.fast ? ctx->irho : nullptr;
   op.lv = ctx->lvm;
   op.add_bvisc = ctx->P.add_bvisc;
   return op;
@@ -2384,15 +2408,21 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b, int keys = 
   na.sc = ctx->sc;
   na.bkeys = keys ? ctx->sc->bkey[keys - 1] : nullptr;
   imex_status s;
+  // Above 2^21 cells (between 1024^2 and 2048^2) the solve's planes outgrow the 126 MB L2 and
+  // the 3-CTA instance is faster (2048^2 vortex sheet: 5.71 -> 4.96 ms of Newton per step;
+  // 1024^2: 1.68 -> 1.74, so that size keeps the 2-CTA instance).
+  const bool wide = ctx->N >= (size_t(1) << 21);
   prof_begin(ctx);
   if (!mixed(ctx, IMEX_MIXED_PRESSURE)) {
-    auto kern = P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton<double, false> : k_nested_newton<double, true>;
+    auto kern = P.eos_type == IMEX_IDEAL_GAS ? (wide ? k_nested_newton<double, false, 3> : k_nested_newton<double, false>)
+                                             : (wide ? k_nested_newton<double, true, 3> : k_nested_newton<double, true>);
     const size_t smem = sizeof(NewtonSmem<double>);
     const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
     GmresWork g = make_work(ctx, T, nb, F_NEWTON);
     s = launch_coop_smem(ctx, kern, nb, smem, o, g, na);
   } else {
-    auto kern = P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton<float, false> : k_nested_newton<float, true>;
+    auto kern = P.eos_type == IMEX_IDEAL_GAS ? (wide ? k_nested_newton<float, false, 3> : k_nested_newton<float, false>)
+                                             : (wide ? k_nested_newton<float, true, 3> : k_nested_newton<float, true>);
     const size_t smem = sizeof(NewtonSmem<float>);
     const int nb = coop_blocks_smem(ctx, (const void*)kern, T, smem);
     GmresWorkT<float> g = make_work_mixed(ctx, T, nb, F_NEWTON, make_work(ctx, T, nb, F_NEWTON).max_restarts,
@@ -2660,7 +2690,11 @@ imex_status mag_rhs(imex_ctx* ctx) {
     prof_begin(ctx);
     k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
     LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
-    prof_end(ctx, F_MAG_RHS, BYTES(14), 1);
+    if (P.fast) {
+      k_recip<<<nb, kThreads, 0, ctx->stream>>>(ctx->cons, ctx->irho, P.N);
+      LAUNCH_CHECK(ctx, "k_recip");
+    }
+    prof_end(ctx, F_MAG_RHS, BYTES(P.fast ? 16 : 14), P.fast ? 2 : 1);
     return IMEX_OK;
   }
   prof_begin(ctx);
@@ -2794,6 +2828,10 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
   if ((op == IMEX_OP_MAGNETIC_A || op == IMEX_OP_MAGNETIC_B) &&
       (s = local_visc(ctx, op == IMEX_OP_MAGNETIC_A ? LV_MAG_A : LV_MAG_B)) != IMEX_OK)
     return s;
+  if (op == IMEX_OP_MAGNETIC_A && ctx->P.fast) {
+    k_recip<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->cons, ctx->irho, ctx->P.N);
+    LAUNCH_CHECK(ctx, "k_recip");
+  }
   if ((s = set_h(ctx, h)) != IMEX_OK) return s;
   if (op == IMEX_OP_PRESSURE_L || op == IMEX_OP_PRESSURE_J) {
     // the Qe pressure / enthalpy planes come from the stage combination; rebuild them here

@@ -105,7 +105,7 @@ def test_gpu_reconstruction_and_shock_detector_bit_exact():
 ])
 def test_gpu_operators_bit_exact(op, settings):
     g = load_golden("fn_vortex16x12.npz")
-    sv = _fn_solver(settings)
+    sv = _fn_solver(dict(settings, arith="exact"))
     dt, h, bmx, bmy, vxm, vym, amax = (float(v) for v in g["scalars"])
     sv.set_scalars(dt=dt, adt=h, B_max_x=bmx, B_max_y=bmy, vx_max=vxm, vy_max=vym, a_max=amax)
     sv.set_buffer("cons", g["ucon"])
@@ -132,7 +132,7 @@ def test_gpu_local_dissipation_operators_bit_exact(op, settings):
     reference's on the inputs of the function fixture."""
     g = load_golden("fn_vortex16x12.npz")
     loc = load_golden("fn_local_vortex16x12.npz")
-    sv = _fn_solver(dict(settings, GLF=0))
+    sv = _fn_solver(dict(settings, GLF=0, arith="exact"))
     dt, h, bmx, bmy, vxm, vym, amax = (float(v) for v in g["scalars"])
     sv.set_scalars(dt=dt, adt=h, B_max_x=bmx, B_max_y=bmy, vx_max=vxm, vy_max=vym, a_max=amax)
     sv.set_buffer("cons", g["ucon"])
@@ -144,6 +144,29 @@ def test_gpu_local_dissipation_operators_bit_exact(op, settings):
         sv.set_newton_state(g["pfreeze"], float(g["mbig"]))
     x = g["x3"] if op.startswith("magnetic") else g["x1"]
     np.testing.assert_array_equal(sv.apply_operator(kind, x), loc[f"op_{op}"])
+    sv.close()
+
+
+@pytest.mark.parametrize("op,settings", [
+    ("magnetic_B", dict(recon="VanLeer", magfield="StaggerCT")),
+    ("magnetic_A", dict(recon="WENO5", magfield="PotentialA", p_floor=1e-8, theta=0.5)),
+])
+def test_gpu_fast_magnetic_operators_within_round_off(op, settings):
+    """The fast arithmetic multiplies by hoisted reciprocals (face 1/rho in the B form, 1/(2 dx)
+    and 1/(2 dy) in the A form's central differences) where the reference divides: a few ulp
+    from the reference's operator, held here to 1e-14 relative L2 per component."""
+    g = load_golden("fn_vortex16x12.npz")
+    sv = _fn_solver(dict(settings, arith="fast"))
+    dt, h, bmx, bmy, vxm, vym, amax = (float(v) for v in g["scalars"])
+    sv.set_scalars(dt=dt, adt=h, B_max_x=bmx, B_max_y=bmy, vx_max=vxm, vy_max=vym, a_max=amax)
+    sv.set_buffer("cons", g["ucon"])
+    sv.set_buffer("Qe", g["Q"])
+    sv.set_buffer("Qs", g["Qs"])
+    sv.prepare_operator(op, float(g["h"]))
+    got = np.asarray(sv.apply_operator(op, g["x3"])).reshape(3, -1)
+    ref = np.asarray(g[f"op_{op}"]).reshape(3, -1)
+    for k in range(3):
+        assert rel(got[k], ref[k]) <= 1e-14, (k, rel(got[k], ref[k]))
     sv.close()
 
 
