@@ -354,7 +354,11 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     launches0 = sum(m.kernel_launches() for m in batch.members)
     batch.step(1)  # captures the step (launch count of one step) and runs it
     info = batch.info()
-    launches_per_step = sum(m.kernel_launches() for m in batch.members) - launches0 + 2 * info["solve_launches_per_step"]
+    if info["explicit_launches_per_step"] >= 0:  # batched explicit sub-steps: the planned step's launches
+        launches_per_step = info["explicit_launches_per_step"] + info["planned_solve_launches_per_step"]
+    else:
+        launches_per_step = (sum(m.kernel_launches() for m in batch.members) - launches0
+                             + 2 * info["solve_launches_per_step"])
     for _ in range(max(args.warmup - 1, 2)):
         batch.step(1)
     cells_per_step = sum(p.nx * p.ny for p in probs) * wl["rks"]

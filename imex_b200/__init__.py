@@ -179,6 +179,7 @@ _SIGS = {
     "imex_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "imex_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(BatchTuning)]),
     "imex_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "imex_batch_explicit_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "imex_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "imex_pressure_nested_newton": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(SolveStats)]),
     "imex_shock_detector": (C.c_int, [C.c_void_p, _D, _D]),
@@ -604,7 +605,9 @@ class Batch:
     advanced together.  ``members[m]`` is a Solver view on member m's context (state I/O
     and diagnostics); the batch owns the members."""
 
-    def __init__(self, problems, rks: int, settings: dict | None = None, streams: int = 8, graph: bool = True):
+    def __init__(self, problems, rks: int, settings: dict | None = None, streams: int = 0, graph: bool = True):
+        """streams = 0: each explicit sub-step is one launch for all members; streams > 0:
+        each member launches its own kernels, the members spread over that many streams."""
         self.lib = load_library()
         p0 = problems[0]
         s = dict(p0.settings)
@@ -625,7 +628,7 @@ class Batch:
             sv = Solver._view(self.lib, c, p.nx, p.ny)
             sv.load(p)
             self.members.append(sv)
-        if streams != 8 or not graph:
+        if streams != 0 or not graph:
             self._check(self.lib.imex_batch_configure(self.b, streams, 1 if graph else 0))
 
     def _check(self, rc: int) -> None:
@@ -649,7 +652,10 @@ class Batch:
         a, g, n = C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.imex_batch_info(self.b, C.byref(a), C.byref(g), C.byref(n)))
         msg = self.lib.imex_batch_last_error(self.b)
+        e, sl = C.c_int(), C.c_int()
+        self._check(self.lib.imex_batch_explicit_launches(self.b, C.byref(e), C.byref(sl)))
         return dict(streams=a.value, graph=bool(g.value), solve_launches_per_step=n.value,
+                    explicit_launches_per_step=e.value, planned_solve_launches_per_step=sl.value,
                     note=msg.decode() if msg else "")
 
     def close(self) -> None:

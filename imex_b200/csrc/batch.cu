@@ -9,6 +9,13 @@
 //     is ONE cooperative launch for all members, in which every member owns a contiguous
 //     range of CTAs with its own barrier and reductions (see batch_solve_build).  Members
 //     never wait on one another, and no two cooperative kernels run at the same time.
+// The explicit sub-steps run in one of two ways:
+//   - batched (streams = 0, the default): each explicit sub-step is ONE launch for all
+//     members.  The step is planned once: every member's launch functions run in recording
+//     mode (launch.cuh), and the launches the members recorded for a sub-step become one
+//     launch of the same kernel body over all their grids, laid end to end;
+//   - on a pool of streams (streams > 0): every member launches its own kernels, members
+//     spread over the streams.
 // The whole step is captured once into a CUDA graph and replayed; if capture fails the
 // same step is launched directly and the reason is kept (imex_batch_last_error).
 #include <cstdio>
@@ -17,6 +24,7 @@
 #include <vector>
 
 #include "imex_internal.h"
+#include "launch.cuh"
 
 struct imex_batch {
   std::vector<imex_ctx*> members;
@@ -28,16 +36,64 @@ struct imex_batch {
   imex::BatchSolvePlan* pres = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  int nstreams = 8;
+  // the planned step of the batched mode: its launches in order, and their device tables
+  std::vector<imex::PlanItem> plan;
+  imex::PlanArena arena;
+  int nstreams = 0;  // 0: batched explicit sub-steps; > 0: streams of the per-member launches
   bool use_graph = true;
+  bool members_on_batch = false;  // the members' streams are the batch's (pool or origin)
   bool prepared = false;
   bool graph_ok = false;
   std::string last_error;
 };
 
+namespace imex {
+
+__global__ void k_copies(const CopyDesc* __restrict__ d) {
+  const CopyDesc c = d[blockIdx.y];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += (long long)gridDim.x * blockDim.x)
+    c.dst[i] = c.src[i];
+}
+
+imex_status plan_alloc(PlanArena& arena, size_t bytes, void** p, std::string& err) {
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    err = std::string("batched launch tables: ") + cudaGetErrorString(e);
+    return IMEX_ERR_CUDA;
+  }
+  arena.dev.push_back(*p);
+  return IMEX_OK;
+}
+imex_status plan_upload(void* dst, const void* src, size_t bytes, std::string& err) {
+  cudaError_t e = bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  if (e != cudaSuccess) {
+    err = std::string("batched launch tables: ") + cudaGetErrorString(e);
+    return IMEX_ERR_CUDA;
+  }
+  return IMEX_OK;
+}
+cudaError_t copy_d2d(imex_ctx* ctx, double* dst, const double* src, long long n) {
+  if (ctx->rec) {
+    RecOp op;
+    op.copy = CopyDesc{dst, src, n};
+    ctx->rec->ops.push_back(std::move(op));
+    return cudaSuccess;
+  }
+  return cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+}
+
+}  // namespace imex
+
 namespace {
 
 using namespace imex;
+
+constexpr unsigned kCopyThreads = 256;
+cudaError_t launch_copies(const PlanItem& it, cudaStream_t s) {
+  k_copies<<<dim3(it.nblocks, it.gy), it.block, 0, s>>>(static_cast<const CopyDesc*>(it.args));
+  return cudaGetLastError();
+}
 
 imex_status berr(imex_batch* b, imex_status s, const std::string& msg) {
   if (b) b->last_error = msg;
@@ -56,14 +112,18 @@ imex_status merr(imex_batch* b, size_t m, imex_status s) {
 // Drop the streams, plans and graph.  Members that are still alive first get a stream of
 // their own again: they must never hold a handle to a destroyed batch stream.
 void release_plans(imex_batch* b, bool members_alive) {
-  if (members_alive && !b->streams.empty())
+  if (members_alive && b->members_on_batch)
     for (imex_ctx* c : b->members) imex_set_stream(c, nullptr);
+  b->members_on_batch = false;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
   batch_solve_free(b->mag);
   batch_solve_free(b->pres);
+  for (void* p : b->arena.dev) cudaFree(p);
+  b->arena.dev.clear();
+  b->plan.clear();
   b->mag = b->pres = nullptr;
   for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
   for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
@@ -73,8 +133,51 @@ void release_plans(imex_batch* b, bool members_alive) {
   b->graph_ok = false;
 }
 
-// one step of every member (main.cpp:335-561 per member), enqueued without a host wait
-imex_status enqueue_step(imex_batch* b) {
+// The sub-steps of one ensemble step (main.cpp:335-561 per member), in order: `group`
+// runs a per-member launch function for every member, `solve` one batched solve
+// (BATCH_MAGNETIC / BATCH_PRESSURE) for all of them.
+template <class G, class V>
+imex_status step_sequence(imex_batch* b, G group, V solve) {
+  const DevParams& P = b->members[0]->P;
+  imex_status s;
+  if ((s = group([](imex_ctx* c) { return launch_step_prologue(c); })) != IMEX_OK) return s;
+  for (int r = 0; r < P.RKs; ++r) {
+    s = group([r](imex_ctx* c) {
+      imex_status t = launch_stage_combine(c, r);
+      if (t == IMEX_OK) t = launch_reconstruct(c, false);
+      if (t == IMEX_OK) t = launch_flux_update(c, 0);
+      if (t == IMEX_OK) t = mag_rhs(c);
+      return t;
+    });
+    if (s != IMEX_OK || (s = solve(BATCH_MAGNETIC)) != IMEX_OK) return s;
+    s = group([](imex_ctx* c) {
+      imex_status t = mag_out(c);
+      if (t == IMEX_OK && c->P.Energy_Modify)
+        t = cuda_check(c, copy_d2d(c, c->Bsave, c->cons + 5 * c->N, 3 * (long long)c->N), "Bsave");
+      if (t == IMEX_OK) t = launch_flux_update(c, second_flux_form(c));
+      if (t == IMEX_OK) t = pres_part1(c);
+      return t;
+    });
+    if (s != IMEX_OK || (s = solve(BATCH_PRESSURE)) != IMEX_OK) return s;
+    bool second = false;
+    s = group([r, &second](imex_ctx* c) { return pres_part2(c, r, &second); });
+    if (s != IMEX_OK) return s;
+    if (second && (s = solve(BATCH_PRESSURE)) != IMEX_OK) return s;
+    s = group([r](imex_ctx* c) {
+      imex_status t = pres_part3(c);
+      if (t == IMEX_OK && c->P.magfield == IMEX_StaggerCT) t = launch_ct(c, 0);
+      else if (t == IMEX_OK && c->P.magfield == IMEX_UnStaggerCT) t = launch_ct(c, 1);
+      if (t == IMEX_OK) t = launch_stage_derivative(c, r);
+      return t;
+    });
+    if (s != IMEX_OK) return s;
+  }
+  return IMEX_OK;
+}
+BatchSolvePlan* solve_plan(imex_batch* b, int kind) { return kind == BATCH_MAGNETIC ? b->mag : b->pres; }
+
+// one step of every member on the pool of streams, enqueued without a host wait
+imex_status enqueue_step_streams(imex_batch* b) {
   cudaError_t e = cudaSuccess;
   auto fork = [&]() {
     e = cudaEventRecord(b->ev_fork, b->origin);
@@ -89,7 +192,7 @@ imex_status enqueue_step(imex_batch* b) {
     }
     return bcheck(b, e, "batch join");
   };
-  auto each = [&](auto f) {
+  auto group = [&](auto f) {
     for (size_t m = 0; m < b->members.size(); ++m) {
       imex_status s = f(b->members[m]);
       if (s != IMEX_OK) return merr(b, m, s);
@@ -97,52 +200,104 @@ imex_status enqueue_step(imex_batch* b) {
     return IMEX_OK;
   };
   imex_ctx* c0 = b->members[0];
-  const DevParams& P = c0->P;
-  imex_status s;
-  if ((s = fork()) != IMEX_OK) return s;
-  if ((s = each([](imex_ctx* c) { return launch_step_prologue(c); })) != IMEX_OK) return s;
-  for (int r = 0; r < P.RKs; ++r) {
-    s = each([r](imex_ctx* c) {
-      imex_status t = launch_stage_combine(c, r);
-      if (t == IMEX_OK) t = launch_reconstruct(c, false);
-      if (t == IMEX_OK) t = launch_flux_update(c, 0);
-      if (t == IMEX_OK) t = mag_rhs(c);
-      return t;
-    });
-    if (s != IMEX_OK) return s;
-    if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->mag, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
-      return s == IMEX_OK ? s : berr(b, s, b->last_error.empty() ? c0->last_error : b->last_error);
-    s = each([](imex_ctx* c) {
-      imex_status t = mag_out(c);
-      if (t == IMEX_OK && c->P.Energy_Modify) {
-        cudaError_t e2 = cudaMemcpyAsync(c->Bsave, c->cons + 5 * c->N, 3 * c->N * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, c->stream);
-        t = cuda_check(c, e2, "Bsave");
-      }
-      if (t == IMEX_OK) t = launch_flux_update(c, second_flux_form(c));
-      if (t == IMEX_OK) t = pres_part1(c);
-      return t;
-    });
-    if (s != IMEX_OK) return s;
-    if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->pres, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
-      return s;
-    bool second = false;
-    s = each([r, &second](imex_ctx* c) { return pres_part2(c, r, &second); });
-    if (s != IMEX_OK) return s;
-    if (second) {
-      if ((s = join()) != IMEX_OK || (s = batch_solve_run(b->pres, b->origin, c0)) != IMEX_OK || (s = fork()) != IMEX_OK)
-        return s;
-    }
-    s = each([r](imex_ctx* c) {
-      imex_status t = pres_part3(c);
-      if (t == IMEX_OK && c->P.magfield == IMEX_StaggerCT) t = launch_ct(c, 0);
-      else if (t == IMEX_OK && c->P.magfield == IMEX_UnStaggerCT) t = launch_ct(c, 1);
-      if (t == IMEX_OK) t = launch_stage_derivative(c, r);
-      return t;
-    });
-    if (s != IMEX_OK) return s;
-  }
+  auto solve = [&](int kind) {
+    imex_status s;
+    if ((s = join()) != IMEX_OK) return s;
+    if ((s = batch_solve_run(solve_plan(b, kind), b->origin, c0)) != IMEX_OK)
+      return berr(b, s, b->last_error.empty() ? c0->last_error : b->last_error);
+    return fork();
+  };
+  imex_status s = fork();
+  if (s == IMEX_OK) s = step_sequence(b, group, solve);
+  if (s != IMEX_OK) return s;
   return join();
+}
+
+// The launches that the members recorded for one group of sub-steps, as launches of the
+// planned step.  Round k takes the k-th recorded operation of every member; operations of
+// a round that run the same kernel body (or are copies) become one launch.  A member's
+// operations therefore run in its own order, one round after another.
+imex_status flush_records(imex_batch* b, const std::vector<Recorder>& R) {
+  std::vector<size_t> idx(R.size(), 0);
+  std::string err;
+  for (;;) {
+    std::vector<std::pair<const void*, std::vector<const RecOp*>>> groups;
+    for (size_t m = 0; m < R.size(); ++m) {
+      if (idx[m] >= R[m].ops.size()) continue;
+      const RecOp* op = &R[m].ops[idx[m]++];
+      const void* key = op->plan ? reinterpret_cast<const void*>(op->plan) : nullptr;
+      auto g = groups.begin();
+      while (g != groups.end() && g->first != key) ++g;
+      if (g == groups.end()) groups.push_back({key, {op}});
+      else g->second.push_back(op);
+    }
+    if (groups.empty()) return IMEX_OK;
+    for (auto& g : groups) {
+      PlanItem it;
+      imex_status s = IMEX_OK;
+      if (g.first) {
+        s = g.second[0]->plan(g.second, b->arena, it, err);
+      } else {
+        std::vector<CopyDesc> d;
+        long long nmax = 1;
+        for (const RecOp* op : g.second) {
+          d.push_back(op->copy);
+          if (op->copy.n > nmax) nmax = op->copy.n;
+        }
+        void* dd = nullptr;
+        s = plan_alloc(b->arena, d.size() * sizeof(CopyDesc), &dd, err);
+        if (s == IMEX_OK) s = plan_upload(dd, d.data(), d.size() * sizeof(CopyDesc), err);
+        long long nb = (nmax + 4 * kCopyThreads - 1) / (4 * kCopyThreads);
+        it.launch = &launch_copies;
+        it.args = dd;
+        it.nblocks = (unsigned)(nb < 1024 ? nb : 1024);
+        it.gy = (unsigned)d.size();
+        it.block = kCopyThreads;
+      }
+      if (s != IMEX_OK) return berr(b, s, err);
+      b->plan.push_back(it);
+    }
+  }
+}
+
+// Plan one step of the batched mode: record every member's launches group by group and
+// turn them into batched launches (device tables are built here, outside any capture).
+imex_status plan_step(imex_batch* b) {
+  b->plan.clear();
+  auto group = [&](auto f) {
+    std::vector<Recorder> R(b->members.size());
+    for (size_t m = 0; m < b->members.size(); ++m) {
+      imex_ctx* c = b->members[m];
+      c->rec = &R[m];
+      imex_status s = f(c);
+      c->rec = nullptr;
+      if (s != IMEX_OK) return merr(b, m, s);
+    }
+    return flush_records(b, R);
+  };
+  auto solve = [&](int kind) {
+    PlanItem it;
+    it.solve = kind;
+    b->plan.push_back(it);
+    return IMEX_OK;
+  };
+  return step_sequence(b, group, solve);
+}
+imex_status enqueue_step_planned(imex_batch* b) {
+  imex_ctx* c0 = b->members[0];
+  for (const PlanItem& it : b->plan) {
+    if (it.solve >= 0) {
+      imex_status s = batch_solve_run(solve_plan(b, it.solve), b->origin, c0);
+      if (s != IMEX_OK) return berr(b, s, b->last_error.empty() ? c0->last_error : b->last_error);
+      continue;
+    }
+    cudaError_t e = it.launch(it, b->origin);
+    if (e != cudaSuccess) return bcheck(b, e, "batched launch");
+  }
+  return IMEX_OK;
+}
+imex_status enqueue_step(imex_batch* b) {
+  return b->nstreams == 0 ? enqueue_step_planned(b) : enqueue_step_streams(b);
 }
 
 // streams, batched-solve plans and (if asked) the captured step
@@ -158,14 +313,18 @@ imex_status prepare(imex_batch* b) {
     if (ev) b->ev_join.push_back(ev);
   }
   if (e != cudaSuccess) return bcheck(b, e, "batch streams");
+  // members run on the pool (streams mode) or on the batch's own stream (batched mode)
   for (size_t m = 0; m < b->members.size(); ++m) {
-    imex_status s = imex_set_stream(b->members[m], b->streams[m % b->streams.size()]);
+    cudaStream_t st = b->streams.empty() ? b->origin : b->streams[m % b->streams.size()];
+    imex_status s = imex_set_stream(b->members[m], st);
     if (s != IMEX_OK) return merr(b, m, s);
     b->members[m]->prof_on = false;
   }
+  b->members_on_batch = true;
   imex_status s = batch_solve_build(b->members, BATCH_MAGNETIC, &b->mag);
   if (s == IMEX_OK) s = batch_solve_build(b->members, BATCH_PRESSURE, &b->pres);
   if (s != IMEX_OK) return berr(b, s, "batched solve set-up: " + b->members[0]->last_error);
+  if (b->nstreams == 0 && (s = plan_step(b)) != IMEX_OK) return s;
   b->prepared = true;
   b->graph_ok = false;
   if (!b->use_graph) return IMEX_OK;
@@ -308,7 +467,7 @@ imex_status imex_batch_member(imex_batch* b, int m, imex_ctx** ctx) {
 const char* imex_batch_last_error(const imex_batch* b) { return b ? b->last_error.c_str() : "no batch"; }
 
 imex_status imex_batch_configure(imex_batch* b, int streams, int use_graph) {
-  if (!b || streams < 1 || streams > 64) return IMEX_ERR_INVALID;
+  if (!b || streams < 0 || streams > 64) return IMEX_ERR_INVALID;
   if (b->origin) cudaStreamSynchronize(b->origin);
   release_plans(b, true);
   b->nstreams = streams;
@@ -356,10 +515,29 @@ imex_status imex_batch_info(imex_batch* b, int* streams, int* graph_used, int* s
   return IMEX_OK;
 }
 
+imex_status imex_batch_explicit_launches(imex_batch* b, int* launches_per_step, int* solve_launches_per_step) {
+  if (!b || !launches_per_step) return IMEX_ERR_INVALID;
+  imex_status s = prepare(b);
+  if (s != IMEX_OK) return s;
+  int n = -1;
+  if (b->nstreams == 0) {
+    n = 0;
+    for (const PlanItem& it : b->plan) n += it.solve < 0 ? 1 : 0;
+  }
+  *launches_per_step = n;
+  if (solve_launches_per_step) {  // a chunk of a batched solve: a barrier reset and the solve
+    int m = 0;
+    for (const PlanItem& it : b->plan)
+      if (it.solve >= 0) m += 2 * (int)solve_plan(b, it.solve)->chunks.size();
+    *solve_launches_per_step = b->nstreams == 0 ? m : -1;
+  }
+  return IMEX_OK;
+}
+
 imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out) {
   if (!b || trial_steps < 1) return IMEX_ERR_INVALID;
   const int restart0 = b->members[0]->cfg.gmres_restart;
-  const int stream_cands[] = {4, 8, 16};
+  const int stream_cands[] = {0, 4, 8, 16};
   const int restart_cands[] = {restart0 < 15 ? restart0 : 15, restart0};
   // in mixed precision, whether the magnetic systems take the FP32 form pays only where
   // FP64 GMRES needs many Krylov steps: time both

@@ -12,6 +12,8 @@
 
 namespace imex {
 
+struct Recorder;  // launch.cuh: the recorded launches of a context while an ensemble plans a step
+
 constexpr int kMaxRK = 3;
 constexpr int kMaxKrylov = 32;  // upper bound on gmres_restart (reference: 25)
 
@@ -156,24 +158,26 @@ struct imex_ctx {
   long long prof_launches[imex::NFAM] = {};
   cudaEvent_t prof_open = nullptr;
   long long kernel_launches = 0;  // every kernel this context launched
+  imex::Recorder* rec = nullptr;  // set while an ensemble records this context's launches
   double barrier_timeout_s = 2.0;  // bound on any single device-wide wait
 };
 
-// Launch kernel template kern<kOpen> with the instance for this context's boundaries
-// (bc_params): transmissive in x or y, or periodic in both.
-#define IMEX_LAUNCH_BC(P, kern, grid, block, smem, stream, ...)                    \
-  do {                                                                             \
-    if ((P).xclamp || (P).yclamp) kern<true><<<grid, block, smem, stream>>>(__VA_ARGS__); \
-    else kern<false><<<grid, block, smem, stream>>>(__VA_ARGS__);                  \
+// Launch (or record, launch.cuh) kernel body kern<kOpen> with the instance for this
+// context's boundaries (bc_params): transmissive in x or y, or periodic in both.  The
+// calling function's `ctx` is the context that launches.
+#define IMEX_LAUNCH_BC(P, kern, grid, block, smem, stream, ...)                         \
+  do {                                                                                  \
+    if ((P).xclamp || (P).yclamp) launch<kern<true>>(ctx, grid, block, smem, stream, __VA_ARGS__); \
+    else launch<kern<false>>(ctx, grid, block, smem, stream, __VA_ARGS__);              \
   } while (0)
 // the same over the boundary kind and the arithmetic of the explicit stencils (kern<kOpen, kFast>)
-#define IMEX_LAUNCH_BC_ARITH(P, kern, grid, block, smem, stream, ...)                              \
-  do {                                                                                             \
-    const bool open_ = (P).xclamp || (P).yclamp;                                                   \
-    if (open_ && (P).fast) kern<true, true><<<grid, block, smem, stream>>>(__VA_ARGS__);            \
-    else if (open_) kern<true, false><<<grid, block, smem, stream>>>(__VA_ARGS__);                 \
-    else if ((P).fast) kern<false, true><<<grid, block, smem, stream>>>(__VA_ARGS__);              \
-    else kern<false, false><<<grid, block, smem, stream>>>(__VA_ARGS__);                           \
+#define IMEX_LAUNCH_BC_ARITH(P, kern, grid, block, smem, stream, ...)                                    \
+  do {                                                                                                   \
+    const bool open_ = (P).xclamp || (P).yclamp;                                                         \
+    if (open_ && (P).fast) launch<kern<true, true>>(ctx, grid, block, smem, stream, __VA_ARGS__);         \
+    else if (open_) launch<kern<true, false>>(ctx, grid, block, smem, stream, __VA_ARGS__);              \
+    else if ((P).fast) launch<kern<false, true>>(ctx, grid, block, smem, stream, __VA_ARGS__);           \
+    else launch<kern<false, false>>(ctx, grid, block, smem, stream, __VA_ARGS__);                        \
   } while (0)
 
 namespace imex {

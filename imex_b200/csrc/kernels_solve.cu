@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "cells.cuh"
+#include "launch.cuh"
 
 namespace imex {
 namespace {
@@ -1641,200 +1642,230 @@ inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads)
 
 // enthalpy ratio h(Qe) rho_e / rho, V slope at p(Qe), rho v* snapshot (imex_subsystems.cpp:92-147)
 template <bool kOpen>
-__global__ void k_pressure_coeffs(DevParams Pin, const double* __restrict__ Qe, const double* __restrict__ ucon,
-                                  const double* __restrict__ hQe, const double* __restrict__ pe,
-                                  double* __restrict__ hh, double* __restrict__ vscale, double* __restrict__ rv,
-                                  unsigned long long* __restrict__ bkeys) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n < 4) bkeys[n] = ~0ull;  // the identities of the min keys k_pressure_rhs forms next
-  if (n >= N) return;
-  const double r = ucon[n], hq = hQe[n], q = Qe[n], pn = pe[n];
-  const double m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
-  rv[n] = m1;
-  rv[N + n] = m2;
-  rv[2 * N + n] = m3;
-  hh[n] = hq * q / r;
-  vscale[n] = Vbase_slope(P, pn, r);
-}
+struct k_pressure_coeffs {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ Qe, const double* __restrict__ ucon,
+                                    const double* __restrict__ hQe, const double* __restrict__ pe,
+                                    double* __restrict__ hh, double* __restrict__ vscale, double* __restrict__ rv,
+                                    unsigned long long* __restrict__ bkeys) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n < 4) bkeys[n] = ~0ull;  // the identities of the min keys k_pressure_rhs forms next
+    if (n >= N) return;
+    const double r = ucon[n], hq = hQe[n], q = Qe[n], pn = pe[n];
+    const double m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
+    rv[n] = m1;
+    rv[N + n] = m2;
+    rv[2 * N + n] = m3;
+    hh[n] = hq * q / r;
+    vscale[n] = Vbase_slope(P, pn, r);
+  }
+};
 // Jacobi diagonal Tdiag (implicit_operators.cpp:631-649)
 template <bool kOpen>
-__global__ void k_pressure_tdiag(DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ hh,
-                                 double* __restrict__ tdiag) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= P.N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double h00 = hh[n], hp0 = hh[cid(P, i + 1, j)], hm0 = hh[cid(P, i - 1, j)], h0p = hh[cid(P, i, j + 1)],
-               h0m = hh[cid(P, i, j - 1)];
-  tdiag[n] = h * h * ((0.5 * (hp0 + h00) + 0.5 * (hm0 + h00)) / (P.dx * P.dx) +
-                      (0.5 * (h0p + h00) + 0.5 * (h0m + h00)) / (P.dy * P.dy));
-}
+struct k_pressure_tdiag {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ hh,
+                                   double* __restrict__ tdiag) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double h00 = hh[n], hp0 = hh[cid(P, i + 1, j)], hm0 = hh[cid(P, i - 1, j)], h0p = hh[cid(P, i, j + 1)],
+                 h0m = hh[cid(P, i, j - 1)];
+    tdiag[n] = h * h * ((0.5 * (hp0 + h00) + 0.5 * (hm0 + h00)) / (P.dx * P.dx) +
+                        (0.5 * (h0p + h00) + 0.5 * (h0m + h00)) / (P.dy * P.dy));
+  }
+};
 // pressure RHS b (imex_subsystems.cpp:123-169 first, 226-269 second); kin = momentum used in
 // the kinetic term, rv = rho v* used in the enthalpy-flux divergence; p0 = initial guess.
 template <bool kOpen>
-__global__ void k_pressure_rhs(DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
-                               const double* __restrict__ hh, const double* __restrict__ rv,
-                               const double* __restrict__ kin, double* __restrict__ b,
-                               const double* __restrict__ p0src, double* __restrict__ p0,
-                               unsigned long long* __restrict__ bkeys) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  unsigned long long kb = ~0ull, kv = ~0ull;  // identities of min
-  if (n < N) {
+struct k_pressure_rhs {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                                 const double* __restrict__ hh, const double* __restrict__ rv,
+                                 const double* __restrict__ kin, double* __restrict__ b,
+                                 const double* __restrict__ p0src, double* __restrict__ p0,
+                                 unsigned long long* __restrict__ bkeys) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned long long kb = ~0ull, kv = ~0ull;  // identities of min
+    if (n < N) {
+      long long nb[9];
+      neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+      const double* arr[4] = {ucon, hh, rv, kin};
+      auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+      double out[1];
+      pressure_rhs_cell<double>(P, h, nb, ld, out);
+      b[n] = out[0];
+      if (p0) p0[n] = p0src[n];
+      if (out[0] == out[0]) kb = dkey(out[0]);
+      if (P.floor_on && P.eos_type != IMEX_IDEAL_GAS) {
+        const double v = Vbase(P, P.p_floor, ucon[n]);
+        if (isfinite(v)) kv = ~dkey(v);
+      }
+    }
+    // the nested Newton's Cor.1 inputs (implicit_operators.cpp:670-686): min b and max V(p_floor,
+    // rho), as exact order-key minima, so that the solve needs no reduction pass of its own
+    if (bkeys) {
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, kb, o), ov = __shfl_xor_sync(0xffffffffu, kv, o);
+        kb = ob < kb ? ob : kb;
+        kv = ov < kv ? ov : kv;
+      }
+      __shared__ unsigned long long sk[2][kThreads / 32];
+      if ((threadIdx.x & 31) == 0) {
+        sk[0][threadIdx.x >> 5] = kb;
+        sk[1][threadIdx.x >> 5] = kv;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+          kb = sk[0][w] < kb ? sk[0][w] : kb;
+          kv = sk[1][w] < kv ? sk[1][w] : kv;
+        }
+        if (kb < *(volatile unsigned long long*)&bkeys[0]) atomicMin(&bkeys[0], kb);
+        if (kv < *(volatile unsigned long long*)&bkeys[1]) atomicMin(&bkeys[1], kv);
+      }
+    }
+  }
+};
+// momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)
+struct k_momentum {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
+                             const double* __restrict__ rv, double* __restrict__ ucon) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
     long long nb[9];
     neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-    const double* arr[4] = {ucon, hh, rv, kin};
+    const double* arr[2] = {p, rv};
+    auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+    double out[2];
+    momentum_cell<double>(P, h, nb, ld, out);
+    ucon[N + n] = out[0];
+    ucon[2 * N + n] = out[1];
+  }
+};
+// E = V(p) + KE + ME (DefinitionofU, imex_subsystems.cpp:286-302)
+struct k_energy_define {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ p, double* __restrict__ ucon) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    long long nb[9];
+    nb[NB_C] = n;
+    const double* arr[2] = {p, ucon};
     auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
     double out[1];
-    pressure_rhs_cell<double>(P, h, nb, ld, out);
-    b[n] = out[0];
-    if (p0) p0[n] = p0src[n];
-    if (out[0] == out[0]) kb = dkey(out[0]);
-    if (P.floor_on && P.eos_type != IMEX_IDEAL_GAS) {
-      const double v = Vbase(P, P.p_floor, ucon[n]);
-      if (isfinite(v)) kv = ~dkey(v);
-    }
+    energy_define_cell<double>(P, nb, ld, out);
+    ucon[4 * N + n] = out[0];
   }
-  // the nested Newton's Cor.1 inputs (implicit_operators.cpp:670-686): min b and max V(p_floor,
-  // rho), as exact order-key minima, so that the solve needs no reduction pass of its own
-  if (bkeys) {
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long ob = __shfl_xor_sync(0xffffffffu, kb, o), ov = __shfl_xor_sync(0xffffffffu, kv, o);
-      kb = ob < kb ? ob : kb;
-      kv = ov < kv ? ov : kv;
-    }
-    __shared__ unsigned long long sk[2][kThreads / 32];
-    if ((threadIdx.x & 31) == 0) {
-      sk[0][threadIdx.x >> 5] = kb;
-      sk[1][threadIdx.x >> 5] = kv;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-        kb = sk[0][w] < kb ? sk[0][w] : kb;
-        kv = sk[1][w] < kv ? sk[1][w] : kv;
-      }
-      if (kb < *(volatile unsigned long long*)&bkeys[0]) atomicMin(&bkeys[0], kb);
-      if (kv < *(volatile unsigned long long*)&bkeys[1]) atomicMin(&bkeys[1], kv);
-    }
-  }
-}
-// momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)
-__global__ void k_momentum(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
-                           const double* __restrict__ rv, double* __restrict__ ucon) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-  const double* arr[2] = {p, rv};
-  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
-  double out[2];
-  momentum_cell<double>(P, h, nb, ld, out);
-  ucon[N + n] = out[0];
-  ucon[2 * N + n] = out[1];
-}
-// E = V(p) + KE + ME (DefinitionofU, imex_subsystems.cpp:286-302)
-__global__ void k_energy_define(DevParams P, const double* __restrict__ p, double* __restrict__ ucon) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  nb[NB_C] = n;
-  const double* arr[2] = {p, ucon};
-  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
-  double out[1];
-  energy_define_cell<double>(P, nb, ld, out);
-  ucon[4 * N + n] = out[0];
-}
+};
 
 // E -= h div(h_e rho v) (ConservationofU, imex_subsystems.cpp:303-392).  Reads only the
 // density and momentum planes of the neighbours, so E is updated in place.
-__global__ void k_energy_conservation(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
-                                      double* __restrict__ ucon) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-  const double* arr[2] = {p, ucon};
-  auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
-  double out[1];
-  energy_conservation_cell<double>(P, h, nb, ld, out);
-  ucon[4 * N + n] = out[0];
-}
+struct k_energy_conservation {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ p,
+                                        double* __restrict__ ucon) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    long long nb[9];
+    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    const double* arr[2] = {p, ucon};
+    auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
+    double out[1];
+    energy_conservation_cell<double>(P, h, nb, ld, out);
+    ucon[4 * N + n] = out[0];
+  }
+};
 
 // total-enthalpy ratio hh = caltotalenthalpy(Qe) rho_e / rho (imex_subsystems.cpp:442-446)
-__global__ void k_energy_coeffs(DevParams P, const double* __restrict__ Qe, const double* __restrict__ ucon,
-                                double* __restrict__ hh) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  double c[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) c[k] = Qe[k * N + n];
-  hh[n] = caltotalenthalpy(P, c) * c[0] / ucon[n];
-}
+struct k_energy_coeffs {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ Qe, const double* __restrict__ ucon,
+                                  double* __restrict__ hh) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double c[8];
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) c[k] = Qe[k * N + n];
+    hh[n] = caltotalenthalpy(P, c) * c[0] / ucon[n];
+  }
+};
 // right-hand side b = U* dx dy (imex_subsystems.cpp:448-452) and the Jacobi scale diag dx dy
 // of precE (imex_subsystems.cpp:499-503); the initial guess is E of u_con (solved in place)
-__global__ void k_energy_rhs(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
-                             const double* __restrict__ hh, double* __restrict__ b, double* __restrict__ tdiag) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const long long e = cid(P, i + 1, j), w = cid(P, i - 1, j), no = cid(P, i, j + 1), s = cid(P, i, j - 1);
-  const double h00 = hh[n], hp0 = hh[e], hm0 = hh[w], h0p = hh[no], h0m = hh[s];
-  const double U_star = ucon[4 * N + n] - 0.5 * h / P.dx * (hp0 * ucon[N + e] - hm0 * ucon[N + w]) -
-                        0.5 * h / P.dy * (h0p * ucon[2 * N + no] - h0m * ucon[2 * N + s]);
-  b[n] = U_star * P.dx * P.dy;
-  const double hhp_x = 0.5 * (h00 + hp0), hhm_x = 0.5 * (h00 + hm0);
-  const double hhp_y = 0.5 * (h00 + h0p), hhm_y = 0.5 * (h00 + h0m);
-  const double diag =
-      1.0 + (P.gamma - 1.0) * h * h * ((hhp_x + hhm_x) / (P.dx * P.dx) + (hhp_y + hhm_y) / (P.dy * P.dy));
-  tdiag[n] = diag * P.dx * P.dy;
-}
+struct k_energy_rhs {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                               const double* __restrict__ hh, double* __restrict__ b, double* __restrict__ tdiag) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const long long e = cid(P, i + 1, j), w = cid(P, i - 1, j), no = cid(P, i, j + 1), s = cid(P, i, j - 1);
+    const double h00 = hh[n], hp0 = hh[e], hm0 = hh[w], h0p = hh[no], h0m = hh[s];
+    const double U_star = ucon[4 * N + n] - 0.5 * h / P.dx * (hp0 * ucon[N + e] - hm0 * ucon[N + w]) -
+                          0.5 * h / P.dy * (h0p * ucon[2 * N + no] - h0m * ucon[2 * N + s]);
+    b[n] = U_star * P.dx * P.dy;
+    const double hhp_x = 0.5 * (h00 + hp0), hhm_x = 0.5 * (h00 + hm0);
+    const double hhp_y = 0.5 * (h00 + h0p), hhm_y = 0.5 * (h00 + h0m);
+    const double diag =
+        1.0 + (P.gamma - 1.0) * h * h * ((hhp_x + hhm_x) / (P.dx * P.dx) + (hhp_y + hhm_y) / (P.dy * P.dy));
+    tdiag[n] = diag * P.dx * P.dy;
+  }
+};
 // momentum correction rho v -= h (g-1) grad E (imex_subsystems.cpp:514-519)
-__global__ void k_energy_momentum(DevParams P, const DevScalars* __restrict__ sc, double* __restrict__ ucon) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double* E = ucon + 4 * N;
-  ucon[N + n] -= h * (1 / (2 * P.dx)) * (P.gamma - 1) * (E[cid(P, i + 1, j)] - E[cid(P, i - 1, j)]);
-  ucon[2 * N + n] -= h * (1 / (2 * P.dy)) * (P.gamma - 1) * (E[cid(P, i, j + 1)] - E[cid(P, i, j - 1)]);
-}
+struct k_energy_momentum {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, double* __restrict__ ucon) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double* E = ucon + 4 * N;
+    ucon[N + n] -= h * (1 / (2 * P.dx)) * (P.gamma - 1) * (E[cid(P, i + 1, j)] - E[cid(P, i - 1, j)]);
+    ucon[2 * N + n] -= h * (1 / (2 * P.dy)) * (P.gamma - 1) * (E[cid(P, i, j + 1)] - E[cid(P, i, j - 1)]);
+  }
+};
 
 // B* right-hand side (imex_subsystems.cpp:549-615) and initial guess x0 = Qe B
-__global__ void k_magnetic_rhs_B(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
-                                 const double* __restrict__ Qe, const double* __restrict__ Qs,
-                                 const double* __restrict__ pe, double* __restrict__ b, double* __restrict__ x0) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-  const double* arr[4] = {ucon, Qe, pe, Qs};
-  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
-  double out[3];
-  mag_rhs_B_cell<double>(P, h, nb, ld, out);
-  b[n] = out[0];
-  b[N + n] = out[1];
-  b[2 * N + n] = out[2];
-  x0[n] = Qe[5 * N + n];
-  x0[N + n] = Qe[6 * N + n];
-  x0[2 * N + n] = Qe[7 * N + n];
-}
+struct k_magnetic_rhs_B {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                                   const double* __restrict__ Qe, const double* __restrict__ Qs,
+                                   const double* __restrict__ pe, double* __restrict__ b, double* __restrict__ x0) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    long long nb[9];
+    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    const double* arr[4] = {ucon, Qe, pe, Qs};
+    auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+    double out[3];
+    mag_rhs_B_cell<double>(P, h, nb, ld, out);
+    b[n] = out[0];
+    b[N + n] = out[1];
+    b[2 * N + n] = out[2];
+    x0[n] = Qe[5 * N + n];
+    x0[N + n] = Qe[6 * N + n];
+    x0[2 * N + n] = Qe[7 * N + n];
+  }
+};
 // ---- local Lax-Friedrichs dissipation (GLF off)
 // The speed of cell m along dir (0: x, 1: y) from its conserved state Q:
 // 0.5 (|v| + sqrt(v^2 + 4 |B|^2 / rho)) of prim(Q) (implicit_operators.cpp:324-335, 473-480,
@@ -1853,121 +1884,136 @@ __device__ __forceinline__ double pv_speed(const DevParams& P, const double* __r
   return fabs(__ldg(Q + (5 + dir) * N + m) / sqrt(__ldg(Q + m)));
 }
 // CollectMagFluxes (ct_flux.cpp:5-130) (collect_cell), GLF or local dissipation
-__global__ void k_collect_mag_fluxes(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
-                                     const double* __restrict__ Qe, const double* __restrict__ pe,
-                                     double* __restrict__ Fx, double* __restrict__ Fy) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
-  const double* arr[3] = {ucon, Qe, pe};
-  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
-  double bmax[2] = {sc->B_max_x, sc->B_max_y};
-  if (!P.GLF) {  // the larger speed of the two cells of each face (ct_flux.cpp:79-87, 114-122)
-    bmax[0] = fmax(lf_speed(Qe, N, n, 0), lf_speed(Qe, N, nb[NB_E], 0));
-    bmax[1] = fmax(lf_speed(Qe, N, n, 1), lf_speed(Qe, N, nb[NB_N], 1));
+struct k_collect_mag_fluxes {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                                       const double* __restrict__ Qe, const double* __restrict__ pe,
+                                       double* __restrict__ Fx, double* __restrict__ Fy) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    long long nb[9];
+    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    const double* arr[3] = {ucon, Qe, pe};
+    auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+    double bmax[2] = {sc->B_max_x, sc->B_max_y};
+    if (!P.GLF) {  // the larger speed of the two cells of each face (ct_flux.cpp:79-87, 114-122)
+      bmax[0] = fmax(lf_speed(Qe, N, n, 0), lf_speed(Qe, N, nb[NB_E], 0));
+      bmax[1] = fmax(lf_speed(Qe, N, n, 1), lf_speed(Qe, N, nb[NB_N], 1));
+    }
+    double out[2];
+    collect_cell<double>(P, sc->h, bmax, nb, ld, out);
+    Fx[n] = out[0];
+    Fy[n] = out[1];
   }
-  double out[2];
-  collect_cell<double>(P, sc->h, bmax, nb, ld, out);
-  Fx[n] = out[0];
-  Fy[n] = out[1];
-}
+};
 
 // A** right-hand side (imex_subsystems.cpp:18-51), x0 = A
-__global__ void k_magnetic_rhs_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
-                                 const double* __restrict__ Qe, const double* __restrict__ pe,
-                                 const double* __restrict__ A_s, double* __restrict__ b) {
-  const long long N = P.N;
-  const double h = sc->h;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  // every input first, so that the divisions do not serialise the loads
-  const double Bxn = Qe[5 * N + n], Byn = Qe[6 * N + n], Bzn = Qe[7 * N + n];
-  const double rho = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
-  const double pxp = pe[cid(P, i + 1, j)], pxm = pe[cid(P, i - 1, j)], pyp = pe[cid(P, i, j + 1)],
-               pym = pe[cid(P, i, j - 1)];
-  const double a0 = A_s[n], a1 = A_s[N + n], a2 = A_s[2 * N + n];
-  const double Sx = m1 / rho - h / rho * (pxp - pxm) / (2.0 * P.dx);
-  const double Sy = m2 / rho - h / rho * (pyp - pym) / (2.0 * P.dy);
-  const double Sz = m3 / rho;
-  b[n] = a0 - h * (Byn * Sz - Bzn * Sy);
-  b[N + n] = a1 - h * (Bzn * Sx - Bxn * Sz);
-  b[2 * N + n] = a2 - h * (Bxn * Sy - Byn * Sx);
-}
+struct k_magnetic_rhs_A {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
+                                   const double* __restrict__ Qe, const double* __restrict__ pe,
+                                   const double* __restrict__ A_s, double* __restrict__ b) {
+    const long long N = P.N;
+    const double h = sc->h;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    // every input first, so that the divisions do not serialise the loads
+    const double Bxn = Qe[5 * N + n], Byn = Qe[6 * N + n], Bzn = Qe[7 * N + n];
+    const double rho = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
+    const double pxp = pe[cid(P, i + 1, j)], pxm = pe[cid(P, i - 1, j)], pyp = pe[cid(P, i, j + 1)],
+                 pym = pe[cid(P, i, j - 1)];
+    const double a0 = A_s[n], a1 = A_s[N + n], a2 = A_s[2 * N + n];
+    const double Sx = m1 / rho - h / rho * (pxp - pxm) / (2.0 * P.dx);
+    const double Sy = m2 / rho - h / rho * (pyp - pym) / (2.0 * P.dy);
+    const double Sz = m3 / rho;
+    b[n] = a0 - h * (Byn * Sz - Bzn * Sy);
+    b[N + n] = a1 - h * (Bzn * Sx - Bxn * Sz);
+    b[2 * N + n] = a2 - h * (Bxn * Sy - Byn * Sx);
+  }
+};
 // global A-viscosity maxima of prim(Qs) over real cells (implicit_operators.cpp:364-374)
-__global__ void k_gmax(DevParams P, const double* __restrict__ Qs, double* __restrict__ partial) {
-  double m0 = 0.0, m1 = 0.0;
-  // four cells per round, all loaded before the first division (the maxima do not depend
-  // on the order cells are visited in)
-  constexpr int kU = 4;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long n0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; n0 < P.N; n0 += kU * stride) {
-    double c[kU][8];
-#pragma unroll
-    for (int u = 0; u < kU; ++u)
-      if (n0 + u * stride < P.N) load_cell<8>(Qs, P.N, n0 + u * stride, c[u]);
-#pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      if (n0 + u * stride >= P.N) break;
-      double p[8];
-      con2pri(P, p, c[u]);
-      double Bsq = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
-      m0 = fmax(m0, 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4.0 * Bsq / p[0])));
-      m1 = fmax(m1, 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4.0 * Bsq / p[0])));
+struct k_gmax {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ Qs, double* __restrict__ partial) {
+    double m0 = 0.0, m1 = 0.0;
+    // four cells per round, all loaded before the first division (the maxima do not depend
+    // on the order cells are visited in)
+    constexpr int kU = 4;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long n0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; n0 < P.N; n0 += kU * stride) {
+      double c[kU][8];
+  #pragma unroll
+      for (int u = 0; u < kU; ++u)
+        if (n0 + u * stride < P.N) load_cell<8>(Qs, P.N, n0 + u * stride, c[u]);
+  #pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (n0 + u * stride >= P.N) break;
+        double p[8];
+        con2pri(P, p, c[u]);
+        double Bsq = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
+        m0 = fmax(m0, 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4.0 * Bsq / p[0])));
+        m1 = fmax(m1, 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4.0 * Bsq / p[0])));
+      }
+    }
+    __shared__ double sh[2][kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+      m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+      m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sh[0][threadIdx.x >> 5] = m0;
+      sh[1][threadIdx.x >> 5] = m1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        a = fmax(a, sh[0][w]);
+        b = fmax(b, sh[1][w]);
+      }
+      partial[2 * blockIdx.x] = a;
+      partial[2 * blockIdx.x + 1] = b;
     }
   }
-  __shared__ double sh[2][kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) {
-    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
-    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sh[0][threadIdx.x >> 5] = m0;
-    sh[1][threadIdx.x >> 5] = m1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      a = fmax(a, sh[0][w]);
-      b = fmax(b, sh[1][w]);
-    }
-    partial[2 * blockIdx.x] = a;
-    partial[2 * blockIdx.x + 1] = b;
-  }
-}
+};
 // r = 1 / a over n values (the A-form operator's 1/rho in the fast arithmetic)
-__global__ void k_recip(const double* __restrict__ a, double* __restrict__ r, long long n) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) r[i] = 1.0 / a[i];
-}
-__global__ void k_gmax_finalize(const double* __restrict__ partial, int nblk, DevScalars* sc) {
-  double a = 0.0, b = 0.0;
-  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
-    a = fmax(a, partial[2 * k]);
-    b = fmax(b, partial[2 * k + 1]);
+struct k_recip {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, const double* __restrict__ a, double* __restrict__ r, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) r[i] = 1.0 / a[i];
   }
-  __shared__ double sh[2][kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) {
-    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
-    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sh[0][threadIdx.x >> 5] = a;
-    sh[1][threadIdx.x >> 5] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-      a = fmax(a, sh[0][w]);
-      b = fmax(b, sh[1][w]);
+};
+struct k_gmax_finalize {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, const double* __restrict__ partial, int nblk, DevScalars* sc) {
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+      a = fmax(a, partial[2 * k]);
+      b = fmax(b, partial[2 * k + 1]);
     }
-    sc->gmax_bx = a;
-    sc->gmax_by = b;
+    __shared__ double sh[2][kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sh[0][threadIdx.x >> 5] = a;
+      sh[1][threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        a = fmax(a, sh[0][w]);
+        b = fmax(b, sh[1][w]);
+      }
+      sc->gmax_bx = a;
+      sc->gmax_by = b;
+    }
   }
-}
+};
 // ---- face viscosities of the local dissipation
 enum { LV_MAG_B = 0, LV_MAG_A = 1, LV_PRES = 2 };
 // The face viscosities of one solve, frozen like its other coefficients: plane f of lv holds,
@@ -1977,50 +2023,56 @@ enum { LV_MAG_B = 0, LV_MAG_A = 1, LV_PRES = 2 };
 //   LV_PRES:  (eta_nb + eta_c) / 2 max(s_c, s_nb) d (implicit_operators.cpp:584-607)
 // d is dx for the x faces and dy for the y faces; a neighbour outside a transmissive
 // direction is the nearest interior cell.
-__global__ void k_local_visc(DevParams P, int mode, const double* __restrict__ Q, const double* __restrict__ eta,
-                             double* __restrict__ lv) {
-  const long long N = P.N;
-  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const long long nbr[4] = {cid(P, i + 1, j), cid(P, i - 1, j), cid(P, i, j + 1), cid(P, i, j - 1)};
-  double own[2], out[4];
-  if (mode == LV_PRES) {
-    own[0] = pv_speed(P, Q, N, n, 0);
-    own[1] = pv_speed(P, Q, N, n, 1);
-    const double ec = __ldg(eta + n);
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const int dir = f >> 1;
-      const double nu = fmax(own[dir], pv_speed(P, Q, N, nbr[f], dir)) * (dir ? P.dy : P.dx);
-      out[f] = 0.5 * (__ldg(eta + nbr[f]) + ec) * nu;
+struct k_local_visc {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, int mode, const double* __restrict__ Q, const double* __restrict__ eta,
+                               double* __restrict__ lv) {
+    const long long N = P.N;
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const long long nbr[4] = {cid(P, i + 1, j), cid(P, i - 1, j), cid(P, i, j + 1), cid(P, i, j - 1)};
+    double own[2], out[4];
+    if (mode == LV_PRES) {
+      own[0] = pv_speed(P, Q, N, n, 0);
+      own[1] = pv_speed(P, Q, N, n, 1);
+      const double ec = __ldg(eta + n);
+  #pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int dir = f >> 1;
+        const double nu = fmax(own[dir], pv_speed(P, Q, N, nbr[f], dir)) * (dir ? P.dy : P.dx);
+        out[f] = 0.5 * (__ldg(eta + nbr[f]) + ec) * nu;
+      }
+    } else {
+      own[0] = lf_speed(Q, N, n, 0);
+      own[1] = lf_speed(Q, N, n, 1);
+  #pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int dir = f >> 1;
+        const double b = lf_speed(Q, N, nbr[f], dir), d = dir ? P.dy : P.dx;
+        out[f] = mode == LV_MAG_B ? fmax(own[dir], b) * d : 0.5 * (own[dir] + b) * d;
+      }
     }
-  } else {
-    own[0] = lf_speed(Q, N, n, 0);
-    own[1] = lf_speed(Q, N, n, 1);
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const int dir = f >> 1;
-      const double b = lf_speed(Q, N, nbr[f], dir), d = dir ? P.dy : P.dx;
-      out[f] = mode == LV_MAG_B ? fmax(own[dir], b) * d : 0.5 * (own[dir] + b) * d;
-    }
+  #pragma unroll
+    for (int f = 0; f < 4; ++f) lv[f * N + n] = out[f];
   }
-#pragma unroll
-  for (int f = 0; f < 4; ++f) lv[f * N + n] = out[f];
-}
+};
 // B = curl A after the A solve (imex_subsystems.cpp:65-72)
 template <bool kOpen>
-__global__ void k_curl_A(DevParams Pin, const double* __restrict__ A, double* __restrict__ ucon) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  auto Ak = [&](int k, int di, int dj) { return a_ghost(P, A + k * N, i + di, j + dj); };
-  ucon[5 * N + n] = 1 / (2.0 * P.dy) * (Ak(2, 0, 1) - Ak(2, 0, -1));
-  ucon[6 * N + n] = -1 / (2.0 * P.dx) * (Ak(2, 1, 0) - Ak(2, -1, 0));
-  ucon[7 * N + n] = 1 / (2.0 * P.dx) * (Ak(1, 1, 0) - Ak(1, -1, 0)) - 1 / (2.0 * P.dy) * (Ak(0, 0, 1) - Ak(0, 0, -1));
-}
+struct k_curl_A {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ A, double* __restrict__ ucon) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    auto Ak = [&](int k, int di, int dj) { return a_ghost(P, A + k * N, i + di, j + dj); };
+    ucon[5 * N + n] = 1 / (2.0 * P.dy) * (Ak(2, 0, 1) - Ak(2, 0, -1));
+    ucon[6 * N + n] = -1 / (2.0 * P.dx) * (Ak(2, 1, 0) - Ak(2, -1, 0));
+    ucon[7 * N + n] = 1 / (2.0 * P.dx) * (Ak(1, 1, 0) - Ak(1, -1, 0)) - 1 / (2.0 * P.dy) * (Ak(0, 0, 1) - Ak(0, 0, -1));
+  }
+};
 
 // ------------------------------------------------------------------ plain operator application
 template <class Op>
@@ -2235,11 +2287,11 @@ imex_status energy_setup(imex_ctx* ctx) {
   const DevParams& P = ctx->P;
   int nb = blocks_for(P.N);
   prof_begin(ctx);
-  k_energy_coeffs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->Qe, ctx->cons, ctx->hh);
+  launch<k_energy_coeffs>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->Qe, ctx->cons, ctx->hh);
   LAUNCH_CHECK(ctx, "k_energy_coeffs");
   prof_end(ctx, F_PRES_SETUP, BYTES(10), 1);
   prof_begin(ctx);
-  k_energy_rhs<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->hh, ctx->pb, ctx->tdiag);
+  launch<k_energy_rhs>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->hh, ctx->pb, ctx->tdiag);
   LAUNCH_CHECK(ctx, "k_energy_rhs");
   prof_end(ctx, F_PRES_RHS, BYTES(6), 1);
   return IMEX_OK;
@@ -2247,7 +2299,7 @@ imex_status energy_setup(imex_ctx* ctx) {
 imex_status energy_momentum(imex_ctx* ctx) {
   int nb = blocks_for(ctx->P.N);
   prof_begin(ctx);
-  k_energy_momentum<<<nb, kThreads, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->cons);
+  launch<k_energy_momentum>(ctx, nb, kThreads, 0, ctx->stream, ctx->P, ctx->sc, ctx->cons);
   LAUNCH_CHECK(ctx, "k_energy_momentum");
   prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
   return IMEX_OK;
@@ -2260,9 +2312,9 @@ imex_status local_visc(imex_ctx* ctx, int mode) {
   const int nb = blocks_for(P.N);
   prof_begin(ctx);
   if (mode == LV_PRES)
-    k_local_visc<<<nb, kThreads, 0, ctx->stream>>>(P, mode, ctx->Qe, ctx->eta, ctx->lvp);
+    launch<k_local_visc>(ctx, nb, kThreads, 0, ctx->stream, P, mode, ctx->Qe, ctx->eta, ctx->lvp);
   else
-    k_local_visc<<<nb, kThreads, 0, ctx->stream>>>(P, mode, mode == LV_MAG_A ? ctx->Qs : ctx->Qe, nullptr, ctx->lvm);
+    launch<k_local_visc>(ctx, nb, kThreads, 0, ctx->stream, P, mode, mode == LV_MAG_A ? ctx->Qs : ctx->Qe, nullptr, ctx->lvm);
   LAUNCH_CHECK(ctx, "k_local_visc");
   prof_end(ctx, mode == LV_PRES ? F_PRES_SETUP : F_MAG_RHS, BYTES(mode == LV_PRES ? 8 : 10), 1);
   return IMEX_OK;
@@ -2651,7 +2703,7 @@ namespace {
 }  // namespace
 // gmax_bx / gmax_by from the per-CTA maxima k_stage_combine left in partial
 imex_status gmax_finalize(imex_ctx* ctx, int nblk) {
-  k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nblk, ctx->sc);
+  launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nblk, ctx->sc);
   LAUNCH_CHECK(ctx, "k_gmax_finalize");
   return IMEX_OK;
 }
@@ -2680,18 +2732,18 @@ imex_status mag_rhs(imex_ctx* ctx) {
     if (!ctx->gmax_ready) {  // the stage combination did not take the maxima of this Qs
       int nred = nb < ctx->max_blocks ? nb : ctx->max_blocks;
       prof_begin(ctx);
-      k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
+      launch<k_gmax>(ctx, nred, kThreads, 0, ctx->stream, P, ctx->Qs, ctx->partial);
       LAUNCH_CHECK(ctx, "k_gmax");
-      k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
+      launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
       LAUNCH_CHECK(ctx, "k_gmax_finalize");
       prof_end(ctx, F_GMAX, BYTES(8), 2);
     }
     ctx->gmax_ready = false;
     prof_begin(ctx);
-    k_magnetic_rhs_A<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
+    launch<k_magnetic_rhs_A>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
     LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
     if (P.fast) {
-      k_recip<<<nb, kThreads, 0, ctx->stream>>>(ctx->cons, ctx->irho, P.N);
+      launch<k_recip>(ctx, nb, kThreads, 0, ctx->stream, ctx->cons, ctx->irho, P.N);
       LAUNCH_CHECK(ctx, "k_recip");
     }
     prof_end(ctx, F_MAG_RHS, BYTES(P.fast ? 16 : 14), P.fast ? 2 : 1);
@@ -2700,7 +2752,7 @@ imex_status mag_rhs(imex_ctx* ctx) {
   prof_begin(ctx);
   // the initial guess Qe B goes straight into the cell B planes of u_con (planes 5-7; the
   // kernel reads only planes 0-3 of u_con), which GMRES then overwrites with the solution
-  k_magnetic_rhs_B<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->Qs, ctx->pe, ctx->mb,
+  launch<k_magnetic_rhs_B>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->Qe, ctx->Qs, ctx->pe, ctx->mb,
                                                     ctx->cons + 5 * P.N);
   LAUNCH_CHECK(ctx, "k_magnetic_rhs_B");
   prof_end(ctx, F_MAG_RHS, BYTES(17), 1);
@@ -2725,7 +2777,7 @@ imex_status mag_out(imex_ctx* ctx) {
     LAUNCH_CHECK(ctx, "k_curl_A");
     prof_end(ctx, F_MAG_OUT, BYTES(6), 1);
   } else {
-    k_collect_mag_fluxes<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
+    launch<k_collect_mag_fluxes>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->Fx, ctx->Fy);
     LAUNCH_CHECK(ctx, "k_collect_mag_fluxes");
     prof_end(ctx, F_COLLECT_FLUX, BYTES(12), 1);
   }
@@ -2768,7 +2820,7 @@ imex_status pres_part2(imex_ctx* ctx, int rks, bool* second) {
     return energy_momentum(ctx);
   }
   prof_begin(ctx);
-  k_momentum<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->rv, ctx->cons);
+  launch<k_momentum>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->pp, ctx->rv, ctx->cons);
   LAUNCH_CHECK(ctx, "k_momentum");
   prof_end(ctx, F_MOMENTUM, BYTES(5), 1);
   *second = P.PressureSolver == IMEX_all_correction || (P.PressureSolver == IMEX_once_correction && rks == P.RKs - 1);
@@ -2787,12 +2839,12 @@ imex_status pres_part3(imex_ctx* ctx) {
   int nb = blocks_for(P.N);
   prof_begin(ctx);
   if (P.U_update == IMEX_ConservationofU) {
-    k_energy_conservation<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->sc, ctx->pp, ctx->cons);
+    launch<k_energy_conservation>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->pp, ctx->cons);
     LAUNCH_CHECK(ctx, "k_energy_conservation");
     prof_end(ctx, F_ENERGY, BYTES(6), 1);  // p, rho, rho vx, rho vy, E in; E out
     return IMEX_OK;
   }
-  k_energy_define<<<nb, kThreads, 0, ctx->stream>>>(P, ctx->pp, ctx->cons);
+  launch<k_energy_define>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->pp, ctx->cons);
   LAUNCH_CHECK(ctx, "k_energy_define");
   prof_end(ctx, F_ENERGY, BYTES(9), 1);
   return IMEX_OK;
@@ -2821,15 +2873,15 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
   if (op == IMEX_OP_MAGNETIC_A) {
     const DevParams& P = ctx->P;
     int nred = blocks_for(P.N) < ctx->max_blocks ? blocks_for(P.N) : ctx->max_blocks;
-    k_gmax<<<nred, kThreads, 0, ctx->stream>>>(P, ctx->Qs, ctx->partial);
-    k_gmax_finalize<<<1, kThreads, 0, ctx->stream>>>(ctx->partial, nred, ctx->sc);
+    launch<k_gmax>(ctx, nred, kThreads, 0, ctx->stream, P, ctx->Qs, ctx->partial);
+    launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
     LAUNCH_CHECK(ctx, "k_gmax");
   }
   if ((op == IMEX_OP_MAGNETIC_A || op == IMEX_OP_MAGNETIC_B) &&
       (s = local_visc(ctx, op == IMEX_OP_MAGNETIC_A ? LV_MAG_A : LV_MAG_B)) != IMEX_OK)
     return s;
   if (op == IMEX_OP_MAGNETIC_A && ctx->P.fast) {
-    k_recip<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->cons, ctx->irho, ctx->P.N);
+    launch<k_recip>(ctx, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, ctx->cons, ctx->irho, ctx->P.N);
     LAUNCH_CHECK(ctx, "k_recip");
   }
   if ((s = set_h(ctx, h)) != IMEX_OK) return s;

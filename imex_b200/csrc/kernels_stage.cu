@@ -9,6 +9,7 @@
 #include <cstring>
 
 #include "cells.cuh"
+#include "launch.cuh"
 
 namespace imex {
 
@@ -59,88 +60,97 @@ __device__ inline void block_reduce(double (&v)[K], F f, double identity) {
 // calch / calca / caldt maxima / MagneticEigenvalues over the primitive state,
 // timestep.cpp:5-148,254-273.  Max is exact, so block order does not matter.
 constexpr int kStepVals = 11;
-__global__ void k_step_reduce(DevParams P, const double* __restrict__ prim, double* __restrict__ partial) {
-  double v[kStepVals];
-  v[0] = v[1] = v[2] = v[3] = v[4] = v[5] = 1e-8;  // ch_x ch_y ch cA_x cA_y cA
-  v[6] = v[7] = v[8] = v[9] = v[10] = 0.0;         // |vx| |vy| |v| bmax_x bmax_y
-  const long long N = P.N;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
-    double p[8];
-    load_cell<8>(prim, N, n, p);
-    double B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
-    double B = sqrt(B2);
-    double vv = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
-    double cfx = eos_fast(P, p[0], p[4], p[5], B2);
-    double cfy = eos_fast(P, p[0], p[4], p[6], B2);
-    double cf = eos_fast(P, p[0], p[4], B, B2);
-    v[0] = fmax(v[0], p[1] + cfx);
-    v[1] = fmax(v[1], p[2] + cfy);
-    v[2] = fmax(v[2], vv + cf);
-    v[3] = fmax(v[3], p[5] / sqrt(p[0]));
-    v[4] = fmax(v[4], p[6] / sqrt(p[0]));
-    v[5] = fmax(v[5], B / sqrt(p[0]));
-    v[6] = fmax(v[6], fabs(p[1]));
-    v[7] = fmax(v[7], fabs(p[2]));
-    v[8] = fmax(v[8], vv);
-    v[9] = fmax(v[9], 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4 * B2 / p[0])));
-    v[10] = fmax(v[10], 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4 * B2 / p[0])));
+struct k_step_reduce {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ prim, double* __restrict__ partial) {
+    double v[kStepVals];
+    v[0] = v[1] = v[2] = v[3] = v[4] = v[5] = 1e-8;  // ch_x ch_y ch cA_x cA_y cA
+    v[6] = v[7] = v[8] = v[9] = v[10] = 0.0;         // |vx| |vy| |v| bmax_x bmax_y
+    const long long N = P.N;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+      double p[8];
+      load_cell<8>(prim, N, n, p);
+      double B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
+      double B = sqrt(B2);
+      double vv = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+      double cfx = eos_fast(P, p[0], p[4], p[5], B2);
+      double cfy = eos_fast(P, p[0], p[4], p[6], B2);
+      double cf = eos_fast(P, p[0], p[4], B, B2);
+      v[0] = fmax(v[0], p[1] + cfx);
+      v[1] = fmax(v[1], p[2] + cfy);
+      v[2] = fmax(v[2], vv + cf);
+      v[3] = fmax(v[3], p[5] / sqrt(p[0]));
+      v[4] = fmax(v[4], p[6] / sqrt(p[0]));
+      v[5] = fmax(v[5], B / sqrt(p[0]));
+      v[6] = fmax(v[6], fabs(p[1]));
+      v[7] = fmax(v[7], fabs(p[2]));
+      v[8] = fmax(v[8], vv);
+      v[9] = fmax(v[9], 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4 * B2 / p[0])));
+      v[10] = fmax(v[10], 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4 * B2 / p[0])));
+    }
+    block_reduce(v, FMax(), -INFINITY);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < kStepVals; ++k) partial[blockIdx.x * kStepVals + k] = v[k];
   }
-  block_reduce(v, FMax(), -INFINITY);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < kStepVals; ++k) partial[blockIdx.x * kStepVals + k] = v[k];
-}
+};
 
 // caldt (timestep.cpp:5-67) + main.cpp:341-353 on one thread
-__global__ void k_step_finalize(DevParams P, const double* __restrict__ partial, int nblk, DevScalars* sc) {
-  double v[kStepVals];
-  for (int k = 0; k < kStepVals; ++k) v[k] = -INFINITY;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
-    for (int k = 0; k < kStepVals; ++k) v[k] = fmax(v[k], partial[b * kStepVals + k]);
-  block_reduce(v, FMax(), -INFINITY);
-  if (threadIdx.x != 0) return;
-  sc->timestep += 1;
-  const int ts = sc->timestep;
-  sc->ch_x = v[0];
-  sc->ch_y = v[1];
-  sc->ch = v[2];
-  sc->cA_x = v[3];
-  sc->cA_y = v[4];
-  sc->cA = v[5];
-  sc->vx_max = v[6];
-  sc->vy_max = v[7];
-  sc->v_max = v[8];
-  const int full_step = 1;
-  double a_max;
-  if (P.caltimestep == IMEX_Fullydt) a_max = sc->ch;
-  else if (P.caltimestep == IMEX_Alfvendt) a_max = (ts < full_step + 1) ? sc->ch : sc->cA;
-  else a_max = (ts < full_step + 1) ? sc->ch : sc->v_max;
-  double dt = P.CFL * 1 / (2 * a_max / fmin(P.dx, P.dy));
-  if (ts > 1 && sc->prev_dt > 0.0) dt = fmin(dt, 2.0 * sc->prev_dt);
-  sc->prev_dt = dt;
-  if (ts > full_step) a_max = sc->v_max;
-  sc->a_max = a_max;
-  dt = fmin(dt, P.time_stop - sc->t);
-  if (P.fixed_dt > 0.0) dt = fmin(P.fixed_dt, P.time_stop - sc->t);
-  sc->dt = dt;
-  sc->B_max_x = v[9];
-  sc->B_max_y = v[10];
-  sc->t = sc->t + dt;
-}
+struct k_step_finalize {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ partial, int nblk, DevScalars* sc) {
+    double v[kStepVals];
+    for (int k = 0; k < kStepVals; ++k) v[k] = -INFINITY;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+      for (int k = 0; k < kStepVals; ++k) v[k] = fmax(v[k], partial[b * kStepVals + k]);
+    block_reduce(v, FMax(), -INFINITY);
+    if (threadIdx.x != 0) return;
+    sc->timestep += 1;
+    const int ts = sc->timestep;
+    sc->ch_x = v[0];
+    sc->ch_y = v[1];
+    sc->ch = v[2];
+    sc->cA_x = v[3];
+    sc->cA_y = v[4];
+    sc->cA = v[5];
+    sc->vx_max = v[6];
+    sc->vy_max = v[7];
+    sc->v_max = v[8];
+    const int full_step = 1;
+    double a_max;
+    if (P.caltimestep == IMEX_Fullydt) a_max = sc->ch;
+    else if (P.caltimestep == IMEX_Alfvendt) a_max = (ts < full_step + 1) ? sc->ch : sc->cA;
+    else a_max = (ts < full_step + 1) ? sc->ch : sc->v_max;
+    double dt = P.CFL * 1 / (2 * a_max / fmin(P.dx, P.dy));
+    if (ts > 1 && sc->prev_dt > 0.0) dt = fmin(dt, 2.0 * sc->prev_dt);
+    sc->prev_dt = dt;
+    if (ts > full_step) a_max = sc->v_max;
+    sc->a_max = a_max;
+    dt = fmin(dt, P.time_stop - sc->t);
+    if (P.fixed_dt > 0.0) dt = fmin(P.fixed_dt, P.time_stop - sc->t);
+    sc->dt = dt;
+    sc->B_max_x = v[9];
+    sc->B_max_y = v[10];
+    sc->t = sc->t + dt;
+  }
+};
 
 // cons = pri2con(prim); cons_n = cons  (main.cpp:356-358)
-__global__ void k_cons_from_prim(DevParams P, const double* __restrict__ prim, double* __restrict__ cons,
-                                 double* __restrict__ cons_n) {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= P.N) return;
-  double p[8], c[8];
-  load_cell<8>(prim, P.N, n, p);
-  pri2con(P, c, p);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    cons[k * P.N + n] = c[k];
-    if (cons_n) cons_n[k * P.N + n] = c[k];
+struct k_cons_from_prim {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ prim, double* __restrict__ cons,
+                                   double* __restrict__ cons_n) {
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= P.N) return;
+    double p[8], c[8];
+    load_cell<8>(prim, P.N, n, p);
+    pri2con(P, c, p);
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      cons[k * P.N + n] = c[k];
+      if (cons_n) cons_n[k * P.N + n] = c[k];
+    }
   }
-}
+};
 __global__ void k_prim_from_cons(DevParams P, const double* __restrict__ cons, double* __restrict__ prim) {
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= P.N) return;
@@ -163,180 +173,189 @@ struct Tableau {
 // it has just formed, one fmax pair per CTA into partial[2 * block], which saves the
 // separate pass over Qs.
 template <int R, bool kG>
-__global__ void __launch_bounds__(kThreads) k_stage_combine(DevParams P, Tableau T, DevScalars* sc, const double* __restrict__ cons_n,
-                                const double* __restrict__ Hs, const double* __restrict__ bx_n,
-                                const double* __restrict__ by_n, const double* __restrict__ HsB,
-                                const double* __restrict__ A_snap, const double* __restrict__ HsA,
-                                double* __restrict__ Qe, double* __restrict__ Qs, double* __restrict__ bxQe,
-                                double* __restrict__ byQe, double* __restrict__ bxQs, double* __restrict__ byQs,
-                                double* __restrict__ A_s, double* __restrict__ A_e, double* __restrict__ A,
-                                double* __restrict__ pe, double* __restrict__ hQe,
-                                double* __restrict__ partial) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double dt = sc->dt;
-  if (n == 0) {
-    sc->adt = T.aii * dt;
-    sc->h = T.aii * dt;
-  }
-  double g0 = 0.0, g1 = 0.0;
-  if (n < N) {
-  constexpr int RR = R > 0 ? R : 1;
-  double u[8], h[RR][8], a[3], ha[RR][3], fx = bx_n[n], fy = by_n[n], hb[RR][2];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) u[k] = cons_n[k * N + n];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) a[k] = A_snap[k * N + n];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) h[r][k] = Hs[((long long)r * 8 + k) * N + n];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) ha[r][k] = HsA[((long long)r * 3 + k) * N + n];
-    hb[r][0] = HsB[((long long)r * 2 + 0) * N + n];
-    hb[r][1] = HsB[((long long)r * 2 + 1) * N + n];
-  }
-  double qe[8], qs[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    double e = u[k], s = e;
-#pragma unroll
+struct k_stage_combine {
+  IMEX_BOUNDS(kThreads, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, Tableau T, DevScalars* sc, const double* __restrict__ cons_n,
+                                  const double* __restrict__ Hs, const double* __restrict__ bx_n,
+                                  const double* __restrict__ by_n, const double* __restrict__ HsB,
+                                  const double* __restrict__ A_snap, const double* __restrict__ HsA,
+                                  double* __restrict__ Qe, double* __restrict__ Qs, double* __restrict__ bxQe,
+                                  double* __restrict__ byQe, double* __restrict__ bxQs, double* __restrict__ byQs,
+                                  double* __restrict__ A_s, double* __restrict__ A_e, double* __restrict__ A,
+                                  double* __restrict__ pe, double* __restrict__ hQe,
+                                  double* __restrict__ partial) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const double dt = sc->dt;
+    if (n == 0) {
+      sc->adt = T.aii * dt;
+      sc->h = T.aii * dt;
+    }
+    double g0 = 0.0, g1 = 0.0;
+    if (n < N) {
+    constexpr int RR = R > 0 ? R : 1;
+    double u[8], h[RR][8], a[3], ha[RR][3], fx = bx_n[n], fy = by_n[n], hb[RR][2];
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) u[k] = cons_n[k * N + n];
+  #pragma unroll
+    for (int k = 0; k < 3; ++k) a[k] = A_snap[k * N + n];
+  #pragma unroll
     for (int r = 0; r < R; ++r) {
-      e = e + T.ae[r] * dt * h[r][k];
-      s = s + T.ai[r] * dt * h[r][k];
+  #pragma unroll
+      for (int k = 0; k < 8; ++k) h[r][k] = Hs[((long long)r * 8 + k) * N + n];
+  #pragma unroll
+      for (int k = 0; k < 3; ++k) ha[r][k] = HsA[((long long)r * 3 + k) * N + n];
+      hb[r][0] = HsB[((long long)r * 2 + 0) * N + n];
+      hb[r][1] = HsB[((long long)r * 2 + 1) * N + n];
     }
-    qe[k] = e;
-    qs[k] = s;
-    Qe[k * N + n] = e;
-    Qs[k * N + n] = s;
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    double e = a[k], s = e;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      e += T.ae[r] * dt * ha[r][k];
-      s += T.ai[r] * dt * ha[r][k];
-    }
-    A_e[k * N + n] = e;
-    A_s[k * N + n] = s;
-    A[k * N + n] = s;
-  }
-  double fxe = fx, fxs = fxe, fye = fy, fys = fye;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    fxe += T.ae[r] * dt * hb[r][0];
-    fye += T.ae[r] * dt * hb[r][1];
-    fxs += T.ai[r] * dt * hb[r][0];
-    fys += T.ai[r] * dt * hb[r][1];
-  }
-  bxQe[n] = fxe;
-  byQe[n] = fye;
-  bxQs[n] = fxs;
-  byQs[n] = fys;
-  double e = calecon(qe);
-  double p = eos_p(P, qe[0], e);
-  pe[n] = p;
-  hQe[n] = e + p / qe[0];
-  if constexpr (kG) {
-    const double vx = qs[1] / qs[0], vy = qs[2] / qs[0];
-    const double Bsq = qs[5] * qs[5] + qs[6] * qs[6] + qs[7] * qs[7];
-    g0 = fmax(g0, 0.5 * (fabs(vx) + sqrt(vx * vx + 4.0 * Bsq / qs[0])));
-    g1 = fmax(g1, 0.5 * (fabs(vy) + sqrt(vy * vy + 4.0 * Bsq / qs[0])));
-  }
-  }
-  if constexpr (kG) {
-    __shared__ double sh[2][kThreads / 32];
-    for (int o = 16; o > 0; o >>= 1) {
-      g0 = fmax(g0, __shfl_xor_sync(0xffffffffu, g0, o));
-      g1 = fmax(g1, __shfl_xor_sync(0xffffffffu, g1, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-      sh[0][threadIdx.x >> 5] = g0;
-      sh[1][threadIdx.x >> 5] = g1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int w = 1; w < kThreads / 32; ++w) {
-        g0 = fmax(g0, sh[0][w]);
-        g1 = fmax(g1, sh[1][w]);
+    double qe[8], qs[8];
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      double e = u[k], s = e;
+  #pragma unroll
+      for (int r = 0; r < R; ++r) {
+        e = e + T.ae[r] * dt * h[r][k];
+        s = s + T.ai[r] * dt * h[r][k];
       }
-      partial[2 * blockIdx.x] = g0;
-      partial[2 * blockIdx.x + 1] = g1;
+      qe[k] = e;
+      qs[k] = s;
+      Qe[k * N + n] = e;
+      Qs[k * N + n] = s;
+    }
+  #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double e = a[k], s = e;
+  #pragma unroll
+      for (int r = 0; r < R; ++r) {
+        e += T.ae[r] * dt * ha[r][k];
+        s += T.ai[r] * dt * ha[r][k];
+      }
+      A_e[k * N + n] = e;
+      A_s[k * N + n] = s;
+      A[k * N + n] = s;
+    }
+    double fxe = fx, fxs = fxe, fye = fy, fys = fye;
+  #pragma unroll
+    for (int r = 0; r < R; ++r) {
+      fxe += T.ae[r] * dt * hb[r][0];
+      fye += T.ae[r] * dt * hb[r][1];
+      fxs += T.ai[r] * dt * hb[r][0];
+      fys += T.ai[r] * dt * hb[r][1];
+    }
+    bxQe[n] = fxe;
+    byQe[n] = fye;
+    bxQs[n] = fxs;
+    byQs[n] = fys;
+    double e = calecon(qe);
+    double p = eos_p(P, qe[0], e);
+    pe[n] = p;
+    hQe[n] = e + p / qe[0];
+    if constexpr (kG) {
+      const double vx = qs[1] / qs[0], vy = qs[2] / qs[0];
+      const double Bsq = qs[5] * qs[5] + qs[6] * qs[6] + qs[7] * qs[7];
+      g0 = fmax(g0, 0.5 * (fabs(vx) + sqrt(vx * vx + 4.0 * Bsq / qs[0])));
+      g1 = fmax(g1, 0.5 * (fabs(vy) + sqrt(vy * vy + 4.0 * Bsq / qs[0])));
+    }
+    }
+    if constexpr (kG) {
+      __shared__ double sh[2][kThreads / 32];
+      for (int o = 16; o > 0; o >>= 1) {
+        g0 = fmax(g0, __shfl_xor_sync(0xffffffffu, g0, o));
+        g1 = fmax(g1, __shfl_xor_sync(0xffffffffu, g1, o));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        sh[0][threadIdx.x >> 5] = g0;
+        sh[1][threadIdx.x >> 5] = g1;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 1; w < kThreads / 32; ++w) {
+          g0 = fmax(g0, sh[0][w]);
+          g1 = fmax(g1, sh[1][w]);
+        }
+        partial[2 * blockIdx.x] = g0;
+        partial[2 * blockIdx.x + 1] = g1;
+      }
     }
   }
-}
+};
 
 // ---------------------------------------------------------------- reconstruction
 // TVDReconstruction (reconstruction.cpp:5-287) of Q into w = [xL | xR | yL | yR] x 8 planes,
 // PrimState (the ConsState form is k_reconstruct_var below).
 // nstore = number of conserved variables written (5 for the stage, 8 for the full buffer).
 template <bool kOpen, bool kFast>
-__global__ void k_reconstruct_prim(DevParams Pin, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  long long ix[5], iy[5];
-#pragma unroll
-  for (int d = 0; d < 5; ++d) {
-    ix[d] = cid(P, i + d - 2, j);
-    iy[d] = cid(P, i, j + d - 2);
-  }
-  const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
-  // PrimState: reconstruct primitive variables, convert each face state back (reconstruction.cpp:272-281)
-  double px[5][8], py[5][8];
-#pragma unroll
-  for (int d = 0; d < 5; ++d) {
+struct k_reconstruct_prim {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ Q, double* __restrict__ w, int nstore) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    long long ix[5], iy[5];
+  #pragma unroll
+    for (int d = 0; d < 5; ++d) {
+      ix[d] = cid(P, i + d - 2, j);
+      iy[d] = cid(P, i, j + d - 2);
+    }
+    const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
+    // PrimState: reconstruct primitive variables, convert each face state back (reconstruction.cpp:272-281)
+    double px[5][8], py[5][8];
+  #pragma unroll
+    for (int d = 0; d < 5; ++d) {
+      double c[8];
+      load_cell<8>(Q, N, ix[d], c);
+      con2pri(P, px[d], c);
+      load_cell<8>(Q, N, iy[d], c);
+      con2pri(P, py[d], c);
+    }
+    double wxl[8], wxr[8], wyl[8], wyr[8];
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      recon_1d<kFast>(P.recon, px[0][k], px[1][k], px[2][k], px[3][k], px[4][k], wxl[k], wxr[k], false);
+      recon_1d<kFast>(P.recon, py[0][k], py[1][k], py[2][k], py[3][k], py[4][k], wyl[k], wyr[k], vortex);
+    }
     double c[8];
-    load_cell<8>(Q, N, ix[d], c);
-    con2pri(P, px[d], c);
-    load_cell<8>(Q, N, iy[d], c);
-    con2pri(P, py[d], c);
+    double* outs[4] = {wxl, wxr, wyl, wyr};
+  #pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      pri2con(P, c, outs[q]);
+      for (int k = 0; k < nstore; ++k) w[(q * 8 + k) * N + n] = c[k];
+    }
   }
-  double wxl[8], wxr[8], wyl[8], wyr[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    recon_1d<kFast>(P.recon, px[0][k], px[1][k], px[2][k], px[3][k], px[4][k], wxl[k], wxr[k], false);
-    recon_1d<kFast>(P.recon, py[0][k], py[1][k], py[2][k], py[3][k], py[4][k], wyl[k], wyr[k], vortex);
-  }
-  double c[8];
-  double* outs[4] = {wxl, wxr, wyl, wyr};
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    pri2con(P, c, outs[q]);
-    for (int k = 0; k < nstore; ++k) w[(q * 8 + k) * N + n] = c[k];
-  }
-}
+};
 
 // ConsState reconstructs every conserved variable on its own (reconstruction.cpp:5-266), so
 // one thread per (cell, variable) pair: variable k = blockIdx.y.  The same recon_1d calls as a
 // per-cell loop over the variables, with a small per-thread working set and 5-8x the threads.
 template <bool kOpen, bool kFast>
-__global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, const double* __restrict__ Q,
-                                                               double* __restrict__ w) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int k = blockIdx.y;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
-  const double* a = Q + k * N;
-  double v[5], u[5];  // both stencils loaded before the divisions of the first reconstruction
-#pragma unroll
-  for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i + d - 2, j));
-#pragma unroll
-  for (int d = 0; d < 5; ++d) u[d] = __ldg(a + cid(P, i, j + d - 2));
-  double xl, xr, yl, yr;
-  recon_1d<kFast>(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
-  recon_1d<kFast>(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
-  w[(0 * 8 + k) * N + n] = xl;
-  w[(1 * 8 + k) * N + n] = xr;
-  w[(2 * 8 + k) * N + n] = yl;
-  w[(3 * 8 + k) * N + n] = yr;
-}
+struct k_reconstruct_var {
+  IMEX_BOUNDS(kThreads, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ Q,
+                                                                 double* __restrict__ w) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int k = blockIdx.y;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
+    const double* a = Q + k * N;
+    double v[5], u[5];  // both stencils loaded before the divisions of the first reconstruction
+  #pragma unroll
+    for (int d = 0; d < 5; ++d) v[d] = __ldg(a + cid(P, i + d - 2, j));
+  #pragma unroll
+    for (int d = 0; d < 5; ++d) u[d] = __ldg(a + cid(P, i, j + d - 2));
+    double xl, xr, yl, yr;
+    recon_1d<kFast>(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
+    recon_1d<kFast>(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
+    w[(0 * 8 + k) * N + n] = xl;
+    w[(1 * 8 + k) * N + n] = xr;
+    w[(2 * 8 + k) * N + n] = yl;
+    w[(3 * 8 + k) * N + n] = yr;
+  }
+};
 
 // ---------------------------------------------------------------- flux updates
 // RusanovC_Update (flux.cpp:409-455) or Pressure_flux_Update (flux.cpp:290-326) with the
@@ -347,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) k_reconstruct_var(DevParams Pin, con
 // fp / fm are the fluxes of the faces at i +- 1/2, gp / gm those at j +- 1/2.
 constexpr int FTX = 32, FTY = 8, FNT = FTX * FTY;
 template <int kForm, bool kFast>
-__device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* __restrict__ sc,
+__device__ __forceinline__ void flux_tile(IMEX_BLK, const DevParams& P, const DevScalars* __restrict__ sc,
                                           const double* __restrict__ w, const double* __restrict__ Qs,
                                           double* __restrict__ ucon) {
   __shared__ double fx[5][FTY][FTX + 1];  // fx[.][ly][fi]: face between cells x0 + fi - 1 and x0 + fi
@@ -405,26 +424,35 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const DevScalars* 
 // The register budgets were measured: the convective form runs fastest as the compiler
 // chooses, the pressure and energy forms at three CTAs per SM.
 template <bool kOpen, bool kFast>
-__global__ void __launch_bounds__(FNT) k_flux_conv(DevParams Pin, const DevScalars* __restrict__ sc,
-                                                   const double* __restrict__ w, const double* __restrict__ Qs,
-                                                   double* __restrict__ ucon) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  flux_tile<0, kFast>(P, sc, w, Qs, ucon);
-}
-template <int kForm, bool kOpen, bool kFast>
-__global__ void __launch_bounds__(FNT, 3) k_flux_mag(DevParams Pin, const DevScalars* __restrict__ sc,
+struct k_flux_conv {
+  IMEX_BOUNDS(FNT, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc,
                                                      const double* __restrict__ w, const double* __restrict__ Qs,
                                                      double* __restrict__ ucon) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  flux_tile<kForm, kFast>(P, sc, w, Qs, ucon);
-}
+    const DevParams P = bc_params<kOpen>(Pin);
+    flux_tile<0, kFast>(blockIdx, gridDim, P, sc, w, Qs, ucon);
+  }
+};
+template <int kForm, bool kOpen, bool kFast>
+struct k_flux_mag {
+  IMEX_BOUNDS(FNT, 3)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc,
+                                                       const double* __restrict__ w, const double* __restrict__ Qs,
+                                                       double* __restrict__ ucon) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    flux_tile<kForm, kFast>(blockIdx, gridDim, P, sc, w, Qs, ucon);
+  }
+};
 template <bool kOpen, bool kFast>
-__global__ void __launch_bounds__(FNT, 3) k_flux_pres(DevParams Pin, const DevScalars* __restrict__ sc,
-                                                      const double* __restrict__ w, const double* __restrict__ Qs,
-                                                      double* __restrict__ ucon) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  flux_tile<1, kFast>(P, sc, w, Qs, ucon);
-}
+struct k_flux_pres {
+  IMEX_BOUNDS(FNT, 3)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc,
+                                                        const double* __restrict__ w, const double* __restrict__ Qs,
+                                                        double* __restrict__ ucon) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    flux_tile<1, kFast>(blockIdx, gridDim, P, sc, w, Qs, ucon);
+  }
+};
 
 // ---------------------------------------------------------------- constrained transport
 // corner EMF (ci + 1/2, cj + 1/2) for ci, cj >= -1 (ct_corner_at): Ez_bar on the corner
@@ -442,28 +470,31 @@ __device__ __forceinline__ double corner_emf(const DevParams& P, double sx, doub
 }
 // Corner EMF of u_con and the collected face fluxes (ct_corner_cell); on a transmissive
 // direction the first column / row of threads also writes the boundary corners (-1/2).
-__global__ void k_ct_corner(DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
-                            double sy, const double* __restrict__ ucon, double* __restrict__ Epp, BoundaryLines L) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  long long nb[9];
-  neighbours(P, i, j, nb);
-  const double* arr[3] = {fx, fy, ucon};
-  auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
-  double out[1];
-  ct_corner_cell<double>(P, sx, sy, nb, ld, out);
-  Epp[n] = out[0];
-  if (P.xclamp && i == 0) {
-    L.ex[j + 1] = corner_emf(P, sx, sy, -1, j, ld);
-    if (j == 0) L.ex[0] = corner_emf(P, sx, sy, -1, -1, ld);
+struct k_ct_corner {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ fx, double sx, const double* __restrict__ fy,
+                              double sy, const double* __restrict__ ucon, double* __restrict__ Epp, BoundaryLines L) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    long long nb[9];
+    neighbours(P, i, j, nb);
+    const double* arr[3] = {fx, fy, ucon};
+    auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
+    double out[1];
+    ct_corner_cell<double>(P, sx, sy, nb, ld, out);
+    Epp[n] = out[0];
+    if (P.xclamp && i == 0) {
+      L.ex[j + 1] = corner_emf(P, sx, sy, -1, j, ld);
+      if (j == 0) L.ex[0] = corner_emf(P, sx, sy, -1, -1, ld);
+    }
+    if (P.yclamp && j == 0) {
+      L.ey[i + 1] = corner_emf(P, sx, sy, i, -1, ld);
+      if (i == 0) L.ey[0] = corner_emf(P, sx, sy, -1, -1, ld);
+    }
   }
-  if (P.yclamp && j == 0) {
-    L.ey[i + 1] = corner_emf(P, sx, sy, i, -1, ld);
-    if (i == 0) L.ey[0] = corner_emf(P, sx, sy, -1, -1, ld);
-  }
-}
+};
 // corner (ci + 1/2, cj + 1/2), ci, cj >= -1, from the corner plane and the boundary lines
 __device__ __forceinline__ double corner_read(const DevParams& P, const double* __restrict__ Epp,
                                               const BoundaryLines& L, int ci, int cj) {
@@ -477,133 +508,154 @@ __device__ __forceinline__ double corner_read(const DevParams& P, const double* 
 // On a transmissive direction the faces left of / below the first column / row are the
 // boundary faces (their own lines, corner EMFs from the boundary corners), which the
 // first column / row of threads also stores.
-__global__ void k_ct_faces(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
-                           const double* __restrict__ bxQs, const double* __restrict__ byQs, double* __restrict__ bx,
-                           double* __restrict__ by, double* __restrict__ ucon, BoundaryLines L) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double h = sc->h;
-  const bool xb = P.xclamp && i == 0, yb = P.yclamp && j == 0;
-  double e00 = __ldg(Epp + n), em0 = corner_read(P, Epp, L, i - 1, j), e0m = corner_read(P, Epp, L, i, j - 1);
-  double emm = corner_read(P, Epp, L, i - 1, j - 1);
-  double fx = __ldg(bxQs + n) - h / P.dy * (e00 - e0m);
-  double fy = __ldg(byQs + n) + h / P.dx * (e00 - em0);
-  double fxm = (xb ? L.bxQs[j] : __ldg(bxQs + cid(P, i - 1, j))) - h / P.dy * (em0 - emm);
-  double fym = (yb ? L.byQs[i] : __ldg(byQs + cid(P, i, j - 1))) + h / P.dx * (e0m - emm);
-  bx[n] = fx;
-  by[n] = fy;
-  if (xb) L.bx[j] = fxm;
-  if (yb) L.by[i] = fym;
-  ucon[5 * N + n] = 0.5 * (fxm + fx);
-  ucon[6 * N + n] = 0.5 * (fym + fy);
-}
+struct k_ct_faces {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
+                             const double* __restrict__ bxQs, const double* __restrict__ byQs, double* __restrict__ bx,
+                             double* __restrict__ by, double* __restrict__ ucon, BoundaryLines L) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double h = sc->h;
+    const bool xb = P.xclamp && i == 0, yb = P.yclamp && j == 0;
+    double e00 = __ldg(Epp + n), em0 = corner_read(P, Epp, L, i - 1, j), e0m = corner_read(P, Epp, L, i, j - 1);
+    double emm = corner_read(P, Epp, L, i - 1, j - 1);
+    double fx = __ldg(bxQs + n) - h / P.dy * (e00 - e0m);
+    double fy = __ldg(byQs + n) + h / P.dx * (e00 - em0);
+    double fxm = (xb ? L.bxQs[j] : __ldg(bxQs + cid(P, i - 1, j))) - h / P.dy * (em0 - emm);
+    double fym = (yb ? L.byQs[i] : __ldg(byQs + cid(P, i, j - 1))) + h / P.dx * (e0m - emm);
+    bx[n] = fx;
+    by[n] = fy;
+    if (xb) L.bx[j] = fxm;
+    if (yb) L.by[i] = fym;
+    ucon[5 * N + n] = 0.5 * (fxm + fx);
+    ucon[6 * N + n] = 0.5 * (fym + fy);
+  }
+};
 // Stage combination (main.cpp:397-407) and stage derivative (main.cpp:550-551) of the
 // boundary-face lines of the transmissive directions; thread q handles row q of the x_0
 // line and column q of the y_0 line.
-__global__ void k_bline_combine(DevParams P, Tableau T, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const double dt = sc->dt;
-  if (P.xclamp && q < P.ny) {
-    double fe = L.bx_n[q], fs = fe;
-    for (int r = 0; r < rks; ++r) {
-      const double h0 = L.hsbx[(long long)r * P.ny + q];
-      fe += T.ae[r] * dt * h0;
-      fs += T.ai[r] * dt * h0;
+struct k_bline_combine {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, Tableau T, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dt = sc->dt;
+    if (P.xclamp && q < P.ny) {
+      double fe = L.bx_n[q], fs = fe;
+      for (int r = 0; r < rks; ++r) {
+        const double h0 = L.hsbx[(long long)r * P.ny + q];
+        fe += T.ae[r] * dt * h0;
+        fs += T.ai[r] * dt * h0;
+      }
+      L.bxQe[q] = fe;
+      L.bxQs[q] = fs;
     }
-    L.bxQe[q] = fe;
-    L.bxQs[q] = fs;
-  }
-  if (P.yclamp && q < P.nx) {
-    double fe = L.by_n[q], fs = fe;
-    for (int r = 0; r < rks; ++r) {
-      const double h1 = L.hsby[(long long)r * P.nx + q];
-      fe += T.ae[r] * dt * h1;
-      fs += T.ai[r] * dt * h1;
+    if (P.yclamp && q < P.nx) {
+      double fe = L.by_n[q], fs = fe;
+      for (int r = 0; r < rks; ++r) {
+        const double h1 = L.hsby[(long long)r * P.nx + q];
+        fe += T.ae[r] * dt * h1;
+        fs += T.ai[r] * dt * h1;
+      }
+      L.byQe[q] = fe;
+      L.byQs[q] = fs;
     }
-    L.byQe[q] = fe;
-    L.byQs[q] = fs;
   }
-}
-__global__ void k_bline_derivative(DevParams P, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const double adt = sc->adt;
-  if (P.xclamp && q < P.ny) L.hsbx[(long long)rks * P.ny + q] = (L.bx[q] - L.bxQs[q]) / adt;
-  if (P.yclamp && q < P.nx) L.hsby[(long long)rks * P.nx + q] = (L.by[q] - L.byQs[q]) / adt;
-}
+};
+struct k_bline_derivative {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, int rks, const DevScalars* __restrict__ sc, BoundaryLines L) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const double adt = sc->adt;
+    if (P.xclamp && q < P.ny) L.hsbx[(long long)rks * P.ny + q] = (L.bx[q] - L.bxQs[q]) / adt;
+    if (P.yclamp && q < P.nx) L.hsby[(long long)rks * P.nx + q] = (L.by[q] - L.byQs[q]) / adt;
+  }
+};
 // Unstaggered_CT_Consistent A_z update (constrained_transport.cpp:523-529)
-__global__ void k_ct_unstag_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
-                              const double* __restrict__ A_s, double* __restrict__ A, BoundaryLines L) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  double Ec = 0.25 * (__ldg(Epp + n) + corner_read(P, Epp, L, i - 1, j) + corner_read(P, Epp, L, i, j - 1) +
-                      corner_read(P, Epp, L, i - 1, j - 1));
-  A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
-}
+struct k_ct_unstag_A {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ Epp,
+                                const double* __restrict__ A_s, double* __restrict__ A, BoundaryLines L) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    double Ec = 0.25 * (__ldg(Epp + n) + corner_read(P, Epp, L, i - 1, j) + corner_read(P, Epp, L, i, j - 1) +
+                        corner_read(P, Epp, L, i - 1, j - 1));
+    A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
+  }
+};
 // Unstaggered_CT upwind A_z advection (constrained_transport.cpp:436-488)
 __device__ __forceinline__ double vanleer_lim(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return 2.0 * a * b / (a + b);
 }
-__global__ void k_ct_unstag_legacy_A(DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ u,
-                                     const double* __restrict__ A_s, double* __restrict__ A) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double h = sc->h, dx = P.dx, dy = P.dy;
-  const double* As = A_s + 2 * N;
-  auto vxc = [&](long long m) { return __ldg(u + N + m) / __ldg(u + m); };
-  auto vyc = [&](long long m) { return __ldg(u + 2 * N + m) / __ldg(u + m); };
-  long long c = n, xm = cid(P, i - 1, j), xp = cid(P, i + 1, j), xmm = cid(P, i - 2, j), xpp = cid(P, i + 2, j);
-  long long ym = cid(P, i, j - 1), yp = cid(P, i, j + 1), ymm = cid(P, i, j - 2), ypp = cid(P, i, j + 2);
-  double uL = 0.5 * (vxc(xm) + vxc(c)), uR = 0.5 * (vxc(c) + vxc(xp));
-  double dAL = As[c] - As[xm], dAR = As[xp] - As[c], dALL = As[xm] - As[xmm], dARR = As[xpp] - As[xp];
-  double fluct_x = fmax(uL, 0.0) * dAL + fmin(uR, 0.0) * dAR;
-  double corrL = 0.5 * fabs(uL) * (1.0 - fabs(uL) * h / dx) * vanleer_lim(dAL, (uL >= 0.0 ? dALL : dAR));
-  double corrR = 0.5 * fabs(uR) * (1.0 - fabs(uR) * h / dx) * vanleer_lim(dAR, (uR >= 0.0 ? dAL : dARR));
-  double dAdt_x = fluct_x / dx + (corrR - corrL) / dx;
-  double vL = 0.5 * (vyc(ym) + vyc(c)), vR = 0.5 * (vyc(c) + vyc(yp));
-  double dAB = As[c] - As[ym], dAT = As[yp] - As[c], dABB = As[ym] - As[ymm], dATT = As[ypp] - As[yp];
-  double fluct_y = fmax(vL, 0.0) * dAB + fmin(vR, 0.0) * dAT;
-  double corrB = 0.5 * fabs(vL) * (1.0 - fabs(vL) * h / dy) * vanleer_lim(dAB, (vL >= 0.0 ? dABB : dAT));
-  double corrT = 0.5 * fabs(vR) * (1.0 - fabs(vR) * h / dy) * vanleer_lim(dAT, (vR >= 0.0 ? dAB : dATT));
-  double dAdt_y = fluct_y / dy + (corrT - corrB) / dy;
-  A[2 * N + n] = As[c] - h * (dAdt_x + dAdt_y);
-}
+struct k_ct_unstag_legacy_A {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ u,
+                                       const double* __restrict__ A_s, double* __restrict__ A) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double h = sc->h, dx = P.dx, dy = P.dy;
+    const double* As = A_s + 2 * N;
+    auto vxc = [&](long long m) { return __ldg(u + N + m) / __ldg(u + m); };
+    auto vyc = [&](long long m) { return __ldg(u + 2 * N + m) / __ldg(u + m); };
+    long long c = n, xm = cid(P, i - 1, j), xp = cid(P, i + 1, j), xmm = cid(P, i - 2, j), xpp = cid(P, i + 2, j);
+    long long ym = cid(P, i, j - 1), yp = cid(P, i, j + 1), ymm = cid(P, i, j - 2), ypp = cid(P, i, j + 2);
+    double uL = 0.5 * (vxc(xm) + vxc(c)), uR = 0.5 * (vxc(c) + vxc(xp));
+    double dAL = As[c] - As[xm], dAR = As[xp] - As[c], dALL = As[xm] - As[xmm], dARR = As[xpp] - As[xp];
+    double fluct_x = fmax(uL, 0.0) * dAL + fmin(uR, 0.0) * dAR;
+    double corrL = 0.5 * fabs(uL) * (1.0 - fabs(uL) * h / dx) * vanleer_lim(dAL, (uL >= 0.0 ? dALL : dAR));
+    double corrR = 0.5 * fabs(uR) * (1.0 - fabs(uR) * h / dx) * vanleer_lim(dAR, (uR >= 0.0 ? dAL : dARR));
+    double dAdt_x = fluct_x / dx + (corrR - corrL) / dx;
+    double vL = 0.5 * (vyc(ym) + vyc(c)), vR = 0.5 * (vyc(c) + vyc(yp));
+    double dAB = As[c] - As[ym], dAT = As[yp] - As[c], dABB = As[ym] - As[ymm], dATT = As[ypp] - As[yp];
+    double fluct_y = fmax(vL, 0.0) * dAB + fmin(vR, 0.0) * dAT;
+    double corrB = 0.5 * fabs(vL) * (1.0 - fabs(vL) * h / dy) * vanleer_lim(dAB, (vL >= 0.0 ? dABB : dAT));
+    double corrT = 0.5 * fabs(vR) * (1.0 - fabs(vR) * h / dy) * vanleer_lim(dAT, (vR >= 0.0 ? dAB : dATT));
+    double dAdt_y = fluct_y / dy + (corrT - corrB) / dy;
+    A[2 * N + n] = As[c] - h * (dAdt_x + dAdt_y);
+  }
+};
 // B = curl A_z for the unstaggered schemes (constrained_transport.cpp:533-538)
-__global__ void k_curl_Az(DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double* Az = A + 2 * N;
-  ucon[5 * N + n] = (a_ghost(P, Az, i, j + 1) - a_ghost(P, Az, i, j - 1)) / (2.0 * P.dy);
-  ucon[6 * N + n] = -(a_ghost(P, Az, i + 1, j) - a_ghost(P, Az, i - 1, j)) / (2.0 * P.dx);
-}
+struct k_curl_Az {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ A, double* __restrict__ ucon) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double* Az = A + 2 * N;
+    ucon[5 * N + n] = (a_ghost(P, Az, i, j + 1) - a_ghost(P, Az, i, j - 1)) / (2.0 * P.dy);
+    ucon[6 * N + n] = -(a_ghost(P, Az, i + 1, j) - a_ghost(P, Az, i - 1, j)) / (2.0 * P.dx);
+  }
+};
 // Face EMFs of the legacy Staggered_CT from the reconstruction of u_con
 // (constrained_transport.cpp:73-97): Ez_p0 = -(f6_L + f6_R)/2, Ez_0p = (g5_L + g5_R)/2.
-__global__ void k_ct_legacy_faces(DevParams P, const double* __restrict__ w, double* __restrict__ ep0,
-                                  double* __restrict__ e0p) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
-  const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
-  auto f6 = [&](const double* q, long long m) {
-    double r = __ldg(q + m);
-    return __ldg(q + 6 * N + m) * (__ldg(q + N + m) / r) - (__ldg(q + 2 * N + m) / r) * __ldg(q + 5 * N + m);
-  };
-  auto g5 = [&](const double* q, long long m) {
-    double r = __ldg(q + m);
-    return __ldg(q + 5 * N + m) * (__ldg(q + 2 * N + m) / r) - (__ldg(q + N + m) / r) * __ldg(q + 6 * N + m);
-  };
-  ep0[n] = -(0.5 * (f6(wxR, n) + f6(wxL, cid(P, i + 1, j))));
-  e0p[n] = (0.5 * (g5(wyR, n) + g5(wyL, cid(P, i, j + 1))));
-}
+struct k_ct_legacy_faces {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ w, double* __restrict__ ep0,
+                                    double* __restrict__ e0p) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
+    auto f6 = [&](const double* q, long long m) {
+      double r = __ldg(q + m);
+      return __ldg(q + 6 * N + m) * (__ldg(q + N + m) / r) - (__ldg(q + 2 * N + m) / r) * __ldg(q + 5 * N + m);
+    };
+    auto g5 = [&](const double* q, long long m) {
+      double r = __ldg(q + m);
+      return __ldg(q + 5 * N + m) * (__ldg(q + 2 * N + m) / r) - (__ldg(q + N + m) / r) * __ldg(q + 6 * N + m);
+    };
+    ep0[n] = -(0.5 * (f6(wxR, n) + f6(wxL, cid(P, i + 1, j))));
+    e0p[n] = (0.5 * (g5(wyR, n) + g5(wyL, cid(P, i, j + 1))));
+  }
+};
 
 // ---------------------------------------------------------------- CT EMF diagnostics
 // Diagnose_CT_EMF (constrained_transport.cpp:183-222), printed by the reference's driver after
@@ -683,48 +735,51 @@ __global__ void k_ct_diag_stats(DevParams P, const double* __restrict__ cp0, con
 
 // ---------------------------------------------------------------- stage derivative
 // Energy_Modify (main.cpp:528-534), Hs / HsA / HsB (main.cpp:539-555), u_pri (main.cpp:537).
-__global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __restrict__ sc, double* __restrict__ cons,
-                                   const double* __restrict__ Qs, const double* __restrict__ A,
-                                   const double* __restrict__ A_s, const double* __restrict__ bx,
-                                   const double* __restrict__ bxQs, const double* __restrict__ by,
-                                   const double* __restrict__ byQs, const double* __restrict__ Bsave,
-                                   double* __restrict__ Hs, double* __restrict__ HsA, double* __restrict__ HsB,
-                                   double* __restrict__ prim) {
-  const long long N = P.N;
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const double adt = sc->adt;
-  // every input first, so that the divisions below do not serialise the loads
-  double c[8], qs[8], a[3], as[3], o[3];
-  load_cell<8>(cons, N, n, c);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) qs[k] = Qs[k * N + n];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    a[k] = A[k * N + n];
-    as[k] = A_s[k * N + n];
+struct k_stage_derivative {
+  IMEX_BOUNDS(0, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, int rks, const DevScalars* __restrict__ sc, double* __restrict__ cons,
+                                     const double* __restrict__ Qs, const double* __restrict__ A,
+                                     const double* __restrict__ A_s, const double* __restrict__ bx,
+                                     const double* __restrict__ bxQs, const double* __restrict__ by,
+                                     const double* __restrict__ byQs, const double* __restrict__ Bsave,
+                                     double* __restrict__ Hs, double* __restrict__ HsA, double* __restrict__ HsB,
+                                     double* __restrict__ prim) {
+    const long long N = P.N;
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double adt = sc->adt;
+    // every input first, so that the divisions below do not serialise the loads
+    double c[8], qs[8], a[3], as[3], o[3];
+    load_cell<8>(cons, N, n, c);
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) qs[k] = Qs[k * N + n];
+  #pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      a[k] = A[k * N + n];
+      as[k] = A_s[k * N + n];
+    }
+    const double fx = bx[n], fxs = bxQs[n], fy = by[n], fys = byQs[n];
+    if (P.Energy_Modify) {
+  #pragma unroll
+      for (int k = 0; k < 3; ++k) o[k] = Bsave[k * N + n];
+      c[4] = c[4] + ((c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) - (o[0] * o[0] + o[1] * o[1] + o[2] * o[2])) / 2.0;
+      cons[4 * N + n] = c[4];
+    }
+    double* H = Hs + (long long)rks * 8 * N;
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) H[k * N + n] = (c[k] - qs[k]) / adt;
+    double* HA = HsA + (long long)rks * 3 * N;
+  #pragma unroll
+    for (int k = 0; k < 3; ++k) HA[k * N + n] = (a[k] - as[k]) / adt;
+    double* HB = HsB + (long long)rks * 2 * N;
+    HB[n] = (fx - fxs) / adt;
+    HB[N + n] = (fy - fys) / adt;
+    double p[8];
+    con2pri(P, p, c);
+  #pragma unroll
+    for (int k = 0; k < 8; ++k) prim[k * N + n] = p[k];
   }
-  const double fx = bx[n], fxs = bxQs[n], fy = by[n], fys = byQs[n];
-  if (P.Energy_Modify) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o[k] = Bsave[k * N + n];
-    c[4] = c[4] + ((c[5] * c[5] + c[6] * c[6] + c[7] * c[7]) - (o[0] * o[0] + o[1] * o[1] + o[2] * o[2])) / 2.0;
-    cons[4 * N + n] = c[4];
-  }
-  double* H = Hs + (long long)rks * 8 * N;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) H[k * N + n] = (c[k] - qs[k]) / adt;
-  double* HA = HsA + (long long)rks * 3 * N;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) HA[k * N + n] = (a[k] - as[k]) / adt;
-  double* HB = HsB + (long long)rks * 2 * N;
-  HB[n] = (fx - fxs) / adt;
-  HB[N + n] = (fy - fys) / adt;
-  double p[8];
-  con2pri(P, p, c);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) prim[k * N + n] = p[k];
-}
+};
 
 // ---------------------------------------------------------------- shock detector
 // ShockDetector (flux.cpp:5-76): fast speed per cell, chi~ (4.40), chi = 3x3 max (4.41), as
@@ -737,73 +792,76 @@ __global__ void k_stage_derivative(DevParams P, int rks, const DevScalars* __res
 // position, which lies in the same tile.
 constexpr int STX = 32, STY = 16, SHX = STX + 4, SHY = STY + 4, SCX = STX + 2, SCY = STY + 2;
 template <bool kOpen>
-__global__ void __launch_bounds__(kThreads) k_shock(DevParams Pin, const double* __restrict__ Q,
-                                                     double* __restrict__ eta, double* __restrict__ chit) {
-  const DevParams P = bc_params<kOpen>(Pin);
-  const long long N = P.N;
-  __shared__ double cf[SHY * SHX];  // c_f at (x0 - 2 + sx, y0 - 2 + sy)
-  __shared__ double ch[SCY * SCX];  // chi~ at (x0 - 1 + px, y0 - 1 + py)
-  const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
-  {  // each thread's cells of the halo-2 tile, every load before the first division
-    constexpr int KC = (SHY * SHX + kThreads - 1) / kThreads;
-    double c[KC][8];
-#pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      const int q = threadIdx.x + k * kThreads;
-      const int qq = q < SHY * SHX ? q : SHY * SHX - 1;  // past the end: a staged cell, loaded again
-      load_cell<8>(Q, N, cid(P, x0 - 2 + qq % SHX, y0 - 2 + qq / SHX), c[k]);
-    }
-#pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      const int q = threadIdx.x + k * kThreads;
-      if (q < SHY * SHX) {
-        const double p = pressure_of(P, c[k]);
-        const double a2 = eos_a2(P, c[k][0], p);
-        const double cA2 = (c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7]) / c[k][0];
-        cf[q] = sqrt(a2 + cA2);
+struct k_shock {
+  IMEX_BOUNDS(kThreads, 0)
+  static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ Q,
+                                                       double* __restrict__ eta, double* __restrict__ chit) {
+    const DevParams P = bc_params<kOpen>(Pin);
+    const long long N = P.N;
+    __shared__ double cf[SHY * SHX];  // c_f at (x0 - 2 + sx, y0 - 2 + sy)
+    __shared__ double ch[SCY * SCX];  // chi~ at (x0 - 1 + px, y0 - 1 + py)
+    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
+    {  // each thread's cells of the halo-2 tile, every load before the first division
+      constexpr int KC = (SHY * SHX + kThreads - 1) / kThreads;
+      double c[KC][8];
+  #pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int q = threadIdx.x + k * kThreads;
+        const int qq = q < SHY * SHX ? q : SHY * SHX - 1;  // past the end: a staged cell, loaded again
+        load_cell<8>(Q, N, cid(P, x0 - 2 + qq % SHX, y0 - 2 + qq / SHX), c[k]);
+      }
+  #pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int q = threadIdx.x + k * kThreads;
+        if (q < SHY * SHX) {
+          const double p = pressure_of(P, c[k]);
+          const double a2 = eos_a2(P, c[k][0], p);
+          const double cA2 = (c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7]) / c[k][0];
+          cf[q] = sqrt(a2 + cA2);
+        }
       }
     }
+    __syncthreads();
+    for (int q = threadIdx.x; q < SCY * SCX; q += kThreads) {
+      int gi = x0 - 1 + q % SCX, gj = y0 - 1 + q / SCX;
+      if (P.xclamp) gi = gi < 0 ? 0 : (gi >= P.nx ? P.nx - 1 : gi);
+      if (P.yclamp) gj = gj < 0 ? 0 : (gj >= P.ny ? P.ny - 1 : gj);
+      const int sx = gi - x0 + 2, sy = gj - y0 + 2;  // within [1, SHX - 2] x [1, SHY - 2]
+      double m = 1.0e300;
+      for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++) {
+          double v = cf[(sy + dj) * SHX + sx + di];
+          if (v < m) m = v;
+        }
+      long long xp = cid(P, gi + 1, gj), xm = cid(P, gi - 1, gj), yp = cid(P, gi, gj + 1), ym = cid(P, gi, gj - 1);
+      // every load before the first division
+      const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
+      const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
+      double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
+      double num = P.hmin * div_u + P.shock_kappa1 * m;
+      double den = P.shock_kappa1 * m;
+      double qv = -num / den;
+      double mx = (0.0 < qv) ? qv : 0.0;
+      ch[q] = (mx < 1.0) ? mx : 1.0;
+      // chi~ of the tile's own cells, when asked for (chit != nullptr)
+      const int lx = q % SCX - 1, ly = q / SCX - 1;
+      if (chit && lx >= 0 && lx < STX && ly >= 0 && ly < STY && x0 + lx < P.nx && y0 + ly < P.ny)
+        chit[(long long)(y0 + ly) * P.nx + (x0 + lx)] = ch[q];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < STX * STY; q += kThreads) {
+      const int lx = q % STX, ly = q / STX, i = x0 + lx, j = y0 + ly;
+      if (i >= P.nx || j >= P.ny) continue;
+      double m = 0.0;
+      for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++) {
+          double v = ch[(ly + 1 + dj) * SCX + lx + 1 + di];
+          if (v > m) m = v;
+        }
+      eta[(long long)j * P.nx + i] = m;
+    }
   }
-  __syncthreads();
-  for (int q = threadIdx.x; q < SCY * SCX; q += kThreads) {
-    int gi = x0 - 1 + q % SCX, gj = y0 - 1 + q / SCX;
-    if (P.xclamp) gi = gi < 0 ? 0 : (gi >= P.nx ? P.nx - 1 : gi);
-    if (P.yclamp) gj = gj < 0 ? 0 : (gj >= P.ny ? P.ny - 1 : gj);
-    const int sx = gi - x0 + 2, sy = gj - y0 + 2;  // within [1, SHX - 2] x [1, SHY - 2]
-    double m = 1.0e300;
-    for (int di = -1; di <= 1; di++)
-      for (int dj = -1; dj <= 1; dj++) {
-        double v = cf[(sy + dj) * SHX + sx + di];
-        if (v < m) m = v;
-      }
-    long long xp = cid(P, gi + 1, gj), xm = cid(P, gi - 1, gj), yp = cid(P, gi, gj + 1), ym = cid(P, gi, gj - 1);
-    // every load before the first division
-    const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
-    const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
-    double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
-    double num = P.hmin * div_u + P.shock_kappa1 * m;
-    double den = P.shock_kappa1 * m;
-    double qv = -num / den;
-    double mx = (0.0 < qv) ? qv : 0.0;
-    ch[q] = (mx < 1.0) ? mx : 1.0;
-    // chi~ of the tile's own cells, when asked for (chit != nullptr)
-    const int lx = q % SCX - 1, ly = q / SCX - 1;
-    if (chit && lx >= 0 && lx < STX && ly >= 0 && ly < STY && x0 + lx < P.nx && y0 + ly < P.ny)
-      chit[(long long)(y0 + ly) * P.nx + (x0 + lx)] = ch[q];
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < STX * STY; q += kThreads) {
-    const int lx = q % STX, ly = q / STX, i = x0 + lx, j = y0 + ly;
-    if (i >= P.nx || j >= P.ny) continue;
-    double m = 0.0;
-    for (int di = -1; di <= 1; di++)
-      for (int dj = -1; dj <= 1; dj++) {
-        double v = ch[(ly + 1 + dj) * SCX + lx + 1 + di];
-        if (v > m) m = v;
-      }
-    eta[(long long)j * P.nx + i] = m;
-  }
-}
+};
 
 // ---------------------------------------------------------------- diagnostics
 // face FV div (StaggerCT; a transmissive direction's first column / row differences against
@@ -889,22 +947,20 @@ imex_status launch_step_prologue(imex_ctx* ctx) {
   int nblk = blocks_for(P.N);
   if (nblk > ctx->max_blocks) nblk = ctx->max_blocks;
   prof_begin(ctx);
-  k_step_reduce<<<nblk, kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->partial);
+  launch<k_step_reduce>(ctx, nblk, kThreads, 0, ctx->stream, P, ctx->prim, ctx->partial);
   LAUNCH_CHECK(ctx, "k_step_reduce");
-  k_step_finalize<<<1, kThreads, 0, ctx->stream>>>(P, ctx->partial, nblk, ctx->sc);
+  launch<k_step_finalize>(ctx, 1, kThreads, 0, ctx->stream, P, ctx->partial, nblk, ctx->sc);
   LAUNCH_CHECK(ctx, "k_step_finalize");
   prof_end(ctx, F_PROLOGUE_REDUCE, BYTES(8), 2);
   prof_begin(ctx);
-  k_cons_from_prim<<<blocks_for(P.N), kThreads, 0, ctx->stream>>>(P, ctx->prim, ctx->cons, ctx->cons_n);
+  launch<k_cons_from_prim>(ctx, blocks_for(P.N), kThreads, 0, ctx->stream, P, ctx->prim, ctx->cons, ctx->cons_n);
   LAUNCH_CHECK(ctx, "k_cons_from_prim");
-  const size_t plane = ctx->N * sizeof(double);
-  cudaError_t e = cudaMemcpyAsync(ctx->bx_n, ctx->bx, plane, cudaMemcpyDeviceToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->by_n, ctx->by, plane, cudaMemcpyDeviceToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->A_snap, ctx->A, 3 * plane, cudaMemcpyDeviceToDevice, ctx->stream);
-  if (e == cudaSuccess && P.xclamp)
-    e = cudaMemcpyAsync(ctx->bl.bx_n, ctx->bl.bx, P.ny * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-  if (e == cudaSuccess && P.yclamp)
-    e = cudaMemcpyAsync(ctx->bl.by_n, ctx->bl.by, P.nx * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+  const long long plane = (long long)ctx->N;
+  cudaError_t e = copy_d2d(ctx, ctx->bx_n, ctx->bx, plane);
+  if (e == cudaSuccess) e = copy_d2d(ctx, ctx->by_n, ctx->by, plane);
+  if (e == cudaSuccess) e = copy_d2d(ctx, ctx->A_snap, ctx->A, 3 * plane);
+  if (e == cudaSuccess && P.xclamp) e = copy_d2d(ctx, ctx->bl.bx_n, ctx->bl.bx, P.ny);
+  if (e == cudaSuccess && P.yclamp) e = copy_d2d(ctx, ctx->bl.by_n, ctx->bl.by, P.nx);
   prof_end(ctx, F_CONS_FROM_PRIM, BYTES(24 + 10), 1);
   return cuda_check(ctx, e, "step snapshot copies");
 }
@@ -923,7 +979,7 @@ imex_status launch_vslope(imex_ctx* ctx) {
 }
 
 imex_status launch_cons_from_prim(imex_ctx* ctx) {
-  k_cons_from_prim<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(ctx->P, ctx->prim, ctx->cons, nullptr);
+  launch<k_cons_from_prim>(ctx, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, ctx->P, ctx->prim, ctx->cons, nullptr);
   LAUNCH_CHECK(ctx, "k_cons_from_prim");
   return IMEX_OK;
 }
@@ -973,12 +1029,21 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
   // the A form's viscosity maxima come with the combination while one pair per CTA fits
   // the partial buffer; otherwise the magnetic sub-system takes them in its own pass
   const bool g = ctx->P.magfield == IMEX_PotentialA && 2LL * nb <= ctx->partial_len;
-  auto kern = g ? (rks == 0 ? k_stage_combine<0, true> : (rks == 1 ? k_stage_combine<1, true> : k_stage_combine<2, true>))
-                : (rks == 0 ? k_stage_combine<0, false> : (rks == 1 ? k_stage_combine<1, false> : k_stage_combine<2, false>));
-  kern<<<nb, kThreads, 0, ctx->stream>>>(
-      ctx->P, T, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n, ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe,
-      ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s, ctx->A_e, ctx->A, ctx->pe, ctx->hQe,
-      ctx->partial);
+  auto combine = [&](auto k) {
+    using K = decltype(k);
+    launch<K>(ctx, nb, kThreads, 0, ctx->stream, ctx->P, T, ctx->sc, ctx->cons_n, ctx->Hs, ctx->bx_n, ctx->by_n,
+              ctx->HsB, ctx->A_snap, ctx->HsA, ctx->Qe, ctx->Qs, ctx->bxQe, ctx->byQe, ctx->bxQs, ctx->byQs, ctx->A_s,
+              ctx->A_e, ctx->A, ctx->pe, ctx->hQe, ctx->partial);
+  };
+  if (g) {
+    if (rks == 0) combine(k_stage_combine<0, true>{});
+    else if (rks == 1) combine(k_stage_combine<1, true>{});
+    else combine(k_stage_combine<2, true>{});
+  } else {
+    if (rks == 0) combine(k_stage_combine<0, false>{});
+    else if (rks == 1) combine(k_stage_combine<1, false>{});
+    else combine(k_stage_combine<2, false>{});
+  }
   LAUNCH_CHECK(ctx, "k_stage_combine");
   ctx->gmax_ready = false;
   if (g) {
@@ -987,7 +1052,7 @@ imex_status launch_stage_combine(imex_ctx* ctx, int rks) {
     ctx->gmax_ready = true;
   }
   if (ctx->P.xclamp || ctx->P.yclamp) {
-    k_bline_combine<<<blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream>>>(ctx->P, T, rks,
+    launch<k_bline_combine>(ctx, blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream, ctx->P, T, rks,
                                                                                                    ctx->sc, ctx->bl);
     LAUNCH_CHECK(ctx, "k_bline_combine");
   }
@@ -1019,9 +1084,9 @@ imex_status launch_flux_update(imex_ctx* ctx, int form) {
   if (form == 1)
     IMEX_LAUNCH_BC_ARITH(ctx->P, k_flux_pres, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else if (form == 2 && open)  // the energy formula's flux keeps the reference's operation order
-    k_flux_mag<2, true, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    launch<k_flux_mag<2, true, false>>(ctx, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else if (form == 2)
-    k_flux_mag<2, false, false><<<nb, FNT, 0, ctx->stream>>>(ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
+    launch<k_flux_mag<2, false, false>>(ctx, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   else
     IMEX_LAUNCH_BC_ARITH(ctx->P, k_flux_conv, nb, FNT, 0, ctx->stream, ctx->P, ctx->sc, ctx->w, ctx->Qs, ctx->cons);
   LAUNCH_CHECK(ctx, "flux update");
@@ -1038,26 +1103,26 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
   cudaStream_t s = ctx->stream;
   prof_begin(ctx);
   if (variant == 0 || variant == 1) {
-    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp, ctx->bl);
+    launch<k_ct_corner>(ctx, nb, kThreads, 0, s, P, ctx->Fx, -1.0, ctx->Fy, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   } else if (variant == 2) {
     if (P.reconstate == IMEX_PrimState) IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_prim, nb, kThreads, 0, s, P, ctx->cons, ctx->w, 8);
     else IMEX_LAUNCH_BC_ARITH(P, k_reconstruct_var, (dim3(nb, 8)), kThreads, 0, s, P, ctx->cons, ctx->w);
     LAUNCH_CHECK(ctx, "k_reconstruct(u_con)");
-    k_ct_legacy_faces<<<nb, kThreads, 0, s>>>(P, ctx->w, ctx->chit, ctx->Et);
+    launch<k_ct_legacy_faces>(ctx, nb, kThreads, 0, s, P, ctx->w, ctx->chit, ctx->Et);
     LAUNCH_CHECK(ctx, "k_ct_legacy_faces");
-    k_ct_corner<<<nb, kThreads, 0, s>>>(P, ctx->chit, 1.0, ctx->Et, 1.0, ctx->cons, ctx->Epp, ctx->bl);
+    launch<k_ct_corner>(ctx, nb, kThreads, 0, s, P, ctx->chit, 1.0, ctx->Et, 1.0, ctx->cons, ctx->Epp, ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_corner");
   }
   if (variant == 0 || variant == 2) {
-    k_ct_faces<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->bxQs, ctx->byQs, ctx->bx, ctx->by, ctx->cons,
+    launch<k_ct_faces>(ctx, nb, kThreads, 0, s, P, ctx->sc, ctx->Epp, ctx->bxQs, ctx->byQs, ctx->bx, ctx->by, ctx->cons,
                                        ctx->bl);
     LAUNCH_CHECK(ctx, "k_ct_faces");
   } else {
-    if (variant == 1) k_ct_unstag_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A, ctx->bl);
-    else k_ct_unstag_legacy_A<<<nb, kThreads, 0, s>>>(P, ctx->sc, ctx->cons, ctx->A_s, ctx->A);
+    if (variant == 1) launch<k_ct_unstag_A>(ctx, nb, kThreads, 0, s, P, ctx->sc, ctx->Epp, ctx->A_s, ctx->A, ctx->bl);
+    else launch<k_ct_unstag_legacy_A>(ctx, nb, kThreads, 0, s, P, ctx->sc, ctx->cons, ctx->A_s, ctx->A);
     LAUNCH_CHECK(ctx, "k_ct_unstag_A");
-    k_curl_Az<<<nb, kThreads, 0, s>>>(P, ctx->A, ctx->cons);
+    launch<k_curl_Az>(ctx, nb, kThreads, 0, s, P, ctx->A, ctx->cons);
     LAUNCH_CHECK(ctx, "k_curl_Az");
   }
   // corner EMF 8 + faces/cell B 7 (consistent); legacy variants add the reconstruction of u_con
@@ -1067,12 +1132,12 @@ imex_status launch_ct(imex_ctx* ctx, int variant) {
 
 imex_status launch_stage_derivative(imex_ctx* ctx, int rks) {
   prof_begin(ctx);
-  k_stage_derivative<<<blocks_for(ctx->P.N), kThreads, 0, ctx->stream>>>(
+  launch<k_stage_derivative>(ctx, blocks_for(ctx->P.N), kThreads, 0, ctx->stream, 
       ctx->P, rks, ctx->sc, ctx->cons, ctx->Qs, ctx->A, ctx->A_s, ctx->bx, ctx->bxQs, ctx->by, ctx->byQs, ctx->Bsave,
       ctx->Hs, ctx->HsA, ctx->HsB, ctx->prim);
   LAUNCH_CHECK(ctx, "k_stage_derivative");
   if (ctx->P.xclamp || ctx->P.yclamp) {
-    k_bline_derivative<<<blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream>>>(
+    launch<k_bline_derivative>(ctx, blocks_for(ctx->nx > ctx->ny ? ctx->nx : ctx->ny), kThreads, 0, ctx->stream, 
         ctx->P, rks, ctx->sc, ctx->bl);
     LAUNCH_CHECK(ctx, "k_bline_derivative");
   }

@@ -391,7 +391,7 @@ imex_status imex_adjoint_vjp(imex_ctx* ctx, const imex_adjoint_opts* opts, const
 
 typedef struct imex_batch imex_batch;
 typedef struct imex_batch_tuning {
-  int streams;          /* streams of the explicit sub-steps */
+  int streams;          /* streams of the explicit sub-steps (0: one batched launch per sub-step) */
   int gmres_restart;    /* Krylov vectors per cycle of every member */
   double ms_per_step;   /* device time of one ensemble step at that choice */
   int mixed_solves;     /* IMEX_MIXED_* flags of every member (mixed precision only) */
@@ -399,11 +399,18 @@ typedef struct imex_batch_tuning {
 imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx, const int* ny, imex_batch** out);
 imex_status imex_batch_destroy(imex_batch* b);
 imex_status imex_batch_member(imex_batch* b, int m, imex_ctx** ctx);
-/* streams of the explicit sub-steps (default 8) and graph capture (default on) */
+/* how the explicit sub-steps run, and graph capture (default on).  streams = 0 (the
+ * default): each explicit sub-step is one launch for all members, whose grids are laid end
+ * to end (the step is planned once by recording every member's launches); streams > 0:
+ * every member launches its own kernels, the members spread over that many streams. */
 imex_status imex_batch_configure(imex_batch* b, int streams, int use_graph);
 /* advance every member `steps` steps; *device_ms (optional) = device time of those steps */
 imex_status imex_batch_step(imex_batch* b, int steps, double* device_ms);
-/* time `trial_steps` ensemble steps for each candidate (streams 4 / 8 / 16, restart
+/* launches of one ensemble step in the batched mode: the explicit sub-steps, and the
+ * batched solves (a barrier reset and a cooperative launch per chunk); -1 in the streams
+ * mode.  The second pointer may be null. */
+imex_status imex_batch_explicit_launches(imex_batch* b, int* launches_per_step, int* solve_launches_per_step);
+/* time `trial_steps` ensemble steps for each candidate (streams 0 / 4 / 8 / 16, restart
  * length 15 or the configured one, and in mixed precision the configured mixed_solves or
  * the same with the magnetic systems' FP32 form toggled), restore every member's state
  * after each trial, and keep the fastest choice */
