@@ -520,6 +520,154 @@ struct MagneticBOpT : MagneticBCoef {
 };
 using MagneticBOp = MagneticBOpT<double>;
 
+// Magnetic_Subsystem_AX in the fast arithmetic (imex_config.arith = fast).  The exact form
+// above evaluates each corner average of Qe B and of x from the cell's own side, four
+// corners per cell, so every corner is formed four times and its 28 corner quantities stay
+// live through the three components (226-240 registers: one CTA per SM).  Here a tile
+// pre-pass forms, once per corner, the corner averages of Qe B and of x (in the reference's
+// order for the corner's lower-left cell, whose upper-right corner it is) and their
+// energy-like sum W, and once per staged cell the sum QX = (q5 x5 + q6 x6 + q7 x7) / 2; the
+// matvec reads them from shared memory.  The corners seen from the other three cells round
+// their four-term sums in another order, a few ulp from the reference's operator; the
+// solves converge to the same tolerance.  It fits two CTAs per SM.
+template <class T>
+struct MagneticBFastOpT : MagneticBOpT<T> {
+  using MagneticBCoef::P;
+  using MagneticBCoef::h;
+  using MagneticBCoef::cx;
+  using MagneticBCoef::cy;
+  // pre-pass planes: corners (indexed by their lower-left staged cell) Bxn, Byn, Bzn, Bx, By,
+  // Bz, W; and QX at every staged cell
+  static constexpr int PT = 8;
+  static constexpr int MIN_BLOCKS = 2;
+  template <class U>
+  __device__ __forceinline__ MagneticBFastOpT<U> as() const {
+    MagneticBFastOpT<U> o;
+    static_cast<MagneticBCoef&>(o) = *this;
+    return o;
+  }
+  template <class TB>
+  __device__ __forceinline__ void prepass(TB& tb, int, int) const {
+    constexpr int SX = TB::SX, SY = TB::SY, SN = TB::SN, PN = TB::PN;
+    static_assert(TB::PN == TB::SN, "halo-1 tile: the pre-pass region is the staged region");
+    const T hf = T(0.5), qf = T(0.25);
+    const T* q5 = tb.c;
+    const T* q6 = tb.c + SN;
+    const T* q7 = tb.c + 2 * SN;
+    const T* x5 = tb.s;
+    const T* x6 = tb.s + SN;
+    const T* x7 = tb.s + 2 * SN;
+    for (int q = threadIdx.x; q < SN; q += NT) {
+      tb.p[7 * PN + q] = hf * (q5[q] * x5[q] + q6[q] * x6[q] + q7[q] * x7[q]);
+      const int sx = q % SX, sy = q / SX;
+      if (sx >= SX - 1 || sy >= SY - 1) continue;  // no upper-right neighbours: not a corner
+      const int e = q + 1, n = q + SX, ne = q + SX + 1;
+      const T bxn = qf * (q5[q] + q5[e] + q5[n] + q5[ne]);
+      const T byn = qf * (q6[q] + q6[e] + q6[n] + q6[ne]);
+      const T bzn = qf * (q7[q] + q7[e] + q7[n] + q7[ne]);
+      const T bx = qf * (x5[q] + x5[e] + x5[n] + x5[ne]);
+      const T by = qf * (x6[q] + x6[e] + x6[n] + x6[ne]);
+      const T bz = qf * (x7[q] + x7[e] + x7[n] + x7[ne]);
+      tb.p[0 * PN + q] = bxn;
+      tb.p[1 * PN + q] = byn;
+      tb.p[2 * PN + q] = bzn;
+      tb.p[3 * PN + q] = bx;
+      tb.p[4 * PN + q] = by;
+      tb.p[5 * PN + q] = bz;
+      tb.p[6 * PN + q] = hf * (bxn * bx + byn * by + bzn * bz);
+    }
+  }
+  // implicit_operators.cpp:214-353 with the corner quantities of the pre-pass: the corners
+  // (i +- 1/2, j +- 1/2) of cell o are the pre-pass entries of o (pp), S (pm), W (mp), SW (mm)
+  template <class TB>
+  __device__ void matvec(const TB& tb, int lx, int ly, long long c, T* out) const {
+    constexpr int SX = TB::SX, SN = TB::SN, PN = TB::PN;
+    const T dx = (T)P.dx, dy = (T)P.dy, hT = (T)h, cxT = (T)cx, cyT = (T)cy;
+    const T hf = T(0.5), one = T(1);
+    const int o = (ly + 1) * SX + lx + 1;
+    const int E = o + 1, W = o - 1, No = o + SX, S = o - SX, SW = S - 1;
+    const T* q5 = tb.c;
+    const T* q6 = tb.c + SN;
+    const T* q7 = tb.c + 2 * SN;
+    const T* rr = tb.c + 3 * SN;
+    const T* x5 = tb.s;
+    const T* x6 = tb.s + SN;
+    const T* x7 = tb.s + 2 * SN;
+    const T* Cxn = tb.p;
+    const T* Cyn = tb.p + PN;
+    const T* Czn = tb.p + 2 * PN;
+    const T* Cx = tb.p + 3 * PN;
+    const T* Cy = tb.p + 4 * PN;
+    const T* Cz = tb.p + 5 * PN;
+    const T* Cw = tb.p + 6 * PN;
+    const T* QX = tb.p + 7 * PN;
+    const T r0 = rr[o];
+    const T ir_p0 = one / (hf * (r0 + rr[E])), ir_m0 = one / (hf * (r0 + rr[W]));
+    const T ir_0p = one / (hf * (r0 + rr[No])), ir_0m = one / (hf * (r0 + rr[S]));
+    const T idx = one / dx, idy = one / dy;
+#define FA(a, t) (hf * (a[o] + a[t]))
+    {  // x component (implicit_operators.cpp:266-275)
+      const T Bx_1 = FA(q5, No) * ir_0p *
+                     (idx * (Cxn[o] * Cy[o] - Cxn[W] * Cy[W]) -
+                      idy * ((QX[No] - q6[No] * x6[No]) - (QX[o] - q6[o] * x6[o])));
+      const T Bx_2 = FA(q6, No) * ir_0p *
+                     (idx * ((Cw[o] - Cxn[o] * Cx[o]) - (Cw[W] - Cxn[W] * Cx[W])) -
+                      idy * (q6[No] * x5[No] - q6[o] * x5[o]));
+      const T Bx_3 = FA(q5, S) * ir_0m *
+                     (idx * (Cxn[S] * Cy[S] - Cxn[SW] * Cy[SW]) -
+                      idy * ((QX[o] - q6[o] * x6[o]) - (QX[S] - q6[S] * x6[S])));
+      const T Bx_4 = FA(q6, S) * ir_0m *
+                     (idx * ((Cw[S] - Cxn[S] * Cx[S]) - (Cw[SW] - Cxn[SW] * Cx[SW])) -
+                      idy * (q6[o] * x5[o] - q6[S] * x5[S]));
+      const T ax5 = x5[o] + (hT * hT / dy) * ((Bx_1 + Bx_2) - (Bx_3 + Bx_4));
+      out[0] = ax5 - hT * this->visc(x5, c, o, SX, cxT, cyT);
+    }
+    {  // y component (implicit_operators.cpp:277-285)
+      const T By_1 = FA(q6, E) * ir_p0 *
+                     (-idx * ((QX[E] - q5[E] * x5[E]) - (QX[o] - q5[o] * x5[o])) +
+                      idy * (Cxn[o] * Cy[o] - Cxn[S] * Cy[S]));
+      const T By_2 = FA(q5, E) * ir_p0 *
+                     (-idx * (q5[E] * x6[E] - q5[o] * x6[o]) +
+                      idy * ((Cw[o] - Cyn[o] * Cy[o]) - (Cw[S] - Cyn[S] * Cy[S])));
+      const T By_3 = FA(q6, W) * ir_m0 *
+                     (-idx * ((QX[o] - q5[o] * x5[o]) - (QX[W] - q5[W] * x5[W])) +
+                      idy * (Cxn[W] * Cy[W] - Cxn[SW] * Cy[SW]));
+      const T By_4 = FA(q5, W) * ir_m0 *
+                     (-idx * (q5[o] * x6[o] - q5[W] * x6[W]) +
+                      idy * ((Cw[W] - Cyn[W] * Cy[W]) - (Cw[SW] - Cyn[SW] * Cy[SW])));
+      const T ax6 = x6[o] + (hT * hT / dx) * ((By_1 + By_2) - (By_3 + By_4));
+      out[1] = ax6 - hT * this->visc(x6, c, o, SX, cxT, cyT);
+    }
+    {  // z component (implicit_operators.cpp:288-306)
+      const T Bz_1 = FA(q7, E) * ir_p0 *
+                     (-idx * ((QX[E] - q5[E] * x5[E]) - (QX[o] - q5[o] * x5[o])) +
+                      idy * (Cyn[o] * Cx[o] - Cyn[S] * Cx[S]));
+      const T Bz_2 = FA(q5, E) * ir_p0 *
+                     (-idx * (q5[E] * x7[E] - q5[o] * x7[o]) - idy * (Cyn[o] * Cz[o] - Cyn[S] * Cz[S]));
+      const T Bz_3 = FA(q7, W) * ir_m0 *
+                     (-idx * ((QX[o] - q5[o] * x5[o]) - (QX[W] - q5[W] * x5[W])) +
+                      idy * (Cyn[W] * Cx[W] - Cyn[SW] * Cx[SW]));
+      const T Bz_4 = FA(q5, W) * ir_m0 *
+                     (-idx * (q5[o] * x7[o] - q5[W] * x7[W]) - idy * (Cyn[W] * Cz[W] - Cyn[SW] * Cz[SW]));
+      const T Bz_5 = FA(q7, No) * ir_0p *
+                     (idx * (Cxn[o] * Cy[o] - Cxn[W] * Cy[W]) -
+                      idy * ((QX[No] - q6[No] * x6[No]) - (QX[o] - q6[o] * x6[o])));
+      const T Bz_6 = FA(q6, No) * ir_0p *
+                     (-idx * (Cxn[o] * Cz[o] - Cxn[W] * Cz[W]) - idy * (q6[No] * x7[No] - q6[o] * x7[o]));
+      const T Bz_7 = FA(q7, S) * ir_0m *
+                     (idx * (Cxn[S] * Cy[S] - Cxn[SW] * Cy[SW]) -
+                      idy * ((QX[o] - q6[o] * x6[o]) - (QX[S] - q6[S] * x6[S])));
+      const T Bz_8 = FA(q6, S) * ir_0m *
+                     (-idx * (Cxn[S] * Cz[S] - Cxn[SW] * Cz[SW]) - idy * (q6[o] * x7[o] - q6[S] * x7[S]));
+      const T ax7 =
+          x7[o] + hT * hT / dx * ((Bz_1 + Bz_2) - (Bz_3 + Bz_4)) + hT * hT / dy * ((Bz_5 + Bz_6) - (Bz_7 + Bz_8));
+      out[2] = ax7 - hT * this->visc(x7, c, o, SX, cxT, cyT);
+    }
+#undef FA
+  }
+};
+using MagneticBFastOp = MagneticBFastOpT<double>;
+
 // Magnetic_Subsystem_potential_AX (implicit_operators.cpp:355-503), GLF or local viscosity.
 // The reference evaluates B = curl A and the stress tensor T^B at the four
 // neighbours of each cell; those values are exactly curl A and T^B of the
@@ -2260,6 +2408,11 @@ MagneticBOp make_magB_op(imex_ctx* ctx) {
   op.lv = ctx->lvm;
   return op;
 }
+MagneticBFastOp make_magB_fast_op(imex_ctx* ctx) {
+  MagneticBFastOp op{};
+  static_cast<MagneticBCoef&>(op) = static_cast<const MagneticBCoef&>(make_magB_op(ctx));
+  return op;
+}
 template <bool kOpen = false>
 MagneticAOpT<double, kOpen> make_magA_op(imex_ctx* ctx) {
   MagneticAOpT<double, kOpen> op{};
@@ -2367,6 +2520,8 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
     o.jac = op == IMEX_OP_PRESSURE_J;
     return gmres_run(ctx, o, F_GMRES_PRES, x, b, IMEX_MIXED_PRESSURE);
   } else if (op == IMEX_OP_MAGNETIC_B) {
+    if (ctx->P.fast)
+      return gmres_run(ctx, make_magB_fast_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
     return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     if (ctx->P.xclamp || ctx->P.yclamp)
@@ -2659,6 +2814,9 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
                                             sys);
     else if (P.magfield == IMEX_PotentialA)
       s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<false>, sys);
+    else if (P.fast)
+      s = add_gmres_chunks<MagneticBFastOp>(plan, members, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B,
+                                            F_GMRES_MAG_B, make_magB_fast_op, sys);
     else
       s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B, F_GMRES_MAG_B,
                                         make_magB_op, sys);
@@ -2913,7 +3071,8 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
     o.jac = op == IMEX_OP_PRESSURE_J;
     launch_apply(ctx, o, nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_B) {
-    launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
+    if (ctx->P.fast) launch_apply(ctx, make_magB_fast_op(ctx), nb, T, x, Ax);
+    else launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     if (ctx->P.xclamp || ctx->P.yclamp) launch_apply(ctx, make_magA_op<true>(ctx), nb, T, x, Ax);
     else launch_apply(ctx, make_magA_op(ctx), nb, T, x, Ax);
