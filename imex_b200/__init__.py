@@ -94,7 +94,7 @@ class SolveStats(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("streams", C.c_int), ("gmres_restart", C.c_int), ("ms_per_step", C.c_double),
-                ("mixed_solves", C.c_int)]
+                ("mixed_solves", C.c_int), ("solve_tile_x", C.c_int), ("solve_tile_y", C.c_int)]
 
 
 class Diagnostics(C.Structure):
@@ -179,6 +179,7 @@ _SIGS = {
     "imex_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "imex_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(BatchTuning)]),
     "imex_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "imex_batch_set_solve_tile": (C.c_int, [C.c_void_p, C.c_int]),
     "imex_batch_explicit_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "imex_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "imex_pressure_nested_newton": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(SolveStats)]),
@@ -646,7 +647,12 @@ class Batch:
         t = BatchTuning()
         self._check(self.lib.imex_batch_autotune(self.b, trial_steps, C.byref(t)))
         return dict(streams=t.streams, gmres_restart=t.gmres_restart, ms_per_step=t.ms_per_step,
-                    mixed_solves=t.mixed_solves)
+                    mixed_solves=t.mixed_solves, solve_tile=(t.solve_tile_x, t.solve_tile_y))
+
+    def set_solve_tile(self, tile: int) -> None:
+        """Tile shape of the batched B-form solve (fast arithmetic): 0 = 32x16, 1 = 64x8,
+        2 = 32x8 cells."""
+        self._check(self.lib.imex_batch_set_solve_tile(self.b, tile))
 
     def info(self) -> dict:
         a, g, n = C.c_int(), C.c_int(), C.c_int()

@@ -40,6 +40,7 @@ struct imex_batch {
   std::vector<imex::PlanItem> plan;
   imex::PlanArena arena;
   int nstreams = 0;  // 0: batched explicit sub-steps; > 0: streams of the per-member launches
+  int solve_tile = 0;  // tile shape of the batched B-form solve (kBatchTileX / kBatchTileY)
   bool use_graph = true;
   bool members_on_batch = false;  // the members' streams are the batch's (pool or origin)
   bool prepared = false;
@@ -321,7 +322,7 @@ imex_status prepare(imex_batch* b) {
     b->members[m]->prof_on = false;
   }
   b->members_on_batch = true;
-  imex_status s = batch_solve_build(b->members, BATCH_MAGNETIC, &b->mag);
+  imex_status s = batch_solve_build(b->members, BATCH_MAGNETIC, &b->mag, b->solve_tile);
   if (s == IMEX_OK) s = batch_solve_build(b->members, BATCH_PRESSURE, &b->pres);
   if (s != IMEX_OK) return berr(b, s, "batched solve set-up: " + b->members[0]->last_error);
   if (b->nstreams == 0 && (s = plan_step(b)) != IMEX_OK) return s;
@@ -534,59 +535,72 @@ imex_status imex_batch_explicit_launches(imex_batch* b, int* launches_per_step, 
   return IMEX_OK;
 }
 
+imex_status imex_batch_set_solve_tile(imex_batch* b, int tile) {
+  if (!b || tile < 0 || tile >= kBatchTiles) return IMEX_ERR_INVALID;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  release_plans(b, true);
+  b->solve_tile = tile;
+  return IMEX_OK;
+}
+
 imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out) {
   if (!b || trial_steps < 1) return IMEX_ERR_INVALID;
-  const int restart0 = b->members[0]->cfg.gmres_restart;
-  const int stream_cands[] = {0, 4, 8, 16};
-  const int restart_cands[] = {restart0 < 15 ? restart0 : 15, restart0};
+  imex_ctx* c0 = b->members[0];
+  const int restart0 = c0->cfg.gmres_restart;
   // in mixed precision, whether the magnetic systems take the FP32 form pays only where
   // FP64 GMRES needs many Krylov steps: time both
-  const int solves0 = b->members[0]->cfg.mixed_solves;
+  const int solves0 = c0->cfg.mixed_solves;
   const int mag = IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B;
-  std::vector<int> solve_cands{solves0};
-  if (b->members[0]->cfg.precision == IMEX_PRECISION_MIXED)
-    solve_cands.push_back((solves0 & mag) ? (solves0 & ~mag) : (solves0 | IMEX_MIXED_MAGNETIC_B));
+  // the tile shape matters for the B-form solve of the fast arithmetic, the one with choices
+  const bool tiles = c0->P.magfield != IMEX_PotentialA && c0->P.fast;
+  struct Choice {
+    int streams, restart, solves, tile;
+  };
+  Choice best{b->nstreams, restart0, solves0, b->solve_tile};
+  double best_ms = 1e300;
   Snapshot snap;
   imex_status s = take_snapshot(b, snap, false);
-  double best = 1e300;
-  int best_streams = b->nstreams, best_restart = restart0, best_solves = solves0;
-  for (int sc : stream_cands) {
-    for (int rc : restart_cands) {
-      for (int mc : solve_cands) {
-        for (imex_ctx* c : b->members) {
-          c->cfg.gmres_restart = rc;
-          c->cfg.mixed_solves = mc;
-        }
-        if (s == IMEX_OK) s = imex_batch_configure(b, sc, b->use_graph ? 1 : 0);
-        double ms = 0.0;
-        if (s == IMEX_OK) s = imex_batch_step(b, 1, nullptr);  // warm-up (and graph capture)
-        if (s == IMEX_OK) s = imex_batch_step(b, trial_steps, &ms);
-        if (s == IMEX_OK) s = take_snapshot(b, snap, true);
-        if (s != IMEX_OK) break;
-        if (ms < best) {
-          best = ms;
-          best_streams = sc;
-          best_restart = rc;
-          best_solves = mc;
-        }
-      }
-      if (s != IMEX_OK) break;
+  auto trial = [&](const Choice& c) {
+    for (imex_ctx* m : b->members) {
+      m->cfg.gmres_restart = c.restart;
+      m->cfg.mixed_solves = c.solves;
     }
-    if (s != IMEX_OK) break;
-  }
+    b->solve_tile = c.tile;
+    if (s == IMEX_OK) s = imex_batch_configure(b, c.streams, b->use_graph ? 1 : 0);
+    double ms = 0.0;
+    if (s == IMEX_OK) s = imex_batch_step(b, 1, nullptr);  // warm-up (and graph capture)
+    if (s == IMEX_OK) s = imex_batch_step(b, trial_steps, &ms);
+    if (s == IMEX_OK) s = take_snapshot(b, snap, true);
+    if (s == IMEX_OK && ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  };
+  // one choice at a time, each from the best so far: explicit mode, solve tile, restart
+  // length, FP32 magnetic solves
+  for (int sc : {0, 4, 8, 16}) trial(Choice{sc, restart0, solves0, 0});
+  if (tiles)
+    for (int t = 1; t < kBatchTiles; ++t) trial(Choice{best.streams, best.restart, best.solves, t});
+  if (restart0 > 15) trial(Choice{best.streams, 15, best.solves, best.tile});
+  if (c0->cfg.precision == IMEX_PRECISION_MIXED)
+    trial(Choice{best.streams, best.restart, (best.solves & mag) ? (best.solves & ~mag) : (best.solves | IMEX_MIXED_MAGNETIC_B),
+                 best.tile});
   for (double* p : snap.planes) cudaFree(p);
-  for (imex_ctx* c : b->members) {
-    c->cfg.gmres_restart = best_restart;
-    c->cfg.mixed_solves = best_solves;
+  for (imex_ctx* m : b->members) {
+    m->cfg.gmres_restart = best.restart;
+    m->cfg.mixed_solves = best.solves;
   }
-  imex_status s2 = imex_batch_configure(b, best_streams, b->use_graph ? 1 : 0);
+  b->solve_tile = best.tile;
+  imex_status s2 = imex_batch_configure(b, best.streams, b->use_graph ? 1 : 0);
   if (s != IMEX_OK) return s;
   if (s2 != IMEX_OK) return s2;
   if (out) {
-    out->streams = best_streams;
-    out->gmres_restart = best_restart;
-    out->ms_per_step = best / trial_steps;
-    out->mixed_solves = best_solves;
+    out->streams = best.streams;
+    out->gmres_restart = best.restart;
+    out->ms_per_step = best_ms / trial_steps;
+    out->mixed_solves = best.solves;
+    out->solve_tile_x = kBatchTileX[best.tile];
+    out->solve_tile_y = kBatchTileY[best.tile];
   }
   return IMEX_OK;
 }

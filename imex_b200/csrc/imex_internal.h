@@ -247,7 +247,12 @@ struct BatchSolvePlan {
   std::vector<BatchChunk> chunks;
   std::vector<void*> dev;  // device arrays of the plan (jobs, CTA map, barrier pointers)
 };
-imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out);
+// tile: the shape of the B-form magnetic solve's tiles in the fast arithmetic (kBatchTiles)
+imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out, int tile = 0);
+// the solve tile shapes an ensemble can choose: cells in x and y of tile 0, 1, 2 (64 x 16
+// tiles were measured too: 1.2 KB of spills at 128 registers, 1.8x slower)
+constexpr int kBatchTiles = 3;
+constexpr int kBatchTileX[kBatchTiles] = {32, 64, 32}, kBatchTileY[kBatchTiles] = {16, 8, 8};
 imex_status batch_solve_run(BatchSolvePlan* plan, cudaStream_t stream, imex_ctx* err_ctx);
 void batch_solve_free(BatchSolvePlan* plan);
 

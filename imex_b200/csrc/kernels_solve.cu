@@ -97,15 +97,16 @@ struct Tiling {
   long long N;
   int xclamp, yclamp;  // transmissive directions: the halo clamps instead of wrapping
 };
-__host__ __device__ inline Tiling make_tiling(int nx, int ny, int xclamp = 0, int yclamp = 0) {
+// tiles of tx x ty cells (the operator's tile shape, TileShape below)
+__host__ __device__ inline Tiling make_tiling(int nx, int ny, int xclamp = 0, int yclamp = 0, int tx = TX, int ty = TY) {
   Tiling t;
   t.nx = nx;
   t.ny = ny;
   t.xclamp = xclamp;
   t.yclamp = yclamp;
   t.N = (long long)nx * ny;
-  t.tiles_x = (nx + TX - 1) / TX;
-  t.ntiles = t.tiles_x * ((ny + TY - 1) / TY);
+  t.tiles_x = (nx + tx - 1) / tx;
+  t.ntiles = t.tiles_x * ((ny + ty - 1) / ty);
   return t;
 }
 
@@ -194,6 +195,30 @@ __device__ inline void grid_reduce(const double* partial, int nblk, int kn, doub
 constexpr int RY = NT / TX;     // rows covered by one pass of the CTA
 constexpr int CPT = TY / RY;    // interior cells per thread
 
+// The tile shape of an operator: TX x TY, unless the operator names its own (kTileX x
+// kTileY, a shape an ensemble's autotuner may choose).  RYo rows per CTA pass, CPTo cells
+// per thread.
+template <class Op, class = void>
+struct TileShape {
+  static constexpr int tx = TX, ty = TY;
+};
+template <class Op>
+struct TileShape<Op, std::void_t<decltype(Op::kTileX)>> {
+  static constexpr int tx = Op::kTileX, ty = Op::kTileY;
+};
+template <class Op>
+constexpr int TXo = TileShape<Op>::tx;
+template <class Op>
+constexpr int TYo = TileShape<Op>::ty;
+template <class Op>
+constexpr int RYo = NT / TXo<Op>;
+template <class Op>
+constexpr int CPTo = TYo<Op> / RYo<Op>;
+template <class Op>
+inline Tiling make_tiling_for(const imex_ctx* ctx) {
+  return make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp, TXo<Op>, TYo<Op>);
+}
+
 __device__ __forceinline__ int wrapc(int i, int n) {
   if (i < 0) {
     i += n;
@@ -209,8 +234,8 @@ template <class Op>
 struct TileBuf {
   using T = typename Op::value_type;
   static constexpr int H = Op::HALO;
-  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SN = SX * SY;
-  static constexpr int PX = TX + 2, PY = TY + 2, PN = PX * PY;  // halo-1 region of the pre-pass
+  static constexpr int SX = TXo<Op> + 2 * H, SY = TYo<Op> + 2 * H, SN = SX * SY;
+  static constexpr int PX = TXo<Op> + 2, PY = TYo<Op> + 2, PN = PX * PY;  // halo-1 region of the pre-pass
   T s[Op::M * SN];           // vector tile
   T c[Op::QT * SN];          // frozen coefficients on the same cells
   T p[Op::PT * PN + 1];      // pre-pass quantities (halo-1 region)
@@ -530,8 +555,9 @@ using MagneticBOp = MagneticBOpT<double>;
 // matvec reads them from shared memory.  The corners seen from the other three cells round
 // their four-term sums in another order, a few ulp from the reference's operator; the
 // solves converge to the same tolerance.  It fits two CTAs per SM.
-template <class T>
+template <class T, int kTX = TX, int kTY = TY>
 struct MagneticBFastOpT : MagneticBOpT<T> {
+  static constexpr int kTileX = kTX, kTileY = kTY;
   using MagneticBCoef::P;
   using MagneticBCoef::h;
   using MagneticBCoef::cx;
@@ -541,8 +567,8 @@ struct MagneticBFastOpT : MagneticBOpT<T> {
   static constexpr int PT = 8;
   static constexpr int MIN_BLOCKS = 2;
   template <class U>
-  __device__ __forceinline__ MagneticBFastOpT<U> as() const {
-    MagneticBFastOpT<U> o;
+  __device__ __forceinline__ MagneticBFastOpT<U, kTX, kTY> as() const {
+    MagneticBFastOpT<U, kTX, kTY> o;
     static_cast<MagneticBCoef&>(o) = *this;
     return o;
   }
@@ -919,10 +945,11 @@ struct Cell {
   long long c;
   bool in;
 };
+template <class Op>
 __device__ __forceinline__ Cell tile_cell(const Tiling& T, int x0, int y0, int r) {
   Cell k;
-  k.lx = threadIdx.x % TX;
-  k.ly = threadIdx.x / TX + r * RY;
+  k.lx = threadIdx.x % TXo<Op>;
+  k.ly = threadIdx.x / TXo<Op> + r * RYo<Op>;
   k.gi = x0 + k.lx;
   k.gj = y0 + k.ly;
   k.in = k.gi < T.nx && k.gj < T.ny;
@@ -972,7 +999,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       // ---- r0 = M^-1 b -> V0 and Av0 = M^-1 A V0 in one pass; |r0|^2 and r0.Av0
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
-        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        const int x0 = (t % T.tiles_x) * TXo<Op>, y0 = (t / T.tiles_x) * TYo<Op>;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -983,8 +1010,8 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         });
         double rr = 0.0, va = 0.0;
 #pragma unroll
-        for (int r = 0; r < CPT; ++r) {
-          const Cell k = tile_cell(T, x0, y0, r);
+        for (int r = 0; r < CPTo<Op>; ++r) {
+          const Cell k = tile_cell<Op>(T, x0, y0, r);
           if (!k.in) continue;
           VT aw[M];
           op.matvec(tb, k.lx, k.ly, k.c, aw);
@@ -1033,7 +1060,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       // ---- residual r0 = M^-1 (b - A x) -> V0, |r0|^2
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
-        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        const int x0 = (t % T.tiles_x) * TXo<Op>, y0 = (t / T.tiles_x) * TYo<Op>;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -1042,8 +1069,8 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         });
         double rr = 0.0;
 #pragma unroll
-        for (int r = 0; r < CPT; ++r) {
-          const Cell k = tile_cell(T, x0, y0, r);
+        for (int r = 0; r < CPTo<Op>; ++r) {
+          const Cell k = tile_cell<Op>(T, x0, y0, r);
           if (!k.in) continue;
           VT ax[M];
           op.matvec(tb, k.lx, k.ly, k.c, ax);
@@ -1082,7 +1109,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       // ---- Av0 = M^-1 A V0 (unnormalised), H[0][0]
       wacc_clear(S.acc);
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
-        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        const int x0 = (t % T.tiles_x) * TXo<Op>, y0 = (t / T.tiles_x) * TYo<Op>;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
 #pragma unroll
           for (int r = 0; r < FQ; ++r)
@@ -1091,8 +1118,8 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         });
         double va = 0.0;
 #pragma unroll
-        for (int r = 0; r < CPT; ++r) {
-          const Cell k = tile_cell(T, x0, y0, r);
+        for (int r = 0; r < CPTo<Op>; ++r) {
+          const Cell k = tile_cell<Op>(T, x0, y0, r);
           if (!k.in) continue;
           VT aw[M];
           op.matvec(tb, k.lx, k.ly, k.c, aw);
@@ -1126,7 +1153,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
       wacc_clear(S.acc);
       const double sj = S.sigma[j];
       for (int t = grank(g); t < T.ntiles; t += g.nblk) {
-        const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+        const int x0 = (t % T.tiles_x) * TXo<Op>, y0 = (t / T.tiles_x) * TYo<Op>;
         fill_tile(op, tb, T, x0, y0, [&](const long long* c, VT (*v)[M]) {
           const TS* AVj = AVp(j);
           double wv[FQ][M];
@@ -1148,12 +1175,12 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
 #pragma unroll
             for (int m = 0; m < M; ++m) v[r][m] = (VT)wv[r][m];
         });
-        VT aw[CPT][M], wc[CPT][M];
-        long long cc[CPT];
-        bool in[CPT];
+        VT aw[CPTo<Op>][M], wc[CPTo<Op>][M];
+        long long cc[CPTo<Op>];
+        bool in[CPTo<Op>];
 #pragma unroll
-        for (int r = 0; r < CPT; ++r) {
-          const Cell k = tile_cell(T, x0, y0, r);
+        for (int r = 0; r < CPTo<Op>; ++r) {
+          const Cell k = tile_cell<Op>(T, x0, y0, r);
           cc[r] = k.c;
           in[r] = k.in;
           if (k.in) {
@@ -1177,7 +1204,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         for (; i + 7 <= j; i += 8) {
           double d[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-          for (int r = 0; r < CPT; ++r)
+          for (int r = 0; r < CPTo<Op>; ++r)
             if (in[r]) {
 #pragma unroll
               for (int u = 0; u < 8; ++u)
@@ -1190,7 +1217,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         for (; i + 3 <= j; i += 4) {
           double d[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-          for (int r = 0; r < CPT; ++r)
+          for (int r = 0; r < CPTo<Op>; ++r)
             if (in[r]) {
 #pragma unroll
               for (int u = 0; u < 4; ++u)
@@ -1202,7 +1229,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         for (; i <= j; ++i) {
           double d = 0.0;
 #pragma unroll
-          for (int r = 0; r < CPT; ++r)
+          for (int r = 0; r < CPTo<Op>; ++r)
             if (in[r]) {
 #pragma unroll
               for (int m = 0; m < M; ++m) d += ldv(Vp(i) + m * N + cc[r]) * (double)aw[r][m];
@@ -1211,7 +1238,7 @@ __device__ int gmres_device(const Op& op, const GmresWorkT<TS>& g, double* x, co
         }
         double wa = 0.0, ww = 0.0;
 #pragma unroll
-        for (int r = 0; r < CPT; ++r)
+        for (int r = 0; r < CPTo<Op>; ++r)
 #pragma unroll
           for (int m = 0; m < M; ++m) {
             wa += (double)wc[r][m] * (double)aw[r][m];
@@ -1408,7 +1435,7 @@ __device__ __forceinline__ void mixed_solve(Op64 op, GmresWorkT<float> g, double
     // ---- FP64: x += pending update; s = b - A x; |M^-1 s|^2
     wacc_clear(S.acc);
     for (int t = grank(g); t < T.ntiles; t += g.nblk) {
-      const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+      const int x0 = (t % T.tiles_x) * TXo<Op64>, y0 = (t / T.tiles_x) * TYo<Op64>;
       fill_tile(op, sm.tb.d, T, x0, y0, [&](const long long* c, double (*v)[M]) {
 #pragma unroll
         for (int r = 0; r < FQ; ++r)
@@ -1423,8 +1450,8 @@ __device__ __forceinline__ void mixed_solve(Op64 op, GmresWorkT<float> g, double
       });
       double rr = 0.0;
 #pragma unroll
-      for (int r = 0; r < CPT; ++r) {
-        const Cell k = tile_cell(T, x0, y0, r);
+      for (int r = 0; r < CPTo<Op64>; ++r) {
+        const Cell k = tile_cell<Op64>(T, x0, y0, r);
         if (!k.in) continue;
         double ax[M], res[M];
         op.matvec(sm.tb.d, k.lx, k.ly, k.c, ax);
@@ -1637,7 +1664,7 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
     // ---- pf += pending update; residual g = L pf - a pf + V_mod(pf) - b -> na.g = -g; vdiag = V_slope(pf)
     wacc_clear(S.acc);
     for (int t = grank(gw); t < T.ntiles; t += gw.nblk) {
-      const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+      const int x0 = (t % T.tiles_x) * TXo<PressureOp>, y0 = (t / T.tiles_x) * TYo<PressureOp>;
       fill_tile(L, tb, T, x0, y0, [&](const long long* c, double (*v)[1]) {
         if (pending) {
 #pragma unroll
@@ -1649,8 +1676,8 @@ __device__ __forceinline__ void newton_solve(PressureOp op, GmresWorkT<TS> gw, N
       });
       double gg = 0.0;
 #pragma unroll
-      for (int r = 0; r < CPT; ++r) {
-        const Cell k = tile_cell(T, x0, y0, r);
+      for (int r = 0; r < CPTo<PressureOp>; ++r) {
+        const Cell k = tile_cell<PressureOp>(T, x0, y0, r);
         if (!k.in) continue;
         double lp[1];
         L.matvec(tb, k.lx, k.ly, k.c, lp);
@@ -2229,7 +2256,7 @@ __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, 
   extern __shared__ __align__(16) unsigned char dsm[];
   TileBuf<Op>& tb = *reinterpret_cast<TileBuf<Op>*>(dsm);
   for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
-    const int x0 = (t % T.tiles_x) * TX, y0 = (t / T.tiles_x) * TY;
+    const int x0 = (t % T.tiles_x) * TXo<Op>, y0 = (t / T.tiles_x) * TYo<Op>;
     fill_tile(op, tb, T, x0, y0, [&](const long long* c, double (*v)[Op::M]) {
 #pragma unroll
       for (int r = 0; r < FillQ<Op>; ++r)
@@ -2237,8 +2264,8 @@ __global__ void __launch_bounds__(NT) k_apply(Op op, Tiling T, const double* x, 
         for (int m = 0; m < Op::M; ++m) v[r][m] = x[m * T.N + c[r]];
     });
 #pragma unroll
-    for (int r = 0; r < CPT; ++r) {
-      const Cell k = tile_cell(T, x0, y0, r);
+    for (int r = 0; r < CPTo<Op>; ++r) {
+      const Cell k = tile_cell<Op>(T, x0, y0, r);
       if (!k.in) continue;
       double ax[Op::M];
       op.matvec(tb, k.lx, k.ly, k.c, ax);
@@ -2408,8 +2435,9 @@ MagneticBOp make_magB_op(imex_ctx* ctx) {
   op.lv = ctx->lvm;
   return op;
 }
-MagneticBFastOp make_magB_fast_op(imex_ctx* ctx) {
-  MagneticBFastOp op{};
+template <int kTX = TX, int kTY = TY>
+MagneticBFastOpT<double, kTX, kTY> make_magB_fast_op(imex_ctx* ctx) {
+  MagneticBFastOpT<double, kTX, kTY> op{};
   static_cast<MagneticBCoef&>(op) = static_cast<const MagneticBCoef&>(make_magB_op(ctx));
   return op;
 }
@@ -2493,7 +2521,7 @@ imex_status pressure_setup(imex_ctx* ctx) {
 // refinement kernel around FP32 inner cycles.
 template <class Op>
 imex_status gmres_run(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, int kind) {
-  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
+  const Tiling T = make_tiling_for<Op>(ctx);
   if (!mixed(ctx, kind)) {
     auto kern = k_gmres<Op>;
     const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
@@ -2521,7 +2549,7 @@ imex_status gmres_launch(imex_ctx* ctx, int op, double* x, const double* b) {
     return gmres_run(ctx, o, F_GMRES_PRES, x, b, IMEX_MIXED_PRESSURE);
   } else if (op == IMEX_OP_MAGNETIC_B) {
     if (ctx->P.fast)
-      return gmres_run(ctx, make_magB_fast_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
+      return gmres_run(ctx, make_magB_fast_op<>(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
     return gmres_run(ctx, make_magB_op(ctx), F_GMRES_MAG_B, x, b, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     if (ctx->P.xclamp || ctx->P.yclamp)
@@ -2549,7 +2577,7 @@ bool on_device(const void* p) {
 template <class Op>
 imex_status gmres_noalloc_op(imex_ctx* ctx, const Op& o, int fam, double* x, const double* b, unsigned char* base,
                              size_t capacity) {
-  const Tiling T = make_tiling(ctx->nx, ctx->ny, ctx->P.xclamp, ctx->P.yclamp);
+  const Tiling T = make_tiling_for<Op>(ctx);
   auto kern = k_gmres<Op>;
   const int nb = coop_blocks<Op>(ctx, (const void*)kern, T);
   const size_t n = (size_t)Op::M * (size_t)T.N;
@@ -2647,7 +2675,7 @@ imex_status newton_launch(imex_ctx* ctx, double* p, const double* b, int keys = 
 // no chunk holds more than C/2 members, so every chunk carries about the same work and has
 // room to give large members many CTAs.  Within a chunk every member gets at least one CTA
 // and at most one per tile, the rest in proportion to its tiles.
-template <class Job, class K, class Make>
+template <class ShapeOp, class Job, class K, class Make>
 imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members, K kernel, size_t smem,
                        Make make_job) {
   imex_ctx* c0 = members[0];
@@ -2659,7 +2687,7 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
   const int cap = per_sm * c0->num_sms;
   const long long limit = wait_cycles(c0);
   const int nm = (int)members.size();
-  auto tiles = [&](int m) { return make_tiling(members[m]->nx, members[m]->ny).ntiles; };  // work only
+  auto tiles = [&](int m) { return make_tiling(members[m]->nx, members[m]->ny, 0, 0, TXo<ShapeOp>, TYo<ShapeOp>).ntiles; };
   std::vector<int> order(nm);
   for (int m = 0; m < nm; ++m) order[m] = m;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tiles(a) > tiles(b); });
@@ -2689,7 +2717,7 @@ imex_status add_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& membe
     int first = 0;
     for (int k = 0; k < n; ++k) {
       imex_ctx* m = members[grp[k]];
-      jobs.push_back(make_job(m, make_tiling(m->nx, m->ny, m->P.xclamp, m->P.yclamp), first, alloc[k]));
+      jobs.push_back(make_job(m, make_tiling_for<ShapeOp>(m), first, alloc[k]));
       for (int q = 0; q < alloc[k]; ++q) map.push_back(k);
       syncs.push_back(m->sync);
       first += alloc[k];
@@ -2744,7 +2772,7 @@ template <class Op, class MakeOp, class Sys>
 imex_status add_gmres_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members, int kind, int fam,
                              MakeOp make_op, Sys system) {
   if (!mixed(members[0], kind)) {
-    return add_chunks<GmresJob<Op>>(plan, members, k_gmres_jobs<Op>, sizeof(SolveSmem<Op>),
+    return add_chunks<Op, GmresJob<Op>>(plan, members, k_gmres_jobs<Op>, sizeof(SolveSmem<Op>),
                                     [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
                                       GmresJob<Op> j{};
                                       j.op = make_op(m);
@@ -2753,7 +2781,7 @@ imex_status add_gmres_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>&
                                       return j;
                                     });
   }
-  return add_chunks<MixedJob<Op>>(plan, members, k_gmres_mixed_jobs<Op>, sizeof(MixedSmem<Op>),
+  return add_chunks<Op, MixedJob<Op>>(plan, members, k_gmres_mixed_jobs<Op>, sizeof(MixedSmem<Op>),
                                   [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
                                     MixedJob<Op> j{};
                                     j.op = make_op(m);
@@ -2771,7 +2799,7 @@ template <class TS>
 imex_status add_newton_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>& members) {
   // members share the configuration, so one instance serves all of them
   auto kern = members[0]->P.eos_type == IMEX_IDEAL_GAS ? k_nested_newton_jobs<TS, false> : k_nested_newton_jobs<TS, true>;
-  return add_chunks<NewtonJob<TS>>(
+  return add_chunks<PressureOp, NewtonJob<TS>>(
       plan, members, kern, sizeof(NewtonSmem<TS>),
       [&](imex_ctx* m, const Tiling& T, int first, int nblk) {
         NewtonJob<TS> j{};
@@ -2798,7 +2826,7 @@ imex_status add_newton_chunks(BatchSolvePlan* plan, const std::vector<imex_ctx*>
 
 // The batched solve of one kind for every member (all members share the configuration
 // flags that select the solve; each has its own grid, data and restart length).
-imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out) {
+imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, BatchSolvePlan** out, int tile) {
   if (members.empty()) return IMEX_ERR_INVALID;
   BatchSolvePlan* plan = new BatchSolvePlan();
   imex_ctx* c0 = members[0];
@@ -2814,9 +2842,17 @@ imex_status batch_solve_build(const std::vector<imex_ctx*>& members, int kind, B
                                             sys);
     else if (P.magfield == IMEX_PotentialA)
       s = add_gmres_chunks<MagneticAOp>(plan, members, IMEX_MIXED_MAGNETIC, F_GMRES_MAG_A, make_magA_op<false>, sys);
-    else if (P.fast)
-      s = add_gmres_chunks<MagneticBFastOp>(plan, members, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B,
-                                            F_GMRES_MAG_B, make_magB_fast_op, sys);
+    else if (P.fast) {  // the tile shape an ensemble chose (imex_batch_set_solve_tile)
+      constexpr int mk = IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B;
+      if (tile == 1)
+        s = add_gmres_chunks<MagneticBFastOpT<double, 64, 8>>(plan, members, mk, F_GMRES_MAG_B,
+                                                              make_magB_fast_op<64, 8>, sys);
+      else if (tile == 2)
+        s = add_gmres_chunks<MagneticBFastOpT<double, 32, 8>>(plan, members, mk, F_GMRES_MAG_B,
+                                                              make_magB_fast_op<32, 8>, sys);
+      else
+        s = add_gmres_chunks<MagneticBFastOp>(plan, members, mk, F_GMRES_MAG_B, make_magB_fast_op<>, sys);
+    }
     else
       s = add_gmres_chunks<MagneticBOp>(plan, members, IMEX_MIXED_MAGNETIC | IMEX_MIXED_MAGNETIC_B, F_GMRES_MAG_B,
                                         make_magB_op, sys);
@@ -3071,7 +3107,7 @@ imex_status apply_operator(imex_ctx* ctx, int op, const double* x, double* Ax) {
     o.jac = op == IMEX_OP_PRESSURE_J;
     launch_apply(ctx, o, nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_B) {
-    if (ctx->P.fast) launch_apply(ctx, make_magB_fast_op(ctx), nb, T, x, Ax);
+    if (ctx->P.fast) launch_apply(ctx, make_magB_fast_op<>(ctx), nb, T, x, Ax);
     else launch_apply(ctx, make_magB_op(ctx), nb, T, x, Ax);
   } else if (op == IMEX_OP_MAGNETIC_A) {
     if (ctx->P.xclamp || ctx->P.yclamp) launch_apply(ctx, make_magA_op<true>(ctx), nb, T, x, Ax);

@@ -395,6 +395,7 @@ typedef struct imex_batch_tuning {
   int gmres_restart;    /* Krylov vectors per cycle of every member */
   double ms_per_step;   /* device time of one ensemble step at that choice */
   int mixed_solves;     /* IMEX_MIXED_* flags of every member (mixed precision only) */
+  int solve_tile_x, solve_tile_y;  /* cells per tile of the batched B-form magnetic solve */
 } imex_batch_tuning;
 imex_status imex_batch_create(const imex_config* cfg, int members, const int* nx, const int* ny, imex_batch** out);
 imex_status imex_batch_destroy(imex_batch* b);
@@ -410,10 +411,14 @@ imex_status imex_batch_step(imex_batch* b, int steps, double* device_ms);
  * batched solves (a barrier reset and a cooperative launch per chunk); -1 in the streams
  * mode.  The second pointer may be null. */
 imex_status imex_batch_explicit_launches(imex_batch* b, int* launches_per_step, int* solve_launches_per_step);
-/* time `trial_steps` ensemble steps for each candidate (streams 0 / 4 / 8 / 16, restart
- * length 15 or the configured one, and in mixed precision the configured mixed_solves or
- * the same with the magnetic systems' FP32 form toggled), restore every member's state
- * after each trial, and keep the fastest choice */
+/* tile shape of the batched B-form magnetic solve in the fast arithmetic: 0 = 32 x 16 cells
+ * (the default, and the shape of every single-context solve), 1 = 64 x 8, 2 = 32 x 8 */
+imex_status imex_batch_set_solve_tile(imex_batch* b, int tile);
+/* time `trial_steps` ensemble steps per candidate, one choice at a time from the best so
+ * far: the explicit mode (batched launches, or 4 / 8 / 16 streams), the B-form solve's tile
+ * shape (B form, fast arithmetic), the restart length (15 or the configured one) and, in
+ * mixed precision, the configured mixed_solves or the same with the magnetic systems' FP32
+ * form toggled; restore every member's state after each trial and keep the fastest */
 imex_status imex_batch_autotune(imex_batch* b, int trial_steps, imex_batch_tuning* out);
 /* streams in use, whether the step runs as a captured graph, batched solve launches per step */
 imex_status imex_batch_info(imex_batch* b, int* streams, int* graph_used, int* solve_launches_per_step);

@@ -111,8 +111,21 @@ def test_batch_autotune_restores_member_state():
     tuned = batch.autotune(trial_steps=1)
     print("autotune:", tuned, batch.info())
     assert tuned["streams"] in (0, 4, 8, 16) and tuned["ms_per_step"] > 0
+    assert tuned["solve_tile"] in ((32, 16), (64, 8), (32, 8))
     for sv in batch.members:
         assert sv.scalars()["timestep"] == 0  # every trial step was undone
     batch.step(2)
     _check_members(batch, probs, 2, settings, 2, 1e-10, 1e-10)
+    batch.close()
+
+
+@pytest.mark.parametrize("tile", [1, 2])
+def test_batch_solve_tile_shapes_match_single_runs(tile):
+    """The batched B-form solve on 64x8 or 32x8 tiles: the same operator on other
+    tiles, so the members still match their single runs (32x16 tiles) and the oracle."""
+    probs = _members()[:3]
+    batch = ix.Batch(probs, 2, CFG0)
+    batch.set_solve_tile(tile)
+    batch.step(2)
+    _check_members(batch, probs, 2, CFG0, 2, 1e-11, 1e-10)
     batch.close()
