@@ -425,7 +425,8 @@ __device__ __forceinline__ void flux_tile(IMEX_BLK, const DevParams& P, const De
 // chooses, the pressure and energy forms at three CTAs per SM.
 template <bool kOpen, bool kFast>
 struct k_flux_conv {
-  IMEX_BOUNDS(FNT, 0)
+  // the fast instance fits 64 registers (four CTAs per SM); the bound keeps it there
+  static constexpr int kNT = FNT, kMinB = kFast ? 4 : 0;
   static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const DevScalars* __restrict__ sc,
                                                      const double* __restrict__ w, const double* __restrict__ Qs,
                                                      double* __restrict__ ucon) {
