@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kAT) k_cell_vjp(DevParams P, CellVjp A, Fn fn)
     }
     if (any) {
       long long nb[9];
-      neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+      neighbours(P, n, nb);
       SeedLoad<L> ld{A, nb, N, {0, 0, 0, 0, 0}, 0};
       int nin = 0;
       for (int a = 0; a < kMaxArr; ++a) {
@@ -298,7 +298,8 @@ __global__ void __launch_bounds__(kAT) k_adj_flux(DevParams P, double h, double 
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double acc_a = 0.0;
   if (n < N) {
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     for (int k = 0; k < 5; ++k) lam_Qs[k * N + n] += lam_u[k * N + n];
     for (int dir = 0; dir < 2; ++dir) {
       const long long m = dir ? cid(P, i, j + 1) : cid(P, i + 1, j);
@@ -369,7 +370,8 @@ __global__ void __launch_bounds__(kAT) k_adj_recon(DevParams P, const double* __
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
   for (int k = 0; k < nvars; ++k) {
     const double* a = Q + k * N;
@@ -451,7 +453,8 @@ __global__ void k_adj_ct_faces1(DevParams P, const double* __restrict__ lam5, co
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   const long long ip = cid(P, i + 1, j), jp = cid(P, i, j + 1);
   const double bxt = lam_bx5[n] + 0.5 * lam5[5 * N + n] + 0.5 * lam5[5 * N + ip];
   const double byt = lam_by5[n] + 0.5 * lam5[6 * N + n] + 0.5 * lam5[6 * N + jp];
@@ -466,7 +469,8 @@ __global__ void k_adj_ct_faces2(DevParams P, double h, const double* __restrict_
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   const long long ip = cid(P, i + 1, j), jp = cid(P, i, j + 1);
   lam_E[n] = -(h / P.dy) * lam_bxt[n] + (h / P.dy) * lam_bxt[jp] + (h / P.dx) * lam_byt[n] - (h / P.dx) * lam_byt[ip];
 }
@@ -484,7 +488,8 @@ __global__ void k_adj_shock_max(DevParams P, const double* __restrict__ chit, co
   if (n >= P.N) return;
   const double le = lam_eta[n];
   if (le == 0.0) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   double m = 0.0;
   long long arg = -1;
   for (int di = -1; di <= 1; di++)
@@ -507,7 +512,8 @@ __global__ void k_adj_shock_tilde(DevParams P, const double* __restrict__ Q, con
   if (n >= N) return;
   const double lc = lam_chit[n];
   if (lc == 0.0) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   double m = 1.0e300;
   long long arg = -1;
   for (int di = -1; di <= 1; di++)

@@ -80,6 +80,7 @@ constexpr int NPSLOTS = 32;
 
 imex_status validate(const imex_config* c, int nx, int ny, std::string& why) {
   if (nx < 4 || ny < 4) return why = "grid must be at least 4 x 4", IMEX_ERR_INVALID;
+  if ((long long)nx * ny > 0x7fffffffLL) return why = "grid larger than 2^31 - 1 cells", IMEX_ERR_INVALID;
   if (c->RKs < 1 || c->RKs > kMaxRK) return why = "RKs must be 1, 2 or 3", IMEX_ERR_INVALID;
   if ((c->x_bc != IMEX_x_Periodic && c->x_bc != IMEX_x_Transmissive) ||
       (c->y_bc != IMEX_y_Periodic && c->y_bc != IMEX_y_Transmissive))
@@ -425,6 +426,15 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
   P.ym = P.yclamp ? 0 : 1;
   P.ylo = P.yclamp ? 0 : ny;
   P.yhi = P.yclamp ? ny - 1 : -ny;
+  {  // q = floor(n / nx) for 32-bit n: m = floor(2^32 (2^l - d) / d) + 1, l = ceil(log2 d)
+     // (Granlund and Montgomery, Division by invariant integers using multiplication, 1994)
+    const unsigned long long d = (unsigned long long)nx;
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    P.nx_magic = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1ull);
+    P.nx_sh1 = l < 1 ? l : 1;
+    P.nx_sh2 = l > 1 ? l - 1 : 0;
+  }
 
   const size_t N = ctx->N;
   const size_t R = (size_t)cfg->RKs;

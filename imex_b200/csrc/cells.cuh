@@ -17,6 +17,11 @@ __device__ __forceinline__ void neighbours(const DevParams& P, int i, int j, lon
 #pragma unroll
     for (int di = -1; di <= 1; ++di) nb[(dj + 1) * 3 + (di + 1)] = cid(P, i + di, j + dj);
 }
+__device__ __forceinline__ void neighbours(const DevParams& P, long long n, long long* nb) {
+  int i, j;
+  cell_of(P, n, i, j);
+  neighbours(P, i, j, nb);
+}
 
 // ---- B* right-hand side of MagSubsystem_UpdateB (imex_subsystems.cpp:549-615)
 enum { MR_UCON = 0, MR_QE = 1, MR_PE = 2, MR_QS = 3 };

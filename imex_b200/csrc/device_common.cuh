@@ -32,6 +32,15 @@ __device__ __forceinline__ int cjy(const DevParams& P, int j) {
 __device__ __forceinline__ long long cid(const DevParams& P, int i, int j) {
   return (long long)cix(P, i) + (long long)P.nx * cjy(P, j);
 }
+// the cell (i, j) of linear index n = i + nx j (n < 2^31): j = floor(n / nx) by the
+// multiply-high of the invariant-divisor method (DevParams::nx_magic), no integer division
+__device__ __forceinline__ void cell_of(const DevParams& P, long long n, int& i, int& j) {
+  const unsigned u = (unsigned)n;
+  const unsigned t = __umulhi(P.nx_magic, u);
+  const unsigned q = (t + ((u - t) >> P.nx_sh1)) >> P.nx_sh2;
+  j = (int)q;
+  i = (int)(u - q * (unsigned)P.nx);
+}
 // Order key of a double: unsigned comparison of keys is numeric comparison of the values.
 __device__ __forceinline__ unsigned long long dkey(double d) {
   const unsigned long long u = (unsigned long long)__double_as_longlong(d);

@@ -34,6 +34,10 @@ struct DevParams {
   // (periodic: xm = 1, xlo = nx, xhi = -nx; transmissive: xm = 0, xlo = 0, xhi = nx - 1)
   int xm, xlo, xhi, ym, ylo, yhi;
   int fast;  // imex_config.arith == IMEX_ARITH_FAST (explicit stencil kernels)
+  // division of a cell index by nx as a multiply-high and two shifts (cell_of): the magic
+  // number and shifts of Granlund and Montgomery's division by an invariant integer
+  unsigned nx_magic;
+  int nx_sh1, nx_sh2;
 };
 
 // Boundary normal faces of the transmissive directions.  The reference keeps Bx_p0 at

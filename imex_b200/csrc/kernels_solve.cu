@@ -1847,7 +1847,8 @@ struct k_pressure_tdiag {
     const double h = sc->h;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= P.N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double h00 = hh[n], hp0 = hh[cid(P, i + 1, j)], hm0 = hh[cid(P, i - 1, j)], h0p = hh[cid(P, i, j + 1)],
                  h0m = hh[cid(P, i, j - 1)];
     tdiag[n] = h * h * ((0.5 * (hp0 + h00) + 0.5 * (hm0 + h00)) / (P.dx * P.dx) +
@@ -1871,7 +1872,7 @@ struct k_pressure_rhs {
     unsigned long long kb = ~0ull, kv = ~0ull;  // identities of min
     if (n < N) {
       long long nb[9];
-      neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+      neighbours(P, n, nb);
       const double* arr[4] = {ucon, hh, rv, kin};
       auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
       double out[1];
@@ -1919,7 +1920,7 @@ struct k_momentum {
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     long long nb[9];
-    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    neighbours(P, n, nb);
     const double* arr[2] = {p, rv};
     auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
     double out[2];
@@ -1956,7 +1957,7 @@ struct k_energy_conservation {
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     long long nb[9];
-    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    neighbours(P, n, nb);
     const double* arr[2] = {p, ucon};
     auto ld = [&](int a, int k, long long m) { return arr[a][k * N + m]; };
     double out[1];
@@ -1989,7 +1990,8 @@ struct k_energy_rhs {
     const double h = sc->h;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const long long e = cid(P, i + 1, j), w = cid(P, i - 1, j), no = cid(P, i, j + 1), s = cid(P, i, j - 1);
     const double h00 = hh[n], hp0 = hh[e], hm0 = hh[w], h0p = hh[no], h0m = hh[s];
     const double U_star = ucon[4 * N + n] - 0.5 * h / P.dx * (hp0 * ucon[N + e] - hm0 * ucon[N + w]) -
@@ -2010,7 +2012,8 @@ struct k_energy_momentum {
     const double h = sc->h;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double* E = ucon + 4 * N;
     ucon[N + n] -= h * (1 / (2 * P.dx)) * (P.gamma - 1) * (E[cid(P, i + 1, j)] - E[cid(P, i - 1, j)]);
     ucon[2 * N + n] -= h * (1 / (2 * P.dy)) * (P.gamma - 1) * (E[cid(P, i, j + 1)] - E[cid(P, i, j - 1)]);
@@ -2028,7 +2031,7 @@ struct k_magnetic_rhs_B {
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     long long nb[9];
-    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    neighbours(P, n, nb);
     const double* arr[4] = {ucon, Qe, pe, Qs};
     auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
     double out[3];
@@ -2068,7 +2071,7 @@ struct k_collect_mag_fluxes {
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     long long nb[9];
-    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    neighbours(P, n, nb);
     const double* arr[3] = {ucon, Qe, pe};
     auto ld = [&](int a, int k, long long m) { return __ldg(arr[a] + k * N + m); };
     double bmax[2] = {sc->B_max_x, sc->B_max_y};
@@ -2093,7 +2096,8 @@ struct k_magnetic_rhs_A {
     const double h = sc->h;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     // every input first, so that the divisions do not serialise the loads
     const double Bxn = Qe[5 * N + n], Byn = Qe[6 * N + n], Bzn = Qe[7 * N + n];
     const double rho = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
@@ -2205,7 +2209,8 @@ struct k_local_visc {
     const long long N = P.N;
     const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const long long nbr[4] = {cid(P, i + 1, j), cid(P, i - 1, j), cid(P, i, j + 1), cid(P, i, j - 1)};
     double own[2], out[4];
     if (mode == LV_PRES) {
@@ -2241,7 +2246,8 @@ struct k_curl_A {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     auto Ak = [&](int k, int di, int dj) { return a_ghost(P, A + k * N, i + di, j + dj); };
     ucon[5 * N + n] = 1 / (2.0 * P.dy) * (Ak(2, 0, 1) - Ak(2, 0, -1));
     ucon[6 * N + n] = -1 / (2.0 * P.dx) * (Ak(2, 1, 0) - Ak(2, -1, 0));
@@ -3215,7 +3221,7 @@ __global__ void k_adj_assemble_T(Op op, DevParams P, double* __restrict__ AT) {
   const auto od = op.template as<D>();
   using OD = typename std::remove_const<decltype(od)>::type;
   long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  neighbours(P, n, nb);
   LocalTile<OD, D> t;
   local_fill(od, t, nb, nullptr, N);
   for (int o = 0; o < 9; ++o) {
@@ -3284,7 +3290,7 @@ __global__ void k_adj_coef_vjp(Op op, DevParams P, const double* __restrict__ x,
   const auto od = op.template as<D>();
   using OD = typename std::remove_const<decltype(od)>::type;
   long long nb[9];
-  neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+  neighbours(P, n, nb);
   LocalTile<OD, D> t;
   local_fill(od, t, nb, x, N);
   double m[M];
@@ -3313,7 +3319,7 @@ __global__ void k_adj_visc_vjp(Op op, DevParams P, const double* __restrict__ x,
   if (n < N) {
     op.bind();
     long long nb[9];
-    neighbours(P, (int)(n % P.nx), (int)(n / P.nx), nb);
+    neighbours(P, n, nb);
     LocalTile<Op, double> t;
     local_fill(op, t, nb, x, N);
     Op o0 = op, ox = op, oy = op;

@@ -292,7 +292,8 @@ struct k_reconstruct_prim {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     long long ix[5], iy[5];
   #pragma unroll
     for (int d = 0; d < 5; ++d) {
@@ -339,7 +340,8 @@ struct k_reconstruct_var {
     const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     const int k = blockIdx.y;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
     const double* a = Q + k * N;
     double v[5], u[5];  // both stencils loaded before the divisions of the first reconstruction
@@ -478,7 +480,8 @@ struct k_ct_corner {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     long long nb[9];
     neighbours(P, i, j, nb);
     const double* arr[3] = {fx, fy, ucon};
@@ -517,7 +520,8 @@ struct k_ct_faces {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double h = sc->h;
     const bool xb = P.xclamp && i == 0, yb = P.yclamp && j == 0;
     double e00 = __ldg(Epp + n), em0 = corner_read(P, Epp, L, i - 1, j), e0m = corner_read(P, Epp, L, i, j - 1);
@@ -581,7 +585,8 @@ struct k_ct_unstag_A {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     double Ec = 0.25 * (__ldg(Epp + n) + corner_read(P, Epp, L, i - 1, j) + corner_read(P, Epp, L, i, j - 1) +
                         corner_read(P, Epp, L, i - 1, j - 1));
     A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
@@ -599,7 +604,8 @@ struct k_ct_unstag_legacy_A {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double h = sc->h, dx = P.dx, dy = P.dy;
     const double* As = A_s + 2 * N;
     auto vxc = [&](long long m) { return __ldg(u + N + m) / __ldg(u + m); };
@@ -628,7 +634,8 @@ struct k_curl_Az {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double* Az = A + 2 * N;
     ucon[5 * N + n] = (a_ghost(P, Az, i, j + 1) - a_ghost(P, Az, i, j - 1)) / (2.0 * P.dy);
     ucon[6 * N + n] = -(a_ghost(P, Az, i + 1, j) - a_ghost(P, Az, i - 1, j)) / (2.0 * P.dx);
@@ -643,7 +650,8 @@ struct k_ct_legacy_faces {
     const long long N = P.N;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
     auto f6 = [&](const double* q, long long m) {
       double r = __ldg(q + m);
@@ -668,7 +676,8 @@ __global__ void k_ct_diag_faces(DevParams P, const double* __restrict__ w, doubl
   const long long N = P.N;
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+  int i, j;
+    cell_of(P, n, i, j);
   const double *wxL = w, *wxR = w + 8 * N, *wyL = w + 16 * N, *wyR = w + 24 * N;
   auto f6 = [&](const double* q, long long m) {  // f_full_con[6], state.cpp:152-175
     double r = __ldg(q + m);
@@ -698,7 +707,8 @@ __global__ void k_ct_diag_stats(DevParams P, const double* __restrict__ cp0, con
   const double* fx[3] = {cp0, rp0, nullptr};
   const double* fy[3] = {c0p, r0p, nullptr};
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     double e[4][3];  // component (C, R, T, total) x corner ((i, j), (i, j-1), (i-1, j))
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -874,7 +884,8 @@ __global__ void k_divergence(DevParams P, const double* __restrict__ ucon, const
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   double m = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(n % P.nx), j = (int)(n / P.nx);
+    int i, j;
+    cell_of(P, n, i, j);
     const double bxm = (P.xclamp && i == 0) ? L.bx[j] : bx[cid(P, i - 1, j)];
     const double bym = (P.yclamp && j == 0) ? L.by[i] : by[cid(P, i, j - 1)];
     double d = (bx[n] - bxm) / P.dx + (by[n] - bym) / P.dy;
