@@ -111,16 +111,46 @@ def ncu_traffic(family: str, workload: str, n: int) -> float | None:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and throttle reasons during the timed region: NVML read every 10 ms from a
+    thread (the timed region of the default workload lasts about 0.1 s), plus nvidia-smi every
+    200 ms.  Both only read the GPU's state."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h): sw power cap, hw slowdown, sw / hw thermal
+    NVML_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                 "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
+        self.nvml = []
+        self._stop = None
+        self._thread = None
+
+    def _nvml_loop(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.nvml_max = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                try:
+                    bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except Exception:
+                    bits = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.nvml.append((float(mhz), int(bits)))
+                self._stop.wait(0.01)
+            pynvml.nvmlShutdown()
+        except Exception:
+            pass
 
     def __enter__(self):
+        import threading
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
+        self._thread.start()
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
@@ -132,6 +162,9 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         self.lines = []
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -156,8 +189,15 @@ class ClockSampler:
             for name, flag in zip(names, parts[5:9]):
                 if flag.lower().startswith("active"):
                     reasons.add(name)
+        for mhz, bits in self.nvml:
+            sm.append(mhz)
+            for name, bit in self.NVML_BITS.items():
+                if bits & bit:
+                    reasons.add(name)
+        if smax is None and getattr(self, "nvml_max", None):
+            smax = float(self.nvml_max)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "nvml_samples": len(self.nvml)}
 
 
 def dist_setup():

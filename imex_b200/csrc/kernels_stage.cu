@@ -350,8 +350,12 @@ struct k_reconstruct_var {
   #pragma unroll
     for (int d = 0; d < 5; ++d) u[d] = __ldg(a + cid(P, i, j + d - 2));
     double xl, xr, yl, yr;
-    recon_1d<kFast>(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
-    recon_1d<kFast>(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
+    if (kFast && P.recon == IMEX_WENO5) {
+      weno5_fast_xy(v, u, xl, xr, yl, yr);
+    } else {
+      recon_1d<kFast>(P.recon, v[0], v[1], v[2], v[3], v[4], xl, xr, false);
+      recon_1d<kFast>(P.recon, u[0], u[1], u[2], u[3], u[4], yl, yr, vortex);
+    }
     w[(0 * 8 + k) * N + n] = xl;
     w[(1 * 8 + k) * N + n] = xr;
     w[(2 * 8 + k) * N + n] = yl;
