@@ -806,7 +806,7 @@ struct k_stage_derivative {
 // value is evaluated at p itself; for a transmissive one it is evaluated at the clamped
 // position, which lies in the same tile.
 constexpr int STX = 32, STY = 16, SHX = STX + 4, SHY = STY + 4, SCX = STX + 2, SCY = STY + 2;
-template <bool kOpen>
+template <bool kOpen, bool kFast>
 struct k_shock {
   IMEX_BOUNDS(kThreads, 0)
   static __device__ __forceinline__ void run(IMEX_BLK, DevParams Pin, const double* __restrict__ Q,
@@ -815,6 +815,8 @@ struct k_shock {
     const long long N = P.N;
     __shared__ double cf[SHY * SHX];  // c_f at (x0 - 2 + sx, y0 - 2 + sy)
     __shared__ double ch[SCY * SCX];  // chi~ at (x0 - 1 + px, y0 - 1 + py)
+    // fast arithmetic: vx, vy of the staged cells (the exact form divides at each use)
+    __shared__ double svx[kFast ? SHY * SHX : 1], svy[kFast ? SHY * SHX : 1];
     const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
     {  // each thread's cells of the halo-2 tile, every load before the first division
       constexpr int KC = (SHY * SHX + kThreads - 1) / kThreads;
@@ -829,10 +831,24 @@ struct k_shock {
       for (int k = 0; k < KC; ++k) {
         const int q = threadIdx.x + k * kThreads;
         if (q < SHY * SHX) {
-          const double p = pressure_of(P, c[k]);
-          const double a2 = eos_a2(P, c[k][0], p);
-          const double cA2 = (c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7]) / c[k][0];
-          cf[q] = sqrt(a2 + cA2);
+          if constexpr (kFast) {
+            // one reciprocal of rho per staged cell; the velocities stay in shared memory for
+            // the divergence of the ring
+            const double ir = 1.0 / c[k][0];
+            const double vx = c[k][1] * ir, vy = c[k][2] * ir, vz = c[k][3] * ir;
+            const double B2 = c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7];
+            const double e = (c[k][4] - 0.5 * c[k][0] * (vx * vx + vy * vy + vz * vz) - 0.5 * B2) * ir;
+            const double p = eos_p(P, c[k][0], e);
+            const double a2 = P.eos_type == IMEX_IDEAL_GAS ? P.gamma * p * ir : eos_a2(P, c[k][0], p);
+            cf[q] = sqrt(a2 + B2 * ir);
+            svx[q] = vx;
+            svy[q] = vy;
+          } else {
+            const double p = pressure_of(P, c[k]);
+            const double a2 = eos_a2(P, c[k][0], p);
+            const double cA2 = (c[k][5] * c[k][5] + c[k][6] * c[k][6] + c[k][7] * c[k][7]) / c[k][0];
+            cf[q] = sqrt(a2 + cA2);
+          }
         }
       }
     }
@@ -848,11 +864,18 @@ struct k_shock {
           double v = cf[(sy + dj) * SHX + sx + di];
           if (v < m) m = v;
         }
-      long long xp = cid(P, gi + 1, gj), xm = cid(P, gi - 1, gj), yp = cid(P, gi, gj + 1), ym = cid(P, gi, gj - 1);
-      // every load before the first division
-      const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
-      const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
-      double div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
+      double div_u;
+      if constexpr (kFast) {
+        // the staged neighbours hold the same (wrapped or clamped) cells as cid's maps
+        const int o = sy * SHX + sx;
+        div_u = (svx[o + 1] - svx[o - 1]) * (0.5 / P.dx) + (svy[o + SHX] - svy[o - SHX]) * (0.5 / P.dy);
+      } else {
+        long long xp = cid(P, gi + 1, gj), xm = cid(P, gi - 1, gj), yp = cid(P, gi, gj + 1), ym = cid(P, gi, gj - 1);
+        // every load before the first division
+        const double mxp = __ldg(Q + N + xp), rxp = __ldg(Q + xp), mxm = __ldg(Q + N + xm), rxm = __ldg(Q + xm);
+        const double myp = __ldg(Q + 2 * N + yp), ryp = __ldg(Q + yp), mym = __ldg(Q + 2 * N + ym), rym = __ldg(Q + ym);
+        div_u = (mxp / rxp - mxm / rxm) / (2.0 * P.dx) + (myp / ryp - mym / rym) / (2.0 * P.dy);
+      }
       double num = P.hmin * div_u + P.shock_kappa1 * m;
       double den = P.shock_kappa1 * m;
       double qv = -num / den;
@@ -1165,7 +1188,7 @@ imex_status launch_shock(imex_ctx* ctx, const double* Q, double* eta) {
   const DevParams& P = ctx->P;
   const dim3 nb((P.nx + STX - 1) / STX, (P.ny + STY - 1) / STY);
   prof_begin(ctx);
-  IMEX_LAUNCH_BC(P, k_shock, nb, kThreads, 0, ctx->stream, P, Q, eta, ctx->keep_shock_chit ? ctx->chit : nullptr);
+  IMEX_LAUNCH_BC_ARITH(P, k_shock, nb, kThreads, 0, ctx->stream, P, Q, eta, ctx->keep_shock_chit ? ctx->chit : nullptr);
   LAUNCH_CHECK(ctx, "shock detector");
   prof_end(ctx, F_SHOCK, BYTES(9), 1);
   return IMEX_OK;

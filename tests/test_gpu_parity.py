@@ -72,6 +72,16 @@ def test_gpu_fast_reconstruction_within_round_off(scheme):
     sv.close()
 
 
+def test_gpu_fast_shock_detector_within_round_off():
+    """The fast shock detector (one 1/rho per staged cell, the velocities of the divergence
+    kept in shared memory) against the reference's output: within 1e-13 relative L2."""
+    g = load_golden("fn_vortex16x12.npz")
+    sv = _fn_solver(dict(recon="Minmod", magfield="StaggerCT", arith="fast"))
+    got = np.asarray(sv.shock_detector(g["Q"]))
+    assert rel(got, g["shock"]) <= 1e-13, rel(got, g["shock"])
+    sv.close()
+
+
 def _fn_solver(settings):
     prob = vortex(16, 12)
     s = dict(prob.settings)
