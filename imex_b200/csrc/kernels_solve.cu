@@ -703,7 +703,7 @@ struct MagneticACoef {
   DevParams P;
   const DevScalars* sc;
   const double *Qe, *rho;
-  const double* irho;  // fast arithmetic: 1/rho (k_recip before the solve), else null
+  const double* irho;  // fast arithmetic: 1/rho (from k_magnetic_rhs_A, or k_recip for a prepared operator), else null
   const double* lv;  // local dissipation (GLF off): nu of the faces x+, x-, y+, y- (k_local_visc), else null
   double h, nu_x, nu_y, cx, cy;
   int add_bvisc;
@@ -2091,14 +2091,15 @@ struct k_magnetic_rhs_A {
   IMEX_BOUNDS(0, 0)
   static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const DevScalars* __restrict__ sc, const double* __restrict__ ucon,
                                    const double* __restrict__ Qe, const double* __restrict__ pe,
-                                   const double* __restrict__ A_s, double* __restrict__ b) {
+                                   const double* __restrict__ A_s, double* __restrict__ b, double* __restrict__ irho) {
     const long long N = P.N;
     const double h = sc->h;
     long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (n >= N) return;
     int i, j;
     cell_of(P, n, i, j);
-    // every input first, so that the divisions do not serialise the loads
+    // every input first, so that the divisions do not serialise the loads; irho (fast
+    // arithmetic, else null) receives 1/rho of u_con for the A-form operator
     const double Bxn = Qe[5 * N + n], Byn = Qe[6 * N + n], Bzn = Qe[7 * N + n];
     const double rho = ucon[n], m1 = ucon[N + n], m2 = ucon[2 * N + n], m3 = ucon[3 * N + n];
     const double pxp = pe[cid(P, i + 1, j)], pxm = pe[cid(P, i - 1, j)], pyp = pe[cid(P, i, j + 1)],
@@ -2110,6 +2111,7 @@ struct k_magnetic_rhs_A {
     b[n] = a0 - h * (Byn * Sz - Bzn * Sy);
     b[N + n] = a1 - h * (Bzn * Sx - Bxn * Sz);
     b[2 * N + n] = a2 - h * (Bxn * Sy - Byn * Sx);
+    if (irho) irho[n] = 1.0 / rho;
   }
 };
 // global A-viscosity maxima of prim(Qs) over real cells (implicit_operators.cpp:364-374)
@@ -2165,6 +2167,7 @@ struct k_recip {
     if (i < n) r[i] = 1.0 / a[i];
   }
 };
+constexpr int kGmaxThreads = 1024;  // one block reduces the per-CTA maxima of a whole plane
 struct k_gmax_finalize {
   IMEX_BOUNDS(0, 0)
   static __device__ __forceinline__ void run(IMEX_BLK, const double* __restrict__ partial, int nblk, DevScalars* sc) {
@@ -2173,7 +2176,7 @@ struct k_gmax_finalize {
       a = fmax(a, partial[2 * k]);
       b = fmax(b, partial[2 * k + 1]);
     }
-    __shared__ double sh[2][kThreads / 32];
+    __shared__ double sh[2][32];  // one slot per warp of up to 1024 threads
     for (int o = 16; o > 0; o >>= 1) {
       a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
       b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
@@ -2903,7 +2906,7 @@ namespace {
 }  // namespace
 // gmax_bx / gmax_by from the per-CTA maxima k_stage_combine left in partial
 imex_status gmax_finalize(imex_ctx* ctx, int nblk) {
-  launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nblk, ctx->sc);
+  launch<k_gmax_finalize>(ctx, 1, kGmaxThreads, 0, ctx->stream, ctx->partial, nblk, ctx->sc);
   LAUNCH_CHECK(ctx, "k_gmax_finalize");
   return IMEX_OK;
 }
@@ -2934,19 +2937,16 @@ imex_status mag_rhs(imex_ctx* ctx) {
       prof_begin(ctx);
       launch<k_gmax>(ctx, nred, kThreads, 0, ctx->stream, P, ctx->Qs, ctx->partial);
       LAUNCH_CHECK(ctx, "k_gmax");
-      launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
+      launch<k_gmax_finalize>(ctx, 1, kGmaxThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
       LAUNCH_CHECK(ctx, "k_gmax_finalize");
       prof_end(ctx, F_GMAX, BYTES(8), 2);
     }
     ctx->gmax_ready = false;
     prof_begin(ctx);
-    launch<k_magnetic_rhs_A>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb);
+    launch<k_magnetic_rhs_A>(ctx, nb, kThreads, 0, ctx->stream, P, ctx->sc, ctx->cons, ctx->Qe, ctx->pe, ctx->A_s, ctx->mb,
+                             P.fast ? ctx->irho : (double*)nullptr);
     LAUNCH_CHECK(ctx, "k_magnetic_rhs_A");
-    if (P.fast) {
-      launch<k_recip>(ctx, nb, kThreads, 0, ctx->stream, ctx->cons, ctx->irho, P.N);
-      LAUNCH_CHECK(ctx, "k_recip");
-    }
-    prof_end(ctx, F_MAG_RHS, BYTES(P.fast ? 16 : 14), P.fast ? 2 : 1);
+    prof_end(ctx, F_MAG_RHS, BYTES(P.fast ? 15 : 14), 1);
     return IMEX_OK;
   }
   prof_begin(ctx);
@@ -3074,7 +3074,7 @@ imex_status prepare_operator(imex_ctx* ctx, int op, double h) {
     const DevParams& P = ctx->P;
     int nred = blocks_for(P.N) < ctx->max_blocks ? blocks_for(P.N) : ctx->max_blocks;
     launch<k_gmax>(ctx, nred, kThreads, 0, ctx->stream, P, ctx->Qs, ctx->partial);
-    launch<k_gmax_finalize>(ctx, 1, kThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
+    launch<k_gmax_finalize>(ctx, 1, kGmaxThreads, 0, ctx->stream, ctx->partial, nred, ctx->sc);
     LAUNCH_CHECK(ctx, "k_gmax");
   }
   if ((op == IMEX_OP_MAGNETIC_A || op == IMEX_OP_MAGNETIC_B) &&
