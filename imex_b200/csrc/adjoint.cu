@@ -599,6 +599,24 @@ __device__ __forceinline__ void glf_quantities(const DevParams& P, const S* p, b
   S B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
   S B = sqrt(B2);
   S vv = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+  if (P.fast) {  // the fast form of k_step_reduce, operation for operation
+    const S ir = 1.0 / p[0];
+    if (first) {
+      const S a2 = P.eos_type == IMEX_IDEAL_GAS ? P.gamma * p[4] * ir : eos_a2(P, p[0], p[4]);
+      const S t = a2 + B2 * ir, tt = t * t, a4 = 4.0 * a2 * ir;
+      S disc = tt - a4 * B * B;
+      if (disc < 0) disc = 0;
+      q[0] = vv + sqrt(0.5 * (t + sqrt(disc)));
+    } else {
+      q[0] = vv;
+    }
+    const S b4 = 4 * B2 * ir;
+    q[1] = 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + b4));
+    q[2] = 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + b4));
+    q[3] = fabs(p[1]);
+    q[4] = fabs(p[2]);
+    return;
+  }
   if (first) q[0] = vv + eos_fast(P, p[0], p[4], B, B2);
   else q[0] = vv;
   q[1] = 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + 4 * B2 / p[0]));

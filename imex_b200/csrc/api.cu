@@ -435,6 +435,8 @@ imex_status imex_create(const imex_config* cfg, int nx, int ny, imex_ctx** out) 
     P.nx_sh1 = l < 1 ? l : 1;
     P.nx_sh2 = l > 1 ? l - 1 : 0;
   }
+  P.rdx = 1.0 / P.dx;
+  P.rdy = 1.0 / P.dy;
 
   const size_t N = ctx->N;
   const size_t R = (size_t)cfg->RKs;

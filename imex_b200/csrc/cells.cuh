@@ -97,11 +97,11 @@ __device__ __forceinline__ void collect_cell(const DevParams& P, double h, const
   const S Fn_x = Byn_p0 / rho_p0 * (rvx_p0 - (h / dx) * (PE(E) - PE(n))) -
                  Bxn_p0 / rho_p0 * (rvy_p0 - (h / dy) * (p_pp - p_pm));
   const S By_1 = Byn_p0 / rho_p0 *
-                 (-1.0 / dx * ((QU(E) - Q(5, E) * U(5, E)) - (QU(n) - Q(5, n) * U(5, n))) +
-                  1.0 / dy * (Bxn_pp * By1_pp - Bxn_pm * By1_pm));
+                 (-P.rdx * ((QU(E) - Q(5, E) * U(5, E)) - (QU(n) - Q(5, n) * U(5, n))) +
+                  P.rdy * (Bxn_pp * By1_pp - Bxn_pm * By1_pm));
   const S By_2 = Bxn_p0 / rho_p0 *
-                 (-1.0 / dx * (Q(5, E) * U(6, E) - Q(5, n) * U(6, n)) +
-                  1.0 / dy * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Byn_pp * By1_pp) -
+                 (-P.rdx * (Q(5, E) * U(6, E) - Q(5, n) * U(6, n)) +
+                  P.rdy * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Byn_pp * By1_pp) -
                               (0.5 * (Bxn_pm * Bx1_pm + Byn_pm * By1_pm + Bzn_pm * Bz1_pm) - Byn_pm * By1_pm)));
   const S nu_x = bmax[0] * dx;
   const S Fdiff_x = -nu_x * (U(6, E) - U(6, n)) / dx;
@@ -109,12 +109,12 @@ __device__ __forceinline__ void collect_cell(const DevParams& P, double h, const
   const S Fn_y = Bxn_0p / rho_0p * (rvy_0p - (h / dy) * (PE(No) - PE(n))) -
                  Byn_0p / rho_0p * (rvx_0p - (h / dx) * (p_pp - p_mp));
   const S Bx_1 = Bxn_0p / rho_0p *
-                 (1.0 / dx * (Bxn_pp * By1_pp - Bxn_mp * By1_mp) -
-                  1.0 / dy * ((QU(No) - Q(6, No) * U(6, No)) - (QU(n) - Q(6, n) * U(6, n))));
+                 (P.rdx * (Bxn_pp * By1_pp - Bxn_mp * By1_mp) -
+                  P.rdy * ((QU(No) - Q(6, No) * U(6, No)) - (QU(n) - Q(6, n) * U(6, n))));
   const S Bx_2 = Byn_0p / rho_0p *
-                 (1.0 / dx * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Bxn_pp * Bx1_pp) -
+                 (P.rdx * ((0.5 * (Bxn_pp * Bx1_pp + Byn_pp * By1_pp + Bzn_pp * Bz1_pp) - Bxn_pp * Bx1_pp) -
                               (0.5 * (Bxn_mp * Bx1_mp + Byn_mp * By1_mp + Bzn_mp * Bz1_mp) - Bxn_mp * Bx1_mp)) -
-                  1.0 / dy * (Q(6, No) * U(5, No) - Q(6, n) * U(5, n)));
+                  P.rdy * (Q(6, No) * U(5, No) - Q(6, n) * U(5, n)));
   const S nu_y = bmax[1] * dy;
   const S Fdiff_y = -nu_y * (U(5, No) - U(5, n)) / dy;
   out[1] = Fn_y + h * (Bx_1 + Bx_2) + Fdiff_y;
@@ -137,8 +137,8 @@ __device__ __forceinline__ void pressure_rhs_cell(const DevParams& P, double h, 
   const S rxe = ld(PR_RV, 0, e), rxn = ld(PR_RV, 0, n), rxw = ld(PR_RV, 0, w);
   const S ryo = ld(PR_RV, 1, no), ryn = ld(PR_RV, 1, n), rys = ld(PR_RV, 1, s);
   out[0] = p_star - 0.5 * (kx * kx + ky * ky + kz * kz) / rho -
-           h * (1 / P.dx * (0.5 * (hp0 + h00) * 0.5 * (rxe + rxn) - 0.5 * (hm0 + h00) * 0.5 * (rxw + rxn)) +
-                (1 / P.dy * (0.5 * (h0p + h00) * 0.5 * (ryo + ryn) - 0.5 * (h0m + h00) * 0.5 * (rys + ryn))));
+           h * (P.rdx * (0.5 * (hp0 + h00) * 0.5 * (rxe + rxn) - 0.5 * (hm0 + h00) * 0.5 * (rxw + rxn)) +
+                (P.rdy * (0.5 * (h0p + h00) * 0.5 * (ryo + ryn) - 0.5 * (h0m + h00) * 0.5 * (rys + ryn))));
 }
 
 // ---- momentum correction rho v = rho v* - h grad p (imex_subsystems.cpp:186-215)

@@ -38,6 +38,9 @@ struct DevParams {
   // number and shifts of Granlund and Montgomery's division by an invariant integer
   unsigned nx_magic;
   int nx_sh1, nx_sh2;
+  // 1 / dx and 1 / dy, divided once on the host (both sides round the quotient to nearest, so
+  // a kernel reading them gets the value its own 1.0 / dx would give)
+  double rdx, rdy;
 };
 
 // Boundary normal faces of the transmissive directions.  The reference keeps Bx_p0 at

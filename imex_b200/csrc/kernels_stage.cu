@@ -60,6 +60,7 @@ __device__ inline void block_reduce(double (&v)[K], F f, double identity) {
 // calch / calca / caldt maxima / MagneticEigenvalues over the primitive state,
 // timestep.cpp:5-148,254-273.  Max is exact, so block order does not matter.
 constexpr int kStepVals = 11;
+template <bool kFast>
 struct k_step_reduce {
   IMEX_BOUNDS(0, 0)
   static __device__ __forceinline__ void run(IMEX_BLK, DevParams P, const double* __restrict__ prim, double* __restrict__ partial) {
@@ -73,6 +74,31 @@ struct k_step_reduce {
       double B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
       double B = sqrt(B2);
       double vv = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+      if constexpr (kFast) {
+        // one 1/rho and one 1/sqrt(rho) for the cell, the shared sound and Alfven terms of
+        // the three fast speeds formed once (the exact form divides in every term)
+        const double ir = 1.0 / p[0], isr = sqrt(ir);
+        const double a2 = P.eos_type == IMEX_IDEAL_GAS ? P.gamma * p[4] * ir : eos_a2(P, p[0], p[4]);
+        const double t = a2 + B2 * ir, tt = t * t, a4 = 4.0 * a2 * ir;
+        auto cf_of = [&](double Bn) {
+          double disc = tt - a4 * Bn * Bn;
+          if (disc < 0) disc = 0;
+          return sqrt(0.5 * (t + sqrt(disc)));
+        };
+        v[0] = fmax(v[0], p[1] + cf_of(p[5]));
+        v[1] = fmax(v[1], p[2] + cf_of(p[6]));
+        v[2] = fmax(v[2], vv + cf_of(B));
+        v[3] = fmax(v[3], p[5] * isr);
+        v[4] = fmax(v[4], p[6] * isr);
+        v[5] = fmax(v[5], B * isr);
+        v[6] = fmax(v[6], fabs(p[1]));
+        v[7] = fmax(v[7], fabs(p[2]));
+        v[8] = fmax(v[8], vv);
+        const double b4 = 4 * B2 * ir;
+        v[9] = fmax(v[9], 0.5 * (fabs(p[1]) + sqrt(p[1] * p[1] + b4)));
+        v[10] = fmax(v[10], 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + b4)));
+        continue;
+      }
       double cfx = eos_fast(P, p[0], p[4], p[5], B2);
       double cfy = eos_fast(P, p[0], p[4], p[6], B2);
       double cf = eos_fast(P, p[0], p[4], B, B2);
@@ -986,7 +1012,8 @@ imex_status launch_step_prologue(imex_ctx* ctx) {
   int nblk = blocks_for(P.N);
   if (nblk > ctx->max_blocks) nblk = ctx->max_blocks;
   prof_begin(ctx);
-  launch<k_step_reduce>(ctx, nblk, kThreads, 0, ctx->stream, P, ctx->prim, ctx->partial);
+  if (P.fast) launch<k_step_reduce<true>>(ctx, nblk, kThreads, 0, ctx->stream, P, ctx->prim, ctx->partial);
+  else launch<k_step_reduce<false>>(ctx, nblk, kThreads, 0, ctx->stream, P, ctx->prim, ctx->partial);
   LAUNCH_CHECK(ctx, "k_step_reduce");
   launch<k_step_finalize>(ctx, 1, kThreads, 0, ctx->stream, P, ctx->partial, nblk, ctx->sc);
   LAUNCH_CHECK(ctx, "k_step_finalize");
