@@ -320,10 +320,11 @@ imex_status imex_shock_detector(imex_ctx* ctx, const double* Q8, double* eta);
  * ordinary context of nx[m] x ny[m] cells: its data go in and out through the usual
  * entry points (imex_upload_prim, imex_download_state, imex_divergence, ...) on the
  * handle from imex_batch_member, and it keeps its own dt, time and statistics.
- * imex_batch_step advances every member by `steps` time steps: the explicit sub-steps
- * of the members run on a pool of streams, and each implicit solve of a stage is one
- * cooperative launch for all members, in which each member owns a range of CTAs.  The
- * step is captured once into a CUDA graph and replayed.  Members must share the RK
+ * imex_batch_step advances every member by `steps` time steps: each explicit sub-step
+ * is one launch for all members (or, with imex_batch_configure(b, streams > 0, ...), the
+ * members launch their own kernels on a pool of streams), and each implicit solve of a
+ * stage is one cooperative launch for all members, in which each member owns a range of
+ * CTAs.  The step is captured once into a CUDA graph and replayed.  Members must share the RK
  * order and the magnetic form; imex_batch_step synchronises and returns the worst
  * member status (imex_batch_last_error names the member). */
 /* ---- output formats and run diagnostics (main.cpp:560-721, output.cpp)
