@@ -276,8 +276,6 @@ imex_status ct_entry(imex_ctx* ctx, double h, int variant, int needed_magfield) 
   if (!ctx) return IMEX_ERR_INVALID;
   if (ctx->P.magfield != needed_magfield)
     return set_error(ctx, IMEX_ERR_INVALID, "CT variant does not match the configured magfield");
-  if (variant >= 2 && (ctx->P.xclamp || ctx->P.yclamp))
-    return set_error(ctx, IMEX_ERR_UNSUPPORTED, "the legacy CT variants are implemented for periodic boundaries");
   imex_status s = set_h(ctx, h);
   return s != IMEX_OK ? s : launch_ct(ctx, variant);
 }

@@ -622,7 +622,8 @@ struct k_ct_unstag_A {
     A[2 * N + n] = A_s[2 * N + n] - sc->h * Ec;
   }
 };
-// Unstaggered_CT upwind A_z advection (constrained_transport.cpp:436-488)
+// Unstaggered_CT upwind A_z advection (constrained_transport.cpp:436-488); A_s is read with
+// the ghosts of bound_cond_A (constrained_transport.cpp:438), u_con with those of bound_cond_u
 __device__ __forceinline__ double vanleer_lim(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return 2.0 * a * b / (a + b);
@@ -640,21 +641,24 @@ struct k_ct_unstag_legacy_A {
     const double* As = A_s + 2 * N;
     auto vxc = [&](long long m) { return __ldg(u + N + m) / __ldg(u + m); };
     auto vyc = [&](long long m) { return __ldg(u + 2 * N + m) / __ldg(u + m); };
-    long long c = n, xm = cid(P, i - 1, j), xp = cid(P, i + 1, j), xmm = cid(P, i - 2, j), xpp = cid(P, i + 2, j);
-    long long ym = cid(P, i, j - 1), yp = cid(P, i, j + 1), ymm = cid(P, i, j - 2), ypp = cid(P, i, j + 2);
+    const long long c = n, xm = cid(P, i - 1, j), xp = cid(P, i + 1, j), ym = cid(P, i, j - 1), yp = cid(P, i, j + 1);
+    const double a00 = As[c], axm = a_ghost(P, As, i - 1, j), axp = a_ghost(P, As, i + 1, j);
+    const double axmm = a_ghost(P, As, i - 2, j), axpp = a_ghost(P, As, i + 2, j);
+    const double aym = a_ghost(P, As, i, j - 1), ayp = a_ghost(P, As, i, j + 1);
+    const double aymm = a_ghost(P, As, i, j - 2), aypp = a_ghost(P, As, i, j + 2);
     double uL = 0.5 * (vxc(xm) + vxc(c)), uR = 0.5 * (vxc(c) + vxc(xp));
-    double dAL = As[c] - As[xm], dAR = As[xp] - As[c], dALL = As[xm] - As[xmm], dARR = As[xpp] - As[xp];
+    double dAL = a00 - axm, dAR = axp - a00, dALL = axm - axmm, dARR = axpp - axp;
     double fluct_x = fmax(uL, 0.0) * dAL + fmin(uR, 0.0) * dAR;
     double corrL = 0.5 * fabs(uL) * (1.0 - fabs(uL) * h / dx) * vanleer_lim(dAL, (uL >= 0.0 ? dALL : dAR));
     double corrR = 0.5 * fabs(uR) * (1.0 - fabs(uR) * h / dx) * vanleer_lim(dAR, (uR >= 0.0 ? dAL : dARR));
     double dAdt_x = fluct_x / dx + (corrR - corrL) / dx;
     double vL = 0.5 * (vyc(ym) + vyc(c)), vR = 0.5 * (vyc(c) + vyc(yp));
-    double dAB = As[c] - As[ym], dAT = As[yp] - As[c], dABB = As[ym] - As[ymm], dATT = As[ypp] - As[yp];
+    double dAB = a00 - aym, dAT = ayp - a00, dABB = aym - aymm, dATT = aypp - ayp;
     double fluct_y = fmax(vL, 0.0) * dAB + fmin(vR, 0.0) * dAT;
     double corrB = 0.5 * fabs(vL) * (1.0 - fabs(vL) * h / dy) * vanleer_lim(dAB, (vL >= 0.0 ? dABB : dAT));
     double corrT = 0.5 * fabs(vR) * (1.0 - fabs(vR) * h / dy) * vanleer_lim(dAT, (vR >= 0.0 ? dAB : dATT));
     double dAdt_y = fluct_y / dy + (corrT - corrB) / dy;
-    A[2 * N + n] = As[c] - h * (dAdt_x + dAdt_y);
+    A[2 * N + n] = a00 - h * (dAdt_x + dAdt_y);
   }
 };
 // B = curl A_z for the unstaggered schemes (constrained_transport.cpp:533-538)

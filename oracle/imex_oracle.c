@@ -1516,12 +1516,14 @@ static double vanleer_lim(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return 2.0 * a * b / (a + b);
 }
-/* Unstaggered_CT (legacy), constrained_transport.cpp:436-498 */
+/* Unstaggered_CT (legacy), constrained_transport.cpp:436-498: A_s and A are read with the
+ * ghosts of bound_cond_A (constrained_transport.cpp:438,486), u_con with those of bound_cond_u */
 static void unstaggered_ct_legacy(double* ucon, double* A, const double* A_s, double h) {
   const size_t N = G.N;
   const double dx = G.dx, dy = G.dy;
+  const double* A2 = A + 2 * N;
 #define UA(k, ii, jj) AT(ucon, k, ii, jj)
-#define AS(ii, jj) A_s[2 * N + ID(ii, jj)]
+#define AS(ii, jj) agh(A_s + 2 * N, ii, jj)
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
       double uL = 0.5 * (UA(1, i - 1, j) / UA(0, i - 1, j) + UA(1, i, j) / UA(0, i, j));
@@ -1546,8 +1548,8 @@ static void unstaggered_ct_legacy(double* ucon, double* A, const double* A_s, do
 #undef AS
   for (int i = 0; i < G.nx; i++)
     for (int j = 0; j < G.ny; j++) {
-      ucon[5 * N + ID(i, j)] = (AT(A, 2, i, j + 1) - AT(A, 2, i, j - 1)) / (2.0 * dy);
-      ucon[6 * N + ID(i, j)] = -(AT(A, 2, i + 1, j) - AT(A, 2, i - 1, j)) / (2.0 * dx);
+      ucon[5 * N + ID(i, j)] = (agh(A2, i, j + 1) - agh(A2, i, j - 1)) / (2.0 * dy);
+      ucon[6 * N + ID(i, j)] = -(agh(A2, i + 1, j) - agh(A2, i - 1, j)) / (2.0 * dx);
     }
 }
 
@@ -2032,7 +2034,7 @@ double ora_div_error(void) {
 
 /* Boundary conditions per direction (config.hpp:36-37 ordinals): 0 Transmissive or
  * 2 Periodic.  Call after ora_setup and before ora_load_prim.  Every magnetic form runs
- * with either; the legacy CT variants (fn_substep 6) are restated for periodic runs. */
+ * with either, the legacy CT variants (fn_substep 6) included. */
 int ora_set_bc(int x_bc, int y_bc) {
   if (!G.ready) return 1;
   if ((x_bc != 0 && x_bc != 2) || (y_bc != 0 && y_bc != 2)) return 2;

@@ -162,14 +162,22 @@ def test_port_refuses_unsupported_boundaries():
 
 
 @pytest.mark.skipif(not RefSolver.available(), reason="oracle/_ref not built")
-def test_port_matches_live_reference_legacy_ct():
-    """Staggered_CT / Unstaggered_CT (reachable only via commented call sites main.cpp:500,504)."""
+@pytest.mark.parametrize("bc", [None, ("x_Transmissive", "y_Transmissive"), ("x_Periodic", "y_Transmissive"),
+                                ("x_Transmissive", "y_Periodic")], ids=["periodic", "open", "y_open", "x_open"])
+def test_port_matches_live_reference_legacy_ct(bc):
+    """Staggered_CT / Unstaggered_CT (reachable only via commented call sites main.cpp:500,504),
+    on periodic and transmissive boundaries (the boundary lines of the faces come from each
+    solver's own state, so both solvers take the same step first)."""
+    from imex_b200.problems import open_blast
     for magfield in ("StaggerCT", "UnStaggerCT"):
-        prob = vortex(16)
+        prob = vortex(16) if bc is None else open_blast(16, 12)
         settings = dict(recon="VanLeer", magfield=magfield)
+        if bc is not None:
+            settings.update(x_bc=bc[0], y_bc=bc[1])
         ref = make_solver("ref", prob, 2, settings)
         port = make_solver("port", prob, 2, settings)
         ref.step(snapshots=True)
+        port.step(snapshots=True)
         Q = ref.snapshot(0, "combine", "Qe")
         Qs = ref.snapshot(0, "combine", "Qs")
         u = ref.snapshot(0, "pressure", "u_con")
@@ -181,6 +189,10 @@ def test_port_matches_live_reference_legacy_ct():
         p = port.substep(6, h, 0, u, Q, Qs, bx, by, bxq, byq, A, As)
         for key in ("u_con", "bx", "by", "A"):
             np.testing.assert_array_equal(p[key], r[key], err_msg=f"{magfield} {key}")
+        if bc is not None:  # the boundary lines of the open directions
+            for u, v, kind in zip(port.boundary_faces(), ref.boundary_faces(), bc):
+                if kind.endswith("Transmissive"):
+                    np.testing.assert_array_equal(u, v, err_msg=f"{magfield} {kind} boundary faces")
 
 
 def test_port_rejects_unsupported_configurations():
