@@ -7,7 +7,8 @@
 //     shared cell functions (cells.cuh) evaluated in dual numbers with L inputs seeded per
 //     pass, the products scattered to the inputs;
 //   * the explicit fluxes: per face, the Rusanov flux in dual numbers, then the
-//     reconstruction per variable and direction;
+//     reconstruction per variable and direction (ConsState) or per stencil cell with its 8
+//     conserved planes seeded through con2pri, recon and pri2con (PrimState);
 //   * each implicit solve A(theta) x = b: one transposed GMRES solve A^T mu = lambda_x on
 //     the assembled transposed stencil, lambda_b = mu, lambda_theta -= mu^T d(A x)/d theta;
 //     the nested Newton is differentiated at its converged p through its active set
@@ -18,9 +19,9 @@
 // Across steps: checkpoints every K steps, the steps of a segment recomputed from its
 // checkpoint, and each step recomputed once more with its sub-step states kept.
 //
-// Supported: PressureFormula, StaggerCT (B-form magnetic solve), ConsState reconstruction,
-// ideal gas, GLF, MaterialSpeedp or no pressure viscosity, fixed dt, FP64, no
-// Energy_Modify; other configurations return IMEX_ERR_UNSUPPORTED.
+// Supported: PressureFormula, StaggerCT (B-form magnetic solve), ConsState or PrimState
+// reconstruction, ideal gas, GLF, MaterialSpeedp or no pressure viscosity, fixed dt, FP64,
+// no Energy_Modify; other configurations return IMEX_ERR_UNSUPPORTED.
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -396,6 +397,81 @@ __global__ void __launch_bounds__(kAT) k_adj_recon(DevParams P, const double* __
     }
     lam_Q[k * N + n] += acc;
   }
+}
+
+// reconstruction (PrimState): each face state is pri2con(recon(con2pri(Q))) with every
+// primitive variable reconstructed on its own (reconstruction.cpp:272-281), so a face state's
+// conserved planes depend on all 8 conserved planes of each stencil cell.  lambda_Q(c) +=
+// sum over the cells whose 5-point stencils contain c of lambda_w(cell) dw(cell)/dQ(c), with
+// the 8 planes of Q(c) seeded at once; only the first nvars conserved planes of the face
+// states carry adjoints (the fluxes take cell B from u_con).
+__global__ void __launch_bounds__(kAT) k_adj_recon_prim(DevParams P, const double* __restrict__ Q,
+                                                       const double* __restrict__ lam_w,
+                                                       double* __restrict__ lam_Q, int nvars) {
+  const long long N = P.N;
+  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  int i, j;
+  cell_of(P, n, i, j);
+  const bool vortex = P.recon == IMEX_Minmod && P.vortex_minmod;
+  Dual<8> dp[8];  // primitive state of cell n, seeded on its conserved planes
+  {
+    Dual<8> c[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      c[k] = Dual<8>(Q[k * N + n]);
+      c[k].d[k] = 1.0;
+    }
+    con2pri(P, dp, c);
+  }
+  double acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+  for (int dir = 0; dir < 2; ++dir) {
+    for (int dd = -2; dd <= 2; ++dd) {
+      const long long m = dir ? cid(P, i, j + dd) : cid(P, i + dd, j);
+      const double* lwl = lam_w + (long long)(dir ? 2 : 0) * 8 * N + m;
+      const double* lwr = lam_w + (long long)(dir ? 3 : 1) * 8 * N + m;
+      bool any = false;
+      for (int k = 0; k < nvars; ++k) any = any || lwl[k * N] != 0.0 || lwr[k * N] != 0.0;
+      if (!any) continue;
+      double pv[5][8];
+      bool seed[5];
+#pragma unroll
+      for (int t = 0; t < 5; ++t) {
+        const long long idx = dir ? cid(P, i, j + dd + t - 2) : cid(P, i + dd + t - 2, j);
+        seed[t] = idx == n;
+        double c[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) c[k] = Q[k * N + idx];
+        con2pri(P, pv[t], c);
+      }
+      Dual<8> wl[8], wr[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        Dual<8> u[5];
+#pragma unroll
+        for (int t = 0; t < 5; ++t) u[t] = seed[t] ? dp[k] : Dual<8>(pv[t][k]);
+        recon_1d(P.recon, u[0], u[1], u[2], u[3], u[4], wl[k], wr[k], dir ? vortex : false);
+      }
+      Dual<8> cl[8], cr[8];
+      pri2con(P, cl, wl);
+      pri2con(P, cr, wr);
+      for (int k = 0; k < nvars; ++k) {
+        const double a = lwl[k * N], b = lwr[k * N];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] += a * cl[k].d[q] + b * cr[k].d[q];
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) lam_Q[q * N + n] += acc[q];
+}
+// the reconstruction's adjoint for the configured reconstructed state
+void adj_recon(const DevParams& P, cudaStream_t st, const double* Q, const double* lam_w, double* lam_Q) {
+  const int nb = ablocks(P.N);
+  if (P.reconstate == IMEX_PrimState) k_adj_recon_prim<<<nb, kAT, 0, st>>>(P, Q, lam_w, lam_Q, 5);
+  else k_adj_recon<<<nb, kAT, 0, st>>>(P, Q, lam_w, lam_Q, 5);
 }
 
 // ------------------------------------------------------------------ linear sub-steps
@@ -1076,7 +1152,7 @@ imex_status reverse_step(Adj& W) {
     if ((s = copy(W, W.w, ctx->w, 32 * N)) != IMEX_OK) return s;
     prof_begin(ctx);
     k_adj_flux<1><<<nb, kAT, 0, st>>>(P, h, S.sc.a_max, W.w, S.u2, W.l3, W.lw, W.l2, W.lQs, W.dscal + 0);
-    k_adj_recon<<<nb, kAT, 0, st>>>(P, S.Qe, W.lw, W.lQe, 5);
+    adj_recon(P, st, S.Qe, W.lw, W.lQe);
     ACHECK(ctx, "adjoint pressure flux");
     prof_end(ctx, F_ADJ_FLUX, 0.0, 2);
     for (int k = 5; k < 8; ++k) k_axpy_planes<<<ablocks(N), kAT, 0, st>>>((long long)N, W.l2 + k * N, W.l3 + k * N, 1.0);
@@ -1124,7 +1200,7 @@ imex_status reverse_step(Adj& W) {
     zero(W, W.lw, 32 * N);
     prof_begin(ctx);
     k_adj_flux<0><<<nb, kAT, 0, st>>>(P, h, S.sc.a_max, W.w, S.u1, W.l1, W.lw, nullptr, W.lQs, W.dscal + 0);
-    k_adj_recon<<<nb, kAT, 0, st>>>(P, S.Qe, W.lw, W.lQe, 5);
+    adj_recon(P, st, S.Qe, W.lw, W.lQe);
     ACHECK(ctx, "adjoint convective flux");
     prof_end(ctx, F_ADJ_FLUX, 0.0, 2);
     // (10) p(Qe) of the combination
@@ -1183,7 +1259,6 @@ imex_status supported(imex_ctx* ctx) {
   const char* why = nullptr;
   if (P.formula != IMEX_PressureFormula) why = "the pressure formula";
   else if (P.magfield != IMEX_StaggerCT) why = "StaggerCT";
-  else if (P.reconstate != IMEX_ConsState) why = "ConsState reconstruction";
   else if (P.eos_type != IMEX_IDEAL_GAS) why = "the ideal-gas EOS";
   else if (!P.GLF) why = "GLF";
   else if (P.add_pvisc == IMEX_AlfvenSpeedp) why = "MaterialSpeedp or Noaddvisp pressure viscosity";

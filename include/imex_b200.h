@@ -303,8 +303,9 @@ imex_status imex_gmres(imex_ctx* ctx, int op, double* x, const double* b, imex_s
  * IMEX_ERR_INVALID before any work, and imex_last_error names the bytes needed.
  *
  * The first call on a device resolves the array's address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture.
- * The barrier state in the array is cleared by every call.  The array is shared by
+ * with that device current).  Every call synchronizes the context's stream and then
+ * reads the solve's status, so it must not be made while that stream is being
+ * captured into a CUDA graph.  The barrier state in the array is cleared by every call.  The array is shared by
  * every context and stream on a device, so calls that overlap in time on one
  * device race: serialise them. */
 #define IMEX_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
@@ -372,8 +373,9 @@ int imex_history_write_host(const char* path, int n, const int* steps, const dou
  * stencil, the nested Newton differentiated at its converged pressure through its active set
  * (with the Cor.1 slope Mbig), the GLF maxima through the cells attaining them.  Checkpoints
  * every `checkpoint_every` steps; each segment and each step are recomputed from them.
- * Supported: PressureFormula, StaggerCT, ConsState, ideal gas, GLF, MaterialSpeedp or
- * Noaddvisp, fixed_dt > 0, FP64, Energy_Modify off (else IMEX_ERR_UNSUPPORTED).
+ * Supported: PressureFormula, StaggerCT, ConsState or PrimState, ideal gas, GLF,
+ * MaterialSpeedp or Noaddvisp, fixed_dt > 0, FP64, Energy_Modify off, periodic boundaries
+ * (else IMEX_ERR_UNSUPPORTED).
  * The run starts from the context's current state and leaves it at the final state. */
 typedef struct imex_adjoint_opts {
   int nsteps;            /* steps of the forward run (>= 1) */

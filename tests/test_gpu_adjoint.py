@@ -107,6 +107,26 @@ def test_adjoint_rk3_floor_off_minmod():
     _fd_check(_base(20, seed=9), 3, cfg, steps=2, ckpt=1)
 
 
+def _generic(n=20, seed=19):
+    """The vortex with each non-uniform primitive plane perturbed by a smooth random field.
+    PrimState reconstructs v, p and B themselves, and their vortex profiles have exactly
+    equal neighbours on the symmetry lines, where the limiters have a kink (zero slope)."""
+    p = vortex(n)
+    rng = np.random.default_rng(seed)
+    prim = p.prim.copy()
+    for k in (0, 1, 2, 4, 5, 6):
+        prim[k] = prim[k] + 0.02 * np.abs(prim[k]).max() * _smooth(rng, p.ny, p.nx)
+    return types.SimpleNamespace(**{**vars(p), "prim": prim})
+
+
+@pytest.mark.parametrize("rks,extra", [(2, dict(recon="VanLeer")), (3, dict(recon="WENO5"))],
+                         ids=["vanleer_rk2", "weno5_rk3"])
+def test_adjoint_prim_state_reconstruction(rks, extra):
+    """PrimState: each face state is pri2con of the reconstructed primitive variables
+    (reconstruction.cpp:272-281), so the reconstruction's adjoint couples all 8 planes."""
+    _fd_check(_generic(20), rks, dict(CFG, reconstate="PrimState", **extra), steps=2, ckpt=1)
+
+
 def test_adjoint_checkpointing_does_not_change_the_gradient():
     prob = _base(20, seed=13)
     rho_t, B_t = _targets(prob, 2, CFG, 4)
