@@ -3,9 +3,9 @@
 // The forward step is a chain of sub-steps (main.cpp:335-561); its adjoint runs the chain
 // backwards, each sub-step contributing its vector-Jacobian product:
 //   * stencil sub-steps (magnetic right-hand side, CollectMagFluxes, pressure right-hand
-//     side, momentum, DefinitionofU, the CT corner EMF, the frozen coefficients): the
-//     shared cell functions (cells.cuh) evaluated in dual numbers with L inputs seeded per
-//     pass, the products scattered to the inputs;
+//     side, momentum, DefinitionofU or ConservationofU, the CT corner EMF, the frozen
+//     coefficients): the shared cell functions (cells.cuh) evaluated in dual numbers with L
+//     inputs seeded per pass, the products scattered to the inputs;
 //   * the explicit fluxes: per face, the Rusanov flux in dual numbers, then the
 //     reconstruction per variable and direction (ConsState) or per stencil cell with its 8
 //     conserved planes seeded through con2pri, recon and pri2con (PrimState);
@@ -21,7 +21,8 @@
 //
 // Supported: PressureFormula, StaggerCT (B-form magnetic solve), ConsState or PrimState
 // reconstruction, ideal gas, GLF, MaterialSpeedp or no pressure viscosity, fixed dt, FP64,
-// no Energy_Modify; other configurations return IMEX_ERR_UNSUPPORTED.
+// either energy update, Energy_Modify on or off; other configurations return
+// IMEX_ERR_UNSUPPORTED.
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -203,6 +204,14 @@ struct FnEnergyDef {
   __device__ void operator()(const DevParams& P, const CellVjp&, const long long* nb, const S*, Ld& ld,
                              S* out) const {
     energy_define_cell<S>(P, nb, ld, out);
+  }
+};
+struct FnEnergyCons {
+  static constexpr int NOUT = 1, NS = 0;
+  template <class S, class Ld>
+  __device__ void operator()(const DevParams& P, const CellVjp& A, const long long* nb, const S*, Ld& ld,
+                             S* out) const {
+    energy_conservation_cell<S>(P, A.h, nb, ld, out);
   }
 };
 struct FnCtCorner {
@@ -500,13 +509,16 @@ __global__ void k_adj_combine(DevParams P, Coefs T, int rks, double dt, const do
     lam_HsB[((long long)r * 2 + 1) * N + n] += T.ai[r] * dt * lby;
   }
 }
-// stage derivative (main.cpp:539-555): Hs = (u - Qs) / adt, HsB = (faces - faces_Qs) / adt
+// stage derivative (main.cpp:539-555): Hs = (u - Qs) / adt, HsB = (faces - faces_Qs) / adt.
+// With Energy_Modify (main.cpp:528-534) u is the CT output with E += (|B|^2 - |B_save|^2) / 2
+// first (bct = cell B of the CT output, bsave = cell B after the magnetic sub-system).
 __global__ void k_adj_derivative(DevParams P, int rks, double adt, const double* __restrict__ lam_out,
                                  const double* __restrict__ lam_bx_out, const double* __restrict__ lam_by_out,
                                  const double* __restrict__ lam_Hs, const double* __restrict__ lam_HsB,
                                  double* __restrict__ lam5, double* __restrict__ lam_Qs, double* __restrict__ lam_bx5,
                                  double* __restrict__ lam_by5, double* __restrict__ lam_bxQs,
-                                 double* __restrict__ lam_byQs) {
+                                 double* __restrict__ lam_byQs, const double* __restrict__ bct,
+                                 const double* __restrict__ bsave, double* __restrict__ lam_bsave) {
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -514,6 +526,13 @@ __global__ void k_adj_derivative(DevParams P, int rks, double adt, const double*
     const double lh = lam_Hs[((long long)rks * 8 + k) * N + n] / adt;
     lam5[k * N + n] = (lam_out ? lam_out[k * N + n] : 0.0) + lh;
     lam_Qs[k * N + n] = -lh;
+  }
+  if (bct) {
+    const double le = lam5[4 * N + n];
+    for (int k = 0; k < 3; ++k) {
+      lam5[(5 + k) * N + n] += le * bct[k * N + n];
+      lam_bsave[k * N + n] = -le * bsave[k * N + n];
+    }
   }
   const double hx = lam_HsB[((long long)rks * 2 + 0) * N + n] / adt, hy = lam_HsB[((long long)rks * 2 + 1) * N + n] / adt;
   lam_bx5[n] = (lam_bx_out ? lam_bx_out[n] : 0.0) + hx;
@@ -765,6 +784,7 @@ struct State {
 };
 struct StageSnap {
   double *Qe, *Qs, *bxQs, *byQs, *pe, *u1, *u2, *Fx, *Fy, *u3, *hh, *eta, *chit, *cf, *b1, *p1, *um, *b2, *p2;
+  double* bct = nullptr;  // cell B after CT (Energy_Modify only)
   DevScalars sc;  // scalars of the stage (h, maxima)
   double mbig1, mbig2;
   bool second;
@@ -786,6 +806,7 @@ struct Adj {
   double *l5, *l4, *lum, *l3, *l2, *l1;              // u_con after each sub-step (8 planes each)
   double *lbx5, *lby5, *lbxt, *lbyt, *lE, *lFx, *lFy;
   double *lQe, *lQs, *lbxQs, *lbyQs, *lpe, *lhh, *leta, *lchit, *lcf, *lrv, *lp, *mu, *w, *lw, *AT, *vdiag;
+  double* lbsave = nullptr;  // adjoint of the cell B saved after the magnetic sub-system (Energy_Modify)
   double* dscal;  // device scalars: [0..4] GLF maxima adjoints, [5..6] magnetic cx cy, [7..8] pressure cvx cvy,
                   // [9] Mbig sum, [10] b min, [11] J
   unsigned long long* didx;  // argmax / argmin cells
@@ -837,6 +858,7 @@ imex_status workspace(Adj& W) {
     AL(S.Qe, 8 * N); AL(S.Qs, 8 * N); AL(S.bxQs, N); AL(S.byQs, N); AL(S.pe, N); AL(S.u1, 8 * N); AL(S.u2, 8 * N);
     AL(S.Fx, N); AL(S.Fy, N); AL(S.u3, 8 * N); AL(S.hh, N); AL(S.eta, N); AL(S.chit, N); AL(S.cf, N); AL(S.b1, N);
     AL(S.p1, N); AL(S.um, 8 * N); AL(S.b2, N); AL(S.p2, N);
+    if (ctx->P.Energy_Modify) AL(S.bct, 3 * N);
   }
   AL(W.step_prim, 8 * N);
   AL(W.lam_u, 8 * N); AL(W.lam_bx, N); AL(W.lam_by, N);
@@ -847,6 +869,7 @@ imex_status workspace(Adj& W) {
   AL(W.lQe, 8 * N); AL(W.lQs, 8 * N); AL(W.lbxQs, N); AL(W.lbyQs, N); AL(W.lpe, N); AL(W.lhh, N); AL(W.leta, N);
   AL(W.lchit, N); AL(W.lcf, N); AL(W.lrv, 3 * N); AL(W.lp, N); AL(W.mu, 3 * N); AL(W.w, 32 * N); AL(W.lw, 32 * N);
   AL(W.AT, 81 * N); AL(W.vdiag, N); AL(W.dscal, 16);
+  if (ctx->P.Energy_Modify) AL(W.lbsave, 3 * N);
 #undef AL
   if (s != IMEX_OK) return s;
   void* q = nullptr;
@@ -911,6 +934,7 @@ imex_status forward_step_snap(Adj& W) {
     if ((s = run_gmres(ctx, op, x, b)) != IMEX_OK) return s;
     copy(W, S.u2, ctx->cons, 8 * N);
     if ((s = mag_out(ctx)) != IMEX_OK) return s;
+    if (ctx->P.Energy_Modify) copy(W, ctx->Bsave, ctx->cons + 5 * N, 3 * N);  // as run_stage does
     copy(W, S.Fx, ctx->Fx, N);
     copy(W, S.Fy, ctx->Fy, N);
     if ((s = launch_flux_update(ctx, 1)) != IMEX_OK) return s;
@@ -936,6 +960,7 @@ imex_status forward_step_snap(Adj& W) {
     }
     if ((s = pres_part3(ctx)) != IMEX_OK) return s;
     if ((s = launch_ct(ctx, 0)) != IMEX_OK) return s;
+    if (ctx->P.Energy_Modify) copy(W, S.bct, ctx->cons + 5 * N, 3 * N);
     if ((s = launch_stage_derivative(ctx, r)) != IMEX_OK) return s;
   }
   return imex_end_step(ctx);
@@ -1044,7 +1069,7 @@ imex_status reverse_step(Adj& W) {
     prof_begin(ctx);
     k_adj_derivative<<<nb, kAT, 0, st>>>(P, r, adt, last ? W.lam_u : nullptr, last ? W.lam_bx : nullptr,
                                           last ? W.lam_by : nullptr, W.lam_Hs, W.lam_HsB, W.l5, W.lQs, W.lbx5, W.lby5,
-                                          W.lbxQs, W.lbyQs);
+                                          W.lbxQs, W.lbyQs, S.bct, S.u2 + 5 * N, W.lbsave);
     // (2) CT faces and cell B
     k_adj_ct_faces1<<<nb, kAT, 0, st>>>(P, W.l5, W.lbx5, W.lby5, W.lbxt, W.lbyt, W.lbxQs, W.lbyQs, W.l4);
     k_adj_ct_faces2<<<nb, kAT, 0, st>>>(P, h, W.lbxt, W.lbyt, W.lE);
@@ -1075,7 +1100,15 @@ imex_status reverse_step(Adj& W) {
     zero(W, W.lQe, 8 * N);
     zero(W, W.lpe, N);
     const double* pE = S.second ? S.p2 : S.p1;
-    {  // DefinitionofU at the final pressure, on um
+    if (P.U_update == IMEX_ConservationofU) {
+      // E -= h div(h_e rho v) at the final pressure, on um (its E plane is the old energy)
+      CellVjp A = cv_empty();
+      cv_arr(A, EC_P, pE, W.lp, 0, 1, OFS_CROSS);
+      cv_arr_planes(A, EC_UCON, S.um, W.lum, 0x17u, OFS_CROSS);  // rho, mx, my, E
+      A.lam_out[0] = W.l4 + 4 * N;
+      A.h = h;
+      if ((s = run_cell_vjp<4>(ctx, A, FnEnergyCons{})) != IMEX_OK) return s;
+    } else {  // DefinitionofU at the final pressure, on um
       CellVjp A = cv_empty();
       cv_arr(A, ED_P, pE, W.lp, 0, 1, OFS_C);
       cv_arr(A, ED_UCON, S.um, W.lum, 0, 8, OFS_C);
@@ -1156,6 +1189,8 @@ imex_status reverse_step(Adj& W) {
     ACHECK(ctx, "adjoint pressure flux");
     prof_end(ctx, F_ADJ_FLUX, 0.0, 2);
     for (int k = 5; k < 8; ++k) k_axpy_planes<<<ablocks(N), kAT, 0, st>>>((long long)N, W.l2 + k * N, W.l3 + k * N, 1.0);
+    if (P.Energy_Modify)  // the saved B is the B of u2
+      k_axpy_planes<<<ablocks(3 * N), kAT, 0, st>>>((long long)(3 * N), W.l2 + 5 * N, W.lbsave, 1.0);
     // (6) CollectMagFluxes
     {
       CellVjp A = cv_empty();
@@ -1263,8 +1298,6 @@ imex_status supported(imex_ctx* ctx) {
   else if (!P.GLF) why = "GLF";
   else if (P.add_pvisc == IMEX_AlfvenSpeedp) why = "MaterialSpeedp or Noaddvisp pressure viscosity";
   else if (!(P.fixed_dt > 0.0)) why = "a fixed time step (fixed_dt > 0)";
-  else if (P.Energy_Modify) why = "Energy_Modify off";
-  else if (P.U_update != IMEX_DefinitionofU) why = "DefinitionofU";
   else if (ctx->cfg.precision != IMEX_PRECISION_FP64) why = "FP64 precision";
   else if (P.xclamp || P.yclamp) why = "periodic boundaries";
   if (!why) return IMEX_OK;

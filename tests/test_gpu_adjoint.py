@@ -127,6 +127,18 @@ def test_adjoint_prim_state_reconstruction(rks, extra):
     _fd_check(_generic(20), rks, dict(CFG, reconstate="PrimState", **extra), steps=2, ckpt=1)
 
 
+def test_adjoint_conservation_of_u():
+    """ConservationofU (imex_subsystems.cpp:303-392): the energy is advanced by the central
+    flux of the enthalpy at the final pressure instead of being redefined from it."""
+    _fd_check(_base(20, seed=23), 2, dict(CFG, U_update="ConservationofU"), steps=2, ckpt=1)
+
+
+def test_adjoint_energy_modify():
+    """Energy_Modify (main.cpp:528-534): E += (|B_CT|^2 - |B_saved|^2) / 2 before the stage
+    derivative, with B_saved the cell B after the magnetic sub-system."""
+    _fd_check(_base(20, seed=29), 2, dict(CFG, Energy_Modify=1), steps=2, ckpt=1)
+
+
 def test_adjoint_checkpointing_does_not_change_the_gradient():
     prob = _base(20, seed=13)
     rho_t, B_t = _targets(prob, 2, CFG, 4)
