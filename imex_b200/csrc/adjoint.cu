@@ -20,7 +20,7 @@
 // checkpoint, and each step recomputed once more with its sub-step states kept.
 //
 // Supported: PressureFormula, StaggerCT (B-form magnetic solve), ConsState or PrimState
-// reconstruction, ideal gas, GLF, MaterialSpeedp or no pressure viscosity, fixed dt, FP64,
+// reconstruction, ideal gas, GLF, any pressure viscosity, fixed dt, FP64,
 // either energy update, Energy_Modify on or off; other configurations return
 // IMEX_ERR_UNSUPPORTED.
 #include <cstdio>
@@ -688,7 +688,9 @@ __global__ void k_min_reduce(long long N, const double* __restrict__ b, double* 
 
 // ------------------------------------------------------------------ GLF maxima (step prologue)
 // per-cell quantities of k_step_reduce (timestep.cpp:5-148,254-273) in the same arithmetic:
-// 0 a_max (ch on the first step, v_max after), 1 B_max_x, 2 B_max_y, 3 vx_max, 4 vy_max
+// 0 a_max (ch on the first step, v_max after), 1 B_max_x, 2 B_max_y, 3 vx_max, 4 vy_max,
+// 5 cA_x, 6 cA_y (the Alfven maxima of the AlfvenSpeedp pressure viscosity)
+constexpr int kGlfQ = 7;
 template <class S>
 __device__ __forceinline__ void glf_quantities(const DevParams& P, const S* p, bool first, S* q) {
   S B2 = p[5] * p[5] + p[6] * p[6] + p[7] * p[7];
@@ -710,6 +712,9 @@ __device__ __forceinline__ void glf_quantities(const DevParams& P, const S* p, b
     q[2] = 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + b4));
     q[3] = fabs(p[1]);
     q[4] = fabs(p[2]);
+    const S isr = sqrt(ir);
+    q[5] = p[5] * isr;
+    q[6] = p[6] * isr;
     return;
   }
   if (first) q[0] = vv + eos_fast(P, p[0], p[4], B, B2);
@@ -718,31 +723,33 @@ __device__ __forceinline__ void glf_quantities(const DevParams& P, const S* p, b
   q[2] = 0.5 * (fabs(p[2]) + sqrt(p[2] * p[2] + 4 * B2 / p[0]));
   q[3] = fabs(p[1]);
   q[4] = fabs(p[2]);
+  q[5] = p[5] / sqrt(p[0]);
+  q[6] = p[6] / sqrt(p[0]);
 }
 struct GlfMax {
-  double v[5];
+  double v[kGlfQ];
 };
 __global__ void k_adj_argmax(DevParams P, const double* __restrict__ prim, GlfMax mx, int first,
                              unsigned long long* __restrict__ idx) {
   const long long N = P.N;
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= N) return;
-  double p[8], q[5];
+  double p[8], q[kGlfQ];
   load_cell<8>(prim, N, n, p);
   glf_quantities(P, p, first != 0, q);
-  for (int s = 0; s < 5; ++s)
+  for (int s = 0; s < kGlfQ; ++s)
     if (q[s] == mx.v[s]) atomicMin(idx + s, (unsigned long long)n);
 }
 // lambda of each maximum -> its cell, through prim = con2pri(cons)
 __global__ void k_adj_glf(DevParams P, const double* __restrict__ cons, const unsigned long long* __restrict__ idx,
                           const double* __restrict__ lam_s, int first, double* __restrict__ lam_cons) {
   const int s = threadIdx.x;
-  if (s >= 5) return;
+  if (s >= kGlfQ) return;
   const double ls = lam_s[s];
   const unsigned long long c = idx[s];
   if (ls == 0.0 || c >= (unsigned long long)P.N) return;
   const long long N = P.N;
-  Dual<8> u[8], p[8], q[5];
+  Dual<8> u[8], p[8], q[kGlfQ];
   for (int k = 0; k < 8; ++k) {
     u[k] = Dual<8>(cons[k * N + c]);
     u[k].d[k] = 1.0;
@@ -807,9 +814,10 @@ struct Adj {
   double *lbx5, *lby5, *lbxt, *lbyt, *lE, *lFx, *lFy;
   double *lQe, *lQs, *lbxQs, *lbyQs, *lpe, *lhh, *leta, *lchit, *lcf, *lrv, *lp, *mu, *w, *lw, *AT, *vdiag;
   double* lbsave = nullptr;  // adjoint of the cell B saved after the magnetic sub-system (Energy_Modify)
-  double* dscal;  // device scalars: [0..4] GLF maxima adjoints, [5..6] magnetic cx cy, [7..8] pressure cvx cvy,
+  double* dscal;  // device scalars: [0..4] GLF maxima adjoints, [5..6] magnetic cx cy (then the cA_x cA_y
+                  // maxima adjoints), [7..8] pressure cvx cvy,
                   // [9] Mbig sum, [10] b min, [11] J
-  unsigned long long* didx;  // argmax / argmin cells
+  unsigned long long* didx;  // argmax cells of the kGlfQ maxima, [7] argmin of b
   double* hscal;             // pinned mirror of dscal
 };
 
@@ -1268,7 +1276,13 @@ imex_status reverse_step(Adj& W) {
       W.hscal[3] += W.hscal[7] * (P.dx / (P.dx * P.dx));
       W.hscal[4] += W.hscal[8] * (P.dy / (P.dy * P.dy));
     }
-    e = cudaMemcpyAsync(W.dscal, W.hscal, 5 * sizeof(double), cudaMemcpyHostToDevice, st);
+    // slots 5 and 6 (the magnetic viscosity's, taken into 1 and 2 above) now carry cA_x, cA_y
+    W.hscal[5] = W.hscal[6] = 0.0;
+    if (P.add_pvisc == IMEX_AlfvenSpeedp) {  // cvx = cA_x dx / dx^2
+      W.hscal[5] = W.hscal[7] * (P.dx / (P.dx * P.dx));
+      W.hscal[6] = W.hscal[8] * (P.dy / (P.dy * P.dy));
+    }
+    e = cudaMemcpyAsync(W.dscal, W.hscal, kGlfQ * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_check(ctx, e, "adjoint maxima");
     const bool first = W.step_sc.timestep <= 1;
     GlfMax mx{};
@@ -1277,7 +1291,9 @@ imex_status reverse_step(Adj& W) {
     mx.v[2] = W.step_sc.B_max_y;
     mx.v[3] = W.step_sc.vx_max;
     mx.v[4] = W.step_sc.vy_max;
-    e = cudaMemsetAsync(W.didx, 0xff, 5 * sizeof(unsigned long long), st);
+    mx.v[5] = W.step_sc.cA_x;
+    mx.v[6] = W.step_sc.cA_y;
+    e = cudaMemsetAsync(W.didx, 0xff, kGlfQ * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return cuda_check(ctx, e, "adjoint maxima");
     k_adj_argmax<<<nb, kAT, 0, st>>>(P, W.step_prim, mx, first ? 1 : 0, W.didx);
     // cons at the step start = pri2con(prim) (cons_n of the prologue)
@@ -1296,7 +1312,6 @@ imex_status supported(imex_ctx* ctx) {
   else if (P.magfield != IMEX_StaggerCT) why = "StaggerCT";
   else if (P.eos_type != IMEX_IDEAL_GAS) why = "the ideal-gas EOS";
   else if (!P.GLF) why = "GLF";
-  else if (P.add_pvisc == IMEX_AlfvenSpeedp) why = "MaterialSpeedp or Noaddvisp pressure viscosity";
   else if (!(P.fixed_dt > 0.0)) why = "a fixed time step (fixed_dt > 0)";
   else if (ctx->cfg.precision != IMEX_PRECISION_FP64) why = "FP64 precision";
   else if (P.xclamp || P.yclamp) why = "periodic boundaries";

@@ -373,9 +373,9 @@ int imex_history_write_host(const char* path, int n, const int* steps, const dou
  * stencil, the nested Newton differentiated at its converged pressure through its active set
  * (with the Cor.1 slope Mbig), the GLF maxima through the cells attaining them.  Checkpoints
  * every `checkpoint_every` steps; each segment and each step are recomputed from them.
- * Supported: PressureFormula, StaggerCT, ConsState or PrimState, ideal gas, GLF,
- * MaterialSpeedp or Noaddvisp, fixed_dt > 0, FP64, DefinitionofU or ConservationofU,
- * Energy_Modify on or off, periodic boundaries (else IMEX_ERR_UNSUPPORTED).
+ * Supported: PressureFormula, StaggerCT, ConsState or PrimState, ideal gas, GLF, any
+ * pressure viscosity, fixed_dt > 0, FP64, DefinitionofU or ConservationofU, Energy_Modify
+ * on or off, periodic boundaries (else IMEX_ERR_UNSUPPORTED).
  * The run starts from the context's current state and leaves it at the final state. */
 typedef struct imex_adjoint_opts {
   int nsteps;            /* steps of the forward run (>= 1) */

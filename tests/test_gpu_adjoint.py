@@ -139,6 +139,12 @@ def test_adjoint_energy_modify():
     _fd_check(_base(20, seed=29), 2, dict(CFG, Energy_Modify=1), steps=2, ckpt=1)
 
 
+def test_adjoint_alfven_speed_pressure_viscosity():
+    """AlfvenSpeedp: the pressure operator's viscosity scales with the step's Alfven maxima
+    max Bx / sqrt(rho) and max By / sqrt(rho), whose adjoints go to the cells attaining them."""
+    _fd_check(_base(20, seed=31), 2, dict(CFG, add_pvisc="AlfvenSpeedp"), steps=2, ckpt=1)
+
+
 def test_adjoint_checkpointing_does_not_change_the_gradient():
     prob = _base(20, seed=13)
     rho_t, B_t = _targets(prob, 2, CFG, 4)
