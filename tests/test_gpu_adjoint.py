@@ -184,8 +184,8 @@ def test_adjoint_vjp_is_linear_in_the_cotangent():
 
 def test_adjoint_rejects_unsupported_configurations():
     prob = vortex(16)
-    for extra in (dict(fixed_dt=0.0), dict(magfield="PotentialA"), dict(eos_type="REDLICH_KWONG"),
-                  dict(precision="mixed")):
+    for extra in (dict(fixed_dt=0.0), dict(magfield="PotentialA"), dict(magfield="UnStaggerCT"),
+                  dict(eos_type="REDLICH_KWONG"), dict(GLF=0), dict(precision="mixed")):
         sv = ix.Solver.for_problem(prob, 2, dict(CFG, **extra))
         with pytest.raises(ix.ImexError) as err:
             sv.adjoint_run(1, prob.prim[0], prob.prim[5:8])
